@@ -1,0 +1,422 @@
+"""ctypes binding of a BEAGLE-style C API.
+
+The same table binds two libraries that share one calling convention:
+
+* ``libbeagle_b200.so`` -- this package's C-ABI (``include/beagle_b200.h``),
+  whose entry points are the ``beagle.h`` calls renamed ``beagleB200*``;
+* a stock ``libhmsbeagle.so`` (``beagle*`` names, ``libhmsbeagle/beagle.h``),
+  which the test-suite uses to run the reference CPU implementation.
+
+Arguments are numpy arrays (converted to contiguous float64 / int32) or plain
+Python numbers; every call returns the library's ``int`` code and raises
+``BeagleError`` on a negative one unless ``check=False`` is passed.
+"""
+
+import ctypes
+import numpy as np
+
+_i = ctypes.c_int
+_l = ctypes.c_long
+_d = ctypes.c_double
+_p = ctypes.c_void_p
+
+# name -> argtypes (all return int unless listed in _RESTYPES)
+_SIGS = {
+    "FinalizeInstance": [_i],
+    "Finalize": [],
+    "SetCPUThreadCount": [_i, _i],
+    "SetTipStates": [_i, _i, _p],
+    "SetTipPartials": [_i, _i, _p],
+    "SetPartials": [_i, _i, _p],
+    "GetPartials": [_i, _i, _i, _p],
+    "SetRootPrePartials": [_i, _p, _p, _i],
+    "SetEigenDecomposition": [_i, _i, _p, _p, _p],
+    "SetStateFrequencies": [_i, _i, _p],
+    "SetCategoryWeights": [_i, _i, _p],
+    "SetCategoryRates": [_i, _p],
+    "SetCategoryRatesWithIndex": [_i, _i, _p],
+    "SetPatternWeights": [_i, _p],
+    "SetPatternPartitions": [_i, _i, _p],
+    "ConvolveTransitionMatrices": [_i, _p, _p, _p, _i],
+    "AddTransitionMatrices": [_i, _p, _p, _p, _i],
+    "TransposeTransitionMatrices": [_i, _p, _p, _i],
+    "UpdateTransitionMatrices": [_i, _i, _p, _p, _p, _p, _i],
+    "UpdateTransitionMatricesWithModelCategories": [_i, _p, _p, _p, _p, _p, _i],
+    "UpdateTransitionMatricesWithMultipleModels": [_i, _p, _p, _p, _p, _p, _p, _i],
+    "SetTransitionMatrix": [_i, _i, _p, _d],
+    "SetDifferentialMatrix": [_i, _i, _p],
+    "GetTransitionMatrix": [_i, _i, _p],
+    "SetTransitionMatrices": [_i, _p, _p, _p, _i],
+    "UpdatePartials": [_i, _p, _i, _i],
+    "UpdatePrePartials": [_i, _p, _i, _i],
+    "UpdatePartialsByPartition": [_i, _p, _i],
+    "UpdatePrePartialsByPartition": [_i, _p, _i],
+    "WaitForPartials": [_i, _p, _i],
+    "AccumulateScaleFactors": [_i, _p, _i, _i],
+    "AccumulateScaleFactorsByPartition": [_i, _p, _i, _i, _i],
+    "RemoveScaleFactors": [_i, _p, _i, _i],
+    "RemoveScaleFactorsByPartition": [_i, _p, _i, _i, _i],
+    "ResetScaleFactors": [_i, _i],
+    "ResetScaleFactorsByPartition": [_i, _i, _i],
+    "CopyScaleFactors": [_i, _i, _i],
+    "GetScaleFactors": [_i, _i, _p],
+    "CalculateRootLogLikelihoods": [_i, _p, _p, _p, _p, _i, _p],
+    "CalculateRootLogLikelihoodsByPartition": [_i, _p, _p, _p, _p, _p, _i, _i, _p, _p],
+    "CalculateEdgeDerivatives": [_i, _p, _p, _p, _p, _i, _p, _p, _p],
+    "CalculateCrossProductDerivative": [_i, _p, _p, _p, _p, _p, _i, _p, _p],
+    "CalculateEdgeLogLikelihoods": [_i, _p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p, _p],
+    "CalculateEdgeLogLikelihoodsByPartition": [_i] + [_p] * 9 + [_i, _i] + [_p] * 6,
+    "GetLogLikelihood": [_i, _p],
+    "GetDerivatives": [_i, _p, _p],
+    "GetSiteLogLikelihoods": [_i, _p],
+    "GetSiteDerivatives": [_i, _p, _p],
+    "GetCudaStream": [_i, _p],
+}
+
+ERRORS = {
+    -1: "BEAGLE_ERROR_GENERAL", -2: "BEAGLE_ERROR_OUT_OF_MEMORY",
+    -3: "BEAGLE_ERROR_UNIDENTIFIED_EXCEPTION", -4: "BEAGLE_ERROR_UNINITIALIZED_INSTANCE",
+    -5: "BEAGLE_ERROR_OUT_OF_RANGE", -6: "BEAGLE_ERROR_NO_RESOURCE",
+    -7: "BEAGLE_ERROR_NO_IMPLEMENTATION", -8: "BEAGLE_ERROR_FLOATING_POINT",
+}
+
+
+class BeagleError(RuntimeError):
+    def __init__(self, call, code):
+        super().__init__(f"{call} returned {code} ({ERRORS.get(code, 'unknown')})")
+        self.code = code
+
+
+class InstanceDetails(ctypes.Structure):
+    """Layout of ``BeagleInstanceDetails`` (libhmsbeagle/beagle.h:216-226)."""
+    _fields_ = [("resourceNumber", _i), ("resourceName", ctypes.c_char_p),
+                ("implName", ctypes.c_char_p), ("implDescription", ctypes.c_char_p),
+                ("flags", _l)]
+
+
+class Resource(ctypes.Structure):
+    """Layout of ``BeagleResource`` (libhmsbeagle/beagle.h:231-236)."""
+    _fields_ = [("name", ctypes.c_char_p), ("description", ctypes.c_char_p),
+                ("supportFlags", _l), ("requiredFlags", _l)]
+
+
+class ResourceList(ctypes.Structure):
+    _fields_ = [("list", ctypes.POINTER(Resource)), ("length", _i)]
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_p)
+
+
+class BeagleLib:
+    """A loaded BEAGLE-style library, with symbols ``<prefix><Name>``."""
+
+    def __init__(self, path, prefix, mode=ctypes.RTLD_GLOBAL):
+        self.path = path
+        self.prefix = prefix
+        self.lib = ctypes.CDLL(path, mode=mode)
+        self.fn = {}
+        for name, args in _SIGS.items():
+            f = getattr(self.lib, prefix + name, None)
+            if f is None:
+                continue
+            f.argtypes = args
+            f.restype = _i
+            self.fn[name] = f
+        ci = getattr(self.lib, prefix + "CreateInstance")
+        ci.argtypes = [_i] * 9 + [_p, _i, _l, _l, ctypes.POINTER(InstanceDetails)]
+        ci.restype = _i
+        self.fn["CreateInstance"] = ci
+        rl = getattr(self.lib, prefix + "GetResourceList")
+        rl.argtypes = []
+        rl.restype = ctypes.POINTER(ResourceList)
+        self.fn["GetResourceList"] = rl
+
+    def resources(self):
+        rl = self.fn["GetResourceList"]().contents
+        return [(rl.list[i].name.decode(), rl.list[i].supportFlags, rl.list[i].requiredFlags)
+                for i in range(rl.length)]
+
+    def create(self, tipCount, partialsBufferCount, compactBufferCount, stateCount,
+               patternCount, eigenBufferCount, matrixBufferCount, categoryCount,
+               scaleBufferCount, resources=None, preferenceFlags=0, requirementFlags=0):
+        info = InstanceDetails()
+        res = None if resources is None else _i32(resources)
+        nres = 0 if resources is None else len(resources)
+        h = self.fn["CreateInstance"](tipCount, partialsBufferCount, compactBufferCount,
+                                      stateCount, patternCount, eigenBufferCount,
+                                      matrixBufferCount, categoryCount, scaleBufferCount,
+                                      _ptr(res), nres, preferenceFlags, requirementFlags,
+                                      ctypes.byref(info))
+        if h < 0:
+            raise BeagleError(self.prefix + "CreateInstance", h)
+        return Instance(self, h, info, dict(
+            tipCount=tipCount, bufferCount=partialsBufferCount + compactBufferCount,
+            stateCount=stateCount, patternCount=patternCount,
+            categoryCount=categoryCount))
+
+
+class Instance:
+    """One instance of a BeagleLib; methods mirror the beagle.h calls."""
+
+    def __init__(self, blib, handle, info, dims):
+        self.blib = blib
+        self.h = handle
+        self.info = info
+        self.impl_name = info.implName.decode() if info.implName else ""
+        self.flags = info.flags
+        self._keep = []           # output arrays an ASYNCH instance fills at its next sync
+        self.__dict__.update(dims)
+
+    def _call(self, name, *args, check=True):
+        code = self.blib.fn[name](self.h, *args)
+        if check and code < 0:
+            raise BeagleError(self.blib.prefix + name, code)
+        return code
+
+    def __del__(self):
+        try:
+            self.finalize()
+        except Exception:
+            pass
+
+    def finalize(self):
+        if self.h is not None and self.h >= 0:
+            self._call("FinalizeInstance")
+            self.h = None
+            self._keep = []
+
+    # data in
+    def setCPUThreadCount(self, n):
+        return self._call("SetCPUThreadCount", n)
+
+    def setTipStates(self, tip, states):
+        a = _i32(states)
+        return self._call("SetTipStates", tip, _ptr(a))
+
+    def setTipPartials(self, tip, partials):
+        a = _f64(partials)
+        return self._call("SetTipPartials", tip, _ptr(a))
+
+    def setPartials(self, buf, partials):
+        a = _f64(partials)
+        return self._call("SetPartials", buf, _ptr(a))
+
+    def getPartials(self, buf, scaleIndex=-1):
+        out = np.zeros(self.categoryCount * self.patternCount * self.stateCount)
+        self._call("GetPartials", buf, scaleIndex, _ptr(out))
+        return out
+
+    def setRootPrePartials(self, bufs, freqIdx, check=True):
+        b, f = _i32(bufs), _i32(freqIdx)
+        return self._call("SetRootPrePartials", _ptr(b), _ptr(f), len(b), check=check)
+
+    def setEigenDecomposition(self, e, evec, ivec, evals):
+        a, b, c = _f64(evec), _f64(ivec), _f64(evals)
+        return self._call("SetEigenDecomposition", e, _ptr(a), _ptr(b), _ptr(c))
+
+    def setStateFrequencies(self, i, f):
+        a = _f64(f)
+        return self._call("SetStateFrequencies", i, _ptr(a))
+
+    def setCategoryWeights(self, i, w):
+        a = _f64(w)
+        return self._call("SetCategoryWeights", i, _ptr(a))
+
+    def setCategoryRates(self, r):
+        a = _f64(r)
+        return self._call("SetCategoryRates", _ptr(a))
+
+    def setCategoryRatesWithIndex(self, i, r):
+        a = _f64(r)
+        return self._call("SetCategoryRatesWithIndex", i, _ptr(a))
+
+    def setPatternWeights(self, w):
+        a = _f64(w)
+        return self._call("SetPatternWeights", _ptr(a))
+
+    def setPatternPartitions(self, n, parts):
+        a = _i32(parts)
+        return self._call("SetPatternPartitions", n, _ptr(a))
+
+    # matrices
+    def updateTransitionMatrices(self, e, probIdx, d1Idx, d2Idx, lengths):
+        p = _i32(probIdx)
+        d1 = None if d1Idx is None else _i32(d1Idx)
+        d2 = None if d2Idx is None else _i32(d2Idx)
+        t = _f64(lengths)
+        return self._call("UpdateTransitionMatrices", e, _ptr(p), _ptr(d1), _ptr(d2),
+                          _ptr(t), len(p))
+
+    def updateTransitionMatricesWithMultipleModels(self, eig, rateIdx, probIdx, d1Idx,
+                                                   d2Idx, lengths):
+        e, r, p = _i32(eig), _i32(rateIdx), _i32(probIdx)
+        d1 = None if d1Idx is None else _i32(d1Idx)
+        d2 = None if d2Idx is None else _i32(d2Idx)
+        t = _f64(lengths)
+        return self._call("UpdateTransitionMatricesWithMultipleModels", _ptr(e), _ptr(r),
+                          _ptr(p), _ptr(d1), _ptr(d2), _ptr(t), len(p))
+
+    def setTransitionMatrix(self, m, mat, padded=1.0):
+        a = _f64(mat)
+        return self._call("SetTransitionMatrix", m, _ptr(a), float(padded))
+
+    def setDifferentialMatrix(self, m, mat):
+        a = _f64(mat)
+        return self._call("SetDifferentialMatrix", m, _ptr(a))
+
+    def setTransitionMatrices(self, idx, mats, pads):
+        i, m, p = _i32(idx), _f64(mats), _f64(pads)
+        return self._call("SetTransitionMatrices", _ptr(i), _ptr(m), _ptr(p), len(i))
+
+    def getTransitionMatrix(self, m):
+        out = np.zeros(self.categoryCount * self.stateCount * self.stateCount)
+        self._call("GetTransitionMatrix", m, _ptr(out))
+        return out
+
+    def transposeTransitionMatrices(self, inIdx, outIdx, check=True):
+        a, b = _i32(inIdx), _i32(outIdx)
+        return self._call("TransposeTransitionMatrices", _ptr(a), _ptr(b), len(a),
+                          check=check)
+
+    def convolveTransitionMatrices(self, first, second, result, check=True):
+        a, b, c = _i32(first), _i32(second), _i32(result)
+        return self._call("ConvolveTransitionMatrices", _ptr(a), _ptr(b), _ptr(c), len(a),
+                          check=check)
+
+    # partials
+    def updatePartials(self, ops, cumulativeScaleIndex=-1, check=True):
+        a = _i32(ops).reshape(-1)
+        return self._call("UpdatePartials", _ptr(a), len(a) // 7, cumulativeScaleIndex,
+                          check=check)
+
+    def updatePrePartials(self, ops, cumulativeScaleIndex=-1, check=True):
+        a = _i32(ops).reshape(-1)
+        return self._call("UpdatePrePartials", _ptr(a), len(a) // 7, cumulativeScaleIndex,
+                          check=check)
+
+    def updatePartialsByPartition(self, ops, check=True):
+        a = _i32(ops).reshape(-1)
+        return self._call("UpdatePartialsByPartition", _ptr(a), len(a) // 9, check=check)
+
+    def updatePrePartialsByPartition(self, ops, check=True):
+        a = _i32(ops).reshape(-1)
+        return self._call("UpdatePrePartialsByPartition", _ptr(a), len(a) // 9, check=check)
+
+    def waitForPartials(self, bufs):
+        a = _i32(bufs)
+        code = self._call("WaitForPartials", _ptr(a), len(a))
+        self._keep = []
+        return code
+
+    # scale factors
+    def resetScaleFactors(self, idx):
+        return self._call("ResetScaleFactors", idx)
+
+    def resetScaleFactorsByPartition(self, idx, part):
+        return self._call("ResetScaleFactorsByPartition", idx, part)
+
+    def accumulateScaleFactors(self, idxs, cumulative):
+        a = _i32(idxs)
+        return self._call("AccumulateScaleFactors", _ptr(a), len(a), cumulative)
+
+    def accumulateScaleFactorsByPartition(self, idxs, cumulative, part):
+        a = _i32(idxs)
+        return self._call("AccumulateScaleFactorsByPartition", _ptr(a), len(a), cumulative,
+                          part)
+
+    def removeScaleFactors(self, idxs, cumulative):
+        a = _i32(idxs)
+        return self._call("RemoveScaleFactors", _ptr(a), len(a), cumulative)
+
+    def removeScaleFactorsByPartition(self, idxs, cumulative, part):
+        a = _i32(idxs)
+        return self._call("RemoveScaleFactorsByPartition", _ptr(a), len(a), cumulative, part)
+
+    def copyScaleFactors(self, dst, src):
+        return self._call("CopyScaleFactors", dst, src)
+
+    def getScaleFactors(self, idx):
+        out = np.zeros(self.patternCount)
+        self._call("GetScaleFactors", idx, _ptr(out))
+        return out
+
+    # reductions
+    def calculateRootLogLikelihoods(self, bufs, cw, sf, cum, check=True):
+        b, w, f, c = _i32(bufs), _i32(cw), _i32(sf), _i32(cum)
+        out = np.zeros(1)
+        code = self._call("CalculateRootLogLikelihoods", _ptr(b), _ptr(w), _ptr(f), _ptr(c),
+                          len(b), _ptr(out), check=check)
+        return (code, float(out[0])) if not check else float(out[0])
+
+    def calculateRootLogLikelihoodsByPartition(self, bufs, cw, sf, cum, parts):
+        b, w, f, c, p = _i32(bufs), _i32(cw), _i32(sf), _i32(cum), _i32(parts)
+        byp = np.zeros(len(p))
+        tot = np.zeros(1)
+        self._call("CalculateRootLogLikelihoodsByPartition", _ptr(b), _ptr(w), _ptr(f),
+                   _ptr(c), _ptr(p), len(p), 1, _ptr(byp), _ptr(tot))
+        return byp, float(tot[0])
+
+    def calculateEdgeDerivatives(self, post, pre, dmat, cw, per_site=True, sums=True,
+                                 sumsq=True, check=True):
+        a, b, d, w = _i32(post), _i32(pre), _i32(dmat), _i32(cw)
+        n = len(a)
+        o1 = np.zeros(n * self.patternCount) if per_site else None
+        o2 = np.zeros(n) if sums else None
+        o3 = np.zeros(n) if sumsq else None
+        self._call("CalculateEdgeDerivatives", _ptr(a), _ptr(b), _ptr(d), _ptr(w), n,
+                   _ptr(o1), _ptr(o2), _ptr(o3), check=check)
+        self._keep.append((o2, o3))
+        return (None if o1 is None else o1.reshape(n, self.patternCount)), o2, o3
+
+    def calculateEdgeLogLikelihoods(self, parent, child, prob, d1, d2, cw, sf, cum,
+                                    check=True):
+        arr = [_i32([parent]), _i32([child]), _i32([prob]),
+               None if d1 is None else _i32([d1]), None if d2 is None else _i32([d2]),
+               _i32([cw]), _i32([sf]), _i32([cum])]
+        o = np.zeros(1)
+        o1 = np.zeros(1) if d1 is not None else None
+        o2 = np.zeros(1) if d2 is not None else None
+        code = self._call("CalculateEdgeLogLikelihoods", *[_ptr(x) for x in arr], 1,
+                          _ptr(o), _ptr(o1), _ptr(o2), check=check)
+        return (code, float(o[0]), None if o1 is None else float(o1[0]),
+                None if o2 is None else float(o2[0]))
+
+    def getLogLikelihood(self, check=True):
+        o = np.zeros(1)
+        code = self._call("GetLogLikelihood", _ptr(o), check=False)
+        self._keep = []
+        if check and code < 0 and code != -8:
+            raise BeagleError(self.blib.prefix + "GetLogLikelihood", code)
+        return float(o[0])
+
+    def getSiteLogLikelihoods(self):
+        out = np.zeros(self.patternCount)
+        self._call("GetSiteLogLikelihoods", _ptr(out))
+        return out
+
+    def cudaStream(self):
+        """The instance's cudaStream_t as an int (libbeagle_b200 only)."""
+        out = ctypes.c_void_p()
+        self._call("GetCudaStream", ctypes.byref(out))
+        return out.value or 0
+
+    def getDerivatives(self):
+        o1, o2 = np.zeros(1), np.zeros(1)
+        self._call("GetDerivatives", _ptr(o1), _ptr(o2))
+        self._keep = []
+        return float(o1[0]), float(o2[0])
+
+    def getSiteDerivatives(self, second=False):
+        o1 = np.zeros(self.patternCount)
+        o2 = np.zeros(self.patternCount) if second else None
+        self._call("GetSiteDerivatives", _ptr(o1), _ptr(o2))
+        return o1, o2

@@ -1,0 +1,822 @@
+// Host side of one B200 instance.  See b200_instance.h.
+//
+// Every call validates its indices on the host before anything reaches the
+// device (the reference GPU implementation does not; out-of-range indices
+// there are undefined behaviour), converts caller arrays into the device
+// layout, and enqueues work on the instance's stream.  Calls that return
+// results synchronise that stream; the others return as soon as the work is
+// queued (the caller's arrays have been copied by then).
+#include "b200_instance.h"
+
+#include <cmath>
+#include <cstring>
+#include <algorithm>
+
+namespace b200 {
+
+enum {
+    kSuccess = 0, kErrGeneral = -1, kErrOOM = -2, kErrRange = -5, kErrNoImpl = -7,
+    kErrFP = -8,
+};
+
+// Flag bits (values of libhmsbeagle/beagle.h:132-177).
+constexpr long F_SINGLE = 1L << 0, F_DOUBLE = 1L << 1, F_SYNCH = 1L << 2, F_ASYNCH = 1L << 3;
+constexpr long F_EIGEN_REAL = 1L << 4, F_EIGEN_COMPLEX = 1L << 5;
+constexpr long F_SCALING_MANUAL = 1L << 6, F_SCALING_AUTO = 1L << 7, F_SCALING_ALWAYS = 1L << 8;
+constexpr long F_SCALERS_RAW = 1L << 9, F_SCALERS_LOG = 1L << 10;
+constexpr long F_VECTOR_NONE = 1L << 12, F_THREADING_NONE = 1L << 14;
+constexpr long F_PROCESSOR_GPU = 1L << 16;
+constexpr long F_INVEVEC_STANDARD = 1L << 20, F_INVEVEC_TRANSPOSED = 1L << 21;
+constexpr long F_FRAMEWORK_CUDA = 1L << 22, F_SCALING_DYNAMIC = 1L << 25;
+constexpr long F_PARALLELOPS_GRID = 1L << 29;
+constexpr long F_PRE_MANUAL = 1L << 30, F_PRE_AUTO = 1L << 31;
+
+#define CK(call)                                                   \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) {                                   \
+            (void)cudaGetLastError();                              \
+            return e_ == cudaErrorMemoryAllocation ? kErrOOM : kErrGeneral; \
+        }                                                          \
+    } while (0)
+
+// Dispatch a templated launcher on the instance precision.
+#define LAUNCH(fn, ...) (dbl_ ? fn<double>(__VA_ARGS__) : fn<float>(__VA_ARGS__))
+
+// ------------------------------------------------------------------ DevBuf
+cudaError_t DevBuf::reserve(size_t n) {
+    if (n <= bytes) return cudaSuccess;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    last.clear();
+    size_t want = std::max<size_t>(n, 256);
+    want = (want + 255) & ~size_t(255);
+    cudaError_t e = cudaMalloc(&ptr, want);
+    if (e == cudaSuccess) bytes = want;
+    return e;
+}
+
+cudaError_t DevBuf::upload(const void* src, size_t n, cudaStream_t s) {
+    cudaError_t e = reserve(n);
+    if (e != cudaSuccess) return e;
+    if (last.size() == n && n > 0 && std::memcmp(last.data(), src, n) == 0) return cudaSuccess;
+    e = cudaMemcpyAsync(ptr, src, n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) last.assign((const uint8_t*)src, (const uint8_t*)src + n);
+    return e;
+}
+
+void DevBuf::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    last.clear();
+}
+
+// -------------------------------------------------------------- lifetime
+Instance::~Instance() {
+    cudaSetDevice(device_);
+    if (stream_) cudaStreamSynchronize(stream_);
+    for (void* p : owned_) cudaFree(p);
+    void* bufs[] = {d_part_pool_, d_mat_, d_scale_, d_cube_, d_evals_, d_rates_, d_catw_,
+                    d_freqs_, d_patw_, d_site_, d_site1_, d_site2_};
+    for (void* p : bufs)
+        if (p) cudaFree(p);
+    for (DevBuf* b : {&t_ops_post_, &t_ops_pre_, &t_jobs_, &t_deriv_, &t_idx_, &t_ptr_,
+                      &scratch_, &out_, &site_d_})
+        b->release();
+    if (h_out_) cudaFreeHost(h_out_);
+    for (auto& c : chunks_) cudaFreeHost(c.first);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+int Instance::create(int tipCount, int partialsBufferCount, int compactBufferCount,
+                     int stateCount, int patternCount, int eigenBufferCount,
+                     int matrixBufferCount, int categoryCount, int scaleBufferCount, int device,
+                     long pref, long req) {
+    if (tipCount < 1 || stateCount < 2 || patternCount < 1 || categoryCount < 1 ||
+        eigenBufferCount < 1 || matrixBufferCount < 0 || scaleBufferCount < 0 ||
+        partialsBufferCount < 0 || compactBufferCount < 0 ||
+        partialsBufferCount + compactBufferCount <= tipCount)
+        return kErrRange;
+    // Requirements this resource cannot meet.
+    const long unsupported = F_EIGEN_COMPLEX | F_SCALING_AUTO | F_SCALING_ALWAYS |
+                             F_SCALING_DYNAMIC | (1L << 11) /*SSE*/ | (1L << 24) /*AVX*/ |
+                             (1L << 15) /*CPU*/ | (1L << 23) /*OpenCL*/ | (1L << 27) /*FW CPU*/ |
+                             (1L << 13) /*OpenMP*/;
+    if (req & unsupported) return kErrNoImpl;
+    if ((req & F_SINGLE) && (req & F_DOUBLE)) return kErrNoImpl;
+    if (stateCount > 64) return kErrNoImpl;
+    // Precision: a single-precision requirement or preference selects the mixed
+    // path (FP32 partials, FP64 matrices formation and reductions).
+    dbl_ = !((req & F_SINGLE) || (!(req & F_DOUBLE) && (pref & F_SINGLE)));
+    log_scalers_ = ((pref | req) & F_SCALERS_LOG) != 0;
+    invevec_t_ = ((pref | req) & F_INVEVEC_TRANSPOSED) != 0;
+    pre_auto_ = ((pref | req) & F_PRE_AUTO) != 0;
+    async_ = ((pref | req) & F_ASYNCH) != 0;
+    flags_ = F_PROCESSOR_GPU | F_FRAMEWORK_CUDA | F_EIGEN_REAL | F_SCALING_MANUAL |
+             F_VECTOR_NONE | F_THREADING_NONE | F_PARALLELOPS_GRID |
+             (((pref | req) & F_ASYNCH) ? F_ASYNCH : F_SYNCH) |
+             (dbl_ ? F_DOUBLE : F_SINGLE) | (log_scalers_ ? F_SCALERS_LOG : F_SCALERS_RAW) |
+             (invevec_t_ ? F_INVEVEC_TRANSPOSED : F_INVEVEC_STANDARD) |
+             (pre_auto_ ? F_PRE_AUTO : F_PRE_MANUAL);
+
+    device_ = device;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        (void)cudaGetLastError();
+        return -6;   // BEAGLE_ERROR_NO_RESOURCE
+    }
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) return -6;
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+
+    N_ = tipCount;
+    nbuf_ = partialsBufferCount + compactBufferCount;
+    S_ = stateCount;
+    Sg_ = (stateCount + 3) / 4 * 4;
+    P_ = patternCount;
+    Pp_ = (patternCount + kPatternPad - 1) / kPatternPad * kPatternPad;
+    C_ = categoryCount;
+    neig_ = eigenBufferCount;
+    nmat_ = matrixBufferCount;
+    nscale_ = scaleBufferCount;
+    rsz_ = dbl_ ? 8 : 4;
+    part_bytes_ = (size_t)Pp_ * C_ * Sg_ * rsz_;
+    mat_bytes_ = (size_t)C_ * Sg_ * Sg_ * rsz_;
+
+    partials_.assign(nbuf_, nullptr);
+    states_.assign(nbuf_, nullptr);
+    const int ninternal = nbuf_ - N_;
+    CK(cudaMalloc(&d_part_pool_, part_bytes_ * ninternal));
+    CK(cudaMemsetAsync(d_part_pool_, 0, part_bytes_ * ninternal, stream_));
+    for (int b = N_; b < nbuf_; ++b)
+        partials_[b] = (char*)d_part_pool_ + part_bytes_ * (size_t)(b - N_);
+    if (nmat_ > 0) {
+        CK(cudaMalloc(&d_mat_, mat_bytes_ * nmat_));
+        CK(cudaMemsetAsync(d_mat_, 0, mat_bytes_ * nmat_, stream_));
+    }
+    mat_pad_.assign(nmat_, 1.0);
+    if (nscale_ > 0) {
+        CK(cudaMalloc(&d_scale_, sizeof(double) * Pp_ * nscale_));
+        CK(cudaMemsetAsync(d_scale_, 0, sizeof(double) * Pp_ * nscale_, stream_));
+    }
+    CK(cudaMalloc(&d_cube_, sizeof(double) * (size_t)neig_ * S_ * S_ * S_));
+    CK(cudaMalloc(&d_evals_, sizeof(double) * neig_ * S_));
+    CK(cudaMalloc(&d_rates_, sizeof(double) * neig_ * C_));
+    CK(cudaMalloc(&d_catw_, sizeof(double) * neig_ * C_));
+    CK(cudaMalloc(&d_freqs_, sizeof(double) * neig_ * S_));
+    CK(cudaMalloc(&d_patw_, sizeof(double) * Pp_));
+    CK(cudaMalloc(&d_site_, sizeof(double) * Pp_));
+    CK(cudaMalloc(&d_site1_, sizeof(double) * Pp_));
+    CK(cudaMalloc(&d_site2_, sizeof(double) * Pp_));
+    CK(cudaMemsetAsync(d_site_, 0, sizeof(double) * Pp_, stream_));
+    CK(cudaMemsetAsync(d_site1_, 0, sizeof(double) * Pp_, stream_));
+    CK(cudaMemsetAsync(d_site2_, 0, sizeof(double) * Pp_, stream_));
+    h_catw_.assign((size_t)neig_ * C_, 0.0);
+    h_freqs_.assign((size_t)neig_ * S_, 0.0);
+    h_rates_.assign((size_t)neig_ * C_, 0.0);
+    eig_set_.assign(neig_, 0);
+    rates_set_.assign(neig_, 0);
+    catw_set_.assign(neig_, 0);
+    freqs_set_.assign(neig_, 0);
+    // Pattern weights default to 1 (padded patterns weigh 0).
+    h_patw_.assign(Pp_, 0.0);
+    std::fill(h_patw_.begin(), h_patw_.begin() + P_, 1.0);
+    CK(cudaMemcpyAsync(d_patw_, h_patw_.data(), sizeof(double) * Pp_, cudaMemcpyHostToDevice,
+                       stream_));
+    h_out_n_ = 64;
+    CK(cudaMallocHost(&h_out_, sizeof(double) * h_out_n_));
+    return sync();
+}
+
+int Instance::sync() {
+    CK(cudaStreamSynchronize(stream_));
+    for (const Pending& pd : pending_) {
+        if (pd.count == 0) {
+            last_lnl_ = pd.slot[0];
+        } else {
+            if (pd.dst_sum) std::copy(pd.slot, pd.slot + pd.count, pd.dst_sum);
+            if (pd.dst_sumsq) std::copy(pd.slot + pd.count, pd.slot + 2 * pd.count, pd.dst_sumsq);
+        }
+    }
+    pending_.clear();
+    chunk_i_ = 0;
+    chunk_off_ = 0;
+    return kSuccess;
+}
+
+// n doubles of pinned staging, valid until the next sync(); chunks are kept
+// and reused, a new one is allocated only when the queued results outgrow them.
+double* Instance::stage(size_t n) {
+    while (chunk_i_ < chunks_.size() && chunk_off_ + n > chunks_[chunk_i_].second) {
+        ++chunk_i_;
+        chunk_off_ = 0;
+    }
+    if (chunk_i_ == chunks_.size()) {
+        const size_t sz = std::max<size_t>(n, 1 << 20);
+        double* p = nullptr;
+        if (cudaMallocHost(&p, sizeof(double) * sz) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return nullptr;
+        }
+        chunks_.emplace_back(p, sz);
+        chunk_off_ = 0;
+    }
+    double* r = chunks_[chunk_i_].first + chunk_off_;
+    chunk_off_ += n;
+    return r;
+}
+
+int Instance::waitForPartials() { return sync(); }
+
+// ------------------------------------------------------------ data in / out
+int Instance::ensure_partials(int b) {
+    if (partials_[b]) return kSuccess;
+    void* p = nullptr;
+    CK(cudaMalloc(&p, part_bytes_));
+    CK(cudaMemsetAsync(p, 0, part_bytes_, stream_));
+    owned_.push_back(p);
+    partials_[b] = p;
+    return kSuccess;
+}
+
+int Instance::setTipStates(int tip, const int* in) {
+    if (!is_tip(tip) || !in) return kErrRange;
+    if (!states_[tip]) {
+        void* p = nullptr;
+        CK(cudaMalloc(&p, sizeof(int) * Pp_));
+        owned_.push_back(p);
+        states_[tip] = (int*)p;
+    }
+    std::vector<int> h(Pp_, S_);
+    for (int p = 0; p < P_; ++p) h[p] = (in[p] < S_ && in[p] >= 0) ? in[p] : S_;
+    CK(cudaMemcpyAsync(states_[tip], h.data(), sizeof(int) * Pp_, cudaMemcpyHostToDevice,
+                       stream_));
+    return sync();
+}
+
+// Convert caller partials ([C][P][S], or [P][S] replicated over categories)
+// into the device layout [Pp][C][Sg] and upload.
+int Instance::upload_partials(int b, const double* in, bool replicate) {
+    int rc = ensure_partials(b);
+    if (rc) return rc;
+    const size_t n = (size_t)Pp_ * C_ * Sg_;
+    std::vector<double> hd;
+    std::vector<float> hf;
+    if (dbl_) hd.assign(n, 0.0); else hf.assign(n, 0.0f);
+    for (int c = 0; c < C_; ++c)
+        for (int p = 0; p < P_; ++p) {
+            const double* src = replicate ? in + (size_t)p * S_ : in + ((size_t)c * P_ + p) * S_;
+            const size_t dst = ((size_t)p * C_ + c) * Sg_;
+            for (int i = 0; i < S_; ++i) {
+                if (dbl_) hd[dst + i] = src[i]; else hf[dst + i] = (float)src[i];
+            }
+        }
+    const void* src = dbl_ ? (const void*)hd.data() : (const void*)hf.data();
+    CK(cudaMemcpyAsync(partials_[b], src, n * rsz_, cudaMemcpyHostToDevice, stream_));
+    return sync();
+}
+
+int Instance::setTipPartials(int tip, const double* in) {
+    if (!is_tip(tip) || !in) return kErrRange;
+    return upload_partials(tip, in, true);
+}
+
+int Instance::setPartials(int b, const double* in) {
+    if (!buf_ok(b) || !in) return kErrRange;
+    return upload_partials(b, in, false);
+}
+
+int Instance::setRootPrePartials(const int* bufs, const int* fidx, int count) {
+    if (count < 0 || (count > 0 && (!bufs || !fidx))) return kErrRange;
+    for (int k = 0; k < count; ++k) {
+        const int b = bufs[k], f = fidx[k];
+        if (!buf_ok(b) || f < 0 || f >= neig_ || !freqs_set_[f]) return kErrRange;
+        int rc = ensure_partials(b);
+        if (rc) return rc;
+        CK(LAUNCH(launch_fill_root, partials_[b], d_freqs_ + (size_t)f * S_, dims(), stream_));
+    }
+    return kSuccess;
+}
+
+int Instance::getPartials(int b, int scaleIndex, double* out) {
+    if (!buf_ok(b) || !partials_[b] || !out) return kErrRange;
+    if (scaleIndex != -1 && (scaleIndex < 0 || scaleIndex >= nscale_)) return kErrRange;
+    const size_t n = (size_t)Pp_ * C_ * Sg_;
+    std::vector<uint8_t> h(n * rsz_);
+    CK(cudaMemcpyAsync(h.data(), partials_[b], n * rsz_, cudaMemcpyDeviceToHost, stream_));
+    std::vector<double> sc;
+    if (scaleIndex != -1) {
+        sc.resize(P_);
+        CK(cudaMemcpyAsync(sc.data(), scale(scaleIndex), sizeof(double) * P_,
+                           cudaMemcpyDeviceToHost, stream_));
+    }
+    int rc = sync();
+    if (rc) return rc;
+    for (int c = 0; c < C_; ++c)
+        for (int p = 0; p < P_; ++p)
+            for (int i = 0; i < S_; ++i) {
+                const size_t src = ((size_t)p * C_ + c) * Sg_ + i;
+                out[((size_t)c * P_ + p) * S_ + i] =
+                    dbl_ ? ((const double*)h.data())[src] : (double)((const float*)h.data())[src];
+            }
+    // CPU/BeagleCPUImpl.hpp:734-745: the cumulative factors are applied to the
+    // first P*S outputs (category 0) only; reproduced as is.
+    if (scaleIndex != -1)
+        for (int p = 0; p < P_; ++p) {
+            const double f = std::exp(sc[p]);
+            for (int i = 0; i < S_; ++i) out[(size_t)p * S_ + i] *= f;
+        }
+    return kSuccess;
+}
+
+int Instance::setEigenDecomposition(int e, const double* evec, const double* ivec,
+                                    const double* evals) {
+    if (e < 0 || e >= neig_ || !evec || !ivec || !evals) return kErrRange;
+    // Cube C[i][j][k] = V[i][k] * Vinv[k][j] (CPU/EigenDecompositionCube.hpp:69-100).
+    const size_t S = S_;
+    std::vector<double> cube(S * S * S);
+    for (size_t i = 0; i < S; ++i)
+        for (size_t j = 0; j < S; ++j)
+            for (size_t k = 0; k < S; ++k) {
+                const double vi = invevec_t_ ? ivec[k + j * S] : ivec[k * S + j];
+                cube[(i * S + j) * S + k] = evec[i * S + k] * vi;
+            }
+    CK(cudaMemcpyAsync(d_cube_ + (size_t)e * S * S * S, cube.data(), sizeof(double) * S * S * S,
+                       cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(d_evals_ + (size_t)e * S, evals, sizeof(double) * S,
+                       cudaMemcpyHostToDevice, stream_));
+    eig_set_[e] = 1;
+    return sync();
+}
+
+int Instance::setStateFrequencies(int i, const double* f) {
+    if (i < 0 || i >= neig_ || !f) return kErrRange;
+    std::copy(f, f + S_, h_freqs_.begin() + (size_t)i * S_);
+    freqs_set_[i] = 1;
+    CK(cudaMemcpyAsync(d_freqs_ + (size_t)i * S_, h_freqs_.data() + (size_t)i * S_,
+                       sizeof(double) * S_, cudaMemcpyHostToDevice, stream_));
+    return sync();
+}
+
+int Instance::setCategoryWeights(int i, const double* w) {
+    if (i < 0 || i >= neig_ || !w) return kErrRange;
+    std::copy(w, w + C_, h_catw_.begin() + (size_t)i * C_);
+    catw_set_[i] = 1;
+    CK(cudaMemcpyAsync(d_catw_ + (size_t)i * C_, h_catw_.data() + (size_t)i * C_,
+                       sizeof(double) * C_, cudaMemcpyHostToDevice, stream_));
+    return sync();
+}
+
+int Instance::setCategoryRatesWithIndex(int i, const double* r) {
+    if (i < 0 || i >= neig_ || !r) return kErrRange;
+    std::copy(r, r + C_, h_rates_.begin() + (size_t)i * C_);
+    rates_set_[i] = 1;
+    CK(cudaMemcpyAsync(d_rates_ + (size_t)i * C_, h_rates_.data() + (size_t)i * C_,
+                       sizeof(double) * C_, cudaMemcpyHostToDevice, stream_));
+    return sync();
+}
+
+int Instance::setPatternWeights(const double* w) {
+    if (!w) return kErrRange;
+    std::copy(w, w + P_, h_patw_.begin());
+    CK(cudaMemcpyAsync(d_patw_, h_patw_.data(), sizeof(double) * Pp_, cudaMemcpyHostToDevice,
+                       stream_));
+    return sync();
+}
+
+int Instance::setPatternPartitions(int n, const int* parts) {
+    // Partitions must be contiguous, ascending pattern ranges here (the
+    // reference CPU reorders patterns otherwise, BeagleCPUImpl.hpp:803-920).
+    if (n < 1 || !parts) return kErrRange;
+    std::vector<int> start(n + 1, -1);
+    int cur = parts[0];
+    if (cur != 0) return kErrNoImpl;
+    start[0] = 0;
+    for (int p = 1; p < P_; ++p) {
+        if (parts[p] == cur) continue;
+        if (parts[p] != cur + 1) return kErrNoImpl;
+        cur = parts[p];
+        start[cur] = p;
+    }
+    if (cur != n - 1) return kErrRange;
+    start[n] = P_;
+    partition_start_ = start;
+    return kSuccess;
+}
+
+// ---------------------------------------------------------------- matrices
+int Instance::upload_matrix(int m, const double* in, double pad) {
+    const size_t n = (size_t)C_ * Sg_ * Sg_;
+    std::vector<double> hd(n, 0.0);
+    for (int c = 0; c < C_; ++c)
+        for (int i = 0; i < S_; ++i)
+            for (int j = 0; j < S_; ++j)
+                hd[((size_t)c * Sg_ + i) * Sg_ + j] = in[((size_t)c * S_ + i) * S_ + j];
+    if (dbl_) {
+        CK(cudaMemcpyAsync(mat(m), hd.data(), n * 8, cudaMemcpyHostToDevice, stream_));
+    } else {
+        std::vector<float> hf(hd.begin(), hd.end());
+        CK(cudaMemcpyAsync(mat(m), hf.data(), n * 4, cudaMemcpyHostToDevice, stream_));
+        return sync();   // hf goes out of scope
+    }
+    mat_pad_[m] = pad;
+    return sync();
+}
+
+int Instance::setTransitionMatrix(int m, const double* in, double pad) {
+    if (m < 0 || m >= nmat_ || !in) return kErrRange;
+    int rc = upload_matrix(m, in, pad);
+    mat_pad_[m] = pad;
+    return rc;
+}
+
+int Instance::setTransitionMatrices(const int* idx, const double* in, const double* pads,
+                                    int count) {
+    for (int k = 0; k < count; ++k) {
+        int rc = setTransitionMatrix(idx[k], in + (size_t)k * C_ * S_ * S_, pads[k]);
+        if (rc) return rc;
+    }
+    return kSuccess;
+}
+
+int Instance::getTransitionMatrix(int m, double* out) {
+    if (m < 0 || m >= nmat_ || !out) return kErrRange;
+    const size_t n = (size_t)C_ * Sg_ * Sg_;
+    std::vector<uint8_t> h(n * rsz_);
+    CK(cudaMemcpyAsync(h.data(), mat(m), n * rsz_, cudaMemcpyDeviceToHost, stream_));
+    int rc = sync();
+    if (rc) return rc;
+    for (int c = 0; c < C_; ++c)
+        for (int i = 0; i < S_; ++i)
+            for (int j = 0; j < S_; ++j) {
+                const size_t src = ((size_t)c * Sg_ + i) * Sg_ + j;
+                out[((size_t)c * S_ + i) * S_ + j] =
+                    dbl_ ? ((const double*)h.data())[src] : (double)((const float*)h.data())[src];
+            }
+    return kSuccess;
+}
+
+int Instance::transposeTransitionMatrices(const int* in, const int* out, int count) {
+    if (count <= 0) return kSuccess;
+    std::vector<const void*> a(count);
+    std::vector<void*> o(count);
+    for (int k = 0; k < count; ++k) {
+        if (in[k] < 0 || in[k] >= nmat_ || out[k] < 0 || out[k] >= nmat_) return kErrRange;
+        if (in[k] == out[k]) return kErrRange;   // in-place not allowed (CPU :1190-1200)
+        a[k] = mat(in[k]);
+        o[k] = mat(out[k]);
+    }
+    std::vector<const void*> tab(2 * count);
+    for (int k = 0; k < count; ++k) { tab[k] = a[k]; tab[count + k] = o[k]; }
+    CK(t_ptr_.upload(tab.data(), sizeof(void*) * tab.size(), stream_));
+    const void* const* da = (const void* const*)t_ptr_.ptr;
+    void* const* dout = (void* const*)((const void**)t_ptr_.ptr + count);
+    CK(LAUNCH(launch_matrix_pairs, da, nullptr, dout, count, 1, dims(), stream_));
+    return kSuccess;
+}
+
+int Instance::convolveTransitionMatrices(const int* first, const int* second,
+                                         const int* result, int count) {
+    if (count <= 0) return kSuccess;
+    std::vector<const void*> tab(3 * count);
+    for (int k = 0; k < count; ++k) {
+        for (int v : {first[k], second[k], result[k]})
+            if (v < 0 || v >= nmat_) return kErrRange;
+        if (first[k] == result[k] || second[k] == result[k]) return kErrRange;
+        tab[k] = mat(first[k]);
+        tab[count + k] = mat(second[k]);
+        tab[2 * count + k] = mat(result[k]);
+        mat_pad_[result[k]] = 1.0;
+    }
+    CK(t_ptr_.upload(tab.data(), sizeof(void*) * tab.size(), stream_));
+    const void* const* base = (const void* const*)t_ptr_.ptr;
+    CK(LAUNCH(launch_matrix_pairs, base, base + count, (void* const*)(base + 2 * count), count, 0,
+              dims(), stream_));
+    return kSuccess;
+}
+
+int Instance::run_matrix_jobs(const std::vector<MatJob>& jobs) {
+    if (jobs.empty()) return kSuccess;
+    CK(t_jobs_.upload(jobs.data(), sizeof(MatJob) * jobs.size(), stream_));
+    CK(LAUNCH(launch_update_matrices, (const MatJob*)t_jobs_.ptr, (int)jobs.size(), dims(),
+              stream_));
+    return kSuccess;
+}
+
+int Instance::updateTransitionMatricesWithMultipleModels(const int* eig, const int* rix,
+                                                         const int* prob, const int* d1,
+                                                         const int* d2, const double* t,
+                                                         int count) {
+    if (count < 0 || (count > 0 && (!prob || !t))) return kErrRange;
+    std::vector<MatJob> jobs(count);
+    for (int u = 0; u < count; ++u) {
+        const int e = eig ? eig[u] : 0, r = rix ? rix[u] : 0;
+        if (e < 0 || e >= neig_ || !eig_set_[e] || r < 0 || r >= neig_ || !rates_set_[r])
+            return kErrRange;
+        if (prob[u] < 0 || prob[u] >= nmat_) return kErrRange;
+        if (d1 && (d1[u] < 0 || d1[u] >= nmat_)) return kErrRange;
+        if (d2 && (d2[u] < 0 || d2[u] >= nmat_)) return kErrRange;
+        MatJob& j = jobs[u];
+        j.p = mat(prob[u]);
+        j.d1 = d1 ? mat(d1[u]) : nullptr;
+        j.d2 = (d1 && d2) ? mat(d2[u]) : nullptr;
+        j.cube = d_cube_ + (size_t)e * S_ * S_ * S_;
+        j.evals = d_evals_ + (size_t)e * S_;
+        j.rates = d_rates_ + (size_t)r * C_;
+        j.t = t[u];
+        mat_pad_[prob[u]] = 1.0;
+        if (j.d1) mat_pad_[d1[u]] = 0.0;
+        if (j.d2) mat_pad_[d2[u]] = 0.0;
+    }
+    return run_matrix_jobs(jobs);
+}
+
+int Instance::updateTransitionMatrices(int e, const int* prob, const int* d1, const int* d2,
+                                       const double* t, int count) {
+    std::vector<int> eig(std::max(count, 0), e), rix(std::max(count, 0), 0);
+    return updateTransitionMatricesWithMultipleModels(eig.data(), rix.data(), prob, d1, d2, t,
+                                                      count);
+}
+
+int Instance::updateTransitionMatricesWithModelCategories(const int*, const int*, const int*,
+                                                          const int*, const double*, int) {
+    return kErrNoImpl;   // per-category eigen systems: not on this resource
+}
+
+// ---------------------------------------------------------------- partials
+int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative, bool pre) {
+    if (count < 0 || (count > 0 && !ops)) return kErrRange;
+    if (cumulative != -1 && (cumulative < 0 || cumulative >= nscale_)) return kErrRange;
+    std::vector<OpDesc> tab(count);
+    // Buffers written earlier in this list count as holding data.
+    std::vector<char> written(nbuf_, 0);
+    for (int k = 0; k < count; ++k) {
+        const int* op = ops + (size_t)k * stride;
+        const int dest = op[0], ws = op[1], rs = op[2], c1 = op[3], m1 = op[4], c2 = op[5],
+                  m2 = op[6];
+        if (!buf_ok(dest) || states_[dest]) return kErrRange;
+        if (!buf_ok(c1) || !buf_ok(c2)) return kErrRange;
+        if (!(has_data(c1) || written[c1]) || !(has_data(c2) || written[c2])) return kErrRange;
+        if (pre && states_[c1]) return kErrRange;   // parent pre-partials are partials
+        if (m1 < 0 || m1 >= nmat_ || m2 < 0 || m2 >= nmat_) return kErrRange;
+        if (ws != -1 && (ws < 0 || ws >= nscale_)) return kErrRange;
+        if (rs != -1 && (rs < 0 || rs >= nscale_)) return kErrRange;
+        if (dest == c1 || dest == c2) return kErrRange;
+        int rc = ensure_partials(dest);
+        if (rc) return rc;
+        written[dest] = 1;
+        OpDesc& d = tab[k];
+        d.x1 = states_[c1] ? (const void*)states_[c1] : partials_[c1];
+        d.x2 = states_[c2] ? (const void*)states_[c2] : partials_[c2];
+        d.dest = partials_[dest];
+        d.m1 = mat(m1);
+        d.m2 = mat(m2);
+        d.pad1 = mat_pad_[m1];
+        d.pad2 = mat_pad_[m2];
+        d.scale_write = ws >= 0 ? scale(ws) : nullptr;
+        // Fixed scaling applies only when no new factors are written
+        // (CPU/BeagleCPUImpl.hpp:1571-1577); pre-order never reads them (:1779-1785).
+        d.scale_read = (ws < 0 && rs >= 0 && !pre) ? scale(rs) : nullptr;
+        d.kind = (states_[c1] ? kX1States : 0) | (states_[c2] ? kX2States : 0);
+        // The reference GPU resource expects the node's matrix transposed in
+        // pre-order ops when S > 4 unless PREORDER_TRANSPOSE_AUTO is set
+        // (GPU/BeagleGPUImpl.hpp:787-788, 2844-2855).
+        if (pre && S_ > 4 && !pre_auto_) d.kind |= kM1Transposed;
+        d.reserved = 0;
+    }
+    DevBuf& t = pre ? t_ops_pre_ : t_ops_post_;
+    CK(t.upload(tab.data(), sizeof(OpDesc) * tab.size(), stream_));
+    double* cum = (cumulative >= 0 && !pre) ? scale(cumulative) : nullptr;
+    if (pre) {
+        CK(LAUNCH(launch_update_pre_partials, (const OpDesc*)t.ptr, count, dims(),
+                  (int)log_scalers_, stream_));
+    } else {
+        CK(LAUNCH(launch_update_partials, (const OpDesc*)t.ptr, count, dims(), cum,
+                  (int)log_scalers_, stream_));
+    }
+    return kSuccess;
+}
+
+int Instance::updatePartials(const int* ops, int count, int cumulative) {
+    return post_or_pre(ops, count, 7, cumulative, false);
+}
+
+int Instance::updatePrePartials(const int* ops, int count, int cumulative) {
+    return post_or_pre(ops, count, 7, cumulative, true);
+}
+
+int Instance::updatePartialsByPartition(const int*, int) { return kErrNoImpl; }
+int Instance::updatePrePartialsByPartition(const int*, int) { return kErrNoImpl; }
+
+// ------------------------------------------------------------ scale factors
+int Instance::accumulateScaleFactors(const int* idx, int count, int cumulative, double sign,
+                                     int partition) {
+    if (cumulative < 0 || cumulative >= nscale_ || count < 0 || (count > 0 && !idx))
+        return kErrRange;
+    for (int k = 0; k < count; ++k)
+        if (idx[k] < 0 || idx[k] >= nscale_) return kErrRange;
+    int p0 = 0, p1 = P_;
+    if (partition >= 0) {
+        if (partition_start_.empty() || partition >= (int)partition_start_.size() - 1)
+            return kErrRange;
+        p0 = partition_start_[partition];
+        p1 = partition_start_[partition + 1];
+    }
+    CK(t_idx_.upload(idx, sizeof(int) * count, stream_));
+    CK(launch_accumulate_scale(scale(cumulative), d_scale_, (const int*)t_idx_.ptr, count, Pp_,
+                               P_, sign, (int)log_scalers_, p0, p1, stream_));
+    return kSuccess;
+}
+
+int Instance::resetScaleFactors(int cumulative, int partition) {
+    if (cumulative < 0 || cumulative >= nscale_) return kErrRange;
+    if (partition < 0) {
+        CK(cudaMemsetAsync(scale(cumulative), 0, sizeof(double) * Pp_, stream_));
+    } else {
+        if (partition_start_.empty() || partition >= (int)partition_start_.size() - 1)
+            return kErrRange;
+        const int p0 = partition_start_[partition], p1 = partition_start_[partition + 1];
+        CK(cudaMemsetAsync(scale(cumulative) + p0, 0, sizeof(double) * (p1 - p0), stream_));
+    }
+    return kSuccess;
+}
+
+int Instance::copyScaleFactors(int dst, int src) {
+    if (dst < 0 || dst >= nscale_ || src < 0 || src >= nscale_) return kErrRange;
+    CK(cudaMemcpyAsync(scale(dst), scale(src), sizeof(double) * Pp_, cudaMemcpyDeviceToDevice,
+                       stream_));
+    return kSuccess;
+}
+
+int Instance::getScaleFactors(int src, double* out) {
+    if (src < 0 || src >= nscale_ || !out) return kErrRange;
+    CK(cudaMemcpyAsync(out, scale(src), sizeof(double) * P_, cudaMemcpyDeviceToHost, stream_));
+    return sync();
+}
+
+// -------------------------------------------------------------- reductions
+int Instance::calculateRootLogLikelihoods(const int* bufs, const int* cw, const int* sf,
+                                          const int* cum, int count, double* out) {
+    if (count != 1) return kErrNoImpl;
+    if (!bufs || !cw || !sf || !out) return kErrRange;
+    const int b = bufs[0], w = cw[0], f = sf[0], c = cum ? cum[0] : -1;
+    if (!buf_ok(b) || !partials_[b]) return kErrRange;
+    if (w < 0 || w >= neig_ || !catw_set_[w] || f < 0 || f >= neig_ || !freqs_set_[f])
+        return kErrRange;
+    if (c != -1 && (c < 0 || c >= nscale_)) return kErrRange;
+    const int nblk = reduction_blocks(P_);
+    CK(scratch_.reserve(sizeof(double) * nblk));
+    CK(out_.reserve(sizeof(double) * 4));
+    CK(LAUNCH(launch_root_lnl, partials_[b], d_catw_ + (size_t)w * C_, d_freqs_ + (size_t)f * S_,
+              c >= 0 ? scale(c) : nullptr, d_patw_, dims(), d_site_, (double*)scratch_.ptr,
+              (double*)out_.ptr, stream_));
+    if (async_) {
+        // ASYNCH (GPU/BeagleGPUImpl.hpp:3398-3407): the value is delivered by
+        // beagleGetLogLikelihood; nothing is written to *out here.
+        double* slot = stage(1);
+        if (!slot) return kErrOOM;
+        CK(cudaMemcpyAsync(slot, out_.ptr, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        pending_.push_back(Pending{slot, nullptr, nullptr, 0});
+        return kSuccess;
+    }
+    CK(cudaMemcpyAsync(h_out_, out_.ptr, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    int rc = sync();
+    if (rc) return rc;
+    *out = h_out_[0];
+    last_lnl_ = *out;
+    return std::isnan(*out) ? kErrFP : kSuccess;
+}
+
+int Instance::calculateRootLogLikelihoodsByPartition(const int*, const int*, const int*,
+                                                     const int*, const int*, int, int, double*,
+                                                     double*) {
+    return kErrNoImpl;
+}
+
+int Instance::calculateEdgeDerivatives(const int* post, const int* pre, const int* dmat,
+                                       const int* cw, int count, double* outDerivs,
+                                       double* outSum, double* outSumSq) {
+    if (count < 0 || (count > 0 && (!post || !pre || !dmat || !cw))) return kErrRange;
+    if (count == 0) return kSuccess;
+    const int w = cw[0];
+    if (w < 0 || w >= neig_ || !catw_set_[w]) return kErrRange;
+    std::vector<DerivDesc> tab(count);
+    for (int k = 0; k < count; ++k) {
+        if (!has_data(post[k]) || !buf_ok(pre[k]) || !partials_[pre[k]]) return kErrRange;
+        if (dmat[k] < 0 || dmat[k] >= nmat_) return kErrRange;
+        DerivDesc& d = tab[k];
+        d.post = states_[post[k]] ? (const void*)states_[post[k]] : partials_[post[k]];
+        d.post_is_states = states_[post[k]] ? 1 : 0;
+        d.pre = partials_[pre[k]];
+        d.dmat = mat(dmat[k]);
+        d.dpad = mat_pad_[dmat[k]];
+        d.reserved = 0;
+    }
+    const int nblk = reduction_blocks(P_);
+    CK(t_deriv_.upload(tab.data(), sizeof(DerivDesc) * count, stream_));
+    CK(scratch_.reserve(sizeof(double) * 2 * (size_t)count * nblk));
+    CK(out_.reserve(sizeof(double) * 2 * count));
+    if (outDerivs) CK(site_d_.reserve(sizeof(double) * (size_t)count * P_));
+    CK(LAUNCH(launch_edge_derivatives, (const DerivDesc*)t_deriv_.ptr, count,
+              d_catw_ + (size_t)w * C_, d_patw_, dims(),
+              outDerivs ? (double*)site_d_.ptr : nullptr, (double*)scratch_.ptr,
+              (double*)out_.ptr, stream_));
+    if (async_ && !outDerivs) {
+        // ASYNCH: sums are written to the caller's arrays at the next
+        // synchronisation point (getters, waitForPartials, synchronous calls).
+        double* slot = stage(2 * (size_t)count);
+        if (!slot) return kErrOOM;
+        CK(cudaMemcpyAsync(slot, out_.ptr, sizeof(double) * 2 * count, cudaMemcpyDeviceToHost,
+                           stream_));
+        pending_.push_back(Pending{slot, outSum, outSumSq, count});
+        return kSuccess;
+    }
+    if ((size_t)2 * count > h_out_n_) {
+        cudaFreeHost(h_out_);
+        h_out_ = nullptr;
+        h_out_n_ = 2 * count;
+        CK(cudaMallocHost(&h_out_, sizeof(double) * h_out_n_));
+    }
+    CK(cudaMemcpyAsync(h_out_, out_.ptr, sizeof(double) * 2 * count, cudaMemcpyDeviceToHost,
+                       stream_));
+    if (outDerivs)
+        CK(cudaMemcpyAsync(outDerivs, site_d_.ptr, sizeof(double) * (size_t)count * P_,
+                           cudaMemcpyDeviceToHost, stream_));
+    int rc = sync();
+    if (rc) return rc;
+    if (outSum) std::copy(h_out_, h_out_ + count, outSum);
+    if (outSumSq) std::copy(h_out_ + count, h_out_ + 2 * count, outSumSq);
+    return kSuccess;
+}
+
+int Instance::calculateEdgeLogLikelihoods(const int* parents, const int* children,
+                                          const int* prob, const int* d1, const int* d2,
+                                          const int* cw, const int* sf, const int* cum, int count,
+                                          double* outLnL, double* outD1, double* outD2) {
+    if (count != 1) return kErrNoImpl;
+    if (!parents || !children || !prob || !cw || !sf || !outLnL) return kErrRange;
+    const int pa = parents[0], ch = children[0], pm = prob[0], w = cw[0], f = sf[0];
+    const int c = cum ? cum[0] : -1;
+    if (!buf_ok(pa) || !partials_[pa] || !has_data(ch)) return kErrRange;
+    if (pm < 0 || pm >= nmat_) return kErrRange;
+    const int m1 = d1 ? d1[0] : -1, m2 = (d1 && d2) ? d2[0] : -1;
+    if ((d1 && (m1 < 0 || m1 >= nmat_)) || (m2 != -1 && (m2 < 0 || m2 >= nmat_)))
+        return kErrRange;
+    if (w < 0 || w >= neig_ || !catw_set_[w] || f < 0 || f >= neig_ || !freqs_set_[f])
+        return kErrRange;
+    if (c != -1 && (c < 0 || c >= nscale_)) return kErrRange;
+    const int nblk = reduction_blocks(P_);
+    CK(scratch_.reserve(sizeof(double) * 3 * nblk));
+    CK(out_.reserve(sizeof(double) * 4));
+    const bool st = states_[ch] != nullptr;
+    CK(LAUNCH(launch_edge_lnl, partials_[pa], st ? (const void*)states_[ch] : partials_[ch],
+              (int)st, mat(pm), mat_pad_[pm], m1 >= 0 ? mat(m1) : nullptr,
+              m1 >= 0 ? mat_pad_[m1] : 0.0, m2 >= 0 ? mat(m2) : nullptr,
+              m2 >= 0 ? mat_pad_[m2] : 0.0, d_catw_ + (size_t)w * C_, d_freqs_ + (size_t)f * S_,
+              c >= 0 ? scale(c) : nullptr, d_patw_, dims(), d_site_, d_site1_, d_site2_,
+              (double*)scratch_.ptr, (double*)out_.ptr, stream_));
+    CK(cudaMemcpyAsync(h_out_, out_.ptr, sizeof(double) * 3, cudaMemcpyDeviceToHost, stream_));
+    int rc = sync();
+    if (rc) return rc;
+    *outLnL = h_out_[0];
+    last_lnl_ = h_out_[0];
+    last_d1_ = h_out_[1];
+    last_d2_ = h_out_[2];
+    if (outD1 && m1 >= 0) *outD1 = h_out_[1];
+    if (outD2 && m2 >= 0) *outD2 = h_out_[2];
+    return std::isnan(*outLnL) ? kErrFP : kSuccess;
+}
+
+int Instance::getLogLikelihood(double* out) {
+    if (!out) return kErrRange;
+    int rc = sync();
+    if (rc) return rc;
+    *out = last_lnl_;
+    return std::isnan(last_lnl_) ? kErrFP : kSuccess;
+}
+
+int Instance::getDerivatives(double* d1, double* d2) {
+    int rc = sync();
+    if (rc) return rc;
+    if (d1) *d1 = last_d1_;
+    if (d2) *d2 = last_d2_;
+    return kSuccess;
+}
+
+int Instance::getSiteLogLikelihoods(double* out) {
+    if (!out) return kErrRange;
+    CK(cudaMemcpyAsync(out, d_site_, sizeof(double) * P_, cudaMemcpyDeviceToHost, stream_));
+    return sync();
+}
+
+int Instance::getSiteDerivatives(double* d1, double* d2) {
+    if (d1) CK(cudaMemcpyAsync(d1, d_site1_, sizeof(double) * P_, cudaMemcpyDeviceToHost, stream_));
+    if (d2) CK(cudaMemcpyAsync(d2, d_site2_, sizeof(double) * P_, cudaMemcpyDeviceToHost, stream_));
+    return sync();
+}
+
+}  // namespace b200

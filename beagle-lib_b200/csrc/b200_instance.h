@@ -1,0 +1,161 @@
+// Host side of one B200 instance: the buffer registry, flag handling, op
+// validation and kernel launches behind every beagleB200* call.  It mirrors
+// the reference's BeagleImpl interface (libhmsbeagle/BeagleImpl.h:31-268):
+// same method set, same argument meaning, same return codes.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+#include "b200_kernels.h"
+
+namespace b200 {
+
+// A device buffer that only grows; used for per-call tables and scratch.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    std::vector<uint8_t> last;     // last uploaded contents (upload is skipped if equal)
+    cudaError_t reserve(size_t n);
+    cudaError_t upload(const void* src, size_t n, cudaStream_t s);
+    void release();
+};
+
+class Instance {
+public:
+    ~Instance();
+
+    // beagleCreateInstance (BeagleImpl.h:36-48); returns a BeagleReturnCode.
+    int create(int tipCount, int partialsBufferCount, int compactBufferCount, int stateCount,
+               int patternCount, int eigenBufferCount, int matrixBufferCount, int categoryCount,
+               int scaleBufferCount, int device, long preferenceFlags, long requirementFlags);
+
+    long flags() const { return flags_; }
+    cudaStream_t stream() const { return stream_; }
+    int device() const { return device_; }
+    const char* implName() const { return dbl_ ? "B200-sm100a-Double" : "B200-sm100a-Mixed"; }
+
+    int setTipStates(int tipIndex, const int* inStates);
+    int setTipPartials(int tipIndex, const double* inPartials);
+    int setPartials(int bufferIndex, const double* inPartials);
+    int setRootPrePartials(const int* bufferIndices, const int* freqIndices, int count);
+    int getPartials(int bufferIndex, int scaleIndex, double* outPartials);
+    int setEigenDecomposition(int eigenIndex, const double* evec, const double* ivec,
+                              const double* evals);
+    int setStateFrequencies(int index, const double* freqs);
+    int setCategoryWeights(int index, const double* weights);
+    int setCategoryRates(const double* rates) { return setCategoryRatesWithIndex(0, rates); }
+    int setCategoryRatesWithIndex(int index, const double* rates);
+    int setPatternWeights(const double* weights);
+    int setPatternPartitions(int partitionCount, const int* partitions);
+
+    int setTransitionMatrix(int matrixIndex, const double* inMatrix, double paddedValue);
+    int setTransitionMatrices(const int* matrixIndices, const double* inMatrices,
+                              const double* paddedValues, int count);
+    int getTransitionMatrix(int matrixIndex, double* outMatrix);
+    int transposeTransitionMatrices(const int* in, const int* out, int count);
+    int convolveTransitionMatrices(const int* first, const int* second, const int* result,
+                                   int count);
+    int updateTransitionMatrices(int eigenIndex, const int* probIdx, const int* d1Idx,
+                                 const int* d2Idx, const double* edgeLengths, int count);
+    int updateTransitionMatricesWithMultipleModels(const int* eigenIndices,
+                                                   const int* rateIndices, const int* probIdx,
+                                                   const int* d1Idx, const int* d2Idx,
+                                                   const double* edgeLengths, int count);
+    int updateTransitionMatricesWithModelCategories(const int* eigenIndices, const int* probIdx,
+                                                    const int* d1Idx, const int* d2Idx,
+                                                    const double* edgeLengths, int count);
+
+    int updatePartials(const int* ops, int count, int cumulativeScaleIndex);
+    int updatePrePartials(const int* ops, int count, int cumulativeScaleIndex);
+    int updatePartialsByPartition(const int* ops, int count);
+    int updatePrePartialsByPartition(const int* ops, int count);
+    int waitForPartials();
+
+    int accumulateScaleFactors(const int* idx, int count, int cumulative, double sign,
+                               int partition);
+    int resetScaleFactors(int cumulative, int partition);
+    int copyScaleFactors(int dst, int src);
+    int getScaleFactors(int src, double* out);
+
+    int calculateRootLogLikelihoods(const int* bufs, const int* cw, const int* sf,
+                                    const int* cum, int count, double* out);
+    int calculateRootLogLikelihoodsByPartition(const int* bufs, const int* cw, const int* sf,
+                                               const int* cum, const int* parts, int nparts,
+                                               int count, double* outByPart, double* out);
+    int calculateEdgeDerivatives(const int* post, const int* pre, const int* dmat,
+                                 const int* cw, int count, double* outDerivs, double* outSum,
+                                 double* outSumSq);
+    int calculateEdgeLogLikelihoods(const int* parents, const int* children, const int* prob,
+                                    const int* d1, const int* d2, const int* cw, const int* sf,
+                                    const int* cum, int count, double* outLnL, double* outD1,
+                                    double* outD2);
+    int getLogLikelihood(double* out);
+    int getDerivatives(double* d1, double* d2);
+    int getSiteLogLikelihoods(double* out);
+    int getSiteDerivatives(double* d1, double* d2);
+
+private:
+    bool is_tip(int b) const { return b >= 0 && b < N_; }
+    bool buf_ok(int b) const { return b >= 0 && b < nbuf_; }
+    bool has_data(int b) const { return buf_ok(b) && (partials_[b] || states_[b]); }
+    void* mat(int m) const { return (char*)d_mat_ + (size_t)m * mat_bytes_; }
+    double* scale(int i) const { return d_scale_ + (size_t)i * Pp_; }
+    int ensure_partials(int b);
+    int upload_matrix(int m, const double* in, double pad);
+    int upload_partials(int b, const double* in, bool replicate);
+    int run_matrix_jobs(const std::vector<MatJob>& jobs);
+    int post_or_pre(const int* ops, int count, int stride, int cumulative, bool pre);
+    int sync();
+    double* stage(size_t n);     // pinned result staging (ASYNCH results)
+    Dims dims() const { return Dims{S_, Sg_, P_, Pp_, C_}; }
+
+    int device_ = 0;
+    cudaStream_t stream_ = nullptr;
+    long flags_ = 0;
+    bool dbl_ = true, log_scalers_ = true, invevec_t_ = false, pre_auto_ = false;
+    int N_ = 0, nbuf_ = 0, S_ = 0, Sg_ = 0, P_ = 0, Pp_ = 0, C_ = 0;
+    int neig_ = 0, nmat_ = 0, nscale_ = 0;
+    size_t rsz_ = 8, part_bytes_ = 0, mat_bytes_ = 0;
+
+    void* d_part_pool_ = nullptr;          // internal partials buffers
+    std::vector<void*> partials_;          // per buffer: device partials or null
+    std::vector<int*> states_;             // per buffer: device tip states or null
+    std::vector<void*> owned_;             // lazily allocated tip buffers
+    void* d_mat_ = nullptr;
+    std::vector<double> mat_pad_;
+    double* d_scale_ = nullptr;
+    double* d_cube_ = nullptr;             // [eig][S][S][S]
+    double* d_evals_ = nullptr;            // [eig][S]
+    double* d_rates_ = nullptr;            // [eig][C]
+    double* d_catw_ = nullptr;             // [eig][C]
+    double* d_freqs_ = nullptr;            // [eig][S]
+    double* d_patw_ = nullptr;             // [Pp]
+    double* d_site_ = nullptr;             // [Pp] site lnL
+    double* d_site1_ = nullptr;            // [Pp] site d1 (edge lnL)
+    double* d_site2_ = nullptr;            // [Pp] site d2 (edge lnL)
+    std::vector<double> h_catw_, h_freqs_, h_rates_;
+    std::vector<char> eig_set_, rates_set_, catw_set_, freqs_set_;
+    std::vector<double> h_patw_;
+    std::vector<int> partition_start_;     // pattern partitions (empty = one partition)
+
+    DevBuf t_ops_post_, t_ops_pre_, t_jobs_, t_deriv_, t_idx_, t_ptr_, scratch_, out_, site_d_;
+    double* h_out_ = nullptr;              // pinned result staging (SYNCH calls)
+    size_t h_out_n_ = 0;
+    // ASYNCH mode: results copied into pinned chunks and delivered at the next
+    // synchronisation point (any getter, waitForPartials, or a synchronous call).
+    bool async_ = false;
+    struct Pending {
+        double* slot;
+        double* dst_sum;          // caller arrays for edge-derivative sums (may be null)
+        double* dst_sumsq;
+        int count;                // edge-derivative branches (0: a log-likelihood)
+    };
+    std::vector<Pending> pending_;
+    std::vector<std::pair<double*, size_t>> chunks_;
+    size_t chunk_i_ = 0, chunk_off_ = 0;
+
+    double last_lnl_ = 0, last_d1_ = 0, last_d2_ = 0;
+};
+
+}  // namespace b200

@@ -1,0 +1,73 @@
+// Host-callable launchers of the sm_100a kernels.  Every launcher takes device
+// pointers, sizes and the instance's stream and returns a cudaError_t; none of
+// them allocates.
+#pragma once
+#include <cuda_runtime.h>
+#include "b200_types.h"
+
+namespace b200 {
+
+struct Dims {
+    int S;       // states
+    int Sg;      // padded state stride
+    int P;       // patterns (unpadded)
+    int Pp;      // padded patterns
+    int C;       // rate categories
+};
+
+// Transition matrices from the eigen cube (FP64), stored as Real.
+template <typename Real>
+cudaError_t launch_update_matrices(const MatJob* d_jobs, int njobs, const Dims& d,
+                                   cudaStream_t s);
+// result[m] = A[m] . B[m] per category (convolution), or transpose A.
+template <typename Real>
+cudaError_t launch_matrix_pairs(const void* const* d_a, const void* const* d_b,
+                                void* const* d_out, int n, int op, const Dims& d,
+                                cudaStream_t s);
+
+// Post-order partials over an op list, one launch for the whole list.
+template <typename Real>
+cudaError_t launch_update_partials(const OpDesc* d_ops, int nops, const Dims& d,
+                                   double* cumulative, int log_scalers, cudaStream_t s);
+// Pre-order partials over an op list.
+template <typename Real>
+cudaError_t launch_update_pre_partials(const OpDesc* d_ops, int nops, const Dims& d,
+                                       int log_scalers, cudaStream_t s);
+
+// Root log-likelihood: site lnL into d_site[P]; the weighted total into d_out[0].
+template <typename Real>
+cudaError_t launch_root_lnl(const void* root, const double* catw, const double* freqs,
+                            const double* cumulative, const double* patw, const Dims& d,
+                            double* d_site, double* d_block, double* d_out, cudaStream_t s);
+
+// Edge log-likelihood (+ optional first / second derivative sums).
+template <typename Real>
+cudaError_t launch_edge_lnl(const void* parent, const void* child, int child_is_states,
+                            const void* pmat, double ppad, const void* d1mat, double d1pad,
+                            const void* d2mat, double d2pad, const double* catw,
+                            const double* freqs, const double* cumulative,
+                            const double* patw, const Dims& d, double* d_site,
+                            double* d_site1, double* d_site2, double* d_block,
+                            double* d_out, cudaStream_t s);
+
+// Edge derivatives for `nb` branches; per-site values optional (d_site may be
+// null), sums and sums of squares into d_sums[2*nb].  d_block holds
+// nb * 2 * ceil(Pp / 128) doubles of per-block partial sums.
+template <typename Real>
+cudaError_t launch_edge_derivatives(const DerivDesc* d_desc, int nb, const double* catw,
+                                    const double* patw, const Dims& d, double* d_site,
+                                    double* d_block, double* d_sums, cudaStream_t s);
+
+// cumulative[p] += sign * sum_i f(scale[idx_i][p]), f = identity (log scalers) or log.
+cudaError_t launch_accumulate_scale(double* cumulative, const double* pool, const int* d_idx,
+                                    int n, int Pp, int P, double sign, int log_scalers,
+                                    int p_begin, int p_end, cudaStream_t s);
+
+// Fill a partials buffer with the state frequencies (pre-order root).
+template <typename Real>
+cudaError_t launch_fill_root(void* dest, const double* freqs, const Dims& d, cudaStream_t s);
+
+// Number of per-block partial sums used by the reductions above.
+int reduction_blocks(int Pp);
+
+}  // namespace b200

@@ -1,0 +1,63 @@
+// Types shared by the host instance (b200_instance.cpp) and the sm_100a
+// kernels (k_*.cu).  Plain C++: no CUDA qualifiers, so g++ and nvcc agree on
+// the layout.
+#pragma once
+#include <cstdint>
+
+namespace b200 {
+
+// Device-side layout of one instance (all buffers are in this GPU's HBM):
+//   partials   [pattern Pp][category C][state Sg]   Real   (pattern-major)
+//   tip states [pattern Pp]                          int32  (S = missing state)
+//   matrices   [category C][row Sg][col Sg]          Real   (zero padded)
+//   scale      [pattern Pp]                          double
+// Sg = S rounded up to a multiple of 4 (one 16-byte row per pattern for S = 4),
+// Pp = P rounded up to a multiple of kPatternPad so pattern tiles need no tail.
+constexpr int kPatternPad = 128;
+
+enum OpKind : int {
+    kX1States = 1,      // first operand is a compact tip-state buffer
+    kX2States = 2,      // second operand is a compact tip-state buffer
+    kM1Transposed = 4,  // pre-order: the node's matrix is given as its transpose
+};
+
+// One resolved partials operation (post-order or pre-order).  Post-order:
+// dest = (M1 . x1) * (M2 . x2).  Pre-order: x1 = parent pre-partials, x2 =
+// sibling post-partials, dest[j] = sum_i M1[i][j] * x1[i] * (M2 . x2)[i].
+struct OpDesc {
+    const void* x1;
+    const void* x2;
+    void* dest;
+    const void* m1;
+    const void* m2;
+    double* scale_write;        // rescale into this buffer (nullptr = no rescale)
+    const double* scale_read;   // divide by these stored factors (nullptr = none)
+    double pad1;                // value of the missing-state column of M1
+    double pad2;                // ... of M2
+    int kind;                   // OpKind bits
+    int reserved;
+};
+
+// One branch of an edge-derivative launch.
+struct DerivDesc {
+    const void* post;           // post-order partials (or tip states) below the branch
+    const void* pre;            // pre-order partials of the same node
+    const void* dmat;           // derivative matrix [C][Sg][Sg]
+    double dpad;                // its missing-state column value
+    int post_is_states;
+    int reserved;
+};
+
+// One matrix of a transition-matrix launch: P (and optionally dP/dt, d2P/dt2)
+// for branch length t under category rates `rates`.
+struct MatJob {
+    void* p;
+    void* d1;
+    void* d2;
+    const double* cube;         // eigen cube [S][S][S] (i, j, k)
+    const double* evals;        // eigenvalues [S]
+    const double* rates;        // category rates [C]
+    double t;
+};
+
+}  // namespace b200

@@ -1,0 +1,119 @@
+// Transition matrices on the device: P(t) from the eigen cube in FP64, and
+// the matrix-pair operations (convolution, transpose).
+//
+// P[c][i][j] = max(0, sum_k cube[i][j][k] * exp(lambda_k * (t * r_c))),
+// dP = sum_k cube[i][j][k] * (lambda_k r_c) e^(..), d2P with (lambda_k r_c)^2,
+// following CPU/EigenDecompositionCube.hpp:105-322 (cube from :69-100).  The
+// missing-state column of the reference's padded layout is not stored here:
+// its value travels with each matrix (1 for P, 0 for derivatives).
+#include "b200_kernels.h"
+
+namespace b200 {
+
+namespace {
+
+// One block per (job, category).  exp(.) is evaluated once per eigenvalue in
+// shared memory; each thread then forms entries (i, j) with a sequential FP64
+// sum over k (the reference's order), clamps P at 0 and rounds to Real.
+template <typename Real>
+__global__ void __launch_bounds__(256)
+k_update_matrices(const MatJob* __restrict__ jobs, int S, int Sg) {
+    extern __shared__ double sh[];
+    double* ex = sh;
+    double* e1 = sh + S;
+    double* e2 = sh + 2 * S;
+    const MatJob jb = jobs[blockIdx.x];
+    const int c = blockIdx.y;
+    const int C = gridDim.y;
+    const double r = jb.rates[c];
+    for (int k = threadIdx.x; k < S; k += blockDim.x) {
+        const double lam = jb.evals[k];
+        const double v = exp(lam * (jb.t * r));
+        const double sl = lam * r;
+        ex[k] = v;
+        e1[k] = sl * v;
+        e2[k] = sl * sl * v;
+    }
+    __syncthreads();
+    Real* P = static_cast<Real*>(jb.p) + (size_t)c * Sg * Sg;
+    Real* D1 = jb.d1 ? static_cast<Real*>(jb.d1) + (size_t)c * Sg * Sg : nullptr;
+    Real* D2 = jb.d2 ? static_cast<Real*>(jb.d2) + (size_t)c * Sg * Sg : nullptr;
+    (void)C;
+    for (int idx = threadIdx.x; idx < Sg * Sg; idx += blockDim.x) {
+        const int i = idx / Sg, j = idx - (idx / Sg) * Sg;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        if (i < S && j < S) {
+            const double* cu = jb.cube + ((size_t)i * S + j) * S;
+            if (D1) {
+                for (int k = 0; k < S; ++k) {
+                    const double cv = cu[k];
+                    s0 += cv * ex[k];
+                    s1 += cv * e1[k];
+                    s2 += cv * e2[k];
+                }
+            } else {
+                for (int k = 0; k < S; ++k) s0 += cu[k] * ex[k];
+            }
+            if (!(s0 > 0.0)) s0 = 0.0;
+        }
+        P[idx] = (Real)s0;
+        if (D1) D1[idx] = (Real)s1;
+        if (D2) D2[idx] = (Real)s2;
+    }
+}
+
+// op 0: out = a . b (convolution, CPU/BeagleCPUImpl.hpp:1096-1160);
+// op 1: out = transpose(a) (CPU/BeagleCPUImpl.hpp:1175-1222).
+template <typename Real>
+__global__ void k_matrix_pairs(const void* const* a, const void* const* b, void* const* out,
+                               int op, int S, int Sg) {
+    const int m = blockIdx.x, c = blockIdx.y;
+    const size_t off = (size_t)c * Sg * Sg;
+    const Real* A = static_cast<const Real*>(a[m]) + off;
+    Real* O = static_cast<Real*>(out[m]) + off;
+    for (int idx = threadIdx.x; idx < Sg * Sg; idx += blockDim.x) {
+        const int i = idx / Sg, j = idx - (idx / Sg) * Sg;
+        Real v = 0;
+        if (i < S && j < S) {
+            if (op == 0) {
+                const Real* B = static_cast<const Real*>(b[m]) + off;
+                Real acc = 0;
+                for (int k = 0; k < S; ++k) acc += A[i * Sg + k] * B[k * Sg + j];
+                v = acc;
+            } else {
+                v = A[j * Sg + i];
+            }
+        }
+        O[idx] = v;
+    }
+}
+
+}  // namespace
+
+template <typename Real>
+cudaError_t launch_update_matrices(const MatJob* d_jobs, int njobs, const Dims& d,
+                                   cudaStream_t s) {
+    if (njobs == 0) return cudaSuccess;
+    dim3 grid(njobs, d.C);
+    k_update_matrices<Real><<<grid, 256, 3 * d.S * sizeof(double), s>>>(d_jobs, d.S, d.Sg);
+    return cudaGetLastError();
+}
+
+template <typename Real>
+cudaError_t launch_matrix_pairs(const void* const* d_a, const void* const* d_b,
+                                void* const* d_out, int n, int op, const Dims& d,
+                                cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    dim3 grid(n, d.C);
+    k_matrix_pairs<Real><<<grid, 256, 0, s>>>(d_a, d_b, d_out, op, d.S, d.Sg);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_update_matrices<float>(const MatJob*, int, const Dims&, cudaStream_t);
+template cudaError_t launch_update_matrices<double>(const MatJob*, int, const Dims&, cudaStream_t);
+template cudaError_t launch_matrix_pairs<float>(const void* const*, const void* const*,
+                                                void* const*, int, int, const Dims&, cudaStream_t);
+template cudaError_t launch_matrix_pairs<double>(const void* const*, const void* const*,
+                                                 void* const*, int, int, const Dims&, cudaStream_t);
+
+}  // namespace b200

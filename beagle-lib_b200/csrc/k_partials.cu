@@ -1,0 +1,465 @@
+// Post-order and pre-order partials: one launch walks a whole operation list.
+//
+// Patterns are independent given the tree and the model, so the launch is
+// split over pattern tiles only and every CTA walks the full op list for its
+// own patterns: an op's children were produced earlier in the same CTA, and no
+// grid-wide synchronisation is needed between dependent ops.
+//
+// Per operation (CPU/BeagleCPUImpl.hpp:1497-1686, :4226-4524, :4665-4722):
+//   post:  dest[c,p,i] = (sum_j M1[c][i][j] x1[c,p,j]) * (sum_j M2[c][i][j] x2[c,p,j])
+//          a compact tip operand selects column x[p] of M (the missing state
+//          selects the matrix's pad value);
+//   pre:   dest[c,p,j] = sum_i M1[c][i][j] * x1[c,p,i] * (M2 . x2)[c,p,i]
+//          (CPU/BeagleCPUImpl.hpp:4530-4662; M1 given transposed when the
+//          op carries kM1Transposed);
+//   rescale (CPU/BeagleCPUImpl.hpp:4008-4056): m[p] = max_{c,i} dest (0 -> 1),
+//          dest *= 1/m, scale[p] = log m (LOG scalers) or m (RAW), and
+//          cumulative[p] += log m when a cumulative buffer is given;
+//   fixed scaling: dest *= 1/scale_read[p].
+//
+// Two kernel families:
+//  * S = 4: one thread per pattern carrying all C categories in registers;
+//    partials rows are 16-byte (FP32) / 32-byte (FP64) vectors, so a warp
+//    moves 32 contiguous pattern rows per load.  HBM-bound.
+//  * generic S (<= 64): a CTA of 8 warps owns 32 patterns; lane = pattern,
+//    warp = a contiguous slice of SPAD/8 states.  Per category the two
+//    matrices and the two child tiles are staged in shared memory; matrix
+//    reads are warp-uniform (broadcast), tile reads are conflict-free.
+#include "b200_kernels.h"
+
+namespace b200 {
+
+namespace {
+
+// ---------------------------------------------------------------- helpers
+__device__ __forceinline__ void ld4(const float* p, float v[4]) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double v[4]) {
+    const double2 a = reinterpret_cast<const double2*>(p)[0];
+    const double2 b = reinterpret_cast<const double2*>(p)[1];
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void ldg4(const float* p, float v[4]) {
+    const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+__device__ __forceinline__ void ldg4(const double* p, double v[4]) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void st4(float* p, const float v[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void st4(double* p, const double v[4]) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
+
+// Rescale one pattern's C*S values in place (see the file comment).
+template <typename Real>
+__device__ __forceinline__ void store_scale(Real m, double* scale_write, double* cum, int p,
+                                            int log_scalers) {
+    const double lm = log((double)m);
+    scale_write[p] = log_scalers ? lm : (double)m;
+    if (cum) cum[p] += lm;
+}
+
+// ------------------------------------------------------------ S = 4 kernels
+// y[c][i] = (M . x)[c][i] for one operand (partials or tip states).
+template <typename Real, int C>
+__device__ __forceinline__ void operand4(const void* x, bool states, const Real* __restrict__ M,
+                                         Real pad, int p, Real y[C][4]) {
+    if (states) {
+        const int s = static_cast<const int*>(x)[p];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) y[c][i] = (s < 4) ? __ldg(M + c * 16 + i * 4 + s) : pad;
+        }
+    } else {
+        const Real* xp = static_cast<const Real*>(x) + (size_t)p * (C * 4);
+        Real xv[C][4];
+#pragma unroll
+        for (int c = 0; c < C; ++c) ld4(xp + c * 4, xv[c]);
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                Real m[4];
+                ldg4(M + c * 16 + i * 4, m);
+                y[c][i] = m[0] * xv[c][0] + m[1] * xv[c][1] + m[2] * xv[c][2] + m[3] * xv[c][3];
+            }
+        }
+    }
+}
+
+template <typename Real, int C>
+__device__ __forceinline__ void finish4(const OpDesc& op, Real out[C][4], int p,
+                                        double* cum, int log_scalers) {
+    if (op.scale_write) {
+        Real m = 0;
+#pragma unroll
+        for (int c = 0; c < C; ++c)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) m = out[c][i] > m ? out[c][i] : m;
+        if (m == Real(0)) m = Real(1);
+        const Real inv = Real(1) / m;
+#pragma unroll
+        for (int c = 0; c < C; ++c)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) out[c][i] *= inv;
+        store_scale(m, op.scale_write, cum, p, log_scalers);
+    } else if (op.scale_read) {
+        const Real inv = Real(1) / (Real)op.scale_read[p];
+#pragma unroll
+        for (int c = 0; c < C; ++c)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) out[c][i] *= inv;
+    }
+    Real* d = static_cast<Real*>(op.dest) + (size_t)p * (C * 4);
+#pragma unroll
+    for (int c = 0; c < C; ++c) st4(d + c * 4, out[c]);
+}
+
+template <typename Real, int C>
+__global__ void __launch_bounds__(128)
+k_post4(const OpDesc* __restrict__ ops, int nops, int Pp, double* cum, int log_scalers) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= Pp) return;
+    for (int o = 0; o < nops; ++o) {
+        const OpDesc op = ops[o];
+        Real y1[C][4], y2[C][4];
+        operand4<Real, C>(op.x1, op.kind & kX1States, static_cast<const Real*>(op.m1),
+                          (Real)op.pad1, p, y1);
+        operand4<Real, C>(op.x2, op.kind & kX2States, static_cast<const Real*>(op.m2),
+                          (Real)op.pad2, p, y2);
+#pragma unroll
+        for (int c = 0; c < C; ++c)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) y1[c][i] *= y2[c][i];
+        finish4<Real, C>(op, y1, p, cum, log_scalers);
+    }
+}
+
+template <typename Real, int C>
+__global__ void __launch_bounds__(128)
+k_pre4(const OpDesc* __restrict__ ops, int nops, int Pp, int log_scalers) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= Pp) return;
+    for (int o = 0; o < nops; ++o) {
+        const OpDesc op = ops[o];
+        Real z[C][4];
+        operand4<Real, C>(op.x2, op.kind & kX2States, static_cast<const Real*>(op.m2),
+                          (Real)op.pad2, p, z);
+        const Real* xp = static_cast<const Real*>(op.x1) + (size_t)p * (C * 4);
+        const Real* M = static_cast<const Real*>(op.m1);
+        const bool tr = op.kind & kM1Transposed;
+        Real out[C][4];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            Real pv[4];
+            ld4(xp + c * 4, pv);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) z[c][i] *= pv[i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) out[c][j] = 0;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                Real m[4];
+                if (tr) {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) m[j] = __ldg(M + c * 16 + j * 4 + i);
+                } else {
+                    ldg4(M + c * 16 + i * 4, m);
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j) out[c][j] += m[j] * z[c][i];
+            }
+        }
+        finish4<Real, C>(op, out, p, nullptr, log_scalers);
+    }
+}
+
+// ---------------------------------------------------------- generic kernels
+constexpr int kNW = 8;          // warps per CTA
+constexpr int kTP = 32;         // patterns per CTA (one per lane)
+constexpr int kXS = kTP + 1;    // padded row length of staged tiles
+
+// Stage one category's matrix into MA[k][i] (row k, column i) such that an
+// operand product reads  y_i = sum_k MA[k][i] v_k:
+//   transpose = true  : MA[k][i] = M[i][k]   (y = M . v)
+//   transpose = false : MA[k][i] = M[k][i]   (y = M^T . v)
+template <typename Real, int SPAD>
+__device__ __forceinline__ void stage_matrix(Real* MA, const Real* __restrict__ M, int Sg,
+                                             bool transpose) {
+    for (int idx = threadIdx.x; idx < SPAD * SPAD; idx += blockDim.x) {
+        const int r = idx / SPAD, q = idx - (idx / SPAD) * SPAD;   // r = row of M, q = col
+        Real v = 0;
+        if (r < Sg && q < Sg) v = __ldg(M + r * Sg + q);
+        if (transpose) MA[q * SPAD + r] = v;
+        else MA[r * SPAD + q] = v;
+    }
+}
+
+// Stage one category's tile of 32 patterns: T[j][p] = x[p0 + p][c][j].
+template <typename Real, int SPAD>
+__device__ __forceinline__ void stage_tile(Real* T, const Real* x, int p0, int c, int C, int Sg) {
+    for (int idx = threadIdx.x; idx < kTP * SPAD; idx += blockDim.x) {
+        const int p = idx / SPAD, j = idx - (idx / SPAD) * SPAD;
+        Real v = 0;
+        if (j < Sg) v = x[((size_t)(p0 + p) * C + c) * Sg + j];
+        T[j * kXS + p] = v;
+    }
+}
+
+// acc[r] = sum_k MA[k][i0 + r] * T[k][lane]  (operand from staged partials),
+// or MA[s][i0 + r] / pad for a tip state s.
+template <typename Real, int SPAD>
+__device__ __forceinline__ void product(const Real* MA, const Real* T, bool states, int s,
+                                        Real pad, int S, int i0, int lane,
+                                        Real acc[SPAD / kNW]) {
+    constexpr int RI = SPAD / kNW;
+    if (states) {
+#pragma unroll
+        for (int r = 0; r < RI; ++r) acc[r] = (s < S) ? MA[s * SPAD + i0 + r] : pad;
+        return;
+    }
+#pragma unroll
+    for (int r = 0; r < RI; ++r) acc[r] = 0;
+    for (int k = 0; k < S; ++k) {
+        const Real v = T[k * kXS + lane];
+        const Real* row = MA + k * SPAD + i0;
+#pragma unroll
+        for (int r = 0; r < RI; ++r) acc[r] += row[r] * v;
+    }
+}
+
+// Rescale pass of the generic kernels: every thread re-reads the values it
+// wrote for its pattern and state slice, after the per-pattern maximum over
+// all categories has been combined across warps in shared memory.
+template <typename Real, int SPAD>
+__device__ __forceinline__ void rescale_tile(const OpDesc& op, Real* red, Real mloc, int p0,
+                                             int lane, int warp, int i0, int S, int C, int Sg,
+                                             double* cum, int log_scalers) {
+    constexpr int RI = SPAD / kNW;
+    red[warp * kTP + lane] = mloc;
+    __syncthreads();
+    Real m = 0;
+#pragma unroll
+    for (int w = 0; w < kNW; ++w) m = red[w * kTP + lane] > m ? red[w * kTP + lane] : m;
+    if (m == Real(0)) m = Real(1);
+    const Real inv = Real(1) / m;
+    Real* d = static_cast<Real*>(op.dest) + (size_t)(p0 + lane) * C * Sg;
+    for (int c = 0; c < C; ++c) {
+#pragma unroll
+        for (int r = 0; r < RI; ++r)
+            if (i0 + r < Sg) d[c * Sg + i0 + r] *= inv;
+    }
+    if (warp == 0) store_scale(m, op.scale_write, cum, p0 + lane, log_scalers);
+    (void)S;
+}
+
+template <typename Real, int SPAD>
+__global__ void __launch_bounds__(256)
+k_postx(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double* cum,
+        int log_scalers) {
+    constexpr int RI = SPAD / kNW;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Real* MA1 = reinterpret_cast<Real*>(smem_raw);
+    Real* MA2 = MA1 + SPAD * SPAD;
+    Real* T1 = MA2 + SPAD * SPAD;
+    Real* T2 = T1 + SPAD * kXS;
+    Real* red = T2 + SPAD * kXS;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int p0 = blockIdx.x * kTP;
+    const int i0 = warp * RI;
+    const int p = p0 + lane;
+    for (int o = 0; o < nops; ++o) {
+        const OpDesc op = ops[o];
+        const bool st1 = op.kind & kX1States, st2 = op.kind & kX2States;
+        const int s1 = st1 ? static_cast<const int*>(op.x1)[p] : 0;
+        const int s2 = st2 ? static_cast<const int*>(op.x2)[p] : 0;
+        const Real inv_read = op.scale_read ? Real(1) / (Real)op.scale_read[p] : Real(1);
+        Real mloc = 0;
+        for (int c = 0; c < C; ++c) {
+            stage_matrix<Real, SPAD>(MA1, static_cast<const Real*>(op.m1) + (size_t)c * Sg * Sg,
+                                     Sg, true);
+            stage_matrix<Real, SPAD>(MA2, static_cast<const Real*>(op.m2) + (size_t)c * Sg * Sg,
+                                     Sg, true);
+            if (!st1) stage_tile<Real, SPAD>(T1, static_cast<const Real*>(op.x1), p0, c, C, Sg);
+            if (!st2) stage_tile<Real, SPAD>(T2, static_cast<const Real*>(op.x2), p0, c, C, Sg);
+            __syncthreads();
+            Real a1[RI], a2[RI];
+            product<Real, SPAD>(MA1, T1, st1, s1, (Real)op.pad1, S, i0, lane, a1);
+            product<Real, SPAD>(MA2, T2, st2, s2, (Real)op.pad2, S, i0, lane, a2);
+            Real* d = static_cast<Real*>(op.dest) + ((size_t)p * C + c) * Sg;
+#pragma unroll
+            for (int r = 0; r < RI; ++r) {
+                Real v = a1[r] * a2[r];
+                if (i0 + r < S) mloc = v > mloc ? v : mloc;
+                if (op.scale_read) v *= inv_read;
+                if (i0 + r < Sg) d[i0 + r] = v;
+            }
+            __syncthreads();
+        }
+        if (op.scale_write)
+            rescale_tile<Real, SPAD>(op, red, mloc, p0, lane, warp, i0, S, C, Sg, cum,
+                                     log_scalers);
+        __syncthreads();
+    }
+}
+
+template <typename Real, int SPAD>
+__global__ void __launch_bounds__(256)
+k_prex(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, int log_scalers) {
+    constexpr int RI = SPAD / kNW;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Real* MA = reinterpret_cast<Real*>(smem_raw);
+    Real* T = MA + SPAD * SPAD;     // sibling tile
+    Real* Z = T + SPAD * kXS;       // parent pre-partials, then z
+    Real* red = Z + SPAD * kXS;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int p0 = blockIdx.x * kTP;
+    const int i0 = warp * RI;
+    const int p = p0 + lane;
+    for (int o = 0; o < nops; ++o) {
+        const OpDesc op = ops[o];
+        const bool st2 = op.kind & kX2States;
+        const bool tr = op.kind & kM1Transposed;
+        const int s2 = st2 ? static_cast<const int*>(op.x2)[p] : 0;
+        Real mloc = 0;
+        for (int c = 0; c < C; ++c) {
+            stage_matrix<Real, SPAD>(MA, static_cast<const Real*>(op.m2) + (size_t)c * Sg * Sg,
+                                     Sg, true);
+            if (!st2) stage_tile<Real, SPAD>(T, static_cast<const Real*>(op.x2), p0, c, C, Sg);
+            stage_tile<Real, SPAD>(Z, static_cast<const Real*>(op.x1), p0, c, C, Sg);
+            __syncthreads();
+            Real a[RI];
+            product<Real, SPAD>(MA, T, st2, s2, (Real)op.pad2, S, i0, lane, a);
+#pragma unroll
+            for (int r = 0; r < RI; ++r) Z[(i0 + r) * kXS + lane] *= a[r];
+            __syncthreads();
+            // dest_j = sum_i P[i][j] z_i: MA[i][j] = P[i][j], or P^T given -> transpose.
+            stage_matrix<Real, SPAD>(MA, static_cast<const Real*>(op.m1) + (size_t)c * Sg * Sg,
+                                     Sg, tr);
+            __syncthreads();
+            product<Real, SPAD>(MA, Z, false, 0, Real(0), S, i0, lane, a);
+            Real* d = static_cast<Real*>(op.dest) + ((size_t)p * C + c) * Sg;
+#pragma unroll
+            for (int r = 0; r < RI; ++r) {
+                if (i0 + r < S) mloc = a[r] > mloc ? a[r] : mloc;
+                if (i0 + r < Sg) d[i0 + r] = a[r];
+            }
+            __syncthreads();
+        }
+        if (op.scale_write)
+            rescale_tile<Real, SPAD>(op, red, mloc, p0, lane, warp, i0, S, C, Sg, nullptr,
+                                     log_scalers);
+        __syncthreads();
+    }
+}
+
+template <typename Real, int SPAD>
+size_t smem_postx() { return sizeof(Real) * (2 * SPAD * SPAD + 2 * SPAD * kXS + kNW * kTP); }
+template <typename Real, int SPAD>
+size_t smem_prex() { return sizeof(Real) * (SPAD * SPAD + 2 * SPAD * kXS + kNW * kTP); }
+
+template <typename Real, int SPAD>
+cudaError_t run_postx(const OpDesc* ops, int nops, const Dims& d, double* cum, int ls,
+                      cudaStream_t s) {
+    const size_t sm = smem_postx<Real, SPAD>();
+    cudaError_t e = cudaFuncSetAttribute(k_postx<Real, SPAD>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_postx<Real, SPAD><<<d.Pp / kTP, kNW * 32, sm, s>>>(ops, nops, d.S, d.Sg, d.C, cum, ls);
+    return cudaGetLastError();
+}
+
+template <typename Real, int SPAD>
+cudaError_t run_prex(const OpDesc* ops, int nops, const Dims& d, int ls, cudaStream_t s) {
+    const size_t sm = smem_prex<Real, SPAD>();
+    cudaError_t e = cudaFuncSetAttribute(k_prex<Real, SPAD>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_prex<Real, SPAD><<<d.Pp / kTP, kNW * 32, sm, s>>>(ops, nops, d.S, d.Sg, d.C, ls);
+    return cudaGetLastError();
+}
+
+template <typename Real, int C>
+cudaError_t run_post4(const OpDesc* ops, int nops, const Dims& d, double* cum, int ls,
+                      cudaStream_t s) {
+    k_post4<Real, C><<<(d.Pp + 127) / 128, 128, 0, s>>>(ops, nops, d.Pp, cum, ls);
+    return cudaGetLastError();
+}
+
+template <typename Real, int C>
+cudaError_t run_pre4(const OpDesc* ops, int nops, const Dims& d, int ls, cudaStream_t s) {
+    k_pre4<Real, C><<<(d.Pp + 127) / 128, 128, 0, s>>>(ops, nops, d.Pp, ls);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+template <typename Real>
+cudaError_t launch_update_partials(const OpDesc* ops, int nops, const Dims& d, double* cum,
+                                   int ls, cudaStream_t s) {
+    if (nops == 0) return cudaSuccess;
+    if (d.S == 4 && d.C <= 8) {
+        switch (d.C) {
+            case 1: return run_post4<Real, 1>(ops, nops, d, cum, ls, s);
+            case 2: return run_post4<Real, 2>(ops, nops, d, cum, ls, s);
+            case 3: return run_post4<Real, 3>(ops, nops, d, cum, ls, s);
+            case 4: return run_post4<Real, 4>(ops, nops, d, cum, ls, s);
+            case 5: return run_post4<Real, 5>(ops, nops, d, cum, ls, s);
+            case 6: return run_post4<Real, 6>(ops, nops, d, cum, ls, s);
+            case 7: return run_post4<Real, 7>(ops, nops, d, cum, ls, s);
+            default: return run_post4<Real, 8>(ops, nops, d, cum, ls, s);
+        }
+    }
+    if (d.Sg <= 8) return run_postx<Real, 8>(ops, nops, d, cum, ls, s);
+    if (d.Sg <= 16) return run_postx<Real, 16>(ops, nops, d, cum, ls, s);
+    if (d.Sg <= 24) return run_postx<Real, 24>(ops, nops, d, cum, ls, s);
+    if (d.Sg <= 32) return run_postx<Real, 32>(ops, nops, d, cum, ls, s);
+    if (d.Sg <= 48) return run_postx<Real, 48>(ops, nops, d, cum, ls, s);
+    if (d.Sg <= 64) return run_postx<Real, 64>(ops, nops, d, cum, ls, s);
+    return cudaErrorInvalidValue;
+}
+
+template <typename Real>
+cudaError_t launch_update_pre_partials(const OpDesc* ops, int nops, const Dims& d, int ls,
+                                       cudaStream_t s) {
+    if (nops == 0) return cudaSuccess;
+    if (d.S == 4 && d.C <= 8) {
+        switch (d.C) {
+            case 1: return run_pre4<Real, 1>(ops, nops, d, ls, s);
+            case 2: return run_pre4<Real, 2>(ops, nops, d, ls, s);
+            case 3: return run_pre4<Real, 3>(ops, nops, d, ls, s);
+            case 4: return run_pre4<Real, 4>(ops, nops, d, ls, s);
+            case 5: return run_pre4<Real, 5>(ops, nops, d, ls, s);
+            case 6: return run_pre4<Real, 6>(ops, nops, d, ls, s);
+            case 7: return run_pre4<Real, 7>(ops, nops, d, ls, s);
+            default: return run_pre4<Real, 8>(ops, nops, d, ls, s);
+        }
+    }
+    if (d.Sg <= 8) return run_prex<Real, 8>(ops, nops, d, ls, s);
+    if (d.Sg <= 16) return run_prex<Real, 16>(ops, nops, d, ls, s);
+    if (d.Sg <= 24) return run_prex<Real, 24>(ops, nops, d, ls, s);
+    if (d.Sg <= 32) return run_prex<Real, 32>(ops, nops, d, ls, s);
+    if (d.Sg <= 48) return run_prex<Real, 48>(ops, nops, d, ls, s);
+    if (d.Sg <= 64) return run_prex<Real, 64>(ops, nops, d, ls, s);
+    return cudaErrorInvalidValue;
+}
+
+template cudaError_t launch_update_partials<float>(const OpDesc*, int, const Dims&, double*, int,
+                                                   cudaStream_t);
+template cudaError_t launch_update_partials<double>(const OpDesc*, int, const Dims&, double*, int,
+                                                    cudaStream_t);
+template cudaError_t launch_update_pre_partials<float>(const OpDesc*, int, const Dims&, int,
+                                                       cudaStream_t);
+template cudaError_t launch_update_pre_partials<double>(const OpDesc*, int, const Dims&, int,
+                                                        cudaStream_t);
+
+}  // namespace b200

@@ -1,0 +1,33 @@
+// Small device utilities used by the host instance: filling pre-order root
+// partials with the state frequencies.
+#include "b200_kernels.h"
+
+namespace b200 {
+
+namespace {
+
+// dest[p][c][i] = freqs[i] for i < S, 0 for the padded states
+// (CPU/BeagleCPUImpl.hpp:621-676, beagleSetRootPrePartials).
+template <typename Real>
+__global__ void k_fill_root(Real* dest, const double* __restrict__ freqs, int S, int Sg,
+                            size_t n) {
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    const int i = (int)(idx % Sg);
+    dest[idx] = (i < S) ? (Real)freqs[i] : Real(0);
+}
+
+}  // namespace
+
+template <typename Real>
+cudaError_t launch_fill_root(void* dest, const double* freqs, const Dims& d, cudaStream_t s) {
+    const size_t n = (size_t)d.Pp * d.C * d.Sg;
+    k_fill_root<Real><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(static_cast<Real*>(dest), freqs,
+                                                                   d.S, d.Sg, n);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_fill_root<float>(void*, const double*, const Dims&, cudaStream_t);
+template cudaError_t launch_fill_root<double>(void*, const double*, const Dims&, cudaStream_t);
+
+}  // namespace b200

@@ -1,0 +1,423 @@
+"""Seeded synthetic phylogenetic workloads and the BEAGLE call sequence that
+evaluates lnL and the branch-length gradient.
+
+There is no public dataset for this path; these generators stand in for one,
+with the shapes and distributions the benchmark configurations name.  They play
+the role of the reference's ``examples/synthetictest`` (random-join trees,
+``synthetictest.cpp:986-1021``) and ``examples/hmctest`` (the pre-order /
+edge-derivative call sequence, ``hmctest.cpp:398-703``), with numpy
+``PCG64(seed)`` streams instead of the reference's LCG.
+
+Buffer conventions used by :class:`Problem` for a rooted binary tree with N
+tips (node ids: tips 0..N-1, internal N..2N-2, root 2N-2, B = 2N-2 branches):
+
+* post-order partials of node v: buffer v;
+* pre-order partials of node v: buffer (2N-1) + v;
+* transition matrix of the branch above node v: matrix v (v < B); the
+  rate-scaled generator Q*r_c used as the derivative matrix: matrix B; the
+  transposed P of node v (pre-order operand under the GPU's manual-transpose
+  convention for S > 4): matrix B + 1 + v;
+* scale buffers: post-order node v -> v - N, pre-order node v -> (N-1) + v,
+  cumulative -> 3N - 3.
+"""
+
+import numpy as np
+from dataclasses import dataclass, field
+
+OP_NONE = -1
+
+# NCBI standard genetic code (table 1), codons ordered TCAG at each position.
+_AA = "FFLLSSSSYY**CC*WLLLLPPPPHHQQRRRRIIIMTTTTNNKKSSRRVVVVAAAADDEEGGGG"
+_NUC = "TCAG"
+
+
+def random_tree(n_taxa, rng):
+    """Random-join rooted binary tree (the topology process of
+    synthetictest.cpp:986-1021): each new tip is joined, through a new parent,
+    to a uniformly chosen existing node.  Returns (parent, children) with tips
+    0..N-1, internal nodes N..2N-2 and the root relabelled 2N-2."""
+    N = n_taxa
+    parent = {0: -1}
+    children = {}
+    nodes = [0]
+    next_internal = N
+    for tip in range(1, N):
+        sib = nodes[int(rng.integers(len(nodes)))]
+        newp = next_internal
+        next_internal += 1
+        gp = parent[sib]
+        parent[newp] = gp
+        if gp >= 0:
+            kids = children[gp]
+            kids[kids.index(sib)] = newp
+        children[newp] = [sib, tip]
+        parent[sib] = newp
+        parent[tip] = newp
+        nodes += [tip, newp]
+    root = next(v for v, p in parent.items() if p < 0)
+    want = 2 * N - 2
+    if root != want:                                  # swap labels root <-> 2N-2
+        def rl(v):
+            return want if v == root else (root if v == want else v)
+        parent = {rl(v): (rl(p) if p >= 0 else -1) for v, p in parent.items()}
+        children = {rl(v): [rl(c) for c in kids] for v, kids in children.items()}
+    par = np.full(2 * N - 1, -1, dtype=np.int64)
+    for v, p in parent.items():
+        par[v] = p
+    ch = np.zeros((2 * N - 1, 2), dtype=np.int64) - 1
+    for v, kids in children.items():
+        ch[v] = kids
+    return par, ch
+
+
+def postorder(ch, root):
+    out, stack = [], [(root, False)]
+    while stack:
+        v, done = stack.pop()
+        if ch[v, 0] < 0:
+            continue
+        if done:
+            out.append(v)
+        else:
+            stack.append((v, True))
+            stack.append((int(ch[v, 1]), False))
+            stack.append((int(ch[v, 0]), False))
+    return out
+
+
+def preorder_nonroot(ch, root):
+    out, stack = [], [root]
+    while stack:
+        v = stack.pop()
+        for c in ch[v]:
+            if c >= 0:
+                out.append(int(c))
+                stack.append(int(c))
+    return out
+
+
+def eigen_reversible(Q, pi):
+    """Eigensystem of a reversible Q through the symmetric form
+    D^1/2 Q D^-1/2; returns (V, V^-1, lambda) with Q = V diag(lambda) V^-1."""
+    d = np.sqrt(pi)
+    A = d[:, None] * Q / d[None, :]
+    A = 0.5 * (A + A.T)
+    lam, U = np.linalg.eigh(A)
+    V = U / d[:, None]
+    Vi = U.T * d[None, :]
+    return V, Vi, lam
+
+
+def _normalise(R, pi):
+    Q = R * pi[None, :]
+    np.fill_diagonal(Q, 0.0)
+    np.fill_diagonal(Q, -Q.sum(axis=1))
+    mu = -np.dot(pi, np.diag(Q))
+    return Q / mu
+
+
+def gtr_model(rng):
+    """4-state GTR: exchangeabilities ~ U(0.5, 2), frequencies ~ Dirichlet(1,1,1,1)."""
+    pi = rng.dirichlet(np.ones(4))
+    R = np.zeros((4, 4))
+    iu = np.triu_indices(4, 1)
+    R[iu] = rng.uniform(0.5, 2.0, size=len(iu[0]))
+    R = R + R.T
+    return _normalise(R, pi), pi
+
+
+def amino_model(rng, S=20):
+    """S-state model: symmetric exchangeabilities ~ Gamma(1,1), pi ~ Dirichlet(1 x S)."""
+    pi = rng.dirichlet(np.ones(S))
+    R = np.zeros((S, S))
+    iu = np.triu_indices(S, 1)
+    R[iu] = rng.gamma(1.0, 1.0, size=len(iu[0]))
+    R = R + R.T
+    return _normalise(R, pi), pi
+
+
+def codon_model(rng):
+    """Goldman-Yang style 61-state codon model: kappa ~ U(1,4), omega ~ U(0.1,1),
+    codon frequencies ~ Dirichlet(1 x 61); single-nucleotide changes only."""
+    kappa = rng.uniform(1.0, 4.0)
+    omega = rng.uniform(0.1, 1.0)
+    codons = [a + b + c for a in _NUC for b in _NUC for c in _NUC]
+    sense = [(cd, _AA[i]) for i, cd in enumerate(codons) if _AA[i] != "*"]
+    S = len(sense)
+    pi = rng.dirichlet(np.ones(S))
+    R = np.zeros((S, S))
+    purine = set("AG")
+    for i, (ci, ai) in enumerate(sense):
+        for j, (cj, aj) in enumerate(sense):
+            if i == j:
+                continue
+            diff = [k for k in range(3) if ci[k] != cj[k]]
+            if len(diff) != 1:
+                continue
+            x, y = ci[diff[0]], cj[diff[0]]
+            r = 1.0
+            if (x in purine) == (y in purine):
+                r *= kappa
+            if ai != aj:
+                r *= omega
+            R[i, j] = r
+    return _normalise(R, pi), pi
+
+
+def discrete_gamma(alpha, ncat):
+    """Mean-of-category discrete gamma rates (Yang 1994), equal weights."""
+    if ncat == 1:
+        return np.ones(1), np.ones(1)
+    from scipy.special import gammainc
+    from scipy.stats import gamma
+    cuts = gamma.ppf(np.arange(1, ncat) / ncat, alpha, scale=1.0 / alpha)
+    edges = np.concatenate([[0.0], cuts, [np.inf]])
+    cdf1 = gammainc(alpha + 1.0, edges * alpha)
+    rates = ncat * np.diff(cdf1)
+    rates *= ncat / rates.sum()
+    return rates, np.full(ncat, 1.0 / ncat)
+
+
+@dataclass
+class Problem:
+    """One likelihood+gradient workload (a tree, a model and data) and the
+    BEAGLE call sequence over it."""
+    N: int
+    S: int
+    P: int
+    C: int
+    parent: np.ndarray
+    children: np.ndarray
+    lengths: np.ndarray            # [B] branch length above node v
+    Q: np.ndarray
+    pi: np.ndarray
+    V: np.ndarray
+    Vi: np.ndarray
+    lam: np.ndarray
+    rates: np.ndarray
+    catw: np.ndarray
+    patw: np.ndarray
+    tip_states: np.ndarray         # [N][P] (S = missing)
+    tip_partials: dict = field(default_factory=dict)   # tip -> [P*S] for ambiguous tips
+    rescale: bool = False
+    seed: int = 0
+    name: str = ""
+
+    @property
+    def B(self):
+        return 2 * self.N - 2
+
+    @property
+    def root(self):
+        return 2 * self.N - 2
+
+    @property
+    def n_buffers(self):
+        return 2 * (2 * self.N - 1)
+
+    @property
+    def n_matrices(self):
+        return 2 * self.B + 1
+
+    @property
+    def n_scale(self):
+        return 3 * self.N - 2
+
+    @property
+    def cumulative(self):
+        return 3 * self.N - 3
+
+    def pre(self, v):
+        return 2 * self.N - 1 + v
+
+    def compact_tips(self):
+        return [t for t in range(self.N) if t not in self.tip_partials]
+
+    def create_args(self):
+        """(tipCount, partialsBufferCount, compactBufferCount, S, P, eigen, matrices,
+        categories, scale buffers) for beagleCreateInstance."""
+        nc = len(self.compact_tips())
+        return (self.N, self.n_buffers - nc, nc, self.S, self.P, 1, self.n_matrices,
+                self.C, self.n_scale)
+
+    def post_ops(self):
+        ops = []
+        for v in postorder(self.children, self.root):
+            c1, c2 = (int(x) for x in self.children[v])
+            ws = v - self.N if self.rescale else OP_NONE
+            ops.append([v, ws, OP_NONE, c1, c1, c2, c2])
+        return np.array(ops, dtype=np.int32)
+
+    def pre_ops(self, transposed_matrices=False):
+        """Pre-order ops (dest, write, read, pre(parent), P_node, sibling, P_sib).
+        With ``transposed_matrices`` the node's matrix index points at its
+        transposed copy (B + 1 + v)."""
+        ops = []
+        for v in preorder_nonroot(self.children, self.root):
+            p = int(self.parent[v])
+            sib = int(self.children[p, 0] if self.children[p, 1] == v else self.children[p, 1])
+            ws = (self.N - 1) + v if self.rescale else OP_NONE
+            m = self.B + 1 + v if transposed_matrices else v
+            ops.append([self.pre(v), ws, OP_NONE, self.pre(p), m, sib, sib])
+        return np.array(ops, dtype=np.int32)
+
+    def scaled_q(self):
+        """[C][S][S] derivative matrices Q * r_c (hmctest.cpp:398-407)."""
+        return np.stack([self.Q * r for r in self.rates])
+
+    def root_pre_partials(self):
+        return np.broadcast_to(self.pi, (self.C, self.P, self.S)).reshape(-1).copy()
+
+    def set_root_pre(self, inst):
+        """Pre-order root partials = state frequencies (hmctest.cpp:550-559),
+        through beagleSetRootPrePartials where the instance implements it."""
+        if getattr(inst, "_no_root_pre", False):
+            inst.setPartials(self.pre(self.root), self.root_pre_partials())
+            return
+        code = inst.setRootPrePartials([self.pre(self.root)], [0], check=False)
+        if code == -7:                       # BEAGLE_ERROR_NO_IMPLEMENTATION
+            inst._no_root_pre = True
+            inst.setPartials(self.pre(self.root), self.root_pre_partials())
+        elif code < 0:
+            raise RuntimeError(f"setRootPrePartials returned {code}")
+
+    def load(self, inst, transposed_pre=False):
+        """Set tips, model and weights on an instance (any object with the
+        beagle.h method names of ``binding.Instance``)."""
+        for t in range(self.N):
+            if t in self.tip_partials:
+                inst.setTipPartials(t, self.tip_partials[t])
+            else:
+                inst.setTipStates(t, self.tip_states[t])
+        inst.setEigenDecomposition(0, self.V.reshape(-1), self.Vi.reshape(-1), self.lam)
+        inst.setStateFrequencies(0, self.pi)
+        inst.setCategoryWeights(0, self.catw)
+        inst.setCategoryRates(self.rates)
+        inst.setPatternWeights(self.patw)
+        inst.setTransitionMatrix(self.B, self.scaled_q().reshape(-1), 0.0)
+
+    def evaluate(self, inst, gradient=True, transposed_pre=False, lengths=None, mark=None):
+        """One lnL (+ gradient) evaluation: the call sequence of BASELINE's metric.
+
+        updateTransitionMatrices (all B branches) -> updatePartials (N-1 ops) ->
+        scale accumulation -> root lnL -> root pre-partials -> updatePrePartials
+        (B ops) -> calculateEdgeDerivatives (all B branches, sums only).
+        Returns (lnL, gradient[B] or None)."""
+        mark = mark or (lambda name: None)
+        t = self.lengths if lengths is None else lengths
+        idx = np.arange(self.B, dtype=np.int32)
+        mark("start")
+        inst.updateTransitionMatrices(0, idx, None, None, t)
+        mark("matrices")
+        inst.updatePartials(self.post_ops(), OP_NONE)
+        mark("post")
+        cum = OP_NONE
+        if self.rescale:
+            cum = self.cumulative
+            inst.resetScaleFactors(cum)
+            inst.accumulateScaleFactors(np.arange(self.N - 1, dtype=np.int32), cum)
+        mark("scale")
+        lnl = inst.calculateRootLogLikelihoods([self.root], [0], [0], [cum])
+        mark("root")
+        if not gradient:
+            return lnl, None
+        if transposed_pre:
+            inst.transposeTransitionMatrices(idx, idx + self.B + 1)
+        self.set_root_pre(inst)
+        mark("rootpre")
+        inst.updatePrePartials(self.pre_ops(transposed_pre), OP_NONE)
+        mark("pre")
+        nonroot = np.arange(self.B, dtype=np.int32)
+        _, sums, _ = inst.calculateEdgeDerivatives(
+            nonroot, nonroot + self.pre(0), np.full(self.B, self.B, dtype=np.int32),
+            [0], per_site=False, sums=True, sumsq=False)
+        mark("deriv")
+        return lnl, sums
+
+    def algorithmic_bytes(self, w):
+        """Compulsory traffic per phase of one evaluation, with w bytes per real:
+        each operation reads each input once and writes each output once
+        (synthetictest.cpp:2567-2580 generalised to the pre-order and derivative
+        passes).  Partials buffer L = P*C*S*w (S unpadded), compact tip = 4P,
+        scale factors 8P per rescaled node (FP64 on this resource)."""
+        L = self.P * self.C * self.S * w
+        tip = 4 * self.P
+        compact = set(self.compact_tips())
+
+        def rd(v):
+            return tip if v in compact else L
+
+        sc = 8 * self.P if self.rescale else 0
+        post = sum(rd(op[3]) + rd(op[5]) + L + sc for op in self.post_ops())
+        pre = sum(L + rd(op[5]) + L + sc for op in self.pre_ops())
+        deriv = sum(L + rd(v) for v in range(self.B))
+        mats = self.B * self.C * self.S * self.S * w
+        return dict(matrices=mats, post=post, pre=pre, deriv=deriv)
+
+
+def make_problem(S, N, P, C, seed, mean_length=0.1, ambiguous=0.0, rescale=False,
+                 alpha=0.5, weights=(1, 5), name=""):
+    """Build a Problem: random-join tree, Exp(mean_length) branch lengths, a
+    GTR (S=4), random-exchangeability (S=20 or other) or GY codon (S=61) model,
+    discrete-gamma rates, uniform tip states (``ambiguous`` fraction of tip
+    cells given as all-ones partials), pattern weights ~ U{lo..hi}."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    par, ch = random_tree(N, rng)
+    B = 2 * N - 2
+    lengths = rng.exponential(mean_length, size=B)
+    if S == 4:
+        Q, pi = gtr_model(rng)
+    elif S == 61:
+        Q, pi = codon_model(rng)
+    else:
+        Q, pi = amino_model(rng, S)
+    V, Vi, lam = eigen_reversible(Q, pi)
+    rates, catw = discrete_gamma(alpha, C)
+    patw = rng.integers(weights[0], weights[1] + 1, size=P).astype(np.float64)
+    states = rng.integers(0, S, size=(N, P))
+    tip_partials = {}
+    if ambiguous > 0:
+        amb = rng.random((N, P)) < ambiguous
+        for t in range(N):
+            part = np.zeros((P, S))
+            part[np.arange(P), states[t]] = 1.0
+            part[amb[t]] = 1.0
+            tip_partials[t] = part.reshape(-1)
+    return Problem(N=N, S=S, P=P, C=C, parent=par, children=ch, lengths=lengths, Q=Q,
+                   pi=pi, V=V, Vi=Vi, lam=lam, rates=rates, catw=catw, patw=patw,
+                   tip_states=states, tip_partials=tip_partials, rescale=rescale,
+                   seed=seed, name=name)
+
+
+# The benchmark configurations (sizes and distributions of each workload).
+CONFIGS = {
+    "gtr4_n16_p1000": dict(S=4, N=16, P=1000, C=4, seed=1000, mean_length=0.1,
+                           ambiguous=0.05, rescale=False),
+    "gtr4_n128_p100k": dict(S=4, N=128, P=100000, C=4, seed=1001, mean_length=0.05,
+                            rescale=True),
+    "aa20_n64_p20k": dict(S=20, N=64, P=20000, C=4, seed=1002, mean_length=0.1,
+                          rescale=True),
+    "codon61_n32_p10k": dict(S=61, N=32, P=10000, C=4, seed=1003, mean_length=0.1,
+                             rescale=True),
+}
+
+
+def config_problem(name, **over):
+    kw = dict(CONFIGS[name])
+    kw.update(over)
+    return make_problem(name=name, **kw)
+
+
+def batched_problems(count=256, seed=2000, max_patterns=50000):
+    """Heterogeneous batch: per partition N ~ U{16..256}, S in {4 (70%), 20 (30%)},
+    C in {1,4,8}, P log-uniform in [100, max_patterns]."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for i in range(count):
+        S = 4 if rng.random() < 0.7 else 20
+        N = int(rng.integers(16, 257))
+        C = int(rng.choice([1, 4, 8]))
+        P = int(np.exp(rng.uniform(np.log(100), np.log(max_patterns))))
+        out.append(make_problem(S=S, N=N, P=P, C=C, seed=seed + 1 + i,
+                                mean_length=0.1, rescale=True, name=f"part{i}"))
+    return out

@@ -1,0 +1,404 @@
+#!/usr/bin/env python
+"""Benchmark: lnL + branch-gradient evaluations per second on B200.
+
+One step is one evaluation of the BEAGLE hot path on the 4-state GTR+Gamma4
+workload with 128 taxa and 100,000 site patterns (FP32 partials, per-node
+rescaling, FP64 P(t) and reductions):
+
+    updateTransitionMatrices (254 branches) -> updatePartials (127 ops)
+    -> scale accumulation -> root lnL -> root pre-partials
+    -> updatePrePartials (254 ops) -> calculateEdgeDerivatives (254 branches)
+
+through libbeagle_b200.so's C ABI.  ``value`` queues K evaluations on the
+instance's stream (ASYNCH instance, inputs resident) and times them with CUDA
+events on that stream; ``e2e`` runs K evaluations that each copy new branch
+lengths in and read lnL and the gradient back (host round trip per step).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun (N > 1) every rank evaluates its own tree (weak scaling, no
+collective on the data path); rank 0 prints the JSON line with the maximum
+device time over ranks.  ``--impl reference`` times the reference's own CPU
+implementation (the compiled beagle-lib CPU plugins under oracle/_ref) on the
+host cores instead, rank 0 only.
+"""
+import argparse
+import importlib
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+WORKLOAD = "gtr4_n128_p100k"
+METRIC = "lnL+gradient evals/s, mixed-batched vs plain FP64 on B200 at rel lnL err ≤1e-6"
+
+SINGLE, DOUBLE, ASYNCH = 1 << 0, 1 << 1, 1 << 3
+SCALERS_LOG = 1 << 10
+THREADING_CPP = 1 << 30
+PROC_CPU, PROC_GPU = 1 << 15, 1 << 16
+FW_CUDA, FW_CPU = 1 << 22, 1 << 27
+PRE_MANUAL = 1 << 30
+
+# Our kernels launched per evaluation: P(t) 1, post-order 1, scale accumulate 1,
+# root lnL 2 (sites + final sum), root pre-partials fill 1, pre-order 1,
+# edge derivatives 2 (branches x pattern blocks + final sum).
+LAUNCHES_PER_EVAL = 9
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.t0 = self.t1 = None
+
+    def start(self):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def mark(self, which):
+        setattr(self, which, time.time())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[4:]))
+            except ValueError:
+                continue
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for _, _, r in rows:
+            for n, v in zip(names, r[1:5]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        sm = [r[0] for r in rows]
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": rows[0][1],
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return ws, rank, local
+
+
+def max_over_ranks(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ----------------------------------------------------------------- CPU side
+def reference_lib():
+    pkg = importlib.import_module("beagle-lib_b200")
+    path = os.path.join(ROOT, "oracle", "_ref", "libhmsbeagle.so")
+    if not os.path.exists(path):
+        return None
+    return pkg.binding.BeagleLib(path, "beagle")
+
+
+def cpu_reference_rate(workload, seconds=10.0, sample_patterns=4000, max_evals=50):
+    """The reference CPU implementation (compiled beagle-lib, SSE plugin with
+    C++ threads on every host core) on a pattern sample of the workload.
+    Returns (evals/s of the full workload, info)."""
+    pkg = importlib.import_module("beagle-lib_b200")
+    lib = reference_lib()
+    if lib is None:
+        return None, {"unavailable": "oracle/_ref not built"}
+    full = pkg.synthetic.CONFIGS[workload]
+    sample = min(sample_patterns, full["P"])
+    pr = pkg.synthetic.config_problem(workload, P=sample)
+    cores = os.cpu_count() or 1
+    inst = lib.create(*pr.create_args(),
+                      preferenceFlags=DOUBLE | PROC_CPU | SCALERS_LOG | THREADING_CPP,
+                      requirementFlags=DOUBLE | FW_CPU)
+    inst.setCPUThreadCount(cores)
+    pr.load(inst)
+    pr.evaluate(inst)
+    n, t0 = 0, time.perf_counter()
+    while n < max_evals and (time.perf_counter() - t0) < seconds:
+        pr.evaluate(inst)
+        n += 1
+    dt = time.perf_counter() - t0
+    rate = n / dt * sample / full["P"]
+    info = {"impl": inst.impl_name, "cores": cores, "evals": n, "seconds": dt,
+            "sample": f"{sample} of {full['P']} patterns, same tree and model, {n} evals "
+                      f"in {dt:.1f}s; evals/s scaled by {sample}/{full['P']}"}
+    inst.finalize()
+    return rate, info
+
+
+def run_reference_arm(args):
+    ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    if reference_lib() is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built"}))
+        return
+    pkg = importlib.import_module("beagle-lib_b200")
+    full = pkg.synthetic.CONFIGS[args.workload]
+    # warm-up, then K steps; each step a bounded pattern sample of the workload
+    sample = min(2000, full["P"])
+    lib = reference_lib()
+    pr = pkg.synthetic.config_problem(args.workload, P=sample)
+    cores = os.cpu_count() or 1
+    inst = lib.create(*pr.create_args(),
+                      preferenceFlags=DOUBLE | PROC_CPU | SCALERS_LOG | THREADING_CPP,
+                      requirementFlags=DOUBLE | FW_CPU)
+    inst.setCPUThreadCount(cores)
+    pr.load(inst)
+    for _ in range(args.warmup):
+        pr.evaluate(inst)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        pr.evaluate(inst)
+    dt = time.perf_counter() - t0
+    rate = args.steps / dt * sample / full["P"]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": "evals/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 / rate, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "implementation": inst.impl_name,
+                   "threads": cores},
+        "cpu_baseline": {"value": rate, "unit": "evals/s", "cores": cores, "kind": "reference",
+                         "sample": f"{sample} of {full['P']} patterns per step, evals/s scaled "
+                                   f"by {sample}/{full['P']}"},
+        "e2e": {"value": rate, "unit": "evals/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ----------------------------------------------------------------- GPU side
+def make_instance(lib, pr, precision, device, asynch=True):
+    pref = (SINGLE if precision == "single" else DOUBLE) | SCALERS_LOG | PROC_GPU | PRE_MANUAL
+    if asynch:
+        pref |= ASYNCH
+    req = (SINGLE if precision == "single" else DOUBLE) | FW_CUDA
+    inst = lib.create(*pr.create_args(), resources=[device], preferenceFlags=pref,
+                      requirementFlags=req)
+    pr.load(inst)
+    return inst
+
+
+def timed_value(torch, inst, pr, steps, warmup, phases=False):
+    """Queue `steps` evaluations (ASYNCH) and time them on the instance's stream.
+    With phases=True also time every phase of every step."""
+    stream = torch.cuda.ExternalStream(inst.cudaStream())
+    tr = pr.S > 4
+    for _ in range(warmup):
+        pr.evaluate(inst, transposed_pre=tr)
+        inst.getLogLikelihood()
+    ev_marks = []
+
+    def mark(name):
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(stream)
+        ev_marks.append((name, e))
+
+    torch.cuda.synchronize()
+    inst.waitForPartials([])
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(steps):
+        pr.evaluate(inst, transposed_pre=tr, mark=mark if phases else None)
+    end.record(stream)
+    end.synchronize()
+    lnl = inst.getLogLikelihood()
+    total = start.elapsed_time(end)
+    per_phase = {}
+    if phases:
+        for (n0, e0), (n1, e1) in zip(ev_marks, ev_marks[1:]):
+            if n1 == "start":
+                continue
+            per_phase.setdefault(n1, []).append(e0.elapsed_time(e1))
+    return total, lnl, per_phase
+
+
+def timed_e2e(torch, inst, pr, steps):
+    """Steps with new branch lengths copied in from pinned host memory and lnL +
+    gradient read back every step (the host round trip a caller sees)."""
+    stream = torch.cuda.ExternalStream(inst.cudaStream())
+    rng = np.random.default_rng(7)
+    lengths = torch.empty(pr.B, dtype=torch.float64).pin_memory()
+    host = lengths.numpy()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    inst.waitForPartials([])
+    start.record(stream)
+    for k in range(steps):
+        host[:] = pr.lengths * (1.0 + 1e-3 * rng.standard_normal(pr.B))
+        pr.evaluate(inst, transposed_pre=pr.S > 4, lengths=host)
+        inst.getLogLikelihood()          # waits for lnL and the gradient sums
+    end.record(stream)
+    end.synchronize()
+    # bytes per step: the P(t) job table (branch lengths inside) in, lnL + gradient out
+    h2d = pr.B * 56
+    d2h = 8 + 2 * pr.B * 8
+    return start.elapsed_time(end), h2d, d2h
+
+
+def run_b200_arm(args):
+    import torch
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    pkg = importlib.import_module("beagle-lib_b200")
+    syn = pkg.synthetic
+    lib = pkg.load()
+    # weak scaling: rank r evaluates its own tree and data (seed offset r)
+    base = syn.CONFIGS[args.workload]
+    pr = syn.config_problem(args.workload, seed=base["seed"] + 7919 * rank)
+
+    clocks = Clocks(local)
+    inst = make_instance(lib, pr, "single", local)
+    clocks.start()
+    barrier(ws)
+    ms_total, lnl, _ = timed_value(torch, inst, pr, args.steps, args.warmup)
+    clocks_info = clocks.stop()
+    ms_total = max_over_ranks(ms_total, ws)
+    ms_step = ms_total / args.steps
+    value = ws * args.steps / (ms_total / 1000.0)
+
+    # per-phase device times (separate pass) for the roofline of the top kernel
+    nph = max(5, min(50, args.steps // 4))
+    _, _, phases = timed_value(torch, inst, pr, nph, 1, phases=True)
+    ph_ms = {k: float(np.mean(v)) for k, v in phases.items()}
+    alg = pr.algorithmic_bytes(4)
+    kern = max(["post", "pre", "deriv"], key=lambda k: ph_ms.get(k, 0))
+    peak, peak_kind = peaks()
+    achieved = alg[kern] / (ph_ms[kern] * 1e-3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "dram_traffic_per_launch.json")
+    if os.path.exists(tf):
+        traffic = json.load(open(tf)).get(args.workload, {}).get(kern)
+
+    # end-to-end through the C ABI with host round trips
+    ms_e2e, h2d, d2h = timed_e2e(torch, inst, pr, max(5, args.steps // 5))
+    e2e_steps = max(5, args.steps // 5)
+    e2e_value = ws * e2e_steps / (max_over_ranks(ms_e2e, ws) / 1000.0)
+    inst.finalize()
+
+    # the plain FP64 path (one instance, same workload) for the mixed/FP64 ratio
+    inst64 = make_instance(lib, pr, "double", local)
+    k64 = max(5, args.steps // 3)
+    ms64, lnl64, _ = timed_value(torch, inst64, pr, k64, min(args.warmup, 3))
+    ms64 = max_over_ranks(ms64, ws)
+    value64 = ws * k64 / (ms64 / 1000.0)
+    inst64.finalize()
+    rel_err = abs(lnl - lnl64) / abs(lnl64)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        rate, info = cpu_reference_rate(args.workload)
+        if rate is not None:
+            cpu = {"value": rate, "unit": "evals/s", "cores": info["cores"],
+                   "kind": "reference", "sample": info["sample"] + f"; {info['impl']}"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "states": pr.S, "taxa": pr.N,
+                       "patterns": pr.P, "categories": pr.C, "branches": pr.B,
+                       "precision": "FP32 partials, FP64 P(t), scalers and reductions",
+                       "rescaling": "every internal node, post- and pre-order",
+                       "l2": "inputs larger than L2 (%.1f GB of partials)" % (
+                           pr.n_buffers * pr.P * pr.C * pr.S * 4 / 1e9),
+                       "parallelism": f"replicas x{ws}", "seed": int(pr.seed)},
+            "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "algorithmic_bytes": alg[kern],
+                         "ms_per_launch": ph_ms[kern], "phase_ms": ph_ms},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "plain_fp64": {"value": value64, "unit": "evals/s", "ms_per_step": ms64 / k64,
+                           "mixed_over_fp64": value / value64,
+                           "mixed_vs_fp64_rel_lnl_err": rel_err},
+            "lnl": lnl,
+            "gpu_launches": LAUNCHES_PER_EVAL * args.steps,
+            "clocks": clocks_info,
+        }
+        print(json.dumps(line))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_b200_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,318 @@
+/*
+ * beagle_b200.h -- C ABI of the B200 (sm_100a) resource for BEAGLE's
+ * phylogenetic-likelihood hot path.
+ *
+ * Every entry point is the beagle.h call of the same name with the prefix
+ * "beagle" replaced by "beagleB200": same arguments, same meaning, same
+ * return codes (0 = success, negative = BeagleB200ReturnCodes).  The comment
+ * on each declaration cites the beagle.h declaration (libhmsbeagle/beagle.h,
+ * beagle-lib 4.0.1) that it replaces.  Only plain C types cross this boundary:
+ * host pointers owned by the caller and valid for the duration of the call.
+ *
+ * Flag bits, operation layouts and return codes have the numeric values of
+ * beagle.h, so a beagle.h client passes its own values unchanged.
+ *
+ * The library runs on one CUDA device per instance (resourceList[0] picks the
+ * device ordinal; default 0).  It has no CPU fallback: with no usable sm_100
+ * device, beagleB200CreateInstance returns BEAGLE_B200_ERROR_NO_RESOURCE.
+ */
+#ifndef BEAGLE_B200_H
+#define BEAGLE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Return codes: values of BeagleReturnCodes (beagle.h:110-122). */
+enum BeagleB200ReturnCodes {
+    BEAGLE_B200_SUCCESS = 0,
+    BEAGLE_B200_ERROR_GENERAL = -1,
+    BEAGLE_B200_ERROR_OUT_OF_MEMORY = -2,
+    BEAGLE_B200_ERROR_UNIDENTIFIED_EXCEPTION = -3,
+    BEAGLE_B200_ERROR_UNINITIALIZED_INSTANCE = -4,
+    BEAGLE_B200_ERROR_OUT_OF_RANGE = -5,
+    BEAGLE_B200_ERROR_NO_RESOURCE = -6,
+    BEAGLE_B200_ERROR_NO_IMPLEMENTATION = -7,
+    BEAGLE_B200_ERROR_FLOATING_POINT = -8
+};
+
+/* Capability flags: bit values of BeagleFlags (beagle.h:132-177). */
+#define BEAGLE_B200_FLAG_PRECISION_SINGLE        (1L << 0)
+#define BEAGLE_B200_FLAG_PRECISION_DOUBLE        (1L << 1)
+#define BEAGLE_B200_FLAG_COMPUTATION_SYNCH       (1L << 2)
+#define BEAGLE_B200_FLAG_COMPUTATION_ASYNCH      (1L << 3)
+#define BEAGLE_B200_FLAG_EIGEN_REAL              (1L << 4)
+#define BEAGLE_B200_FLAG_EIGEN_COMPLEX           (1L << 5)
+#define BEAGLE_B200_FLAG_SCALING_MANUAL          (1L << 6)
+#define BEAGLE_B200_FLAG_SCALING_AUTO            (1L << 7)
+#define BEAGLE_B200_FLAG_SCALING_ALWAYS          (1L << 8)
+#define BEAGLE_B200_FLAG_SCALERS_RAW             (1L << 9)
+#define BEAGLE_B200_FLAG_SCALERS_LOG             (1L << 10)
+#define BEAGLE_B200_FLAG_VECTOR_NONE             (1L << 12)
+#define BEAGLE_B200_FLAG_THREADING_NONE          (1L << 14)
+#define BEAGLE_B200_FLAG_PROCESSOR_GPU           (1L << 16)
+#define BEAGLE_B200_FLAG_INVEVEC_STANDARD        (1L << 20)
+#define BEAGLE_B200_FLAG_INVEVEC_TRANSPOSED      (1L << 21)
+#define BEAGLE_B200_FLAG_FRAMEWORK_CUDA          (1L << 22)
+#define BEAGLE_B200_FLAG_SCALING_DYNAMIC         (1L << 25)
+#define BEAGLE_B200_FLAG_PARALLELOPS_STREAMS     (1L << 28)
+#define BEAGLE_B200_FLAG_PARALLELOPS_GRID        (1L << 29)
+#define BEAGLE_B200_FLAG_PREORDER_TRANSPOSE_MANUAL (1L << 30)
+#define BEAGLE_B200_FLAG_PREORDER_TRANSPOSE_AUTO   (1L << 31)
+
+/* Operation sizes and the "no buffer" index (BeagleOpCodes, beagle.h:201-205). */
+#define BEAGLE_B200_OP_COUNT            7
+#define BEAGLE_B200_PARTITION_OP_COUNT  9
+#define BEAGLE_B200_OP_NONE             (-1)
+
+/* Layout of BeagleOperation (beagle.h:870-878): seven ints per operation. */
+typedef struct {
+    int destinationPartials;
+    int destinationScaleWrite;
+    int destinationScaleRead;
+    int child1Partials;
+    int child1TransitionMatrix;
+    int child2Partials;
+    int child2TransitionMatrix;
+} BeagleB200Operation;
+
+/* Layout of BeagleOperationByPartition (beagle.h:922-932). */
+typedef struct {
+    int destinationPartials;
+    int destinationScaleWrite;
+    int destinationScaleRead;
+    int child1Partials;
+    int child1TransitionMatrix;
+    int child2Partials;
+    int child2TransitionMatrix;
+    int partition;
+    int cumulativeScaleIndex;
+} BeagleB200OperationByPartition;
+
+/* Layout of BeagleInstanceDetails (beagle.h:210-219). */
+typedef struct {
+    int resourceNumber;
+    char* resourceName;
+    char* implName;
+    char* implDescription;
+    long flags;
+} BeagleB200InstanceDetails;
+
+/* Layouts of BeagleResource / BeagleResourceList (beagle.h:224-237). */
+typedef struct {
+    char* name;
+    char* description;
+    long supportFlags;
+    long requiredFlags;
+} BeagleB200Resource;
+
+typedef struct {
+    BeagleB200Resource* list;
+    int length;
+} BeagleB200ResourceList;
+
+/* ---- library / instance lifetime ------------------------------------- */
+/* replaces beagleGetVersion (beagle.h:280) */
+const char* beagleB200GetVersion(void);
+/* replaces beagleGetResourceList (beagle.h:300): one resource per CUDA device */
+BeagleB200ResourceList* beagleB200GetResourceList(void);
+/* replaces beagleCreateInstance (beagle.h:378-391); resourceList[0], when
+ * given, is the CUDA device ordinal.  Returns the instance index (>= 0). */
+int beagleB200CreateInstance(int tipCount, int partialsBufferCount, int compactBufferCount,
+                             int stateCount, int patternCount, int eigenBufferCount,
+                             int matrixBufferCount, int categoryCount, int scaleBufferCount,
+                             int* resourceList, int resourceCount, long preferenceFlags,
+                             long requirementFlags, BeagleB200InstanceDetails* returnInfo);
+/* replaces beagleFinalizeInstance (beagle.h:402) */
+int beagleB200FinalizeInstance(int instance);
+/* replaces beagleFinalize (beagle.h:412) */
+int beagleB200Finalize(void);
+/* replaces beagleSetCPUThreadCount (beagle.h:429-430); a GPU resource: returns
+ * BEAGLE_B200_ERROR_NO_IMPLEMENTATION like the reference GPU implementation */
+int beagleB200SetCPUThreadCount(int instance, int threadCount);
+
+/* ---- data in / out ----------------------------------------------------- */
+/* replaces beagleSetTipStates (beagle.h:446-448): patternCount states, >= stateCount = missing */
+int beagleB200SetTipStates(int instance, int tipIndex, const int* inStates);
+/* replaces beagleSetTipPartials (beagle.h:464-466): [pattern][state], copied to every category */
+int beagleB200SetTipPartials(int instance, int tipIndex, const double* inPartials);
+/* replaces beagleSetRootPrePartials (beagle.h:481-484): pre-order root = state frequencies */
+int beagleB200SetRootPrePartials(int instance, const int* bufferIndices,
+                                 const int* stateFrequenciesIndices, int count);
+/* replaces beagleSetPartials (beagle.h:498-500): [category][pattern][state] */
+int beagleB200SetPartials(int instance, int bufferIndex, const double* inPartials);
+/* replaces beagleGetPartials (beagle.h:515-518) */
+int beagleB200GetPartials(int instance, int bufferIndex, int scaleIndex, double* outPartials);
+/* replaces beagleSetEigenDecomposition (beagle.h:534-538) */
+int beagleB200SetEigenDecomposition(int instance, int eigenIndex, const double* inEigenVectors,
+                                    const double* inInverseEigenVectors,
+                                    const double* inEigenValues);
+/* replaces beagleSetStateFrequencies (beagle.h:551-553) */
+int beagleB200SetStateFrequencies(int instance, int stateFrequenciesIndex,
+                                  const double* inStateFrequencies);
+/* replaces beagleSetCategoryWeights (beagle.h:566-568) */
+int beagleB200SetCategoryWeights(int instance, int categoryWeightsIndex,
+                                 const double* inCategoryWeights);
+/* replaces beagleSetCategoryRates (beagle.h:580-581) */
+int beagleB200SetCategoryRates(int instance, const double* inCategoryRates);
+/* replaces beagleSetCategoryRatesWithIndex (beagle.h:594-596) */
+int beagleB200SetCategoryRatesWithIndex(int instance, int categoryRatesIndex,
+                                        const double* inCategoryRates);
+/* replaces beagleSetPatternWeights (beagle.h:608-609) */
+int beagleB200SetPatternWeights(int instance, const double* inPatternWeights);
+/* replaces beagleSetPatternPartitions (beagle.h:623-625) */
+int beagleB200SetPatternPartitions(int instance, int partitionCount,
+                                   const int* inPatternPartitions);
+
+/* ---- transition matrices ----------------------------------------------- */
+/* replaces beagleConvolveTransitionMatrices (beagle.h:661-665) */
+int beagleB200ConvolveTransitionMatrices(int instance, const int* firstIndices,
+                                         const int* secondIndices, const int* resultIndices,
+                                         int matrixCount);
+/* replaces beagleAddTransitionMatrices (beagle.h:681-685) */
+int beagleB200AddTransitionMatrices(int instance, const int* firstIndices,
+                                    const int* secondIndices, const int* resultIndices,
+                                    int matrixCount);
+/* replaces beagleTransposeTransitionMatrices (beagle.h:699-702) */
+int beagleB200TransposeTransitionMatrices(int instance, const int* inputIndices,
+                                          const int* resultIndices, int matrixCount);
+/* replaces beagleUpdateTransitionMatrices (beagle.h:723-729): P(t) formed in FP64 */
+int beagleB200UpdateTransitionMatrices(int instance, int eigenIndex,
+                                       const int* probabilityIndices,
+                                       const int* firstDerivativeIndices,
+                                       const int* secondDerivativeIndices,
+                                       const double* edgeLengths, int count);
+/* replaces beagleUpdateTransitionMatricesWithModelCategories (beagle.h:753-759) */
+int beagleB200UpdateTransitionMatricesWithModelCategories(int instance, int* eigenIndices,
+                                                          const int* probabilityIndices,
+                                                          const int* firstDerivativeIndices,
+                                                          const int* secondDerivativeIndices,
+                                                          const double* edgeLengths, int count);
+/* replaces beagleUpdateTransitionMatricesWithMultipleModels (beagle.h:782-789) */
+int beagleB200UpdateTransitionMatricesWithMultipleModels(int instance, const int* eigenIndices,
+                                                         const int* categoryRateIndices,
+                                                         const int* probabilityIndices,
+                                                         const int* firstDerivativeIndices,
+                                                         const int* secondDerivativeIndices,
+                                                         const double* edgeLengths, int count);
+/* replaces beagleSetTransitionMatrix (beagle.h:806-809) */
+int beagleB200SetTransitionMatrix(int instance, int matrixIndex, const double* inMatrix,
+                                  double paddedValue);
+/* replaces beagleSetDifferentialMatrix (beagle.h:823-825) */
+int beagleB200SetDifferentialMatrix(int instance, int matrixIndex, const double* inMatrix);
+/* replaces beagleGetTransitionMatrix (beagle.h:840-842) */
+int beagleB200GetTransitionMatrix(int instance, int matrixIndex, double* outMatrix);
+/* replaces beagleSetTransitionMatrices (beagle.h:860-864) */
+int beagleB200SetTransitionMatrices(int instance, const int* matrixIndices,
+                                    const double* inMatrices, const double* paddedValues,
+                                    int count);
+
+/* ---- partials ------------------------------------------------------------ */
+/* replaces beagleUpdatePartials (beagle.h:894-897): the whole operation list
+ * runs as one op-walking kernel launch per call */
+int beagleB200UpdatePartials(const int instance, const BeagleB200Operation* operations,
+                             int operationCount, int cumulativeScaleIndex);
+/* replaces beagleUpdatePrePartials (beagle.h:914-917) */
+int beagleB200UpdatePrePartials(const int instance, const BeagleB200Operation* operations,
+                                int operationCount, int cumulativeScaleIndex);
+/* replaces beagleUpdatePartialsByPartition (beagle.h:947-949) */
+int beagleB200UpdatePartialsByPartition(const int instance,
+                                        const BeagleB200OperationByPartition* operations,
+                                        int operationCount);
+/* replaces beagleUpdatePrePartialsByPartition (beagle.h:964-966) */
+int beagleB200UpdatePrePartialsByPartition(const int instance,
+                                           const BeagleB200OperationByPartition* operations,
+                                           int operationCount);
+/* replaces beagleWaitForPartials (beagle.h:984-986) */
+int beagleB200WaitForPartials(const int instance, const int* destinationPartials,
+                              int destinationPartialsCount);
+
+/* ---- scale factors -------------------------------------------------------- */
+/* replaces beagleAccumulateScaleFactors (beagle.h:999-1002) */
+int beagleB200AccumulateScaleFactors(int instance, const int* scaleIndices, int count,
+                                     int cumulativeScaleIndex);
+/* replaces beagleAccumulateScaleFactorsByPartition (beagle.h:1016-1020) */
+int beagleB200AccumulateScaleFactorsByPartition(int instance, const int* scaleIndices, int count,
+                                                int cumulativeScaleIndex, int partitionIndex);
+/* replaces beagleRemoveScaleFactors (beagle.h:1033-1036) */
+int beagleB200RemoveScaleFactors(int instance, const int* scaleIndices, int count,
+                                 int cumulativeScaleIndex);
+/* replaces beagleRemoveScaleFactorsByPartition (beagle.h:1052-1056) */
+int beagleB200RemoveScaleFactorsByPartition(int instance, const int* scaleIndices, int count,
+                                            int cumulativeScaleIndex, int partitionIndex);
+/* replaces beagleResetScaleFactors (beagle.h:1067-1068) */
+int beagleB200ResetScaleFactors(int instance, int cumulativeScaleIndex);
+/* replaces beagleResetScaleFactorsByPartition (beagle.h:1080-1082) */
+int beagleB200ResetScaleFactorsByPartition(int instance, int cumulativeScaleIndex,
+                                           int partitionIndex);
+/* replaces beagleCopyScaleFactors (beagle.h:1094-1096) */
+int beagleB200CopyScaleFactors(int instance, int destScalingIndex, int srcScalingIndex);
+/* replaces beagleGetScaleFactors (beagle.h:1107-1109) */
+int beagleB200GetScaleFactors(int instance, int srcScalingIndex, double* outScaleFactors);
+
+/* ---- likelihoods and derivatives ------------------------------------------ */
+/* replaces beagleCalculateRootLogLikelihoods (beagle.h:1133-1139): FP64 site
+ * sums and FP64 weighted reduction on the device */
+int beagleB200CalculateRootLogLikelihoods(int instance, const int* bufferIndices,
+                                          const int* categoryWeightsIndices,
+                                          const int* stateFrequenciesIndices,
+                                          const int* cumulativeScaleIndices, int count,
+                                          double* outSumLogLikelihood);
+/* replaces beagleCalculateRootLogLikelihoodsByPartition (beagle.h:1167-1176) */
+int beagleB200CalculateRootLogLikelihoodsByPartition(int instance, const int* bufferIndices,
+                                                     const int* categoryWeightsIndices,
+                                                     const int* stateFrequenciesIndices,
+                                                     const int* cumulativeScaleIndices,
+                                                     const int* partitionIndices,
+                                                     int partitionCount, int count,
+                                                     double* outSumLogLikelihoodByPartition,
+                                                     double* outSumLogLikelihood);
+/* replaces beagleCalculateEdgeDerivatives (beagle.h:1218-1226): d lnL / d t for
+ * every listed branch in one launch; per-site values, weighted sums and sums of squares */
+int beagleB200CalculateEdgeDerivatives(int instance, const int* postBufferIndices,
+                                       const int* preBufferIndices,
+                                       const int* derivativeMatrixIndices,
+                                       const int* categoryWeightsIndices, int count,
+                                       double* outDerivatives, double* outSumDerivatives,
+                                       double* outSumSquaredDerivatives);
+/* replaces beagleCalculateCrossProductDerivative (beagle.h:1228-1236) */
+int beagleB200CalculateCrossProductDerivative(int instance, const int* postBufferIndices,
+                                              const int* preBufferIndices,
+                                              const int* categoryRateIndices,
+                                              const int* categoryWeightsIndices,
+                                              const double* edgeLengths, int count,
+                                              double* outSumDerivatives,
+                                              double* outSumSquaredDerivatives);
+/* replaces beagleCalculateEdgeLogLikelihoods (beagle.h:1265-1277) */
+int beagleB200CalculateEdgeLogLikelihoods(int instance, const int* parentBufferIndices,
+                                          const int* childBufferIndices,
+                                          const int* probabilityIndices,
+                                          const int* firstDerivativeIndices,
+                                          const int* secondDerivativeIndices,
+                                          const int* categoryWeightsIndices,
+                                          const int* stateFrequenciesIndices,
+                                          const int* cumulativeScaleIndices, int count,
+                                          double* outSumLogLikelihood,
+                                          double* outSumFirstDerivative,
+                                          double* outSumSecondDerivative);
+/* replaces beagleGetLogLikelihood (beagle.h:1350-1351) */
+int beagleB200GetLogLikelihood(int instance, double* outSumLogLikelihood);
+/* replaces beagleGetDerivatives (beagle.h:1368-1370) */
+int beagleB200GetDerivatives(int instance, double* outSumFirstDerivative,
+                             double* outSumSecondDerivative);
+/* replaces beagleGetSiteLogLikelihoods (beagle.h:1383-1384) */
+int beagleB200GetSiteLogLikelihoods(int instance, double* outLogLikelihoods);
+/* replaces beagleGetSiteDerivatives (beagle.h:1397-1399) */
+int beagleB200GetSiteDerivatives(int instance, double* outFirstDerivatives,
+                                 double* outSecondDerivatives);
+
+/* ---- extensions (no counterpart in beagle.h) ---------------------------- */
+/* The cudaStream_t (as void*) on which the instance queues all its work, for
+ * callers that time it with CUDA events or order their own work against it.
+ * The stream belongs to the instance and lives until it is finalised. */
+int beagleB200GetCudaStream(int instance, void** outStream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BEAGLE_B200_H */

@@ -1,0 +1,170 @@
+"""Parity of the B200 resource against the oracle, through the C ABI.
+
+Every test runs the same seeded inputs through libbeagle_b200.so (on the GPU)
+and through the float64 numpy oracle (``oracle/oracle.py``, itself pinned to
+the compiled reference by test_oracle.py), and compares with the tolerance
+written in tests/helpers.py: FP64 path relative lnL <= 1e-10, mixed FP32 path
+relative lnL <= 1e-6 and gradient error <= 1e-4.
+"""
+import numpy as np
+import pytest
+
+from helpers import TOL, grad_err, rel, run_b200, run_oracle, gpu_flags
+
+pytestmark = pytest.mark.gpu
+
+SMALL = [
+    ("gtr4_n16_p1000", {}),
+    ("gtr4_n128_p100k", dict(N=32, P=3000)),
+    ("aa20_n64_p20k", dict(N=16, P=1000)),
+    ("codon61_n32_p10k", dict(N=8, P=600)),
+]
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+@pytest.mark.parametrize("name,over", SMALL, ids=[c[0] for c in SMALL])
+def test_lnl_and_gradient_small(b200, syn, oracle, name, over, precision):
+    pr = syn.config_problem(name, **over)
+    inst, lnl, g = run_b200(b200, pr, precision)
+    oi, lnl_o, g_o = run_oracle(oracle, pr)
+    tol = TOL[precision]
+    assert rel(lnl, lnl_o) <= tol["lnl"], (lnl, lnl_o)
+    assert grad_err(g, g_o) <= tol["grad"], grad_err(g, g_o)
+    site = inst.getSiteLogLikelihoods()
+    site_o = oi.getSiteLogLikelihoods()
+    assert np.max(np.abs(site - site_o) / np.abs(site_o)) <= 100 * tol["lnl"]
+    inst.finalize()
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_auto_transpose_matches_manual(b200, syn, oracle, precision):
+    pr = syn.config_problem("aa20_n64_p20k", N=12, P=700)
+    _, l1, g1 = run_b200(b200, pr, precision, auto_transpose=True)
+    _, l2, g2 = run_b200(b200, pr, precision, auto_transpose=False)
+    _, lo, go = run_oracle(oracle, pr)
+    tol = TOL[precision]
+    assert rel(l1, lo) <= tol["lnl"] and rel(l2, lo) <= tol["lnl"]
+    assert grad_err(g1, go) <= tol["grad"] and grad_err(g2, go) <= tol["grad"]
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+@pytest.mark.parametrize("S", [4, 5, 20, 61])
+def test_partials_matrices_and_scalers(b200, syn, oracle, precision, S):
+    """Intermediate buffers: P(t), post-order partials, scale factors,
+    pre-order partials and per-site derivatives against the oracle."""
+    pr = syn.make_problem(S=S, N=10, P=333, C=3, seed=77 + S, rescale=True)
+    inst, _, _ = run_b200(b200, pr, precision)
+    oi, _, _ = run_oracle(oracle, pr)
+    tight = precision == "double"
+    # transition matrices
+    for m in [0, 3, pr.B]:
+        a, b = inst.getTransitionMatrix(m), oi.getTransitionMatrix(m)
+        assert np.max(np.abs(a - b)) <= (1e-13 if tight else 1e-6)
+    # post-order root partials and scale buffers
+    a, b = inst.getPartials(pr.root), oi.getPartials(pr.root)
+    assert np.max(np.abs(a - b)) <= (1e-12 if tight else 1e-5) * np.max(np.abs(b))
+    for s in range(pr.N - 1):
+        a, b = inst.getScaleFactors(s), oi.getScaleFactors(s)
+        assert np.max(np.abs(a - b)) <= (1e-10 if tight else 1e-4)
+    # pre-order partials of a few nodes (both sides rescale per pattern)
+    for v in [0, pr.N, pr.B - 1]:
+        a, b = inst.getPartials(pr.pre(v)), oi.getPartials(pr.pre(v))
+        assert np.max(np.abs(a - b)) <= (1e-11 if tight else 1e-4) * np.max(np.abs(b))
+    # per-site derivatives and sums of squares
+    nonroot = np.arange(pr.B, dtype=np.int32)
+    dm = np.full(pr.B, pr.B, dtype=np.int32)
+    d, s1, s2 = inst.calculateEdgeDerivatives(nonroot, nonroot + pr.pre(0), dm, [0])
+    do, s1o, s2o = oi.calculateEdgeDerivatives(nonroot, nonroot + pr.pre(0), dm, [0])
+    scale = np.max(np.abs(do))
+    assert np.max(np.abs(d - do)) <= (1e-9 if tight else 1e-4) * scale
+    assert grad_err(s1, s1o) <= (1e-9 if tight else 1e-4)
+    assert grad_err(s2, s2o) <= (1e-9 if tight else 1e-4)
+    inst.finalize()
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_raw_scalers_and_cumulative_in_update(b200, syn, oracle, precision):
+    """RAW scalers, with the cumulative buffer filled by updatePartials itself."""
+    pr = syn.make_problem(S=4, N=24, P=513, C=4, seed=5, rescale=True)
+    pref, req = gpu_flags(precision, log_scalers=False)
+    inst = b200.create(*pr.create_args(), preferenceFlags=pref, requirementFlags=req)
+    oi = oracle.OracleInstance(*pr.create_args(), flags=0)
+    out = []
+    for x in (inst, oi):
+        pr.load(x)
+        x.updateTransitionMatrices(0, np.arange(pr.B), None, None, pr.lengths)
+        x.resetScaleFactors(pr.cumulative)
+        x.updatePartials(pr.post_ops(), pr.cumulative)
+        out.append(x.calculateRootLogLikelihoods([pr.root], [0], [0], [pr.cumulative]))
+        out.append(x.getScaleFactors(3))
+    assert rel(out[0], out[2]) <= TOL[precision]["lnl"]
+    assert np.max(np.abs(out[1] - out[3]) / out[3]) <= (1e-12 if precision == "double" else 1e-6)
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_edge_loglikelihood_and_derivatives(b200, syn, oracle, precision):
+    pr = syn.make_problem(S=4, N=12, P=400, C=4, seed=9)
+    pref, req = gpu_flags(precision)
+    inst = b200.create(*pr.create_args(), preferenceFlags=pref, requirementFlags=req)
+    oi = oracle.OracleInstance(*pr.create_args(), flags=1 << 10)
+    res = []
+    # edge between node v's pre-order partials and its post-order partials
+    v = pr.N + 1
+    for x in (inst, oi):
+        pr.load(x)
+        idx = np.arange(pr.B)
+        x.updateTransitionMatrices(0, idx, idx + pr.B + 1, None, pr.lengths)
+        # matrix indices B+1.. hold dP/dt here
+        x.updatePartials(pr.post_ops())
+        x.calculateRootLogLikelihoods([pr.root], [0], [0], [-1])
+        pr.set_root_pre(x)
+        x.updatePrePartials(pr.pre_ops(False))
+        res.append(x.calculateEdgeLogLikelihoods(pr.pre(int(pr.parent[v])), v, v,
+                                                 v + pr.B + 1, None, 0, 0, -1))
+    (c0, l0, d0, _), (c1, l1, d1, _) = res
+    tol = TOL[precision]
+    assert rel(l0, l1) <= tol["lnl"]
+    assert abs(d0 - d1) <= tol["grad"] * max(1.0, abs(d1))
+
+
+def test_missing_states_and_ragged_patterns(b200, syn, oracle):
+    """States >= S are missing (all-ones); pattern counts off the 128 tile."""
+    for P in (1, 127, 129, 1000):
+        pr = syn.make_problem(S=4, N=9, P=P, C=2, seed=P)
+        rng = np.random.default_rng(P)
+        pr.tip_states[rng.random(pr.tip_states.shape) < 0.1] = 4 + rng.integers(0, 3)
+        _, l, _ = run_b200(b200, pr, "double", gradient=False)
+        _, lo, _ = run_oracle(oracle, pr, gradient=False)
+        assert rel(l, lo) <= 1e-10
+
+
+def test_error_codes(b200, syn):
+    pr = syn.make_problem(S=4, N=6, P=50, C=2, seed=1)
+    pref, req = gpu_flags("double")
+    inst = b200.create(*pr.create_args(), preferenceFlags=pref, requirementFlags=req)
+    pr.load(inst)
+    bad = np.array([[pr.root, -1, -1, 9999, 0, 1, 1]], dtype=np.int32)
+    assert inst.updatePartials(bad, check=False) == -5
+    assert inst.transposeTransitionMatrices([0], [0], check=False) == -5
+    code, _ = inst.calculateRootLogLikelihoods([pr.n_buffers + 5], [0], [0], [-1], check=False)
+    assert code == -5
+    # NaN partials -> BEAGLE_ERROR_FLOATING_POINT, value still written
+    nanp = np.full(pr.C * pr.P * pr.S, np.nan)
+    inst.setPartials(pr.root, nanp)
+    code, v = inst.calculateRootLogLikelihoods([pr.root], [0], [0], [-1], check=False)
+    assert code == -8 and np.isnan(v)
+    inst.finalize()
+    assert b200.fn["SetPatternWeights"](inst.h if inst.h is not None else 12345, None) == -4
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("precision", ["double", "single"])
+@pytest.mark.parametrize("name", ["gtr4_n128_p100k", "aa20_n64_p20k", "codon61_n32_p10k"])
+def test_full_size_configs(b200, syn, oracle, name, precision):
+    pr = syn.config_problem(name)
+    inst, lnl, g = run_b200(b200, pr, precision)
+    inst.finalize()
+    _, lo, go = run_oracle(oracle, pr)
+    tol = TOL[precision]
+    assert rel(lnl, lo) <= tol["lnl"], (lnl, lo, rel(lnl, lo))
+    assert grad_err(g, go) <= tol["grad"], grad_err(g, go)

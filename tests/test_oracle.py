@@ -1,0 +1,91 @@
+"""The oracle itself, on the CPU: the numpy restatement against the golden
+fixtures produced by the compiled reference (tests/golden/make_golden.py),
+and, where oracle/_ref is built, against the reference library live."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from helpers import DOUBLE, PROCESSOR_CPU, SCALERS_LOG, SCALERS_RAW, grad_err, rel
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "golden.npz")
+
+
+def _golden():
+    g = np.load(GOLDEN)
+    return g, json.loads(str(g["meta"]))
+
+
+def _cases():
+    _, meta = _golden()
+    return sorted(meta)
+
+
+@pytest.mark.parametrize("case", _cases())
+def test_oracle_matches_golden(syn, oracle, case):
+    g, meta = _golden()
+    m = meta[case]
+    pr = syn.make_problem(name=case, **m["kw"])
+    flags = SCALERS_LOG if m["scalers"] == "log" else SCALERS_RAW
+    inst = oracle.OracleInstance(*pr.create_args(), flags=flags)
+    pr.load(inst)
+    lnl, grad = pr.evaluate(inst)
+    assert rel(lnl, g[case + "/lnl"][0]) <= 1e-13
+    assert grad_err(grad, g[case + "/grad"]) <= 1e-10
+    site = inst.getSiteLogLikelihoods()
+    assert np.max(np.abs(site - g[case + "/site_lnl"])) <= 1e-9
+    nonroot = np.arange(pr.B, dtype=np.int32)
+    d, _, sq = inst.calculateEdgeDerivatives(nonroot, nonroot + pr.pre(0),
+                                             np.full(pr.B, pr.B, dtype=np.int32), [0])
+    assert np.max(np.abs(d[0] - g[case + "/site_d_branch0"])) <= 1e-9 * max(
+        1.0, np.max(np.abs(d[0])))
+    assert grad_err(sq, g[case + "/sumsq"]) <= 1e-10
+
+
+def test_golden_is_from_reference():
+    _, meta = _golden()
+    assert all(m["impl"].startswith("CPU-") for m in meta.values())
+
+
+@pytest.mark.parametrize("S,N,P,C,rescale", [(4, 12, 257, 4, True), (4, 7, 31, 1, False),
+                                             (13, 9, 100, 2, True), (64, 5, 40, 4, True)])
+def test_oracle_matches_compiled_reference(reflib, syn, oracle, S, N, P, C, rescale):
+    pr = syn.make_problem(S=S, N=N, P=P, C=C, seed=S * 100 + N, rescale=rescale)
+    ri = reflib.create(*pr.create_args(), preferenceFlags=DOUBLE | PROCESSOR_CPU | SCALERS_LOG,
+                       requirementFlags=DOUBLE)
+    pr.load(ri)
+    lr, gr = pr.evaluate(ri)
+    oi = oracle.OracleInstance(*pr.create_args(), flags=SCALERS_LOG)
+    pr.load(oi)
+    lo, go = pr.evaluate(oi)
+    assert rel(lo, lr) <= 1e-12
+    assert grad_err(go, gr) <= 1e-9
+    # intermediate buffers
+    assert np.max(np.abs(ri.getTransitionMatrix(1) - oi.getTransitionMatrix(1))) <= 1e-13
+    a, b = ri.getPartials(pr.root), oi.getPartials(pr.root)
+    assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(a))
+    ri.finalize()
+
+
+def test_oracle_fixed_scaling_and_transpose(reflib, syn, oracle):
+    """Read-only (fixed) scale factors and matrix transposition/convolution."""
+    pr = syn.make_problem(S=4, N=10, P=90, C=2, seed=3, rescale=True)
+    ri = reflib.create(*pr.create_args(), preferenceFlags=DOUBLE | PROCESSOR_CPU | SCALERS_RAW,
+                       requirementFlags=DOUBLE)
+    oi = oracle.OracleInstance(*pr.create_args(), flags=SCALERS_RAW)
+    res = []
+    for x in (ri, oi):
+        pr.load(x)
+        x.updateTransitionMatrices(0, np.arange(pr.B), None, None, pr.lengths)
+        x.updatePartials(pr.post_ops())
+        ops = pr.post_ops()
+        ops[:, 2] = ops[:, 1]      # read the factors just written ...
+        ops[:, 1] = -1             # ... without writing new ones
+        x.updatePartials(ops)
+        x.transposeTransitionMatrices([0, 1], [pr.B + 1, pr.B + 2])
+        x.convolveTransitionMatrices([0], [1], [pr.B + 3])
+        res.append((x.getPartials(pr.root), x.getTransitionMatrix(pr.B + 1),
+                    x.getTransitionMatrix(pr.B + 3)))
+    for a, b in zip(*res):
+        assert np.max(np.abs(a - b)) <= 1e-12 * max(1.0, np.max(np.abs(b)))
