@@ -716,7 +716,7 @@ int Instance::calculateEdgeDerivatives(const int* post, const int* pre, const in
         d.dpad = mat_pad_[dmat[k]];
         d.reserved = 0;
     }
-    const int nblk = reduction_blocks(P_);
+    const int nblk = deriv_blocks(dims());
     CK(t_deriv_.upload(tab.data(), sizeof(DerivDesc) * count, stream_));
     CK(scratch_.reserve(sizeof(double) * 2 * (size_t)count * nblk));
     CK(out_.reserve(sizeof(double) * 2 * count));

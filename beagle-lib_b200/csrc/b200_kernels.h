@@ -52,7 +52,7 @@ cudaError_t launch_edge_lnl(const void* parent, const void* child, int child_is_
 
 // Edge derivatives for `nb` branches; per-site values optional (d_site may be
 // null), sums and sums of squares into d_sums[2*nb].  d_block holds
-// nb * 2 * ceil(Pp / 128) doubles of per-block partial sums.
+// 2 * nb * deriv_blocks(d) doubles of per-block partial sums.
 template <typename Real>
 cudaError_t launch_edge_derivatives(const DerivDesc* d_desc, int nb, const double* catw,
                                     const double* patw, const Dims& d, double* d_site,
@@ -69,5 +69,7 @@ cudaError_t launch_fill_root(void* dest, const double* freqs, const Dims& d, cud
 
 // Number of per-block partial sums used by the reductions above.
 int reduction_blocks(int Pp);
+// ... and by one branch of an edge-derivative launch.
+int deriv_blocks(const Dims& d);
 
 }  // namespace b200

@@ -18,45 +18,19 @@
 //   fixed scaling: dest *= 1/scale_read[p].
 //
 // Two kernel families:
-//  * S = 4: one thread per pattern carrying all C categories in registers;
-//    partials rows are 16-byte (FP32) / 32-byte (FP64) vectors, so a warp
-//    moves 32 contiguous pattern rows per load.  HBM-bound.
+//  * S = 4: one thread per (pattern, category), vector loads and stores of
+//    one 4-state row, lane-group shuffles for the rescaling maximum.
+//    HBM-bound.
 //  * generic S (<= 64): a CTA of 8 warps owns 32 patterns; lane = pattern,
 //    warp = a contiguous slice of SPAD/8 states.  Per category the two
 //    matrices and the two child tiles are staged in shared memory; matrix
 //    reads are warp-uniform (broadcast), tile reads are conflict-free.
 #include "b200_kernels.h"
+#include "b200_vec.cuh"
 
 namespace b200 {
 
 namespace {
-
-// ---------------------------------------------------------------- helpers
-__device__ __forceinline__ void ld4(const float* p, float v[4]) {
-    const float4 t = *reinterpret_cast<const float4*>(p);
-    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
-}
-__device__ __forceinline__ void ld4(const double* p, double v[4]) {
-    const double2 a = reinterpret_cast<const double2*>(p)[0];
-    const double2 b = reinterpret_cast<const double2*>(p)[1];
-    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-}
-__device__ __forceinline__ void ldg4(const float* p, float v[4]) {
-    const float4 t = __ldg(reinterpret_cast<const float4*>(p));
-    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
-}
-__device__ __forceinline__ void ldg4(const double* p, double v[4]) {
-    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
-    const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
-    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-}
-__device__ __forceinline__ void st4(float* p, const float v[4]) {
-    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
-}
-__device__ __forceinline__ void st4(double* p, const double v[4]) {
-    reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
-    reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
-}
 
 // Rescale one pattern's C*S values in place (see the file comment).
 template <typename Real>
@@ -68,7 +42,174 @@ __device__ __forceinline__ void store_scale(Real m, double* scale_write, double*
 }
 
 // ------------------------------------------------------------ S = 4 kernels
-// y[c][i] = (M . x)[c][i] for one operand (partials or tip states).
+// One thread per (pattern, category): a category's four states are one
+// 16-byte (FP32) / 32-byte (FP64) vector, so consecutive threads read and
+// write consecutive vectors of the [pattern][category][state] layout.  The C
+// threads of a pattern form an aligned lane group; the rescaling maximum over
+// categories is a shuffle reduction inside that group.  Each thread carries
+// PPT patterns (PPT chosen at launch so the grid is a single resident wave),
+// and the op descriptors are staged in shared memory chunk by chunk so the
+// per-op loads (children, matrices) all issue together.
+constexpr int kOpChunk = 64;
+constexpr int kT4 = 256;        // threads per CTA of the S = 4 kernels
+
+__device__ __forceinline__ void stage_ops(OpDesc* s_ops, const OpDesc* __restrict__ ops, int n) {
+    const int* src = reinterpret_cast<const int*>(ops);
+    int* dst = reinterpret_cast<int*>(s_ops);
+    const int words = n * (int)(sizeof(OpDesc) / sizeof(int));
+    for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+}
+
+// y[i] = (M_c . x)[i] for one operand of one category: partials vector x, or
+// column s of M_c (pad value for the missing state).
+template <typename Real>
+__device__ __forceinline__ void operand4c(const Real* __restrict__ Mc, bool states, int s,
+                                          const Real x[4], Real pad, Real y[4]) {
+    if (states) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) y[i] = (s < 4) ? __ldg(Mc + i * 4 + (s & 3)) : pad;
+    } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            Real m[4];
+            ldg4(Mc + i * 4, m);
+            y[i] = m[0] * x[0] + m[1] * x[1] + m[2] * x[2] + m[3] * x[3];
+        }
+    }
+}
+
+template <int C, typename Real>
+__device__ __forceinline__ Real group_max(Real v) {
+#pragma unroll
+    for (int o = 1; o < C; o <<= 1) {
+        const Real u = __shfl_xor_sync(0xffffffffu, v, o);
+        v = u > v ? u : v;
+    }
+    return v;
+}
+
+// Rescale / fixed-scale and store one pattern-category vector.
+template <typename Real, int C>
+__device__ __forceinline__ void finish4c(const OpDesc& op, Real out[4], int p, bool valid, int c,
+                                         double* cum, int log_scalers) {
+    if (op.scale_write) {
+        Real m = out[0];
+#pragma unroll
+        for (int i = 1; i < 4; ++i) m = out[i] > m ? out[i] : m;
+        m = group_max<C>(m);
+        if (m == Real(0)) m = Real(1);
+        const Real inv = Real(1) / m;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) out[i] *= inv;
+        if (valid && c == 0) store_scale(m, op.scale_write, cum, p, log_scalers);
+    } else if (op.scale_read) {
+        const Real inv = Real(1) / (Real)op.scale_read[p];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) out[i] *= inv;
+    }
+    if (valid) st4(static_cast<Real*>(op.dest) + ((size_t)p * C + c) * 4, out);
+}
+
+template <typename Real, int C, int PPT>
+__global__ void __launch_bounds__(kT4)
+k_post4(const OpDesc* __restrict__ ops, int nops, int Pp, double* cum, int log_scalers) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    OpDesc* s_ops = reinterpret_cast<OpDesc*>(smem_raw);
+    const int c = threadIdx.x % C;
+    const int ppb = kT4 / C;                                 // patterns per CTA per slot
+    const int pstride = gridDim.x * ppb;
+    const int p0 = blockIdx.x * ppb + threadIdx.x / C;
+    for (int o0 = 0; o0 < nops; o0 += kOpChunk) {
+        const int n = min(kOpChunk, nops - o0);
+        __syncthreads();
+        stage_ops(s_ops, ops + o0, n);
+        __syncthreads();
+        for (int oi = 0; oi < n; ++oi) {
+            const OpDesc& op = s_ops[oi];
+            const bool st1 = op.kind & kX1States, st2 = op.kind & kX2States;
+            const Real* M1 = static_cast<const Real*>(op.m1) + c * 16;
+            const Real* M2 = static_cast<const Real*>(op.m2) + c * 16;
+            Real x1[PPT][4], x2[PPT][4];
+            int s1[PPT], s2[PPT];
+#pragma unroll
+            for (int k = 0; k < PPT; ++k) {
+                const int p = min(p0 + k * pstride, Pp - 1);
+                if (st1) s1[k] = static_cast<const int*>(op.x1)[p];
+                else ld4(static_cast<const Real*>(op.x1) + ((size_t)p * C + c) * 4, x1[k]);
+                if (st2) s2[k] = static_cast<const int*>(op.x2)[p];
+                else ld4(static_cast<const Real*>(op.x2) + ((size_t)p * C + c) * 4, x2[k]);
+            }
+#pragma unroll
+            for (int k = 0; k < PPT; ++k) {
+                const int p = p0 + k * pstride;
+                Real y1[4], y2[4];
+                operand4c(M1, st1, s1[k], x1[k], (Real)op.pad1, y1);
+                operand4c(M2, st2, s2[k], x2[k], (Real)op.pad2, y2);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) y1[i] *= y2[i];
+                finish4c<Real, C>(op, y1, min(p, Pp - 1), p < Pp, c, cum, log_scalers);
+            }
+        }
+    }
+}
+
+template <typename Real, int C, int PPT>
+__global__ void __launch_bounds__(kT4)
+k_pre4(const OpDesc* __restrict__ ops, int nops, int Pp, int log_scalers) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    OpDesc* s_ops = reinterpret_cast<OpDesc*>(smem_raw);
+    const int c = threadIdx.x % C;
+    const int ppb = kT4 / C;
+    const int pstride = gridDim.x * ppb;
+    const int p0 = blockIdx.x * ppb + threadIdx.x / C;
+    for (int o0 = 0; o0 < nops; o0 += kOpChunk) {
+        const int n = min(kOpChunk, nops - o0);
+        __syncthreads();
+        stage_ops(s_ops, ops + o0, n);
+        __syncthreads();
+        for (int oi = 0; oi < n; ++oi) {
+            const OpDesc& op = s_ops[oi];
+            const bool st2 = op.kind & kX2States;
+            const bool tr = op.kind & kM1Transposed;
+            const Real* M1 = static_cast<const Real*>(op.m1) + c * 16;
+            const Real* M2 = static_cast<const Real*>(op.m2) + c * 16;
+            Real pv[PPT][4], x2[PPT][4];
+            int s2[PPT];
+#pragma unroll
+            for (int k = 0; k < PPT; ++k) {
+                const int p = min(p0 + k * pstride, Pp - 1);
+                ld4(static_cast<const Real*>(op.x1) + ((size_t)p * C + c) * 4, pv[k]);
+                if (st2) s2[k] = static_cast<const int*>(op.x2)[p];
+                else ld4(static_cast<const Real*>(op.x2) + ((size_t)p * C + c) * 4, x2[k]);
+            }
+#pragma unroll
+            for (int k = 0; k < PPT; ++k) {
+                const int p = p0 + k * pstride;
+                Real z[4];
+                operand4c(M2, st2, s2[k], x2[k], (Real)op.pad2, z);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) z[i] *= pv[k][i];
+                Real out[4] = {0, 0, 0, 0};
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    Real m[4];
+                    if (tr) {
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) m[j] = __ldg(M1 + j * 4 + i);
+                    } else {
+                        ldg4(M1 + i * 4, m);
+                    }
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) out[j] += m[j] * z[i];
+                }
+                finish4c<Real, C>(op, out, min(p, Pp - 1), p < Pp, c, nullptr, log_scalers);
+            }
+        }
+    }
+}
+
+// Thread-per-pattern S = 4 kernels for category counts that are not a power
+// of two (the lane-group layout above needs C | 32).
 template <typename Real, int C>
 __device__ __forceinline__ void operand4(const void* x, bool states, const Real* __restrict__ M,
                                          Real pad, int p, Real y[C][4]) {
@@ -126,7 +267,7 @@ __device__ __forceinline__ void finish4(const OpDesc& op, Real out[C][4], int p,
 
 template <typename Real, int C>
 __global__ void __launch_bounds__(128)
-k_post4(const OpDesc* __restrict__ ops, int nops, int Pp, double* cum, int log_scalers) {
+k_post4p(const OpDesc* __restrict__ ops, int nops, int Pp, double* cum, int log_scalers) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= Pp) return;
     for (int o = 0; o < nops; ++o) {
@@ -146,7 +287,7 @@ k_post4(const OpDesc* __restrict__ ops, int nops, int Pp, double* cum, int log_s
 
 template <typename Real, int C>
 __global__ void __launch_bounds__(128)
-k_pre4(const OpDesc* __restrict__ ops, int nops, int Pp, int log_scalers) {
+k_pre4p(const OpDesc* __restrict__ ops, int nops, int Pp, int log_scalers) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= Pp) return;
     for (int o = 0; o < nops; ++o) {
@@ -388,16 +529,74 @@ cudaError_t run_prex(const OpDesc* ops, int nops, const Dims& d, int ls, cudaStr
     return cudaGetLastError();
 }
 
+// Patterns per thread for the lane-group kernels: the smallest PPT whose grid
+// fits in one resident wave (occupancy from the CUDA runtime for that very
+// instantiation), else the largest.
+template <typename K>
+long wave_patterns(K kernel, int C, int ppt) {
+    int dev = 0, sms = 0, blocks = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, kT4,
+                                                  kOpChunk * sizeof(OpDesc));
+    return (long)sms * blocks * (kT4 / C) * ppt;
+}
+
+template <typename Real, int C>
+int pick_ppt_post(int Pp) {
+    static const long w1 = wave_patterns(k_post4<Real, C, 1>, C, 1);
+    static const long w2 = wave_patterns(k_post4<Real, C, 2>, C, 2);
+    return Pp <= w1 ? 1 : Pp <= w2 ? 2 : 4;
+}
+
+template <typename Real, int C>
+int pick_ppt_pre(int Pp) {
+    static const long w1 = wave_patterns(k_pre4<Real, C, 1>, C, 1);
+    static const long w2 = wave_patterns(k_pre4<Real, C, 2>, C, 2);
+    return Pp <= w1 ? 1 : Pp <= w2 ? 2 : 4;
+}
+
+template <typename Real, int C, int PPT>
+cudaError_t run_post4_ppt(const OpDesc* ops, int nops, const Dims& d, double* cum, int ls,
+                          cudaStream_t s) {
+    const int ppb = kT4 / C * PPT;
+    const int grid = (d.Pp + ppb - 1) / ppb;
+    k_post4<Real, C, PPT><<<grid, kT4, kOpChunk * sizeof(OpDesc), s>>>(ops, nops, d.Pp, cum, ls);
+    return cudaGetLastError();
+}
+
+template <typename Real, int C, int PPT>
+cudaError_t run_pre4_ppt(const OpDesc* ops, int nops, const Dims& d, int ls, cudaStream_t s) {
+    const int ppb = kT4 / C * PPT;
+    const int grid = (d.Pp + ppb - 1) / ppb;
+    k_pre4<Real, C, PPT><<<grid, kT4, kOpChunk * sizeof(OpDesc), s>>>(ops, nops, d.Pp, ls);
+    return cudaGetLastError();
+}
+
 template <typename Real, int C>
 cudaError_t run_post4(const OpDesc* ops, int nops, const Dims& d, double* cum, int ls,
                       cudaStream_t s) {
-    k_post4<Real, C><<<(d.Pp + 127) / 128, 128, 0, s>>>(ops, nops, d.Pp, cum, ls);
+    if (32 % C == 0) {
+        switch (pick_ppt_post<Real, (32 % C == 0 ? C : 1)>(d.Pp)) {
+            case 1: return run_post4_ppt<Real, (32 % C == 0 ? C : 1), 1>(ops, nops, d, cum, ls, s);
+            case 2: return run_post4_ppt<Real, (32 % C == 0 ? C : 1), 2>(ops, nops, d, cum, ls, s);
+            default: return run_post4_ppt<Real, (32 % C == 0 ? C : 1), 4>(ops, nops, d, cum, ls, s);
+        }
+    }
+    k_post4p<Real, C><<<(d.Pp + 127) / 128, 128, 0, s>>>(ops, nops, d.Pp, cum, ls);
     return cudaGetLastError();
 }
 
 template <typename Real, int C>
 cudaError_t run_pre4(const OpDesc* ops, int nops, const Dims& d, int ls, cudaStream_t s) {
-    k_pre4<Real, C><<<(d.Pp + 127) / 128, 128, 0, s>>>(ops, nops, d.Pp, ls);
+    if (32 % C == 0) {
+        switch (pick_ppt_pre<Real, (32 % C == 0 ? C : 1)>(d.Pp)) {
+            case 1: return run_pre4_ppt<Real, (32 % C == 0 ? C : 1), 1>(ops, nops, d, ls, s);
+            case 2: return run_pre4_ppt<Real, (32 % C == 0 ? C : 1), 2>(ops, nops, d, ls, s);
+            default: return run_pre4_ppt<Real, (32 % C == 0 ? C : 1), 4>(ops, nops, d, ls, s);
+        }
+    }
+    k_pre4p<Real, C><<<(d.Pp + 127) / 128, 128, 0, s>>>(ops, nops, d.Pp, ls);
     return cudaGetLastError();
 }
 

@@ -1,9 +1,10 @@
 // Pattern reductions: root and edge log-likelihoods, edge derivatives and
 // scale-factor accumulation.  All sums that leave the device are FP64 and
 // deterministic: fixed 128-thread blocks reduce by warp shuffles and shared
-// memory into per-block partial sums, and a second single-block pass adds the
-// partials in block order.
+// memory into per-block partial sums, and a second pass (one CTA per output)
+// adds the partials in a fixed order.
 #include "b200_kernels.h"
+#include "b200_vec.cuh"
 
 namespace b200 {
 
@@ -30,19 +31,16 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
     return t;
 }
 
-// out[k] = sum over nblk partials in[k * nblk + b], b in order.
+// out[k] = sum over the nblk partials in[k * nblk + b]; one CTA per output,
+// each thread adding a fixed strided subset, then a fixed-order block sum.
 __global__ void k_final_sum(const double* __restrict__ in, int nblk, int nout, double* out) {
     __shared__ double sh[kRB / 32];
-    for (int k = 0; k < nout; ++k) {
-        double v = 0;
-        // Each thread adds a contiguous run of block partials, then the block sum.
-        const int per = (nblk + kRB - 1) / kRB;
-        const int b0 = threadIdx.x * per;
-        for (int b = b0; b < b0 + per && b < nblk; ++b) v += in[(size_t)k * nblk + b];
-        const double t = block_sum(v, sh);
-        if (threadIdx.x == 0) out[k] = t;
-        __syncthreads();
-    }
+    const int k = blockIdx.x;
+    double v = 0;
+    for (int b = threadIdx.x; b < nblk; b += kRB) v += in[(size_t)k * nblk + b];
+    const double t = block_sum(v, sh);
+    if (threadIdx.x == 0) out[k] = t;
+    (void)nout;
 }
 
 // Site value of sum_c w_c sum_i pi_i x[p][c][i] for a partials buffer; the
@@ -217,63 +215,60 @@ k_edge_deriv(const DerivDesc* __restrict__ desc, const double* __restrict__ catw
     if (threadIdx.x == 0) block[(size_t)(gridDim.y + b) * nblk + blockIdx.x] = t;
 }
 
-// S = 4 specialisation of k_edge_deriv: one 16-byte / 32-byte row per category.
+// S = 4 specialisation of k_edge_deriv: one thread per (pattern, category)
+// with 16-byte (FP32) / 32-byte (FP64) vector loads; the C threads of a
+// pattern combine their weighted terms with shuffles.  kRB / C patterns per
+// CTA, blockIdx.y = branch.
 template <typename Real, int C>
 __global__ void __launch_bounds__(kRB)
 k_edge_deriv4(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
               const double* __restrict__ patw, int P, double* site, double* block) {
     __shared__ double sh[kRB / 32];
     const int b = blockIdx.y;
-    const DerivDesc dd = desc[b];
-    const int p = blockIdx.x * kRB + threadIdx.x;
-    double d = 0;
-    if (p < P) {
-        const Real* pre = static_cast<const Real*>(dd.pre) + (size_t)p * C * 4;
-        const Real* D = static_cast<const Real*>(dd.dmat);
-        double num = 0, den = 0;
-        if (dd.post_is_states) {
-            const int s = static_cast<const int*>(dd.post)[p];
+    const int c = threadIdx.x % C;
+    const int p = blockIdx.x * (kRB / C) + threadIdx.x / C;
+    const DerivDesc& dd = desc[b];
+    const int pc = min(p, P - 1);
+    const Real* D = static_cast<const Real*>(dd.dmat) + c * 16;
+    const Real* pre = static_cast<const Real*>(dd.pre) + ((size_t)pc * C + c) * 4;
+    Real z[4], x[4];
+    ld4(pre, z);
+    Real n = 0, q = 0;
+    if (dd.post_is_states) {
+        const int s = static_cast<const int*>(dd.post)[pc];
 #pragma unroll
-            for (int c = 0; c < C; ++c) {
-                const Real* pc = pre + c * 4;
-                Real n = 0, q = 0;
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const Real dk = (s < 4) ? __ldg(D + c * 16 + k * 4 + s) : (Real)dd.dpad;
-                    n += pc[k] * dk;
-                    q += (s >= 4 || k == s) ? pc[k] : Real(0);
-                }
-                num += catw[c] * (double)n;
-                den += catw[c] * (double)q;
-            }
-        } else {
-            const Real* post = static_cast<const Real*>(dd.post) + (size_t)p * C * 4;
-#pragma unroll
-            for (int c = 0; c < C; ++c) {
-                Real x[4], z[4];
-#pragma unroll
-                for (int k = 0; k < 4; ++k) { x[k] = post[c * 4 + k]; z[k] = pre[c * 4 + k]; }
-                Real n = 0, q = 0;
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const Real* row = D + c * 16 + k * 4;
-                    const Real y = __ldg(row) * x[0] + __ldg(row + 1) * x[1] +
-                                   __ldg(row + 2) * x[2] + __ldg(row + 3) * x[3];
-                    n += z[k] * y;
-                    q += z[k] * x[k];
-                }
-                num += catw[c] * (double)n;
-                den += catw[c] * (double)q;
-            }
+        for (int k = 0; k < 4; ++k) {
+            const Real dk = (s < 4) ? __ldg(D + k * 4 + (s & 3)) : (Real)dd.dpad;
+            n += z[k] * dk;
+            q += (s >= 4 || k == s) ? z[k] : Real(0);
         }
+    } else {
+        ld4(static_cast<const Real*>(dd.post) + ((size_t)pc * C + c) * 4, x);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const Real y = __ldg(D + k * 4) * x[0] + __ldg(D + k * 4 + 1) * x[1] +
+                           __ldg(D + k * 4 + 2) * x[2] + __ldg(D + k * 4 + 3) * x[3];
+            n += z[k] * y;
+            q += z[k] * x[k];
+        }
+    }
+    const double w = catw[c];
+    double num = w * (double)n, den = w * (double)q;
+#pragma unroll
+    for (int o = 1; o < C; o <<= 1) {
+        num += __shfl_xor_sync(0xffffffffu, num, o);
+        den += __shfl_xor_sync(0xffffffffu, den, o);
+    }
+    double d = 0;
+    if (c == 0 && p < P) {
         d = num / den;
         if (site) site[(size_t)b * P + p] = d;
     }
-    const double w = (p < P) ? patw[p] : 0.0;
+    const double wp = (c == 0 && p < P) ? patw[p] : 0.0;
     const int nblk = gridDim.x;
-    double t = block_sum(d * w, sh);
+    double t = block_sum(d * wp, sh);
     if (threadIdx.x == 0) block[(size_t)b * nblk + blockIdx.x] = t;
-    t = block_sum(d * d * w, sh);
+    t = block_sum(d * d * wp, sh);
     if (threadIdx.x == 0) block[(size_t)(gridDim.y + b) * nblk + blockIdx.x] = t;
 }
 
@@ -317,7 +312,7 @@ cudaError_t launch_edge_lnl(const void* parent, const void* child, int child_is_
         static_cast<const Real*>(parent), child, child_is_states, static_cast<const Real*>(pmat),
         ppad, static_cast<const Real*>(d1mat), d1pad, static_cast<const Real*>(d2mat), d2pad,
         catw, freqs, cum, patw, d.S, d.Sg, d.C, d.P, d_site, d_site1, d_site2, d_block);
-    k_final_sum<<<1, kRB, 0, s>>>(d_block, nblk, 3, d_out);
+    k_final_sum<<<3, kRB, 0, s>>>(d_block, nblk, 3, d_out);
     return cudaGetLastError();
 }
 
@@ -326,24 +321,30 @@ cudaError_t launch_edge_derivatives(const DerivDesc* desc, int nb, const double*
                                     const double* patw, const Dims& d, double* d_site,
                                     double* d_block, double* d_sums, cudaStream_t s) {
     if (nb == 0) return cudaSuccess;
-    const int nblk = reduction_blocks(d.P);
-    dim3 grid(nblk, nb);
-    if (d.S == 4 && d.Sg == 4) {
+    int nblk = reduction_blocks(d.P);
+    if (d.S == 4 && d.Sg == 4 && (d.C == 1 || d.C == 2 || d.C == 4 || d.C == 8)) {
+        nblk = (d.P + kRB / d.C - 1) / (kRB / d.C);
+        dim3 grid(nblk, nb);
         switch (d.C) {
             case 1: k_edge_deriv4<Real, 1><<<grid, kRB, 0, s>>>(desc, catw, patw, d.P, d_site, d_block); break;
             case 2: k_edge_deriv4<Real, 2><<<grid, kRB, 0, s>>>(desc, catw, patw, d.P, d_site, d_block); break;
             case 4: k_edge_deriv4<Real, 4><<<grid, kRB, 0, s>>>(desc, catw, patw, d.P, d_site, d_block); break;
-            case 8: k_edge_deriv4<Real, 8><<<grid, kRB, 0, s>>>(desc, catw, patw, d.P, d_site, d_block); break;
-            default:
-                k_edge_deriv<Real><<<grid, kRB, 0, s>>>(desc, catw, patw, d.S, d.Sg, d.C, d.P, d_site,
-                                                        d_block);
+            default: k_edge_deriv4<Real, 8><<<grid, kRB, 0, s>>>(desc, catw, patw, d.P, d_site, d_block); break;
         }
     } else {
+        dim3 grid(nblk, nb);
         k_edge_deriv<Real><<<grid, kRB, 0, s>>>(desc, catw, patw, d.S, d.Sg, d.C, d.P, d_site,
                                                 d_block);
     }
-    k_final_sum<<<1, kRB, 0, s>>>(d_block, nblk, 2 * nb, d_sums);
+    k_final_sum<<<2 * nb, kRB, 0, s>>>(d_block, nblk, 2 * nb, d_sums);
     return cudaGetLastError();
+}
+
+// Per-block partial sums an edge-derivative launch needs (per branch, twice).
+int deriv_blocks(const Dims& d) {
+    if (d.S == 4 && d.Sg == 4 && (d.C == 1 || d.C == 2 || d.C == 4 || d.C == 8))
+        return (d.P + kRB / d.C - 1) / (kRB / d.C);
+    return reduction_blocks(d.P);
 }
 
 cudaError_t launch_accumulate_scale(double* cum, const double* pool, const int* d_idx, int n,

