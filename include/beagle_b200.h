@@ -312,6 +312,40 @@ int beagleB200GetSiteDerivatives(int instance, double* outFirstDerivatives,
  * The stream belongs to the instance and lives until it is finalised. */
 int beagleB200GetCudaStream(int instance, void** outStream);
 
+/* No counterpart in the reference.  The pattern-weighted root log-likelihood
+ * of caller-owned device buffers, for callers that cannot let a library call
+ * cudaMalloc: frameworks that own all device memory through their own
+ * allocator, or loops where cudaMalloc's implicit device synchronisation is not
+ * acceptable.  The call allocates nothing.  Its only scratch, the per-block
+ * partial sums of the FP64 reduction, is a fixed 64 KiB device array built into
+ * the library (held on every GPU that loads it until the process exits), so
+ * patternCount is limited to 8192 * 128 = 1,048,576; larger counts return
+ * BEAGLE_B200_ERROR_OUT_OF_RANGE.
+ *
+ * All pointers except `stream` are device pointers on `device`:
+ *   rootPartials            [patternCount][categoryCount][Sg], Sg = stateCount
+ *                           rounded up to a multiple of 4 (this library's
+ *                           partials layout); float if doublePrecision == 0,
+ *                           else double
+ *   categoryWeights         [categoryCount]     stateFrequencies  [stateCount]
+ *   cumulativeScaleFactors  [patternCount] log scale factors, or NULL
+ *   patternWeights          [patternCount]
+ *   outSiteLogLikelihoods   [patternCount]      outSumLogLikelihood  [1]
+ * The work is queued on `stream` (a cudaStream_t; NULL = the default stream)
+ * and the call returns without waiting.  The first call on a device looks up
+ * the scratch array's device address; make that first call before any stream
+ * capture.  Every call shares the array, so calls that overlap on the GPU race:
+ * order them on one stream.  Calls from different host threads that target the
+ * same device must not overlap either. */
+int beagleB200RootLogLikelihoodsNoAlloc(int device, void* stream, const void* rootPartials,
+                                        int doublePrecision, int stateCount, int patternCount,
+                                        int categoryCount, const double* categoryWeights,
+                                        const double* stateFrequencies,
+                                        const double* cumulativeScaleFactors,
+                                        const double* patternWeights,
+                                        double* outSiteLogLikelihoods,
+                                        double* outSumLogLikelihood);
+
 #ifdef __cplusplus
 }
 #endif
