@@ -78,12 +78,12 @@ Instance::~Instance() {
     cudaSetDevice(device_);
     if (stream_) cudaStreamSynchronize(stream_);
     for (void* p : owned_) cudaFree(p);
-    void* bufs[] = {d_part_pool_, d_mat_, d_scale_, d_cube_, d_evals_, d_rates_, d_catw_,
-                    d_freqs_, d_patw_, d_site_, d_site1_, d_site2_};
+    void* bufs[] = {d_part_pool_, d_mat_, d_mat_t_, d_scale_, d_cube_, d_evals_, d_rates_,
+                    d_catw_, d_freqs_, d_patw_, d_site_, d_site1_, d_site2_};
     for (void* p : bufs)
         if (p) cudaFree(p);
     for (DevBuf* b : {&t_ops_post_, &t_ops_pre_, &t_jobs_, &t_deriv_, &t_idx_, &t_ptr_,
-                      &scratch_, &out_, &site_d_})
+                      &scratch_, &out_, &site_d_, &t_dep_post_, &t_dep_pre_})
         b->release();
     if (h_out_) cudaFreeHost(h_out_);
     for (auto& c : chunks_) cudaFreeHost(c.first);
@@ -106,7 +106,9 @@ int Instance::create(int tipCount, int partialsBufferCount, int compactBufferCou
                              (1L << 13) /*OpenMP*/;
     if (req & unsupported) return kErrNoImpl;
     if ((req & F_SINGLE) && (req & F_DOUBLE)) return kErrNoImpl;
-    if (stateCount > 64) return kErrNoImpl;
+    // State counts up to 64 and up to 8 rate categories (one CTA per category
+    // in a thread-block cluster for S != 4).
+    if (stateCount > 64 || categoryCount > 8) return kErrNoImpl;
     // Precision: a single-precision requirement or preference selects the mixed
     // path (FP32 partials, FP64 matrices formation and reductions).
     dbl_ = !((req & F_SINGLE) || (!(req & F_DOUBLE) && (pref & F_SINGLE)));
@@ -157,6 +159,8 @@ int Instance::create(int tipCount, int partialsBufferCount, int compactBufferCou
     if (nmat_ > 0) {
         CK(cudaMalloc(&d_mat_, mat_bytes_ * nmat_));
         CK(cudaMemsetAsync(d_mat_, 0, mat_bytes_ * nmat_, stream_));
+        CK(cudaMalloc(&d_mat_t_, mat_bytes_ * nmat_));
+        CK(cudaMemsetAsync(d_mat_t_, 0, mat_bytes_ * nmat_, stream_));
     }
     mat_pad_.assign(nmat_, 1.0);
     if (nscale_ > 0) {
@@ -410,17 +414,24 @@ int Instance::setPatternPartitions(int n, const int* parts) {
 
 // ---------------------------------------------------------------- matrices
 int Instance::upload_matrix(int m, const double* in, double pad) {
+    // Natural image [C][Sg][Sg] and its transpose, zero padded.
     const size_t n = (size_t)C_ * Sg_ * Sg_;
-    std::vector<double> hd(n, 0.0);
+    std::vector<double> hd(2 * n, 0.0);
     for (int c = 0; c < C_; ++c)
         for (int i = 0; i < S_; ++i)
-            for (int j = 0; j < S_; ++j)
-                hd[((size_t)c * Sg_ + i) * Sg_ + j] = in[((size_t)c * S_ + i) * S_ + j];
+            for (int j = 0; j < S_; ++j) {
+                const double v = in[((size_t)c * S_ + i) * S_ + j];
+                hd[((size_t)c * Sg_ + i) * Sg_ + j] = v;
+                hd[n + ((size_t)c * Sg_ + j) * Sg_ + i] = v;
+            }
     if (dbl_) {
         CK(cudaMemcpyAsync(mat(m), hd.data(), n * 8, cudaMemcpyHostToDevice, stream_));
+        CK(cudaMemcpyAsync(mat_t(m), hd.data() + n, n * 8, cudaMemcpyHostToDevice, stream_));
     } else {
         std::vector<float> hf(hd.begin(), hd.end());
         CK(cudaMemcpyAsync(mat(m), hf.data(), n * 4, cudaMemcpyHostToDevice, stream_));
+        CK(cudaMemcpyAsync(mat_t(m), hf.data() + n, n * 4, cudaMemcpyHostToDevice, stream_));
+        mat_pad_[m] = pad;
         return sync();   // hf goes out of scope
     }
     mat_pad_[m] = pad;
@@ -462,27 +473,27 @@ int Instance::getTransitionMatrix(int m, double* out) {
 
 int Instance::transposeTransitionMatrices(const int* in, const int* out, int count) {
     if (count <= 0) return kSuccess;
-    std::vector<const void*> a(count);
-    std::vector<void*> o(count);
+    // pointer table: inputs, results, results' transposed images
+    std::vector<const void*> tab(3 * count);
     for (int k = 0; k < count; ++k) {
         if (in[k] < 0 || in[k] >= nmat_ || out[k] < 0 || out[k] >= nmat_) return kErrRange;
         if (in[k] == out[k]) return kErrRange;   // in-place not allowed (CPU :1190-1200)
-        a[k] = mat(in[k]);
-        o[k] = mat(out[k]);
+        tab[k] = mat(in[k]);
+        tab[count + k] = mat(out[k]);
+        tab[2 * count + k] = mat_t(out[k]);
     }
-    std::vector<const void*> tab(2 * count);
-    for (int k = 0; k < count; ++k) { tab[k] = a[k]; tab[count + k] = o[k]; }
     CK(t_ptr_.upload(tab.data(), sizeof(void*) * tab.size(), stream_));
-    const void* const* da = (const void* const*)t_ptr_.ptr;
-    void* const* dout = (void* const*)((const void**)t_ptr_.ptr + count);
-    CK(LAUNCH(launch_matrix_pairs, da, nullptr, dout, count, 1, dims(), stream_));
+    const void* const* base = (const void* const*)t_ptr_.ptr;
+    CK(LAUNCH(launch_matrix_pairs, base, nullptr, (void* const*)(base + count), count, 1, dims(),
+              stream_));
     return kSuccess;
 }
 
 int Instance::convolveTransitionMatrices(const int* first, const int* second,
                                          const int* result, int count) {
     if (count <= 0) return kSuccess;
-    std::vector<const void*> tab(3 * count);
+    // pointer table: first, second, results, results' transposed images
+    std::vector<const void*> tab(4 * count);
     for (int k = 0; k < count; ++k) {
         for (int v : {first[k], second[k], result[k]})
             if (v < 0 || v >= nmat_) return kErrRange;
@@ -490,6 +501,7 @@ int Instance::convolveTransitionMatrices(const int* first, const int* second,
         tab[k] = mat(first[k]);
         tab[count + k] = mat(second[k]);
         tab[2 * count + k] = mat(result[k]);
+        tab[3 * count + k] = mat_t(result[k]);
         mat_pad_[result[k]] = 1.0;
     }
     CK(t_ptr_.upload(tab.data(), sizeof(void*) * tab.size(), stream_));
@@ -524,6 +536,9 @@ int Instance::updateTransitionMatricesWithMultipleModels(const int* eig, const i
         j.p = mat(prob[u]);
         j.d1 = d1 ? mat(d1[u]) : nullptr;
         j.d2 = (d1 && d2) ? mat(d2[u]) : nullptr;
+        j.pt = mat_t(prob[u]);
+        j.d1t = d1 ? mat_t(d1[u]) : nullptr;
+        j.d2t = (d1 && d2) ? mat_t(d2[u]) : nullptr;
         j.cube = d_cube_ + (size_t)e * S_ * S_ * S_;
         j.evals = d_evals_ + (size_t)e * S_;
         j.rates = d_rates_ + (size_t)r * C_;
@@ -552,6 +567,7 @@ int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative,
     if (count < 0 || (count > 0 && !ops)) return kErrRange;
     if (cumulative != -1 && (cumulative < 0 || cumulative >= nscale_)) return kErrRange;
     std::vector<OpDesc> tab(count);
+    std::vector<uint8_t> dep(count, 0);
     // Buffers written earlier in this list count as holding data.
     std::vector<char> written(nbuf_, 0);
     for (int k = 0; k < count; ++k) {
@@ -575,6 +591,10 @@ int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative,
         d.dest = partials_[dest];
         d.m1 = mat(m1);
         d.m2 = mat(m2);
+        d.m1t = mat_t(m1);
+        d.m2t = mat_t(m2);
+        if (k > 0 && (c1 == ops[(size_t)(k - 1) * stride] || c2 == ops[(size_t)(k - 1) * stride]))
+            dep[k] = 1;
         d.pad1 = mat_pad_[m1];
         d.pad2 = mat_pad_[m2];
         d.scale_write = ws >= 0 ? scale(ws) : nullptr;
@@ -591,7 +611,12 @@ int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative,
     DevBuf& t = pre ? t_ops_pre_ : t_ops_post_;
     CK(t.upload(tab.data(), sizeof(OpDesc) * tab.size(), stream_));
     double* cum = (cumulative >= 0 && !pre) ? scale(cumulative) : nullptr;
-    if (pre) {
+    if (S_ != 4) {
+        DevBuf& td = pre ? t_dep_pre_ : t_dep_post_;
+        CK(td.upload(dep.data(), dep.size(), stream_));
+        CK(LAUNCH(launch_opwalk_generic, (const OpDesc*)t.ptr, (const uint8_t*)td.ptr, count, pre,
+                  dims(), cum, (int)log_scalers_, stream_));
+    } else if (pre) {
         CK(LAUNCH(launch_update_pre_partials, (const OpDesc*)t.ptr, count, dims(),
                   (int)log_scalers_, stream_));
     } else {
@@ -713,18 +738,26 @@ int Instance::calculateEdgeDerivatives(const int* post, const int* pre, const in
         d.post_is_states = states_[post[k]] ? 1 : 0;
         d.pre = partials_[pre[k]];
         d.dmat = mat(dmat[k]);
+        d.dmatt = mat_t(dmat[k]);
         d.dpad = mat_pad_[dmat[k]];
         d.reserved = 0;
     }
-    const int nblk = deriv_blocks(dims());
+    const int nblk = S_ == 4 ? deriv_blocks(dims()) : Pp_ / generic_tile_patterns(Sg_, dbl_);
     CK(t_deriv_.upload(tab.data(), sizeof(DerivDesc) * count, stream_));
     CK(scratch_.reserve(sizeof(double) * 2 * (size_t)count * nblk));
     CK(out_.reserve(sizeof(double) * 2 * count));
     if (outDerivs) CK(site_d_.reserve(sizeof(double) * (size_t)count * P_));
-    CK(LAUNCH(launch_edge_derivatives, (const DerivDesc*)t_deriv_.ptr, count,
-              d_catw_ + (size_t)w * C_, d_patw_, dims(),
-              outDerivs ? (double*)site_d_.ptr : nullptr, (double*)scratch_.ptr,
-              (double*)out_.ptr, stream_));
+    if (S_ == 4) {
+        CK(LAUNCH(launch_edge_derivatives, (const DerivDesc*)t_deriv_.ptr, count,
+                  d_catw_ + (size_t)w * C_, d_patw_, dims(),
+                  outDerivs ? (double*)site_d_.ptr : nullptr, (double*)scratch_.ptr,
+                  (double*)out_.ptr, stream_));
+    } else {
+        CK(LAUNCH(launch_deriv_generic, (const DerivDesc*)t_deriv_.ptr, count,
+                  d_catw_ + (size_t)w * C_, d_patw_, dims(),
+                  outDerivs ? (double*)site_d_.ptr : nullptr, (double*)scratch_.ptr, stream_));
+        CK(launch_deriv_final((double*)scratch_.ptr, nblk, count, (double*)out_.ptr, stream_));
+    }
     if (async_ && !outDerivs) {
         // ASYNCH: sums are written to the caller's arrays at the next
         // synchronisation point (getters, waitForPartials, synchronous calls).

@@ -100,6 +100,7 @@ private:
     bool buf_ok(int b) const { return b >= 0 && b < nbuf_; }
     bool has_data(int b) const { return buf_ok(b) && (partials_[b] || states_[b]); }
     void* mat(int m) const { return (char*)d_mat_ + (size_t)m * mat_bytes_; }
+    void* mat_t(int m) const { return (char*)d_mat_t_ + (size_t)m * mat_bytes_; }
     double* scale(int i) const { return d_scale_ + (size_t)i * Pp_; }
     int ensure_partials(int b);
     int upload_matrix(int m, const double* in, double pad);
@@ -123,6 +124,7 @@ private:
     std::vector<int*> states_;             // per buffer: device tip states or null
     std::vector<void*> owned_;             // lazily allocated tip buffers
     void* d_mat_ = nullptr;
+    void* d_mat_t_ = nullptr;              // transposed images of the matrices
     std::vector<double> mat_pad_;
     double* d_scale_ = nullptr;
     double* d_cube_ = nullptr;             // [eig][S][S][S]
@@ -140,6 +142,7 @@ private:
     std::vector<int> partition_start_;     // pattern partitions (empty = one partition)
 
     DevBuf t_ops_post_, t_ops_pre_, t_jobs_, t_deriv_, t_idx_, t_ptr_, scratch_, out_, site_d_;
+    DevBuf t_dep_post_, t_dep_pre_;        // per op: reads the previous op's output
     double* h_out_ = nullptr;              // pinned result staging (SYNCH calls)
     size_t h_out_n_ = 0;
     // ASYNCH mode: results copied into pinned chunks and delivered at the next

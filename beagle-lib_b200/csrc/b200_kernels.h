@@ -34,6 +34,19 @@ template <typename Real>
 cudaError_t launch_update_pre_partials(const OpDesc* d_ops, int nops, const Dims& d,
                                        int log_scalers, cudaStream_t s);
 
+// The same op lists for S != 4 (S <= 64, C <= 8): clustered CUDA-core kernels.
+// dep[o] != 0 when op o reads the output of op o - 1.
+template <typename Real>
+cudaError_t launch_opwalk_generic(const OpDesc* d_ops, const uint8_t* d_dep, int nops, bool pre,
+                                  const Dims& d, double* cumulative, int log_scalers,
+                                  cudaStream_t s);
+template <typename Real>
+cudaError_t launch_deriv_generic(const DerivDesc* d_desc, int nb, const double* catw,
+                                 const double* patw, const Dims& d, double* d_site,
+                                 double* d_block, cudaStream_t s);
+// Pattern tile of the clustered kernels (one derivative partial per tile).
+int generic_tile_patterns(int Sg, bool dbl);
+
 // Root log-likelihood: site lnL into d_site[P]; the weighted total into d_out[0].
 template <typename Real>
 cudaError_t launch_root_lnl(const void* root, const double* catw, const double* freqs,
@@ -69,7 +82,10 @@ cudaError_t launch_fill_root(void* dest, const double* freqs, const Dims& d, cud
 
 // Number of per-block partial sums used by the reductions above.
 int reduction_blocks(int Pp);
-// ... and by one branch of an edge-derivative launch.
+// ... and by one branch of an edge-derivative launch (S = 4 kernels).
 int deriv_blocks(const Dims& d);
+// Final pass of an edge-derivative launch: sums[k] over nblk block partials.
+cudaError_t launch_deriv_final(const double* d_block, int nblk, int nb, double* d_sums,
+                               cudaStream_t s);
 
 }  // namespace b200

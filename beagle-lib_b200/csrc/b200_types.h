@@ -13,6 +13,9 @@ namespace b200 {
 //   scale      [pattern Pp]                          double
 // Sg = S rounded up to a multiple of 4 (one 16-byte row per pattern for S = 4),
 // Pp = P rounded up to a multiple of kPatternPad so pattern tiles need no tail.
+// Every matrix also has a transposed image (same layout, P^T), kept in step by
+// whatever writes the matrix, so kernels stage either orientation by a plain
+// contiguous copy.
 constexpr int kPatternPad = 128;
 
 enum OpKind : int {
@@ -30,6 +33,8 @@ struct OpDesc {
     void* dest;
     const void* m1;
     const void* m2;
+    const void* m1t;            // transposed images of m1 / m2 ([C][Sg][Sg], P^T)
+    const void* m2t;
     double* scale_write;        // rescale into this buffer (nullptr = no rescale)
     const double* scale_read;   // divide by these stored factors (nullptr = none)
     double pad1;                // value of the missing-state column of M1
@@ -43,6 +48,7 @@ struct DerivDesc {
     const void* post;           // post-order partials (or tip states) below the branch
     const void* pre;            // pre-order partials of the same node
     const void* dmat;           // derivative matrix [C][Sg][Sg]
+    const void* dmatt;          // its transposed image
     double dpad;                // its missing-state column value
     int post_is_states;
     int reserved;
@@ -54,6 +60,9 @@ struct MatJob {
     void* p;
     void* d1;
     void* d2;
+    void* pt;                   // transposed images (written alongside)
+    void* d1t;
+    void* d2t;
     const double* cube;         // eigen cube [S][S][S] (i, j, k)
     const double* evals;        // eigenvalues [S]
     const double* rates;        // category rates [C]

@@ -59,11 +59,16 @@ k_update_matrices(const MatJob* __restrict__ jobs, int S, int Sg) {
         P[idx] = (Real)s0;
         if (D1) D1[idx] = (Real)s1;
         if (D2) D2[idx] = (Real)s2;
+        const size_t tix = (size_t)c * Sg * Sg + j * Sg + i;   // transposed image
+        static_cast<Real*>(jb.pt)[tix] = (Real)s0;
+        if (D1) static_cast<Real*>(jb.d1t)[tix] = (Real)s1;
+        if (D2) static_cast<Real*>(jb.d2t)[tix] = (Real)s2;
     }
 }
 
 // op 0: out = a . b (convolution, CPU/BeagleCPUImpl.hpp:1096-1160);
 // op 1: out = transpose(a) (CPU/BeagleCPUImpl.hpp:1175-1222).
+// `out` holds 2n pointers: the n results, then their transposed images.
 template <typename Real>
 __global__ void k_matrix_pairs(const void* const* a, const void* const* b, void* const* out,
                                int op, int S, int Sg) {
@@ -71,6 +76,7 @@ __global__ void k_matrix_pairs(const void* const* a, const void* const* b, void*
     const size_t off = (size_t)c * Sg * Sg;
     const Real* A = static_cast<const Real*>(a[m]) + off;
     Real* O = static_cast<Real*>(out[m]) + off;
+    Real* OT = static_cast<Real*>(out[gridDim.x + m]) + off;
     for (int idx = threadIdx.x; idx < Sg * Sg; idx += blockDim.x) {
         const int i = idx / Sg, j = idx - (idx / Sg) * Sg;
         Real v = 0;
@@ -85,6 +91,7 @@ __global__ void k_matrix_pairs(const void* const* a, const void* const* b, void*
             }
         }
         O[idx] = v;
+        OT[j * Sg + i] = v;
     }
 }
 

@@ -17,14 +17,9 @@
 //          cumulative[p] += log m when a cumulative buffer is given;
 //   fixed scaling: dest *= 1/scale_read[p].
 //
-// Two kernel families:
-//  * S = 4: one thread per (pattern, category), vector loads and stores of
-//    one 4-state row, lane-group shuffles for the rescaling maximum.
-//    HBM-bound.
-//  * generic S (<= 64): a CTA of 8 warps owns 32 patterns; lane = pattern,
-//    warp = a contiguous slice of SPAD/8 states.  Per category the two
-//    matrices and the two child tiles are staged in shared memory; matrix
-//    reads are warp-uniform (broadcast), tile reads are conflict-free.
+// This file holds the S = 4 kernels: one thread per (pattern, category),
+// vector loads and stores of one 4-state row, lane-group shuffles for the
+// rescaling maximum.  HBM-bound.  Other state counts: k_generic.cu.
 #include "b200_kernels.h"
 #include "b200_vec.cuh"
 
@@ -324,211 +319,6 @@ k_pre4p(const OpDesc* __restrict__ ops, int nops, int Pp, int log_scalers) {
     }
 }
 
-// ---------------------------------------------------------- generic kernels
-constexpr int kNW = 8;          // warps per CTA
-constexpr int kTP = 32;         // patterns per CTA (one per lane)
-constexpr int kXS = kTP + 1;    // padded row length of staged tiles
-
-// Stage one category's matrix into MA[k][i] (row k, column i) such that an
-// operand product reads  y_i = sum_k MA[k][i] v_k:
-//   transpose = true  : MA[k][i] = M[i][k]   (y = M . v)
-//   transpose = false : MA[k][i] = M[k][i]   (y = M^T . v)
-template <typename Real, int SPAD>
-__device__ __forceinline__ void stage_matrix(Real* MA, const Real* __restrict__ M, int Sg,
-                                             bool transpose) {
-    for (int idx = threadIdx.x; idx < SPAD * SPAD; idx += blockDim.x) {
-        const int r = idx / SPAD, q = idx - (idx / SPAD) * SPAD;   // r = row of M, q = col
-        Real v = 0;
-        if (r < Sg && q < Sg) v = __ldg(M + r * Sg + q);
-        if (transpose) MA[q * SPAD + r] = v;
-        else MA[r * SPAD + q] = v;
-    }
-}
-
-// Stage one category's tile of 32 patterns: T[j][p] = x[p0 + p][c][j].
-template <typename Real, int SPAD>
-__device__ __forceinline__ void stage_tile(Real* T, const Real* x, int p0, int c, int C, int Sg) {
-    for (int idx = threadIdx.x; idx < kTP * SPAD; idx += blockDim.x) {
-        const int p = idx / SPAD, j = idx - (idx / SPAD) * SPAD;
-        Real v = 0;
-        if (j < Sg) v = x[((size_t)(p0 + p) * C + c) * Sg + j];
-        T[j * kXS + p] = v;
-    }
-}
-
-// acc[r] = sum_k MA[k][i0 + r] * T[k][lane]  (operand from staged partials),
-// or MA[s][i0 + r] / pad for a tip state s.
-template <typename Real, int SPAD>
-__device__ __forceinline__ void product(const Real* MA, const Real* T, bool states, int s,
-                                        Real pad, int S, int i0, int lane,
-                                        Real acc[SPAD / kNW]) {
-    constexpr int RI = SPAD / kNW;
-    if (states) {
-#pragma unroll
-        for (int r = 0; r < RI; ++r) acc[r] = (s < S) ? MA[s * SPAD + i0 + r] : pad;
-        return;
-    }
-#pragma unroll
-    for (int r = 0; r < RI; ++r) acc[r] = 0;
-    for (int k = 0; k < S; ++k) {
-        const Real v = T[k * kXS + lane];
-        const Real* row = MA + k * SPAD + i0;
-#pragma unroll
-        for (int r = 0; r < RI; ++r) acc[r] += row[r] * v;
-    }
-}
-
-// Rescale pass of the generic kernels: every thread re-reads the values it
-// wrote for its pattern and state slice, after the per-pattern maximum over
-// all categories has been combined across warps in shared memory.
-template <typename Real, int SPAD>
-__device__ __forceinline__ void rescale_tile(const OpDesc& op, Real* red, Real mloc, int p0,
-                                             int lane, int warp, int i0, int S, int C, int Sg,
-                                             double* cum, int log_scalers) {
-    constexpr int RI = SPAD / kNW;
-    red[warp * kTP + lane] = mloc;
-    __syncthreads();
-    Real m = 0;
-#pragma unroll
-    for (int w = 0; w < kNW; ++w) m = red[w * kTP + lane] > m ? red[w * kTP + lane] : m;
-    if (m == Real(0)) m = Real(1);
-    const Real inv = Real(1) / m;
-    Real* d = static_cast<Real*>(op.dest) + (size_t)(p0 + lane) * C * Sg;
-    for (int c = 0; c < C; ++c) {
-#pragma unroll
-        for (int r = 0; r < RI; ++r)
-            if (i0 + r < Sg) d[c * Sg + i0 + r] *= inv;
-    }
-    if (warp == 0) store_scale(m, op.scale_write, cum, p0 + lane, log_scalers);
-    (void)S;
-}
-
-template <typename Real, int SPAD>
-__global__ void __launch_bounds__(256)
-k_postx(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double* cum,
-        int log_scalers) {
-    constexpr int RI = SPAD / kNW;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    Real* MA1 = reinterpret_cast<Real*>(smem_raw);
-    Real* MA2 = MA1 + SPAD * SPAD;
-    Real* T1 = MA2 + SPAD * SPAD;
-    Real* T2 = T1 + SPAD * kXS;
-    Real* red = T2 + SPAD * kXS;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int p0 = blockIdx.x * kTP;
-    const int i0 = warp * RI;
-    const int p = p0 + lane;
-    for (int o = 0; o < nops; ++o) {
-        const OpDesc op = ops[o];
-        const bool st1 = op.kind & kX1States, st2 = op.kind & kX2States;
-        const int s1 = st1 ? static_cast<const int*>(op.x1)[p] : 0;
-        const int s2 = st2 ? static_cast<const int*>(op.x2)[p] : 0;
-        const Real inv_read = op.scale_read ? Real(1) / (Real)op.scale_read[p] : Real(1);
-        Real mloc = 0;
-        for (int c = 0; c < C; ++c) {
-            stage_matrix<Real, SPAD>(MA1, static_cast<const Real*>(op.m1) + (size_t)c * Sg * Sg,
-                                     Sg, true);
-            stage_matrix<Real, SPAD>(MA2, static_cast<const Real*>(op.m2) + (size_t)c * Sg * Sg,
-                                     Sg, true);
-            if (!st1) stage_tile<Real, SPAD>(T1, static_cast<const Real*>(op.x1), p0, c, C, Sg);
-            if (!st2) stage_tile<Real, SPAD>(T2, static_cast<const Real*>(op.x2), p0, c, C, Sg);
-            __syncthreads();
-            Real a1[RI], a2[RI];
-            product<Real, SPAD>(MA1, T1, st1, s1, (Real)op.pad1, S, i0, lane, a1);
-            product<Real, SPAD>(MA2, T2, st2, s2, (Real)op.pad2, S, i0, lane, a2);
-            Real* d = static_cast<Real*>(op.dest) + ((size_t)p * C + c) * Sg;
-#pragma unroll
-            for (int r = 0; r < RI; ++r) {
-                Real v = a1[r] * a2[r];
-                if (i0 + r < S) mloc = v > mloc ? v : mloc;
-                if (op.scale_read) v *= inv_read;
-                if (i0 + r < Sg) d[i0 + r] = v;
-            }
-            __syncthreads();
-        }
-        if (op.scale_write)
-            rescale_tile<Real, SPAD>(op, red, mloc, p0, lane, warp, i0, S, C, Sg, cum,
-                                     log_scalers);
-        __syncthreads();
-    }
-}
-
-template <typename Real, int SPAD>
-__global__ void __launch_bounds__(256)
-k_prex(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, int log_scalers) {
-    constexpr int RI = SPAD / kNW;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    Real* MA = reinterpret_cast<Real*>(smem_raw);
-    Real* T = MA + SPAD * SPAD;     // sibling tile
-    Real* Z = T + SPAD * kXS;       // parent pre-partials, then z
-    Real* red = Z + SPAD * kXS;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int p0 = blockIdx.x * kTP;
-    const int i0 = warp * RI;
-    const int p = p0 + lane;
-    for (int o = 0; o < nops; ++o) {
-        const OpDesc op = ops[o];
-        const bool st2 = op.kind & kX2States;
-        const bool tr = op.kind & kM1Transposed;
-        const int s2 = st2 ? static_cast<const int*>(op.x2)[p] : 0;
-        Real mloc = 0;
-        for (int c = 0; c < C; ++c) {
-            stage_matrix<Real, SPAD>(MA, static_cast<const Real*>(op.m2) + (size_t)c * Sg * Sg,
-                                     Sg, true);
-            if (!st2) stage_tile<Real, SPAD>(T, static_cast<const Real*>(op.x2), p0, c, C, Sg);
-            stage_tile<Real, SPAD>(Z, static_cast<const Real*>(op.x1), p0, c, C, Sg);
-            __syncthreads();
-            Real a[RI];
-            product<Real, SPAD>(MA, T, st2, s2, (Real)op.pad2, S, i0, lane, a);
-#pragma unroll
-            for (int r = 0; r < RI; ++r) Z[(i0 + r) * kXS + lane] *= a[r];
-            __syncthreads();
-            // dest_j = sum_i P[i][j] z_i: MA[i][j] = P[i][j], or P^T given -> transpose.
-            stage_matrix<Real, SPAD>(MA, static_cast<const Real*>(op.m1) + (size_t)c * Sg * Sg,
-                                     Sg, tr);
-            __syncthreads();
-            product<Real, SPAD>(MA, Z, false, 0, Real(0), S, i0, lane, a);
-            Real* d = static_cast<Real*>(op.dest) + ((size_t)p * C + c) * Sg;
-#pragma unroll
-            for (int r = 0; r < RI; ++r) {
-                if (i0 + r < S) mloc = a[r] > mloc ? a[r] : mloc;
-                if (i0 + r < Sg) d[i0 + r] = a[r];
-            }
-            __syncthreads();
-        }
-        if (op.scale_write)
-            rescale_tile<Real, SPAD>(op, red, mloc, p0, lane, warp, i0, S, C, Sg, nullptr,
-                                     log_scalers);
-        __syncthreads();
-    }
-}
-
-template <typename Real, int SPAD>
-size_t smem_postx() { return sizeof(Real) * (2 * SPAD * SPAD + 2 * SPAD * kXS + kNW * kTP); }
-template <typename Real, int SPAD>
-size_t smem_prex() { return sizeof(Real) * (SPAD * SPAD + 2 * SPAD * kXS + kNW * kTP); }
-
-template <typename Real, int SPAD>
-cudaError_t run_postx(const OpDesc* ops, int nops, const Dims& d, double* cum, int ls,
-                      cudaStream_t s) {
-    const size_t sm = smem_postx<Real, SPAD>();
-    cudaError_t e = cudaFuncSetAttribute(k_postx<Real, SPAD>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    k_postx<Real, SPAD><<<d.Pp / kTP, kNW * 32, sm, s>>>(ops, nops, d.S, d.Sg, d.C, cum, ls);
-    return cudaGetLastError();
-}
-
-template <typename Real, int SPAD>
-cudaError_t run_prex(const OpDesc* ops, int nops, const Dims& d, int ls, cudaStream_t s) {
-    const size_t sm = smem_prex<Real, SPAD>();
-    cudaError_t e = cudaFuncSetAttribute(k_prex<Real, SPAD>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    k_prex<Real, SPAD><<<d.Pp / kTP, kNW * 32, sm, s>>>(ops, nops, d.S, d.Sg, d.C, ls);
-    return cudaGetLastError();
-}
-
 // Patterns per thread for the lane-group kernels: the smallest PPT whose grid
 // fits in one resident wave (occupancy from the CUDA runtime for that very
 // instantiation), else the largest.
@@ -618,13 +408,7 @@ cudaError_t launch_update_partials(const OpDesc* ops, int nops, const Dims& d, d
             default: return run_post4<Real, 8>(ops, nops, d, cum, ls, s);
         }
     }
-    if (d.Sg <= 8) return run_postx<Real, 8>(ops, nops, d, cum, ls, s);
-    if (d.Sg <= 16) return run_postx<Real, 16>(ops, nops, d, cum, ls, s);
-    if (d.Sg <= 24) return run_postx<Real, 24>(ops, nops, d, cum, ls, s);
-    if (d.Sg <= 32) return run_postx<Real, 32>(ops, nops, d, cum, ls, s);
-    if (d.Sg <= 48) return run_postx<Real, 48>(ops, nops, d, cum, ls, s);
-    if (d.Sg <= 64) return run_postx<Real, 64>(ops, nops, d, cum, ls, s);
-    return cudaErrorInvalidValue;
+    return cudaErrorInvalidValue;   // other state counts: k_generic.cu
 }
 
 template <typename Real>
@@ -643,13 +427,7 @@ cudaError_t launch_update_pre_partials(const OpDesc* ops, int nops, const Dims& 
             default: return run_pre4<Real, 8>(ops, nops, d, ls, s);
         }
     }
-    if (d.Sg <= 8) return run_prex<Real, 8>(ops, nops, d, ls, s);
-    if (d.Sg <= 16) return run_prex<Real, 16>(ops, nops, d, ls, s);
-    if (d.Sg <= 24) return run_prex<Real, 24>(ops, nops, d, ls, s);
-    if (d.Sg <= 32) return run_prex<Real, 32>(ops, nops, d, ls, s);
-    if (d.Sg <= 48) return run_prex<Real, 48>(ops, nops, d, ls, s);
-    if (d.Sg <= 64) return run_prex<Real, 64>(ops, nops, d, ls, s);
-    return cudaErrorInvalidValue;
+    return cudaErrorInvalidValue;   // other state counts: k_generic.cu
 }
 
 template cudaError_t launch_update_partials<float>(const OpDesc*, int, const Dims&, double*, int,

@@ -340,6 +340,12 @@ cudaError_t launch_edge_derivatives(const DerivDesc* desc, int nb, const double*
     return cudaGetLastError();
 }
 
+cudaError_t launch_deriv_final(const double* d_block, int nblk, int nb, double* d_sums,
+                               cudaStream_t s) {
+    k_final_sum<<<2 * nb, kRB, 0, s>>>(d_block, nblk, 2 * nb, d_sums);
+    return cudaGetLastError();
+}
+
 // Per-block partial sums an edge-derivative launch needs (per branch, twice).
 int deriv_blocks(const Dims& d) {
     if (d.S == 4 && d.Sg == 4 && (d.C == 1 || d.C == 2 || d.C == 4 || d.C == 8))
