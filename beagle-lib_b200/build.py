@@ -5,6 +5,12 @@ g++ for the host instance and the C ABI, linked in-tree into ``lib/``.
     python beagle-lib_b200/build.py --clean
 
 Object files go to ``_build/`` at the repository root (git-ignored).
+
+When the BEAGLE sources are at hand (``BEAGLE_REF`` or the default path
+below), it also builds ``lib/libhmsbeagle-cuda.so.40.0.0``: the plugin that
+lets the stock libhmsbeagle.so dispatcher run on this library
+(``plugin/b200_plugin.cpp``, compiled against the dispatcher's public headers
+BeagleImpl.h / Plugin.h / beagle.h).  Without them the plugin is not rebuilt.
 """
 import concurrent.futures as cf
 import os
@@ -20,6 +26,9 @@ OBJ = os.path.join(ROOT, "_build", "beagle_b200")
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 LIBNAME = "libbeagle_b200.so"
+PLUGIN = "libhmsbeagle-cuda.so.40.0.0"     # name the dispatcher dlopens (PLUGIN_VERSION 40)
+PLUGIN_SRC = os.path.join(HERE, "plugin", "b200_plugin.cpp")
+BEAGLE_REF = os.environ.get("BEAGLE_REF", "/root/reference")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 INC = ["-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
@@ -78,13 +87,37 @@ def build(verbose=False):
     lib = os.path.join(LIBDIR, LIBNAME)
     if jobs or not os.path.exists(lib):
         cmd = [NVCC] + ARCH + ["-shared", "-o", lib] + objs + ["-lcudart_static", "-lrt", "-ldl",
-                                                                 "-lpthread"]
+                                                                 "-lpthread", "-Xlinker",
+                                                                 "-soname=" + LIBNAME]
         cmd, rc, out = _compile(cmd)
         if rc:
             print(" ".join(cmd))
             print(out)
             raise RuntimeError("link failed")
+    build_plugin(lib, verbose)
     return lib
+
+
+def build_plugin(lib, verbose=False):
+    """libhmsbeagle-cuda.so.40.0.0 beside libbeagle_b200.so (run path
+    $ORIGIN).  Returns its path, or None when the BEAGLE headers are absent."""
+    hdr = os.path.join(BEAGLE_REF, "libhmsbeagle", "BeagleImpl.h")
+    out = os.path.join(LIBDIR, PLUGIN)
+    if not os.path.exists(hdr):
+        return out if os.path.exists(out) else None
+    deps = [PLUGIN_SRC, lib, os.path.join(ROOT, "include", "beagle_b200.h")]
+    if os.path.exists(out) and all(os.path.getmtime(d) <= os.path.getmtime(out) for d in deps):
+        return out
+    cmd = ["g++", "-std=c++11", "-O2", "-fPIC", "-shared", "-Wall", "-Wno-unused-function",
+           "-Wno-delete-non-virtual-dtor", "-I" + BEAGLE_REF, "-I" + os.path.join(ROOT, "include"), PLUGIN_SRC, "-o", out,
+           "-L" + LIBDIR, "-l:" + LIBNAME, "-Wl,-soname," + PLUGIN, "-Wl,-rpath,$ORIGIN"]
+    cmd, rc, outp = _compile(cmd)
+    if verbose or rc:
+        print(" ".join(cmd))
+        print(outp)
+    if rc:
+        raise RuntimeError("plugin build failed")
+    return out
 
 
 if __name__ == "__main__":

@@ -70,18 +70,26 @@ BeagleB200ResourceList* beagleB200GetResourceList(void) {
             (void)cudaGetLastError();
             n = 0;
         }
+        // One entry per CUDA device, entry k = device ordinal k.  Devices the
+        // sm_100a kernels cannot run on are listed with no support flags.
+        std::vector<long> support;
         for (int d = 0; d < n; ++d) {
             cudaDeviceProp prop;
-            if (cudaGetDeviceProperties(&prop, d) != cudaSuccess || prop.major < 10) continue;
+            if (cudaGetDeviceProperties(&prop, d) != cudaSuccess) {
+                (void)cudaGetLastError();
+                prop.major = prop.minor = 0;
+                prop.name[0] = 0;
+            }
             g_resource_names.push_back(std::string(prop.name) + " (sm_" +
                                        std::to_string(prop.major) + std::to_string(prop.minor) +
-                                       "a), device " + std::to_string(d));
+                                       "), device " + std::to_string(d));
+            support.push_back(prop.major == 10 && prop.minor == 0 ? kSupportFlags : 0L);
         }
         g_resources.resize(g_resource_names.size());
         for (size_t k = 0; k < g_resources.size(); ++k) {
             g_resources[k].name = const_cast<char*>(g_resource_names[k].c_str());
-            g_resources[k].description = const_cast<char*>("B200 likelihood kernels");
-            g_resources[k].supportFlags = kSupportFlags;
+            g_resources[k].description = const_cast<char*>("B200 likelihood kernels (sm_100a)");
+            g_resources[k].supportFlags = support[k];
             g_resources[k].requiredFlags = BEAGLE_B200_FLAG_FRAMEWORK_CUDA;
         }
         g_resource_list.list = g_resources.empty() ? nullptr : g_resources.data();

@@ -7,6 +7,7 @@
 // results synchronise that stream; the others return as soon as the work is
 // queued (the caller's arrays have been copied by then).
 #include "b200_instance.h"
+#include "b200_tune.h"
 
 #include <cmath>
 #include <cstring>
@@ -131,7 +132,7 @@ int Instance::create(int tipCount, int partialsBufferCount, int compactBufferCou
     }
     cudaDeviceProp prop;
     CK(cudaGetDeviceProperties(&prop, device));
-    if (prop.major < 10) return -6;
+    if (prop.major != 10 || prop.minor != 0) return -6;   // sm_100 only
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
 
@@ -570,6 +571,18 @@ int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative,
     std::vector<uint8_t> dep(count, 0);
     // Buffers written earlier in this list count as holding data.
     std::vector<char> written(nbuf_, 0);
+    // A list is idempotent (may be run again by the autotuner) when no op
+    // reads a partials or scale buffer that the list writes at or after it.
+    bool idempotent = true;
+    std::vector<char> later(nbuf_, 0), later_scale(nscale_ > 0 ? nscale_ : 1, 0);
+    for (int k = count - 1; k >= 0; --k) {
+        const int* op = ops + (size_t)k * stride;
+        if (!buf_ok(op[0]) || !buf_ok(op[3]) || !buf_ok(op[5])) break;   // rejected below
+        later[op[0]] = 1;
+        if (op[1] >= 0 && op[1] < nscale_) later_scale[op[1]] = 1;
+        if (later[op[3]] || later[op[5]]) idempotent = false;
+        if (op[1] < 0 && op[2] >= 0 && op[2] < nscale_ && later_scale[op[2]]) idempotent = false;
+    }
     for (int k = 0; k < count; ++k) {
         const int* op = ops + (size_t)k * stride;
         const int dest = op[0], ws = op[1], rs = op[2], c1 = op[3], m1 = op[4], c2 = op[5],
@@ -616,12 +629,18 @@ int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative,
         CK(td.upload(dep.data(), dep.size(), stream_));
         CK(LAUNCH(launch_opwalk_generic, (const OpDesc*)t.ptr, (const uint8_t*)td.ptr, count, pre,
                   dims(), cum, (int)log_scalers_, stream_));
-    } else if (pre) {
-        CK(LAUNCH(launch_update_pre_partials, (const OpDesc*)t.ptr, count, dims(),
-                  (int)log_scalers_, stream_));
     } else {
-        CK(LAUNCH(launch_update_partials, (const OpDesc*)t.ptr, count, dims(), cum,
-                  (int)log_scalers_, stream_));
+        const OpDesc* d_ops = (const OpDesc*)t.ptr;
+        const Dims dm = dims();
+        const int ls = (int)log_scalers_;
+        auto run = [&](int v) -> cudaError_t {
+            return pre ? LAUNCH(launch_update_pre_partials, d_ops, count, dm, ls, stream_, v)
+                       : LAUNCH(launch_update_partials, d_ops, count, dm, cum, ls, stream_, v);
+        };
+        const TuneKey key{pre ? kTuneWalkPre : kTuneWalkPost, (int)dbl_, C_, Pp_,
+                          tune_count_class(count), device_};
+        const int v = tune_pick(key, s4_walk_variants(C_), idempotent && !cum, stream_, run);
+        CK(run(v));
     }
     return kSuccess;
 }
@@ -748,10 +767,16 @@ int Instance::calculateEdgeDerivatives(const int* post, const int* pre, const in
     CK(out_.reserve(sizeof(double) * 2 * count));
     if (outDerivs) CK(site_d_.reserve(sizeof(double) * (size_t)count * P_));
     if (S_ == 4) {
-        CK(LAUNCH(launch_edge_derivatives, (const DerivDesc*)t_deriv_.ptr, count,
-                  d_catw_ + (size_t)w * C_, d_patw_, dims(),
-                  outDerivs ? (double*)site_d_.ptr : nullptr, (double*)scratch_.ptr,
-                  (double*)out_.ptr, stream_));
+        const DerivDesc* d_desc = (const DerivDesc*)t_deriv_.ptr;
+        const double* catw = d_catw_ + (size_t)w * C_;
+        double* site = outDerivs ? (double*)site_d_.ptr : nullptr;
+        const Dims dm = dims();
+        auto run = [&](int v) -> cudaError_t {
+            return LAUNCH(launch_edge_derivatives, d_desc, count, catw, d_patw_, dm, site,
+                          (double*)scratch_.ptr, (double*)out_.ptr, stream_, v);
+        };
+        const TuneKey key{kTuneDeriv, (int)dbl_, C_, Pp_, tune_count_class(count), device_};
+        CK(run(tune_pick(key, deriv4_variants(dm), true, stream_, run)));
     } else {
         CK(LAUNCH(launch_deriv_generic, (const DerivDesc*)t_deriv_.ptr, count,
                   d_catw_ + (size_t)w * C_, d_patw_, dims(),

@@ -25,14 +25,18 @@ cudaError_t launch_matrix_pairs(const void* const* d_a, const void* const* d_b,
                                 void* const* d_out, int n, int op, const Dims& d,
                                 cudaStream_t s);
 
-// Post-order partials over an op list, one launch for the whole list.
+// Post-order partials over an op list (S = 4), one launch for the whole list.
+// `variant` selects the kernel shape (see s4_walk_variants; < 0 = default).
 template <typename Real>
 cudaError_t launch_update_partials(const OpDesc* d_ops, int nops, const Dims& d,
-                                   double* cumulative, int log_scalers, cudaStream_t s);
-// Pre-order partials over an op list.
+                                   double* cumulative, int log_scalers, cudaStream_t s,
+                                   int variant = -1);
+// Pre-order partials over an op list (S = 4).
 template <typename Real>
 cudaError_t launch_update_pre_partials(const OpDesc* d_ops, int nops, const Dims& d,
-                                       int log_scalers, cudaStream_t s);
+                                       int log_scalers, cudaStream_t s, int variant = -1);
+// Number of S = 4 op-walk variants for C categories (variants 0 .. n-1).
+int s4_walk_variants(int C);
 
 // The same op lists for S != 4 (S <= 64, C <= 8): clustered CUDA-core kernels.
 // dep[o] != 0 when op o reads the output of op o - 1.
@@ -65,11 +69,14 @@ cudaError_t launch_edge_lnl(const void* parent, const void* child, int child_is_
 
 // Edge derivatives for `nb` branches; per-site values optional (d_site may be
 // null), sums and sums of squares into d_sums[2*nb].  d_block holds
-// 2 * nb * deriv_blocks(d) doubles of per-block partial sums.
+// 2 * nb * deriv_blocks(d) doubles of per-block partial sums.  `variant`
+// selects the S = 4 kernel shape (0 .. deriv4_variants(d) - 1; < 0 = default).
 template <typename Real>
 cudaError_t launch_edge_derivatives(const DerivDesc* d_desc, int nb, const double* catw,
                                     const double* patw, const Dims& d, double* d_site,
-                                    double* d_block, double* d_sums, cudaStream_t s);
+                                    double* d_block, double* d_sums, cudaStream_t s,
+                                    int variant = -1);
+int deriv4_variants(const Dims& d);
 
 // cumulative[p] += sign * sum_i f(scale[idx_i][p]), f = identity (log scalers) or log.
 cudaError_t launch_accumulate_scale(double* cumulative, const double* pool, const int* d_idx,

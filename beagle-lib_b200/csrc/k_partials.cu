@@ -319,9 +319,13 @@ k_pre4p(const OpDesc* __restrict__ ops, int nops, int Pp, int log_scalers) {
     }
 }
 
-// Patterns per thread for the lane-group kernels: the smallest PPT whose grid
-// fits in one resident wave (occupancy from the CUDA runtime for that very
-// instantiation), else the largest.
+// Variants of the S = 4 op walks (chosen per shape by the instance's
+// autotuner, b200_instance.cpp):
+//   0      thread per pattern, all categories in registers (any C <= 8);
+//   1,2,3  thread per (pattern, category) with 1, 2 or 4 patterns per thread
+//          (C dividing 32).
+// variant < 0 picks the default: the smallest patterns-per-thread whose grid
+// fits in one resident wave, thread per pattern when C does not divide 32.
 template <typename K>
 long wave_patterns(K kernel, int C, int ppt) {
     int dev = 0, sms = 0, blocks = 0;
@@ -333,17 +337,15 @@ long wave_patterns(K kernel, int C, int ppt) {
 }
 
 template <typename Real, int C>
-int pick_ppt_post(int Pp) {
-    static const long w1 = wave_patterns(k_post4<Real, C, 1>, C, 1);
-    static const long w2 = wave_patterns(k_post4<Real, C, 2>, C, 2);
-    return Pp <= w1 ? 1 : Pp <= w2 ? 2 : 4;
-}
-
-template <typename Real, int C>
-int pick_ppt_pre(int Pp) {
-    static const long w1 = wave_patterns(k_pre4<Real, C, 1>, C, 1);
-    static const long w2 = wave_patterns(k_pre4<Real, C, 2>, C, 2);
-    return Pp <= w1 ? 1 : Pp <= w2 ? 2 : 4;
+int default_variant(int Pp, bool pre) {
+    if (32 % C != 0) return 0;
+    constexpr int CC = (32 % C == 0 ? C : 1);
+    static const long p1 = wave_patterns(k_post4<Real, CC, 1>, CC, 1);
+    static const long p2 = wave_patterns(k_post4<Real, CC, 2>, CC, 2);
+    static const long q1 = wave_patterns(k_pre4<Real, CC, 1>, CC, 1);
+    static const long q2 = wave_patterns(k_pre4<Real, CC, 2>, CC, 2);
+    const long w1 = pre ? q1 : p1, w2 = pre ? q2 : p2;
+    return Pp <= w1 ? 1 : Pp <= w2 ? 2 : 3;
 }
 
 template <typename Real, int C, int PPT>
@@ -365,12 +367,14 @@ cudaError_t run_pre4_ppt(const OpDesc* ops, int nops, const Dims& d, int ls, cud
 
 template <typename Real, int C>
 cudaError_t run_post4(const OpDesc* ops, int nops, const Dims& d, double* cum, int ls,
-                      cudaStream_t s) {
-    if (32 % C == 0) {
-        switch (pick_ppt_post<Real, (32 % C == 0 ? C : 1)>(d.Pp)) {
-            case 1: return run_post4_ppt<Real, (32 % C == 0 ? C : 1), 1>(ops, nops, d, cum, ls, s);
-            case 2: return run_post4_ppt<Real, (32 % C == 0 ? C : 1), 2>(ops, nops, d, cum, ls, s);
-            default: return run_post4_ppt<Real, (32 % C == 0 ? C : 1), 4>(ops, nops, d, cum, ls, s);
+                      cudaStream_t s, int variant) {
+    if (variant < 0) variant = default_variant<Real, C>(d.Pp, false);
+    if (variant > 0 && 32 % C == 0) {
+        constexpr int CC = (32 % C == 0 ? C : 1);
+        switch (variant) {
+            case 1: return run_post4_ppt<Real, CC, 1>(ops, nops, d, cum, ls, s);
+            case 2: return run_post4_ppt<Real, CC, 2>(ops, nops, d, cum, ls, s);
+            default: return run_post4_ppt<Real, CC, 4>(ops, nops, d, cum, ls, s);
         }
     }
     k_post4p<Real, C><<<(d.Pp + 127) / 128, 128, 0, s>>>(ops, nops, d.Pp, cum, ls);
@@ -378,12 +382,15 @@ cudaError_t run_post4(const OpDesc* ops, int nops, const Dims& d, double* cum, i
 }
 
 template <typename Real, int C>
-cudaError_t run_pre4(const OpDesc* ops, int nops, const Dims& d, int ls, cudaStream_t s) {
-    if (32 % C == 0) {
-        switch (pick_ppt_pre<Real, (32 % C == 0 ? C : 1)>(d.Pp)) {
-            case 1: return run_pre4_ppt<Real, (32 % C == 0 ? C : 1), 1>(ops, nops, d, ls, s);
-            case 2: return run_pre4_ppt<Real, (32 % C == 0 ? C : 1), 2>(ops, nops, d, ls, s);
-            default: return run_pre4_ppt<Real, (32 % C == 0 ? C : 1), 4>(ops, nops, d, ls, s);
+cudaError_t run_pre4(const OpDesc* ops, int nops, const Dims& d, int ls, cudaStream_t s,
+                     int variant) {
+    if (variant < 0) variant = default_variant<Real, C>(d.Pp, true);
+    if (variant > 0 && 32 % C == 0) {
+        constexpr int CC = (32 % C == 0 ? C : 1);
+        switch (variant) {
+            case 1: return run_pre4_ppt<Real, CC, 1>(ops, nops, d, ls, s);
+            case 2: return run_pre4_ppt<Real, CC, 2>(ops, nops, d, ls, s);
+            default: return run_pre4_ppt<Real, CC, 4>(ops, nops, d, ls, s);
         }
     }
     k_pre4p<Real, C><<<(d.Pp + 127) / 128, 128, 0, s>>>(ops, nops, d.Pp, ls);
@@ -392,20 +399,22 @@ cudaError_t run_pre4(const OpDesc* ops, int nops, const Dims& d, int ls, cudaStr
 
 }  // namespace
 
+int s4_walk_variants(int C) { return (32 % C == 0) ? 4 : 1; }
+
 template <typename Real>
 cudaError_t launch_update_partials(const OpDesc* ops, int nops, const Dims& d, double* cum,
-                                   int ls, cudaStream_t s) {
+                                   int ls, cudaStream_t s, int variant) {
     if (nops == 0) return cudaSuccess;
     if (d.S == 4 && d.C <= 8) {
         switch (d.C) {
-            case 1: return run_post4<Real, 1>(ops, nops, d, cum, ls, s);
-            case 2: return run_post4<Real, 2>(ops, nops, d, cum, ls, s);
-            case 3: return run_post4<Real, 3>(ops, nops, d, cum, ls, s);
-            case 4: return run_post4<Real, 4>(ops, nops, d, cum, ls, s);
-            case 5: return run_post4<Real, 5>(ops, nops, d, cum, ls, s);
-            case 6: return run_post4<Real, 6>(ops, nops, d, cum, ls, s);
-            case 7: return run_post4<Real, 7>(ops, nops, d, cum, ls, s);
-            default: return run_post4<Real, 8>(ops, nops, d, cum, ls, s);
+            case 1: return run_post4<Real, 1>(ops, nops, d, cum, ls, s, variant);
+            case 2: return run_post4<Real, 2>(ops, nops, d, cum, ls, s, variant);
+            case 3: return run_post4<Real, 3>(ops, nops, d, cum, ls, s, variant);
+            case 4: return run_post4<Real, 4>(ops, nops, d, cum, ls, s, variant);
+            case 5: return run_post4<Real, 5>(ops, nops, d, cum, ls, s, variant);
+            case 6: return run_post4<Real, 6>(ops, nops, d, cum, ls, s, variant);
+            case 7: return run_post4<Real, 7>(ops, nops, d, cum, ls, s, variant);
+            default: return run_post4<Real, 8>(ops, nops, d, cum, ls, s, variant);
         }
     }
     return cudaErrorInvalidValue;   // other state counts: k_generic.cu
@@ -413,30 +422,30 @@ cudaError_t launch_update_partials(const OpDesc* ops, int nops, const Dims& d, d
 
 template <typename Real>
 cudaError_t launch_update_pre_partials(const OpDesc* ops, int nops, const Dims& d, int ls,
-                                       cudaStream_t s) {
+                                       cudaStream_t s, int variant) {
     if (nops == 0) return cudaSuccess;
     if (d.S == 4 && d.C <= 8) {
         switch (d.C) {
-            case 1: return run_pre4<Real, 1>(ops, nops, d, ls, s);
-            case 2: return run_pre4<Real, 2>(ops, nops, d, ls, s);
-            case 3: return run_pre4<Real, 3>(ops, nops, d, ls, s);
-            case 4: return run_pre4<Real, 4>(ops, nops, d, ls, s);
-            case 5: return run_pre4<Real, 5>(ops, nops, d, ls, s);
-            case 6: return run_pre4<Real, 6>(ops, nops, d, ls, s);
-            case 7: return run_pre4<Real, 7>(ops, nops, d, ls, s);
-            default: return run_pre4<Real, 8>(ops, nops, d, ls, s);
+            case 1: return run_pre4<Real, 1>(ops, nops, d, ls, s, variant);
+            case 2: return run_pre4<Real, 2>(ops, nops, d, ls, s, variant);
+            case 3: return run_pre4<Real, 3>(ops, nops, d, ls, s, variant);
+            case 4: return run_pre4<Real, 4>(ops, nops, d, ls, s, variant);
+            case 5: return run_pre4<Real, 5>(ops, nops, d, ls, s, variant);
+            case 6: return run_pre4<Real, 6>(ops, nops, d, ls, s, variant);
+            case 7: return run_pre4<Real, 7>(ops, nops, d, ls, s, variant);
+            default: return run_pre4<Real, 8>(ops, nops, d, ls, s, variant);
         }
     }
     return cudaErrorInvalidValue;   // other state counts: k_generic.cu
 }
 
 template cudaError_t launch_update_partials<float>(const OpDesc*, int, const Dims&, double*, int,
-                                                   cudaStream_t);
+                                                   cudaStream_t, int);
 template cudaError_t launch_update_partials<double>(const OpDesc*, int, const Dims&, double*, int,
-                                                    cudaStream_t);
+                                                    cudaStream_t, int);
 template cudaError_t launch_update_pre_partials<float>(const OpDesc*, int, const Dims&, int,
-                                                       cudaStream_t);
+                                                       cudaStream_t, int);
 template cudaError_t launch_update_pre_partials<double>(const OpDesc*, int, const Dims&, int,
-                                                        cudaStream_t);
+                                                        cudaStream_t, int);
 
 }  // namespace b200

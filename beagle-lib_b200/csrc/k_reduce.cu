@@ -217,58 +217,81 @@ k_edge_deriv(const DerivDesc* __restrict__ desc, const double* __restrict__ catw
 
 // S = 4 specialisation of k_edge_deriv: one thread per (pattern, category)
 // with 16-byte (FP32) / 32-byte (FP64) vector loads; the C threads of a
-// pattern combine their weighted terms with shuffles.  kRB / C patterns per
-// CTA, blockIdx.y = branch.
-template <typename Real, int C>
+// pattern combine their weighted terms with shuffles.  Each thread covers PPT
+// patterns kRB / C apart, so a CTA covers kRB / C * PPT patterns and pays its
+// two block reductions once for all of them; blockIdx.y = branch.  The
+// category's 4x4 derivative matrix is held in registers across the PPT
+// patterns.
+template <typename Real, int C, int PPT>
 __global__ void __launch_bounds__(kRB)
 k_edge_deriv4(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
               const double* __restrict__ patw, int P, double* site, double* block) {
     __shared__ double sh[kRB / 32];
+    constexpr int kSlots = kRB / C;
     const int b = blockIdx.y;
     const int c = threadIdx.x % C;
-    const int p = blockIdx.x * (kRB / C) + threadIdx.x / C;
+    const int p0 = blockIdx.x * (kSlots * PPT) + threadIdx.x / C;
     const DerivDesc& dd = desc[b];
-    const int pc = min(p, P - 1);
     const Real* D = static_cast<const Real*>(dd.dmat) + c * 16;
-    const Real* pre = static_cast<const Real*>(dd.pre) + ((size_t)pc * C + c) * 4;
-    Real z[4], x[4];
-    ld4(pre, z);
-    Real n = 0, q = 0;
-    if (dd.post_is_states) {
-        const int s = static_cast<const int*>(dd.post)[pc];
+    Real dm[16];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const Real dk = (s < 4) ? __ldg(D + k * 4 + (s & 3)) : (Real)dd.dpad;
-            n += z[k] * dk;
-            q += (s >= 4 || k == s) ? z[k] : Real(0);
-        }
-    } else {
-        ld4(static_cast<const Real*>(dd.post) + ((size_t)pc * C + c) * 4, x);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const Real y = __ldg(D + k * 4) * x[0] + __ldg(D + k * 4 + 1) * x[1] +
-                           __ldg(D + k * 4 + 2) * x[2] + __ldg(D + k * 4 + 3) * x[3];
-            n += z[k] * y;
-            q += z[k] * x[k];
-        }
-    }
+    for (int k = 0; k < 4; ++k) ld4(D + 4 * k, dm + 4 * k);
     const double w = catw[c];
-    double num = w * (double)n, den = w * (double)q;
+    Real z[PPT][4], x[PPT][4];
+    int st[PPT];
+    const bool states = dd.post_is_states;
 #pragma unroll
-    for (int o = 1; o < C; o <<= 1) {
-        num += __shfl_xor_sync(0xffffffffu, num, o);
-        den += __shfl_xor_sync(0xffffffffu, den, o);
+    for (int j = 0; j < PPT; ++j) {
+        const int pc = min(p0 + j * kSlots, P - 1);
+        ld4(static_cast<const Real*>(dd.pre) + ((size_t)pc * C + c) * 4, z[j]);
+        if (states)
+            st[j] = static_cast<const int*>(dd.post)[pc];
+        else
+            ld4(static_cast<const Real*>(dd.post) + ((size_t)pc * C + c) * 4, x[j]);
     }
-    double d = 0;
-    if (c == 0 && p < P) {
-        d = num / den;
-        if (site) site[(size_t)b * P + p] = d;
+    double s1 = 0, s2 = 0;
+#pragma unroll
+    for (int j = 0; j < PPT; ++j) {
+        const int p = p0 + j * kSlots;
+        Real n = 0, q = 0;
+        if (states) {
+            const int s = st[j];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                Real dk = (Real)dd.dpad;
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    if (s == i) dk = dm[k * 4 + i];
+                n += z[j][k] * dk;
+                q += (s >= 4 || k == s) ? z[j][k] : Real(0);
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const Real y = dm[k * 4] * x[j][0] + dm[k * 4 + 1] * x[j][1] +
+                               dm[k * 4 + 2] * x[j][2] + dm[k * 4 + 3] * x[j][3];
+                n += z[j][k] * y;
+                q += z[j][k] * x[j][k];
+            }
+        }
+        double num = w * (double)n, den = w * (double)q;
+#pragma unroll
+        for (int o = 1; o < C; o <<= 1) {
+            num += __shfl_xor_sync(0xffffffffu, num, o);
+            den += __shfl_xor_sync(0xffffffffu, den, o);
+        }
+        if (c == 0 && p < P) {
+            const double d = num / den;
+            if (site) site[(size_t)b * P + p] = d;
+            const double wp = patw[p];
+            s1 += d * wp;
+            s2 += d * d * wp;
+        }
     }
-    const double wp = (c == 0 && p < P) ? patw[p] : 0.0;
     const int nblk = gridDim.x;
-    double t = block_sum(d * wp, sh);
+    double t = block_sum(s1, sh);
     if (threadIdx.x == 0) block[(size_t)b * nblk + blockIdx.x] = t;
-    t = block_sum(d * d * wp, sh);
+    t = block_sum(s2, sh);
     if (threadIdx.x == 0) block[(size_t)(gridDim.y + b) * nblk + blockIdx.x] = t;
 }
 
@@ -316,20 +339,48 @@ cudaError_t launch_edge_lnl(const void* parent, const void* child, int child_is_
     return cudaGetLastError();
 }
 
+namespace {
+
+bool deriv4_shape(const Dims& d) {
+    return d.S == 4 && d.Sg == 4 && (d.C == 1 || d.C == 2 || d.C == 4 || d.C == 8);
+}
+
+// Patterns per thread of variant v of the S = 4 derivative kernel.
+int deriv4_ppt(int v) { return v <= 0 ? 1 : v == 1 ? 2 : v == 2 ? 4 : 8; }
+
+template <typename Real, int C>
+void run_deriv4(int ppt, dim3 grid, cudaStream_t s, const DerivDesc* desc, const double* catw,
+                const double* patw, int P, double* site, double* block) {
+    switch (ppt) {
+        case 1: k_edge_deriv4<Real, C, 1><<<grid, kRB, 0, s>>>(desc, catw, patw, P, site, block); break;
+        case 2: k_edge_deriv4<Real, C, 2><<<grid, kRB, 0, s>>>(desc, catw, patw, P, site, block); break;
+        case 4: k_edge_deriv4<Real, C, 4><<<grid, kRB, 0, s>>>(desc, catw, patw, P, site, block); break;
+        default: k_edge_deriv4<Real, C, 8><<<grid, kRB, 0, s>>>(desc, catw, patw, P, site, block); break;
+    }
+}
+
+}  // namespace
+
+int deriv4_variants(const Dims& d) { return deriv4_shape(d) ? 4 : 1; }
+
 template <typename Real>
 cudaError_t launch_edge_derivatives(const DerivDesc* desc, int nb, const double* catw,
                                     const double* patw, const Dims& d, double* d_site,
-                                    double* d_block, double* d_sums, cudaStream_t s) {
+                                    double* d_block, double* d_sums, cudaStream_t s,
+                                    int variant) {
     if (nb == 0) return cudaSuccess;
     int nblk = reduction_blocks(d.P);
-    if (d.S == 4 && d.Sg == 4 && (d.C == 1 || d.C == 2 || d.C == 4 || d.C == 8)) {
-        nblk = (d.P + kRB / d.C - 1) / (kRB / d.C);
+    if (deriv4_shape(d)) {
+        if (variant < 0) variant = d.P >= 32768 ? 2 : 0;
+        const int ppt = deriv4_ppt(variant);
+        const int ppb = kRB / d.C * ppt;
+        nblk = (d.P + ppb - 1) / ppb;
         dim3 grid(nblk, nb);
         switch (d.C) {
-            case 1: k_edge_deriv4<Real, 1><<<grid, kRB, 0, s>>>(desc, catw, patw, d.P, d_site, d_block); break;
-            case 2: k_edge_deriv4<Real, 2><<<grid, kRB, 0, s>>>(desc, catw, patw, d.P, d_site, d_block); break;
-            case 4: k_edge_deriv4<Real, 4><<<grid, kRB, 0, s>>>(desc, catw, patw, d.P, d_site, d_block); break;
-            default: k_edge_deriv4<Real, 8><<<grid, kRB, 0, s>>>(desc, catw, patw, d.P, d_site, d_block); break;
+            case 1: run_deriv4<Real, 1>(ppt, grid, s, desc, catw, patw, d.P, d_site, d_block); break;
+            case 2: run_deriv4<Real, 2>(ppt, grid, s, desc, catw, patw, d.P, d_site, d_block); break;
+            case 4: run_deriv4<Real, 4>(ppt, grid, s, desc, catw, patw, d.P, d_site, d_block); break;
+            default: run_deriv4<Real, 8>(ppt, grid, s, desc, catw, patw, d.P, d_site, d_block); break;
         }
     } else {
         dim3 grid(nblk, nb);
@@ -346,10 +397,10 @@ cudaError_t launch_deriv_final(const double* d_block, int nblk, int nb, double* 
     return cudaGetLastError();
 }
 
-// Per-block partial sums an edge-derivative launch needs (per branch, twice).
+// Per-block partial sums an edge-derivative launch needs (per branch, twice),
+// for the variant with the most blocks.
 int deriv_blocks(const Dims& d) {
-    if (d.S == 4 && d.Sg == 4 && (d.C == 1 || d.C == 2 || d.C == 4 || d.C == 8))
-        return (d.P + kRB / d.C - 1) / (kRB / d.C);
+    if (deriv4_shape(d)) return (d.P + kRB / d.C - 1) / (kRB / d.C);
     return reduction_blocks(d.P);
 }
 
@@ -375,7 +426,7 @@ cudaError_t launch_accumulate_scale(double* cum, const double* pool, const int* 
                                             double*, double*, double*, cudaStream_t);            \
     template cudaError_t launch_edge_derivatives<R>(const DerivDesc*, int, const double*,        \
                                                     const double*, const Dims&, double*,         \
-                                                    double*, double*, cudaStream_t);
+                                                    double*, double*, cudaStream_t, int);
 INST(float)
 INST(double)
 #undef INST

@@ -13,8 +13,9 @@
  * beagle.h, so a beagle.h client passes its own values unchanged.
  *
  * The library runs on one CUDA device per instance (resourceList[0] picks the
- * device ordinal; default 0).  It has no CPU fallback: with no usable sm_100
- * device, beagleB200CreateInstance returns BEAGLE_B200_ERROR_NO_RESOURCE.
+ * device ordinal; default 0; entry k of beagleB200GetResourceList is device
+ * k).  It has no CPU fallback: on a device other than sm_100,
+ * beagleB200CreateInstance returns BEAGLE_B200_ERROR_NO_RESOURCE.
  */
 #ifndef BEAGLE_B200_H
 #define BEAGLE_B200_H
@@ -114,7 +115,8 @@ typedef struct {
 /* ---- library / instance lifetime ------------------------------------- */
 /* replaces beagleGetVersion (beagle.h:280) */
 const char* beagleB200GetVersion(void);
-/* replaces beagleGetResourceList (beagle.h:300): one resource per CUDA device */
+/* replaces beagleGetResourceList (beagle.h:300): one resource per CUDA device,
+ * in ordinal order; devices other than sm_100 carry no support flags */
 BeagleB200ResourceList* beagleB200GetResourceList(void);
 /* replaces beagleCreateInstance (beagle.h:378-391); resourceList[0], when
  * given, is the CUDA device ordinal.  Returns the instance index (>= 0). */

@@ -171,3 +171,21 @@ def test_full_size_configs(b200, syn, oracle, name, precision):
     tol = TOL[precision]
     assert rel(lnl, lo) <= tol["lnl"], (lnl, lo, rel(lnl, lo))
     assert grad_err(g, go) <= tol["grad"], grad_err(g, go)
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+def test_s4_kernel_variants(b200, syn, oracle, monkeypatch, precision, variant):
+    """Every S = 4 op-walk and derivative kernel shape the autotuner can pick
+    (forced through BEAGLE_B200_FORCE_VARIANT) against the oracle, with C = 4
+    (lane-group shapes; tips as states and as partials) and C = 3
+    (thread-per-pattern walk)."""
+    monkeypatch.setenv("BEAGLE_B200_FORCE_VARIANT", str(variant))
+    for C, amb in ((4, 0.0), (4, 0.02), (3, 0.0)):
+        pr = syn.make_problem(S=4, N=20, P=2900, C=C, seed=40 + variant, rescale=True,
+                              ambiguous=amb)
+        _, lnl, g = run_b200(b200, pr, precision)
+        _, lo, go = run_oracle(oracle, pr)
+        tol = TOL[precision]
+        assert rel(lnl, lo) <= tol["lnl"], (C, lnl, lo)
+        assert grad_err(g, go) <= tol["grad"], (C, grad_err(g, go))
