@@ -87,6 +87,7 @@ Instance::~Instance() {
                       &scratch_, &out_, &site_d_, &t_dep_post_, &t_dep_pre_})
         b->release();
     if (h_out_) cudaFreeHost(h_out_);
+    if (h_tc_status_) cudaFreeHost(h_tc_status_);
     for (auto& c : chunks_) cudaFreeHost(c.first);
     if (stream_) cudaStreamDestroy(stream_);
 }
@@ -194,11 +195,24 @@ int Instance::create(int tipCount, int partialsBufferCount, int compactBufferCou
                        stream_));
     h_out_n_ = 64;
     CK(cudaMallocHost(&h_out_, sizeof(double) * h_out_n_));
+    CK(cudaMallocHost(&h_tc_status_, sizeof(int)));
+    *h_tc_status_ = 0;
     return sync();
 }
 
 int Instance::sync() {
+    if (tc_used_) CK(tc_status_async(h_tc_status_, stream_));
     CK(cudaStreamSynchronize(stream_));
+    if (tc_used_ && *h_tc_status_) {
+        // A tensor-core kernel gave up waiting on its MMAs and computed
+        // garbage: report it instead of the results.
+        *h_tc_status_ = 0;
+        CK(tc_clear_status(stream_));
+        pending_.clear();
+        chunk_i_ = 0;
+        chunk_off_ = 0;
+        return kErrGeneral;
+    }
     for (const Pending& pd : pending_) {
         if (pd.count == 0) {
             last_lnl_ = pd.slot[0];
@@ -627,8 +641,29 @@ int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative,
     if (S_ != 4) {
         DevBuf& td = pre ? t_dep_pre_ : t_dep_post_;
         CK(td.upload(dep.data(), dep.size(), stream_));
-        CK(LAUNCH(launch_opwalk_generic, (const OpDesc*)t.ptr, (const uint8_t*)td.ptr, count, pre,
-                  dims(), cum, (int)log_scalers_, stream_));
+        const OpDesc* d_ops = (const OpDesc*)t.ptr;
+        const Dims dm = dims();
+        const int ls = (int)log_scalers_;
+        // variant 0: CUDA-core cluster kernels; 1: tensor cores (FP32 only)
+        auto run = [&](int v) -> cudaError_t {
+            if (v == 1) {
+                tc_used_ = true;
+                return launch_opwalk_tc(d_ops, count, pre, dm, cum, ls, stream_);
+            }
+            return LAUNCH(launch_opwalk_generic, d_ops, (const uint8_t*)td.ptr, count, pre, dm,
+                          cum, ls, stream_);
+        };
+        const bool tc = !dbl_ && tc_supported(dm);
+        const TuneKey key{pre ? kTuneWalkPre : kTuneWalkPost, (int)dbl_, C_ * 100 + Sg_, Pp_,
+                          tune_count_class(count), device_};
+        int v = tune_pick(key, tc ? 2 : 1, idempotent && !cum, stream_, run);
+        if (v < 0) v = tc ? 1 : 0;
+        cudaError_t e = run(v);
+        if (e == cudaErrorInvalidConfiguration && v == 1) {
+            (void)cudaGetLastError();
+            e = run(0);
+        }
+        CK(e);
     } else {
         const OpDesc* d_ops = (const OpDesc*)t.ptr;
         const Dims dm = dims();
@@ -761,7 +796,9 @@ int Instance::calculateEdgeDerivatives(const int* post, const int* pre, const in
         d.dpad = mat_pad_[dmat[k]];
         d.reserved = 0;
     }
-    const int nblk = S_ == 4 ? deriv_blocks(dims()) : Pp_ / generic_tile_patterns(Sg_, dbl_);
+    const int nblk_generic = Pp_ / generic_tile_patterns(Sg_, dbl_);
+    const int nblk_tc = Pp_ / tc_tile_patterns();
+    const int nblk = S_ == 4 ? deriv_blocks(dims()) : std::max(nblk_generic, nblk_tc);
     CK(t_deriv_.upload(tab.data(), sizeof(DerivDesc) * count, stream_));
     CK(scratch_.reserve(sizeof(double) * 2 * (size_t)count * nblk));
     CK(out_.reserve(sizeof(double) * 2 * count));
@@ -778,10 +815,36 @@ int Instance::calculateEdgeDerivatives(const int* post, const int* pre, const in
         const TuneKey key{kTuneDeriv, (int)dbl_, C_, Pp_, tune_count_class(count), device_};
         CK(run(tune_pick(key, deriv4_variants(dm), true, stream_, run)));
     } else {
-        CK(LAUNCH(launch_deriv_generic, (const DerivDesc*)t_deriv_.ptr, count,
-                  d_catw_ + (size_t)w * C_, d_patw_, dims(),
-                  outDerivs ? (double*)site_d_.ptr : nullptr, (double*)scratch_.ptr, stream_));
-        CK(launch_deriv_final((double*)scratch_.ptr, nblk, count, (double*)out_.ptr, stream_));
+        const DerivDesc* d_desc = (const DerivDesc*)t_deriv_.ptr;
+        const double* catw = d_catw_ + (size_t)w * C_;
+        double* site = outDerivs ? (double*)site_d_.ptr : nullptr;
+        const Dims dm = dims();
+        // variant 0: CUDA-core cluster kernel; 1: tensor cores (FP32 only)
+        auto run = [&](int v) -> cudaError_t {
+            cudaError_t e;
+            if (v == 1) {
+                tc_used_ = true;
+                e = launch_deriv_tc(d_desc, count, catw, d_patw_, dm, site,
+                                    (double*)scratch_.ptr, stream_);
+            } else {
+                e = LAUNCH(launch_deriv_generic, d_desc, count, catw, d_patw_, dm, site,
+                           (double*)scratch_.ptr, stream_);
+            }
+            if (e != cudaSuccess) return e;
+            return launch_deriv_final((double*)scratch_.ptr, v == 1 ? nblk_tc : nblk_generic,
+                                      count, (double*)out_.ptr, stream_);
+        };
+        const bool tc = !dbl_ && tc_supported(dm);
+        const TuneKey key{kTuneDeriv, (int)dbl_, C_ * 100 + Sg_, Pp_, tune_count_class(count),
+                          device_};
+        int v = tune_pick(key, tc ? 2 : 1, true, stream_, run);
+        if (v < 0) v = tc ? 1 : 0;
+        cudaError_t e = run(v);
+        if (e == cudaErrorInvalidConfiguration && v == 1) {
+            (void)cudaGetLastError();
+            e = run(0);
+        }
+        CK(e);
     }
     if (async_ && !outDerivs) {
         // ASYNCH: sums are written to the caller's arrays at the next

@@ -51,6 +51,24 @@ cudaError_t launch_deriv_generic(const DerivDesc* d_desc, int nb, const double* 
 // Pattern tile of the clustered kernels (one derivative partial per tile).
 int generic_tile_patterns(int Sg, bool dbl);
 
+// The FP32 op lists and edge derivatives for 4 < S <= 64 on the tensor cores
+// (tcgen05, 3 x tf32 split products), k_tc.cu.  Same arguments and results as
+// the clustered CUDA-core kernels; one derivative partial per tc_tile_patterns()
+// patterns.  A launch that cannot guarantee TMEM for every resident CTA is
+// refused with cudaErrorInvalidConfiguration.
+bool tc_supported(const Dims& d);
+int tc_tile_patterns();
+cudaError_t launch_opwalk_tc(const OpDesc* d_ops, int nops, bool pre, const Dims& d,
+                             double* cumulative, int log_scalers, cudaStream_t s);
+cudaError_t launch_deriv_tc(const DerivDesc* d_desc, int nb, const double* catw,
+                            const double* patw, const Dims& d, double* d_site, double* d_block,
+                            cudaStream_t s);
+// The flag a tensor-core kernel sets when a bounded wait on its tensor-core
+// work timed out: queue its copy into pinned host memory on `s` (read it after
+// the stream completes), and clear it (synchronises `s`).
+cudaError_t tc_status_async(int* pinned_dst, cudaStream_t s);
+cudaError_t tc_clear_status(cudaStream_t s);
+
 // Root log-likelihood: site lnL into d_site[P]; the weighted total into d_out[0].
 template <typename Real>
 cudaError_t launch_root_lnl(const void* root, const double* catw, const double* freqs,

@@ -203,6 +203,161 @@ k_pre4(const OpDesc* __restrict__ ops, int nops, int Pp, int log_scalers) {
     }
 }
 
+// ------------------------------------------- S = 4, software-pipelined walk
+// Same thread layout as k_post4 / k_pre4, but the loads of op i+1's operands
+// are issued before op i is computed, so two ops' loads are in flight per
+// thread.  An operand that op i or op i-1 produced is not re-read: every
+// thread computes the same (pattern, category) rows in every op, so the value
+// is already in its registers (op i's result is forwarded when op i+1 starts,
+// op i-1's result is copied at prefetch time).  Operands written earlier than
+// that were stored by this same thread before the prefetch load is issued.
+//
+// Op descriptors are staged in two shared-memory chunks: chunk j+1 is staged
+// while chunk j is walked, so the prefetch of the first op of a chunk reads a
+// staged descriptor too.
+template <typename Real, int PPT>
+struct Rows4 {
+    Real v[PPT][4];
+};
+
+// Load one operand (partials rows or tip states) of PPT patterns.
+template <typename Real, int C, int PPT>
+__device__ __forceinline__ void load_operand4(const void* x, bool states, const int* pc, int c,
+                                              Rows4<Real, PPT>& r, int* st) {
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+        if (states) st[k] = static_cast<const int*>(x)[pc[k]];
+        else ld4(static_cast<const Real*>(x) + ((size_t)pc[k] * C + c) * 4, r.v[k]);
+    }
+}
+
+// Where op `nx`'s operand x comes from: 0 = load, 1 = result of the op being
+// computed now (`cur_dest`), 2 = result of the op before it (`prev_dest`).
+__device__ __forceinline__ int operand_source(const void* x, bool states, const void* cur_dest,
+                                              const void* prev_dest) {
+    if (states) return 0;
+    if (x == cur_dest) return 1;
+    if (x == prev_dest) return 2;
+    return 0;
+}
+
+__device__ __forceinline__ const OpDesc& staged_op(const OpDesc* s_ops, int i) {
+    return s_ops[((i / kOpChunk) & 1) * kOpChunk + (i % kOpChunk)];
+}
+
+// Stage chunk j of the op list into its shared-memory half (j & 1).
+__device__ __forceinline__ void stage_chunk(OpDesc* s_ops, const OpDesc* __restrict__ ops,
+                                            int nops, int j) {
+    const int o0 = j * kOpChunk;
+    if (o0 >= nops) return;
+    stage_ops(s_ops + (j & 1) * kOpChunk, ops + o0, min(kOpChunk, nops - o0));
+}
+
+template <typename Real, int C, int PPT, bool PRE>
+__global__ void __launch_bounds__(kT4)
+k_walk4_pipe(const OpDesc* __restrict__ ops, int nops, int Pp, double* cum, int log_scalers) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    OpDesc* s_ops = reinterpret_cast<OpDesc*>(smem_raw);      // [2][kOpChunk]
+    const int c = threadIdx.x % C;
+    const int ppb = kT4 / C;
+    const int pstride = gridDim.x * ppb;
+    const int p0 = blockIdx.x * ppb + threadIdx.x / C;
+    int pc[PPT];
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) pc[k] = min(p0 + k * pstride, Pp - 1);
+
+    Rows4<Real, PPT> a, b, hist;       // operands of op i; result of op i-1
+    int sa[PPT] = {}, sb[PPT] = {};
+    int src_a = 0, src_b = 0;          // 1: take the operand from `hist` (op i-1's result)
+    const void* prev_dest = nullptr;
+
+    stage_chunk(s_ops, ops, nops, 0);
+    __syncthreads();
+    {
+        const OpDesc& op = staged_op(s_ops, 0);
+        load_operand4<Real, C, PPT>(op.x1, !PRE && (op.kind & kX1States), pc, c, a, sa);
+        load_operand4<Real, C, PPT>(op.x2, op.kind & kX2States, pc, c, b, sb);
+    }
+    for (int i = 0; i < nops; ++i) {
+        if (i % kOpChunk == 0) {
+            // chunk i / kOpChunk is staged; stage the next one into the other half
+            // (its previous contents, chunk i / kOpChunk - 1, are no longer read).
+            __syncthreads();
+            stage_chunk(s_ops, ops, nops, i / kOpChunk + 1);
+            __syncthreads();
+        }
+        const OpDesc& op = staged_op(s_ops, i);
+        const bool sta = !PRE && (op.kind & kX1States), stb = op.kind & kX2States;
+        // Operands forwarded from op i-1's result.
+        if (src_a == 1) a = hist;
+        if (src_b == 1) b = hist;
+        // Prefetch op i+1's operands.
+        Rows4<Real, PPT> na, nb;
+        int nsa[PPT] = {}, nsb[PPT] = {};
+        int nsrc_a = 0, nsrc_b = 0;
+        if (i + 1 < nops) {
+            const OpDesc& nx = staged_op(s_ops, i + 1);
+            const bool nsta = !PRE && (nx.kind & kX1States), nstb = nx.kind & kX2States;
+            nsrc_a = operand_source(nx.x1, nsta, op.dest, prev_dest);
+            nsrc_b = operand_source(nx.x2, nstb, op.dest, prev_dest);
+            if (nsrc_a == 0) load_operand4<Real, C, PPT>(nx.x1, nsta, pc, c, na, nsa);
+            else if (nsrc_a == 2) na = hist;
+            if (nsrc_b == 0) load_operand4<Real, C, PPT>(nx.x2, nstb, pc, c, nb, nsb);
+            else if (nsrc_b == 2) nb = hist;
+        }
+        // Compute op i.
+        const Real* M1 = static_cast<const Real*>(op.m1) + c * 16;
+        const Real* M2 = static_cast<const Real*>(op.m2) + c * 16;
+        Rows4<Real, PPT> res;
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) {
+            const int p = p0 + k * pstride;
+            Real out[4];
+            if (!PRE) {
+                Real y2[4];
+                operand4c(M1, sta, sa[k], a.v[k], (Real)op.pad1, out);
+                operand4c(M2, stb, sb[k], b.v[k], (Real)op.pad2, y2);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) out[q] *= y2[q];
+            } else {
+                Real z[4];
+                operand4c(M2, stb, sb[k], b.v[k], (Real)op.pad2, z);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) z[q] *= a.v[k][q];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) out[q] = 0;
+                const bool tr = op.kind & kM1Transposed;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    Real m[4];
+                    if (tr) {
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) m[j] = __ldg(M1 + j * 4 + q);
+                    } else {
+                        ldg4(M1 + q * 4, m);
+                    }
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) out[j] += m[j] * z[q];
+                }
+            }
+            finish4c<Real, C>(op, out, pc[k], p < Pp, c, PRE ? nullptr : cum, log_scalers);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) res.v[k][q] = out[q];
+        }
+        hist = res;
+        prev_dest = op.dest;
+        a = na;
+        b = nb;
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) {
+            sa[k] = nsa[k];
+            sb[k] = nsb[k];
+        }
+        src_a = nsrc_a;
+        src_b = nsrc_b;
+    }
+}
+
 // Thread-per-pattern S = 4 kernels for category counts that are not a power
 // of two (the lane-group layout above needs C | 32).
 template <typename Real, int C>
@@ -323,6 +478,8 @@ k_pre4p(const OpDesc* __restrict__ ops, int nops, int Pp, int log_scalers) {
 // autotuner, b200_instance.cpp):
 //   0      thread per pattern, all categories in registers (any C <= 8);
 //   1,2,3  thread per (pattern, category) with 1, 2 or 4 patterns per thread
+//          (C dividing 32);
+//   4,5    the software-pipelined walk with 1 or 2 patterns per thread
 //          (C dividing 32).
 // variant < 0 picks the default: the smallest patterns-per-thread whose grid
 // fits in one resident wave, thread per pattern when C does not divide 32.
@@ -365,6 +522,16 @@ cudaError_t run_pre4_ppt(const OpDesc* ops, int nops, const Dims& d, int ls, cud
     return cudaGetLastError();
 }
 
+template <typename Real, int C, int PPT, bool PRE>
+cudaError_t run_pipe4(const OpDesc* ops, int nops, const Dims& d, double* cum, int ls,
+                      cudaStream_t s) {
+    const int ppb = kT4 / C * PPT;
+    const int grid = (d.Pp + ppb - 1) / ppb;
+    k_walk4_pipe<Real, C, PPT, PRE><<<grid, kT4, 2 * kOpChunk * sizeof(OpDesc), s>>>(
+        ops, nops, d.Pp, cum, ls);
+    return cudaGetLastError();
+}
+
 template <typename Real, int C>
 cudaError_t run_post4(const OpDesc* ops, int nops, const Dims& d, double* cum, int ls,
                       cudaStream_t s, int variant) {
@@ -372,6 +539,8 @@ cudaError_t run_post4(const OpDesc* ops, int nops, const Dims& d, double* cum, i
     if (variant > 0 && 32 % C == 0) {
         constexpr int CC = (32 % C == 0 ? C : 1);
         switch (variant) {
+            case 4: return run_pipe4<Real, CC, 1, false>(ops, nops, d, cum, ls, s);
+            case 5: return run_pipe4<Real, CC, 2, false>(ops, nops, d, cum, ls, s);
             case 1: return run_post4_ppt<Real, CC, 1>(ops, nops, d, cum, ls, s);
             case 2: return run_post4_ppt<Real, CC, 2>(ops, nops, d, cum, ls, s);
             default: return run_post4_ppt<Real, CC, 4>(ops, nops, d, cum, ls, s);
@@ -388,6 +557,8 @@ cudaError_t run_pre4(const OpDesc* ops, int nops, const Dims& d, int ls, cudaStr
     if (variant > 0 && 32 % C == 0) {
         constexpr int CC = (32 % C == 0 ? C : 1);
         switch (variant) {
+            case 4: return run_pipe4<Real, CC, 1, true>(ops, nops, d, nullptr, ls, s);
+            case 5: return run_pipe4<Real, CC, 2, true>(ops, nops, d, nullptr, ls, s);
             case 1: return run_pre4_ppt<Real, CC, 1>(ops, nops, d, ls, s);
             case 2: return run_pre4_ppt<Real, CC, 2>(ops, nops, d, ls, s);
             default: return run_pre4_ppt<Real, CC, 4>(ops, nops, d, ls, s);
@@ -399,7 +570,7 @@ cudaError_t run_pre4(const OpDesc* ops, int nops, const Dims& d, int ls, cudaStr
 
 }  // namespace
 
-int s4_walk_variants(int C) { return (32 % C == 0) ? 4 : 1; }
+int s4_walk_variants(int C) { return (32 % C == 0) ? 6 : 1; }
 
 template <typename Real>
 cudaError_t launch_update_partials(const OpDesc* ops, int nops, const Dims& d, double* cum,

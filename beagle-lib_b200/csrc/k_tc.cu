@@ -1,0 +1,794 @@
+// Partials and edge derivatives of the mixed-precision (FP32) path for
+// 4 < S <= 64 on the fifth-generation tensor cores (tcgen05, kind::tf32).
+//
+// Every post-order child, the pre-order sibling and the derivative are the
+// same contraction per rate category c and pattern tile:
+//     Y[p][i] = sum_k X[p][k] * M[i][k]        (X: 128 patterns x K states)
+// i.e. a 128 x N x K GEMM with A = the partials tile (K-major, one pattern per
+// row) and B = the matrix rows (K-major).  The pre-order op chains a second
+// one: Z = pre_parent (.) (X_sib . P_sib^T), dest = Z . P_node, with Z written
+// back to shared memory from registers.
+//
+// Precision.  tf32 keeps 10 explicit mantissa bits, so both operands are split
+// into hi = x with the low 13 mantissa bits cleared (exactly representable)
+// and lo = x - hi (exact in FP32), and each K-step issues three MMAs into the
+// same FP32 accumulator: hi*hi + hi*lo + lo*hi.  The dropped lo*lo term and
+// the tf32 rounding of lo are below 2^-20 relative, the accuracy class of the
+// FP32 CUDA-core kernels (k_generic.cu) this path replaces.
+//
+// Work decomposition (as in k_generic.cu): a thread-block cluster owns one
+// 128-pattern tile, CTA r of the cluster owns rate category r, every CTA
+// walks the whole op list for its (tile, category), and the rescaling maximum
+// over categories (CPU/BeagleCPUImpl.hpp:4008-4056) is exchanged through
+// distributed shared memory.  A CTA has 128 threads: thread t owns pattern row
+// t, which is TMEM lane t of every accumulator.
+//
+// Per contraction, K is processed in chunks of KC (<= 32) states: the CTA's
+// threads load the A rows and the B rows of the chunk from global memory,
+// split them and store both halves in the canonical no-swizzle K-major layout
+// (8-row x 16-byte core matrices, LBO = 128 B between the two 16-byte K halves
+// of an MMA step, SBO = KC * 32 B between 8-row groups); thread 0 issues the
+// MMAs and commits them to an mbarrier, whose completion frees the chunk's
+// shared memory for the next one.  Loads of other CTAs on the SM overlap the
+// MMAs (up to 4 CTAs per SM).
+//
+// TMEM: a CTA allocates 2 N (post / pre) or N (derivative) columns, rounded up
+// to a power of two.  The launch reserves enough shared memory per CTA that
+// the CTAs resident on one SM can never ask for more than the 512 columns an
+// SM has, so an allocation never waits on another cluster's CTA.
+//
+// Every wait on an mbarrier is bounded (about a second); on time-out the
+// thread sets b200_tc_status, stops waiting for the rest of the launch, keeps
+// to the same barrier sequence as its cluster and frees its TMEM at the end.
+#include <cooperative_groups.h>
+
+#include "b200_kernels.h"
+#include "b200_vec.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace b200 {
+
+__device__ int b200_tc_status;   // nonzero: a tensor-core kernel gave up waiting
+
+namespace {
+
+constexpr int kTM = 128;                    // patterns per tile = MMA M = TMEM lanes
+constexpr int kTT = 128;                    // threads per CTA
+constexpr long long kWaitCycles = 2000000000LL;
+
+// ------------------------------------------------------------ PTX wrappers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for phase `parity` of `bar`.  After one time-out the thread
+// stops waiting (`failed` stays set) and the status flag tells the host.
+__device__ __forceinline__ void mbar_wait(uint64_t* bar, uint32_t parity, bool& failed) {
+    if (failed) return;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (clock64() - t0 > kWaitCycles) {
+            failed = true;
+            atomicExch(&b200_tc_status, 1);
+            return;
+        }
+    }
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(dst)),
+                 "r"(ncols)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish() {
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// Generic-proxy shared-memory writes -> visible to the tensor core's reads.
+__device__ __forceinline__ void fence_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc,
+                                         uint32_t idesc, uint32_t accumulate) {
+    const uint32_t mask0 = 0, mask1 = 0, mask2 = 0, mask3 = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(mask0),
+        "r"(mask1), "r"(mask2), "r"(mask3)
+        : "memory");
+}
+
+// Arrive once on `bar` when every MMA this thread issued so far has completed.
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+            smem_u32(bar))
+        : "memory");
+}
+
+// 16 consecutive FP32 columns of this thread's TMEM lane (the warp's 32
+// lanes start at `taddr`); the wait is inside the same asm statement, so the
+// registers are complete when it returns.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Shared-memory matrix descriptor, no swizzle, K-major (sm100 version 1).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+// Instruction descriptor: FP32 accumulator, tf32 A and B, both K-major.
+__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void split_tf32(float x, float& hi, float& lo) {
+    hi = __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
+    lo = x - hi;
+}
+
+// ------------------------------------------------------------- geometry
+// N (output states) padded to 16, K (input states) padded to 8, or to 16 when
+// it is split into two chunks; KC = states per K chunk (<= 32).
+template <int NP>
+struct TcGeo {
+    static constexpr int TCOLS = 2 * NP <= 32 ? 32 : 2 * NP <= 64 ? 64 : 128;   // post / pre
+    static constexpr int DCOLS = NP <= 32 ? 32 : 64;                           // derivative
+};
+
+// K chunking of a state count: K padded to 8 (one chunk) or, above 32
+// states, to 16 and split into two chunks of KC = K / 2 = NP / 2 (the
+// (NP, KC) pairs of B200_TC_DISPATCH below).
+template <int NP>
+__host__ __device__ constexpr int chunks_of() { return NP >= 48 ? 2 : 1; }
+
+// Shared memory of one CTA (floats unless noted):
+//   A_hi, A_lo [kTM * 32]   B_hi, B_lo [64 * 32]   smax [kTM]
+//   nd [kTM * 2] doubles, red [kTT * 2] doubles, mbarrier, TMEM address.
+struct TcSmem {
+    float a_hi[kTM * 32];
+    float a_lo[kTM * 32];
+    float b_hi[64 * 32];
+    float b_lo[64 * 32];
+    float smax[kTM];
+    double nd[kTM * 2];
+    double red[kTT * 2];
+    uint64_t bar;
+    uint32_t tmem;
+};
+
+// A K chunk of a contraction is an NROWS x KC block (128 pattern rows of A,
+// NP matrix rows of B) stored as hi / lo halves in the canonical layout.  Lane
+// l of warp w handles rows 8 w + (l & 7) + 32 gi (gi = 0 .. NROWS / 32 - 1) and
+// sixteen-byte columns 4 h + (l >> 3): a store phase of 8 lanes covers the 8
+// rows of one core matrix (conflict-free), a warp reads 8 rows x 64 contiguous
+// bytes per load, and all offsets but one base per lane are compile-time.
+// A has at most 8 pieces per lane (128 rows, KC <= 32), B at most 4 (NP <= 64).
+template <int NROWS, int KC>
+struct Pieces {
+    static constexpr int NKC = KC / 4;               // sixteen-byte columns
+    static constexpr int NH = (NKC + 3) / 4;         // column groups of 4
+    static constexpr int NG = (NROWS / 8 + 3) / 4;   // row groups per warp
+};
+
+// This lane's pieces of chunk [k0, k0 + KC) of a row-major source (row r at
+// src + r * rstride; rows >= nvalid and columns >= Sg are zero), all loads
+// issued before any is used.
+template <int NROWS, int KC, bool RO>
+__device__ __forceinline__ void gather(float v[][4], const float* src, size_t rstride, int nvalid,
+                                       int k0, int Sg) {
+    using PC = Pieces<NROWS, KC>;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r0 = warp * 8 + (lane & 7), c0 = lane >> 3;
+    const float* base = src + (size_t)r0 * rstride + k0 + 4 * c0;
+#pragma unroll
+    for (int gi = 0; gi < PC::NG; ++gi)
+#pragma unroll
+        for (int h = 0; h < PC::NH; ++h) {
+            float* d = v[gi * PC::NH + h];
+            d[0] = d[1] = d[2] = d[3] = 0.f;
+            const int r = r0 + 32 * gi, kc = 4 * h + c0;
+            if (warp + 4 * gi < NROWS / 8 && kc < PC::NKC && r < nvalid && k0 + 4 * kc < Sg) {
+                const float* g = base + (size_t)(32 * gi) * rstride + 16 * h;
+                if (RO) ldg4(g, d);
+                else ld4(g, d);
+            }
+        }
+}
+
+// Split this lane's pieces and store both halves.
+template <int NROWS, int KC>
+__device__ __forceinline__ void scatter(const float v[][4], float* hi, float* lo) {
+    using PC = Pieces<NROWS, KC>;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s0 = (warp * PC::NKC + (lane >> 3)) * 32 + (lane & 7) * 4;
+#pragma unroll
+    for (int gi = 0; gi < PC::NG; ++gi)
+#pragma unroll
+        for (int h = 0; h < PC::NH; ++h) {
+            if (warp + 4 * gi >= NROWS / 8 || 4 * h + (lane >> 3) >= PC::NKC) continue;
+            const float* v4 = v[gi * PC::NH + h];
+            float h4[4], l4[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) split_tf32(v4[q], h4[q], l4[q]);
+            const int off = s0 + (4 * gi * PC::NKC + 4 * h) * 32;
+            st4(hi + off, h4);
+            st4(lo + off, l4);
+        }
+}
+
+// One K chunk in flight: this lane's pieces of A and of B.
+struct ChunkRegs {
+    float a[8][4];
+    float b[4][4];
+};
+
+// One K chunk of a contraction Y[p][i] = sum_k X[p][k] M[i][k]: A rows from
+// partials `x`, B rows from matrix `m` (row stride Sg), the accumulator at
+// TMEM column `col`, chunk index `q`.
+struct Job {
+    const float* x;
+    const float* m;
+    uint32_t col;
+    int q;
+};
+
+template <int NP, int KC>
+__device__ __forceinline__ void gather_job(ChunkRegs& cr, const Job& jb, size_t xs, int Sg) {
+    gather<kTM, KC, false>(cr.a, jb.x, xs, kTM, jb.q * KC, Sg);
+    gather<NP, KC, true>(cr.b, jb.m, Sg, Sg, jb.q * KC, Sg);
+}
+
+// Row t of A chunk Q from registers: z[Q KC .. Q KC + KC).  Compile-time
+// indices keep z in registers.
+template <int NP, int KC, int Q>
+__device__ __forceinline__ void store_row(float* hi, float* lo, const float z[NP]) {
+    constexpr int NKC = KC / 4;
+    const int t = threadIdx.x;
+    const int s0 = (t >> 3) * NKC * 32 + (t & 7) * 4;
+#pragma unroll
+    for (int kc = 0; kc < NKC; ++kc) {
+        float h4[4], l4[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int k = Q * KC + kc * 4 + q;
+            split_tf32(k < NP ? z[k < NP ? k : 0] : 0.f, h4[q], l4[q]);
+        }
+        st4(hi + s0 + kc * 32, h4);
+        st4(lo + s0 + kc * 32, l4);
+    }
+}
+
+// Issue the 3 x KC / 8 MMAs of one chunk (thread 0 only); `first` clears the
+// accumulator with the first MMA.  Completion arrives on sm.bar.
+template <int KC>
+__device__ __forceinline__ void issue_chunk(TcSmem& sm, uint32_t d_tmem, int N, bool first) {
+    const uint32_t idesc = idesc_tf32(kTM, N);
+    const uint32_t ah = smem_u32(sm.a_hi), al = smem_u32(sm.a_lo);
+    const uint32_t bh = smem_u32(sm.b_hi), bl = smem_u32(sm.b_lo);
+    constexpr uint32_t sbo = (uint32_t)KC * 32u;   // bytes between 8-row groups
+    tc_fence_after();
+#pragma unroll
+    for (int s = 0; s < KC / 8; ++s) {
+        const uint32_t o = (uint32_t)s * 256u;
+        const uint64_t dah = smem_desc(ah + o, 128, sbo), dal = smem_desc(al + o, 128, sbo);
+        const uint64_t dbh = smem_desc(bh + o, 128, sbo), dbl = smem_desc(bl + o, 128, sbo);
+        mma_tf32(d_tmem, dah, dbh, idesc, (first && s == 0) ? 0u : 1u);
+        mma_tf32(d_tmem, dah, dbl, idesc, 1u);
+        mma_tf32(d_tmem, dal, dbh, idesc, 1u);
+    }
+    mma_commit(&sm.bar);
+}
+
+// Per-CTA state of the MMA pipeline: phase of sm.bar and whether a commit is
+// outstanding (the chunk buffers are busy until it completes).
+struct Pipe {
+    uint32_t phase = 0;
+    bool pending = false;
+    bool failed = false;
+};
+
+__device__ __forceinline__ void pipe_drain(TcSmem& sm, Pipe& pp) {
+    if (pp.pending) {
+        mbar_wait(&sm.bar, pp.phase, pp.failed);
+        pp.phase ^= 1u;
+        pp.pending = false;
+    }
+}
+
+// Run up to 4 chunk jobs through the single chunk buffer: the registers of
+// job i + 1 are gathered while the MMAs of job i run.
+template <int NP, int KC>
+__device__ __forceinline__ void run_jobs(TcSmem& sm, Pipe& pp, uint32_t tmem, const Job (&jobs)[4],
+                                         int n, size_t xs, int Sg, ChunkRegs& cr) {
+    if (n > 0) gather_job<NP, KC>(cr, jobs[0], xs, Sg);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        if (i >= n) break;
+        pipe_drain(sm, pp);   // chunk buffer free
+        scatter<kTM, KC>(cr.a, sm.a_hi, sm.a_lo);
+        scatter<NP, KC>(cr.b, sm.b_hi, sm.b_lo);
+        fence_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) issue_chunk<KC>(sm, tmem + jobs[i].col, NP, jobs[i].q == 0);
+        pp.pending = true;
+        if (i + 1 < n) gather_job<NP, KC>(cr, jobs[i + 1], xs, Sg);
+    }
+}
+
+// Columns [col + 16 j, col + 16 j + 16) of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_chunk(uint32_t tmem, int col, int j, float y[16]) {
+    tmem_ld16(tmem + ((uint32_t)(threadIdx.x & ~31) << 16) + (uint32_t)(col + 16 * j), y);
+}
+
+// y[q] = M[16 j + q][s] for a compact tip state s (the pad value for the
+// missing state, zero for states >= S), read from the transposed image: row s
+// of M^T is column s of M.
+__device__ __forceinline__ void tip_chunk(const float* mt, int s, int S, int Sg, float pad, int j,
+                                          float y[16]) {
+    const bool ok = s >= 0 && s < S;
+    const float* row = mt + (size_t)(ok ? s : 0) * Sg + 16 * j;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        float v[4] = {0.f, 0.f, 0.f, 0.f};
+        if (16 * j + 4 * k < Sg) ldg4(row + 4 * k, v);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int i = 16 * j + 4 * k + q;
+            y[4 * k + q] = i < S ? (ok ? v[q] : pad) : 0.f;
+        }
+    }
+}
+
+// out[16 j + q] *= operand chunk j, for all chunks: the operand comes from
+// TMEM columns [col, col + NP) or, for a tip child, from the matrix image.
+template <int NP>
+__device__ __forceinline__ void mul_operand(float out[NP], bool states, uint32_t tmem, int col,
+                                            const float* mt, int s, int S, int Sg, float pad) {
+#pragma unroll
+    for (int j = 0; j < NP / 16; ++j) {
+        float y[16];
+        if (states) tip_chunk(mt, s, S, Sg, pad, j, y);
+        else tmem_chunk(tmem, col, j, y);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) out[16 * j + q] *= y[q];
+    }
+}
+
+// Rescale (cluster-wide maximum over categories and states < S) or fixed
+// scaling, then store row t of the tile.  Same arithmetic as finish_tile in
+// k_generic.cu.
+template <int NP>
+__device__ __forceinline__ void finish_row(TcSmem& sm, const OpDesc& op, float out[NP], int p,
+                                           int c, int C, int S, int Sg, double* cum,
+                                           int log_scalers) {
+    if (op.scale_write) {
+        float m = 0.f;
+#pragma unroll
+        for (int i = 0; i < NP; ++i)
+            if (i < S) m = out[i] > m ? out[i] : m;
+        sm.smax[threadIdx.x] = m;
+        cg::cluster_group cluster = cg::this_cluster();
+        cluster.sync();
+        m = 0.f;
+        for (int r = 0; r < C; ++r) {
+            const float u = cluster.map_shared_rank(sm.smax, r)[threadIdx.x];
+            m = u > m ? u : m;
+        }
+        cluster.sync();
+        if (m == 0.f) m = 1.f;
+        const float inv = 1.f / m;
+#pragma unroll
+        for (int i = 0; i < NP; ++i) out[i] *= inv;
+        if (c == 0) {
+            const double lm = log((double)m);
+            op.scale_write[p] = log_scalers ? lm : (double)m;
+            if (cum) cum[p] += lm;
+        }
+    } else if (op.scale_read) {
+        const float inv = 1.f / (float)op.scale_read[p];
+#pragma unroll
+        for (int i = 0; i < NP; ++i) out[i] *= inv;
+    }
+    float* d = static_cast<float*>(op.dest) + ((size_t)p * C + c) * Sg;
+#pragma unroll
+    for (int j = 0; j < NP / 4; ++j)
+        if (4 * j < Sg) st4(d + 4 * j, out + 4 * j);
+}
+
+// At least 3 resident CTAs per SM (<= 170 registers a thread): with 316-CTA
+// grids of 10k-pattern, 4-category data that keeps a launch in one wave.
+template <int NP, int KC, bool PRE>
+__global__ void __launch_bounds__(kTT, 3)
+k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double* cum,
+          int log_scalers) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    TcSmem& sm = *reinterpret_cast<TcSmem*>(smem_raw);
+    using G = TcGeo<NP>;
+    const int t = threadIdx.x;
+    const int c = blockIdx.x % C;
+    const int p0 = (blockIdx.x / C) * kTM;
+    const int p = p0 + t;
+    constexpr int NKC = chunks_of<NP>();
+    const size_t xs = (size_t)C * Sg;            // partials row stride (elements)
+    const size_t mo = (size_t)c * Sg * Sg;       // category offset in a matrix
+
+    if (t == 0) {
+        mbar_init(&sm.bar, 1);
+        mbar_init_fence();
+    }
+    if (t < 32) {
+        tmem_alloc(&sm.tmem, G::TCOLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = sm.tmem;
+    Pipe pp;
+
+    ChunkRegs cr;
+    for (int o = 0; o < nops; ++o) {
+        const OpDesc& op = ops[o];
+        const bool st1 = !PRE && (op.kind & kX1States), st2 = op.kind & kX2States;
+        const float* x1 = static_cast<const float*>(op.x1);
+        const float* x2 = static_cast<const float*>(op.x2);
+        Job jobs[4];
+        int nj = 0;
+        float out[NP];
+        if (!PRE) {
+            // child 1 -> columns [0, NP), child 2 -> [NP, 2 NP)
+            for (int q = 0; q < NKC; ++q) {
+                if (!st1) jobs[nj++] = Job{x1 + (size_t)p0 * xs + (size_t)c * Sg,
+                                           static_cast<const float*>(op.m1) + mo, 0u, q};
+            }
+            for (int q = 0; q < NKC; ++q) {
+                if (!st2) jobs[nj++] = Job{x2 + (size_t)p0 * xs + (size_t)c * Sg,
+                                           static_cast<const float*>(op.m2) + mo, (uint32_t)NP, q};
+            }
+            run_jobs<NP, KC>(sm, pp, tmem, jobs, nj, xs, Sg, cr);
+            int s1 = 0, s2 = 0;
+            if (st1) s1 = static_cast<const int*>(op.x1)[p];
+            if (st2) s2 = static_cast<const int*>(op.x2)[p];
+            pipe_drain(sm, pp);
+            tc_fence_after();
+#pragma unroll
+            for (int i = 0; i < NP; ++i) out[i] = 1.f;
+            mul_operand<NP>(out, st1, tmem, 0, static_cast<const float*>(op.m1t) + mo, s1, S, Sg,
+                            (float)op.pad1);
+            mul_operand<NP>(out, st2, tmem, NP, static_cast<const float*>(op.m2t) + mo, s2, S, Sg,
+                            (float)op.pad2);
+        } else {
+            // GEMM 1: (P_sib . x_sib) -> columns [0, NP)
+            for (int q = 0; q < NKC; ++q) {
+                if (!st2) jobs[nj++] = Job{x2 + (size_t)p0 * xs + (size_t)c * Sg,
+                                           static_cast<const float*>(op.m2) + mo, 0u, q};
+            }
+            run_jobs<NP, KC>(sm, pp, tmem, jobs, nj, xs, Sg, cr);
+            // While GEMM 1 runs: the parent row, the sibling's tip state and the
+            // first B chunk of GEMM 2 (rows of P_node^T).
+            const float* mt =
+                static_cast<const float*>((op.kind & kM1Transposed) ? op.m1 : op.m1t) + mo;
+            float par[NP];
+            {
+                const float* pr = x1 + ((size_t)p * C + c) * Sg;
+#pragma unroll
+                for (int j = 0; j < NP / 4; ++j) {
+                    par[4 * j] = par[4 * j + 1] = par[4 * j + 2] = par[4 * j + 3] = 0.f;
+                    if (4 * j < Sg) ld4(pr + 4 * j, par + 4 * j);
+                }
+            }
+            int s2 = 0;
+            if (st2) s2 = static_cast<const int*>(op.x2)[p];
+            gather<NP, KC, true>(cr.b, mt, Sg, Sg, 0, Sg);
+            pipe_drain(sm, pp);
+            tc_fence_after();
+            // z = pre_parent (.) y, in place; states >= Sg stay zero (K padding)
+            float* z = par;
+            mul_operand<NP>(z, st2, tmem, 0, static_cast<const float*>(op.m2t) + mo, s2, S, Sg,
+                            (float)op.pad2);
+            // GEMM 2: dest = z . P_node -> columns [NP, 2 NP)
+            for (int q = 0; q < NKC; ++q) {
+                pipe_drain(sm, pp);
+                if (q == 0) store_row<NP, KC, 0>(sm.a_hi, sm.a_lo, z);
+                else store_row<NP, KC, 1>(sm.a_hi, sm.a_lo, z);
+                scatter<NP, KC>(cr.b, sm.b_hi, sm.b_lo);
+                fence_async_smem();
+                tc_fence_before();
+                __syncthreads();
+                if (t == 0) issue_chunk<KC>(sm, tmem + NP, NP, q == 0);
+                pp.pending = true;
+                if (q + 1 < NKC) gather<NP, KC, true>(cr.b, mt, Sg, Sg, (q + 1) * KC, Sg);
+            }
+            pipe_drain(sm, pp);
+            tc_fence_after();
+#pragma unroll
+            for (int j = 0; j < NP / 16; ++j) tmem_chunk(tmem, NP, j, out + 16 * j);
+        }
+        finish_row<NP>(sm, op, out, p, c, C, S, Sg, PRE ? nullptr : cum, log_scalers);
+        // TMEM reads of this op done before the next op's MMAs overwrite them;
+        // this op's stores visible to the CTA before the next op's loads.
+        tc_fence_before();
+        __syncthreads();
+    }
+    pipe_drain(sm, pp);
+    tc_fence_after();
+    __syncthreads();
+    if (t < 32) tmem_dealloc(tmem, G::TCOLS);
+}
+
+// Edge derivatives: cluster = (pattern tile, branch), CTA = category (the
+// decomposition of k_deriv_x in k_generic.cu).  Y = post . D^T on the tensor
+// cores; num / den per category in FP32, combined over categories in FP64.
+template <int NP, int KC>
+__global__ void __launch_bounds__(kTT, 3)
+k_deriv_tc(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
+           const double* __restrict__ patw, int S, int Sg, int C, int P, int ntiles,
+           double* site, double* block) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    TcSmem& sm = *reinterpret_cast<TcSmem*>(smem_raw);
+    using G = TcGeo<NP>;
+    const int t = threadIdx.x;
+    const int c = blockIdx.x % C;
+    const int tile = (blockIdx.x / C) % ntiles;
+    const int b = blockIdx.x / (C * ntiles);
+    const int p0 = tile * kTM;
+    const int p = p0 + t;
+    constexpr int NKC = chunks_of<NP>();
+    const size_t xs = (size_t)C * Sg;
+    const DerivDesc& dd = desc[b];
+    const size_t mo = (size_t)c * Sg * Sg;
+    const bool states = dd.post_is_states;
+
+    if (t == 0) {
+        mbar_init(&sm.bar, 1);
+        mbar_init_fence();
+    }
+    if (t < 32) {
+        tmem_alloc(&sm.tmem, G::DCOLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = sm.tmem;
+    Pipe pp;
+
+    const float* post = static_cast<const float*>(dd.post);
+    ChunkRegs cr;
+    Job jobs[4];
+    int nj = 0;
+    for (int q = 0; q < NKC; ++q) {
+        if (!states) jobs[nj++] = Job{post + (size_t)p0 * xs + (size_t)c * Sg,
+                                      static_cast<const float*>(dd.dmat) + mo, 0u, q};
+    }
+    run_jobs<NP, KC>(sm, pp, tmem, jobs, nj, xs, Sg, cr);
+    // While the MMAs run: this row of the pre-order partials and of the
+    // post-order partials (or the tip state).
+    const float* pre = static_cast<const float*>(dd.pre) + ((size_t)p * C + c) * Sg;
+    const float* xr = post + ((size_t)p * C + c) * Sg;
+    float pv[NP], xv[NP];
+    int s = 0;
+    if (states) s = static_cast<const int*>(dd.post)[p];
+#pragma unroll
+    for (int j = 0; j < NP / 4; ++j) {
+        pv[4 * j] = pv[4 * j + 1] = pv[4 * j + 2] = pv[4 * j + 3] = 0.f;
+        xv[4 * j] = xv[4 * j + 1] = xv[4 * j + 2] = xv[4 * j + 3] = 0.f;
+        if (4 * j < Sg) {
+            ld4(pre + 4 * j, pv + 4 * j);
+            if (!states) ld4(xr + 4 * j, xv + 4 * j);
+        }
+    }
+    pipe_drain(sm, pp);
+    tc_fence_after();
+    float n = 0.f, d = 0.f;
+#pragma unroll
+    for (int j = 0; j < NP / 16; ++j) {
+        float y[16];
+        if (states) tip_chunk(static_cast<const float*>(dd.dmatt) + mo, s, S, Sg, (float)dd.dpad, j, y);
+        else tmem_chunk(tmem, 0, j, y);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int i = 16 * j + q;
+            if (i >= S) continue;
+            const float x = states ? ((s < 0 || s >= S || s == i) ? 1.f : 0.f) : xv[i];
+            n += pv[i] * y[q];
+            d += pv[i] * x;
+        }
+    }
+    const double w = catw[c];
+    sm.nd[t * 2 + 0] = w * (double)n;
+    sm.nd[t * 2 + 1] = w * (double)d;
+    cg::cluster_group cluster = cg::this_cluster();
+    cluster.sync();
+    if (c == 0) {
+        double nn = 0, dn = 0;
+        for (int r = 0; r < C; ++r) {
+            const double* rem = cluster.map_shared_rank(sm.nd, r);
+            nn += rem[t * 2 + 0];
+            dn += rem[t * 2 + 1];
+        }
+        double v1 = 0, v2 = 0;
+        if (p < P) {
+            const double dv = nn / dn;
+            if (site) site[(size_t)b * P + p] = dv;
+            v1 = dv * patw[p];
+            v2 = dv * dv * patw[p];
+        }
+        sm.red[t * 2 + 0] = v1;
+        sm.red[t * 2 + 1] = v2;
+        __syncthreads();
+        if (t == 0) {
+            double t1 = 0, t2 = 0;
+            for (int k = 0; k < kTT; ++k) {
+                t1 += sm.red[k * 2 + 0];
+                t2 += sm.red[k * 2 + 1];
+            }
+            const int nb = gridDim.x / (C * ntiles);
+            block[(size_t)b * ntiles + tile] = t1;
+            block[(size_t)(nb + b) * ntiles + tile] = t2;
+        }
+    }
+    cluster.sync();   // remote reads done before any CTA of the cluster exits
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (t < 32) tmem_dealloc(tmem, G::DCOLS);
+}
+
+// Dynamic shared memory of a launch: the struct, raised so that at most
+// 512 / cols CTAs fit on one SM (228 KB per SM, 1 KB reserved per CTA).
+size_t tc_smem(int cols) {
+    const size_t need = sizeof(TcSmem) + 1024;   // + alignment slack
+    const int max_ctas = 512 / cols;
+    const size_t floor_bytes = 233472 / (max_ctas + 1) + 1;
+    return need > floor_bytes ? need : floor_bytes;
+}
+
+template <typename K, typename... Args>
+cudaError_t launch_tc(K kernel, int grid, size_t smem, int cluster, int cols, cudaStream_t s,
+                      Args... args) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTT, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm * cols > 512) return cudaErrorInvalidConfiguration;   // TMEM could be oversubscribed
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid, 1, 1);
+    cfg.blockDim = dim3(kTT, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+template <int NP, int KC>
+cudaError_t run_walk_tc(const OpDesc* ops, int nops, bool pre, const Dims& d, double* cum,
+                        int ls, cudaStream_t s) {
+    const int cols = TcGeo<NP>::TCOLS;
+    const int grid = (d.Pp / kTM) * d.C;
+    return pre ? launch_tc(k_walk_tc<NP, KC, true>, grid, tc_smem(cols), d.C, cols, s, ops, nops,
+                           d.S, d.Sg, d.C, (double*)nullptr, ls)
+               : launch_tc(k_walk_tc<NP, KC, false>, grid, tc_smem(cols), d.C, cols, s, ops,
+                           nops, d.S, d.Sg, d.C, cum, ls);
+}
+
+template <int NP, int KC>
+cudaError_t run_deriv_tc(const DerivDesc* desc, int nb, const double* catw, const double* patw,
+                         const Dims& d, double* site, double* block, cudaStream_t s) {
+    const int cols = TcGeo<NP>::DCOLS;
+    const int ntiles = d.Pp / kTM;
+    return launch_tc(k_deriv_tc<NP, KC>, ntiles * d.C * nb, tc_smem(cols), d.C, cols, s, desc,
+                     catw, patw, d.S, d.Sg, d.C, d.P, ntiles, site, block);
+}
+
+// (N, KC) of a padded state count: N = Sg rounded up to 16, KC as above.
+#define B200_TC_DISPATCH(Sg, CALL)                                         \
+    ((Sg) <= 8    ? CALL(16, 8)                                            \
+     : (Sg) <= 16 ? CALL(16, 16)                                           \
+     : (Sg) <= 24 ? CALL(32, 24)                                           \
+     : (Sg) <= 32 ? CALL(32, 32)                                           \
+     : (Sg) <= 48 ? CALL(48, 24)                                           \
+                  : CALL(64, 32))
+
+}  // namespace
+
+bool tc_supported(const Dims& d) {
+    return d.S > 4 && d.Sg <= 64 && d.C >= 1 && d.C <= 8 && d.Pp % kTM == 0;
+}
+
+int tc_tile_patterns() { return kTM; }
+
+cudaError_t launch_opwalk_tc(const OpDesc* ops, int nops, bool pre, const Dims& d, double* cum,
+                             int ls, cudaStream_t s) {
+    if (nops == 0) return cudaSuccess;
+    if (!tc_supported(d)) return cudaErrorInvalidValue;
+#define WALK_(NP, KC) run_walk_tc<NP, KC>(ops, nops, pre, d, cum, ls, s)
+    return B200_TC_DISPATCH(d.Sg, WALK_);
+#undef WALK_
+}
+
+cudaError_t launch_deriv_tc(const DerivDesc* desc, int nb, const double* catw,
+                            const double* patw, const Dims& d, double* site, double* block,
+                            cudaStream_t s) {
+    if (nb == 0) return cudaSuccess;
+    if (!tc_supported(d)) return cudaErrorInvalidValue;
+#define DER_(NP, KC) run_deriv_tc<NP, KC>(desc, nb, catw, patw, d, site, block, s)
+    return B200_TC_DISPATCH(d.Sg, DER_);
+#undef DER_
+}
+
+cudaError_t tc_status_async(int* pinned_dst, cudaStream_t s) {
+    return cudaMemcpyFromSymbolAsync(pinned_dst, b200_tc_status, sizeof(int), 0,
+                                     cudaMemcpyDeviceToHost, s);
+}
+
+cudaError_t tc_clear_status(cudaStream_t s) {
+    static const int zero = 0;
+    cudaError_t e = cudaMemcpyToSymbolAsync(b200_tc_status, &zero, sizeof(int), 0,
+                                            cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(s);
+}
+
+}  // namespace b200
