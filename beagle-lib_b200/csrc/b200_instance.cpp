@@ -583,6 +583,7 @@ int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative,
     if (cumulative != -1 && (cumulative < 0 || cumulative >= nscale_)) return kErrRange;
     std::vector<OpDesc> tab(count);
     std::vector<uint8_t> dep(count, 0);
+    bool has_op_cum = false;
     // Buffers written earlier in this list count as holding data.
     std::vector<char> written(nbuf_, 0);
     // A list is idempotent (may be run again by the autotuner) when no op
@@ -633,6 +634,24 @@ int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative,
         // pre-order ops when S > 4 unless PREORDER_TRANSPOSE_AUTO is set
         // (GPU/BeagleGPUImpl.hpp:787-788, 2844-2855).
         if (pre && S_ > 4 && !pre_auto_) d.kind |= kM1Transposed;
+        d.p_begin = 0;
+        d.p_end = Pp_;
+        d.cum = nullptr;
+        if (stride == 9) {
+            // Partition op (beagle.h:922-932): the partition's pattern range and
+            // its own cumulative scale buffer (CPU/BeagleCPUImpl.hpp:1527-1534).
+            const int part = op[7], pcum = op[8];
+            if (partition_start_.empty() || part < 0 ||
+                part >= (int)partition_start_.size() - 1)
+                return kErrRange;
+            if (pcum != -1 && (pcum < 0 || pcum >= nscale_)) return kErrRange;
+            d.p_begin = partition_start_[part];
+            d.p_end = partition_start_[part + 1];
+            if (pcum >= 0 && !pre) {
+                d.cum = scale(pcum);
+                has_op_cum = true;
+            }
+        }
         d.reserved = 0;
     }
     DevBuf& t = pre ? t_ops_pre_ : t_ops_post_;
@@ -656,7 +675,7 @@ int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative,
         const bool tc = !dbl_ && tc_supported(dm);
         const TuneKey key{pre ? kTuneWalkPre : kTuneWalkPost, (int)dbl_, C_ * 100 + Sg_, Pp_,
                           tune_count_class(count), device_};
-        int v = tune_pick(key, tc ? 2 : 1, idempotent && !cum, stream_, run);
+        int v = tune_pick(key, tc ? 2 : 1, idempotent && !cum && !has_op_cum, stream_, run);
         if (v < 0) v = tc ? 1 : 0;
         cudaError_t e = run(v);
         if (e == cudaErrorInvalidConfiguration && v == 1) {
@@ -668,13 +687,17 @@ int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative,
         const OpDesc* d_ops = (const OpDesc*)t.ptr;
         const Dims dm = dims();
         const int ls = (int)log_scalers_;
+        const bool ranged = stride == 9;
         auto run = [&](int v) -> cudaError_t {
-            return pre ? LAUNCH(launch_update_pre_partials, d_ops, count, dm, ls, stream_, v)
-                       : LAUNCH(launch_update_partials, d_ops, count, dm, cum, ls, stream_, v);
+            return pre ? LAUNCH(launch_update_pre_partials, d_ops, count, dm, ls, stream_, v,
+                                ranged)
+                       : LAUNCH(launch_update_partials, d_ops, count, dm, cum, ls, stream_, v,
+                                ranged);
         };
         const TuneKey key{pre ? kTuneWalkPre : kTuneWalkPost, (int)dbl_, C_, Pp_,
                           tune_count_class(count), device_};
-        const int v = tune_pick(key, s4_walk_variants(C_), idempotent && !cum, stream_, run);
+        const int v = tune_pick(key, s4_walk_variants(C_), idempotent && !cum && !has_op_cum,
+                                stream_, run);
         CK(run(v));
     }
     return kSuccess;
@@ -688,8 +711,15 @@ int Instance::updatePrePartials(const int* ops, int count, int cumulative) {
     return post_or_pre(ops, count, 7, cumulative, true);
 }
 
-int Instance::updatePartialsByPartition(const int*, int) { return kErrNoImpl; }
-int Instance::updatePrePartialsByPartition(const int*, int) { return kErrNoImpl; }
+// Partition ops (9 ints) run as one launch over the whole list, each op
+// writing only its partition's patterns (CPU/BeagleCPUImpl.hpp:1395-1434).
+int Instance::updatePartialsByPartition(const int* ops, int count) {
+    return post_or_pre(ops, count, 9, -1, false);
+}
+
+int Instance::updatePrePartialsByPartition(const int* ops, int count) {
+    return post_or_pre(ops, count, 9, -1, true);
+}
 
 // ------------------------------------------------------------ scale factors
 int Instance::accumulateScaleFactors(const int* idx, int count, int cumulative, double sign,
@@ -770,10 +800,55 @@ int Instance::calculateRootLogLikelihoods(const int* bufs, const int* cw, const 
     return std::isnan(*out) ? kErrFP : kSuccess;
 }
 
-int Instance::calculateRootLogLikelihoodsByPartition(const int*, const int*, const int*,
-                                                     const int*, const int*, int, int, double*,
-                                                     double*) {
-    return kErrNoImpl;
+// CPU/BeagleCPUImpl.hpp:2349-2388: one root per partition (count == 1), the
+// lnL of each partition over its patterns and their total.
+int Instance::calculateRootLogLikelihoodsByPartition(const int* bufs, const int* cw,
+                                                     const int* sf, const int* cum,
+                                                     const int* parts, int nparts, int count,
+                                                     double* outByPart, double* out) {
+    if (count != 1) return kErrNoImpl;
+    if (nparts < 1 || !bufs || !cw || !sf || !parts || !outByPart || !out) return kErrRange;
+    if (partition_start_.empty()) return kErrRange;
+    const int npart_defined = (int)partition_start_.size() - 1;
+    int total_blocks = 0;
+    for (int i = 0; i < nparts; ++i) {
+        const int b = bufs[i], w = cw[i], f = sf[i], c = cum ? cum[i] : -1, q = parts[i];
+        if (!buf_ok(b) || !partials_[b]) return kErrRange;
+        if (w < 0 || w >= neig_ || !catw_set_[w] || f < 0 || f >= neig_ || !freqs_set_[f])
+            return kErrRange;
+        if (c != -1 && (c < 0 || c >= nscale_)) return kErrRange;
+        if (q < 0 || q >= npart_defined) return kErrRange;
+        total_blocks += reduction_blocks(partition_start_[q + 1] - partition_start_[q]);
+    }
+    CK(scratch_.reserve(sizeof(double) * std::max(total_blocks, 1)));
+    CK(out_.reserve(sizeof(double) * std::max(nparts, 4)));
+    double* blocks = (double*)scratch_.ptr;
+    for (int i = 0; i < nparts; ++i) {
+        const int b = bufs[i], w = cw[i], f = sf[i], c = cum ? cum[i] : -1, q = parts[i];
+        const int p0 = partition_start_[q], p1 = partition_start_[q + 1];
+        CK(LAUNCH(launch_root_lnl_range, partials_[b], d_catw_ + (size_t)w * C_,
+                  d_freqs_ + (size_t)f * S_, c >= 0 ? scale(c) : nullptr, d_patw_, dims(), p0, p1,
+                  d_site_, blocks, (double*)out_.ptr + i, stream_));
+        blocks += reduction_blocks(p1 - p0);
+    }
+    if ((size_t)nparts > h_out_n_) {
+        cudaFreeHost(h_out_);
+        h_out_ = nullptr;
+        h_out_n_ = nparts;
+        CK(cudaMallocHost(&h_out_, sizeof(double) * h_out_n_));
+    }
+    CK(cudaMemcpyAsync(h_out_, out_.ptr, sizeof(double) * nparts, cudaMemcpyDeviceToHost,
+                       stream_));
+    int rc = sync();
+    if (rc) return rc;
+    double total = 0;
+    for (int i = 0; i < nparts; ++i) {
+        outByPart[i] = h_out_[i];
+        total += h_out_[i];
+    }
+    *out = total;
+    last_lnl_ = total;
+    return std::isnan(total) ? kErrFP : kSuccess;
 }
 
 int Instance::calculateEdgeDerivatives(const int* post, const int* pre, const int* dmat,

@@ -27,14 +27,17 @@ cudaError_t launch_matrix_pairs(const void* const* d_a, const void* const* d_b,
 
 // Post-order partials over an op list (S = 4), one launch for the whole list.
 // `variant` selects the kernel shape (see s4_walk_variants; < 0 = default).
+// `ranged`: some op has its own pattern range or cumulative buffer (partition
+// ops); without it the lane-group kernels skip those per-op checks.
 template <typename Real>
 cudaError_t launch_update_partials(const OpDesc* d_ops, int nops, const Dims& d,
                                    double* cumulative, int log_scalers, cudaStream_t s,
-                                   int variant = -1);
+                                   int variant = -1, bool ranged = true);
 // Pre-order partials over an op list (S = 4).
 template <typename Real>
 cudaError_t launch_update_pre_partials(const OpDesc* d_ops, int nops, const Dims& d,
-                                       int log_scalers, cudaStream_t s, int variant = -1);
+                                       int log_scalers, cudaStream_t s, int variant = -1,
+                                       bool ranged = true);
 // Number of S = 4 op-walk variants for C categories (variants 0 .. n-1).
 int s4_walk_variants(int C);
 
@@ -74,6 +77,13 @@ template <typename Real>
 cudaError_t launch_root_lnl(const void* root, const double* catw, const double* freqs,
                             const double* cumulative, const double* patw, const Dims& d,
                             double* d_site, double* d_block, double* d_out, cudaStream_t s);
+// The same over patterns [p_begin, p_end) (one partition); d_block holds
+// reduction_blocks(p_end - p_begin) doubles.
+template <typename Real>
+cudaError_t launch_root_lnl_range(const void* root, const double* catw, const double* freqs,
+                                  const double* cumulative, const double* patw, const Dims& d,
+                                  int p_begin, int p_end, double* d_site, double* d_block,
+                                  double* d_out, cudaStream_t s);
 
 // Edge log-likelihood (+ optional first / second derivative sums).
 template <typename Real>

@@ -39,7 +39,10 @@ struct OpDesc {
     const double* scale_read;   // divide by these stored factors (nullptr = none)
     double pad1;                // value of the missing-state column of M1
     double pad2;                // ... of M2
+    double* cum;                // cumulative scale buffer of this op (partition ops) or null
     int kind;                   // OpKind bits
+    int p_begin;                // only patterns [p_begin, p_end) are written: the op's
+    int p_end;                  //   partition, or [0, Pp) for a whole-instance op
     int reserved;
 };
 

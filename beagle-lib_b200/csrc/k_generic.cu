@@ -185,6 +185,7 @@ __device__ __forceinline__ void finish_tile(const OpDesc& op, Real out[4][4], in
                                             int i0, int pg, int sg, int c, int S, int Sg, int C,
                                             Real* s_red, Real* s_max, double* cum,
                                             int log_scalers) {
+    if (op.cum) cum = op.cum;
     if (op.scale_write) {
         Real m[4];
         cluster_max<Real, SPAD>(out, S, i0, pg, sg, s_red, s_max, C, m);
@@ -194,8 +195,8 @@ __device__ __forceinline__ void finish_tile(const OpDesc& op, Real out[4][4], in
             const Real inv = Real(1) / mq;
 #pragma unroll
             for (int r = 0; r < 4; ++r) out[q][r] *= inv;
-            if (c == 0 && sg == 0) {
-                const int p = p0 + pl + q;
+            const int p = p0 + pl + q;
+            if (c == 0 && sg == 0 && p >= op.p_begin && p < op.p_end) {
                 const double lm = log((double)mq);
                 op.scale_write[p] = log_scalers ? lm : (double)mq;
                 if (cum) cum[p] += lm;
@@ -212,7 +213,11 @@ __device__ __forceinline__ void finish_tile(const OpDesc& op, Real out[4][4], in
     if (i0 < Sg) {
         Real* d = static_cast<Real*>(op.dest);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) st4(d + ((size_t)(p0 + pl + q) * C + c) * Sg + i0, out[q]);
+        for (int q = 0; q < 4; ++q) {
+            const int p = p0 + pl + q;
+            if (p >= op.p_begin && p < op.p_end)
+                st4(d + ((size_t)p * C + c) * Sg + i0, out[q]);
+        }
     }
 }
 

@@ -84,9 +84,15 @@ __device__ __forceinline__ Real group_max(Real v) {
 }
 
 // Rescale / fixed-scale and store one pattern-category vector.
-template <typename Real, int C>
+// RANGED: the list has partition ops (own pattern range and cumulative
+// buffer); whole-instance lists skip those checks.
+template <typename Real, int C, bool RANGED = true>
 __device__ __forceinline__ void finish4c(const OpDesc& op, Real out[4], int p, bool valid, int c,
                                          double* cum, int log_scalers) {
+    if (RANGED) {
+        valid = valid && p >= op.p_begin && p < op.p_end;
+        if (op.cum) cum = op.cum;
+    }
     if (op.scale_write) {
         Real m = out[0];
 #pragma unroll
@@ -105,7 +111,7 @@ __device__ __forceinline__ void finish4c(const OpDesc& op, Real out[4], int p, b
     if (valid) st4(static_cast<Real*>(op.dest) + ((size_t)p * C + c) * 4, out);
 }
 
-template <typename Real, int C, int PPT>
+template <typename Real, int C, int PPT, bool RANGED>
 __global__ void __launch_bounds__(kT4)
 k_post4(const OpDesc* __restrict__ ops, int nops, int Pp, double* cum, int log_scalers) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -142,13 +148,13 @@ k_post4(const OpDesc* __restrict__ ops, int nops, int Pp, double* cum, int log_s
                 operand4c(M2, st2, s2[k], x2[k], (Real)op.pad2, y2);
 #pragma unroll
                 for (int i = 0; i < 4; ++i) y1[i] *= y2[i];
-                finish4c<Real, C>(op, y1, min(p, Pp - 1), p < Pp, c, cum, log_scalers);
+                finish4c<Real, C, RANGED>(op, y1, min(p, Pp - 1), p < Pp, c, cum, log_scalers);
             }
         }
     }
 }
 
-template <typename Real, int C, int PPT>
+template <typename Real, int C, int PPT, bool RANGED>
 __global__ void __launch_bounds__(kT4)
 k_pre4(const OpDesc* __restrict__ ops, int nops, int Pp, int log_scalers) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -197,7 +203,7 @@ k_pre4(const OpDesc* __restrict__ ops, int nops, int Pp, int log_scalers) {
 #pragma unroll
                     for (int j = 0; j < 4; ++j) out[j] += m[j] * z[i];
                 }
-                finish4c<Real, C>(op, out, min(p, Pp - 1), p < Pp, c, nullptr, log_scalers);
+                finish4c<Real, C, RANGED>(op, out, min(p, Pp - 1), p < Pp, c, nullptr, log_scalers);
             }
         }
     }
@@ -232,12 +238,15 @@ __device__ __forceinline__ void load_operand4(const void* x, bool states, const 
 }
 
 // Where op `nx`'s operand x comes from: 0 = load, 1 = result of the op being
-// computed now (`cur_dest`), 2 = result of the op before it (`prev_dest`).
+// computed now (`cur_dest`), 2 = result of the op before it (`prev_dest`).  A
+// result is forwarded only between ops that write the same pattern range
+// (partition): outside its range an op computes values it does not store.
 __device__ __forceinline__ int operand_source(const void* x, bool states, const void* cur_dest,
-                                              const void* prev_dest) {
+                                              bool cur_same, const void* prev_dest,
+                                              bool prev_same) {
     if (states) return 0;
-    if (x == cur_dest) return 1;
-    if (x == prev_dest) return 2;
+    if (x == cur_dest) return cur_same ? 1 : 0;
+    if (x == prev_dest) return prev_same ? 2 : 0;
     return 0;
 }
 
@@ -270,6 +279,7 @@ k_walk4_pipe(const OpDesc* __restrict__ ops, int nops, int Pp, double* cum, int 
     int sa[PPT] = {}, sb[PPT] = {};
     int src_a = 0, src_b = 0;          // 1: take the operand from `hist` (op i-1's result)
     const void* prev_dest = nullptr;
+    int prev_b = 0, prev_e = 0;        // pattern range of op i-1
 
     stage_chunk(s_ops, ops, nops, 0);
     __syncthreads();
@@ -298,8 +308,10 @@ k_walk4_pipe(const OpDesc* __restrict__ ops, int nops, int Pp, double* cum, int 
         if (i + 1 < nops) {
             const OpDesc& nx = staged_op(s_ops, i + 1);
             const bool nsta = !PRE && (nx.kind & kX1States), nstb = nx.kind & kX2States;
-            nsrc_a = operand_source(nx.x1, nsta, op.dest, prev_dest);
-            nsrc_b = operand_source(nx.x2, nstb, op.dest, prev_dest);
+            const bool cur_same = nx.p_begin == op.p_begin && nx.p_end == op.p_end;
+            const bool prev_same = nx.p_begin == prev_b && nx.p_end == prev_e;
+            nsrc_a = operand_source(nx.x1, nsta, op.dest, cur_same, prev_dest, prev_same);
+            nsrc_b = operand_source(nx.x2, nstb, op.dest, cur_same, prev_dest, prev_same);
             if (nsrc_a == 0) load_operand4<Real, C, PPT>(nx.x1, nsta, pc, c, na, nsa);
             else if (nsrc_a == 2) na = hist;
             if (nsrc_b == 0) load_operand4<Real, C, PPT>(nx.x2, nstb, pc, c, nb, nsb);
@@ -346,6 +358,8 @@ k_walk4_pipe(const OpDesc* __restrict__ ops, int nops, int Pp, double* cum, int 
         }
         hist = res;
         prev_dest = op.dest;
+        prev_b = op.p_begin;
+        prev_e = op.p_end;
         a = na;
         b = nb;
 #pragma unroll
@@ -390,6 +404,8 @@ __device__ __forceinline__ void operand4(const void* x, bool states, const Real*
 template <typename Real, int C>
 __device__ __forceinline__ void finish4(const OpDesc& op, Real out[C][4], int p,
                                         double* cum, int log_scalers) {
+    if (p < op.p_begin || p >= op.p_end) return;
+    if (op.cum) cum = op.cum;
     if (op.scale_write) {
         Real m = 0;
 #pragma unroll
@@ -497,28 +513,33 @@ template <typename Real, int C>
 int default_variant(int Pp, bool pre) {
     if (32 % C != 0) return 0;
     constexpr int CC = (32 % C == 0 ? C : 1);
-    static const long p1 = wave_patterns(k_post4<Real, CC, 1>, CC, 1);
-    static const long p2 = wave_patterns(k_post4<Real, CC, 2>, CC, 2);
-    static const long q1 = wave_patterns(k_pre4<Real, CC, 1>, CC, 1);
-    static const long q2 = wave_patterns(k_pre4<Real, CC, 2>, CC, 2);
+    static const long p1 = wave_patterns(k_post4<Real, CC, 1, false>, CC, 1);
+    static const long p2 = wave_patterns(k_post4<Real, CC, 2, false>, CC, 2);
+    static const long q1 = wave_patterns(k_pre4<Real, CC, 1, false>, CC, 1);
+    static const long q2 = wave_patterns(k_pre4<Real, CC, 2, false>, CC, 2);
     const long w1 = pre ? q1 : p1, w2 = pre ? q2 : p2;
     return Pp <= w1 ? 1 : Pp <= w2 ? 2 : 3;
 }
 
 template <typename Real, int C, int PPT>
 cudaError_t run_post4_ppt(const OpDesc* ops, int nops, const Dims& d, double* cum, int ls,
-                          cudaStream_t s) {
+                          cudaStream_t s, bool ranged) {
     const int ppb = kT4 / C * PPT;
     const int grid = (d.Pp + ppb - 1) / ppb;
-    k_post4<Real, C, PPT><<<grid, kT4, kOpChunk * sizeof(OpDesc), s>>>(ops, nops, d.Pp, cum, ls);
+    const size_t sm = kOpChunk * sizeof(OpDesc);
+    if (ranged) k_post4<Real, C, PPT, true><<<grid, kT4, sm, s>>>(ops, nops, d.Pp, cum, ls);
+    else k_post4<Real, C, PPT, false><<<grid, kT4, sm, s>>>(ops, nops, d.Pp, cum, ls);
     return cudaGetLastError();
 }
 
 template <typename Real, int C, int PPT>
-cudaError_t run_pre4_ppt(const OpDesc* ops, int nops, const Dims& d, int ls, cudaStream_t s) {
+cudaError_t run_pre4_ppt(const OpDesc* ops, int nops, const Dims& d, int ls, cudaStream_t s,
+                         bool ranged) {
     const int ppb = kT4 / C * PPT;
     const int grid = (d.Pp + ppb - 1) / ppb;
-    k_pre4<Real, C, PPT><<<grid, kT4, kOpChunk * sizeof(OpDesc), s>>>(ops, nops, d.Pp, ls);
+    const size_t sm = kOpChunk * sizeof(OpDesc);
+    if (ranged) k_pre4<Real, C, PPT, true><<<grid, kT4, sm, s>>>(ops, nops, d.Pp, ls);
+    else k_pre4<Real, C, PPT, false><<<grid, kT4, sm, s>>>(ops, nops, d.Pp, ls);
     return cudaGetLastError();
 }
 
@@ -534,16 +555,16 @@ cudaError_t run_pipe4(const OpDesc* ops, int nops, const Dims& d, double* cum, i
 
 template <typename Real, int C>
 cudaError_t run_post4(const OpDesc* ops, int nops, const Dims& d, double* cum, int ls,
-                      cudaStream_t s, int variant) {
+                      cudaStream_t s, int variant, bool ranged) {
     if (variant < 0) variant = default_variant<Real, C>(d.Pp, false);
     if (variant > 0 && 32 % C == 0) {
         constexpr int CC = (32 % C == 0 ? C : 1);
         switch (variant) {
             case 4: return run_pipe4<Real, CC, 1, false>(ops, nops, d, cum, ls, s);
             case 5: return run_pipe4<Real, CC, 2, false>(ops, nops, d, cum, ls, s);
-            case 1: return run_post4_ppt<Real, CC, 1>(ops, nops, d, cum, ls, s);
-            case 2: return run_post4_ppt<Real, CC, 2>(ops, nops, d, cum, ls, s);
-            default: return run_post4_ppt<Real, CC, 4>(ops, nops, d, cum, ls, s);
+            case 1: return run_post4_ppt<Real, CC, 1>(ops, nops, d, cum, ls, s, ranged);
+            case 2: return run_post4_ppt<Real, CC, 2>(ops, nops, d, cum, ls, s, ranged);
+            default: return run_post4_ppt<Real, CC, 4>(ops, nops, d, cum, ls, s, ranged);
         }
     }
     k_post4p<Real, C><<<(d.Pp + 127) / 128, 128, 0, s>>>(ops, nops, d.Pp, cum, ls);
@@ -552,16 +573,16 @@ cudaError_t run_post4(const OpDesc* ops, int nops, const Dims& d, double* cum, i
 
 template <typename Real, int C>
 cudaError_t run_pre4(const OpDesc* ops, int nops, const Dims& d, int ls, cudaStream_t s,
-                     int variant) {
+                     int variant, bool ranged) {
     if (variant < 0) variant = default_variant<Real, C>(d.Pp, true);
     if (variant > 0 && 32 % C == 0) {
         constexpr int CC = (32 % C == 0 ? C : 1);
         switch (variant) {
             case 4: return run_pipe4<Real, CC, 1, true>(ops, nops, d, nullptr, ls, s);
             case 5: return run_pipe4<Real, CC, 2, true>(ops, nops, d, nullptr, ls, s);
-            case 1: return run_pre4_ppt<Real, CC, 1>(ops, nops, d, ls, s);
-            case 2: return run_pre4_ppt<Real, CC, 2>(ops, nops, d, ls, s);
-            default: return run_pre4_ppt<Real, CC, 4>(ops, nops, d, ls, s);
+            case 1: return run_pre4_ppt<Real, CC, 1>(ops, nops, d, ls, s, ranged);
+            case 2: return run_pre4_ppt<Real, CC, 2>(ops, nops, d, ls, s, ranged);
+            default: return run_pre4_ppt<Real, CC, 4>(ops, nops, d, ls, s, ranged);
         }
     }
     k_pre4p<Real, C><<<(d.Pp + 127) / 128, 128, 0, s>>>(ops, nops, d.Pp, ls);
@@ -574,18 +595,18 @@ int s4_walk_variants(int C) { return (32 % C == 0) ? 6 : 1; }
 
 template <typename Real>
 cudaError_t launch_update_partials(const OpDesc* ops, int nops, const Dims& d, double* cum,
-                                   int ls, cudaStream_t s, int variant) {
+                                   int ls, cudaStream_t s, int variant, bool ranged) {
     if (nops == 0) return cudaSuccess;
     if (d.S == 4 && d.C <= 8) {
         switch (d.C) {
-            case 1: return run_post4<Real, 1>(ops, nops, d, cum, ls, s, variant);
-            case 2: return run_post4<Real, 2>(ops, nops, d, cum, ls, s, variant);
-            case 3: return run_post4<Real, 3>(ops, nops, d, cum, ls, s, variant);
-            case 4: return run_post4<Real, 4>(ops, nops, d, cum, ls, s, variant);
-            case 5: return run_post4<Real, 5>(ops, nops, d, cum, ls, s, variant);
-            case 6: return run_post4<Real, 6>(ops, nops, d, cum, ls, s, variant);
-            case 7: return run_post4<Real, 7>(ops, nops, d, cum, ls, s, variant);
-            default: return run_post4<Real, 8>(ops, nops, d, cum, ls, s, variant);
+            case 1: return run_post4<Real, 1>(ops, nops, d, cum, ls, s, variant, ranged);
+            case 2: return run_post4<Real, 2>(ops, nops, d, cum, ls, s, variant, ranged);
+            case 3: return run_post4<Real, 3>(ops, nops, d, cum, ls, s, variant, ranged);
+            case 4: return run_post4<Real, 4>(ops, nops, d, cum, ls, s, variant, ranged);
+            case 5: return run_post4<Real, 5>(ops, nops, d, cum, ls, s, variant, ranged);
+            case 6: return run_post4<Real, 6>(ops, nops, d, cum, ls, s, variant, ranged);
+            case 7: return run_post4<Real, 7>(ops, nops, d, cum, ls, s, variant, ranged);
+            default: return run_post4<Real, 8>(ops, nops, d, cum, ls, s, variant, ranged);
         }
     }
     return cudaErrorInvalidValue;   // other state counts: k_generic.cu
@@ -593,30 +614,30 @@ cudaError_t launch_update_partials(const OpDesc* ops, int nops, const Dims& d, d
 
 template <typename Real>
 cudaError_t launch_update_pre_partials(const OpDesc* ops, int nops, const Dims& d, int ls,
-                                       cudaStream_t s, int variant) {
+                                       cudaStream_t s, int variant, bool ranged) {
     if (nops == 0) return cudaSuccess;
     if (d.S == 4 && d.C <= 8) {
         switch (d.C) {
-            case 1: return run_pre4<Real, 1>(ops, nops, d, ls, s, variant);
-            case 2: return run_pre4<Real, 2>(ops, nops, d, ls, s, variant);
-            case 3: return run_pre4<Real, 3>(ops, nops, d, ls, s, variant);
-            case 4: return run_pre4<Real, 4>(ops, nops, d, ls, s, variant);
-            case 5: return run_pre4<Real, 5>(ops, nops, d, ls, s, variant);
-            case 6: return run_pre4<Real, 6>(ops, nops, d, ls, s, variant);
-            case 7: return run_pre4<Real, 7>(ops, nops, d, ls, s, variant);
-            default: return run_pre4<Real, 8>(ops, nops, d, ls, s, variant);
+            case 1: return run_pre4<Real, 1>(ops, nops, d, ls, s, variant, ranged);
+            case 2: return run_pre4<Real, 2>(ops, nops, d, ls, s, variant, ranged);
+            case 3: return run_pre4<Real, 3>(ops, nops, d, ls, s, variant, ranged);
+            case 4: return run_pre4<Real, 4>(ops, nops, d, ls, s, variant, ranged);
+            case 5: return run_pre4<Real, 5>(ops, nops, d, ls, s, variant, ranged);
+            case 6: return run_pre4<Real, 6>(ops, nops, d, ls, s, variant, ranged);
+            case 7: return run_pre4<Real, 7>(ops, nops, d, ls, s, variant, ranged);
+            default: return run_pre4<Real, 8>(ops, nops, d, ls, s, variant, ranged);
         }
     }
     return cudaErrorInvalidValue;   // other state counts: k_generic.cu
 }
 
 template cudaError_t launch_update_partials<float>(const OpDesc*, int, const Dims&, double*, int,
-                                                   cudaStream_t, int);
+                                                   cudaStream_t, int, bool);
 template cudaError_t launch_update_partials<double>(const OpDesc*, int, const Dims&, double*, int,
-                                                    cudaStream_t, int);
+                                                    cudaStream_t, int, bool);
 template cudaError_t launch_update_pre_partials<float>(const OpDesc*, int, const Dims&, int,
-                                                       cudaStream_t, int);
+                                                       cudaStream_t, int, bool);
 template cudaError_t launch_update_pre_partials<double>(const OpDesc*, int, const Dims&, int,
-                                                        cudaStream_t, int);
+                                                        cudaStream_t, int, bool);
 
 }  // namespace b200

@@ -63,12 +63,12 @@ template <typename Real>
 __global__ void __launch_bounds__(kRB)
 k_root_lnl(const Real* __restrict__ root, const double* __restrict__ catw,
            const double* __restrict__ freqs, const double* __restrict__ cum,
-           const double* __restrict__ patw, int S, int Sg, int C, int P, double* site,
-           double* block) {
+           const double* __restrict__ patw, int S, int Sg, int C, int p_begin, int p_end,
+           double* site, double* block) {
     __shared__ double sh[kRB / 32];
-    const int p = blockIdx.x * kRB + threadIdx.x;
+    const int p = p_begin + blockIdx.x * kRB + threadIdx.x;
     double v = 0;
-    if (p < P) {
+    if (p < p_end) {
         double l = log(integrate_site(root, catw, freqs, S, Sg, C, p));
         if (cum) l += cum[p];
         site[p] = l;
@@ -316,9 +316,19 @@ template <typename Real>
 cudaError_t launch_root_lnl(const void* root, const double* catw, const double* freqs,
                             const double* cum, const double* patw, const Dims& d,
                             double* d_site, double* d_block, double* d_out, cudaStream_t s) {
-    const int nblk = reduction_blocks(d.P);
+    return launch_root_lnl_range<Real>(root, catw, freqs, cum, patw, d, 0, d.P, d_site, d_block,
+                                       d_out, s);
+}
+
+template <typename Real>
+cudaError_t launch_root_lnl_range(const void* root, const double* catw, const double* freqs,
+                                  const double* cum, const double* patw, const Dims& d,
+                                  int p_begin, int p_end, double* d_site, double* d_block,
+                                  double* d_out, cudaStream_t s) {
+    const int nblk = reduction_blocks(p_end - p_begin);
+    if (nblk == 0) return cudaMemsetAsync(d_out, 0, sizeof(double), s);
     k_root_lnl<Real><<<nblk, kRB, 0, s>>>(static_cast<const Real*>(root), catw, freqs, cum, patw,
-                                          d.S, d.Sg, d.C, d.P, d_site, d_block);
+                                          d.S, d.Sg, d.C, p_begin, p_end, d_site, d_block);
     k_final_sum<<<1, kRB, 0, s>>>(d_block, nblk, 1, d_out);
     return cudaGetLastError();
 }
@@ -419,6 +429,10 @@ cudaError_t launch_accumulate_scale(double* cum, const double* pool, const int* 
     template cudaError_t launch_root_lnl<R>(const void*, const double*, const double*,           \
                                             const double*, const double*, const Dims&, double*,  \
                                             double*, double*, cudaStream_t);                     \
+    template cudaError_t launch_root_lnl_range<R>(const void*, const double*, const double*,     \
+                                                  const double*, const double*, const Dims&,     \
+                                                  int, int, double*, double*, double*,           \
+                                                  cudaStream_t);                                 \
     template cudaError_t launch_edge_lnl<R>(const void*, const void*, int, const void*, double,  \
                                             const void*, double, const void*, double,            \
                                             const double*, const double*, const double*,         \

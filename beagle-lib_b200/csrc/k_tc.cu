@@ -414,6 +414,8 @@ template <int NP>
 __device__ __forceinline__ void finish_row(TcSmem& sm, const OpDesc& op, float out[NP], int p,
                                            int c, int C, int S, int Sg, double* cum,
                                            int log_scalers) {
+    const bool mine = p >= op.p_begin && p < op.p_end;   // the op's pattern range
+    if (op.cum) cum = op.cum;
     if (op.scale_write) {
         float m = 0.f;
 #pragma unroll
@@ -432,7 +434,7 @@ __device__ __forceinline__ void finish_row(TcSmem& sm, const OpDesc& op, float o
         const float inv = 1.f / m;
 #pragma unroll
         for (int i = 0; i < NP; ++i) out[i] *= inv;
-        if (c == 0) {
+        if (c == 0 && mine) {
             const double lm = log((double)m);
             op.scale_write[p] = log_scalers ? lm : (double)m;
             if (cum) cum[p] += lm;
@@ -442,6 +444,7 @@ __device__ __forceinline__ void finish_row(TcSmem& sm, const OpDesc& op, float o
 #pragma unroll
         for (int i = 0; i < NP; ++i) out[i] *= inv;
     }
+    if (!mine) return;
     float* d = static_cast<float*>(op.dest) + ((size_t)p * C + c) * Sg;
 #pragma unroll
     for (int j = 0; j < NP / 4; ++j)

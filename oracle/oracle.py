@@ -234,6 +234,84 @@ class OracleInstance:
                 self._rescale(out, wsc, None)
             self.partials[dest] = out
 
+    # ---- partitions ---------------------------------------------------------
+    def setPatternPartitions(self, n, parts):
+        """CPU/BeagleCPUImpl.hpp:803-920 for contiguous, ascending partitions
+        (the reference reorders patterns otherwise): start pattern of each."""
+        parts = np.asarray(parts, dtype=np.int64)
+        assert parts[0] == 0 and np.all(np.diff(parts) >= 0) and parts[-1] == n - 1
+        self.part_start = np.searchsorted(parts, np.arange(n + 1), side='left')
+        self.part_start[n] = self.P
+
+    def _range(self, part):
+        return slice(int(self.part_start[part]), int(self.part_start[part + 1]))
+
+    def _rescale_range(self, out, rng, scale_idx, cumulative):
+        """rescalePartialsByPartition (CPU/BeagleCPUImpl.hpp:4060-4110): the
+        rescaling of _rescale restricted to the partition's patterns."""
+        mx = out.max(axis=(0, 2))
+        mx = np.where(mx == 0, 1.0, mx)
+        out *= (1.0 / mx)[None, :, None]
+        lg = np.log(mx)
+        self.scale[scale_idx][rng] = lg if self.log_scalers else mx
+        if cumulative is not None:
+            cumulative[rng] += lg
+
+    def updatePartialsByPartition(self, ops):
+        """upPartials with byPartition (CPU/BeagleCPUImpl.hpp:1497-1686): 9-int ops,
+        field 7 the partition, field 8 its cumulative scale index; only the
+        partition's patterns of dest are computed."""
+        ops = np.asarray(ops, dtype=np.int64).reshape(-1, 9)
+        for dest, wsc, rsc, c1, m1, c2, m2, part, cidx in ops:
+            rng = self._range(part)
+            out = (self._child(c1, m1) * self._child(c2, m2))[:, rng, :]
+            cum = self.scale[cidx] if cidx != OP_NONE else None
+            if wsc >= 0:
+                self._rescale_range(out, rng, wsc, cum)
+            elif rsc >= 0:
+                out *= (1.0 / self.scale[rsc][rng])[None, :, None]
+            self.partials[dest][:, rng, :] = out
+
+    def updatePrePartialsByPartition(self, ops):
+        """upPrePartials with byPartition (CPU/BeagleCPUImpl.hpp:1689-1862)."""
+        ops = np.asarray(ops, dtype=np.int64).reshape(-1, 9)
+        for dest, wsc, rsc, par, m1, sib, m2, part, cidx in ops:
+            rng = self._range(part)
+            z = (self.partials[par] * self._child(sib, m2))[:, rng, :]
+            M = self.matrices[m1][:, :, :self.S]
+            out = np.einsum('cij,cpi->cpj', M, z)
+            if wsc >= 0:
+                self._rescale_range(out, rng, wsc, None)
+            self.partials[dest][:, rng, :] = out
+
+    def resetScaleFactorsByPartition(self, idx, part):
+        """CPU/BeagleCPUImpl.hpp:2885-2900."""
+        self.scale[idx][self._range(part)] = 0.0
+
+    def accumulateScaleFactorsByPartition(self, idxs, cumulative, part):
+        """CPU/BeagleCPUImpl.hpp:2804-2828."""
+        rng = self._range(part)
+        for i in idxs:
+            s = self.scale[i][rng]
+            self.scale[cumulative][rng] += s if self.log_scalers else np.log(s)
+
+    def calculateRootLogLikelihoodsByPartition(self, bufs, cws, sfs, cums, parts):
+        """CPU/BeagleCPUImpl.hpp:2349-2388 (count 1): per partition i the lnL of
+        root bufs[i] over partition parts[i]'s patterns; and their total."""
+        if not hasattr(self, 'site_lnl') or self.site_lnl is None:
+            self.site_lnl = np.zeros(self.P)
+        byp = []
+        for buf, cw, sf, cum, part in zip(bufs, cws, sfs, cums, parts):
+            rng = self._range(part)
+            root = self.partials[buf][:, rng, :]
+            integ = np.einsum('c,cpi->pi', self.catw[cw], root)
+            site = np.log(integ @ self.freqs[sf])
+            if cum != OP_NONE:
+                site = site + self.scale[cum][rng]
+            self.site_lnl[rng] = site
+            byp.append(float(np.dot(site, self.patw[rng])))
+        return np.array(byp), float(sum(byp))
+
     # ---- scale factors -----------------------------------------------------
     def resetScaleFactors(self, idx):
         """CPU/BeagleCPUImpl.hpp:2874-2883."""

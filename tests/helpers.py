@@ -51,3 +51,54 @@ def rel(a, b):
 def grad_err(g, gref):
     g, gref = np.asarray(g), np.asarray(gref)
     return float(np.max(np.abs(g - gref)) / max(np.max(np.abs(gref)), 1e-300))
+
+
+def partitioned_args(problem, nparts):
+    """create_args with room for per-partition matrices, scale buffers and
+    cumulative buffers."""
+    args = list(problem.create_args())
+    args[6] = max(args[6], nparts * problem.B + 1)
+    args[8] = max(args[8], nparts * (problem.N - 1) + nparts)
+    return args
+
+
+def run_partitioned(inst, problem, nparts, rescale=True, pre=True):
+    """Contiguous pattern partitions, each with its own branch-length scaling
+    (matrices q * B + v), scale buffers (q * (N - 1) + v - N) and cumulative
+    buffer (nparts * (N - 1) + q): post-order partition ops in one call, the
+    per-partition root lnL, then (unscaled) pre-order partition ops in one call.
+    Returns (byPartition, total).  S > 4 GPU instances need
+    PREORDER_TRANSPOSE_AUTO (the pre-order ops carry untransposed matrices)."""
+    from importlib import import_module
+    syn = import_module("beagle-lib_b200").synthetic
+    pr = problem
+    bounds = np.linspace(0, pr.P, nparts + 1).astype(int)
+    parts = np.repeat(np.arange(nparts), np.diff(bounds)).astype(np.int32)
+    inst.setPatternPartitions(nparts, parts)
+    idx = np.arange(pr.B, dtype=np.int32)
+    for q in range(nparts):
+        inst.updateTransitionMatrices(0, q * pr.B + idx, None, None, pr.lengths * (1 + 0.3 * q))
+    cum0 = nparts * (pr.N - 1)
+    for q in range(nparts):
+        inst.resetScaleFactorsByPartition(cum0 + q, q)
+    ops = []
+    for v in syn.postorder(pr.children, pr.root):
+        c1, c2 = (int(x) for x in pr.children[v])
+        for q in range(nparts):
+            ws = q * (pr.N - 1) + (v - pr.N) if rescale else -1
+            ops.append([v, ws, -1, c1, q * pr.B + c1, c2, q * pr.B + c2, q, cum0 + q])
+    inst.updatePartialsByPartition(np.array(ops, dtype=np.int32))
+    byp, tot = inst.calculateRootLogLikelihoodsByPartition(
+        [pr.root] * nparts, [0] * nparts, [0] * nparts, [cum0 + q for q in range(nparts)],
+        list(range(nparts)))
+    if pre:
+        pr.set_root_pre(inst)
+        pops = []
+        for v in syn.preorder_nonroot(pr.children, pr.root):
+            par = int(pr.parent[v])
+            sib = int(pr.children[par, 0] if pr.children[par, 1] == v else pr.children[par, 1])
+            for q in range(nparts):
+                pops.append([pr.pre(v), -1, -1, pr.pre(par), q * pr.B + v, sib, q * pr.B + sib,
+                             q, -1])
+        inst.updatePrePartialsByPartition(np.array(pops, dtype=np.int32))
+    return np.asarray(byp), tot

@@ -189,3 +189,34 @@ def test_s4_kernel_variants(b200, syn, oracle, monkeypatch, precision, variant):
         tol = TOL[precision]
         assert rel(lnl, lo) <= tol["lnl"], (C, lnl, lo)
         assert grad_err(g, go) <= tol["grad"], (C, grad_err(g, go))
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+@pytest.mark.parametrize("S,C,variant", [(4, 4, 1), (4, 4, 4), (4, 3, 0), (20, 4, 0), (20, 4, 1)])
+def test_partitions(b200, syn, oracle, monkeypatch, precision, S, C, variant):
+    """updatePartialsByPartition / updatePrePartialsByPartition (one launch
+    each over every partition's ops) and calculateRootLogLikelihoodsByPartition
+    against the oracle, for each kernel family the partitions run on."""
+    from helpers import PRE_AUTO, SCALERS_LOG, partitioned_args, run_partitioned
+    monkeypatch.setenv("BEAGLE_B200_FORCE_VARIANT", str(variant))
+    pr = syn.make_problem(S=S, N=10, P=777, C=C, seed=90 + S + C, rescale=True)
+    args = partitioned_args(pr, 3)
+    pref, req = gpu_flags(precision, auto_transpose=True)
+    inst = b200.create(*args, preferenceFlags=pref, requirementFlags=req)
+    oi = oracle.OracleInstance(*args, flags=SCALERS_LOG)
+    res = []
+    for x in (inst, oi):
+        pr.load(x)
+        res.append(run_partitioned(x, pr, 3))
+    (b1, t1), (b2, t2) = res
+    tol = TOL[precision]["lnl"]
+    assert np.max(np.abs(b1 - b2) / np.abs(b2)) <= tol and rel(t1, t2) <= tol
+    big = 1e-9 if precision == "double" else 2e-4
+    for v in [pr.root, pr.pre(0), pr.pre(pr.N), pr.pre(pr.B - 1)]:
+        a, b = inst.getPartials(v), oi.getPartials(v)
+        assert np.max(np.abs(a - b)) <= big * np.max(np.abs(b)), v
+    cum0 = 3 * (pr.N - 1)
+    for s in [0, pr.N - 2, (pr.N - 1) + 3, cum0, cum0 + 2]:
+        a, b = inst.getScaleFactors(s), oi.getScaleFactors(s)
+        assert np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b))) <= big, s
+    inst.finalize()
