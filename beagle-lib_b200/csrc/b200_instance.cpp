@@ -195,18 +195,20 @@ int Instance::create(int tipCount, int partialsBufferCount, int compactBufferCou
                        stream_));
     h_out_n_ = 64;
     CK(cudaMallocHost(&h_out_, sizeof(double) * h_out_n_));
-    CK(cudaMallocHost(&h_tc_status_, sizeof(int)));
-    *h_tc_status_ = 0;
+    CK(cudaMallocHost(&h_tc_status_, 2 * sizeof(int)));
+    h_tc_status_[0] = h_tc_status_[1] = 0;
     return sync();
 }
 
 int Instance::sync() {
     if (tc_used_) CK(tc_status_async(h_tc_status_, stream_));
+    if (bulk_used_) CK(bulk_status_async(h_tc_status_ + 1, stream_));
     CK(cudaStreamSynchronize(stream_));
-    if (tc_used_ && *h_tc_status_) {
-        // A tensor-core kernel gave up waiting on its MMAs and computed
-        // garbage: report it instead of the results.
-        *h_tc_status_ = 0;
+    if ((tc_used_ && h_tc_status_[0]) || (bulk_used_ && h_tc_status_[1])) {
+        // A kernel gave up waiting on its tensor-core work or bulk copies and
+        // computed garbage: report it instead of the results.
+        h_tc_status_[0] = h_tc_status_[1] = 0;
+        CK(bulk_clear_status(stream_));
         CK(tc_clear_status(stream_));
         pending_.clear();
         chunk_i_ = 0;
@@ -888,6 +890,7 @@ int Instance::calculateEdgeDerivatives(const int* post, const int* pre, const in
                           (double*)scratch_.ptr, (double*)out_.ptr, stream_, v);
         };
         const TuneKey key{kTuneDeriv, (int)dbl_, C_, Pp_, tune_count_class(count), device_};
+        bulk_used_ = true;   // variant 6 may run (chosen, forced or being timed)
         CK(run(tune_pick(key, deriv4_variants(dm), true, stream_, run)));
     } else {
         const DerivDesc* d_desc = (const DerivDesc*)t_deriv_.ptr;

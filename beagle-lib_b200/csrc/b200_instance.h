@@ -116,7 +116,9 @@ private:
     long flags_ = 0;
     bool dbl_ = true, log_scalers_ = true, invevec_t_ = false, pre_auto_ = false;
     bool tc_used_ = false;                 // tensor-core kernels launched (status to check)
-    int* h_tc_status_ = nullptr;           // pinned copy of the tensor-core time-out flag
+    bool bulk_used_ = false;               // bulk-copy derivative launched (status to check)
+    int* h_tc_status_ = nullptr;           // pinned copies of the tensor-core and bulk-copy
+                                           // time-out flags
     int N_ = 0, nbuf_ = 0, S_ = 0, Sg_ = 0, P_ = 0, Pp_ = 0, C_ = 0;
     int neig_ = 0, nmat_ = 0, nscale_ = 0;
     size_t rsz_ = 8, part_bytes_ = 0, mat_bytes_ = 0;

@@ -71,6 +71,10 @@ cudaError_t launch_deriv_tc(const DerivDesc* d_desc, int nb, const double* catw,
 // the stream completes), and clear it (synchronises `s`).
 cudaError_t tc_status_async(int* pinned_dst, cudaStream_t s);
 cudaError_t tc_clear_status(cudaStream_t s);
+// The same for the bulk-copy derivative stream (k_reduce.cu); clearing does
+// not synchronise.
+cudaError_t bulk_status_async(int* pinned_dst, cudaStream_t s);
+cudaError_t bulk_clear_status(cudaStream_t s);
 
 // Root log-likelihood: site lnL into d_site[P]; the weighted total into d_out[0].
 template <typename Real>

@@ -3,6 +3,7 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -20,6 +21,22 @@ int env_int(const char* name, int fallback) {
     return std::atoi(v);
 }
 
+// BEAGLE_B200_FORCE_VARIANT: one variant for every kind ("3"), or one per
+// kind in TuneKind order ("1,1,4" = post-order walk, pre-order walk,
+// derivative); -1 or a missing entry leaves that kind to the tuner.
+int forced_variant(int kind) {
+    const char* v = std::getenv("BEAGLE_B200_FORCE_VARIANT");
+    if (!v || !*v) return -1;
+    if (!std::strchr(v, ',')) return std::atoi(v);
+    int k = 1;
+    for (const char* q = v; q && *q; ++k) {
+        if (k == kind) return std::atoi(q);
+        q = std::strchr(q, ',');
+        if (q) ++q;
+    }
+    return -1;
+}
+
 }  // namespace
 
 int tune_count_class(int n) {
@@ -34,7 +51,7 @@ int tune_count_class(int n) {
 int tune_pick(const TuneKey& k, int nvariants, bool may_time, cudaStream_t s,
               const std::function<cudaError_t(int)>& run) {
     if (nvariants <= 1) return -1;
-    const int forced = env_int("BEAGLE_B200_FORCE_VARIANT", -1);
+    const int forced = forced_variant(k.kind);
     if (forced >= 0) return forced < nvariants ? forced : nvariants - 1;
     if (env_int("BEAGLE_B200_TUNE", 1) == 0) return -1;
     const auto key = std::make_tuple(k.kind, k.dbl, k.C, k.Pp, k.count_class, k.device);

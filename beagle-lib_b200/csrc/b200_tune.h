@@ -15,6 +15,8 @@
 //   BEAGLE_B200_TUNE=0            no tuning, always the default variant;
 //   BEAGLE_B200_FORCE_VARIANT=v   always variant v (clamped to the range),
 //                                 used by the parity tests to cover each one;
+//                                 "a,b,c" pins post-order walk, pre-order walk
+//                                 and derivative separately (-1 = tune);
 //   BEAGLE_B200_TUNE_LOG=1        print each candidate's time to stderr.
 #pragma once
 #include <cuda_runtime.h>

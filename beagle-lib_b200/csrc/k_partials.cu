@@ -27,7 +27,8 @@ namespace b200 {
 
 namespace {
 
-// Rescale one pattern's C*S values in place (see the file comment).
+// Store the scale factor of one pattern (see the file comment), its log
+// taken, stored and accumulated in FP64.
 template <typename Real>
 __device__ __forceinline__ void store_scale(Real m, double* scale_write, double* cum, int p,
                                             int log_scalers) {
@@ -111,8 +112,8 @@ __device__ __forceinline__ void finish4c(const OpDesc& op, Real out[4], int p, b
     if (valid) st4(static_cast<Real*>(op.dest) + ((size_t)p * C + c) * 4, out);
 }
 
-template <typename Real, int C, int PPT, bool RANGED>
-__global__ void __launch_bounds__(kT4)
+template <typename Real, int C, int PPT, bool RANGED, int MINB = 1>
+__global__ void __launch_bounds__(kT4, MINB)
 k_post4(const OpDesc* __restrict__ ops, int nops, int Pp, double* cum, int log_scalers) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     OpDesc* s_ops = reinterpret_cast<OpDesc*>(smem_raw);
@@ -154,8 +155,8 @@ k_post4(const OpDesc* __restrict__ ops, int nops, int Pp, double* cum, int log_s
     }
 }
 
-template <typename Real, int C, int PPT, bool RANGED>
-__global__ void __launch_bounds__(kT4)
+template <typename Real, int C, int PPT, bool RANGED, int MINB = 1>
+__global__ void __launch_bounds__(kT4, MINB)
 k_pre4(const OpDesc* __restrict__ ops, int nops, int Pp, int log_scalers) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     OpDesc* s_ops = reinterpret_cast<OpDesc*>(smem_raw);
@@ -496,7 +497,12 @@ k_pre4p(const OpDesc* __restrict__ ops, int nops, int Pp, int log_scalers) {
 //   1,2,3  thread per (pattern, category) with 1, 2 or 4 patterns per thread
 //          (C dividing 32);
 //   4,5    the software-pipelined walk with 1 or 2 patterns per thread
-//          (C dividing 32).
+//          (C dividing 32);
+//   6      2 patterns per thread held to <= 42 registers (6 CTAs per SM), so
+//          about 110 k patterns of 4 categories fit one resident wave (FP32;
+//          FP64 rows need more registers and run as variant 2).
+template <typename Real>
+constexpr int kMinB6 = sizeof(Real) == 4 ? 6 : 1;
 // variant < 0 picks the default: the smallest patterns-per-thread whose grid
 // fits in one resident wave, thread per pattern when C does not divide 32.
 template <typename K>
@@ -521,25 +527,27 @@ int default_variant(int Pp, bool pre) {
     return Pp <= w1 ? 1 : Pp <= w2 ? 2 : 3;
 }
 
-template <typename Real, int C, int PPT>
+template <typename Real, int C, int PPT, int MINB = 1>
 cudaError_t run_post4_ppt(const OpDesc* ops, int nops, const Dims& d, double* cum, int ls,
                           cudaStream_t s, bool ranged) {
     const int ppb = kT4 / C * PPT;
     const int grid = (d.Pp + ppb - 1) / ppb;
     const size_t sm = kOpChunk * sizeof(OpDesc);
-    if (ranged) k_post4<Real, C, PPT, true><<<grid, kT4, sm, s>>>(ops, nops, d.Pp, cum, ls);
-    else k_post4<Real, C, PPT, false><<<grid, kT4, sm, s>>>(ops, nops, d.Pp, cum, ls);
+    if (ranged)
+        k_post4<Real, C, PPT, true, MINB><<<grid, kT4, sm, s>>>(ops, nops, d.Pp, cum, ls);
+    else
+        k_post4<Real, C, PPT, false, MINB><<<grid, kT4, sm, s>>>(ops, nops, d.Pp, cum, ls);
     return cudaGetLastError();
 }
 
-template <typename Real, int C, int PPT>
+template <typename Real, int C, int PPT, int MINB = 1>
 cudaError_t run_pre4_ppt(const OpDesc* ops, int nops, const Dims& d, int ls, cudaStream_t s,
                          bool ranged) {
     const int ppb = kT4 / C * PPT;
     const int grid = (d.Pp + ppb - 1) / ppb;
     const size_t sm = kOpChunk * sizeof(OpDesc);
-    if (ranged) k_pre4<Real, C, PPT, true><<<grid, kT4, sm, s>>>(ops, nops, d.Pp, ls);
-    else k_pre4<Real, C, PPT, false><<<grid, kT4, sm, s>>>(ops, nops, d.Pp, ls);
+    if (ranged) k_pre4<Real, C, PPT, true, MINB><<<grid, kT4, sm, s>>>(ops, nops, d.Pp, ls);
+    else k_pre4<Real, C, PPT, false, MINB><<<grid, kT4, sm, s>>>(ops, nops, d.Pp, ls);
     return cudaGetLastError();
 }
 
@@ -562,6 +570,7 @@ cudaError_t run_post4(const OpDesc* ops, int nops, const Dims& d, double* cum, i
         switch (variant) {
             case 4: return run_pipe4<Real, CC, 1, false>(ops, nops, d, cum, ls, s);
             case 5: return run_pipe4<Real, CC, 2, false>(ops, nops, d, cum, ls, s);
+            case 6: return run_post4_ppt<Real, CC, 2, kMinB6<Real>>(ops, nops, d, cum, ls, s, ranged);
             case 1: return run_post4_ppt<Real, CC, 1>(ops, nops, d, cum, ls, s, ranged);
             case 2: return run_post4_ppt<Real, CC, 2>(ops, nops, d, cum, ls, s, ranged);
             default: return run_post4_ppt<Real, CC, 4>(ops, nops, d, cum, ls, s, ranged);
@@ -580,6 +589,7 @@ cudaError_t run_pre4(const OpDesc* ops, int nops, const Dims& d, int ls, cudaStr
         switch (variant) {
             case 4: return run_pipe4<Real, CC, 1, true>(ops, nops, d, nullptr, ls, s);
             case 5: return run_pipe4<Real, CC, 2, true>(ops, nops, d, nullptr, ls, s);
+            case 6: return run_pre4_ppt<Real, CC, 2, kMinB6<Real>>(ops, nops, d, ls, s, ranged);
             case 1: return run_pre4_ppt<Real, CC, 1>(ops, nops, d, ls, s, ranged);
             case 2: return run_pre4_ppt<Real, CC, 2>(ops, nops, d, ls, s, ranged);
             default: return run_pre4_ppt<Real, CC, 4>(ops, nops, d, ls, s, ranged);
@@ -591,7 +601,7 @@ cudaError_t run_pre4(const OpDesc* ops, int nops, const Dims& d, int ls, cudaStr
 
 }  // namespace
 
-int s4_walk_variants(int C) { return (32 % C == 0) ? 6 : 1; }
+int s4_walk_variants(int C) { return (32 % C == 0) ? 7 : 1; }
 
 template <typename Real>
 cudaError_t launch_update_partials(const OpDesc* ops, int nops, const Dims& d, double* cum,

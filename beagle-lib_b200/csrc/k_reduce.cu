@@ -8,6 +8,8 @@
 
 namespace b200 {
 
+__device__ int b200_bulk_status;   // nonzero: a bulk-copy kernel gave up waiting
+
 namespace {
 
 constexpr int kRB = 128;   // reduction block size (patterns per block)
@@ -28,6 +30,20 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
     double t = 0;
     if (threadIdx.x == 0)
         for (int w = 0; w < kRB / 32; ++w) t += sh[w];
+    return t;
+}
+
+// Sum of v over a block of N threads; result valid in thread 0.
+template <int N>
+__device__ __forceinline__ double block_sum_n(double v, double* sh) {
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    double t = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < N / 32; ++w) t += sh[w];
     return t;
 }
 
@@ -217,82 +233,334 @@ k_edge_deriv(const DerivDesc* __restrict__ desc, const double* __restrict__ catw
 
 // S = 4 specialisation of k_edge_deriv: one thread per (pattern, category)
 // with 16-byte (FP32) / 32-byte (FP64) vector loads; the C threads of a
-// pattern combine their weighted terms with shuffles.  Each thread covers PPT
-// patterns kRB / C apart, so a CTA covers kRB / C * PPT patterns and pays its
-// two block reductions once for all of them; blockIdx.y = branch.  The
-// category's 4x4 derivative matrix is held in registers across the PPT
-// patterns.
+// pattern combine their weighted terms with shuffles.  A tile is kRB / C * PPT
+// patterns (each thread covers PPT patterns kRB / C apart); a CTA walks ITER
+// consecutive tiles of one branch (blockIdx.y), loading tile i + 1 while it
+// computes tile i, and pays its two block reductions once at the end.  The
+// category's 4x4 derivative matrix is held in registers throughout.
+// d = sum_c w_c num_c / sum_c w_c den_c over the C lanes of one pattern, in
+// the partials' precision (the FP64 path stays FP64); callers accumulate the
+// weighted sums of d in FP64.
+template <typename Real, int C>
+__device__ __forceinline__ Real combine_categories(Real n, Real q, Real w) {
+    Real num = w * n, den = w * q;
+#pragma unroll
+    for (int o = 1; o < C; o <<= 1) {
+        num += __shfl_xor_sync(0xffffffffu, num, o);
+        den += __shfl_xor_sync(0xffffffffu, den, o);
+    }
+    return num / den;
+}
+
+template <typename Real, int PPT>
+struct DerivRows4 {
+    Real z[PPT][4];   // pre-order partials
+    Real x[PPT][4];   // post-order partials
+    int st[PPT];      // or tip states
+};
+
 template <typename Real, int C, int PPT>
+__device__ __forceinline__ void deriv4_load(DerivRows4<Real, PPT>& r, const DerivDesc& dd,
+                                            bool states, int p0, int P, int c) {
+    constexpr int kSlots = kRB / C;
+#pragma unroll
+    for (int j = 0; j < PPT; ++j) {
+        const int pc = min(p0 + j * kSlots, P - 1);
+        ld4(static_cast<const Real*>(dd.pre) + ((size_t)pc * C + c) * 4, r.z[j]);
+        if (states)
+            r.st[j] = static_cast<const int*>(dd.post)[pc];
+        else
+            ld4(static_cast<const Real*>(dd.post) + ((size_t)pc * C + c) * 4, r.x[j]);
+    }
+}
+
+template <typename Real, int C, int ITER, int PPT>
 __global__ void __launch_bounds__(kRB)
 k_edge_deriv4(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
               const double* __restrict__ patw, int P, double* site, double* block) {
     __shared__ double sh[kRB / 32];
     constexpr int kSlots = kRB / C;
+    constexpr int kTile = kSlots * PPT;
     const int b = blockIdx.y;
     const int c = threadIdx.x % C;
-    const int p0 = blockIdx.x * (kSlots * PPT) + threadIdx.x / C;
+    const int t0 = blockIdx.x * ITER;                  // first tile of this CTA
+    const int ntiles = (P + kTile - 1) / kTile;
     const DerivDesc& dd = desc[b];
     const Real* D = static_cast<const Real*>(dd.dmat) + c * 16;
     Real dm[16];
 #pragma unroll
     for (int k = 0; k < 4; ++k) ld4(D + 4 * k, dm + 4 * k);
-    const double w = catw[c];
-    Real z[PPT][4], x[PPT][4];
-    int st[PPT];
+    const Real w = (Real)catw[c];
     const bool states = dd.post_is_states;
-#pragma unroll
-    for (int j = 0; j < PPT; ++j) {
-        const int pc = min(p0 + j * kSlots, P - 1);
-        ld4(static_cast<const Real*>(dd.pre) + ((size_t)pc * C + c) * 4, z[j]);
-        if (states)
-            st[j] = static_cast<const int*>(dd.post)[pc];
-        else
-            ld4(static_cast<const Real*>(dd.post) + ((size_t)pc * C + c) * 4, x[j]);
-    }
+    DerivRows4<Real, PPT> cur, nxt;
+    deriv4_load<Real, C, PPT>(cur, dd, states, t0 * kTile + threadIdx.x / C, P, c);
     double s1 = 0, s2 = 0;
+#pragma unroll 1
+    for (int it = 0; it < ITER; ++it) {
+        if (t0 + it >= ntiles) break;
+        const int p0 = (t0 + it) * kTile + threadIdx.x / C;
+        if (it + 1 < ITER && t0 + it + 1 < ntiles)
+            deriv4_load<Real, C, PPT>(nxt, dd, states, p0 + kTile, P, c);
 #pragma unroll
-    for (int j = 0; j < PPT; ++j) {
-        const int p = p0 + j * kSlots;
-        Real n = 0, q = 0;
-        if (states) {
-            const int s = st[j];
+        for (int j = 0; j < PPT; ++j) {
+            const int p = p0 + j * kSlots;
+            Real n = 0, q = 0;
+            if (states) {
+                const int s = cur.st[j];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                Real dk = (Real)dd.dpad;
+                for (int k = 0; k < 4; ++k) {
+                    Real dk = (Real)dd.dpad;
 #pragma unroll
-                for (int i = 0; i < 4; ++i)
-                    if (s == i) dk = dm[k * 4 + i];
-                n += z[j][k] * dk;
-                q += (s >= 4 || k == s) ? z[j][k] : Real(0);
+                    for (int i = 0; i < 4; ++i)
+                        if (s == i) dk = dm[k * 4 + i];
+                    n += cur.z[j][k] * dk;
+                    q += (s >= 4 || k == s) ? cur.z[j][k] : Real(0);
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const Real y = dm[k * 4] * cur.x[j][0] + dm[k * 4 + 1] * cur.x[j][1] +
+                                   dm[k * 4 + 2] * cur.x[j][2] + dm[k * 4 + 3] * cur.x[j][3];
+                    n += cur.z[j][k] * y;
+                    q += cur.z[j][k] * cur.x[j][k];
+                }
             }
-        } else {
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const Real y = dm[k * 4] * x[j][0] + dm[k * 4 + 1] * x[j][1] +
-                               dm[k * 4 + 2] * x[j][2] + dm[k * 4 + 3] * x[j][3];
-                n += z[j][k] * y;
-                q += z[j][k] * x[j][k];
+            const Real dr = combine_categories<Real, C>(n, q, w);
+            if (c == 0 && p < P) {
+                const double d = (double)dr;
+                if (site) site[(size_t)b * P + p] = d;
+                const double wp = patw[p];
+                s1 += d * wp;
+                s2 += d * d * wp;
             }
         }
-        double num = w * (double)n, den = w * (double)q;
-#pragma unroll
-        for (int o = 1; o < C; o <<= 1) {
-            num += __shfl_xor_sync(0xffffffffu, num, o);
-            den += __shfl_xor_sync(0xffffffffu, den, o);
-        }
-        if (c == 0 && p < P) {
-            const double d = num / den;
-            if (site) site[(size_t)b * P + p] = d;
-            const double wp = patw[p];
-            s1 += d * wp;
-            s2 += d * d * wp;
-        }
+        cur = nxt;
     }
     const int nblk = gridDim.x;
     double t = block_sum(s1, sh);
     if (threadIdx.x == 0) block[(size_t)b * nblk + blockIdx.x] = t;
     t = block_sum(s2, sh);
     if (threadIdx.x == 0) block[(size_t)(gridDim.y + b) * nblk + blockIdx.x] = t;
+}
+
+// ---------------------------------------------------- S = 4, bulk-copy stream
+// The derivative pass is a pure stream: per branch it reads the pre-order and
+// the post-order partials (or tip states) once.  This variant keeps that
+// stream in flight with bulk asynchronous copies.  One CTA per SM walks work
+// items (branch, chunk of 16 KB per operand: 256 patterns of 4 FP32
+// categories) in a fixed order; a chunk of a
+// partials buffer is contiguous in the [pattern][category][state] layout, so
+// each operand is one cp.async.bulk into a shared-memory stage, completed on
+// the stage's mbarrier.  Thread 0 keeps kBulkStages - 1 items in flight
+// ahead of the one the CTA computes.  Every item writes its own pair of block
+// partial sums (branch, chunk), so the final sums do not depend on which CTA
+// took which item.  Waits are bounded (b200_bulk_status on time-out).
+constexpr int kBulkStageBytes = 16384;   // per operand and stage
+constexpr int kBulkStages = 3;
+constexpr int kBulkThreads = 512;
+constexpr long long kBulkWaitCycles = 2000000000LL;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void bulk_bar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void bulk_expect(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// dst (shared) <- src (global), `bytes` a multiple of 16, both 16-byte aligned.
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes,
+                                          uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void bulk_wait(uint64_t* bar, uint32_t parity, bool& failed) {
+    if (failed) return;
+    const long long t0 = clock64();
+    for (;;) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(smem_addr(bar)), "r"(parity)
+            : "memory");
+        if (ok) return;
+        if (clock64() - t0 > kBulkWaitCycles) {
+            failed = true;
+            atomicExch(&b200_bulk_status, 1);
+            return;
+        }
+    }
+}
+
+// Issue the copies of work item `item` into stage `st` (thread 0 only).
+template <typename Real, int C>
+constexpr int bulk_tile() { return kBulkStageBytes / (C * 4 * (int)sizeof(Real)); }
+
+template <typename Real, int C>
+__device__ __forceinline__ void bulk_issue(const DerivDesc* desc, int item, int nchunks, int Pp,
+                                           unsigned char* stage_pre, unsigned char* stage_post,
+                                           uint64_t* bar) {
+    const int b = item / nchunks, q = item - b * nchunks;
+    const DerivDesc& dd = desc[b];
+    const int p0 = q * bulk_tile<Real, C>();
+    const int rows = min(bulk_tile<Real, C>(), Pp - p0);
+    const uint32_t row_bytes = (uint32_t)(C * 4 * sizeof(Real));
+    const uint32_t pre_bytes = rows * row_bytes;
+    const uint32_t post_bytes = dd.post_is_states ? (uint32_t)(((rows * 4) + 15) & ~15)
+                                                  : pre_bytes;
+    bulk_expect(bar, pre_bytes + post_bytes);
+    bulk_copy(stage_pre, static_cast<const unsigned char*>(dd.pre) + (size_t)p0 * row_bytes,
+              pre_bytes, bar);
+    if (dd.post_is_states)
+        bulk_copy(stage_post, static_cast<const int*>(dd.post) + p0, post_bytes, bar);
+    else
+        bulk_copy(stage_post, static_cast<const unsigned char*>(dd.post) + (size_t)p0 * row_bytes,
+                  post_bytes, bar);
+}
+
+template <typename Real, int C>
+__global__ void __launch_bounds__(kBulkThreads)
+k_edge_deriv4_bulk(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
+                   const double* __restrict__ patw, int P, int Pp, int nb, double* site,
+                   double* block) {
+    constexpr int kTile = bulk_tile<Real, C>();
+    constexpr size_t kStageBytes = kBulkStageBytes;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char* st_pre = smem_raw;                                   // [stages][kStageBytes]
+    unsigned char* st_post = smem_raw + kBulkStages * kStageBytes;      // [stages][kStageBytes]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + 2 * kBulkStages * kStageBytes);
+    __shared__ double sh[kBulkThreads / 32];
+    const int nchunks = (Pp + kTile - 1) / kTile;
+    const int nitems = nb * nchunks;
+    const int c = threadIdx.x % C;
+    constexpr int kSlots = kBulkThreads / C;          // patterns per pass over the chunk
+    constexpr int kPasses = kTile / kSlots;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kBulkStages; ++s) bulk_bar_init(&bars[s]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    // Prologue: the first kBulkStages items of this CTA.
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kBulkStages; ++s) {
+            const int item = blockIdx.x + s * gridDim.x;
+            if (item < nitems)
+                bulk_issue<Real, C>(desc, item, nchunks, Pp, st_pre + s * kStageBytes,
+                                    st_post + s * kStageBytes, &bars[s]);
+        }
+    }
+    bool failed = false;
+    uint32_t phase[kBulkStages] = {};
+    int s = 0;
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int b = item / nchunks, q = item - b * nchunks;
+        const DerivDesc& dd = desc[b];
+        bulk_wait(&bars[s], phase[s], failed);
+        phase[s] ^= 1u;
+        const Real* pre = reinterpret_cast<const Real*>(st_pre + s * kStageBytes);
+        const Real* post = reinterpret_cast<const Real*>(st_post + s * kStageBytes);
+        const int* tip = reinterpret_cast<const int*>(st_post + s * kStageBytes);
+        const bool states = dd.post_is_states;
+        const Real* D = static_cast<const Real*>(dd.dmat) + c * 16;
+        Real dm[16];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) ldg4(D + 4 * k, dm + 4 * k);
+        const Real w = (Real)catw[c];
+        double s1 = 0, s2 = 0;
+#pragma unroll
+        for (int j = 0; j < kPasses; ++j) {
+            const int r = j * kSlots + threadIdx.x / C;     // row in the chunk
+            const int p = q * kTile + r;
+            Real z[4], x[4];
+            ld4(pre + ((size_t)r * C + c) * 4, z);
+            Real n = 0, qd = 0;
+            if (states) {
+                const int st = p < Pp ? tip[r] : 4;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    Real dk = (Real)dd.dpad;
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        if (st == i) dk = dm[k * 4 + i];
+                    n += z[k] * dk;
+                    qd += (st >= 4 || k == st) ? z[k] : Real(0);
+                }
+            } else {
+                ld4(post + ((size_t)r * C + c) * 4, x);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const Real y = dm[k * 4] * x[0] + dm[k * 4 + 1] * x[1] + dm[k * 4 + 2] * x[2] +
+                                   dm[k * 4 + 3] * x[3];
+                    n += z[k] * y;
+                    qd += z[k] * x[k];
+                }
+            }
+            const Real dr = combine_categories<Real, C>(n, qd, w);
+            if (c == 0 && p < P) {
+                const double d = (double)dr;
+                if (site) site[(size_t)b * P + p] = d;
+                const double wp = patw[p];
+                s1 += d * wp;
+                s2 += d * d * wp;
+            }
+        }
+        // block_sum's barriers also mark stage s as consumed by every thread
+        double t = block_sum_n<kBulkThreads>(s1, sh);
+        if (threadIdx.x == 0) block[(size_t)b * nchunks + q] = t;
+        t = block_sum_n<kBulkThreads>(s2, sh);
+        if (threadIdx.x == 0) {
+            block[(size_t)(nb + b) * nchunks + q] = t;
+            const int next = item + kBulkStages * gridDim.x;
+            if (next < nitems && !failed) {
+                // every thread's reads of stage s are done (block_sum's barriers)
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                bulk_issue<Real, C>(desc, next, nchunks, Pp, st_pre + s * kStageBytes,
+                                    st_post + s * kStageBytes, &bars[s]);
+            }
+        }
+        s = (s + 1) % kBulkStages;
+    }
+    // After a time-out, copies may still be in flight into this CTA's shared
+    // memory: wait for them (bounded again) before the CTA exits.
+    if (failed && threadIdx.x == 0) {
+        bool again = false;
+        for (int k = 0; k < kBulkStages; ++k) bulk_wait(&bars[k], phase[k], again);
+    }
+}
+
+template <typename Real, int C>
+cudaError_t run_deriv4_bulk(const DerivDesc* desc, int nb, const double* catw,
+                            const double* patw, const Dims& d, double* site, double* block,
+                            cudaStream_t s) {
+    const size_t smem = 2 * kBulkStages * (size_t)kBulkStageBytes + kBulkStages * sizeof(uint64_t);
+    auto kern = k_edge_deriv4_bulk<Real, C>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBulkThreads, smem);
+    if (e != cudaSuccess) return e;
+    constexpr int kTile = bulk_tile<Real, C>();
+    const int nitems = nb * ((d.Pp + kTile - 1) / kTile);
+    const int slots = sms * (per_sm > 0 ? per_sm : 1);
+    const int grid = nitems < slots ? nitems : slots;
+    kern<<<grid, kBulkThreads, smem, s>>>(desc, catw, patw, d.P, d.Pp, nb, site, block);
+    return cudaGetLastError();
 }
 
 __global__ void k_accumulate_scale(double* cum, const double* __restrict__ pool,
@@ -355,23 +623,33 @@ bool deriv4_shape(const Dims& d) {
     return d.S == 4 && d.Sg == 4 && (d.C == 1 || d.C == 2 || d.C == 4 || d.C == 8);
 }
 
-// Patterns per thread of variant v of the S = 4 derivative kernel.
-int deriv4_ppt(int v) { return v <= 0 ? 1 : v == 1 ? 2 : v == 2 ? 4 : 8; }
+// Variant v of the S = 4 derivative kernel: (patterns per thread, tiles per
+// CTA) = (1,1) (2,1) (4,1) (8,1) (2,8) (4,4).
+struct Deriv4Shape {
+    int ppt, iter;
+};
+Deriv4Shape deriv4_shape_of(int v) {
+    static const Deriv4Shape kShapes[] = {{1, 1}, {2, 1}, {4, 1}, {8, 1}, {2, 8}, {4, 4}};
+    return kShapes[v < 0 ? 0 : v > 5 ? 5 : v];
+}
 
 template <typename Real, int C>
-void run_deriv4(int ppt, dim3 grid, cudaStream_t s, const DerivDesc* desc, const double* catw,
-                const double* patw, int P, double* site, double* block) {
-    switch (ppt) {
-        case 1: k_edge_deriv4<Real, C, 1><<<grid, kRB, 0, s>>>(desc, catw, patw, P, site, block); break;
-        case 2: k_edge_deriv4<Real, C, 2><<<grid, kRB, 0, s>>>(desc, catw, patw, P, site, block); break;
-        case 4: k_edge_deriv4<Real, C, 4><<<grid, kRB, 0, s>>>(desc, catw, patw, P, site, block); break;
-        default: k_edge_deriv4<Real, C, 8><<<grid, kRB, 0, s>>>(desc, catw, patw, P, site, block); break;
-    }
+void run_deriv4(Deriv4Shape sh, dim3 grid, cudaStream_t s, const DerivDesc* desc,
+                const double* catw, const double* patw, int P, double* site, double* block) {
+#define D4_(PPT, IT) k_edge_deriv4<Real, C, IT, PPT><<<grid, kRB, 0, s>>>(desc, catw, patw, P, site, block)
+    if (sh.iter == 8) D4_(2, 8);
+    else if (sh.iter == 4) D4_(4, 4);
+    else if (sh.ppt == 1) D4_(1, 1);
+    else if (sh.ppt == 2) D4_(2, 1);
+    else if (sh.ppt == 4) D4_(4, 1);
+    else D4_(8, 1);
+#undef D4_
 }
 
 }  // namespace
 
-int deriv4_variants(const Dims& d) { return deriv4_shape(d) ? 4 : 1; }
+// Variants 0-5: k_edge_deriv4 shapes (deriv4_shape_of); 6: the bulk-copy stream.
+int deriv4_variants(const Dims& d) { return deriv4_shape(d) ? 7 : 1; }
 
 template <typename Real>
 cudaError_t launch_edge_derivatives(const DerivDesc* desc, int nb, const double* catw,
@@ -380,17 +658,29 @@ cudaError_t launch_edge_derivatives(const DerivDesc* desc, int nb, const double*
                                     int variant) {
     if (nb == 0) return cudaSuccess;
     int nblk = reduction_blocks(d.P);
-    if (deriv4_shape(d)) {
+    if (deriv4_shape(d) && variant == 6) {
+        cudaError_t e;
+        int tile;
+        switch (d.C) {
+            case 1: e = run_deriv4_bulk<Real, 1>(desc, nb, catw, patw, d, d_site, d_block, s); tile = bulk_tile<Real, 1>(); break;
+            case 2: e = run_deriv4_bulk<Real, 2>(desc, nb, catw, patw, d, d_site, d_block, s); tile = bulk_tile<Real, 2>(); break;
+            case 4: e = run_deriv4_bulk<Real, 4>(desc, nb, catw, patw, d, d_site, d_block, s); tile = bulk_tile<Real, 4>(); break;
+            default: e = run_deriv4_bulk<Real, 8>(desc, nb, catw, patw, d, d_site, d_block, s); tile = bulk_tile<Real, 8>(); break;
+        }
+        if (e != cudaSuccess) return e;
+        nblk = (d.Pp + tile - 1) / tile;
+    } else if (deriv4_shape(d)) {
         if (variant < 0) variant = d.P >= 32768 ? 2 : 0;
-        const int ppt = deriv4_ppt(variant);
-        const int ppb = kRB / d.C * ppt;
-        nblk = (d.P + ppb - 1) / ppb;
+        const Deriv4Shape sh = deriv4_shape_of(variant);
+        const int tile = kRB / d.C * sh.ppt;
+        const int ntiles = (d.P + tile - 1) / tile;
+        nblk = (ntiles + sh.iter - 1) / sh.iter;
         dim3 grid(nblk, nb);
         switch (d.C) {
-            case 1: run_deriv4<Real, 1>(ppt, grid, s, desc, catw, patw, d.P, d_site, d_block); break;
-            case 2: run_deriv4<Real, 2>(ppt, grid, s, desc, catw, patw, d.P, d_site, d_block); break;
-            case 4: run_deriv4<Real, 4>(ppt, grid, s, desc, catw, patw, d.P, d_site, d_block); break;
-            default: run_deriv4<Real, 8>(ppt, grid, s, desc, catw, patw, d.P, d_site, d_block); break;
+            case 1: run_deriv4<Real, 1>(sh, grid, s, desc, catw, patw, d.P, d_site, d_block); break;
+            case 2: run_deriv4<Real, 2>(sh, grid, s, desc, catw, patw, d.P, d_site, d_block); break;
+            case 4: run_deriv4<Real, 4>(sh, grid, s, desc, catw, patw, d.P, d_site, d_block); break;
+            default: run_deriv4<Real, 8>(sh, grid, s, desc, catw, patw, d.P, d_site, d_block); break;
         }
     } else {
         dim3 grid(nblk, nb);
@@ -399,6 +689,17 @@ cudaError_t launch_edge_derivatives(const DerivDesc* desc, int nb, const double*
     }
     k_final_sum<<<2 * nb, kRB, 0, s>>>(d_block, nblk, 2 * nb, d_sums);
     return cudaGetLastError();
+}
+
+cudaError_t bulk_status_async(int* pinned_dst, cudaStream_t s) {
+    return cudaMemcpyFromSymbolAsync(pinned_dst, b200_bulk_status, sizeof(int), 0,
+                                     cudaMemcpyDeviceToHost, s);
+}
+
+cudaError_t bulk_clear_status(cudaStream_t s) {
+    static const int zero = 0;
+    return cudaMemcpyToSymbolAsync(b200_bulk_status, &zero, sizeof(int), 0,
+                                   cudaMemcpyHostToDevice, s);
 }
 
 cudaError_t launch_deriv_final(const double* d_block, int nblk, int nb, double* d_sums,

@@ -60,7 +60,9 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
-                    help="small case for ncu: 20,000 patterns, mixed path only, no JSON")
+                    help="small case for ncu: mixed path only, no JSON")
+    ap.add_argument("--profile-patterns", type=int, default=20000,
+                    help="patterns of the --profile case")
     return ap.parse_args()
 
 
@@ -307,12 +309,14 @@ def timed_e2e(torch, inst, pr, steps):
 
 
 def run_profile_case(args):
-    """The workload's tree and model on 20,000 patterns (partials larger than
-    L2), mixed path only: warm-up then `steps` queued evaluations."""
+    """The workload's tree and model on --profile-patterns patterns (default
+    20,000: partials larger than L2, a few hundred MB on the device), mixed
+    path only: warm-up then `steps` queued evaluations.  For ncu captures."""
     import torch
     pkg = importlib.import_module("beagle-lib_b200")
-    pr = pkg.synthetic.config_problem(args.workload, P=min(20000, pkg.synthetic.CONFIGS[
-        args.workload]["P"]))
+    pr = pkg.synthetic.config_problem(args.workload, P=min(args.profile_patterns,
+                                                           pkg.synthetic.CONFIGS[
+                                                               args.workload]["P"]))
     inst = make_instance(pkg.load(), pr, "single", 0)
     timed_value(torch, inst, pr, args.steps, args.warmup)
     inst.finalize()
