@@ -690,11 +690,12 @@ int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative,
         const Dims dm = dims();
         const int ls = (int)log_scalers_;
         const bool ranged = stride == 9;
+        const OpDesc* h_ops = tab.data();
         auto run = [&](int v) -> cudaError_t {
             return pre ? LAUNCH(launch_update_pre_partials, d_ops, count, dm, ls, stream_, v,
-                                ranged)
+                                ranged, h_ops)
                        : LAUNCH(launch_update_partials, d_ops, count, dm, cum, ls, stream_, v,
-                                ranged);
+                                ranged, h_ops);
         };
         const TuneKey key{pre ? kTuneWalkPre : kTuneWalkPost, (int)dbl_, C_, Pp_,
                           tune_count_class(count), device_};

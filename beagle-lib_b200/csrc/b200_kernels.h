@@ -29,15 +29,18 @@ cudaError_t launch_matrix_pairs(const void* const* d_a, const void* const* d_b,
 // `variant` selects the kernel shape (see s4_walk_variants; < 0 = default).
 // `ranged`: some op has its own pattern range or cumulative buffer (partition
 // ops); without it the lane-group kernels skip those per-op checks.
+// `h_ops`, when given, is the host copy of the list (for the variants that
+// take it as a kernel parameter).
 template <typename Real>
 cudaError_t launch_update_partials(const OpDesc* d_ops, int nops, const Dims& d,
                                    double* cumulative, int log_scalers, cudaStream_t s,
-                                   int variant = -1, bool ranged = true);
+                                   int variant = -1, bool ranged = true,
+                                   const OpDesc* h_ops = nullptr);
 // Pre-order partials over an op list (S = 4).
 template <typename Real>
 cudaError_t launch_update_pre_partials(const OpDesc* d_ops, int nops, const Dims& d,
                                        int log_scalers, cudaStream_t s, int variant = -1,
-                                       bool ranged = true);
+                                       bool ranged = true, const OpDesc* h_ops = nullptr);
 // Number of S = 4 op-walk variants for C categories (variants 0 .. n-1).
 int s4_walk_variants(int C);
 

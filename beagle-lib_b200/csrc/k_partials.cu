@@ -20,6 +20,8 @@
 // This file holds the S = 4 kernels: one thread per (pattern, category),
 // vector loads and stores of one 4-state row, lane-group shuffles for the
 // rescaling maximum.  HBM-bound.  Other state counts: k_generic.cu.
+#include <cstring>
+
 #include "b200_kernels.h"
 #include "b200_vec.cuh"
 
@@ -112,6 +114,35 @@ __device__ __forceinline__ void finish4c(const OpDesc& op, Real out[4], int p, b
     if (valid) st4(static_cast<Real*>(op.dest) + ((size_t)p * C + c) * 4, out);
 }
 
+// One post-order op for this thread's PPT patterns (p0 + k pstride).
+template <typename Real, int C, int PPT, bool RANGED>
+__device__ __forceinline__ void post4_op(const OpDesc& op, int c, int p0, int pstride, int Pp,
+                                         double* cum, int log_scalers) {
+    const bool st1 = op.kind & kX1States, st2 = op.kind & kX2States;
+    const Real* M1 = static_cast<const Real*>(op.m1) + c * 16;
+    const Real* M2 = static_cast<const Real*>(op.m2) + c * 16;
+    Real x1[PPT][4], x2[PPT][4];
+    int s1[PPT], s2[PPT];
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+        const int p = min(p0 + k * pstride, Pp - 1);
+        if (st1) s1[k] = static_cast<const int*>(op.x1)[p];
+        else ld4(static_cast<const Real*>(op.x1) + ((size_t)p * C + c) * 4, x1[k]);
+        if (st2) s2[k] = static_cast<const int*>(op.x2)[p];
+        else ld4(static_cast<const Real*>(op.x2) + ((size_t)p * C + c) * 4, x2[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+        const int p = p0 + k * pstride;
+        Real y1[4], y2[4];
+        operand4c(M1, st1, s1[k], x1[k], (Real)op.pad1, y1);
+        operand4c(M2, st2, s2[k], x2[k], (Real)op.pad2, y2);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) y1[i] *= y2[i];
+        finish4c<Real, C, RANGED>(op, y1, min(p, Pp - 1), p < Pp, c, cum, log_scalers);
+    }
+}
+
 template <typename Real, int C, int PPT, bool RANGED, int MINB = 1>
 __global__ void __launch_bounds__(kT4, MINB)
 k_post4(const OpDesc* __restrict__ ops, int nops, int Pp, double* cum, int log_scalers) {
@@ -126,32 +157,49 @@ k_post4(const OpDesc* __restrict__ ops, int nops, int Pp, double* cum, int log_s
         __syncthreads();
         stage_ops(s_ops, ops + o0, n);
         __syncthreads();
-        for (int oi = 0; oi < n; ++oi) {
-            const OpDesc& op = s_ops[oi];
-            const bool st1 = op.kind & kX1States, st2 = op.kind & kX2States;
-            const Real* M1 = static_cast<const Real*>(op.m1) + c * 16;
-            const Real* M2 = static_cast<const Real*>(op.m2) + c * 16;
-            Real x1[PPT][4], x2[PPT][4];
-            int s1[PPT], s2[PPT];
+        for (int oi = 0; oi < n; ++oi)
+            post4_op<Real, C, PPT, RANGED>(s_ops[oi], c, p0, pstride, Pp, cum, log_scalers);
+    }
+}
+
+// One pre-order op for this thread's PPT patterns.
+template <typename Real, int C, int PPT, bool RANGED>
+__device__ __forceinline__ void pre4_op(const OpDesc& op, int c, int p0, int pstride, int Pp,
+                                        int log_scalers) {
+    const bool st2 = op.kind & kX2States;
+    const bool tr = op.kind & kM1Transposed;
+    const Real* M1 = static_cast<const Real*>(op.m1) + c * 16;
+    const Real* M2 = static_cast<const Real*>(op.m2) + c * 16;
+    Real pv[PPT][4], x2[PPT][4];
+    int s2[PPT];
 #pragma unroll
-            for (int k = 0; k < PPT; ++k) {
-                const int p = min(p0 + k * pstride, Pp - 1);
-                if (st1) s1[k] = static_cast<const int*>(op.x1)[p];
-                else ld4(static_cast<const Real*>(op.x1) + ((size_t)p * C + c) * 4, x1[k]);
-                if (st2) s2[k] = static_cast<const int*>(op.x2)[p];
-                else ld4(static_cast<const Real*>(op.x2) + ((size_t)p * C + c) * 4, x2[k]);
+    for (int k = 0; k < PPT; ++k) {
+        const int p = min(p0 + k * pstride, Pp - 1);
+        ld4(static_cast<const Real*>(op.x1) + ((size_t)p * C + c) * 4, pv[k]);
+        if (st2) s2[k] = static_cast<const int*>(op.x2)[p];
+        else ld4(static_cast<const Real*>(op.x2) + ((size_t)p * C + c) * 4, x2[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+        const int p = p0 + k * pstride;
+        Real z[4];
+        operand4c(M2, st2, s2[k], x2[k], (Real)op.pad2, z);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) z[i] *= pv[k][i];
+        Real out[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            Real m[4];
+            if (tr) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) m[j] = __ldg(M1 + j * 4 + i);
+            } else {
+                ldg4(M1 + i * 4, m);
             }
 #pragma unroll
-            for (int k = 0; k < PPT; ++k) {
-                const int p = p0 + k * pstride;
-                Real y1[4], y2[4];
-                operand4c(M1, st1, s1[k], x1[k], (Real)op.pad1, y1);
-                operand4c(M2, st2, s2[k], x2[k], (Real)op.pad2, y2);
-#pragma unroll
-                for (int i = 0; i < 4; ++i) y1[i] *= y2[i];
-                finish4c<Real, C, RANGED>(op, y1, min(p, Pp - 1), p < Pp, c, cum, log_scalers);
-            }
+            for (int j = 0; j < 4; ++j) out[j] += m[j] * z[i];
         }
+        finish4c<Real, C, RANGED>(op, out, min(p, Pp - 1), p < Pp, c, nullptr, log_scalers);
     }
 }
 
@@ -169,45 +217,40 @@ k_pre4(const OpDesc* __restrict__ ops, int nops, int Pp, int log_scalers) {
         __syncthreads();
         stage_ops(s_ops, ops + o0, n);
         __syncthreads();
-        for (int oi = 0; oi < n; ++oi) {
-            const OpDesc& op = s_ops[oi];
-            const bool st2 = op.kind & kX2States;
-            const bool tr = op.kind & kM1Transposed;
-            const Real* M1 = static_cast<const Real*>(op.m1) + c * 16;
-            const Real* M2 = static_cast<const Real*>(op.m2) + c * 16;
-            Real pv[PPT][4], x2[PPT][4];
-            int s2[PPT];
-#pragma unroll
-            for (int k = 0; k < PPT; ++k) {
-                const int p = min(p0 + k * pstride, Pp - 1);
-                ld4(static_cast<const Real*>(op.x1) + ((size_t)p * C + c) * 4, pv[k]);
-                if (st2) s2[k] = static_cast<const int*>(op.x2)[p];
-                else ld4(static_cast<const Real*>(op.x2) + ((size_t)p * C + c) * 4, x2[k]);
-            }
-#pragma unroll
-            for (int k = 0; k < PPT; ++k) {
-                const int p = p0 + k * pstride;
-                Real z[4];
-                operand4c(M2, st2, s2[k], x2[k], (Real)op.pad2, z);
-#pragma unroll
-                for (int i = 0; i < 4; ++i) z[i] *= pv[k][i];
-                Real out[4] = {0, 0, 0, 0};
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    Real m[4];
-                    if (tr) {
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) m[j] = __ldg(M1 + j * 4 + i);
-                    } else {
-                        ldg4(M1 + i * 4, m);
-                    }
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) out[j] += m[j] * z[i];
-                }
-                finish4c<Real, C, RANGED>(op, out, min(p, Pp - 1), p < Pp, c, nullptr, log_scalers);
-            }
-        }
+        for (int oi = 0; oi < n; ++oi)
+            pre4_op<Real, C, PPT, RANGED>(s_ops[oi], c, p0, pstride, Pp, log_scalers);
     }
+}
+
+// The same walks with the op list passed by value as a kernel parameter (at
+// most kParamOps ops, CUDA 12.1+ on sm_70+): descriptor fields are then
+// warp-uniform constant-bank reads instead of shared-memory loads, and no
+// staging or barriers are needed between ops.
+constexpr int kParamOps = 256;
+struct OpParams {
+    OpDesc op[kParamOps];
+};
+
+template <typename Real, int C, int PPT, bool RANGED>
+__global__ void __launch_bounds__(kT4)
+k_post4c(const __grid_constant__ OpParams P, int nops, int Pp, double* cum, int log_scalers) {
+    const int c = threadIdx.x % C;
+    const int ppb = kT4 / C;
+    const int pstride = gridDim.x * ppb;
+    const int p0 = blockIdx.x * ppb + threadIdx.x / C;
+    for (int o = 0; o < nops; ++o)
+        post4_op<Real, C, PPT, RANGED>(P.op[o], c, p0, pstride, Pp, cum, log_scalers);
+}
+
+template <typename Real, int C, int PPT, bool RANGED>
+__global__ void __launch_bounds__(kT4)
+k_pre4c(const __grid_constant__ OpParams P, int nops, int Pp, int log_scalers) {
+    const int c = threadIdx.x % C;
+    const int ppb = kT4 / C;
+    const int pstride = gridDim.x * ppb;
+    const int p0 = blockIdx.x * ppb + threadIdx.x / C;
+    for (int o = 0; o < nops; ++o)
+        pre4_op<Real, C, PPT, RANGED>(P.op[o], c, p0, pstride, Pp, log_scalers);
 }
 
 // ------------------------------------------- S = 4, software-pipelined walk
@@ -503,6 +546,9 @@ k_pre4p(const OpDesc* __restrict__ ops, int nops, int Pp, int log_scalers) {
 //          FP64 rows need more registers and run as variant 2).
 template <typename Real>
 constexpr int kMinB6 = sizeof(Real) == 4 ? 6 : 1;
+//   7,8    1 or 2 patterns per thread with the op list passed by value as a
+//          kernel parameter (lists of up to kParamOps ops; otherwise the
+//          launch is refused and the tuner skips the variant).
 // variant < 0 picks the default: the smallest patterns-per-thread whose grid
 // fits in one resident wave, thread per pattern when C does not divide 32.
 template <typename K>
@@ -551,6 +597,24 @@ cudaError_t run_pre4_ppt(const OpDesc* ops, int nops, const Dims& d, int ls, cud
     return cudaGetLastError();
 }
 
+template <typename Real, int C, int PPT>
+cudaError_t run_param4(const OpDesc* h_ops, int nops, const Dims& d, double* cum, int ls,
+                       cudaStream_t s, bool ranged, bool pre) {
+    if (!h_ops || nops > kParamOps) return cudaErrorInvalidValue;
+    static thread_local OpParams prm;    // 28 KB: copied into the launch
+    std::memcpy(prm.op, h_ops, sizeof(OpDesc) * nops);
+    const int ppb = kT4 / C * PPT;
+    const int grid = (d.Pp + ppb - 1) / ppb;
+    if (pre) {
+        if (ranged) k_pre4c<Real, C, PPT, true><<<grid, kT4, 0, s>>>(prm, nops, d.Pp, ls);
+        else k_pre4c<Real, C, PPT, false><<<grid, kT4, 0, s>>>(prm, nops, d.Pp, ls);
+    } else {
+        if (ranged) k_post4c<Real, C, PPT, true><<<grid, kT4, 0, s>>>(prm, nops, d.Pp, cum, ls);
+        else k_post4c<Real, C, PPT, false><<<grid, kT4, 0, s>>>(prm, nops, d.Pp, cum, ls);
+    }
+    return cudaGetLastError();
+}
+
 template <typename Real, int C, int PPT, bool PRE>
 cudaError_t run_pipe4(const OpDesc* ops, int nops, const Dims& d, double* cum, int ls,
                       cudaStream_t s) {
@@ -562,8 +626,8 @@ cudaError_t run_pipe4(const OpDesc* ops, int nops, const Dims& d, double* cum, i
 }
 
 template <typename Real, int C>
-cudaError_t run_post4(const OpDesc* ops, int nops, const Dims& d, double* cum, int ls,
-                      cudaStream_t s, int variant, bool ranged) {
+cudaError_t run_post4(const OpDesc* ops, const OpDesc* h_ops, int nops, const Dims& d,
+                      double* cum, int ls, cudaStream_t s, int variant, bool ranged) {
     if (variant < 0) variant = default_variant<Real, C>(d.Pp, false);
     if (variant > 0 && 32 % C == 0) {
         constexpr int CC = (32 % C == 0 ? C : 1);
@@ -571,6 +635,8 @@ cudaError_t run_post4(const OpDesc* ops, int nops, const Dims& d, double* cum, i
             case 4: return run_pipe4<Real, CC, 1, false>(ops, nops, d, cum, ls, s);
             case 5: return run_pipe4<Real, CC, 2, false>(ops, nops, d, cum, ls, s);
             case 6: return run_post4_ppt<Real, CC, 2, kMinB6<Real>>(ops, nops, d, cum, ls, s, ranged);
+            case 7: return run_param4<Real, CC, 1>(h_ops, nops, d, cum, ls, s, ranged, false);
+            case 8: return run_param4<Real, CC, 2>(h_ops, nops, d, cum, ls, s, ranged, false);
             case 1: return run_post4_ppt<Real, CC, 1>(ops, nops, d, cum, ls, s, ranged);
             case 2: return run_post4_ppt<Real, CC, 2>(ops, nops, d, cum, ls, s, ranged);
             default: return run_post4_ppt<Real, CC, 4>(ops, nops, d, cum, ls, s, ranged);
@@ -581,8 +647,8 @@ cudaError_t run_post4(const OpDesc* ops, int nops, const Dims& d, double* cum, i
 }
 
 template <typename Real, int C>
-cudaError_t run_pre4(const OpDesc* ops, int nops, const Dims& d, int ls, cudaStream_t s,
-                     int variant, bool ranged) {
+cudaError_t run_pre4(const OpDesc* ops, const OpDesc* h_ops, int nops, const Dims& d, int ls,
+                     cudaStream_t s, int variant, bool ranged) {
     if (variant < 0) variant = default_variant<Real, C>(d.Pp, true);
     if (variant > 0 && 32 % C == 0) {
         constexpr int CC = (32 % C == 0 ? C : 1);
@@ -590,6 +656,8 @@ cudaError_t run_pre4(const OpDesc* ops, int nops, const Dims& d, int ls, cudaStr
             case 4: return run_pipe4<Real, CC, 1, true>(ops, nops, d, nullptr, ls, s);
             case 5: return run_pipe4<Real, CC, 2, true>(ops, nops, d, nullptr, ls, s);
             case 6: return run_pre4_ppt<Real, CC, 2, kMinB6<Real>>(ops, nops, d, ls, s, ranged);
+            case 7: return run_param4<Real, CC, 1>(h_ops, nops, d, nullptr, ls, s, ranged, true);
+            case 8: return run_param4<Real, CC, 2>(h_ops, nops, d, nullptr, ls, s, ranged, true);
             case 1: return run_pre4_ppt<Real, CC, 1>(ops, nops, d, ls, s, ranged);
             case 2: return run_pre4_ppt<Real, CC, 2>(ops, nops, d, ls, s, ranged);
             default: return run_pre4_ppt<Real, CC, 4>(ops, nops, d, ls, s, ranged);
@@ -601,22 +669,23 @@ cudaError_t run_pre4(const OpDesc* ops, int nops, const Dims& d, int ls, cudaStr
 
 }  // namespace
 
-int s4_walk_variants(int C) { return (32 % C == 0) ? 7 : 1; }
+int s4_walk_variants(int C) { return (32 % C == 0) ? 9 : 1; }
 
 template <typename Real>
 cudaError_t launch_update_partials(const OpDesc* ops, int nops, const Dims& d, double* cum,
-                                   int ls, cudaStream_t s, int variant, bool ranged) {
+                                   int ls, cudaStream_t s, int variant, bool ranged,
+                                   const OpDesc* h_ops) {
     if (nops == 0) return cudaSuccess;
     if (d.S == 4 && d.C <= 8) {
         switch (d.C) {
-            case 1: return run_post4<Real, 1>(ops, nops, d, cum, ls, s, variant, ranged);
-            case 2: return run_post4<Real, 2>(ops, nops, d, cum, ls, s, variant, ranged);
-            case 3: return run_post4<Real, 3>(ops, nops, d, cum, ls, s, variant, ranged);
-            case 4: return run_post4<Real, 4>(ops, nops, d, cum, ls, s, variant, ranged);
-            case 5: return run_post4<Real, 5>(ops, nops, d, cum, ls, s, variant, ranged);
-            case 6: return run_post4<Real, 6>(ops, nops, d, cum, ls, s, variant, ranged);
-            case 7: return run_post4<Real, 7>(ops, nops, d, cum, ls, s, variant, ranged);
-            default: return run_post4<Real, 8>(ops, nops, d, cum, ls, s, variant, ranged);
+            case 1: return run_post4<Real, 1>(ops, h_ops, nops, d, cum, ls, s, variant, ranged);
+            case 2: return run_post4<Real, 2>(ops, h_ops, nops, d, cum, ls, s, variant, ranged);
+            case 3: return run_post4<Real, 3>(ops, h_ops, nops, d, cum, ls, s, variant, ranged);
+            case 4: return run_post4<Real, 4>(ops, h_ops, nops, d, cum, ls, s, variant, ranged);
+            case 5: return run_post4<Real, 5>(ops, h_ops, nops, d, cum, ls, s, variant, ranged);
+            case 6: return run_post4<Real, 6>(ops, h_ops, nops, d, cum, ls, s, variant, ranged);
+            case 7: return run_post4<Real, 7>(ops, h_ops, nops, d, cum, ls, s, variant, ranged);
+            default: return run_post4<Real, 8>(ops, h_ops, nops, d, cum, ls, s, variant, ranged);
         }
     }
     return cudaErrorInvalidValue;   // other state counts: k_generic.cu
@@ -624,30 +693,31 @@ cudaError_t launch_update_partials(const OpDesc* ops, int nops, const Dims& d, d
 
 template <typename Real>
 cudaError_t launch_update_pre_partials(const OpDesc* ops, int nops, const Dims& d, int ls,
-                                       cudaStream_t s, int variant, bool ranged) {
+                                       cudaStream_t s, int variant, bool ranged,
+                                       const OpDesc* h_ops) {
     if (nops == 0) return cudaSuccess;
     if (d.S == 4 && d.C <= 8) {
         switch (d.C) {
-            case 1: return run_pre4<Real, 1>(ops, nops, d, ls, s, variant, ranged);
-            case 2: return run_pre4<Real, 2>(ops, nops, d, ls, s, variant, ranged);
-            case 3: return run_pre4<Real, 3>(ops, nops, d, ls, s, variant, ranged);
-            case 4: return run_pre4<Real, 4>(ops, nops, d, ls, s, variant, ranged);
-            case 5: return run_pre4<Real, 5>(ops, nops, d, ls, s, variant, ranged);
-            case 6: return run_pre4<Real, 6>(ops, nops, d, ls, s, variant, ranged);
-            case 7: return run_pre4<Real, 7>(ops, nops, d, ls, s, variant, ranged);
-            default: return run_pre4<Real, 8>(ops, nops, d, ls, s, variant, ranged);
+            case 1: return run_pre4<Real, 1>(ops, h_ops, nops, d, ls, s, variant, ranged);
+            case 2: return run_pre4<Real, 2>(ops, h_ops, nops, d, ls, s, variant, ranged);
+            case 3: return run_pre4<Real, 3>(ops, h_ops, nops, d, ls, s, variant, ranged);
+            case 4: return run_pre4<Real, 4>(ops, h_ops, nops, d, ls, s, variant, ranged);
+            case 5: return run_pre4<Real, 5>(ops, h_ops, nops, d, ls, s, variant, ranged);
+            case 6: return run_pre4<Real, 6>(ops, h_ops, nops, d, ls, s, variant, ranged);
+            case 7: return run_pre4<Real, 7>(ops, h_ops, nops, d, ls, s, variant, ranged);
+            default: return run_pre4<Real, 8>(ops, h_ops, nops, d, ls, s, variant, ranged);
         }
     }
     return cudaErrorInvalidValue;   // other state counts: k_generic.cu
 }
 
 template cudaError_t launch_update_partials<float>(const OpDesc*, int, const Dims&, double*, int,
-                                                   cudaStream_t, int, bool);
+                                                   cudaStream_t, int, bool, const OpDesc*);
 template cudaError_t launch_update_partials<double>(const OpDesc*, int, const Dims&, double*, int,
-                                                    cudaStream_t, int, bool);
+                                                    cudaStream_t, int, bool, const OpDesc*);
 template cudaError_t launch_update_pre_partials<float>(const OpDesc*, int, const Dims&, int,
-                                                       cudaStream_t, int, bool);
+                                                       cudaStream_t, int, bool, const OpDesc*);
 template cudaError_t launch_update_pre_partials<double>(const OpDesc*, int, const Dims&, int,
-                                                        cudaStream_t, int, bool);
+                                                        cudaStream_t, int, bool, const OpDesc*);
 
 }  // namespace b200

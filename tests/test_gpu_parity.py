@@ -174,7 +174,7 @@ def test_full_size_configs(b200, syn, oracle, name, precision):
 
 
 @pytest.mark.parametrize("precision", ["double", "single"])
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8])
 def test_s4_kernel_variants(b200, syn, oracle, monkeypatch, precision, variant):
     """Every S = 4 op-walk and derivative kernel shape the autotuner can pick
     (forced through BEAGLE_B200_FORCE_VARIANT) against the oracle, with C = 4
