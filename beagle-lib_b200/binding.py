@@ -420,3 +420,112 @@ class Instance:
         o2 = np.zeros(self.patternCount) if second else None
         self._call("GetSiteDerivatives", _ptr(o1), _ptr(o2))
         return o1, o2
+
+
+# beagleB200 batch entry points: name -> argument types.
+_BATCH_SIGS = {
+    "CreateBatch": [_p, _i], "FinalizeBatch": [_i],
+    "BatchUpdateTransitionMatrices": [_i, _p, _p, _p, _p],
+    "BatchUpdatePartials": [_i, _p, _p, _p],
+    "BatchUpdatePrePartials": [_i, _p, _p],
+    "BatchAccumulateScaleFactors": [_i, _p, _p, _p, _i],
+    "BatchSetRootPrePartials": [_i, _p, _p],
+    "BatchCalculateRootLogLikelihoods": [_i, _p, _p, _p, _p, _p],
+    "BatchCalculateEdgeDerivatives": [_i, _p, _p, _p, _p, _p, _p, _p],
+    "BatchWait": [_i],
+}
+
+
+class Batch:
+    """A batch of instances of one BeagleLib (``beagleB200*Batch*`` calls):
+    per-member arguments are lists indexed by member position."""
+
+    def __init__(self, blib, instances):
+        self.blib = blib
+        self.members = list(instances)
+        lib = blib.lib
+        p = blib.prefix
+        self._f = {}
+        for name, args in _BATCH_SIGS.items():
+            f = getattr(lib, p + name)
+            f.argtypes = args
+            f.restype = _i
+            self._f[name] = f
+        h = _i32([m.h for m in self.members])
+        code = self._f["CreateBatch"](_ptr(h), len(h))
+        if code < 0:
+            raise BeagleError(p + "CreateBatch", code)
+        self.h = code
+
+    def _call(self, name, *args):
+        code = self._f[name](self.h, *args)
+        if code < 0:
+            raise BeagleError(self.blib.prefix + name, code)
+        return code
+
+    @staticmethod
+    def _ptrs(arrays, dtype):
+        """A C array of pointers to contiguous numpy arrays (kept alive by the caller)."""
+        keep = [np.ascontiguousarray(a, dtype=dtype) for a in arrays]
+        tab = (ctypes.c_void_p * len(keep))(*[a.ctypes.data for a in keep])
+        return tab, keep
+
+    def finalize(self):
+        if self.h is not None:
+            self._f["FinalizeBatch"](self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.finalize()
+        except Exception:
+            pass
+
+    def updateTransitionMatrices(self, eigen, prob, lengths):
+        pt, k1 = self._ptrs(prob, np.int32)
+        lt, k2 = self._ptrs(lengths, np.float64)
+        cnt = _i32([len(a) for a in prob])
+        return self._call("BatchUpdateTransitionMatrices", _ptr(_i32(eigen)), pt, lt, _ptr(cnt))
+
+    def updatePartials(self, ops, cumulative=None):
+        ot, k = self._ptrs([np.asarray(o).reshape(-1) for o in ops], np.int32)
+        cnt = _i32([np.asarray(o).size // 7 for o in ops])
+        cum = _i32(cumulative) if cumulative is not None else None
+        return self._call("BatchUpdatePartials", ot, _ptr(cnt), _ptr(cum))
+
+    def updatePrePartials(self, ops):
+        ot, k = self._ptrs([np.asarray(o).reshape(-1) for o in ops], np.int32)
+        cnt = _i32([np.asarray(o).size // 7 for o in ops])
+        return self._call("BatchUpdatePrePartials", ot, _ptr(cnt))
+
+    def accumulateScaleFactors(self, idx, cumulative, reset=True):
+        it, k = self._ptrs(idx, np.int32)
+        cnt = _i32([len(a) for a in idx])
+        return self._call("BatchAccumulateScaleFactors", it, _ptr(cnt), _ptr(_i32(cumulative)),
+                          1 if reset else 0)
+
+    def setRootPrePartials(self, bufs, freqs):
+        return self._call("BatchSetRootPrePartials", _ptr(_i32(bufs)), _ptr(_i32(freqs)))
+
+    def wait(self):
+        """Deliver deferred results (ASYNCH members) into the arrays returned
+        by the result calls."""
+        return self._call("BatchWait")
+
+    def calculateRootLogLikelihoods(self, bufs, cw, sf, cum):
+        out = np.zeros(len(self.members))
+        self._call("BatchCalculateRootLogLikelihoods", _ptr(_i32(bufs)), _ptr(_i32(cw)),
+                   _ptr(_i32(sf)), _ptr(_i32(cum)), _ptr(out))
+        return out
+
+    def calculateEdgeDerivatives(self, post, pre, dmat, cw):
+        pt, k1 = self._ptrs(post, np.int32)
+        qt, k2 = self._ptrs(pre, np.int32)
+        dt, k3 = self._ptrs(dmat, np.int32)
+        cnt = _i32([len(a) for a in post])
+        sums = [np.zeros(len(a)) for a in post]
+        sq = [np.zeros(len(a)) for a in post]
+        st, k4 = self._ptrs(sums, np.float64)
+        qq, k5 = self._ptrs(sq, np.float64)
+        self._call("BatchCalculateEdgeDerivatives", pt, qt, dt, _ptr(_i32(cw)), _ptr(cnt), st, qq)
+        return k4, k5

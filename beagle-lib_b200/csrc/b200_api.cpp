@@ -6,18 +6,23 @@
 #include "beagle_b200.h"
 
 #include <cuda_runtime.h>
+
+#include <algorithm>
 #include <memory>
 #include <mutex>
 #include <new>
 #include <string>
 #include <vector>
 
+#include "b200_batch.h"
 #include "b200_instance.h"
 
 namespace {
 
 std::mutex g_mu;
 std::vector<std::unique_ptr<b200::Instance>> g_instances;
+std::vector<std::unique_ptr<b200::Batch>> g_batches;
+std::vector<std::vector<int>> g_batch_members;   // instance handles of each batch
 std::vector<BeagleB200Resource> g_resources;
 std::vector<std::string> g_resource_names;
 BeagleB200ResourceList g_resource_list{nullptr, 0};
@@ -37,6 +42,32 @@ int call(int h, F&& f) {
     try {
         if (cudaSetDevice(in->device()) != cudaSuccess) return BEAGLE_B200_ERROR_GENERAL;
         return f(in);
+    } catch (const std::bad_alloc&) {
+        return BEAGLE_B200_ERROR_OUT_OF_MEMORY;
+    } catch (...) {
+        return BEAGLE_B200_ERROR_UNIDENTIFIED_EXCEPTION;
+    }
+}
+
+// Run one batch method with the batch's device current, after checking that
+// every member instance still exists.
+template <typename F>
+int call_batch(int h, F&& f) {
+    b200::Batch* bt = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        if (h < 0 || h >= (int)g_batches.size() || !g_batches[h])
+            return BEAGLE_B200_ERROR_UNINITIALIZED_INSTANCE;
+        for (int m : g_batch_members[h])
+            if (m < 0 || m >= (int)g_instances.size() || !g_instances[m])
+                return BEAGLE_B200_ERROR_UNINITIALIZED_INSTANCE;
+        bt = g_batches[h].get();
+    }
+    try {
+        b200::Instance* first = get(g_batch_members[h][0]);
+        if (!first || cudaSetDevice(first->device()) != cudaSuccess)
+            return BEAGLE_B200_ERROR_GENERAL;
+        return f(bt);
     } catch (const std::bad_alloc&) {
         return BEAGLE_B200_ERROR_OUT_OF_MEMORY;
     } catch (...) {
@@ -354,6 +385,127 @@ int beagleB200GetCudaStream(int h, void** out) {
         *out = (void*)in->stream();
         return BEAGLE_B200_SUCCESS;
     });
+}
+
+
+int beagleB200CreateBatch(const int* instances, int count) {
+    if (!instances || count <= 0) return BEAGLE_B200_ERROR_OUT_OF_RANGE;
+    std::vector<b200::Instance*> members;
+    std::vector<int> handles(instances, instances + count);
+    for (int h : handles) {
+        b200::Instance* in = get(h);
+        if (!in) return BEAGLE_B200_ERROR_UNINITIALIZED_INSTANCE;
+        members.push_back(in);
+    }
+    {
+        // an instance belongs to at most one batch
+        std::lock_guard<std::mutex> lk(g_mu);
+        for (size_t b = 0; b < g_batch_members.size(); ++b)
+            if (g_batches[b])
+                for (int h : g_batch_members[b])
+                    if (std::find(handles.begin(), handles.end(), h) != handles.end())
+                        return BEAGLE_B200_ERROR_OUT_OF_RANGE;
+    }
+    try {
+        if (cudaSetDevice(members[0]->device()) != cudaSuccess) return BEAGLE_B200_ERROR_GENERAL;
+        std::unique_ptr<b200::Batch> bt(new b200::Batch());
+        const int rc = bt->create(members);
+        if (rc) return rc;
+        std::lock_guard<std::mutex> lk(g_mu);
+        for (size_t k = 0; k < g_batches.size(); ++k)
+            if (!g_batches[k]) {
+                g_batches[k] = std::move(bt);
+                g_batch_members[k] = handles;
+                return (int)k;
+            }
+        g_batches.push_back(std::move(bt));
+        g_batch_members.push_back(handles);
+        return (int)g_batches.size() - 1;
+    } catch (const std::bad_alloc&) {
+        return BEAGLE_B200_ERROR_OUT_OF_MEMORY;
+    } catch (...) {
+        return BEAGLE_B200_ERROR_UNIDENTIFIED_EXCEPTION;
+    }
+}
+
+int beagleB200FinalizeBatch(int batch) {
+    std::unique_ptr<b200::Batch> bt;
+    std::vector<int> members;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        if (batch < 0 || batch >= (int)g_batches.size() || !g_batches[batch])
+            return BEAGLE_B200_ERROR_UNINITIALIZED_INSTANCE;
+        bt = std::move(g_batches[batch]);
+        members = g_batch_members[batch];
+        g_batch_members[batch].clear();
+    }
+    // Members that were finalized meanwhile are skipped: release only the live ones.
+    b200::Instance* first = members.empty() ? nullptr : get(members[0]);
+    if (first) cudaSetDevice(first->device());
+    bool all_alive = true;
+    for (int h : members) all_alive = all_alive && get(h) != nullptr;
+    if (all_alive) bt->release();
+    bt.reset();
+    return BEAGLE_B200_SUCCESS;
+}
+
+int beagleB200BatchUpdateTransitionMatrices(int batch, const int* eig, const int* const* prob,
+                                            const double* const* t, const int* counts) {
+    if (!prob || !t || !counts) return BEAGLE_B200_ERROR_OUT_OF_RANGE;
+    return call_batch(batch, [&](b200::Batch* b) {
+        return b->updateTransitionMatrices(eig, prob, t, counts);
+    });
+}
+
+int beagleB200BatchUpdatePartials(int batch, const int* const* ops, const int* counts,
+                                  const int* cumulative) {
+    if (!ops || !counts) return BEAGLE_B200_ERROR_OUT_OF_RANGE;
+    return call_batch(batch, [&](b200::Batch* b) {
+        return b->updatePartials(ops, counts, cumulative, false);
+    });
+}
+
+int beagleB200BatchUpdatePrePartials(int batch, const int* const* ops, const int* counts) {
+    if (!ops || !counts) return BEAGLE_B200_ERROR_OUT_OF_RANGE;
+    return call_batch(batch, [&](b200::Batch* b) {
+        return b->updatePartials(ops, counts, nullptr, true);
+    });
+}
+
+int beagleB200BatchAccumulateScaleFactors(int batch, const int* const* idx, const int* counts,
+                                          const int* cumulative, int reset) {
+    if (!idx || !counts || !cumulative) return BEAGLE_B200_ERROR_OUT_OF_RANGE;
+    return call_batch(batch, [&](b200::Batch* b) {
+        return b->accumulateScaleFactors(idx, counts, cumulative, reset);
+    });
+}
+
+int beagleB200BatchSetRootPrePartials(int batch, const int* bufs, const int* freqs) {
+    if (!bufs || !freqs) return BEAGLE_B200_ERROR_OUT_OF_RANGE;
+    return call_batch(batch, [&](b200::Batch* b) { return b->setRootPrePartials(bufs, freqs); });
+}
+
+int beagleB200BatchCalculateRootLogLikelihoods(int batch, const int* bufs, const int* cw,
+                                               const int* sf, const int* cum, double* out) {
+    if (!bufs || !cw || !sf || !out) return BEAGLE_B200_ERROR_OUT_OF_RANGE;
+    return call_batch(batch, [&](b200::Batch* b) {
+        return b->rootLogLikelihoods(bufs, cw, sf, cum, out);
+    });
+}
+
+int beagleB200BatchCalculateEdgeDerivatives(int batch, const int* const* post,
+                                            const int* const* pre, const int* const* dmat,
+                                            const int* cw, const int* counts,
+                                            double* const* sums, double* const* sumsq) {
+    if (!post || !pre || !dmat || !cw || !counts || !sums || !sumsq)
+        return BEAGLE_B200_ERROR_OUT_OF_RANGE;
+    return call_batch(batch, [&](b200::Batch* b) {
+        return b->edgeDerivatives(post, pre, dmat, cw, counts, sums, sumsq);
+    });
+}
+
+int beagleB200BatchWait(int batch) {
+    return call_batch(batch, [&](b200::Batch* b) { return b->wait(); });
 }
 
 }  // extern "C"

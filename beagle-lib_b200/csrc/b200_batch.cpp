@@ -1,0 +1,450 @@
+// Batched calls over several instances; see b200_batch.h.
+#include "b200_batch.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <tuple>
+
+namespace b200 {
+
+namespace {
+
+enum { kSuccess = 0, kErrGeneral = -1, kErrOOM = -2, kErrRange = -5, kErrFP = -8 };
+
+#define CK(call)                                                              \
+    do {                                                                      \
+        cudaError_t e_ = (call);                                              \
+        if (e_ != cudaSuccess) {                                              \
+            (void)cudaGetLastError();                                         \
+            return e_ == cudaErrorMemoryAllocation ? kErrOOM : kErrGeneral;   \
+        }                                                                     \
+    } while (0)
+
+#define LAUNCH(fn, ...) (dbl_ ? fn<double>(__VA_ARGS__) : fn<float>(__VA_ARGS__))
+
+// 4-state members with a lane-group category count run in the batched kernels.
+bool batched4(const Instance* in, int S, int C) {
+    (void)in;
+    return S == 4 && (C == 1 || C == 2 || C == 4 || C == 8);
+}
+
+int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// Bytes of `v`, appended to a byte table at a 256-byte aligned offset.
+template <typename T>
+size_t append(std::vector<unsigned char>& table, const std::vector<T>& v) {
+    const size_t off = (table.size() + 255) & ~size_t(255);
+    table.resize(off + sizeof(T) * v.size());
+    if (!v.empty()) std::memcpy(table.data() + off, v.data(), sizeof(T) * v.size());
+    return off;
+}
+
+}  // namespace
+
+Batch::~Batch() {
+    release();
+    for (DevBuf* b : {&t_a_, &t_b_, &t_c_, &t_block_, &t_out_, &t_out2_}) b->release();
+    for (auto& c : chunks_) cudaFreeHost(c.first);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+int Batch::create(const std::vector<Instance*>& members) {
+    if (members.empty()) return kErrRange;
+    device_ = members[0]->device_;
+    dbl_ = members[0]->dbl_;
+    for (Instance* in : members)
+        if (!in || in->device_ != device_ || in->dbl_ != dbl_) return kErrRange;
+    for (size_t i = 0; i < members.size(); ++i)
+        for (size_t j = i + 1; j < members.size(); ++j)
+            if (members[i] == members[j]) return kErrRange;
+    CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    for (Instance* in : members) {
+        const int rc = in->use_stream(stream_);
+        if (rc) return rc;
+        m_.push_back(in);
+    }
+    return kSuccess;
+}
+
+void Batch::release() {
+    if (!m_.empty()) wait();
+    for (Instance* in : m_) in->use_stream(nullptr);
+    m_.clear();
+}
+
+bool Batch::deferred() const {
+    for (const Instance* in : m_)
+        if (!in->async_) return false;
+    return true;
+}
+
+int Batch::sync() {
+    CK(cudaStreamSynchronize(stream_));
+    for (const Pending& pd : pending_) {
+        std::copy(pd.src, pd.src + pd.n, pd.dst);
+        if (pd.member >= 0) m_[pd.member]->last_lnl_ = pd.src[0];
+    }
+    pending_.clear();
+    chunk_i_ = 0;
+    chunk_off_ = 0;
+    // Members that ran their own result calls (ASYNCH) deliver theirs too.
+    for (Instance* in : m_)
+        if (!in->pending_.empty()) {
+            const int rc = in->sync();
+            if (rc) return rc;
+        }
+    return kSuccess;
+}
+
+int Batch::wait() { return sync(); }
+
+// n doubles of pinned staging, valid until the next sync().
+double* Batch::stage(size_t n) {
+    while (chunk_i_ < chunks_.size() && chunk_off_ + n > chunks_[chunk_i_].second) {
+        ++chunk_i_;
+        chunk_off_ = 0;
+    }
+    if (chunk_i_ == chunks_.size()) {
+        const size_t sz = std::max<size_t>(n, 1 << 16);
+        double* p = nullptr;
+        if (cudaMallocHost(&p, sizeof(double) * sz) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return nullptr;
+        }
+        chunks_.emplace_back(p, sz);
+    }
+    double* p = chunks_[chunk_i_].first + chunk_off_;
+    chunk_off_ += n;
+    return p;
+}
+
+// ------------------------------------------------------------ matrices
+int Batch::updateTransitionMatrices(const int* eig, const int* const* prob,
+                                    const double* const* t, const int* counts) {
+    const int n = size();
+    std::map<std::tuple<int, int, int>, std::vector<MatJob>> groups;   // (S, Sg, C) -> jobs
+    for (int i = 0; i < n; ++i) {
+        Instance* in = m_[i];
+        std::vector<MatJob> jobs;
+        std::vector<int> e(std::max(counts[i], 0), eig ? eig[i] : 0), r(e.size(), 0);
+        const int rc = in->build_matrix_jobs(e.data(), r.data(), prob[i], nullptr, nullptr, t[i],
+                                             counts[i], jobs);
+        if (rc) return rc;
+        auto& g = groups[std::make_tuple(in->S_, in->Sg_, in->C_)];
+        g.insert(g.end(), jobs.begin(), jobs.end());
+    }
+    std::vector<unsigned char> table;
+    std::vector<std::pair<size_t, size_t>> where;   // (offset, jobs) per group
+    for (auto& kv : groups) where.emplace_back(append(table, kv.second), kv.second.size());
+    if (table.empty()) return kSuccess;
+    CK(t_a_.upload(table.data(), table.size(), stream_));
+    size_t k = 0;
+    for (auto& kv : groups) {
+        const Dims d{std::get<0>(kv.first), std::get<1>(kv.first), 0, 0, std::get<2>(kv.first)};
+        const MatJob* jobs = (const MatJob*)((unsigned char*)t_a_.ptr + where[k].first);
+        CK(LAUNCH(launch_update_matrices, jobs, (int)where[k].second, d, stream_));
+        ++k;
+    }
+    return kSuccess;
+}
+
+// ----------------------------------------------------------------- walks
+int Batch::updatePartials(const int* const* ops, const int* counts, const int* cumulative,
+                          bool pre) {
+    const int n = size();
+    struct Member {
+        int i;
+        size_t ops_off;
+        int nops;
+    };
+    std::map<int, std::vector<Member>> groups;   // C -> batched 4-state members
+    std::vector<unsigned char> table;
+    std::vector<int> fallback;
+    for (int i = 0; i < n; ++i) {
+        Instance* in = m_[i];
+        const int cum = cumulative ? cumulative[i] : -1;
+        if (cum != -1 && (cum < 0 || cum >= in->nscale_)) return kErrRange;
+        if (!batched4(in, in->S_, in->C_)) {
+            fallback.push_back(i);
+            continue;
+        }
+        std::vector<OpDesc> tab;
+        std::vector<uint8_t> dep;
+        bool idem = true, has_cum = false;
+        const int rc = in->build_walk(ops[i], counts[i], 7, pre, tab, dep, idem, has_cum);
+        if (rc) return rc;
+        if (tab.empty()) continue;
+        groups[in->C_].push_back(Member{i, append(table, tab), (int)tab.size()});
+    }
+    // Single-instance launches of the other members (shared stream).
+    for (int i : fallback) {
+        const int rc = m_[i]->post_or_pre(ops[i], counts[i], 7, cumulative ? cumulative[i] : -1,
+                                          pre);
+        if (rc) return rc;
+    }
+    if (groups.empty()) return kSuccess;
+    CK(t_a_.upload(table.data(), table.size(), stream_));
+    // Segment tables (device pointers into t_a_), one per category count.
+    std::vector<unsigned char> segtab;
+    struct G {
+        int C;
+        size_t off;
+        int nseg;
+        int ncta;
+    };
+    std::vector<G> gl;
+    for (auto& kv : groups) {
+        const int C = kv.first;
+        std::vector<WalkSeg> segs;
+        int cta = 0;
+        for (const Member& mb : kv.second) {
+            Instance* in = m_[mb.i];
+            const int cum = cumulative ? cumulative[mb.i] : -1;
+            WalkSeg sg{};
+            sg.ops = (const OpDesc*)((unsigned char*)t_a_.ptr + mb.ops_off);
+            sg.cum = (!pre && cum >= 0) ? in->scale(cum) : nullptr;
+            sg.nops = mb.nops;
+            sg.Pp = in->Pp_;
+            sg.log_scalers = (int)in->log_scalers_;
+            sg.first_cta = cta;
+            cta += ceil_div(in->Pp_, 256 / C);
+            segs.push_back(sg);
+        }
+        gl.push_back(G{C, append(segtab, segs), (int)segs.size(), cta});
+    }
+    CK(t_b_.upload(segtab.data(), segtab.size(), stream_));
+    for (const G& g : gl)
+        CK(LAUNCH(launch_walk4_batch, (const WalkSeg*)((unsigned char*)t_b_.ptr + g.off), g.nseg,
+                  g.ncta, g.C, pre, stream_));
+    return kSuccess;
+}
+
+// ---------------------------------------------------------- scale factors
+int Batch::accumulateScaleFactors(const int* const* idx, const int* counts,
+                                  const int* cumulative, int reset) {
+    const int n = size();
+    std::vector<unsigned char> itab;
+    std::vector<size_t> ioff(n);
+    for (int i = 0; i < n; ++i) {
+        Instance* in = m_[i];
+        if (cumulative[i] < 0 || cumulative[i] >= in->nscale_ || counts[i] < 0) return kErrRange;
+        std::vector<int> v(idx[i], idx[i] + counts[i]);
+        for (int x : v)
+            if (x < 0 || x >= in->nscale_) return kErrRange;
+        ioff[i] = append(itab, v);
+    }
+    if (itab.empty()) itab.resize(16);
+    CK(t_a_.upload(itab.data(), itab.size(), stream_));
+    std::vector<AccSeg> segs(n);
+    int cta = 0;
+    for (int i = 0; i < n; ++i) {
+        Instance* in = m_[i];
+        AccSeg& sg = segs[i];
+        sg.cum = in->scale(cumulative[i]);
+        sg.pool = in->d_scale_;
+        sg.idx = (const int*)((unsigned char*)t_a_.ptr + ioff[i]);
+        sg.n = counts[i];
+        sg.Pp = in->Pp_;
+        sg.P = in->P_;
+        sg.log_scalers = (int)in->log_scalers_;
+        sg.reset = reset;
+        sg.first_cta = cta;
+        cta += ceil_div(in->P_, accumulate_batch_patterns());
+    }
+    CK(t_b_.upload(segs.data(), sizeof(AccSeg) * n, stream_));
+    CK(launch_accumulate_batch((const AccSeg*)t_b_.ptr, n, cta, stream_));
+    return kSuccess;
+}
+
+// --------------------------------------------------------- root partials
+int Batch::setRootPrePartials(const int* bufs, const int* freqs) {
+    const int n = size();
+    std::vector<FillSeg> segs(n);
+    int cta = 0;
+    for (int i = 0; i < n; ++i) {
+        Instance* in = m_[i];
+        const int b = bufs[i], f = freqs[i];
+        if (!in->buf_ok(b) || f < 0 || f >= in->neig_ || !in->freqs_set_[f]) return kErrRange;
+        const int rc = in->ensure_partials(b);
+        if (rc) return rc;
+        FillSeg& sg = segs[i];
+        sg.dest = in->partials_[b];
+        sg.freqs = in->d_freqs_ + (size_t)f * in->S_;
+        sg.n = (long long)in->Pp_ * in->C_ * in->Sg_;
+        sg.S = in->S_;
+        sg.Sg = in->Sg_;
+        sg.first_cta = cta;
+        cta += ceil_div(sg.n, 256);
+    }
+    CK(t_c_.upload(segs.data(), sizeof(FillSeg) * n, stream_));
+    CK(LAUNCH(launch_fill_batch, (const FillSeg*)t_c_.ptr, n, cta, stream_));
+    return kSuccess;
+}
+
+// ----------------------------------------------------------- root lnL
+int Batch::rootLogLikelihoods(const int* bufs, const int* cw, const int* sf, const int* cum,
+                              double* out) {
+    const int n = size();
+    std::vector<RootSeg> segs(n);
+    std::vector<FinalSeg> fin(n);
+    int cta = 0;
+    size_t blocks = 0;
+    for (int i = 0; i < n; ++i) {
+        Instance* in = m_[i];
+        const int b = bufs[i], w = cw[i], f = sf[i], c = cum ? cum[i] : -1;
+        if (!in->buf_ok(b) || !in->partials_[b]) return kErrRange;
+        if (w < 0 || w >= in->neig_ || !in->catw_set_[w] || f < 0 || f >= in->neig_ ||
+            !in->freqs_set_[f])
+            return kErrRange;
+        if (c != -1 && (c < 0 || c >= in->nscale_)) return kErrRange;
+        const int nblk = reduction_blocks(in->P_);
+        RootSeg& sg = segs[i];
+        sg.root = in->partials_[b];
+        sg.catw = in->d_catw_ + (size_t)w * in->C_;
+        sg.freqs = in->d_freqs_ + (size_t)f * in->S_;
+        sg.cum = c >= 0 ? in->scale(c) : nullptr;
+        sg.patw = in->d_patw_;
+        sg.site = in->d_site_;
+        sg.block = nullptr;   // set below, after t_block_ is sized
+        sg.S = in->S_;
+        sg.Sg = in->Sg_;
+        sg.C = in->C_;
+        sg.P = in->P_;
+        sg.first_cta = cta;
+        cta += nblk;
+        fin[i].nblk = nblk;
+        fin[i].nout = 1;
+        fin[i].first_out = i;
+        blocks += nblk;
+    }
+    CK(t_block_.reserve(sizeof(double) * std::max<size_t>(blocks, 1)));
+    CK(t_out_.reserve(sizeof(double) * n));
+    size_t boff = 0;
+    for (int i = 0; i < n; ++i) {
+        segs[i].block = (double*)t_block_.ptr + boff;
+        fin[i].block = segs[i].block;
+        fin[i].out = (double*)t_out_.ptr + i;
+        boff += fin[i].nblk;
+    }
+    std::vector<unsigned char> table;
+    const size_t o1 = append(table, segs), o2 = append(table, fin);
+    CK(t_c_.upload(table.data(), table.size(), stream_));
+    CK(LAUNCH(launch_root_batch, (const RootSeg*)((unsigned char*)t_c_.ptr + o1), n, cta,
+              stream_));
+    CK(launch_final_batch((const FinalSeg*)((unsigned char*)t_c_.ptr + o2), n, n, stream_));
+    double* h = stage(n);
+    if (!h) return kErrOOM;
+    CK(cudaMemcpyAsync(h, t_out_.ptr, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_));
+    for (int i = 0; i < n; ++i) pending_.push_back(Pending{h + i, out + i, 1, i});
+    if (deferred()) return kSuccess;   // delivered by wait()
+    int rc = sync();
+    if (rc) return rc;
+    bool nan = false;
+    for (int i = 0; i < n; ++i) nan = nan || std::isnan(out[i]);
+    return nan ? kErrFP : kSuccess;
+}
+
+// ------------------------------------------------------- edge derivatives
+int Batch::edgeDerivatives(const int* const* post, const int* const* pre,
+                           const int* const* dmat, const int* cw, const int* counts,
+                           double* const* sums, double* const* sumsq) {
+    const int n = size();
+    struct Member {
+        int i;
+        size_t desc_off;
+        int nb;
+        int nblk;
+    };
+    std::map<int, std::vector<Member>> groups;
+    std::vector<unsigned char> table;
+    std::vector<int> fallback;
+    for (int i = 0; i < n; ++i) {
+        Instance* in = m_[i];
+        if (counts[i] <= 0) continue;
+        if (!batched4(in, in->S_, in->C_)) {
+            fallback.push_back(i);
+            continue;
+        }
+        std::vector<DerivDesc> tab;
+        const int rc = in->build_deriv(post[i], pre[i], dmat[i], &cw[i], counts[i], tab);
+        if (rc) return rc;
+        groups[in->C_].push_back(
+            Member{i, append(table, tab), counts[i], ceil_div(in->P_, deriv4_batch_tile(in->C_))});
+    }
+    for (int i : fallback) {
+        const int rc = m_[i]->calculateEdgeDerivatives(post[i], pre[i], dmat[i], &cw[i],
+                                                       counts[i], nullptr, sums[i], sumsq[i]);
+        if (rc) return rc;
+    }
+    if (groups.empty()) return kSuccess;
+    CK(t_a_.upload(table.data(), table.size(), stream_));
+    size_t blocks = 0, outs = 0;
+    for (auto& kv : groups)
+        for (const Member& mb : kv.second) {
+            blocks += (size_t)2 * mb.nb * mb.nblk;
+            outs += (size_t)2 * mb.nb;
+        }
+    CK(t_block_.reserve(sizeof(double) * blocks));
+    CK(t_out2_.reserve(sizeof(double) * outs));
+    std::vector<unsigned char> segtab;
+    struct G {
+        int C;
+        size_t off;
+        int nseg;
+        int ncta;
+    };
+    std::vector<G> gl;
+    std::vector<FinalSeg> fin;
+    std::vector<std::pair<int, size_t>> out_of;   // (member, first output) in t_out_
+    size_t boff = 0, ooff = 0;
+    for (auto& kv : groups) {
+        std::vector<DerivSeg> segs;
+        int cta = 0;
+        for (const Member& mb : kv.second) {
+            Instance* in = m_[mb.i];
+            DerivSeg sg{};
+            sg.desc = (const DerivDesc*)((unsigned char*)t_a_.ptr + mb.desc_off);
+            sg.catw = in->d_catw_ + (size_t)cw[mb.i] * in->C_;
+            sg.patw = in->d_patw_;
+            sg.block = (double*)t_block_.ptr + boff;
+            sg.nb = mb.nb;
+            sg.P = in->P_;
+            sg.nblk = mb.nblk;
+            sg.first_cta = cta;
+            cta += mb.nb * mb.nblk;
+            segs.push_back(sg);
+            FinalSeg f{};
+            f.block = sg.block;
+            f.out = (double*)t_out2_.ptr + ooff;
+            f.nblk = mb.nblk;
+            f.nout = 2 * mb.nb;
+            f.first_out = (int)ooff;
+            fin.push_back(f);
+            out_of.emplace_back(mb.i, ooff);
+            boff += (size_t)2 * mb.nb * mb.nblk;
+            ooff += (size_t)2 * mb.nb;
+        }
+        gl.push_back(G{kv.first, append(segtab, segs), (int)segs.size(), cta});
+    }
+    const size_t foff = append(segtab, fin);
+    CK(t_b_.upload(segtab.data(), segtab.size(), stream_));
+    for (const G& g : gl)
+        CK(LAUNCH(launch_deriv4_batch, (const DerivSeg*)((unsigned char*)t_b_.ptr + g.off),
+                  g.nseg, g.ncta, g.C, stream_));
+    CK(launch_final_batch((const FinalSeg*)((unsigned char*)t_b_.ptr + foff), (int)fin.size(),
+                          (int)ooff, stream_));
+    double* h = stage(ooff);
+    if (!h) return kErrOOM;
+    CK(cudaMemcpyAsync(h, t_out2_.ptr, sizeof(double) * ooff, cudaMemcpyDeviceToHost, stream_));
+    for (const auto& mo : out_of) {
+        const int i = mo.first, nb = counts[i];
+        if (sums[i]) pending_.push_back(Pending{h + mo.second, sums[i], (size_t)nb, -1});
+        if (sumsq[i]) pending_.push_back(Pending{h + mo.second + nb, sumsq[i], (size_t)nb, -1});
+    }
+    if (deferred()) return kSuccess;   // delivered by wait()
+    return sync();
+}
+
+}  // namespace b200

@@ -1,0 +1,72 @@
+// Batched calls over several instances (the beagleB200Batch* entry points):
+// many trees / partitions of uneven pattern and state counts evaluated with a
+// handful of launches instead of one launch chain per instance.
+//
+// The members share one CUDA stream for the batch's lifetime, so a batch call
+// and any single-instance call stay ordered.  Each batched call validates and
+// resolves every member's arguments exactly as the single-instance call does
+// (Instance::build_*), then:
+//   * transition matrices: one launch per (S, C) group of members;
+//   * post- / pre-order walks and edge derivatives: one launch per category
+//     count for the 4-state members (k_walk4_batch, k_deriv4_batch); other
+//     members run their own single-instance launch on the shared stream;
+//   * scale accumulation, root pre-partials, root log-likelihoods and the
+//     final derivative sums: one launch for all members.
+#pragma once
+#include <cuda_runtime.h>
+#include <vector>
+
+#include "b200_instance.h"
+
+namespace b200 {
+
+class Batch {
+public:
+    ~Batch();
+    // Members must share device and precision.  Returns a BeagleReturnCode.
+    int create(const std::vector<Instance*>& members);
+    int size() const { return (int)m_.size(); }
+
+    int updateTransitionMatrices(const int* eigenIndices, const int* const* probIdx,
+                                 const double* const* edgeLengths, const int* counts);
+    int updatePartials(const int* const* ops, const int* counts, const int* cumulative,
+                       bool pre);
+    int accumulateScaleFactors(const int* const* idx, const int* counts, const int* cumulative,
+                               int reset);
+    int setRootPrePartials(const int* bufs, const int* freqs);
+    int rootLogLikelihoods(const int* bufs, const int* cw, const int* sf, const int* cum,
+                           double* out);
+    int edgeDerivatives(const int* const* post, const int* const* pre,
+                        const int* const* dmat, const int* cw, const int* counts,
+                        double* const* sums, double* const* sumsq);
+    // Wait for the batch's queued work and deliver deferred results.
+    int wait();
+    // Members back on their own streams.
+    void release();
+
+private:
+    int sync();
+    double* stage(size_t n);
+    bool deferred() const;     // every member is ASYNCH: results wait for wait()
+
+    // A result copied to pinned memory, delivered to dst[0 .. n) at wait();
+    // member >= 0 also records the value as that member's last lnL.
+    struct Pending {
+        const double* src;
+        double* dst;
+        size_t n;
+        int member;
+    };
+    std::vector<Pending> pending_;
+    std::vector<std::pair<double*, size_t>> chunks_;   // pinned staging, reused after wait()
+    size_t chunk_i_ = 0, chunk_off_ = 0;
+
+    std::vector<Instance*> m_;
+    cudaStream_t stream_ = nullptr;
+    int device_ = 0;
+    bool dbl_ = false;
+    DevBuf t_a_, t_b_, t_c_, t_block_, t_out_;   // per-call tables and scratch
+    DevBuf t_out2_;                              // derivative sums (root lnL uses t_out_)
+};
+
+}  // namespace b200

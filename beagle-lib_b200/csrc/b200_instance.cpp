@@ -89,7 +89,7 @@ Instance::~Instance() {
     if (h_out_) cudaFreeHost(h_out_);
     if (h_tc_status_) cudaFreeHost(h_tc_status_);
     for (auto& c : chunks_) cudaFreeHost(c.first);
-    if (stream_) cudaStreamDestroy(stream_);
+    if (own_stream_) cudaStreamDestroy(own_stream_);
 }
 
 int Instance::create(int tipCount, int partialsBufferCount, int compactBufferCount,
@@ -136,6 +136,7 @@ int Instance::create(int tipCount, int partialsBufferCount, int compactBufferCou
     if (prop.major != 10 || prop.minor != 0) return -6;   // sm_100 only
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    own_stream_ = stream_;
 
     N_ = tipCount;
     nbuf_ = partialsBufferCount + compactBufferCount;
@@ -198,6 +199,14 @@ int Instance::create(int tipCount, int partialsBufferCount, int compactBufferCou
     CK(cudaMallocHost(&h_tc_status_, 2 * sizeof(int)));
     h_tc_status_[0] = h_tc_status_[1] = 0;
     return sync();
+}
+
+// Queue this instance's work on `s` (a batch's stream) from now on, after
+// everything queued so far; nullptr returns to the instance's own stream.
+int Instance::use_stream(cudaStream_t s) {
+    CK(cudaStreamSynchronize(stream_));
+    stream_ = s ? s : own_stream_;
+    return kSuccess;
 }
 
 int Instance::sync() {
@@ -540,8 +549,18 @@ int Instance::updateTransitionMatricesWithMultipleModels(const int* eig, const i
                                                          const int* prob, const int* d1,
                                                          const int* d2, const double* t,
                                                          int count) {
+    std::vector<MatJob> jobs;
+    const int rc = build_matrix_jobs(eig, rix, prob, d1, d2, t, count, jobs);
+    if (rc) return rc;
+    return run_matrix_jobs(jobs);
+}
+
+// Validate and resolve transition-matrix requests into device jobs.
+int Instance::build_matrix_jobs(const int* eig, const int* rix, const int* prob, const int* d1,
+                                const int* d2, const double* t, int count,
+                                std::vector<MatJob>& jobs) {
     if (count < 0 || (count > 0 && (!prob || !t))) return kErrRange;
-    std::vector<MatJob> jobs(count);
+    jobs.assign(count, MatJob{});
     for (int u = 0; u < count; ++u) {
         const int e = eig ? eig[u] : 0, r = rix ? rix[u] : 0;
         if (e < 0 || e >= neig_ || !eig_set_[e] || r < 0 || r >= neig_ || !rates_set_[r])
@@ -564,7 +583,7 @@ int Instance::updateTransitionMatricesWithMultipleModels(const int* eig, const i
         if (j.d1) mat_pad_[d1[u]] = 0.0;
         if (j.d2) mat_pad_[d2[u]] = 0.0;
     }
-    return run_matrix_jobs(jobs);
+    return kSuccess;
 }
 
 int Instance::updateTransitionMatrices(int e, const int* prob, const int* d1, const int* d2,
@@ -580,17 +599,20 @@ int Instance::updateTransitionMatricesWithModelCategories(const int*, const int*
 }
 
 // ---------------------------------------------------------------- partials
-int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative, bool pre) {
+// Validate an op list (7 ints, or 9 for partition ops) and resolve it into
+// device descriptors.  dep[k] != 0 when op k reads op k - 1's output;
+// `idempotent`: the list may be run again (no op reads a buffer the list
+// writes at or after it); `has_op_cum`: some partition op adds into its own
+// cumulative buffer.
+int Instance::build_walk(const int* ops, int count, int stride, bool pre, std::vector<OpDesc>& tab,
+                         std::vector<uint8_t>& dep, bool& idempotent, bool& has_op_cum) {
     if (count < 0 || (count > 0 && !ops)) return kErrRange;
-    if (cumulative != -1 && (cumulative < 0 || cumulative >= nscale_)) return kErrRange;
-    std::vector<OpDesc> tab(count);
-    std::vector<uint8_t> dep(count, 0);
-    bool has_op_cum = false;
+    tab.assign(count, OpDesc{});
+    dep.assign(count, 0);
+    has_op_cum = false;
     // Buffers written earlier in this list count as holding data.
     std::vector<char> written(nbuf_, 0);
-    // A list is idempotent (may be run again by the autotuner) when no op
-    // reads a partials or scale buffer that the list writes at or after it.
-    bool idempotent = true;
+    idempotent = true;
     std::vector<char> later(nbuf_, 0), later_scale(nscale_ > 0 ? nscale_ : 1, 0);
     for (int k = count - 1; k >= 0; --k) {
         const int* op = ops + (size_t)k * stride;
@@ -656,6 +678,17 @@ int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative,
         }
         d.reserved = 0;
     }
+    return kSuccess;
+}
+
+int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative, bool pre) {
+    if (cumulative != -1 && (cumulative < 0 || cumulative >= nscale_)) return kErrRange;
+    std::vector<OpDesc> tab;
+    std::vector<uint8_t> dep;
+    bool idempotent = true, has_op_cum = false;
+    int rc = build_walk(ops, count, stride, pre, tab, dep, idempotent, has_op_cum);
+    if (rc) return rc;
+    if (count == 0) return kSuccess;
     DevBuf& t = pre ? t_ops_pre_ : t_ops_post_;
     CK(t.upload(tab.data(), sizeof(OpDesc) * tab.size(), stream_));
     double* cum = (cumulative >= 0 && !pre) ? scale(cumulative) : nullptr;
@@ -854,14 +887,14 @@ int Instance::calculateRootLogLikelihoodsByPartition(const int* bufs, const int*
     return std::isnan(total) ? kErrFP : kSuccess;
 }
 
-int Instance::calculateEdgeDerivatives(const int* post, const int* pre, const int* dmat,
-                                       const int* cw, int count, double* outDerivs,
-                                       double* outSum, double* outSumSq) {
+// Validate and resolve an edge-derivative request into device descriptors.
+int Instance::build_deriv(const int* post, const int* pre, const int* dmat, const int* cw,
+                          int count, std::vector<DerivDesc>& tab) {
     if (count < 0 || (count > 0 && (!post || !pre || !dmat || !cw))) return kErrRange;
     if (count == 0) return kSuccess;
     const int w = cw[0];
     if (w < 0 || w >= neig_ || !catw_set_[w]) return kErrRange;
-    std::vector<DerivDesc> tab(count);
+    tab.assign(count, DerivDesc{});
     for (int k = 0; k < count; ++k) {
         if (!has_data(post[k]) || !buf_ok(pre[k]) || !partials_[pre[k]]) return kErrRange;
         if (dmat[k] < 0 || dmat[k] >= nmat_) return kErrRange;
@@ -874,6 +907,17 @@ int Instance::calculateEdgeDerivatives(const int* post, const int* pre, const in
         d.dpad = mat_pad_[dmat[k]];
         d.reserved = 0;
     }
+    return kSuccess;
+}
+
+int Instance::calculateEdgeDerivatives(const int* post, const int* pre, const int* dmat,
+                                       const int* cw, int count, double* outDerivs,
+                                       double* outSum, double* outSumSq) {
+    std::vector<DerivDesc> tab;
+    const int rc0 = build_deriv(post, pre, dmat, cw, count, tab);
+    if (rc0) return rc0;
+    if (count == 0) return kSuccess;
+    const int w = cw[0];
     const int nblk_generic = Pp_ / generic_tile_patterns(Sg_, dbl_);
     const int nblk_tc = Pp_ / tc_tile_patterns();
     const int nblk = S_ == 4 ? deriv_blocks(dims()) : std::max(nblk_generic, nblk_tc);

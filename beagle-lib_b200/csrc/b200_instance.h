@@ -95,6 +95,16 @@ public:
     int getSiteLogLikelihoods(double* out);
     int getSiteDerivatives(double* d1, double* d2);
 
+    // For batched calls (b200_batch.cpp).
+    int use_stream(cudaStream_t s);
+    int build_walk(const int* ops, int count, int stride, bool pre, std::vector<OpDesc>& tab,
+                   std::vector<uint8_t>& dep, bool& idempotent, bool& has_op_cum);
+    int build_matrix_jobs(const int* eig, const int* rix, const int* prob, const int* d1,
+                          const int* d2, const double* t, int count, std::vector<MatJob>& jobs);
+    int build_deriv(const int* post, const int* pre, const int* dmat, const int* cw, int count,
+                    std::vector<DerivDesc>& tab);
+    friend class Batch;
+
 private:
     bool is_tip(int b) const { return b >= 0 && b < N_; }
     bool buf_ok(int b) const { return b >= 0 && b < nbuf_; }
@@ -112,7 +122,8 @@ private:
     Dims dims() const { return Dims{S_, Sg_, P_, Pp_, C_}; }
 
     int device_ = 0;
-    cudaStream_t stream_ = nullptr;
+    cudaStream_t stream_ = nullptr;        // where work is queued (own or a batch's)
+    cudaStream_t own_stream_ = nullptr;
     long flags_ = 0;
     bool dbl_ = true, log_scalers_ = true, invevec_t_ = false, pre_auto_ = false;
     bool tc_used_ = false;                 // tensor-core kernels launched (status to check)

@@ -130,4 +130,29 @@ int deriv_blocks(const Dims& d);
 cudaError_t launch_deriv_final(const double* d_block, int nblk, int nb, double* d_sums,
                                cudaStream_t s);
 
+// ---- batched launches over several instances (segment tables on the device;
+// ncta = the segments' total CTAs; see b200_types.h) ------------------------
+// S = 4 walks, one pattern per thread (256-thread CTAs of 256 / C patterns);
+// C in {1, 2, 4, 8}.
+template <typename Real>
+cudaError_t launch_walk4_batch(const WalkSeg* d_segs, int nseg, int ncta, int C, bool pre,
+                               cudaStream_t s);
+// S = 4 edge derivatives (one CTA per deriv4_batch_tile(C) patterns of a branch).
+int deriv4_batch_tile(int C);
+template <typename Real>
+cudaError_t launch_deriv4_batch(const DerivSeg* d_segs, int nseg, int ncta, int C,
+                                cudaStream_t s);
+// Root log-likelihoods (one CTA per reduction_blocks' 128 patterns).
+template <typename Real>
+cudaError_t launch_root_batch(const RootSeg* d_segs, int nseg, int ncta, cudaStream_t s);
+// Scale-factor accumulation (one CTA per accumulate_batch_patterns() patterns).
+int accumulate_batch_patterns();
+cudaError_t launch_accumulate_batch(const AccSeg* d_segs, int nseg, int ncta, cudaStream_t s);
+// Final sums of block partials: one CTA per output (nout in total).
+cudaError_t launch_final_batch(const FinalSeg* d_segs, int nseg, int nout, cudaStream_t s);
+// Pre-order root fills (one CTA per 256 values).
+template <typename Real>
+cudaError_t launch_fill_batch(const FillSeg* d_segs, int nseg, int ncta, cudaStream_t s);
+
 }  // namespace b200
+

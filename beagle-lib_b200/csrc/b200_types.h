@@ -72,4 +72,80 @@ struct MatJob {
     double t;
 };
 
+// ---- batched launches over several instances (b200_batch.cpp) ----------
+// Each launch takes one segment per instance; a CTA finds its segment by
+// binary search over the segments' first_cta (ascending, first one 0).
+
+// One instance's op list in a batched S = 4 walk (one pattern per thread).
+struct WalkSeg {
+    const OpDesc* ops;
+    double* cum;                // cumulative scale buffer of a post-order list, or null
+    int nops;
+    int Pp;
+    int log_scalers;
+    int first_cta;
+};
+
+// One instance's branches in a batched S = 4 edge-derivative launch.
+struct DerivSeg {
+    const DerivDesc* desc;
+    const double* catw;
+    const double* patw;
+    double* block;              // this instance's 2 * nb * nblk block partial sums
+    int nb;
+    int P;
+    int nblk;                   // blocks per branch
+    int first_cta;
+};
+
+// One instance's root log-likelihood in a batched launch (any state count).
+struct RootSeg {
+    const void* root;
+    const double* catw;
+    const double* freqs;
+    const double* cum;          // or null
+    const double* patw;
+    double* site;               // site log-likelihoods [P]
+    double* block;              // block partial sums [nblk]
+    int S, Sg, C, P;
+    int first_cta;
+    int reserved;
+};
+
+// One instance's scale-factor accumulation (optionally after resetting the
+// cumulative buffer) in a batched launch.
+struct AccSeg {
+    double* cum;
+    const double* pool;         // the instance's scale buffers, Pp doubles each
+    const int* idx;             // scale buffer indices to add
+    int n;
+    int Pp;
+    int P;
+    int log_scalers;
+    int reset;
+    int first_cta;
+};
+
+// One instance's pre-order root partials (state frequencies) in a batched fill.
+struct FillSeg {
+    void* dest;
+    const double* freqs;
+    long long n;                // Pp * C * Sg values
+    int S, Sg;
+    int first_cta;
+    int reserved;
+};
+
+// Outputs [first_out, first_out + nout) of a batched final sum: out[k] = sum of
+// the nblk block partials block[k * nblk ...].
+struct FinalSeg {
+    const double* block;
+    double* out;
+    int nblk;
+    int nout;
+    int first_out;
+    int reserved;
+};
+
 }  // namespace b200
+

@@ -274,6 +274,50 @@ __device__ __forceinline__ void deriv4_load(DerivRows4<Real, PPT>& r, const Deri
     }
 }
 
+// Derivative terms of one tile (this thread's PPT patterns p0 + j kRB / C):
+// per-site value into site[b * P + p] when requested, weighted sums into s1, s2.
+template <typename Real, int C, int PPT>
+__device__ __forceinline__ void deriv4_tile(const DerivRows4<Real, PPT>& cur, const Real dm[16],
+                                            Real w, const DerivDesc& dd, bool states, int p0,
+                                            int P, const double* __restrict__ patw, int b,
+                                            double* site, double& s1, double& s2) {
+    constexpr int kSlots = kRB / C;
+    const int c = threadIdx.x % C;
+#pragma unroll
+    for (int j = 0; j < PPT; ++j) {
+        const int p = p0 + j * kSlots;
+        Real n = 0, q = 0;
+        if (states) {
+            const int s = cur.st[j];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                Real dk = (Real)dd.dpad;
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    if (s == i) dk = dm[k * 4 + i];
+                n += cur.z[j][k] * dk;
+                q += (s >= 4 || k == s) ? cur.z[j][k] : Real(0);
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const Real y = dm[k * 4] * cur.x[j][0] + dm[k * 4 + 1] * cur.x[j][1] +
+                               dm[k * 4 + 2] * cur.x[j][2] + dm[k * 4 + 3] * cur.x[j][3];
+                n += cur.z[j][k] * y;
+                q += cur.z[j][k] * cur.x[j][k];
+            }
+        }
+        const Real dr = combine_categories<Real, C>(n, q, w);
+        if (c == 0 && p < P) {
+            const double d = (double)dr;
+            if (site) site[(size_t)b * P + p] = d;
+            const double wp = patw[p];
+            s1 += d * wp;
+            s2 += d * d * wp;
+        }
+    }
+}
+
 template <typename Real, int C, int ITER, int PPT>
 __global__ void __launch_bounds__(kRB)
 k_edge_deriv4(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
@@ -301,39 +345,7 @@ k_edge_deriv4(const DerivDesc* __restrict__ desc, const double* __restrict__ cat
         const int p0 = (t0 + it) * kTile + threadIdx.x / C;
         if (it + 1 < ITER && t0 + it + 1 < ntiles)
             deriv4_load<Real, C, PPT>(nxt, dd, states, p0 + kTile, P, c);
-#pragma unroll
-        for (int j = 0; j < PPT; ++j) {
-            const int p = p0 + j * kSlots;
-            Real n = 0, q = 0;
-            if (states) {
-                const int s = cur.st[j];
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    Real dk = (Real)dd.dpad;
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-                        if (s == i) dk = dm[k * 4 + i];
-                    n += cur.z[j][k] * dk;
-                    q += (s >= 4 || k == s) ? cur.z[j][k] : Real(0);
-                }
-            } else {
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const Real y = dm[k * 4] * cur.x[j][0] + dm[k * 4 + 1] * cur.x[j][1] +
-                                   dm[k * 4 + 2] * cur.x[j][2] + dm[k * 4 + 3] * cur.x[j][3];
-                    n += cur.z[j][k] * y;
-                    q += cur.z[j][k] * cur.x[j][k];
-                }
-            }
-            const Real dr = combine_categories<Real, C>(n, q, w);
-            if (c == 0 && p < P) {
-                const double d = (double)dr;
-                if (site) site[(size_t)b * P + p] = d;
-                const double wp = patw[p];
-                s1 += d * wp;
-                s2 += d * d * wp;
-            }
-        }
+        deriv4_tile<Real, C, PPT>(cur, dm, w, dd, states, p0, P, patw, b, site, s1, s2);
         cur = nxt;
     }
     const int nblk = gridDim.x;
@@ -563,6 +575,116 @@ cudaError_t run_deriv4_bulk(const DerivDesc* desc, int nb, const double* catw,
     return cudaGetLastError();
 }
 
+// ------------------------------------------------- batched reductions
+// One launch for several instances (b200_batch.cpp).  CTA x belongs to the
+// segment whose first_cta is the largest one <= x.
+template <typename Seg>
+__device__ __forceinline__ int find_seg(const Seg* segs, int nseg, int x) {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (segs[mid].first_cta <= x) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// S = 4 edge derivatives of several instances with the same C: CTA (segment,
+// branch b, block k) covers the 2 kRB / C patterns of tile k (two per thread).
+template <typename Real, int C>
+__global__ void __launch_bounds__(kRB)
+k_deriv4_batch(const DerivSeg* __restrict__ segs, int nseg) {
+    __shared__ double sh[kRB / 32];
+    __shared__ int s_seg;
+    constexpr int PPT = 2;
+    constexpr int kTile = kRB / C * PPT;
+    if (threadIdx.x == 0) s_seg = find_seg(segs, nseg, blockIdx.x);
+    __syncthreads();
+    const DerivSeg sg = segs[s_seg];
+    const int local = blockIdx.x - sg.first_cta;
+    const int b = local / sg.nblk, k = local - b * sg.nblk;
+    const int c = threadIdx.x % C;
+    const DerivDesc& dd = sg.desc[b];
+    const Real* D = static_cast<const Real*>(dd.dmat) + c * 16;
+    Real dm[16];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) ld4(D + 4 * q, dm + 4 * q);
+    const Real w = (Real)sg.catw[c];
+    const bool states = dd.post_is_states;
+    const int p0 = k * kTile + threadIdx.x / C;
+    DerivRows4<Real, PPT> cur;
+    deriv4_load<Real, C, PPT>(cur, dd, states, p0, sg.P, c);
+    double s1 = 0, s2 = 0;
+    deriv4_tile<Real, C, PPT>(cur, dm, w, dd, states, p0, sg.P, sg.patw, b, nullptr, s1, s2);
+    double t = block_sum(s1, sh);
+    if (threadIdx.x == 0) sg.block[(size_t)b * sg.nblk + k] = t;
+    t = block_sum(s2, sh);
+    if (threadIdx.x == 0) sg.block[(size_t)(sg.nb + b) * sg.nblk + k] = t;
+}
+
+// Root log-likelihoods of several instances (any state count): CTA (segment,
+// block k) covers patterns [k kRB, (k + 1) kRB).
+template <typename Real>
+__global__ void __launch_bounds__(kRB)
+k_root_batch(const RootSeg* __restrict__ segs, int nseg) {
+    __shared__ double sh[kRB / 32];
+    __shared__ int s_seg;
+    if (threadIdx.x == 0) s_seg = find_seg(segs, nseg, blockIdx.x);
+    __syncthreads();
+    const RootSeg sg = segs[s_seg];
+    const int k = blockIdx.x - sg.first_cta;
+    const int p = k * kRB + threadIdx.x;
+    double v = 0;
+    if (p < sg.P) {
+        double l = log(integrate_site(static_cast<const Real*>(sg.root), sg.catw, sg.freqs, sg.S,
+                                      sg.Sg, sg.C, p));
+        if (sg.cum) l += sg.cum[p];
+        sg.site[p] = l;
+        v = l * sg.patw[p];
+    }
+    const double t = block_sum(v, sh);
+    if (threadIdx.x == 0) sg.block[k] = t;
+}
+
+// cumulative[p] = (reset ? 0 : cumulative[p]) + sum_i f(scale[idx_i][p]) for
+// several instances; 256 patterns per CTA.
+__global__ void k_accumulate_batch(const AccSeg* __restrict__ segs, int nseg) {
+    __shared__ int s_seg;
+    if (threadIdx.x == 0) s_seg = find_seg(segs, nseg, blockIdx.x);
+    __syncthreads();
+    const AccSeg sg = segs[s_seg];
+    const int p = (blockIdx.x - sg.first_cta) * blockDim.x + threadIdx.x;
+    if (p >= sg.P) return;
+    double acc = sg.reset ? 0.0 : sg.cum[p];
+    for (int i = 0; i < sg.n; ++i) {
+        const double v = sg.pool[(size_t)sg.idx[i] * sg.Pp + p];
+        acc += sg.log_scalers ? v : log(v);
+    }
+    sg.cum[p] = acc;
+}
+
+// Final sums of several instances' block partials: one CTA per output.
+__global__ void k_final_batch(const FinalSeg* __restrict__ segs, int nseg) {
+    __shared__ double sh[kRB / 32];
+    __shared__ int s_seg;
+    if (threadIdx.x == 0) {
+        int lo = 0, hi = nseg - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (segs[mid].first_out <= (int)blockIdx.x) lo = mid;
+            else hi = mid - 1;
+        }
+        s_seg = lo;
+    }
+    __syncthreads();
+    const FinalSeg sg = segs[s_seg];
+    const int k = blockIdx.x - sg.first_out;
+    double v = 0;
+    for (int b = threadIdx.x; b < sg.nblk; b += kRB) v += sg.block[(size_t)k * sg.nblk + b];
+    const double t = block_sum(v, sh);
+    if (threadIdx.x == 0) sg.out[k] = t;
+}
+
 __global__ void k_accumulate_scale(double* cum, const double* __restrict__ pool,
                                    const int* __restrict__ idx, int n, int Pp, int p_begin,
                                    int p_end, double sign, int log_scalers) {
@@ -725,6 +847,48 @@ cudaError_t launch_accumulate_scale(double* cum, const double* pool, const int* 
                                                          sign, log_scalers);
     return cudaGetLastError();
 }
+
+int deriv4_batch_tile(int C) { return kRB / C * 2; }
+
+template <typename Real>
+cudaError_t launch_deriv4_batch(const DerivSeg* d_segs, int nseg, int ncta, int C,
+                                cudaStream_t s) {
+    if (nseg == 0 || ncta == 0) return cudaSuccess;
+    switch (C) {
+        case 1: k_deriv4_batch<Real, 1><<<ncta, kRB, 0, s>>>(d_segs, nseg); break;
+        case 2: k_deriv4_batch<Real, 2><<<ncta, kRB, 0, s>>>(d_segs, nseg); break;
+        case 4: k_deriv4_batch<Real, 4><<<ncta, kRB, 0, s>>>(d_segs, nseg); break;
+        case 8: k_deriv4_batch<Real, 8><<<ncta, kRB, 0, s>>>(d_segs, nseg); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <typename Real>
+cudaError_t launch_root_batch(const RootSeg* d_segs, int nseg, int ncta, cudaStream_t s) {
+    if (nseg == 0 || ncta == 0) return cudaSuccess;
+    k_root_batch<Real><<<ncta, kRB, 0, s>>>(d_segs, nseg);
+    return cudaGetLastError();
+}
+
+int accumulate_batch_patterns() { return 256; }
+
+cudaError_t launch_accumulate_batch(const AccSeg* d_segs, int nseg, int ncta, cudaStream_t s) {
+    if (nseg == 0 || ncta == 0) return cudaSuccess;
+    k_accumulate_batch<<<ncta, 256, 0, s>>>(d_segs, nseg);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_final_batch(const FinalSeg* d_segs, int nseg, int nout, cudaStream_t s) {
+    if (nseg == 0 || nout == 0) return cudaSuccess;
+    k_final_batch<<<nout, kRB, 0, s>>>(d_segs, nseg);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_deriv4_batch<float>(const DerivSeg*, int, int, int, cudaStream_t);
+template cudaError_t launch_deriv4_batch<double>(const DerivSeg*, int, int, int, cudaStream_t);
+template cudaError_t launch_root_batch<float>(const RootSeg*, int, int, cudaStream_t);
+template cudaError_t launch_root_batch<double>(const RootSeg*, int, int, cudaStream_t);
 
 #define INST(R)                                                                                  \
     template cudaError_t launch_root_lnl<R>(const void*, const double*, const double*,           \

@@ -17,7 +17,38 @@ __global__ void k_fill_root(Real* dest, const double* __restrict__ freqs, int S,
     dest[idx] = (i < S) ? (Real)freqs[i] : Real(0);
 }
 
+// The same for several instances (b200_batch.cpp): 256 values per CTA.
+template <typename Real>
+__global__ void k_fill_batch(const FillSeg* __restrict__ segs, int nseg) {
+    __shared__ int s_seg;
+    if (threadIdx.x == 0) {
+        int lo = 0, hi = nseg - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (segs[mid].first_cta <= (int)blockIdx.x) lo = mid;
+            else hi = mid - 1;
+        }
+        s_seg = lo;
+    }
+    __syncthreads();
+    const FillSeg sg = segs[s_seg];
+    const long long idx = (long long)(blockIdx.x - sg.first_cta) * blockDim.x + threadIdx.x;
+    if (idx >= sg.n) return;
+    const int i = (int)(idx % sg.Sg);
+    static_cast<Real*>(sg.dest)[idx] = (i < sg.S) ? (Real)sg.freqs[i] : Real(0);
+}
+
 }  // namespace
+
+template <typename Real>
+cudaError_t launch_fill_batch(const FillSeg* d_segs, int nseg, int ncta, cudaStream_t s) {
+    if (nseg == 0 || ncta == 0) return cudaSuccess;
+    k_fill_batch<Real><<<ncta, 256, 0, s>>>(d_segs, nseg);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_fill_batch<float>(const FillSeg*, int, int, cudaStream_t);
+template cudaError_t launch_fill_batch<double>(const FillSeg*, int, int, cudaStream_t);
 
 template <typename Real>
 cudaError_t launch_fill_root(void* dest, const double* freqs, const Dims& d, cudaStream_t s) {

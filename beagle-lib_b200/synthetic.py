@@ -241,6 +241,13 @@ class Problem:
                 self.C, self.n_scale)
 
     def post_ops(self):
+        """Post-order ops (dest, write scale, read scale, child 1, its matrix,
+        child 2, its matrix); built once per problem (the topology is fixed)."""
+        if getattr(self, "_post_ops", None) is None:
+            self._post_ops = self._build_post_ops()
+        return self._post_ops.copy()
+
+    def _build_post_ops(self):
         ops = []
         for v in postorder(self.children, self.root):
             c1, c2 = (int(x) for x in self.children[v])
@@ -251,7 +258,13 @@ class Problem:
     def pre_ops(self, transposed_matrices=False):
         """Pre-order ops (dest, write, read, pre(parent), P_node, sibling, P_sib).
         With ``transposed_matrices`` the node's matrix index points at its
-        transposed copy (B + 1 + v)."""
+        transposed copy (B + 1 + v).  Built once per problem and flag."""
+        cache = self.__dict__.setdefault("_pre_ops", {})
+        if transposed_matrices not in cache:
+            cache[transposed_matrices] = self._build_pre_ops(transposed_matrices)
+        return cache[transposed_matrices].copy()
+
+    def _build_pre_ops(self, transposed_matrices):
         ops = []
         for v in preorder_nonroot(self.children, self.root):
             p = int(self.parent[v])
@@ -421,3 +434,41 @@ def batched_problems(count=256, seed=2000, max_patterns=50000):
         out.append(make_problem(S=S, N=N, P=P, C=C, seed=seed + 1 + i,
                                 mean_length=0.1, rescale=True, name=f"part{i}"))
     return out
+
+
+def batch_evaluate(batch, problems, lengths=None):
+    """One lnL + gradient evaluation of every problem of a batch (members in
+    the same order), the call sequence of Problem.evaluate with one batched
+    call per step.  S > 4 members need PREORDER_TRANSPOSE_AUTO (their pre-order
+    ops carry untransposed matrices).  Returns (lnL[n], [gradient_m])."""
+    plan = getattr(batch, "_plan", None)
+    if plan is None or plan["problems"] is not problems:
+        n = len(problems)
+        resc = [p.rescale for p in problems]
+        if any(resc) and not all(resc):
+            raise ValueError("a batch rescales all members or none")
+        nonroot = [np.arange(p.B, dtype=np.int32) for p in problems]
+        plan = batch._plan = dict(
+            problems=problems, n=n, rescale=all(resc),
+            idx=nonroot, post=[p.post_ops() for p in problems],
+            pre=[p.pre_ops(False) for p in problems],
+            cums=[p.cumulative if p.rescale else OP_NONE for p in problems],
+            scales=[np.arange(p.N - 1, dtype=np.int32) for p in problems],
+            roots=[p.root for p in problems], roots_pre=[p.pre(p.root) for p in problems],
+            pre_idx=[nr + p.pre(0) for nr, p in zip(nonroot, problems)],
+            dmat=[np.full(p.B, p.B, dtype=np.int32) for p in problems], zeros=[0] * n,
+            none=[OP_NONE] * n)
+    n = plan["n"]
+    ts = [p.lengths if lengths is None else lengths[i] for i, p in enumerate(problems)]
+    batch.updateTransitionMatrices(plan["zeros"], plan["idx"], ts)
+    batch.updatePartials(plan["post"], plan["none"])
+    if plan["rescale"]:
+        batch.accumulateScaleFactors(plan["scales"], plan["cums"], reset=True)
+    lnl = batch.calculateRootLogLikelihoods(plan["roots"], plan["zeros"], plan["zeros"],
+                                            plan["cums"])
+    batch.setRootPrePartials(plan["roots_pre"], plan["zeros"])
+    batch.updatePrePartials(plan["pre"])
+    sums, _ = batch.calculateEdgeDerivatives(plan["idx"], plan["pre_idx"], plan["dmat"],
+                                             plan["zeros"])
+    batch.wait()
+    return lnl, sums

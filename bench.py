@@ -43,7 +43,8 @@ SCALERS_LOG = 1 << 10
 THREADING_CPP = 1 << 30
 PROC_CPU, PROC_GPU = 1 << 15, 1 << 16
 FW_CUDA, FW_CPU = 1 << 22, 1 << 27
-PRE_MANUAL = 1 << 30
+PRE_MANUAL, PRE_AUTO = 1 << 30, 1 << 31
+BATCH_WORKLOAD = "batch256"
 
 # Our kernels launched per evaluation: P(t) 1, post-order 1, scale accumulate 1,
 # root lnL 2 (sites + final sum), root pre-partials fill 1, pre-order 1,
@@ -239,8 +240,9 @@ def run_reference_arm(args):
 
 
 # ----------------------------------------------------------------- GPU side
-def make_instance(lib, pr, precision, device, asynch=True):
-    pref = (SINGLE if precision == "single" else DOUBLE) | SCALERS_LOG | PROC_GPU | PRE_MANUAL
+def make_instance(lib, pr, precision, device, asynch=True, auto_transpose=False):
+    pref = (SINGLE if precision == "single" else DOUBLE) | SCALERS_LOG | PROC_GPU
+    pref |= PRE_AUTO if auto_transpose else PRE_MANUAL
     if asynch:
         pref |= ASYNCH
     req = (SINGLE if precision == "single" else DOUBLE) | FW_CUDA
@@ -410,12 +412,99 @@ def run_b200_arm(args):
         dist.destroy_process_group()
 
 
+def run_batch_arm(args):
+    """--workload batch256: 256 independent trees as the batched multi-instance
+    configuration draws them (16-256 taxa, 4 or 20 states, 1/4/8 categories),
+    with patterns log-uniform in 100-10,000 instead of 100-50,000 so that the
+    FP64 instances (101 GB of partials) fit one GPU.  One step evaluates lnL and
+    the full gradient of every tree.  value: tree-evals/s of the mixed path
+    through the batched calls (one launch per kernel family and category
+    count); per_instance_mixed / plain_fp64: the same trees evaluated one
+    instance at a time (each instance's own launches) on one shared stream.
+    All device-timed with CUDA events on that stream."""
+    import torch
+    pkg = importlib.import_module("beagle-lib_b200")
+    syn = pkg.synthetic
+    lib = pkg.load()
+    probs = syn.batched_problems(count=256, seed=2000, max_patterns=10000)
+    n = len(probs)
+
+    def instances(precision):
+        return [make_instance(lib, pr, precision, 0, asynch=True, auto_transpose=pr.S > 4)
+                for pr in probs]
+
+    def timed(stream, body, steps, warmup):
+        for _ in range(warmup):
+            body()
+        torch.cuda.synchronize()
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(steps):
+            body()
+        end.record(stream)
+        end.synchronize()
+        return start.elapsed_time(end)
+
+    def per_instance(insts):
+        for pr, inst in zip(probs, insts):
+            pr.evaluate(inst, transposed_pre=False)
+
+    steps = max(3, min(args.steps, 20))
+    warmup = max(3, args.warmup)
+    insts = instances("single")
+    batch = pkg.binding.Batch(lib, insts)
+    stream = torch.cuda.ExternalStream(insts[0].cudaStream())
+    state = {}
+
+    def batched():
+        state["lnl"], _ = syn.batch_evaluate(batch, probs)
+
+    ms_b = timed(stream, batched, steps, warmup)
+    ms_i = timed(stream, lambda: per_instance(insts), max(2, steps // 2), 1)
+    lnl32 = np.array(state["lnl"])
+    batch.finalize()
+    for x in insts:
+        x.finalize()
+    del insts, batch
+    insts = instances("double")
+    batch = pkg.binding.Batch(lib, insts)        # only to share one stream
+    stream = torch.cuda.ExternalStream(insts[0].cudaStream())
+    ms_64 = timed(stream, lambda: per_instance(insts), max(2, steps // 2), 1)
+    lnl64 = np.array([x.getLogLikelihood() for x in insts])
+    batch.finalize()
+    for x in insts:
+        x.finalize()
+    value = n * steps / (ms_b / 1000.0)
+    v_i = n * max(2, steps // 2) / (ms_i / 1000.0)
+    v_64 = n * max(2, steps // 2) / (ms_64 / 1000.0)
+    rel_err = float(np.max(np.abs(lnl32 - lnl64) / np.abs(lnl64)))
+    line = {
+        "metric": "tree lnL+gradient evals/s, 256-tree batch, mixed batched vs per-instance",
+        "value": value, "unit": "tree-evals/s", "n_gpus": 1, "steps": steps, "warmup": warmup,
+        "ms_per_step": ms_b / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": BATCH_WORKLOAD, "trees": n,
+                   "patterns_total": int(sum(p.P for p in probs)),
+                   "states": {"4": sum(p.S == 4 for p in probs),
+                              "20": sum(p.S == 20 for p in probs)},
+                   "patterns": "log-uniform 100-10,000 (configuration: 100-50,000)"},
+        "per_instance_mixed": {"value": v_i, "unit": "tree-evals/s"},
+        "plain_fp64": {"value": v_64, "unit": "tree-evals/s", "batched_mixed_over_fp64": value / v_64,
+                       "mixed_vs_fp64_max_rel_lnl_err": rel_err},
+        "gpu_launches": None,
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference_arm(args)
     elif args.profile:
         run_profile_case(args)
+    elif args.workload == BATCH_WORKLOAD:
+        run_batch_arm(args)
     else:
         run_b200_arm(args)
 

@@ -348,6 +348,73 @@ int beagleB200RootLogLikelihoodsNoAlloc(int device, void* stream, const void* ro
                                         double* outSiteLogLikelihoods,
                                         double* outSumLogLikelihood);
 
+/* ---- batches of instances (no beagle.h counterpart) ------------------
+ * Many independent trees or partitions of uneven pattern and state counts,
+ * one instance each, evaluated with a handful of launches per step instead of
+ * one launch chain per instance.  A batch groups instances of one precision on
+ * one device; while it exists they share one CUDA stream, so batch calls and
+ * their single-instance calls stay ordered.  Per-member arguments are arrays
+ * indexed by member position (the order of `instances` at creation); pointer
+ * arrays hold one pointer per member.  Each member's arguments are validated
+ * and mean what the single-instance call's arguments mean; an error in any
+ * member returns its code before anything is queued for the rest of that
+ * call's batched launches.
+ *
+ * Launches: transition matrices, one per (states, categories) group; post-
+ * and pre-order walks and edge derivatives, one per category count for the
+ * 4-state members (1, 2, 4 or 8 categories), the other members' own launches
+ * otherwise; scale accumulation, root pre-partials, root log-likelihoods and
+ * the final derivative sums, one each for all members. */
+/* Returns the batch index (>= 0) or a negative code. */
+int beagleB200CreateBatch(const int* instances, int count);
+/* Members return to their own streams; the instances stay valid. */
+int beagleB200FinalizeBatch(int batch);
+/* beagleUpdateTransitionMatrices for every member: eigenIndices[m],
+ * probabilityIndices[m][count[m]], edgeLengths[m][count[m]] (no derivative
+ * matrices). */
+int beagleB200BatchUpdateTransitionMatrices(int batch, const int* eigenIndices,
+                                            const int* const* probabilityIndices,
+                                            const double* const* edgeLengths,
+                                            const int* counts);
+/* beagleUpdatePartials for every member (7-int operations). */
+int beagleB200BatchUpdatePartials(int batch, const int* const* operations,
+                                  const int* operationCounts,
+                                  const int* cumulativeScaleIndices);
+/* beagleUpdatePrePartials for every member. */
+int beagleB200BatchUpdatePrePartials(int batch, const int* const* operations,
+                                     const int* operationCounts);
+/* beagleAccumulateScaleFactors for every member, after zeroing its cumulative
+ * buffer first when `reset` is nonzero (beagleResetScaleFactors). */
+int beagleB200BatchAccumulateScaleFactors(int batch, const int* const* scaleIndices,
+                                          const int* counts,
+                                          const int* cumulativeScaleIndices, int reset);
+/* beagleSetRootPrePartials for every member (one buffer each). */
+int beagleB200BatchSetRootPrePartials(int batch, const int* bufferIndices,
+                                      const int* stateFrequenciesIndices);
+/* beagleCalculateRootLogLikelihoods for every member (one root each);
+ * outSumLogLikelihoods[m].  Waits for the results, unless every member was
+ * created with BEAGLE_B200_FLAG_COMPUTATION_ASYNCH: then the values are
+ * written at beagleB200BatchWait, and the array must stay valid until then. */
+int beagleB200BatchCalculateRootLogLikelihoods(int batch, const int* bufferIndices,
+                                               const int* categoryWeightsIndices,
+                                               const int* stateFrequenciesIndices,
+                                               const int* cumulativeScaleIndices,
+                                               double* outSumLogLikelihoods);
+/* beagleCalculateEdgeDerivatives for every member (sums only):
+ * outSumDerivatives[m][counts[m]], outSumSquaredDerivatives[m][counts[m]]
+ * (either may be NULL per member).  Waits for the results, or defers them to
+ * beagleB200BatchWait as beagleB200BatchCalculateRootLogLikelihoods does. */
+int beagleB200BatchCalculateEdgeDerivatives(int batch, const int* const* postBufferIndices,
+                                            const int* const* preBufferIndices,
+                                            const int* const* derivativeMatrixIndices,
+                                            const int* categoryWeightsIndices,
+                                            const int* counts,
+                                            double* const* outSumDerivatives,
+                                            double* const* outSumSquaredDerivatives);
+/* Wait for everything queued on the batch's stream and write the deferred
+ * results of ASYNCH members. */
+int beagleB200BatchWait(int batch);
+
 #ifdef __cplusplus
 }
 #endif

@@ -46,6 +46,7 @@ def test_header_compiles_as_c(tmp_path):
 
 def test_binding_table_covers_header(pkg):
     bound = set("beagleB200" + n for n in pkg.binding._SIGS)
+    bound |= set("beagleB200" + n for n in pkg.binding._BATCH_SIGS)
     bound |= {"beagleB200CreateInstance", "beagleB200GetResourceList", "beagleB200GetVersion"}
     # bound directly by its own test (raw device pointers, no instance)
     bound |= {"beagleB200RootLogLikelihoodsNoAlloc"}

@@ -1,0 +1,73 @@
+"""Batched calls (beagleB200Batch*): a heterogeneous batch of trees (4 and
+20 states; 1, 3, 4 and 8 categories; uneven tree sizes and pattern counts)
+evaluated with one batched call per step, against the same problems evaluated
+one instance at a time and against the oracle."""
+import numpy as np
+import pytest
+
+from helpers import TOL, grad_err, gpu_flags, rel, run_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _problems(syn):
+    probs = syn.batched_problems(count=10, seed=7, max_patterns=3000)
+    # members the batched kernels do not take (3 categories; 20 states) run
+    # their single-instance launches on the batch's stream
+    probs.append(syn.make_problem(S=4, N=11, P=500, C=3, seed=3, rescale=True))
+    probs.append(syn.make_problem(S=20, N=9, P=300, C=4, seed=4, rescale=True))
+    return probs
+
+
+def _create(b200, pr, precision, asynch=False):
+    pref, req = gpu_flags(precision, auto_transpose=True)
+    if asynch:
+        pref |= 1 << 3                      # BEAGLE_FLAG_COMPUTATION_ASYNCH
+    inst = b200.create(*pr.create_args(), preferenceFlags=pref, requirementFlags=req)
+    pr.load(inst)
+    return inst
+
+
+@pytest.mark.parametrize("asynch", [False, True], ids=["synch", "asynch"])
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_batch_matches_single_instances_and_oracle(b200, pkg, syn, oracle, precision, asynch):
+    """ASYNCH members: the batched result calls defer their values to
+    beagleB200BatchWait (batch_evaluate calls it at the end of a step)."""
+    probs = _problems(syn)
+    singles = [_create(b200, pr, precision) for pr in probs]
+    ref = [pr.evaluate(inst, transposed_pre=False) for pr, inst in zip(probs, singles)]
+    members = [_create(b200, pr, precision, asynch) for pr in probs]
+    batch = pkg.binding.Batch(b200, members)
+    for rep in range(2):                    # the second pass reuses the batch's tables
+        lnl, grads = syn.batch_evaluate(batch, probs)
+        tol = TOL[precision]
+        for k, (pr, (l1, g1)) in enumerate(zip(probs, ref)):
+            assert rel(lnl[k], l1) <= (1e-12 if precision == "double" else tol["lnl"]), k
+            assert grad_err(grads[k], g1) <= (1e-10 if precision == "double" else tol["grad"]), k
+    for k in (0, 3, len(probs) - 1):
+        _, lo, go = run_oracle(oracle, probs[k])
+        assert rel(lnl[k], lo) <= TOL[precision]["lnl"]
+        assert grad_err(grads[k], go) <= TOL[precision]["grad"]
+    batch.finalize()
+    # members work on their own streams again (an ASYNCH instance delivers
+    # its lnL through getLogLikelihood)
+    l_after, _ = probs[0].evaluate(members[0], transposed_pre=False)
+    if asynch:
+        l_after = members[0].getLogLikelihood()
+    assert rel(l_after, ref[0][0]) <= 1e-6
+    for x in singles + members:
+        x.finalize()
+
+
+def test_batch_rejects_bad_members(b200, pkg, syn):
+    pr = syn.make_problem(S=4, N=6, P=100, C=2, seed=1)
+    a = _create(b200, pr, "double")
+    b = _create(b200, pr, "single")
+    with pytest.raises(pkg.binding.BeagleError):
+        pkg.binding.Batch(b200, [a, b])          # mixed precision
+    batch = pkg.binding.Batch(b200, [a])
+    with pytest.raises(pkg.binding.BeagleError):
+        pkg.binding.Batch(b200, [a])             # already in a batch
+    batch.finalize()
+    a.finalize()
+    b.finalize()
