@@ -22,6 +22,7 @@ _p = ctypes.c_void_p
 
 # name -> argtypes (all return int unless listed in _RESTYPES)
 _SIGS = {
+    "BeginCapture": [_i], "EndCapture": [_i, _p], "LaunchGraph": [_i, _i],
     "FinalizeInstance": [_i],
     "Finalize": [],
     "SetCPUThreadCount": [_i, _i],
@@ -174,6 +175,8 @@ class Instance:
         self.impl_name = info.implName.decode() if info.implName else ""
         self.flags = info.flags
         self._keep = []           # output arrays an ASYNCH instance fills at its next sync
+        self._graph_keep = []     # ... and those a captured graph fills at every launch
+        self._capturing = False
         self.__dict__.update(dims)
 
     def _call(self, name, *args, check=True):
@@ -187,6 +190,21 @@ class Instance:
             self.finalize()
         except Exception:
             pass
+
+    # CUDA graphs (ASYNCH instances)
+    def beginCapture(self):
+        code = self._call("BeginCapture")
+        self._capturing = True
+        return code
+
+    def endCapture(self):
+        g = np.full(1, -1, dtype=np.int32)
+        self._capturing = False
+        self._call("EndCapture", _ptr(g))
+        return int(g[0])
+
+    def launchGraph(self, graph):
+        return self._call("LaunchGraph", graph)
 
     def finalize(self):
         if self.h is not None and self.h >= 0:
@@ -374,7 +392,7 @@ class Instance:
         o3 = np.zeros(n) if sumsq else None
         self._call("CalculateEdgeDerivatives", _ptr(a), _ptr(b), _ptr(d), _ptr(w), n,
                    _ptr(o1), _ptr(o2), _ptr(o3), check=check)
-        self._keep.append((o2, o3))
+        (self._graph_keep if self._capturing else self._keep).append((o2, o3))
         return (None if o1 is None else o1.reshape(n, self.patternCount)), o2, o3
 
     def calculateEdgeLogLikelihoods(self, parent, child, prob, d1, d2, cw, sf, cum,

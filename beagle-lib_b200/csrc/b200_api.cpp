@@ -508,4 +508,16 @@ int beagleB200BatchWait(int batch) {
     return call_batch(batch, [&](b200::Batch* b) { return b->wait(); });
 }
 
+int beagleB200BeginCapture(int instance) {
+    return call(instance, [&](b200::Instance* in) { return in->beginCapture(); });
+}
+
+int beagleB200EndCapture(int instance, int* graph) {
+    return call(instance, [&](b200::Instance* in) { return in->endCapture(graph); });
+}
+
+int beagleB200LaunchGraph(int instance, int graph) {
+    return call(instance, [&](b200::Instance* in) { return in->launchGraph(graph); });
+}
+
 }  // extern "C"

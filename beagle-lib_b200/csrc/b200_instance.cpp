@@ -58,11 +58,27 @@ cudaError_t DevBuf::reserve(size_t n) {
     return e;
 }
 
+// While this thread captures a CUDA graph (Instance::beginCapture), uploads
+// copy through pinned blocks that the graph keeps: a captured copy node reads
+// its source at every launch.
+namespace {
+thread_local std::vector<void*>* t_capture_pinned = nullptr;
+}
+
 cudaError_t DevBuf::upload(const void* src, size_t n, cudaStream_t s) {
     cudaError_t e = reserve(n);
     if (e != cudaSuccess) return e;
     if (last.size() == n && n > 0 && std::memcmp(last.data(), src, n) == 0) return cudaSuccess;
-    e = cudaMemcpyAsync(ptr, src, n, cudaMemcpyHostToDevice, s);
+    if (t_capture_pinned) {
+        void* h = nullptr;
+        e = cudaMallocHost(&h, n);
+        if (e != cudaSuccess) return e;
+        t_capture_pinned->push_back(h);
+        std::memcpy(h, src, n);
+        e = cudaMemcpyAsync(ptr, h, n, cudaMemcpyHostToDevice, s);
+    } else {
+        e = cudaMemcpyAsync(ptr, src, n, cudaMemcpyHostToDevice, s);
+    }
     if (e == cudaSuccess) last.assign((const uint8_t*)src, (const uint8_t*)src + n);
     return e;
 }
@@ -77,7 +93,17 @@ void DevBuf::release() {
 // -------------------------------------------------------------- lifetime
 Instance::~Instance() {
     cudaSetDevice(device_);
+    if (capturing_) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(stream_, &g);
+        if (g) cudaGraphDestroy(g);
+        t_capture_pinned = nullptr;
+        capturing_ = false;
+        (void)cudaGetLastError();
+    }
     if (stream_) cudaStreamSynchronize(stream_);
+    for (GraphRec& g : graphs_) free_graph(g);
+    free_graph(cap_);
     for (void* p : owned_) cudaFree(p);
     void* bufs[] = {d_part_pool_, d_mat_, d_mat_t_, d_scale_, d_cube_, d_evals_, d_rates_,
                     d_catw_, d_freqs_, d_patw_, d_site_, d_site1_, d_site2_};
@@ -201,6 +227,65 @@ int Instance::create(int tipCount, int partialsBufferCount, int compactBufferCou
     return sync();
 }
 
+// A deferred result: delivered at the next sync, or, while capturing, at
+// every launch of the captured graph.
+void Instance::defer(const Pending& pd) {
+    if (capturing_) cap_.deliveries.push_back(pd);
+    else pending_.push_back(pd);
+}
+
+// Capture the work of the following calls into a CUDA graph instead of
+// running it (ASYNCH instances; calls that wait for results are refused while
+// capturing).  Call the same sequence once before capturing, so that every
+// device table already has its size and contents: a table that changes is
+// uploaded through a pinned copy the graph keeps.
+int Instance::beginCapture() {
+    if (capturing_ || !async_) return kErrGeneral;
+    int rc = sync();
+    if (rc) return rc;
+    cap_ = GraphRec{};
+    CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed));
+    capturing_ = true;
+    t_capture_pinned = &cap_.pinned;
+    return kSuccess;
+}
+
+int Instance::endCapture(int* graph) {
+    if (!capturing_ || !graph) return kErrGeneral;
+    capturing_ = false;
+    t_capture_pinned = nullptr;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(stream_, &g);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&cap_.exec, g, 0ULL);
+    cap_.graph = g;
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        free_graph(cap_);
+        return kErrGeneral;
+    }
+    graphs_.push_back(cap_);
+    cap_ = GraphRec{};
+    *graph = (int)graphs_.size() - 1;
+    return kSuccess;
+}
+
+// Launch a captured graph on the instance's stream; its deferred results
+// are delivered at the next sync as the captured calls' would be.
+int Instance::launchGraph(int graph) {
+    if (capturing_ || graph < 0 || graph >= (int)graphs_.size() || !graphs_[graph].exec)
+        return kErrRange;
+    CK(cudaGraphLaunch(graphs_[graph].exec, stream_));
+    for (const Pending& pd : graphs_[graph].deliveries) pending_.push_back(pd);
+    return kSuccess;
+}
+
+void Instance::free_graph(GraphRec& g) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+    for (void* p : g.pinned) cudaFreeHost(p);
+    g = GraphRec{};
+}
+
 // Queue this instance's work on `s` (a batch's stream) from now on, after
 // everything queued so far; nullptr returns to the instance's own stream.
 int Instance::use_stream(cudaStream_t s) {
@@ -210,6 +295,7 @@ int Instance::use_stream(cudaStream_t s) {
 }
 
 int Instance::sync() {
+    if (capturing_) return kErrGeneral;   // a wait would break the capture
     if (tc_used_) CK(tc_status_async(h_tc_status_, stream_));
     if (bulk_used_) CK(bulk_status_async(h_tc_status_ + 1, stream_));
     CK(cudaStreamSynchronize(stream_));
@@ -241,6 +327,16 @@ int Instance::sync() {
 // n doubles of pinned staging, valid until the next sync(); chunks are kept
 // and reused, a new one is allocated only when the queued results outgrow them.
 double* Instance::stage(size_t n) {
+    if (capturing_) {
+        // a captured copy writes here at every launch of the graph
+        double* p = nullptr;
+        if (cudaMallocHost(&p, sizeof(double) * n) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return nullptr;
+        }
+        cap_.pinned.push_back(p);
+        return p;
+    }
     while (chunk_i_ < chunks_.size() && chunk_off_ + n > chunks_[chunk_i_].second) {
         ++chunk_i_;
         chunk_off_ = 0;
@@ -825,7 +921,7 @@ int Instance::calculateRootLogLikelihoods(const int* bufs, const int* cw, const 
         double* slot = stage(1);
         if (!slot) return kErrOOM;
         CK(cudaMemcpyAsync(slot, out_.ptr, sizeof(double), cudaMemcpyDeviceToHost, stream_));
-        pending_.push_back(Pending{slot, nullptr, nullptr, 0});
+        defer(Pending{slot, nullptr, nullptr, 0});
         return kSuccess;
     }
     CK(cudaMemcpyAsync(h_out_, out_.ptr, sizeof(double), cudaMemcpyDeviceToHost, stream_));
@@ -976,7 +1072,7 @@ int Instance::calculateEdgeDerivatives(const int* post, const int* pre, const in
         if (!slot) return kErrOOM;
         CK(cudaMemcpyAsync(slot, out_.ptr, sizeof(double) * 2 * count, cudaMemcpyDeviceToHost,
                            stream_));
-        pending_.push_back(Pending{slot, outSum, outSumSq, count});
+        defer(Pending{slot, outSum, outSumSq, count});
         return kSuccess;
     }
     if ((size_t)2 * count > h_out_n_) {

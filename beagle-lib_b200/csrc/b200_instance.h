@@ -95,6 +95,11 @@ public:
     int getSiteLogLikelihoods(double* out);
     int getSiteDerivatives(double* d1, double* d2);
 
+    // CUDA graphs of an ASYNCH instance's work (beagleB200BeginCapture ...).
+    int beginCapture();
+    int endCapture(int* graph);
+    int launchGraph(int graph);
+
     // For batched calls (b200_batch.cpp).
     int use_stream(cudaStream_t s);
     int build_walk(const int* ops, int count, int stride, bool pre, std::vector<OpDesc>& tab,
@@ -170,6 +175,19 @@ private:
         int count;                // edge-derivative branches (0: a log-likelihood)
     };
     std::vector<Pending> pending_;
+    // A captured graph: its executable, the deliveries its copies feed and the
+    // pinned blocks those copies (and its table uploads) use.
+    struct GraphRec {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        std::vector<Pending> deliveries;
+        std::vector<void*> pinned;
+    };
+    std::vector<GraphRec> graphs_;
+    GraphRec cap_;
+    bool capturing_ = false;
+    void defer(const Pending& pd);
+    void free_graph(GraphRec& g);
     std::vector<std::pair<double*, size_t>> chunks_;
     size_t chunk_i_ = 0, chunk_off_ = 0;
 

@@ -310,7 +310,7 @@ class Problem:
         inst.setTransitionMatrix(self.B, self.scaled_q().reshape(-1), 0.0)
 
     def evaluate(self, inst, gradient=True, transposed_pre=False, lengths=None, mark=None):
-        """One lnL (+ gradient) evaluation: the call sequence of BASELINE's metric.
+        """One lnL (+ gradient) evaluation: the call sequence the benchmark times.
 
         updateTransitionMatrices (all B branches) -> updatePartials (N-1 ops) ->
         scale accumulation -> root lnL -> root pre-partials -> updatePrePartials
@@ -322,6 +322,10 @@ class Problem:
         mark("start")
         inst.updateTransitionMatrices(0, idx, None, None, t)
         mark("matrices")
+        return self._after_matrices(inst, gradient, transposed_pre, mark)
+
+    def _after_matrices(self, inst, gradient, transposed_pre, mark):
+        idx = np.arange(self.B, dtype=np.int32)
         inst.updatePartials(self.post_ops(), OP_NONE)
         mark("post")
         cum = OP_NONE
@@ -346,6 +350,29 @@ class Problem:
             [0], per_site=False, sums=True, sumsq=False)
         mark("deriv")
         return lnl, sums
+
+    def capture(self, inst, transposed_pre=False):
+        """Record one evaluation after the transition matrices (partials,
+        scaling, root lnL, pre-order partials, edge derivatives) as a CUDA
+        graph of an ASYNCH instance; returns (graph, gradient array the graph
+        fills).  Runs the sequence once first, as the capture requires."""
+        self.evaluate(inst, transposed_pre=transposed_pre)
+        inst.getLogLikelihood()
+        inst.beginCapture()
+        try:
+            _, grad = self._after_matrices(inst, True, transposed_pre, lambda name: None)
+        finally:
+            graph = inst.endCapture()
+        return graph, grad
+
+    def evaluate_graph(self, inst, graph, grad, lengths=None):
+        """One evaluation through a captured graph: new transition matrices
+        (outside the graph), the graph, then lnL and the gradient."""
+        t = self.lengths if lengths is None else lengths
+        inst.updateTransitionMatrices(0, np.arange(self.B, dtype=np.int32), None, None, t)
+        inst.launchGraph(graph)
+        lnl = inst.getLogLikelihood()            # waits; delivers the gradient too
+        return lnl, grad
 
     def algorithmic_bytes(self, w):
         """Compulsory traffic per phase of one evaluation, with w bytes per real:

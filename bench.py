@@ -310,6 +310,28 @@ def timed_e2e(torch, inst, pr, steps):
     return start.elapsed_time(end), h2d, d2h
 
 
+def timed_e2e_graph(torch, inst, pr, steps):
+    """As timed_e2e, with everything after the transition matrices replayed
+    from a CUDA graph captured once (beagleB200BeginCapture / LaunchGraph)."""
+    stream = torch.cuda.ExternalStream(inst.cudaStream())
+    graph, grad = pr.capture(inst, transposed_pre=pr.S > 4)
+    rng = np.random.default_rng(7)
+    lengths = torch.empty(pr.B, dtype=torch.float64).pin_memory()
+    host = lengths.numpy()
+    for _ in range(2):
+        pr.evaluate_graph(inst, graph, grad)
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    inst.waitForPartials([])
+    start.record(stream)
+    for _ in range(steps):
+        host[:] = pr.lengths * (1.0 + 1e-3 * rng.standard_normal(pr.B))
+        pr.evaluate_graph(inst, graph, grad, lengths=host)
+    end.record(stream)
+    end.synchronize()
+    return start.elapsed_time(end)
+
+
 def run_profile_case(args):
     """The workload's tree and model on --profile-patterns patterns (default
     20,000: partials larger than L2, a few hundred MB on the device), mixed
@@ -362,6 +384,8 @@ def run_b200_arm(args):
     ms_e2e, h2d, d2h = timed_e2e(torch, inst, pr, max(5, args.steps // 5))
     e2e_steps = max(5, args.steps // 5)
     e2e_value = ws * e2e_steps / (max_over_ranks(ms_e2e, ws) / 1000.0)
+    ms_graph = timed_e2e_graph(torch, inst, pr, e2e_steps)
+    e2e_graph_value = ws * e2e_steps / (max_over_ranks(ms_graph, ws) / 1000.0)
     inst.finalize()
 
     # the plain FP64 path (one instance, same workload) for the mixed/FP64 ratio
@@ -399,6 +423,8 @@ def run_b200_arm(args):
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
+            "e2e_graph": {"value": e2e_graph_value, "unit": "evals/s",
+                          "how": "same steps, post-matrix work replayed from a CUDA graph"},
             "plain_fp64": {"value": value64, "unit": "evals/s", "ms_per_step": ms64 / k64,
                            "mixed_over_fp64": value / value64,
                            "mixed_vs_fp64_rel_lnl_err": rel_err},

@@ -348,6 +348,25 @@ int beagleB200RootLogLikelihoodsNoAlloc(int device, void* stream, const void* ro
                                         double* outSiteLogLikelihoods,
                                         double* outSumLogLikelihood);
 
+/* ---- CUDA graphs of an instance's work (no beagle.h counterpart) ------
+ * Between BeginCapture and EndCapture the calls on an ASYNCH instance
+ * (BEAGLE_B200_FLAG_COMPUTATION_ASYNCH) are recorded into a CUDA graph instead
+ * of running; LaunchGraph replays the recorded work on the instance's stream,
+ * and the recorded result calls deliver again at the next synchronisation
+ * point (getters, waitForPartials, synchronous calls), into the same caller
+ * arrays, which must stay valid.  Calls that wait for results are refused with
+ * BEAGLE_B200_ERROR_GENERAL while capturing.  Make the same calls once before
+ * capturing so that every device table already has its size and contents;
+ * argument tables that differ are copied through pinned memory the graph
+ * keeps.  Typical use: capture partials, scaling, root lnL, pre-order partials
+ * and edge derivatives once, then per step update the transition matrices
+ * (outside the graph) and launch the graph.  Graphs live until the instance
+ * is finalized. */
+int beagleB200BeginCapture(int instance);
+/* Returns the graph index in *graph. */
+int beagleB200EndCapture(int instance, int* graph);
+int beagleB200LaunchGraph(int instance, int graph);
+
 /* ---- batches of instances (no beagle.h counterpart) ------------------
  * Many independent trees or partitions of uneven pattern and state counts,
  * one instance each, evaluated with a handful of launches per step instead of
