@@ -2,13 +2,14 @@
 
 ``load()`` opens the native C-ABI library ``lib/libbeagle_b200.so`` (built
 in-tree by ``build.py``) through :mod:`.binding`; the seeded workloads and the
-lnL + gradient call sequence live in :mod:`.synthetic`.  There is no CPU
+lnL + gradient call sequence live in :mod:`.synthetic`; the subtree
+checkpointed schedule for trees whose partials do not fit in :mod:`.checkpoint`.  There is no CPU
 fallback: without the built library, or without an sm_100 device,
 ``load()`` / instance creation raise.
 """
 import os
 
-from . import binding, synthetic  # noqa: F401
+from . import binding, checkpoint, synthetic  # noqa: F401
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libbeagle_b200.so")

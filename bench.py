@@ -332,6 +332,55 @@ def timed_e2e_graph(torch, inst, pr, steps):
     return start.elapsed_time(end)
 
 
+def timed_checkpointed(torch, lib, pr, device, steps, ref_lnl, ref_grad):
+    """lnL + gradient with subtree checkpointing of the post-order partials
+    (beagle-lib_b200/checkpoint.py, the plan with the fewest buffers), captured
+    as one CUDA graph and timed as timed_e2e_graph times the full schedule.
+    Returns the summary object of the JSON line."""
+    pkg = importlib.import_module("beagle-lib_b200")
+    plan = pkg.checkpoint.smallest_plan(pr, transposed_pre=pr.S > 4)
+    pref = SINGLE | SCALERS_LOG | PROC_GPU | PRE_MANUAL | ASYNCH
+    inst = lib.create(*plan.create_args(), resources=[device], preferenceFlags=pref,
+                      requirementFlags=SINGLE | FW_CUDA)
+    pr.load(inst)
+    stream = torch.cuda.ExternalStream(inst.cudaStream())
+    graph, gradient = plan.capture(inst)
+    idx = np.arange(pr.B, dtype=np.int32)
+
+    def step(t):
+        inst.updateTransitionMatrices(0, idx, None, None, t)
+        inst.launchGraph(graph)
+        return inst.getLogLikelihood()
+
+    lnl = step(pr.lengths)
+    g = gradient()
+    lnl_err = abs(lnl - ref_lnl) / abs(ref_lnl)
+    grad_err = float(np.max(np.abs(g - ref_grad)) / np.max(np.abs(ref_grad)))
+    rng = np.random.default_rng(7)
+    lengths = torch.empty(pr.B, dtype=torch.float64).pin_memory()
+    host = lengths.numpy()
+    step(pr.lengths)
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    inst.waitForPartials([])
+    start.record(stream)
+    for _ in range(steps):
+        host[:] = pr.lengths * (1.0 + 1e-3 * rng.standard_normal(pr.B))
+        step(host)
+    end.record(stream)
+    end.synchronize()
+    ms = start.elapsed_time(end)
+    inst.finalize()
+    per_buffer = pr.P * pr.C * pr.S * 4
+    return {"value": steps / (ms / 1000.0), "unit": "evals/s",
+            "how": "new lengths in, lnL + gradient out; post-matrix work from a CUDA graph",
+            "block": plan.block, "blocks": plan.n_blocks, "calls_per_eval": plan.calls,
+            "partials_buffers": plan.pool, "partials_buffers_full": pr.B + pr.N - 1,
+            "partials_gb": plan.pool * per_buffer / 1e9,
+            "partials_gb_full": (pr.B + pr.N - 1) * per_buffer / 1e9,
+            "rel_lnl_vs_full": lnl_err, "grad_err_vs_full": grad_err}
+
+
 def run_profile_case(args):
     """The workload's tree and model on --profile-patterns patterns (default
     20,000: partials larger than L2, a few hundred MB on the device), mixed
@@ -386,7 +435,10 @@ def run_b200_arm(args):
     e2e_value = ws * e2e_steps / (max_over_ranks(ms_e2e, ws) / 1000.0)
     ms_graph = timed_e2e_graph(torch, inst, pr, e2e_steps)
     e2e_graph_value = ws * e2e_steps / (max_over_ranks(ms_graph, ws) / 1000.0)
+    _, ref_grad = pr.evaluate(inst, transposed_pre=pr.S > 4)
+    ref_lnl = inst.getLogLikelihood()        # ASYNCH: delivers lnL and the gradient
     inst.finalize()
+    ckpt = timed_checkpointed(torch, lib, pr, local, e2e_steps, ref_lnl, ref_grad)
 
     # the plain FP64 path (one instance, same workload) for the mixed/FP64 ratio
     inst64 = make_instance(lib, pr, "double", local)
@@ -425,6 +477,7 @@ def run_b200_arm(args):
                     "d2h_bytes_per_step": d2h},
             "e2e_graph": {"value": e2e_graph_value, "unit": "evals/s",
                           "how": "same steps, post-matrix work replayed from a CUDA graph"},
+            "checkpointed": ckpt,
             "plain_fp64": {"value": value64, "unit": "evals/s", "ms_per_step": ms64 / k64,
                            "mixed_over_fp64": value / value64,
                            "mixed_vs_fp64_rel_lnl_err": rel_err},
