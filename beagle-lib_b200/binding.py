@@ -64,6 +64,8 @@ _SIGS = {
     "CalculateRootLogLikelihoods": [_i, _p, _p, _p, _p, _i, _p],
     "CalculateRootLogLikelihoodsByPartition": [_i, _p, _p, _p, _p, _p, _i, _i, _p, _p],
     "CalculateEdgeDerivatives": [_i, _p, _p, _p, _p, _i, _p, _p, _p],
+    "UpdatePrePartialsWithDerivatives": [_i, _p, _i, _p, _p, _p, _p, _p],
+    "GetTunedVariants": [_i, _p],
     "CalculateCrossProductDerivative": [_i, _p, _p, _p, _p, _p, _i, _p, _p],
     "CalculateEdgeLogLikelihoods": [_i, _p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p, _p],
     "CalculateEdgeLogLikelihoodsByPartition": [_i] + [_p] * 9 + [_i, _i] + [_p] * 6,
@@ -394,6 +396,29 @@ class Instance:
                    _ptr(o1), _ptr(o2), _ptr(o3), check=check)
         (self._graph_keep if self._capturing else self._keep).append((o2, o3))
         return (None if o1 is None else o1.reshape(n, self.patternCount)), o2, o3
+
+    def supports(self, name):
+        """Whether the library exports <prefix><name>."""
+        return name in self.blib.fn
+
+    def tunedVariants(self):
+        """{kind: variant} the autotuner last ran (beagleB200GetTunedVariants)."""
+        o = np.zeros(4, dtype=np.int32)
+        self._call("GetTunedVariants", _ptr(o))
+        return dict(zip(("post", "pre", "deriv", "fused"), (int(x) for x in o)))
+
+    def updatePrePartialsWithDerivatives(self, ops, post, dmat, cw, check=True):
+        """Pre-order ops, then the edge derivative of each op's node from
+        (post[k], dest of op k, dmat[k]): (sums, sums of squares) in op order
+        (beagleB200UpdatePrePartialsWithDerivatives)."""
+        o = _i32(ops)
+        a, d, w = _i32(post), _i32(dmat), _i32(cw)
+        n = len(a)
+        o2, o3 = np.zeros(n), np.zeros(n)
+        self._call("UpdatePrePartialsWithDerivatives", _ptr(o), n, _ptr(a), _ptr(d), _ptr(w),
+                   _ptr(o2), _ptr(o3), check=check)
+        (self._graph_keep if self._capturing else self._keep).append((o2, o3))
+        return o2, o3
 
     def calculateEdgeLogLikelihoods(self, parent, child, prob, d1, d2, cw, sf, cum,
                                     check=True):

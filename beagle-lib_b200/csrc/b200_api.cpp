@@ -354,6 +354,20 @@ int beagleB200CalculateEdgeDerivatives(int h, const int* post, const int* pre, c
         return in->calculateEdgeDerivatives(post, pre, d, w, n, o, s, sq);
     });
 }
+int beagleB200UpdatePrePartialsWithDerivatives(int h, const int* ops, int count,
+                                               const int* post, const int* dmat, const int* cw,
+                                               double* s, double* sq) {
+    return call(h, [&](b200::Instance* in) {
+        return in->updatePrePartialsWithDerivatives(ops, count, post, dmat, cw, s, sq);
+    });
+}
+int beagleB200GetTunedVariants(int h, int* out) {
+    if (!out) return BEAGLE_B200_ERROR_OUT_OF_RANGE;
+    return call(h, [&](b200::Instance* in) {
+        for (int k = 0; k < 4; ++k) out[k] = in->picked(k + 1);
+        return BEAGLE_B200_SUCCESS;
+    });
+}
 int beagleB200CalculateCrossProductDerivative(int h, const int*, const int*, const int*,
                                               const int*, const double*, int, double*, double*) {
     return call(h, [](b200::Instance*) { return BEAGLE_B200_ERROR_NO_IMPLEMENTATION; });

@@ -12,8 +12,11 @@
 #include <cmath>
 #include <cstring>
 #include <algorithm>
+#include <unordered_map>
 
 namespace b200 {
+
+void assign_slots(const int* ops, int count, int stride, std::vector<OpDesc>& tab);
 
 enum {
     kSuccess = 0, kErrGeneral = -1, kErrOOM = -2, kErrRange = -5, kErrNoImpl = -7,
@@ -772,9 +775,43 @@ int Instance::build_walk(const int* ops, int count, int stride, bool pre, std::v
                 has_op_cum = true;
             }
         }
-        d.reserved = 0;
+        d.slots = 0;
     }
+    if (stride == 7) assign_slots(ops, count, stride, tab);
     return kSuccess;
+}
+
+// Shared-memory slots for the S = 4 slot walks: a linear scan over the list
+// gives each result that a later op reads one of kMaxSlots slots, from its op
+// to its last reader (a buffer rewritten later in the list starts a new value);
+// results that find no free slot are read back from device memory as usual.
+void assign_slots(const int* ops, int count, int stride, std::vector<OpDesc>& tab) {
+    std::unordered_map<int, int> producer;          // buffer -> op that wrote its value
+    std::vector<int> src1(count, -1), src2(count, -1), last(count, -1);
+    for (int k = 0; k < count; ++k) {
+        const int* op = ops + (size_t)k * stride;
+        auto it = producer.find(op[3]);
+        if (it != producer.end()) src1[k] = it->second, last[it->second] = k;
+        it = producer.find(op[5]);
+        if (it != producer.end()) src2[k] = it->second, last[it->second] = k;
+        producer[op[0]] = k;
+    }
+    std::vector<int> slot(count, -1), free_slots;
+    std::vector<std::vector<int>> ends(count);
+    for (int s = kMaxSlots - 1; s >= 0; --s) free_slots.push_back(s);
+    for (int k = 0; k < count; ++k) {
+        for (int j : ends[k]) free_slots.push_back(slot[j]);   // op k reads, then writes
+        if (last[k] > k && !free_slots.empty()) {
+            slot[k] = free_slots.back();
+            free_slots.pop_back();
+            ends[last[k]].push_back(k);
+        }
+    }
+    for (int k = 0; k < count; ++k) {
+        const int in1 = src1[k] >= 0 ? slot[src1[k]] : -1;
+        const int in2 = src2[k] >= 0 ? slot[src2[k]] : -1;
+        tab[k].slots = (slot[k] + 1) | ((in1 + 1) << 4) | ((in2 + 1) << 8);
+    }
 }
 
 int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative, bool pre) {
@@ -808,6 +845,7 @@ int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative,
                           tune_count_class(count), device_};
         int v = tune_pick(key, tc ? 2 : 1, idempotent && !cum && !has_op_cum, stream_, run);
         if (v < 0) v = tc ? 1 : 0;
+        picked_[pre ? kTuneWalkPre : kTuneWalkPost] = v;
         cudaError_t e = run(v);
         if (e == cudaErrorInvalidConfiguration && v == 1) {
             (void)cudaGetLastError();
@@ -830,6 +868,7 @@ int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative,
                           tune_count_class(count), device_};
         const int v = tune_pick(key, s4_walk_variants(C_), idempotent && !cum && !has_op_cum,
                                 stream_, run);
+        picked_[pre ? kTuneWalkPre : kTuneWalkPost] = v;
         CK(run(v));
     }
     return kSuccess;
@@ -1032,7 +1071,9 @@ int Instance::calculateEdgeDerivatives(const int* post, const int* pre, const in
         };
         const TuneKey key{kTuneDeriv, (int)dbl_, C_, Pp_, tune_count_class(count), device_};
         bulk_used_ = true;   // variant 6 may run (chosen, forced or being timed)
-        CK(run(tune_pick(key, deriv4_variants(dm), true, stream_, run)));
+        const int v = tune_pick(key, deriv4_variants(dm), true, stream_, run);
+        picked_[kTuneDeriv] = v;
+        CK(run(v));
     } else {
         const DerivDesc* d_desc = (const DerivDesc*)t_deriv_.ptr;
         const double* catw = d_catw_ + (size_t)w * C_;
@@ -1058,6 +1099,7 @@ int Instance::calculateEdgeDerivatives(const int* post, const int* pre, const in
                           device_};
         int v = tune_pick(key, tc ? 2 : 1, true, stream_, run);
         if (v < 0) v = tc ? 1 : 0;
+        picked_[kTuneDeriv] = v;
         cudaError_t e = run(v);
         if (e == cudaErrorInvalidConfiguration && v == 1) {
             (void)cudaGetLastError();
@@ -1065,6 +1107,12 @@ int Instance::calculateEdgeDerivatives(const int* post, const int* pre, const in
         }
         CK(e);
     }
+    return deliver_sums(count, outDerivs, outSum, outSumSq);
+}
+
+// The 2 * count sums of an edge-derivative launch (out_), and the per-site
+// values (site_d_) when requested, to the caller's arrays.
+int Instance::deliver_sums(int count, double* outDerivs, double* outSum, double* outSumSq) {
     if (async_ && !outDerivs) {
         // ASYNCH: sums are written to the caller's arrays at the next
         // synchronisation point (getters, waitForPartials, synchronous calls).
@@ -1091,6 +1139,106 @@ int Instance::calculateEdgeDerivatives(const int* post, const int* pre, const in
     if (outSum) std::copy(h_out_, h_out_ + count, outSum);
     if (outSumSq) std::copy(h_out_ + count, h_out_ + 2 * count, outSumSq);
     return kSuccess;
+}
+
+// updatePrePartials(ops) then calculateEdgeDerivatives(post[k], dest of op k,
+// dmat[k]) in one S = 4 walk (k_fused.cu) where the list allows it: at most
+// 256 ops, no op rewriting a buffer that an earlier op's derivative reads (a
+// destination written twice, or a post-order operand that is also a
+// destination).  Otherwise the two calls run as they are; where the fused
+// walk can run, the autotuner picks it or the two calls' kernels by time.
+int Instance::updatePrePartialsWithDerivatives(const int* ops, int count, const int* post,
+                                               const int* dmat, const int* cw, double* outSum,
+                                               double* outSumSq) {
+    if (count < 0 || (count > 0 && (!ops || !post || !dmat || !cw))) return kErrRange;
+    std::vector<int> pre(count);
+    for (int k = 0; k < count; ++k) pre[k] = ops[(size_t)k * 7];
+    auto separate = [&]() -> int {
+        int rc = updatePrePartials(ops, count, -1);
+        if (rc) return rc;
+        return calculateEdgeDerivatives(post, pre.data(), dmat, cw, count, nullptr, outSum,
+                                        outSumSq);
+    };
+    const Dims dm = dims();
+    if (count == 0 || !fused_supported(dm, count)) return separate();
+    std::vector<OpDesc> tab;
+    std::vector<uint8_t> dep;
+    bool idempotent = false, has_op_cum = false;
+    int rc = build_walk(ops, count, 7, true, tab, dep, idempotent, has_op_cum);
+    if (rc) return rc;
+    std::vector<DerivDesc> dtab;
+    rc = build_deriv(post, pre.data(), dmat, cw, count, dtab);
+    if (rc) return rc;
+    std::unordered_map<int, int> writes;
+    for (int k = 0; k < count; ++k) ++writes[pre[k]];
+    for (int k = 0; k < count; ++k)
+        if (writes[pre[k]] != 1 || writes.count(post[k])) return separate();
+    std::vector<PreDerivOp> fops(count);
+    for (int k = 0; k < count; ++k) {
+        const OpDesc& t = tab[k];
+        const DerivDesc& d = dtab[k];
+        PreDerivOp& f = fops[k];
+        f.parent = t.x1;
+        f.sib = t.x2;
+        f.dest = t.dest;
+        f.mnode = t.m1;
+        f.msib = t.m2;
+        f.post = d.post;
+        f.dmat = d.dmat;
+        f.scale_write = t.scale_write;
+        f.pad_sib = t.pad2;
+        f.dpad = d.dpad;
+        f.kind = (t.kind & (kX2States | kM1Transposed)) | (d.post_is_states ? kPostStates : 0);
+        f.reserved = 0;
+    }
+    // Sibling pairs: same parent, each op's sibling the other's node, and
+    // neither op's destination read by the other.
+    for (int k = 0; k + 1 < count; ++k) {
+        const int* a = ops + (size_t)k * 7;
+        const int* b = a + 7;
+        const bool pair = a[3] == b[3] && a[5] == post[k + 1] && b[5] == post[k] &&
+                          a[0] != b[0] && a[0] != b[3] && a[0] != b[5] && a[0] != post[k + 1] &&
+                          b[0] != a[5] && b[0] != post[k];
+        if (pair) {
+            fops[k].kind |= kPairFirst;
+            ++k;
+        }
+    }
+    const int w = cw[0];
+    const int nblk = std::max(fused_blocks(dm), deriv_blocks(dm));
+    CK(scratch_.reserve(sizeof(double) * 2 * (size_t)count * nblk));
+    CK(out_.reserve(sizeof(double) * 2 * count));
+    CK(t_deriv_.upload(dtab.data(), sizeof(DerivDesc) * count, stream_));
+    const double* catw = d_catw_ + (size_t)w * C_;
+    const int ls = (int)log_scalers_;
+    // Both variants leave the sums in out_.  0: the pre-order walk and the
+    // derivative kernels of the two calls; 1: the fused walk.  The autotuner
+    // times them when the list may run repeatedly (no op reads what a later
+    // op writes); the first, untimed run also settles the two calls' own
+    // autotuner choices.
+    auto run = [&](int v) -> cudaError_t {
+        if (v == 0) {
+            if (post_or_pre(ops, count, 7, -1, true) != kSuccess) return cudaErrorUnknown;
+            const TuneKey dk{kTuneDeriv, (int)dbl_, C_, Pp_, tune_count_class(count), device_};
+            bulk_used_ = true;
+            auto deriv = [&](int dv) -> cudaError_t {
+                return LAUNCH(launch_edge_derivatives, (const DerivDesc*)t_deriv_.ptr, count,
+                              catw, d_patw_, dm, nullptr, (double*)scratch_.ptr,
+                              (double*)out_.ptr, stream_, dv);
+            };
+            const int dv = tune_pick(dk, deriv4_variants(dm), true, stream_, deriv);
+            picked_[kTuneDeriv] = dv;
+            return deriv(dv);
+        }
+        return LAUNCH(launch_pre_deriv4, fops.data(), count, dm, catw, d_patw_, ls,
+                      (double*)scratch_.ptr, (double*)out_.ptr, stream_);
+    };
+    const TuneKey key{kTuneFused, (int)dbl_, C_, Pp_, tune_count_class(count), device_};
+    int v = tune_pick(key, 2, idempotent, stream_, run);
+    if (v < 0) v = 1;
+    picked_[kTuneFused] = v;
+    CK(run(v));
+    return deliver_sums(count, nullptr, outSum, outSumSq);
 }
 
 int Instance::calculateEdgeLogLikelihoods(const int* parents, const int* children,

@@ -86,6 +86,14 @@ public:
     int calculateEdgeDerivatives(const int* post, const int* pre, const int* dmat,
                                  const int* cw, int count, double* outDerivs, double* outSum,
                                  double* outSumSq);
+    // Kernel variant last run per autotuner kind (1 post-order walk, 2
+    // pre-order walk, 3 edge derivatives, 4 fused pre-order + derivatives;
+    // -1 = default shape, -2 = not run yet).
+    int picked(int kind) const { return kind >= 1 && kind <= 4 ? picked_[kind] : -2; }
+    // updatePrePartials + calculateEdgeDerivatives (sums only) in one walk.
+    int updatePrePartialsWithDerivatives(const int* ops, int count, const int* post,
+                                         const int* dmat, const int* cw, double* outSum,
+                                         double* outSumSq);
     int calculateEdgeLogLikelihoods(const int* parents, const int* children, const int* prob,
                                     const int* d1, const int* d2, const int* cw, const int* sf,
                                     const int* cum, int count, double* outLnL, double* outD1,
@@ -122,6 +130,7 @@ private:
     int upload_partials(int b, const double* in, bool replicate);
     int run_matrix_jobs(const std::vector<MatJob>& jobs);
     int post_or_pre(const int* ops, int count, int stride, int cumulative, bool pre);
+    int deliver_sums(int count, double* outDerivs, double* outSum, double* outSumSq);
     int sync();
     double* stage(size_t n);     // pinned result staging (ASYNCH results)
     Dims dims() const { return Dims{S_, Sg_, P_, Pp_, C_}; }
@@ -174,6 +183,7 @@ private:
         double* dst_sumsq;
         int count;                // edge-derivative branches (0: a log-likelihood)
     };
+    int picked_[5] = {-2, -2, -2, -2, -2};
     std::vector<Pending> pending_;
     // A captured graph: its executable, the deliveries its copies feed and the
     // pinned blocks those copies (and its table uploads) use.

@@ -130,6 +130,16 @@ int deriv_blocks(const Dims& d);
 cudaError_t launch_deriv_final(const double* d_block, int nblk, int nb, double* d_sums,
                                cudaStream_t s);
 
+// Fused pre-order partials + edge derivatives (k_fused.cu): S = 4, C in
+// {1, 2, 4, 8}, at most 256 ops.  d_block needs 2 * nops * fused_blocks(d)
+// doubles; d_sums receives the nops sums, then the nops sums of squares.
+bool fused_supported(const Dims& d, int nops);
+int fused_blocks(const Dims& d);
+template <typename Real>
+cudaError_t launch_pre_deriv4(const PreDerivOp* h_ops, int nops, const Dims& d,
+                              const double* catw, const double* patw, int ls, double* d_block,
+                              double* d_sums, cudaStream_t s);
+
 // ---- batched launches over several instances (segment tables on the device;
 // ncta = the segments' total CTAs; see b200_types.h) ------------------------
 // S = 4 walks, one pattern per thread (256-thread CTAs of 256 / C patterns);

@@ -24,7 +24,7 @@
 
 namespace b200 {
 
-enum TuneKind { kTuneWalkPost = 1, kTuneWalkPre = 2, kTuneDeriv = 3 };
+enum TuneKind { kTuneWalkPost = 1, kTuneWalkPre = 2, kTuneDeriv = 3, kTuneFused = 4 };
 
 struct TuneKey {
     int kind, dbl, C, Pp, count_class, device;

@@ -22,6 +22,8 @@ enum OpKind : int {
     kX1States = 1,      // first operand is a compact tip-state buffer
     kX2States = 2,      // second operand is a compact tip-state buffer
     kM1Transposed = 4,  // pre-order: the node's matrix is given as its transpose
+    kPostStates = 8,    // fused pre-order op: the node's own post-order operand is tip states
+    kPairFirst = 16,    // fused pre-order op: this op and the next are a sibling pair
 };
 
 // One resolved partials operation (post-order or pre-order).  Post-order:
@@ -43,6 +45,34 @@ struct OpDesc {
     int kind;                   // OpKind bits
     int p_begin;                // only patterns [p_begin, p_end) are written: the op's
     int p_end;                  //   partition, or [0, Pp) for a whole-instance op
+    int slots;                  // shared-memory slots of the S = 4 slot walks (kSlot*)
+};
+
+// OpDesc::slots packs three 4-bit fields, each a slot index + 1 (0 = none):
+// the slot that keeps the op's result for a later op of the same list (bits
+// 0-3), and the slots its operands x1 (bits 4-7) and x2 (bits 8-11) are read
+// from instead of device memory.  Only whole-instance lists get slots.
+constexpr int kMaxSlots = 8;
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+inline int slot_field(int packed, int field) { return ((packed >> (4 * field)) & 15) - 1; }
+
+// One op of the fused pre-order + edge-derivative walk (S = 4): the
+// pre-order op (dest = P_node^T (parent o P_sib sib)) and the derivative of the
+// node's branch from its new pre-order row and its post-order operand.
+struct PreDerivOp {
+    const void* parent;         // parent's pre-order partials
+    const void* sib;            // sibling's post-order partials or tip states
+    void* dest;                 // this node's pre-order partials
+    const void* mnode;          // P of this node's branch (transposed if kM1Transposed)
+    const void* msib;           // P of the sibling's branch
+    const void* post;           // this node's post-order partials or tip states
+    const void* dmat;           // derivative matrix of this node's branch
+    double* scale_write;        // rescale into this buffer (nullptr = none)
+    double pad_sib;             // missing-state value of msib
+    double dpad;                // missing-state value of dmat
+    int kind;                   // OpKind bits: kX2States, kM1Transposed, kPostStates, kPairFirst
     int reserved;
 };
 

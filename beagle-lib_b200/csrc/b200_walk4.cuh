@@ -9,12 +9,12 @@
 namespace b200 {
 namespace {
 
-// Store the scale factor of one pattern (see the file comment), its log
-// taken, stored and accumulated in FP64.
+// Store the scale factor of one pattern (see the file comment): its log
+// (scale_log) stored and accumulated in FP64.
 template <typename Real>
 __device__ __forceinline__ void store_scale(Real m, double* scale_write, double* cum, int p,
                                             int log_scalers) {
-    const double lm = log((double)m);
+    const double lm = scale_log(m);
     scale_write[p] = log_scalers ? lm : (double)m;
     if (cum) cum[p] += lm;
 }

@@ -1,0 +1,271 @@
+// Pre-order partials and the edge derivatives of the same branches in one
+// walk (S = 4): beagleB200UpdatePrePartialsWithDerivatives.
+//
+// The call means updatePrePartials(ops) followed by calculateEdgeDerivatives
+// over (post[k], dest of op k) for every op k (CPU/BeagleCPUImpl.hpp:1689-1862
+// and :1940-2285).  Run separately, the derivative pass reads back every
+// pre-order buffer the walk has just written, and every post-order buffer
+// the walk has just read as a sibling.  Here the derivative terms of a branch
+// are formed from the registers that hold its new pre-order row, so the
+// walk's traffic is the whole cost.
+//
+// Sibling pairs: the pre-order ops of the two children a, b of one parent
+// (consecutive in the list, same parent, each the other's sibling) run as
+// one step that loads the parent's row and both children's post-order rows
+// once:
+//   pre[a] = P_a^T (pre[parent] o P_b post[b]),  pre[b] = P_b^T (pre[parent] o P_a post[a])
+// and both branches' derivative terms come from the same registers.
+//
+// Per branch and pattern (as k_edge_deriv4): n_c = sum_k pre_k (D_c post)_k,
+// q_c = sum_k pre_k post_k; d = sum_c w_c n_c / sum_c w_c q_c in the partials'
+// precision; the pattern-weighted sums of d and d^2 in FP64.  Each warp
+// reduces its patterns' terms and writes one partial sum per branch; the
+// final-sum kernel adds them in a fixed order.
+//
+// Thread per (pattern, category) as in the S = 4 walks; the op list is a
+// kernel parameter (constant-bank reads).
+#include <algorithm>
+#include <cstring>
+
+#include "b200_kernels.h"
+#include "b200_vec.cuh"
+#include "b200_walk4.cuh"
+
+namespace b200 {
+
+namespace {
+
+constexpr int kFusedOps = 256;
+struct FusedParams {
+    PreDerivOp op[kFusedOps];
+};
+
+template <typename Real, int C>
+__device__ __forceinline__ void rescale_store4(const PreDerivOp& op, Real out[4], int p,
+                                               bool valid, int c, int log_scalers) {
+    if (op.scale_write) {
+        Real m = out[0];
+#pragma unroll
+        for (int i = 1; i < 4; ++i) m = out[i] > m ? out[i] : m;
+        m = group_max<C>(m);
+        if (m == Real(0)) m = Real(1);
+        const Real inv = Real(1) / m;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) out[i] *= inv;
+        if (valid && c == 0) store_scale(m, op.scale_write, nullptr, p, log_scalers);
+    }
+    if (valid) st4(static_cast<Real*>(op.dest) + ((size_t)p * C + c) * 4, out);
+}
+
+// out_j = sum_i M[i][j] z_i (M given transposed when `tr`).
+template <typename Real>
+__device__ __forceinline__ void apply_node(const Real* M, bool tr, const Real z[4], Real out[4]) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) out[j] = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        Real m[4];
+        if (tr) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) m[j] = __ldg(M + j * 4 + i);
+        } else {
+            ldg4(M + i * 4, m);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) out[j] += m[j] * z[i];
+    }
+}
+
+// num / den: FP64 division; FP32 through the hardware reciprocal (__fdividef,
+// 2 ulp), within the FP32 partials' own error.
+__device__ __forceinline__ double quotient(double a, double b) { return a / b; }
+__device__ __forceinline__ float quotient(float a, float b) { return __fdividef(a, b); }
+
+// Category-combined derivative value of one pattern for one branch; D is
+// this category's derivative matrix (dm, when every op shares one, else the
+// op's own, loaded here).
+template <typename Real, int C, bool SHARED_D>
+__device__ __forceinline__ Real deriv_value(const PreDerivOp& op, const Real dm_shared[16],
+                                            const Real pre[4], const Real x[4], int s,
+                                            bool states, int c, Real w) {
+    Real dm[16];
+    if (SHARED_D) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) dm[i] = dm_shared[i];
+    } else {
+        const Real* D = static_cast<const Real*>(op.dmat) + c * 16;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) ldg4(D + 4 * k, dm + 4 * k);
+    }
+    Real n = 0, q = 0;
+    if (states) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            Real dk = (Real)op.dpad;
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                if (s == i) dk = dm[k * 4 + i];
+            n += pre[k] * dk;
+            q += (s >= 4 || k == s) ? pre[k] : Real(0);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const Real y = dm[k * 4] * x[0] + dm[k * 4 + 1] * x[1] + dm[k * 4 + 2] * x[2] +
+                           dm[k * 4 + 3] * x[3];
+            n += pre[k] * y;
+            q += pre[k] * x[k];
+        }
+    }
+    Real num = w * n, den = w * q;
+#pragma unroll
+    for (int o = 1; o < C; o <<= 1) {
+        num += __shfl_xor_sync(0xffffffffu, num, o);
+        den += __shfl_xor_sync(0xffffffffu, den, o);
+    }
+    return quotient(num, den);
+}
+
+// Warp sums of the weighted value and its square for branch k (values sit in
+// the lanes of category 0, every C-th lane; zero elsewhere); lane 0 writes
+// them to this warp's column of the block partials in FP64.  The 32 / C terms
+// of one warp are added in the partials' precision: with FP32 partials each
+// term already carries FP32 rounding.
+template <typename Real, int C>
+__device__ __forceinline__ void warp_emit(Real v, Real wp, int k, int nops, int nblk, int wid,
+                                          double* block) {
+    Real s1 = v * wp, s2 = v * v * wp;
+#pragma unroll
+    for (int o = C; o < 32; o <<= 1) {
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        block[(size_t)k * nblk + wid] = (double)s1;
+        block[(size_t)(nops + k) * nblk + wid] = (double)s2;
+    }
+}
+
+template <typename Real>
+__device__ __forceinline__ void load_row(const void* x, bool states, int pc, int C, int c,
+                                         Real v[4], int& s) {
+    if (states) s = static_cast<const int*>(x)[pc];
+    else ld4(static_cast<const Real*>(x) + ((size_t)pc * C + c) * 4, v);
+}
+
+// Resident CTAs per SM: FP32 4 (64 registers a thread), 3 when the shared
+// derivative matrix is held in registers; FP64 2.
+template <typename Real, int C, bool SHARED_D>
+__global__ void __launch_bounds__(kT4, sizeof(Real) == 4 ? (SHARED_D ? 3 : 4) : 2)
+k_pre_deriv4(const __grid_constant__ FusedParams F, int nops, int P, int Pp,
+             const double* __restrict__ catw, const double* __restrict__ patw, int log_scalers,
+             double* block) {
+    const int c = threadIdx.x % C;
+    Real dm[16];
+    if (SHARED_D) {
+        const Real* D = static_cast<const Real*>(F.op[0].dmat) + c * 16;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) ldg4(D + 4 * k, dm + 4 * k);
+    }
+    const int p = blockIdx.x * (kT4 / C) + threadIdx.x / C;
+    const bool valid = p < Pp;
+    const int pc = valid ? p : Pp - 1;
+    const Real w = (Real)catw[c];
+    const bool counted = c == 0 && p < P;
+    const Real wp = counted ? (Real)patw[p] : Real(0);
+    const int nblk = gridDim.x * (kT4 / 32);
+    const int wid = blockIdx.x * (kT4 / 32) + threadIdx.x / 32;
+    for (int o = 0; o < nops;) {
+        const PreDerivOp& A = F.op[o];
+        const bool tra = A.kind & kM1Transposed;
+        Real pv[4];
+        ld4(static_cast<const Real*>(A.parent) + ((size_t)pc * C + c) * 4, pv);
+        if (A.kind & kPairFirst) {
+            const PreDerivOp& B = F.op[o + 1];
+            const bool sta = A.kind & kPostStates, stb = A.kind & kX2States;
+            Real xa[4], xb[4];
+            int sa = 0, sb = 0;
+            load_row(A.post, sta, pc, C, c, xa, sa);     // post[a] (= B's sibling)
+            load_row(A.sib, stb, pc, C, c, xb, sb);      // post[b] (= A's sibling)
+            Real ya[4], yb[4], za[4], zb[4], pa[4], pb[4];
+            operand4c(static_cast<const Real*>(A.msib) + c * 16, stb, sb, xb, (Real)A.pad_sib, yb);
+            operand4c(static_cast<const Real*>(B.msib) + c * 16, sta, sa, xa, (Real)B.pad_sib, ya);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                za[i] = pv[i] * yb[i];
+                zb[i] = pv[i] * ya[i];
+            }
+            apply_node(static_cast<const Real*>(A.mnode) + c * 16, tra, za, pa);
+            apply_node(static_cast<const Real*>(B.mnode) + c * 16, (B.kind & kM1Transposed) != 0,
+                       zb, pb);
+            rescale_store4<Real, C>(A, pa, pc, valid, c, log_scalers);
+            rescale_store4<Real, C>(B, pb, pc, valid, c, log_scalers);
+            const Real da = deriv_value<Real, C, SHARED_D>(A, dm, pa, xa, sa, sta, c, w);
+            const Real db = deriv_value<Real, C, SHARED_D>(B, dm, pb, xb, sb, stb, c, w);
+            warp_emit<Real, C>(counted ? da : Real(0), wp, o, nops, nblk, wid, block);
+            warp_emit<Real, C>(counted ? db : Real(0), wp, o + 1, nops, nblk, wid, block);
+            o += 2;
+        } else {
+            const bool sts = A.kind & kX2States, stp = A.kind & kPostStates;
+            Real xs[4], xp[4];
+            int ss = 0, sp = 0;
+            load_row(A.sib, sts, pc, C, c, xs, ss);
+            load_row(A.post, stp, pc, C, c, xp, sp);
+            Real y[4], z[4], pa[4];
+            operand4c(static_cast<const Real*>(A.msib) + c * 16, sts, ss, xs, (Real)A.pad_sib, y);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) z[i] = pv[i] * y[i];
+            apply_node(static_cast<const Real*>(A.mnode) + c * 16, tra, z, pa);
+            rescale_store4<Real, C>(A, pa, pc, valid, c, log_scalers);
+            const Real da = deriv_value<Real, C, SHARED_D>(A, dm, pa, xp, sp, stp, c, w);
+            warp_emit<Real, C>(counted ? da : Real(0), wp, o, nops, nblk, wid, block);
+            o += 1;
+        }
+    }
+}
+
+}  // namespace
+
+int fused_blocks(const Dims& d) { return (d.Pp + kT4 / d.C - 1) / (kT4 / d.C) * (kT4 / 32); }
+
+bool fused_supported(const Dims& d, int nops) {
+    return d.S == 4 && d.Sg == 4 && (d.C == 1 || d.C == 2 || d.C == 4 || d.C == 8) &&
+           nops <= kFusedOps;
+}
+
+template <typename Real>
+cudaError_t launch_pre_deriv4(const PreDerivOp* h_ops, int nops, const Dims& d,
+                              const double* catw, const double* patw, int ls, double* d_block,
+                              double* d_sums, cudaStream_t s) {
+    if (nops == 0) return cudaSuccess;
+    if (!fused_supported(d, nops)) return cudaErrorInvalidValue;
+    static thread_local FusedParams prm;
+    std::memcpy(prm.op, h_ops, sizeof(PreDerivOp) * nops);
+    const int grid = (d.Pp + kT4 / d.C - 1) / (kT4 / d.C);
+    bool shared_d = true;             // one derivative matrix for every branch
+    for (int k = 1; k < nops; ++k)
+        shared_d = shared_d && h_ops[k].dmat == h_ops[0].dmat && h_ops[k].dpad == h_ops[0].dpad;
+#define PD_(CC)                                                                            \
+    (shared_d ? (k_pre_deriv4<Real, CC, true><<<grid, kT4, 0, s>>>(prm, nops, d.P, d.Pp, catw, \
+                                                                  patw, ls, d_block), 0)    \
+              : (k_pre_deriv4<Real, CC, false><<<grid, kT4, 0, s>>>(prm, nops, d.P, d.Pp,  \
+                                                                   catw, patw, ls, d_block), 0))
+    switch (d.C) {
+        case 1: PD_(1); break;
+        case 2: PD_(2); break;
+        case 4: PD_(4); break;
+        default: PD_(8); break;
+    }
+#undef PD_
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_deriv_final(d_block, fused_blocks(d), nops, d_sums, s);
+}
+
+template cudaError_t launch_pre_deriv4<float>(const PreDerivOp*, int, const Dims&, const double*,
+                                              const double*, int, double*, double*, cudaStream_t);
+template cudaError_t launch_pre_deriv4<double>(const PreDerivOp*, int, const Dims&, const double*,
+                                               const double*, int, double*, double*,
+                                               cudaStream_t);
+
+}  // namespace b200

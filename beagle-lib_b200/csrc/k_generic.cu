@@ -197,7 +197,7 @@ __device__ __forceinline__ void finish_tile(const OpDesc& op, Real out[4][4], in
             for (int r = 0; r < 4; ++r) out[q][r] *= inv;
             const int p = p0 + pl + q;
             if (c == 0 && sg == 0 && p >= op.p_begin && p < op.p_end) {
-                const double lm = log((double)mq);
+                const double lm = scale_log(mq);
                 op.scale_write[p] = log_scalers ? lm : (double)mq;
                 if (cum) cum[p] += lm;
             }

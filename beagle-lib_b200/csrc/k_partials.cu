@@ -20,7 +20,10 @@
 // This file holds the S = 4 kernels: one thread per (pattern, category),
 // vector loads and stores of one 4-state row, lane-group shuffles for the
 // rescaling maximum.  HBM-bound.  Other state counts: k_generic.cu.
+#include <algorithm>
 #include <cstring>
+#include <unordered_map>
+#include <vector>
 
 #include "b200_kernels.h"
 #include "b200_vec.cuh"
@@ -97,6 +100,188 @@ k_pre4c(const __grid_constant__ OpParams P, int nops, int Pp, int log_scalers) {
     const int p0 = blockIdx.x * ppb + threadIdx.x / C;
     for (int o = 0; o < nops; ++o)
         pre4_op<Real, C, PPT, RANGED>(P.op[o], c, p0, pstride, Pp, log_scalers);
+}
+
+// -------------------------------------------------- S = 4, slot walks
+// The parameter-list walks with a per-thread cache in shared memory: an op
+// whose result a later op of the list reads also writes it to a slot, and the
+// reader takes it from there (OpDesc::slots, assigned on the host).  A chain
+// of dependent ops then waits on shared memory instead of an L2 round trip
+// for the value the same thread stored an op or a few ops before.  Every slot
+// row belongs to one thread, so no barriers are needed; the device-memory
+// store of every result is kept (the buffers are the API's output).
+template <typename Real, int PPT>
+__device__ __forceinline__ Real* slot_row(Real* slots, int s, int k) {
+    return slots + ((size_t)(s * PPT + k) * kT4 + threadIdx.x) * 4;
+}
+
+template <typename Real, int C, int PPT>
+__device__ __forceinline__ void post4s_op(const OpDesc& op, Real* slots, int c, int p0,
+                                          int pstride, int Pp, double* cum, int log_scalers) {
+    const bool st1 = op.kind & kX1States, st2 = op.kind & kX2States;
+    const int so = slot_field(op.slots, 0), s1x = slot_field(op.slots, 1),
+              s2x = slot_field(op.slots, 2);
+    const Real* M1 = static_cast<const Real*>(op.m1) + c * 16;
+    const Real* M2 = static_cast<const Real*>(op.m2) + c * 16;
+    Real x1[PPT][4], x2[PPT][4];
+    int s1[PPT], s2[PPT];
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+        const int p = min(p0 + k * pstride, Pp - 1);
+        if (st1) s1[k] = static_cast<const int*>(op.x1)[p];
+        else if (s1x >= 0) ld4(slot_row<Real, PPT>(slots, s1x, k), x1[k]);
+        else ld4(static_cast<const Real*>(op.x1) + ((size_t)p * C + c) * 4, x1[k]);
+        if (st2) s2[k] = static_cast<const int*>(op.x2)[p];
+        else if (s2x >= 0) ld4(slot_row<Real, PPT>(slots, s2x, k), x2[k]);
+        else ld4(static_cast<const Real*>(op.x2) + ((size_t)p * C + c) * 4, x2[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+        const int p = p0 + k * pstride;
+        Real y1[4], y2[4];
+        operand4c(M1, st1, s1[k], x1[k], (Real)op.pad1, y1);
+        operand4c(M2, st2, s2[k], x2[k], (Real)op.pad2, y2);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) y1[i] *= y2[i];
+        finish4c<Real, C, false>(op, y1, min(p, Pp - 1), p < Pp, c, cum, log_scalers);
+        if (so >= 0) st4(slot_row<Real, PPT>(slots, so, k), y1);
+    }
+}
+
+template <typename Real, int C, int PPT>
+__device__ __forceinline__ void pre4s_op(const OpDesc& op, Real* slots, int c, int p0,
+                                         int pstride, int Pp, int log_scalers) {
+    const bool st2 = op.kind & kX2States;
+    const bool tr = op.kind & kM1Transposed;
+    const int so = slot_field(op.slots, 0), s1x = slot_field(op.slots, 1),
+              s2x = slot_field(op.slots, 2);
+    const Real* M1 = static_cast<const Real*>(op.m1) + c * 16;
+    const Real* M2 = static_cast<const Real*>(op.m2) + c * 16;
+    Real pv[PPT][4], x2[PPT][4];
+    int s2[PPT];
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+        const int p = min(p0 + k * pstride, Pp - 1);
+        if (s1x >= 0) ld4(slot_row<Real, PPT>(slots, s1x, k), pv[k]);
+        else ld4(static_cast<const Real*>(op.x1) + ((size_t)p * C + c) * 4, pv[k]);
+        if (st2) s2[k] = static_cast<const int*>(op.x2)[p];
+        else if (s2x >= 0) ld4(slot_row<Real, PPT>(slots, s2x, k), x2[k]);
+        else ld4(static_cast<const Real*>(op.x2) + ((size_t)p * C + c) * 4, x2[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+        const int p = p0 + k * pstride;
+        Real z[4];
+        operand4c(M2, st2, s2[k], x2[k], (Real)op.pad2, z);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) z[i] *= pv[k][i];
+        Real out[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            Real m[4];
+            if (tr) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) m[j] = __ldg(M1 + j * 4 + i);
+            } else {
+                ldg4(M1 + i * 4, m);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) out[j] += m[j] * z[i];
+        }
+        finish4c<Real, C, false>(op, out, min(p, Pp - 1), p < Pp, c, nullptr, log_scalers);
+        if (so >= 0) st4(slot_row<Real, PPT>(slots, so, k), out);
+    }
+}
+
+template <typename Real, int C, int PPT, bool PRE>
+__global__ void __launch_bounds__(kT4)
+k_walk4s(const __grid_constant__ OpParams P, int nops, int Pp, double* cum, int log_scalers) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Real* slots = reinterpret_cast<Real*>(smem_raw);
+    const int c = threadIdx.x % C;
+    const int ppb = kT4 / C;
+    const int pstride = gridDim.x * ppb;
+    const int p0 = blockIdx.x * ppb + threadIdx.x / C;
+    for (int o = 0; o < nops; ++o) {
+        if (PRE) pre4s_op<Real, C, PPT>(P.op[o], slots, c, p0, pstride, Pp, log_scalers);
+        else post4s_op<Real, C, PPT>(P.op[o], slots, c, p0, pstride, Pp, cum, log_scalers);
+    }
+}
+
+// ------------------------------------------------ S = 4, grouped walks
+// An op list executes in order, but its dependency depth is the tree's
+// height, not its length.  The launcher reorders the list by dependency level
+// (ops of one level read and write disjoint buffers: no read-after-write,
+// write-after-read or write-after-write between them, scale buffers included)
+// and cuts each level into groups of at most G ops.  A thread issues the
+// operand loads of a whole group before computing any of it, so one memory
+// round trip serves G ops: for a 128-taxon tree the pre-order walk's chain of
+// 254 dependent steps becomes about 70 with G = 4.  One pattern per thread.
+struct GroupParams {
+    OpDesc op[kParamOps];
+    unsigned char size[kParamOps];      // group size at a group's first op
+};
+
+template <typename Real, int C, int G, bool PRE>
+__global__ void __launch_bounds__(kT4)
+k_walk4g(const __grid_constant__ GroupParams P, int nops, int Pp, double* cum, int log_scalers) {
+    const int c = threadIdx.x % C;
+    const int p = blockIdx.x * (kT4 / C) + threadIdx.x / C;
+    const bool valid = p < Pp;
+    const int pc = valid ? p : Pp - 1;
+    for (int o = 0; o < nops;) {
+        const int g = P.size[o];
+        Real a[G][4], b[G][4];
+        int s1[G], s2[G];
+#pragma unroll
+        for (int k = 0; k < G; ++k) {
+            if (k < g) {
+                const OpDesc& op = P.op[o + k];
+                if (!PRE && (op.kind & kX1States)) s1[k] = static_cast<const int*>(op.x1)[pc];
+                else ld4(static_cast<const Real*>(op.x1) + ((size_t)pc * C + c) * 4, a[k]);
+                if (op.kind & kX2States) s2[k] = static_cast<const int*>(op.x2)[pc];
+                else ld4(static_cast<const Real*>(op.x2) + ((size_t)pc * C + c) * 4, b[k]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < G; ++k) {
+            if (k < g) {
+                const OpDesc& op = P.op[o + k];
+                const Real* M1 = static_cast<const Real*>(op.m1) + c * 16;
+                const Real* M2 = static_cast<const Real*>(op.m2) + c * 16;
+                const bool st2 = op.kind & kX2States;
+                if (!PRE) {
+                    Real y1[4], y2[4];
+                    operand4c(M1, (op.kind & kX1States) != 0, s1[k], a[k], (Real)op.pad1, y1);
+                    operand4c(M2, st2, s2[k], b[k], (Real)op.pad2, y2);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) y1[i] *= y2[i];
+                    finish4c<Real, C, false>(op, y1, pc, valid, c, cum, log_scalers);
+                } else {
+                    const bool tr = op.kind & kM1Transposed;
+                    Real z[4];
+                    operand4c(M2, st2, s2[k], b[k], (Real)op.pad2, z);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) z[i] *= a[k][i];
+                    Real out[4] = {0, 0, 0, 0};
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        Real m[4];
+                        if (tr) {
+#pragma unroll
+                            for (int j = 0; j < 4; ++j) m[j] = __ldg(M1 + j * 4 + i);
+                        } else {
+                            ldg4(M1 + i * 4, m);
+                        }
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) out[j] += m[j] * z[i];
+                    }
+                    finish4c<Real, C, false>(op, out, pc, valid, c, nullptr, log_scalers);
+                }
+            }
+        }
+        o += g;
+    }
 }
 
 // ------------------------------------------- S = 4, software-pipelined walk
@@ -433,6 +618,9 @@ constexpr int kMinB6 = sizeof(Real) == 4 ? 6 : 1;
 //   7,8    1 or 2 patterns per thread with the op list passed by value as a
 //          kernel parameter (lists of up to kParamOps ops; otherwise the
 //          launch is refused and the tuner skips the variant).
+//   9,10   7, 8 with results that later ops read kept in shared-memory slots;
+//   11-13  the list reordered by dependency level, groups of 2, 4 or 8
+//          independent ops loaded together (one pattern per thread).
 // variant < 0 picks the default: the smallest patterns-per-thread whose grid
 // fits in one resident wave, thread per pattern when C does not divide 32.
 template <typename K>
@@ -499,6 +687,105 @@ cudaError_t run_param4(const OpDesc* h_ops, int nops, const Dims& d, double* cum
     return cudaGetLastError();
 }
 
+// Variants 9, 10: the slot walks.  Lists of partition ops carry no slots and
+// run as variants 7, 8.
+template <typename Real, int C, int PPT>
+cudaError_t run_slot4(const OpDesc* h_ops, int nops, const Dims& d, double* cum, int ls,
+                      cudaStream_t s, bool ranged, bool pre) {
+    if (ranged) return run_param4<Real, C, PPT>(h_ops, nops, d, cum, ls, s, ranged, pre);
+    if (!h_ops || nops > kParamOps) return cudaErrorInvalidValue;
+    static thread_local OpParams prm;
+    std::memcpy(prm.op, h_ops, sizeof(OpDesc) * nops);
+    int nslots = 0;
+    for (int o = 0; o < nops; ++o)
+        for (int f = 0; f < 3; ++f) nslots = std::max(nslots, slot_field(h_ops[o].slots, f) + 1);
+    const size_t smem = (size_t)nslots * PPT * kT4 * 4 * sizeof(Real);
+    auto kern = pre ? k_walk4s<Real, C, PPT, true> : k_walk4s<Real, C, PPT, false>;
+    if (smem > 48 * 1024) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    const int ppb = kT4 / C * PPT;
+    const int grid = (d.Pp + ppb - 1) / ppb;
+    kern<<<grid, kT4, smem, s>>>(prm, nops, d.Pp, pre ? nullptr : cum, ls);
+    return cudaGetLastError();
+}
+
+// Dependency level of every op of a list (0 = reads nothing an earlier op of
+// the list writes): one more than the level of each earlier op it must follow,
+// i.e. the last writer of a buffer it reads (partials or scale factors), and
+// the last writer and every reader since of a buffer it writes.  Buffers are
+// compared by device address.  The shared cumulative scale buffer is an
+// accumulation, whose order changes only the rounding of its FP64 sum.
+static void op_levels(const OpDesc* ops, int n, std::vector<int>& level) {
+    struct Use {
+        int written = -1;   // level of the last writer
+        int read = -1;      // highest level of a reader
+    };
+    std::unordered_map<const void*, Use> use;
+    use.reserve(4 * n);
+    level.assign(n, 0);
+    for (int j = 0; j < n; ++j) {
+        const OpDesc& op = ops[j];
+        const void* rd[3] = {op.x1, op.x2, op.scale_read};
+        const void* wr[2] = {op.dest, op.scale_write};
+        int L = 0;
+        for (const void* q : rd) {
+            if (!q) continue;
+            auto it = use.find(q);
+            if (it != use.end()) L = std::max(L, it->second.written + 1);
+        }
+        for (const void* q : wr) {
+            if (!q) continue;
+            auto it = use.find(q);
+            if (it != use.end())
+                L = std::max(L, std::max(it->second.written, it->second.read) + 1);
+        }
+        level[j] = L;
+        for (const void* q : rd)
+            if (q) use[q].read = std::max(use[q].read, L);
+        for (const void* q : wr)
+            if (q) use[q].written = L;
+    }
+}
+
+// Variants 11-13: the grouped walks with G = 2, 4, 8.  Lists of partition
+// ops run as variant 7.
+template <typename Real, int C, int G>
+cudaError_t run_group4(const OpDesc* h_ops, int nops, const Dims& d, double* cum, int ls,
+                       cudaStream_t s, bool ranged, bool pre) {
+    if (ranged) return run_param4<Real, C, 1>(h_ops, nops, d, cum, ls, s, ranged, pre);
+    if (!h_ops || nops > kParamOps) return cudaErrorInvalidValue;
+    static thread_local GroupParams prm;
+    static thread_local std::vector<int> level, order, first;
+    op_levels(h_ops, nops, level);
+    const int nl = *std::max_element(level.begin(), level.end()) + 1;
+    first.assign(nl + 1, 0);                     // counting sort by level (stable)
+    for (int j = 0; j < nops; ++j) ++first[level[j] + 1];
+    for (int l = 0; l < nl; ++l) first[l + 1] += first[l];
+    order.assign(nops, 0);
+    for (int j = 0; j < nops; ++j) order[first[level[j]]++] = j;
+    int run = 0;
+    for (int k = 0; k < nops; ++k) {
+        prm.op[k] = h_ops[order[k]];
+        prm.size[k] = 0;
+        // a group ends at G ops or at a change of level
+        if (run == 0 || level[order[k]] != level[order[k - 1]] || run == G) {
+            int g = 0;
+            while (g < G && k + g < nops && level[order[k + g]] == level[order[k]]) ++g;
+            prm.size[k] = (unsigned char)g;
+            run = 0;
+        }
+        ++run;
+    }
+    const int ppb = kT4 / C;
+    const int grid = (d.Pp + ppb - 1) / ppb;
+    if (pre) k_walk4g<Real, C, G, true><<<grid, kT4, 0, s>>>(prm, nops, d.Pp, nullptr, ls);
+    else k_walk4g<Real, C, G, false><<<grid, kT4, 0, s>>>(prm, nops, d.Pp, cum, ls);
+    return cudaGetLastError();
+}
+
 template <typename Real, int C, int PPT, bool PRE>
 cudaError_t run_pipe4(const OpDesc* ops, int nops, const Dims& d, double* cum, int ls,
                       cudaStream_t s) {
@@ -521,6 +808,11 @@ cudaError_t run_post4(const OpDesc* ops, const OpDesc* h_ops, int nops, const Di
             case 6: return run_post4_ppt<Real, CC, 2, kMinB6<Real>>(ops, nops, d, cum, ls, s, ranged);
             case 7: return run_param4<Real, CC, 1>(h_ops, nops, d, cum, ls, s, ranged, false);
             case 8: return run_param4<Real, CC, 2>(h_ops, nops, d, cum, ls, s, ranged, false);
+            case 9: return run_slot4<Real, CC, 1>(h_ops, nops, d, cum, ls, s, ranged, false);
+            case 10: return run_slot4<Real, CC, 2>(h_ops, nops, d, cum, ls, s, ranged, false);
+            case 11: return run_group4<Real, CC, 2>(h_ops, nops, d, cum, ls, s, ranged, false);
+            case 12: return run_group4<Real, CC, 4>(h_ops, nops, d, cum, ls, s, ranged, false);
+            case 13: return run_group4<Real, CC, 8>(h_ops, nops, d, cum, ls, s, ranged, false);
             case 1: return run_post4_ppt<Real, CC, 1>(ops, nops, d, cum, ls, s, ranged);
             case 2: return run_post4_ppt<Real, CC, 2>(ops, nops, d, cum, ls, s, ranged);
             default: return run_post4_ppt<Real, CC, 4>(ops, nops, d, cum, ls, s, ranged);
@@ -542,6 +834,11 @@ cudaError_t run_pre4(const OpDesc* ops, const OpDesc* h_ops, int nops, const Dim
             case 6: return run_pre4_ppt<Real, CC, 2, kMinB6<Real>>(ops, nops, d, ls, s, ranged);
             case 7: return run_param4<Real, CC, 1>(h_ops, nops, d, nullptr, ls, s, ranged, true);
             case 8: return run_param4<Real, CC, 2>(h_ops, nops, d, nullptr, ls, s, ranged, true);
+            case 9: return run_slot4<Real, CC, 1>(h_ops, nops, d, nullptr, ls, s, ranged, true);
+            case 10: return run_slot4<Real, CC, 2>(h_ops, nops, d, nullptr, ls, s, ranged, true);
+            case 11: return run_group4<Real, CC, 2>(h_ops, nops, d, nullptr, ls, s, ranged, true);
+            case 12: return run_group4<Real, CC, 4>(h_ops, nops, d, nullptr, ls, s, ranged, true);
+            case 13: return run_group4<Real, CC, 8>(h_ops, nops, d, nullptr, ls, s, ranged, true);
             case 1: return run_pre4_ppt<Real, CC, 1>(ops, nops, d, ls, s, ranged);
             case 2: return run_pre4_ppt<Real, CC, 2>(ops, nops, d, ls, s, ranged);
             default: return run_pre4_ppt<Real, CC, 4>(ops, nops, d, ls, s, ranged);
@@ -553,7 +850,7 @@ cudaError_t run_pre4(const OpDesc* ops, const OpDesc* h_ops, int nops, const Dim
 
 }  // namespace
 
-int s4_walk_variants(int C) { return (32 % C == 0) ? 9 : 1; }
+int s4_walk_variants(int C) { return (32 % C == 0) ? 14 : 1; }
 
 template <typename Real>
 cudaError_t launch_update_partials(const OpDesc* ops, int nops, const Dims& d, double* cum,

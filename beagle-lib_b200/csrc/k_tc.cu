@@ -435,7 +435,7 @@ __device__ __forceinline__ void finish_row(TcSmem& sm, const OpDesc& op, float o
 #pragma unroll
         for (int i = 0; i < NP; ++i) out[i] *= inv;
         if (c == 0 && mine) {
-            const double lm = log((double)m);
+            const double lm = scale_log(m);
             op.scale_write[p] = log_scalers ? lm : (double)m;
             if (cum) cum[p] += lm;
         }

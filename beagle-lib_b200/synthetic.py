@@ -309,12 +309,16 @@ class Problem:
         inst.setPatternWeights(self.patw)
         inst.setTransitionMatrix(self.B, self.scaled_q().reshape(-1), 0.0)
 
-    def evaluate(self, inst, gradient=True, transposed_pre=False, lengths=None, mark=None):
+    def evaluate(self, inst, gradient=True, transposed_pre=False, lengths=None, mark=None,
+                 fused=False):
         """One lnL (+ gradient) evaluation: the call sequence the benchmark times.
 
         updateTransitionMatrices (all B branches) -> updatePartials (N-1 ops) ->
         scale accumulation -> root lnL -> root pre-partials -> updatePrePartials
         (B ops) -> calculateEdgeDerivatives (all B branches, sums only).
+        With ``fused`` the last two are one beagleB200UpdatePrePartialsWithDerivatives
+        call, whose sums come in pre-order op order (``fused_branches()``
+        names the branch of each; ``branch_gradient`` reorders them).
         Returns (lnL, gradient[B] or None)."""
         mark = mark or (lambda name: None)
         t = self.lengths if lengths is None else lengths
@@ -322,9 +326,19 @@ class Problem:
         mark("start")
         inst.updateTransitionMatrices(0, idx, None, None, t)
         mark("matrices")
-        return self._after_matrices(inst, gradient, transposed_pre, mark)
+        return self._after_matrices(inst, gradient, transposed_pre, mark, fused)
 
-    def _after_matrices(self, inst, gradient, transposed_pre, mark):
+    def fused_branches(self):
+        """Branch (node) of each pre-order op: the order of the fused call's sums."""
+        return self.pre_ops()[:, 0] - self.pre(0)
+
+    def branch_gradient(self, sums):
+        """Fused-call sums (op order) as gradient[B] in branch order."""
+        g = np.empty(self.B)
+        g[self.fused_branches()] = sums
+        return g
+
+    def _after_matrices(self, inst, gradient, transposed_pre, mark, fused=False):
         idx = np.arange(self.B, dtype=np.int32)
         inst.updatePartials(self.post_ops(), OP_NONE)
         mark("post")
@@ -342,6 +356,12 @@ class Problem:
             inst.transposeTransitionMatrices(idx, idx + self.B + 1)
         self.set_root_pre(inst)
         mark("rootpre")
+        if fused:
+            nodes = self.fused_branches()
+            sums, _ = inst.updatePrePartialsWithDerivatives(
+                self.pre_ops(transposed_pre), nodes, np.full(self.B, self.B, dtype=np.int32), [0])
+            mark("deriv")
+            return lnl, sums
         inst.updatePrePartials(self.pre_ops(transposed_pre), OP_NONE)
         mark("pre")
         nonroot = np.arange(self.B, dtype=np.int32)
@@ -351,16 +371,17 @@ class Problem:
         mark("deriv")
         return lnl, sums
 
-    def capture(self, inst, transposed_pre=False):
+    def capture(self, inst, transposed_pre=False, fused=False):
         """Record one evaluation after the transition matrices (partials,
         scaling, root lnL, pre-order partials, edge derivatives) as a CUDA
         graph of an ASYNCH instance; returns (graph, gradient array the graph
-        fills).  Runs the sequence once first, as the capture requires."""
-        self.evaluate(inst, transposed_pre=transposed_pre)
+        fills: branch order, or op order with ``fused``).  Runs the sequence
+        once first, as the capture requires."""
+        self.evaluate(inst, transposed_pre=transposed_pre, fused=fused)
         inst.getLogLikelihood()
         inst.beginCapture()
         try:
-            _, grad = self._after_matrices(inst, True, transposed_pre, lambda name: None)
+            _, grad = self._after_matrices(inst, True, transposed_pre, lambda name: None, fused)
         finally:
             graph = inst.endCapture()
         return graph, grad
@@ -392,7 +413,20 @@ class Problem:
         pre = sum(L + rd(op[5]) + L + sc for op in self.pre_ops())
         deriv = sum(L + rd(v) for v in range(self.B))
         mats = self.B * self.C * self.S * self.S * w
-        return dict(matrices=mats, post=post, pre=pre, deriv=deriv)
+        # fused pre-order + derivative walk: a sibling pair reads its parent
+        # row and both children's post-order rows once, writes two rows
+        ops = self.pre_ops()
+        fused, k = 0, 0
+        while k < len(ops):
+            a = ops[k]
+            if k + 1 < len(ops) and ops[k + 1][3] == a[3]:
+                b = ops[k + 1]
+                fused += L + rd(a[5]) + rd(b[5]) + 2 * L + 2 * sc
+                k += 2
+            else:
+                fused += L + rd(a[5]) + rd(a[0] - self.pre(0)) + L + sc
+                k += 1
+        return dict(matrices=mats, post=post, pre=pre, deriv=deriv, fused=fused)
 
 
 def make_problem(S, N, P, C, seed, mean_length=0.1, ambiguous=0.0, rescale=False,

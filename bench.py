@@ -9,7 +9,8 @@ rescaling, FP64 P(t) and reductions):
     -> scale accumulation -> root lnL -> root pre-partials
     -> updatePrePartials (254 ops) -> calculateEdgeDerivatives (254 branches)
 
-through libbeagle_b200.so's C ABI.  ``value`` queues K evaluations on the
+through libbeagle_b200.so's C ABI, the last two as one
+beagleB200UpdatePrePartialsWithDerivatives call.  ``value`` queues K evaluations on the
 instance's stream (ASYNCH instance, inputs resident) and times them with CUDA
 events on that stream; ``e2e`` runs K evaluations that each copy new branch
 lengths in and read lnL and the gradient back (host round trip per step).
@@ -48,7 +49,8 @@ BATCH_WORKLOAD = "batch256"
 
 # Our kernels launched per evaluation: P(t) 1, post-order 1, scale accumulate 1,
 # root lnL 2 (sites + final sum), root pre-partials fill 1, pre-order 1,
-# edge derivatives 2 (branches x pattern blocks + final sum).
+# edge derivatives 2 (branches x pattern blocks + final sum); one fewer when
+# the fused pre-order + derivative walk runs (walk + final sum).
 LAUNCHES_PER_EVAL = 9
 
 
@@ -252,13 +254,16 @@ def make_instance(lib, pr, precision, device, asynch=True, auto_transpose=False)
     return inst
 
 
-def timed_value(torch, inst, pr, steps, warmup, phases=False):
+def timed_value(torch, inst, pr, steps, warmup, phases=False, fused=True):
     """Queue `steps` evaluations (ASYNCH) and time them on the instance's stream.
-    With phases=True also time every phase of every step."""
+    With phases=True also time every phase of every step.  ``fused``: the
+    pre-order walk and the edge derivatives as one
+    beagleB200UpdatePrePartialsWithDerivatives call (the library runs its fused
+    walk or the two calls' kernels, whichever its autotuner timed faster)."""
     stream = torch.cuda.ExternalStream(inst.cudaStream())
     tr = pr.S > 4
     for _ in range(warmup):
-        pr.evaluate(inst, transposed_pre=tr)
+        pr.evaluate(inst, transposed_pre=tr, fused=fused)
         inst.getLogLikelihood()
     ev_marks = []
 
@@ -273,7 +278,7 @@ def timed_value(torch, inst, pr, steps, warmup, phases=False):
     end = torch.cuda.Event(enable_timing=True)
     start.record(stream)
     for _ in range(steps):
-        pr.evaluate(inst, transposed_pre=tr, mark=mark if phases else None)
+        pr.evaluate(inst, transposed_pre=tr, mark=mark if phases else None, fused=fused)
     end.record(stream)
     end.synchronize()
     lnl = inst.getLogLikelihood()
@@ -300,8 +305,9 @@ def timed_e2e(torch, inst, pr, steps):
     start.record(stream)
     for k in range(steps):
         host[:] = pr.lengths * (1.0 + 1e-3 * rng.standard_normal(pr.B))
-        pr.evaluate(inst, transposed_pre=pr.S > 4, lengths=host)
+        _, sums = pr.evaluate(inst, transposed_pre=pr.S > 4, lengths=host, fused=True)
         inst.getLogLikelihood()          # waits for lnL and the gradient sums
+        pr.branch_gradient(sums)
     end.record(stream)
     end.synchronize()
     # bytes per step: the P(t) job table (branch lengths inside) in, lnL + gradient out
@@ -314,7 +320,7 @@ def timed_e2e_graph(torch, inst, pr, steps):
     """As timed_e2e, with everything after the transition matrices replayed
     from a CUDA graph captured once (beagleB200BeginCapture / LaunchGraph)."""
     stream = torch.cuda.ExternalStream(inst.cudaStream())
-    graph, grad = pr.capture(inst, transposed_pre=pr.S > 4)
+    graph, grad = pr.capture(inst, transposed_pre=pr.S > 4, fused=True)
     rng = np.random.default_rng(7)
     lengths = torch.empty(pr.B, dtype=torch.float64).pin_memory()
     host = lengths.numpy()
@@ -327,6 +333,7 @@ def timed_e2e_graph(torch, inst, pr, steps):
     for _ in range(steps):
         host[:] = pr.lengths * (1.0 + 1e-3 * rng.standard_normal(pr.B))
         pr.evaluate_graph(inst, graph, grad, lengths=host)
+        pr.branch_gradient(grad)
     end.record(stream)
     end.synchronize()
     return start.elapsed_time(end)
@@ -416,12 +423,18 @@ def run_b200_arm(args):
     ms_step = ms_total / args.steps
     value = ws * args.steps / (ms_total / 1000.0)
 
-    # per-phase device times (separate pass) for the roofline of the top kernel
+    # per-phase device times (separate pass) for the roofline of the top kernel.
+    # With the fused walk picked, the "deriv" phase is that one kernel (plus
+    # its final sum); otherwise the phases of the two calls are timed apart.
+    tuned = inst.tunedVariants()
+    fused_walk = tuned["fused"] == 1
     nph = max(5, min(50, args.steps // 4))
-    _, _, phases = timed_value(torch, inst, pr, nph, 1, phases=True)
+    _, _, phases = timed_value(torch, inst, pr, nph, 1, phases=True, fused=fused_walk)
     ph_ms = {k: float(np.mean(v)) for k, v in phases.items()}
+    if fused_walk:
+        ph_ms["fused"] = ph_ms.pop("deriv")
     alg = pr.algorithmic_bytes(4)
-    kern = max(["post", "pre", "deriv"], key=lambda k: ph_ms.get(k, 0))
+    kern = max(["post", "pre", "deriv", "fused"], key=lambda k: ph_ms.get(k, 0))
     peak, peak_kind = peaks()
     achieved = alg[kern] / (ph_ms[kern] * 1e-3) / 1e9
     traffic = None
@@ -482,7 +495,8 @@ def run_b200_arm(args):
                            "mixed_over_fp64": value / value64,
                            "mixed_vs_fp64_rel_lnl_err": rel_err},
             "lnl": lnl,
-            "gpu_launches": LAUNCHES_PER_EVAL * args.steps,
+            "gpu_launches": (LAUNCHES_PER_EVAL - (1 if fused_walk else 0)) * args.steps,
+            "tuned_variants": tuned,
             "clocks": clocks_info,
         }
         print(json.dumps(line))

@@ -277,6 +277,25 @@ int beagleB200CalculateEdgeDerivatives(int instance, const int* postBufferIndice
                                        const int* categoryWeightsIndices, int count,
                                        double* outDerivatives, double* outSumDerivatives,
                                        double* outSumSquaredDerivatives);
+/* Extension, no beagle.h counterpart: beagleUpdatePrePartials(operations,
+ * count, BEAGLE_OP_NONE) followed by beagleCalculateEdgeDerivatives over
+ * (postBufferIndices[k], destination of operation k, derivativeMatrixIndices[k])
+ * for k < count, sums only.  Same results and error codes as those two calls.
+ * For 4-state instances with 1, 2, 4 or 8 categories and at most 256
+ * operations, one kernel walks the list and forms each branch's derivative
+ * from the pre-order row it has just computed (sibling pairs share their
+ * loads); other shapes run the two calls. */
+int beagleB200UpdatePrePartialsWithDerivatives(int instance, const int* operations, int count,
+                                               const int* postBufferIndices,
+                                               const int* derivativeMatrixIndices,
+                                               const int* categoryWeightsIndices,
+                                               double* outSumDerivatives,
+                                               double* outSumSquaredDerivatives);
+/* Extension, diagnostics: the kernel variant the autotuner last ran for this
+ * instance, per kind: outVariants[0] post-order walk, [1] pre-order walk,
+ * [2] edge derivatives, [3] fused pre-order + derivatives (0 = the two
+ * calls' kernels, 1 = the fused walk).  -1 = default shape, -2 = not run. */
+int beagleB200GetTunedVariants(int instance, int* outVariants);
 /* replaces beagleCalculateCrossProductDerivative (beagle.h:1228-1236) */
 int beagleB200CalculateCrossProductDerivative(int instance, const int* postBufferIndices,
                                               const int* preBufferIndices,

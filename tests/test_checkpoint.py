@@ -92,3 +92,28 @@ def test_checkpointed_gpu_matches_full(b200, pkg, syn, precision, S, N, C):
         assert grad_err(gradient(), g0) <= tol["grad"], step
     for x in (full, inst, gi):
         x.finalize()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["double", "single"])
+@pytest.mark.parametrize("variant", [1, 7, 9, 11, 12, 13])
+def test_checkpointed_buffer_reuse_each_s4_walk(b200, pkg, syn, monkeypatch, precision, variant):
+    """The checkpointed schedule reuses buffers inside one op list (a result's
+    buffer becomes a later op's destination): every S = 4 walk shape, the
+    level-reordering ones included, must keep those write-after-read orders."""
+    monkeypatch.setenv("BEAGLE_B200_FORCE_VARIANT", f"{variant},{variant},1")
+    ck = pkg.checkpoint
+    pr = syn.make_problem(S=4, N=48, P=700, C=4, seed=77, rescale=True)
+    pref, req = gpu_flags(precision)
+    full = b200.create(*pr.create_args(), preferenceFlags=pref, requirementFlags=req)
+    pr.load(full)
+    l0, g0 = pr.evaluate(full)
+    plan = ck.CheckpointPlan(pr, 3)
+    inst = b200.create(*plan.create_args(), preferenceFlags=pref, requirementFlags=req)
+    pr.load(inst)
+    l1, g1 = plan.evaluate(inst)
+    tol = TOL[precision]
+    assert rel(l1, l0) <= tol["lnl"], (l1, l0)
+    assert grad_err(g1, g0) <= tol["grad"]
+    full.finalize()
+    inst.finalize()

@@ -1,0 +1,99 @@
+"""beagleB200UpdatePrePartialsWithDerivatives: the pre-order walk and the edge
+derivatives of its branches in one kernel (4-state) against the two separate
+calls and the oracle, for every category count the fused walk takes, tips as
+states and as partials, with and without rescaling; lists without sibling
+pairs, lists too long for the fused walk, other state counts (both run as
+the separate calls), and a captured graph."""
+import numpy as np
+import pytest
+
+from helpers import TOL, gpu_flags, grad_err, rel, run_oracle
+
+pytestmark = pytest.mark.gpu
+
+ASYNCH = 1 << 3
+
+
+def _pair(b200, pr, precision, **kw):
+    pref, req = gpu_flags(precision)
+    inst = b200.create(*pr.create_args(), preferenceFlags=pref | kw.get("extra", 0),
+                       requirementFlags=req)
+    pr.load(inst)
+    return inst
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+@pytest.mark.parametrize("C,rescale,amb", [(1, True, 0.0), (2, False, 0.03), (4, True, 0.03),
+                                           (8, True, 0.0)])
+def test_fused_matches_separate_calls_and_oracle(b200, syn, oracle, precision, C, rescale, amb):
+    pr = syn.make_problem(S=4, N=33, P=1300, C=C, seed=500 + C, rescale=rescale, ambiguous=amb)
+    inst = _pair(b200, pr, precision)
+    l0, g0 = pr.evaluate(inst)
+    l1, sums = pr.evaluate(inst, fused=True)
+    g1 = pr.branch_gradient(sums)
+    _, lo, go = run_oracle(oracle, pr)
+    tol = TOL[precision]
+    assert rel(l1, l0) == 0.0
+    assert grad_err(g1, g0) <= tol["grad"] * 1e-2, grad_err(g1, g0)
+    assert grad_err(g1, go) <= tol["grad"], grad_err(g1, go)
+    # the pre-order buffers the fused walk wrote are the separate walk's
+    for v in (0, pr.N, pr.B - 1):
+        a = inst.getPartials(pr.pre(v))
+        pr.evaluate(inst)
+        b = inst.getPartials(pr.pre(v))
+        assert np.array_equal(a, b), v
+    inst.finalize()
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_fused_without_sibling_pairs(b200, syn, precision):
+    """Pre-order ops sorted by depth, then by node: siblings are not adjacent,
+    so every op runs on its own (three loads, one store)."""
+    pr = syn.make_problem(S=4, N=40, P=900, C=4, seed=61, rescale=True)
+    inst = _pair(b200, pr, precision)
+    l0, g0 = pr.evaluate(inst)
+    ops = pr.pre_ops()
+    depth = {pr.pre(pr.root): 0}
+    for op in ops:
+        depth[op[0]] = depth[op[3]] + 1
+    ops = ops[np.lexsort((ops[:, 0] % 7, [depth[o[0]] for o in ops]))]
+    adjacent = sum(1 for a, b in zip(ops, ops[1:]) if a[3] == b[3])
+    assert adjacent < len(ops) // 4
+    nodes = ops[:, 0] - pr.pre(0)
+    sums, _ = inst.updatePrePartialsWithDerivatives(ops, nodes, np.full(pr.B, pr.B), [0])
+    g1 = np.empty(pr.B)
+    g1[nodes] = sums
+    assert grad_err(g1, g0) <= TOL[precision]["grad"] * 1e-2
+    inst.finalize()
+
+
+@pytest.mark.parametrize("S,N", [(4, 150), (20, 12)])
+def test_fused_call_falls_back_to_separate_calls(b200, syn, oracle, S, N):
+    """More than 256 ops (N = 150: 298) or S != 4: the same call runs the two
+    separate calls, same results."""
+    pr = syn.make_problem(S=S, N=N, P=500, C=4, seed=7 + S, rescale=True)
+    inst = _pair(b200, pr, "double")
+    tr = S > 4
+    l0, g0 = pr.evaluate(inst, transposed_pre=tr)
+    l1, sums = pr.evaluate(inst, transposed_pre=tr, fused=True)
+    assert rel(l1, l0) == 0.0
+    assert grad_err(pr.branch_gradient(sums), g0) <= 1e-12
+    inst.finalize()
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_fused_graph_replay(b200, syn, precision):
+    pr = syn.make_problem(S=4, N=30, P=2000, C=4, seed=88, rescale=True)
+    plain = _pair(b200, pr, precision)
+    gi = _pair(b200, pr, precision, extra=ASYNCH)
+    graph, raw = pr.capture(gi, fused=True)
+    rng = np.random.default_rng(2)
+    tol = TOL[precision]
+    for step in range(3):
+        t = pr.lengths * (1 + 0.05 * rng.standard_normal(pr.B))
+        l0, g0 = pr.evaluate(plain, lengths=t)
+        l1, _ = pr.evaluate_graph(gi, graph, raw, lengths=t)
+        assert rel(l1, l0) <= tol["lnl"], step
+        assert grad_err(pr.branch_gradient(raw), g0) <= tol["grad"], step
+    plain.finalize()
+    gi.finalize()

@@ -9,7 +9,7 @@ relative lnL <= 1e-6 and gradient error <= 1e-4.
 import numpy as np
 import pytest
 
-from helpers import TOL, grad_err, rel, run_b200, run_oracle, gpu_flags
+from helpers import SCALERS_LOG, TOL, grad_err, rel, run_b200, run_oracle, gpu_flags
 
 pytestmark = pytest.mark.gpu
 
@@ -174,7 +174,7 @@ def test_full_size_configs(b200, syn, oracle, name, precision):
 
 
 @pytest.mark.parametrize("precision", ["double", "single"])
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("variant", list(range(14)))
 def test_s4_kernel_variants(b200, syn, oracle, monkeypatch, precision, variant):
     """Every S = 4 op-walk and derivative kernel shape the autotuner can pick
     (forced through BEAGLE_B200_FORCE_VARIANT) against the oracle, with C = 4
@@ -189,6 +189,34 @@ def test_s4_kernel_variants(b200, syn, oracle, monkeypatch, precision, variant):
         tol = TOL[precision]
         assert rel(lnl, lo) <= tol["lnl"], (C, lnl, lo)
         assert grad_err(g, go) <= tol["grad"], (C, grad_err(g, go))
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+@pytest.mark.parametrize("variant", [9, 10, 12])
+def test_s4_slot_walks_more_live_values_than_slots(b200, syn, oracle, monkeypatch, precision,
+                                                   variant):
+    """The slot walks on a post-order list in height order (every cherry
+    first, then their parents, ...): far more results are live at once than
+    there are slots, so most operands come back from device memory; and with
+    the pre-order list reversed per level likewise."""
+    monkeypatch.setenv("BEAGLE_B200_FORCE_VARIANT", str(variant))
+    pr = syn.make_problem(S=4, N=96, P=1100, C=4, seed=321, rescale=True)
+    ops = pr.post_ops()
+    height = {}
+    for op in ops:                      # post order: children first
+        height[op[0]] = 1 + max(height.get(op[3], 0), height.get(op[5], 0))
+    by_height = ops[np.argsort([height[o[0]] for o in ops], kind="stable")]
+    pref, req = gpu_flags(precision)
+    res = []
+    for x in (b200.create(*pr.create_args(), preferenceFlags=pref, requirementFlags=req),
+              oracle.OracleInstance(*pr.create_args(), flags=SCALERS_LOG)):
+        pr.load(x)
+        x.updateTransitionMatrices(0, np.arange(pr.B, dtype=np.int32), None, None, pr.lengths)
+        x.updatePartials(by_height, -1)
+        x.resetScaleFactors(pr.cumulative)
+        x.accumulateScaleFactors(np.arange(pr.N - 1, dtype=np.int32), pr.cumulative)
+        res.append(x.calculateRootLogLikelihoods([pr.root], [0], [0], [pr.cumulative]))
+    assert rel(res[0], res[1]) <= TOL[precision]["lnl"], res
 
 
 @pytest.mark.parametrize("precision", ["double", "single"])
