@@ -1201,6 +1201,10 @@ int Instance::updatePrePartialsWithDerivatives(const int* ops, int count, const 
                           b[0] != a[5] && b[0] != post[k];
         if (pair) {
             fops[k].kind |= kPairFirst;
+            const PreDerivOp &fa = fops[k], &fb = fops[k + 1];
+            if (fa.mnode == fb.msib && fa.msib == fb.mnode &&
+                !((fa.kind | fb.kind) & kM1Transposed))
+                fops[k].kind |= kPairMats;
             ++k;
         }
     }

@@ -24,6 +24,7 @@ enum OpKind : int {
     kM1Transposed = 4,  // pre-order: the node's matrix is given as its transpose
     kPostStates = 8,    // fused pre-order op: the node's own post-order operand is tip states
     kPairFirst = 16,    // fused pre-order op: this op and the next are a sibling pair
+    kPairMats = 32,     // ... whose two ops use the same two matrices, untransposed
 };
 
 // One resolved partials operation (post-order or pre-order).  Post-order:

@@ -76,6 +76,35 @@ __device__ __forceinline__ void apply_node(const Real* M, bool tr, const Real z[
     }
 }
 
+// y = M x for a register-held M (row-major 4 x 4), or column s of M for a tip
+// state (pad for the missing state).
+template <typename Real>
+__device__ __forceinline__ void operand4r(const Real m[16], bool states, int s, const Real x[4],
+                                          Real pad, Real y[4]) {
+    if (states) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            Real v = pad;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (s == j) v = m[i * 4 + j];
+            y[i] = v;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            y[i] = m[i * 4] * x[0] + m[i * 4 + 1] * x[1] + m[i * 4 + 2] * x[2] + m[i * 4 + 3] * x[3];
+    }
+}
+
+// out_j = sum_i m[i][j] z_i for a register-held m.
+template <typename Real>
+__device__ __forceinline__ void apply_reg(const Real m[16], const Real z[4], Real out[4]) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        out[j] = m[j] * z[0] + m[4 + j] * z[1] + m[8 + j] * z[2] + m[12 + j] * z[3];
+}
+
 // num / den: FP64 division; FP32 through the hardware reciprocal (__fdividef,
 // 2 ulp), within the FP32 partials' own error.
 __device__ __forceinline__ double quotient(double a, double b) { return a / b; }
@@ -153,10 +182,11 @@ __device__ __forceinline__ void load_row(const void* x, bool states, int pc, int
     else ld4(static_cast<const Real*>(x) + ((size_t)pc * C + c) * 4, v);
 }
 
-// Resident CTAs per SM: FP32 4 (64 registers a thread), 3 when the shared
-// derivative matrix is held in registers; FP64 2.
-template <typename Real, int C, bool SHARED_D>
-__global__ void __launch_bounds__(kT4, sizeof(Real) == 4 ? (SHARED_D ? 3 : 4) : 2)
+// MATS: every sibling pair's two ops use the same two matrices (kPairMats),
+// held in registers.  Resident CTAs per SM: FP32 4 (64 registers a thread),
+// 3 with matrices or the shared derivative matrix in registers; FP64 2.
+template <typename Real, int C, bool SHARED_D, bool MATS>
+__global__ void __launch_bounds__(kT4, sizeof(Real) == 4 ? (SHARED_D || MATS ? 3 : 4) : 2)
 k_pre_deriv4(const __grid_constant__ FusedParams F, int nops, int P, int Pp,
              const double* __restrict__ catw, const double* __restrict__ patw, int log_scalers,
              double* block) {
@@ -188,16 +218,39 @@ k_pre_deriv4(const __grid_constant__ FusedParams F, int nops, int P, int Pp,
             load_row(A.post, sta, pc, C, c, xa, sa);     // post[a] (= B's sibling)
             load_row(A.sib, stb, pc, C, c, xb, sb);      // post[b] (= A's sibling)
             Real ya[4], yb[4], za[4], zb[4], pa[4], pb[4];
-            operand4c(static_cast<const Real*>(A.msib) + c * 16, stb, sb, xb, (Real)A.pad_sib, yb);
-            operand4c(static_cast<const Real*>(B.msib) + c * 16, sta, sa, xa, (Real)B.pad_sib, ya);
+            if (MATS) {
+                // P_a and P_b serve both ops: loaded once, kept in registers
+                Real ma[16], mb[16];
+                const Real* Ma = static_cast<const Real*>(A.mnode) + c * 16;
+                const Real* Mb = static_cast<const Real*>(A.msib) + c * 16;
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                za[i] = pv[i] * yb[i];
-                zb[i] = pv[i] * ya[i];
+                for (int k = 0; k < 4; ++k) {
+                    ldg4(Ma + 4 * k, ma + 4 * k);
+                    ldg4(Mb + 4 * k, mb + 4 * k);
+                }
+                operand4r(mb, stb, sb, xb, (Real)A.pad_sib, yb);
+                operand4r(ma, sta, sa, xa, (Real)B.pad_sib, ya);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    za[i] = pv[i] * yb[i];
+                    zb[i] = pv[i] * ya[i];
+                }
+                apply_reg(ma, za, pa);
+                apply_reg(mb, zb, pb);
+            } else {
+                operand4c(static_cast<const Real*>(A.msib) + c * 16, stb, sb, xb,
+                          (Real)A.pad_sib, yb);
+                operand4c(static_cast<const Real*>(B.msib) + c * 16, sta, sa, xa,
+                          (Real)B.pad_sib, ya);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    za[i] = pv[i] * yb[i];
+                    zb[i] = pv[i] * ya[i];
+                }
+                apply_node(static_cast<const Real*>(A.mnode) + c * 16, tra, za, pa);
+                apply_node(static_cast<const Real*>(B.mnode) + c * 16,
+                           (B.kind & kM1Transposed) != 0, zb, pb);
             }
-            apply_node(static_cast<const Real*>(A.mnode) + c * 16, tra, za, pa);
-            apply_node(static_cast<const Real*>(B.mnode) + c * 16, (B.kind & kM1Transposed) != 0,
-                       zb, pb);
             rescale_store4<Real, C>(A, pa, pc, valid, c, log_scalers);
             rescale_store4<Real, C>(B, pb, pc, valid, c, log_scalers);
             const Real da = deriv_value<Real, C, SHARED_D>(A, dm, pa, xa, sa, sta, c, w);
@@ -245,17 +298,25 @@ cudaError_t launch_pre_deriv4(const PreDerivOp* h_ops, int nops, const Dims& d,
     bool shared_d = true;             // one derivative matrix for every branch
     for (int k = 1; k < nops; ++k)
         shared_d = shared_d && h_ops[k].dmat == h_ops[0].dmat && h_ops[k].dpad == h_ops[0].dpad;
-#define PD_(CC)                                                                            \
-    (shared_d ? (k_pre_deriv4<Real, CC, true><<<grid, kT4, 0, s>>>(prm, nops, d.P, d.Pp, catw, \
-                                                                  patw, ls, d_block), 0)    \
-              : (k_pre_deriv4<Real, CC, false><<<grid, kT4, 0, s>>>(prm, nops, d.P, d.Pp,  \
+    // Every pair shares its two matrices: FP32 holds them in registers (and
+    // loads the derivative matrix per op: both in registers would spill).
+    bool mats = sizeof(Real) == 4;
+    for (int k = 0; k < nops; ++k)
+        if ((h_ops[k].kind & kPairFirst) && !(h_ops[k].kind & kPairMats)) mats = false;
+    if (mats) shared_d = false;
+#define PD2_(CC, SD)                                                                        \
+    (mats ? (k_pre_deriv4<Real, CC, SD, true><<<grid, kT4, 0, s>>>(prm, nops, d.P, d.Pp, catw,  \
+                                                                  patw, ls, d_block), 0)     \
+          : (k_pre_deriv4<Real, CC, SD, false><<<grid, kT4, 0, s>>>(prm, nops, d.P, d.Pp,    \
                                                                    catw, patw, ls, d_block), 0))
+#define PD_(CC) (shared_d ? PD2_(CC, true) : PD2_(CC, false))
     switch (d.C) {
         case 1: PD_(1); break;
         case 2: PD_(2); break;
         case 4: PD_(4); break;
         default: PD_(8); break;
     }
+#undef PD2_
 #undef PD_
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
