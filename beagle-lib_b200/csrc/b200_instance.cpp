@@ -1205,6 +1205,7 @@ int Instance::updatePrePartialsWithDerivatives(const int* ops, int count, const 
             if (fa.mnode == fb.msib && fa.msib == fb.mnode &&
                 !((fa.kind | fb.kind) & kM1Transposed))
                 fops[k].kind |= kPairMats;
+            if (fa.dmat == fb.dmat && fa.dpad == fb.dpad) fops[k].kind |= kPairD;
             ++k;
         }
     }

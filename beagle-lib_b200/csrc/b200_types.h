@@ -25,6 +25,7 @@ enum OpKind : int {
     kPostStates = 8,    // fused pre-order op: the node's own post-order operand is tip states
     kPairFirst = 16,    // fused pre-order op: this op and the next are a sibling pair
     kPairMats = 32,     // ... whose two ops use the same two matrices, untransposed
+    kPairD = 64,        // ... whose two branches share one derivative matrix
 };
 
 // One resolved partials operation (post-order or pre-order).  Post-order:

@@ -253,8 +253,19 @@ k_pre_deriv4(const __grid_constant__ FusedParams F, int nops, int P, int Pp,
             }
             rescale_store4<Real, C>(A, pa, pc, valid, c, log_scalers);
             rescale_store4<Real, C>(B, pb, pc, valid, c, log_scalers);
-            const Real da = deriv_value<Real, C, SHARED_D>(A, dm, pa, xa, sa, sta, c, w);
-            const Real db = deriv_value<Real, C, SHARED_D>(B, dm, pb, xb, sb, stb, c, w);
+            Real da, db;
+            if (!SHARED_D && (A.kind & kPairD)) {
+                // one derivative matrix for both branches: loaded once
+                Real dp[16];
+                const Real* D = static_cast<const Real*>(A.dmat) + c * 16;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) ldg4(D + 4 * k, dp + 4 * k);
+                da = deriv_value<Real, C, true>(A, dp, pa, xa, sa, sta, c, w);
+                db = deriv_value<Real, C, true>(B, dp, pb, xb, sb, stb, c, w);
+            } else {
+                da = deriv_value<Real, C, SHARED_D>(A, dm, pa, xa, sa, sta, c, w);
+                db = deriv_value<Real, C, SHARED_D>(B, dm, pb, xb, sb, stb, c, w);
+            }
             warp_emit<Real, C>(counted ? da : Real(0), wp, o, nops, nblk, wid, block);
             warp_emit<Real, C>(counted ? db : Real(0), wp, o + 1, nops, nblk, wid, block);
             o += 2;
