@@ -1216,8 +1216,9 @@ int Instance::updatePrePartialsWithDerivatives(const int* ops, int count, const 
     CK(t_deriv_.upload(dtab.data(), sizeof(DerivDesc) * count, stream_));
     const double* catw = d_catw_ + (size_t)w * C_;
     const int ls = (int)log_scalers_;
-    // Both variants leave the sums in out_.  0: the pre-order walk and the
-    // derivative kernels of the two calls; 1: the fused walk.  The autotuner
+    // Every variant leaves the sums in out_.  0: the pre-order walk and the
+    // derivative kernels of the two calls; 1: the fused walk; 2: its
+    // pairs-only form with 2 patterns a thread (FP32 lists of sibling pairs).  The autotuner
     // times them when the list may run repeatedly (no op reads what a later
     // op writes); the first, untimed run also settles the two calls' own
     // autotuner choices.
@@ -1236,13 +1237,19 @@ int Instance::updatePrePartialsWithDerivatives(const int* ops, int count, const 
             return deriv(dv);
         }
         return LAUNCH(launch_pre_deriv4, fops.data(), count, dm, catw, d_patw_, ls,
-                      (double*)scratch_.ptr, (double*)out_.ptr, stream_);
+                      (double*)scratch_.ptr, (double*)out_.ptr, stream_, v);
     };
     const TuneKey key{kTuneFused, (int)dbl_, C_, Pp_, tune_count_class(count), device_};
-    int v = tune_pick(key, 2, idempotent, stream_, run);
+    int v = tune_pick(key, 3, idempotent, stream_, run);
     if (v < 0) v = 1;
+    cudaError_t e = run(v);
+    if (e == cudaErrorInvalidValue && v == 2) {   // a forced pairs-only form the list refuses
+        (void)cudaGetLastError();
+        v = 1;
+        e = run(v);
+    }
     picked_[kTuneFused] = v;
-    CK(run(v));
+    CK(e);
     return deliver_sums(count, nullptr, outSum, outSumSq);
 }
 

@@ -135,10 +135,12 @@ cudaError_t launch_deriv_final(const double* d_block, int nblk, int nb, double* 
 // doubles; d_sums receives the nops sums, then the nops sums of squares.
 bool fused_supported(const Dims& d, int nops);
 int fused_blocks(const Dims& d);
+// variant 1: the walk of k_fused.cu; 2: pairs-only FP32 lists, 2 patterns a
+// thread (cudaErrorInvalidValue for other lists).
 template <typename Real>
 cudaError_t launch_pre_deriv4(const PreDerivOp* h_ops, int nops, const Dims& d,
                               const double* catw, const double* patw, int ls, double* d_block,
-                              double* d_sums, cudaStream_t s);
+                              double* d_sums, cudaStream_t s, int variant);
 
 // ---- batched launches over several instances (segment tables on the device;
 // ncta = the segments' total CTAs; see b200_types.h) ------------------------

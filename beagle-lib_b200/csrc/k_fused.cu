@@ -175,6 +175,21 @@ __device__ __forceinline__ void warp_emit(Real v, Real wp, int k, int nops, int 
     }
 }
 
+// As warp_emit, for terms already weighted: (sum w d, sum w d^2).
+template <typename Real, int C>
+__device__ __forceinline__ void warp_emit2(Real s1, Real s2, int k, int nops, int nblk, int wid,
+                                           double* block) {
+#pragma unroll
+    for (int o = C; o < 32; o <<= 1) {
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        block[(size_t)k * nblk + wid] = (double)s1;
+        block[(size_t)(nops + k) * nblk + wid] = (double)s2;
+    }
+}
+
 template <typename Real>
 __device__ __forceinline__ void load_row(const void* x, bool states, int pc, int C, int c,
                                          Real v[4], int& s) {
@@ -288,6 +303,86 @@ k_pre_deriv4(const __grid_constant__ FusedParams F, int nops, int P, int Pp,
     }
 }
 
+// Lists made only of sibling pairs that share their matrices and derivative
+// matrix (kPairFirst | kPairMats | kPairD on every even op), FP32: PPT
+// patterns per thread (p, p + grid stride, ...), so each pair step's matrix
+// loads, descriptor reads and warp reductions serve PPT patterns.
+template <int C, int PPT>
+__global__ void __launch_bounds__(kT4, 2)
+k_pre_deriv4_pairs(const __grid_constant__ FusedParams F, int nops, int P, int Pp,
+                   const double* __restrict__ catw, const double* __restrict__ patw,
+                   int log_scalers, double* block) {
+    using Real = float;
+    const int c = threadIdx.x % C;
+    const int pstride = gridDim.x * (kT4 / C);
+    const int p0 = blockIdx.x * (kT4 / C) + threadIdx.x / C;
+    int pc[PPT];
+    bool valid[PPT];
+    Real wp[PPT];
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+        const int p = p0 + k * pstride;
+        valid[k] = p < Pp;
+        pc[k] = valid[k] ? p : Pp - 1;
+        wp[k] = (c == 0 && p < P) ? (Real)patw[p] : Real(0);
+    }
+    const Real w = (Real)catw[c];
+    const int nblk = gridDim.x * (kT4 / 32);
+    const int wid = blockIdx.x * (kT4 / 32) + threadIdx.x / 32;
+    for (int o = 0; o < nops; o += 2) {
+        const PreDerivOp& A = F.op[o];
+        const PreDerivOp& B = F.op[o + 1];
+        const bool sta = A.kind & kPostStates, stb = A.kind & kX2States;
+        Real ma[16], mb[16];
+        const Real* Ma = static_cast<const Real*>(A.mnode) + c * 16;
+        const Real* Mb = static_cast<const Real*>(A.msib) + c * 16;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            ldg4(Ma + 4 * k, ma + 4 * k);
+            ldg4(Mb + 4 * k, mb + 4 * k);
+        }
+        Real pa[PPT][4], pb[PPT][4], xa[PPT][4], xb[PPT][4];
+        int sa[PPT], sb[PPT];
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) {
+            Real pv[4], ya[4], yb[4], za[4], zb[4];
+            ld4(static_cast<const Real*>(A.parent) + ((size_t)pc[k] * C + c) * 4, pv);
+            sa[k] = sb[k] = 0;
+            load_row(A.post, sta, pc[k], C, c, xa[k], sa[k]);
+            load_row(A.sib, stb, pc[k], C, c, xb[k], sb[k]);
+            operand4r(mb, stb, sb[k], xb[k], (Real)A.pad_sib, yb);
+            operand4r(ma, sta, sa[k], xa[k], (Real)B.pad_sib, ya);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                za[i] = pv[i] * yb[i];
+                zb[i] = pv[i] * ya[i];
+            }
+            apply_reg(ma, za, pa[k]);
+            apply_reg(mb, zb, pb[k]);
+            rescale_store4<Real, C>(A, pa[k], pc[k], valid[k], c, log_scalers);
+            rescale_store4<Real, C>(B, pb[k], pc[k], valid[k], c, log_scalers);
+        }
+        Real dp[16];
+        const Real* D = static_cast<const Real*>(A.dmat) + c * 16;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) ldg4(D + 4 * k, dp + 4 * k);
+        Real a1 = 0, a2 = 0, b1 = 0, b2 = 0;
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) {
+            const Real da = deriv_value<Real, C, true>(A, dp, pa[k], xa[k], sa[k], sta, c, w);
+            const Real db = deriv_value<Real, C, true>(B, dp, pb[k], xb[k], sb[k], stb, c, w);
+            const Real ea = wp[k] != Real(0) ? da : Real(0);
+            const Real eb = wp[k] != Real(0) ? db : Real(0);
+            a1 += ea * wp[k];
+            a2 += ea * ea * wp[k];
+            b1 += eb * wp[k];
+            b2 += eb * eb * wp[k];
+        }
+        warp_emit2<Real, C>(a1, a2, o, nops, nblk, wid, block);
+        warp_emit2<Real, C>(b1, b2, o + 1, nops, nblk, wid, block);
+    }
+}
+
 }  // namespace
 
 int fused_blocks(const Dims& d) { return (d.Pp + kT4 / d.C - 1) / (kT4 / d.C) * (kT4 / 32); }
@@ -300,11 +395,28 @@ bool fused_supported(const Dims& d, int nops) {
 template <typename Real>
 cudaError_t launch_pre_deriv4(const PreDerivOp* h_ops, int nops, const Dims& d,
                               const double* catw, const double* patw, int ls, double* d_block,
-                              double* d_sums, cudaStream_t s) {
+                              double* d_sums, cudaStream_t s, int variant) {
     if (nops == 0) return cudaSuccess;
     if (!fused_supported(d, nops)) return cudaErrorInvalidValue;
     static thread_local FusedParams prm;
     std::memcpy(prm.op, h_ops, sizeof(PreDerivOp) * nops);
+    if (variant == 2) {
+        // pairs-only lists, FP32, 2 patterns per thread
+        constexpr int kAll = kPairFirst | kPairMats | kPairD;
+        if (sizeof(Real) != 4 || nops % 2) return cudaErrorInvalidValue;
+        for (int k = 0; k < nops; k += 2)
+            if ((h_ops[k].kind & kAll) != kAll) return cudaErrorInvalidValue;
+        const int grid2 = (d.Pp + 2 * (kT4 / d.C) - 1) / (2 * (kT4 / d.C));
+        switch (d.C) {
+            case 1: k_pre_deriv4_pairs<1, 2><<<grid2, kT4, 0, s>>>(prm, nops, d.P, d.Pp, catw, patw, ls, d_block); break;
+            case 2: k_pre_deriv4_pairs<2, 2><<<grid2, kT4, 0, s>>>(prm, nops, d.P, d.Pp, catw, patw, ls, d_block); break;
+            case 4: k_pre_deriv4_pairs<4, 2><<<grid2, kT4, 0, s>>>(prm, nops, d.P, d.Pp, catw, patw, ls, d_block); break;
+            default: k_pre_deriv4_pairs<8, 2><<<grid2, kT4, 0, s>>>(prm, nops, d.P, d.Pp, catw, patw, ls, d_block); break;
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        return launch_deriv_final(d_block, grid2 * (kT4 / 32), nops, d_sums, s);
+    }
     const int grid = (d.Pp + kT4 / d.C - 1) / (kT4 / d.C);
     bool shared_d = true;             // one derivative matrix for every branch
     for (int k = 1; k < nops; ++k)
@@ -335,9 +447,10 @@ cudaError_t launch_pre_deriv4(const PreDerivOp* h_ops, int nops, const Dims& d,
 }
 
 template cudaError_t launch_pre_deriv4<float>(const PreDerivOp*, int, const Dims&, const double*,
-                                              const double*, int, double*, double*, cudaStream_t);
+                                              const double*, int, double*, double*, cudaStream_t,
+                                              int);
 template cudaError_t launch_pre_deriv4<double>(const PreDerivOp*, int, const Dims&, const double*,
                                                const double*, int, double*, double*,
-                                               cudaStream_t);
+                                               cudaStream_t, int);
 
 }  // namespace b200

@@ -25,7 +25,12 @@ def _pair(b200, pr, precision, **kw):
 @pytest.mark.parametrize("precision", ["double", "single"])
 @pytest.mark.parametrize("C,rescale,amb", [(1, True, 0.0), (2, False, 0.03), (4, True, 0.03),
                                            (8, True, 0.0)])
-def test_fused_matches_separate_calls_and_oracle(b200, syn, oracle, precision, C, rescale, amb):
+@pytest.mark.parametrize("form", [1, 2])
+def test_fused_matches_separate_calls_and_oracle(b200, syn, oracle, monkeypatch, precision, C,
+                                                 rescale, amb, form):
+    """form 1: the fused walk; 2: its pairs-only, 2-patterns-a-thread form
+    (FP32 only: an FP64 instance forced to it runs form 1)."""
+    monkeypatch.setenv("BEAGLE_B200_FORCE_VARIANT", f"-1,-1,-1,{form}")
     pr = syn.make_problem(S=4, N=33, P=1300, C=C, seed=500 + C, rescale=rescale, ambiguous=amb)
     inst = _pair(b200, pr, precision)
     l0, g0 = pr.evaluate(inst)
