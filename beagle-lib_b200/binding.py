@@ -467,6 +467,7 @@ class Instance:
 
 # beagleB200 batch entry points: name -> argument types.
 _BATCH_SIGS = {
+    "BatchBeginCapture": [_i], "BatchEndCapture": [_i, _p], "BatchLaunchGraph": [_i, _i],
     "CreateBatch": [_p, _i], "FinalizeBatch": [_i],
     "BatchUpdateTransitionMatrices": [_i, _p, _p, _p, _p],
     "BatchUpdatePartials": [_i, _p, _p, _p],
@@ -553,12 +554,38 @@ class Batch:
     def wait(self):
         """Deliver deferred results (ASYNCH members) into the arrays returned
         by the result calls."""
-        return self._call("BatchWait")
+        code = self._call("BatchWait")
+        self._keep = []
+        return code
+
+    # CUDA graphs of batch calls (ASYNCH members)
+    def beginCapture(self):
+        self._capturing = True
+        return self._call("BatchBeginCapture")
+
+    def endCapture(self):
+        self._capturing = False
+        g = ctypes.c_int(-1)
+        self._call("BatchEndCapture", ctypes.byref(g))
+        return g.value
+
+    def launchGraph(self, graph):
+        return self._call("BatchLaunchGraph", graph)
+
+    def _keep_result(self, *arrays):
+        """Result arrays stay alive until the wait() that fills them (ASYNCH
+        members), and with the batch when a captured call fills them at every
+        graph launch."""
+        if getattr(self, "_capturing", False):
+            self.__dict__.setdefault("_graph_keep", []).append(arrays)
+        else:
+            self.__dict__.setdefault("_keep", []).append(arrays)
 
     def calculateRootLogLikelihoods(self, bufs, cw, sf, cum):
         out = np.zeros(len(self.members))
         self._call("BatchCalculateRootLogLikelihoods", _ptr(_i32(bufs)), _ptr(_i32(cw)),
                    _ptr(_i32(sf)), _ptr(_i32(cum)), _ptr(out))
+        self._keep_result(out)
         return out
 
     def calculateEdgeDerivatives(self, post, pre, dmat, cw):
@@ -571,4 +598,5 @@ class Batch:
         st, k4 = self._ptrs(sums, np.float64)
         qq, k5 = self._ptrs(sq, np.float64)
         self._call("BatchCalculateEdgeDerivatives", pt, qt, dt, _ptr(_i32(cw)), _ptr(cnt), st, qq)
+        self._keep_result(k4, k5)
         return k4, k5

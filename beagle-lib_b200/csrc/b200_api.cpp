@@ -518,6 +518,19 @@ int beagleB200BatchCalculateEdgeDerivatives(int batch, const int* const* post,
     });
 }
 
+int beagleB200BatchBeginCapture(int batch) {
+    return call_batch(batch, [&](b200::Batch* b) { return b->beginCapture(); });
+}
+
+int beagleB200BatchEndCapture(int batch, int* graph) {
+    if (!graph) return BEAGLE_B200_ERROR_OUT_OF_RANGE;
+    return call_batch(batch, [&](b200::Batch* b) { return b->endCapture(graph); });
+}
+
+int beagleB200BatchLaunchGraph(int batch, int graph) {
+    return call_batch(batch, [&](b200::Batch* b) { return b->launchGraph(graph); });
+}
+
 int beagleB200BatchWait(int batch) {
     return call_batch(batch, [&](b200::Batch* b) { return b->wait(); });
 }

@@ -45,6 +45,7 @@ size_t append(std::vector<unsigned char>& table, const std::vector<T>& v) {
 
 Batch::~Batch() {
     release();
+    for (GraphRec& g : graphs_) free_graph(g);
     for (DevBuf* b : {&t_a_, &t_b_, &t_c_, &t_block_, &t_out_, &t_out2_}) b->release();
     for (auto& c : chunks_) cudaFreeHost(c.first);
     if (stream_) cudaStreamDestroy(stream_);
@@ -69,6 +70,11 @@ int Batch::create(const std::vector<Instance*>& members) {
 }
 
 void Batch::release() {
+    if (capturing_) {   // an unfinished capture is dropped
+        int g = -1;
+        (void)endCapture(&g);
+        if (g >= 0) free_graph(graphs_[g]);
+    }
     if (!m_.empty()) wait();
     for (Instance* in : m_) in->use_stream(nullptr);
     m_.clear();
@@ -81,6 +87,7 @@ bool Batch::deferred() const {
 }
 
 int Batch::sync() {
+    if (capturing_) return kErrGeneral;   // a wait would break the capture
     CK(cudaStreamSynchronize(stream_));
     for (const Pending& pd : pending_) {
         std::copy(pd.src, pd.src + pd.n, pd.dst);
@@ -100,8 +107,23 @@ int Batch::sync() {
 
 int Batch::wait() { return sync(); }
 
-// n doubles of pinned staging, valid until the next sync().
+void Batch::push_pending(const Pending& pd) {
+    if (capturing_) cap_.deliveries.push_back(pd);
+    else pending_.push_back(pd);
+}
+
+// n doubles of pinned staging, valid until the next sync(); while capturing,
+// a block the graph owns (its copy writes there at every launch).
 double* Batch::stage(size_t n) {
+    if (capturing_) {
+        double* p = nullptr;
+        if (cudaMallocHost(&p, sizeof(double) * n) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return nullptr;
+        }
+        cap_.pinned.push_back(p);
+        return p;
+    }
     while (chunk_i_ < chunks_.size() && chunk_off_ + n > chunks_[chunk_i_].second) {
         ++chunk_i_;
         chunk_off_ = 0;
@@ -118,6 +140,77 @@ double* Batch::stage(size_t n) {
     double* p = chunks_[chunk_i_].first + chunk_off_;
     chunk_off_ += n;
     return p;
+}
+
+// ------------------------------------------------------------ CUDA graphs
+// The batch's calls between beginCapture and endCapture become one CUDA graph
+// of the shared stream: the batched kernels, the members' own launches, every
+// table upload (through pinned blocks the graph owns) and every result copy.
+// Members are marked as capturing, so their own result copies and deliveries
+// are recorded too and no call may wait.  Results of a launch are delivered at
+// the next wait(), as the captured calls' would be.  The captured sequence
+// must have run once before (its tables and scratch are then sized).
+int Batch::beginCapture() {
+    if (capturing_ || !deferred()) return kErrGeneral;
+    for (Instance* in : m_)
+        if (in->capturing_) return kErrGeneral;
+    int rc = sync();
+    if (rc) return rc;
+    cap_ = GraphRec{};
+    CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed));
+    capturing_ = true;
+    capture_pinned() = &cap_.pinned;
+    for (Instance* in : m_) {
+        in->cap_ = Instance::GraphRec{};
+        in->capturing_ = true;
+    }
+    return kSuccess;
+}
+
+int Batch::endCapture(int* graph) {
+    if (!capturing_ || !graph) return kErrGeneral;
+    capturing_ = false;
+    capture_pinned() = nullptr;
+    for (size_t i = 0; i < m_.size(); ++i) {
+        Instance* in = m_[i];
+        in->capturing_ = false;
+        if (!in->cap_.deliveries.empty())
+            cap_.member_deliveries.emplace_back((int)i, std::move(in->cap_.deliveries));
+        cap_.pinned.insert(cap_.pinned.end(), in->cap_.pinned.begin(), in->cap_.pinned.end());
+        in->cap_ = Instance::GraphRec{};
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(stream_, &g);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&cap_.exec, g, 0ULL);
+    cap_.graph = g;
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        free_graph(cap_);
+        return kErrGeneral;
+    }
+    graphs_.push_back(std::move(cap_));
+    cap_ = GraphRec{};
+    *graph = (int)graphs_.size() - 1;
+    return kSuccess;
+}
+
+int Batch::launchGraph(int graph) {
+    if (capturing_ || graph < 0 || graph >= (int)graphs_.size() || !graphs_[graph].exec)
+        return kErrRange;
+    note_graph_launch();
+    CK(cudaGraphLaunch(graphs_[graph].exec, stream_));
+    const GraphRec& g = graphs_[graph];
+    for (const Pending& pd : g.deliveries) pending_.push_back(pd);
+    for (const auto& md : g.member_deliveries)
+        for (const Instance::Pending& pd : md.second) m_[md.first]->pending_.push_back(pd);
+    return kSuccess;
+}
+
+void Batch::free_graph(GraphRec& g) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+    for (void* p : g.pinned) cudaFreeHost(p);
+    g = GraphRec{};
 }
 
 // ------------------------------------------------------------ matrices
@@ -337,7 +430,7 @@ int Batch::rootLogLikelihoods(const int* bufs, const int* cw, const int* sf, con
     double* h = stage(n);
     if (!h) return kErrOOM;
     CK(cudaMemcpyAsync(h, t_out_.ptr, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_));
-    for (int i = 0; i < n; ++i) pending_.push_back(Pending{h + i, out + i, 1, i});
+    for (int i = 0; i < n; ++i) push_pending(Pending{h + i, out + i, 1, i});
     if (deferred()) return kSuccess;   // delivered by wait()
     int rc = sync();
     if (rc) return rc;
@@ -440,8 +533,8 @@ int Batch::edgeDerivatives(const int* const* post, const int* const* pre,
     CK(cudaMemcpyAsync(h, t_out2_.ptr, sizeof(double) * ooff, cudaMemcpyDeviceToHost, stream_));
     for (const auto& mo : out_of) {
         const int i = mo.first, nb = counts[i];
-        if (sums[i]) pending_.push_back(Pending{h + mo.second, sums[i], (size_t)nb, -1});
-        if (sumsq[i]) pending_.push_back(Pending{h + mo.second + nb, sumsq[i], (size_t)nb, -1});
+        if (sums[i]) push_pending(Pending{h + mo.second, sums[i], (size_t)nb, -1});
+        if (sumsq[i]) push_pending(Pending{h + mo.second + nb, sumsq[i], (size_t)nb, -1});
     }
     if (deferred()) return kSuccess;   // delivered by wait()
     return sync();

@@ -41,6 +41,11 @@ public:
                         double* const* sums, double* const* sumsq);
     // Wait for the batch's queued work and deliver deferred results.
     int wait();
+    // CUDA graph of the calls between beginCapture and endCapture (every
+    // member ASYNCH); launchGraph replays it, results at the next wait().
+    int beginCapture();
+    int endCapture(int* graph);
+    int launchGraph(int graph);
     // Members back on their own streams.
     void release();
 
@@ -58,6 +63,18 @@ private:
         int member;
     };
     std::vector<Pending> pending_;
+    void push_pending(const Pending& pd);   // or into the capture's deliveries
+    struct GraphRec {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        std::vector<Pending> deliveries;
+        std::vector<std::pair<int, std::vector<Instance::Pending>>> member_deliveries;
+        std::vector<void*> pinned;
+    };
+    std::vector<GraphRec> graphs_;
+    GraphRec cap_;
+    bool capturing_ = false;
+    void free_graph(GraphRec& g);
     std::vector<std::pair<double*, size_t>> chunks_;   // pinned staging, reused after wait()
     size_t chunk_i_ = 0, chunk_off_ = 0;
 

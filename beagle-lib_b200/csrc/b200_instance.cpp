@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstring>
 #include <algorithm>
+#include <atomic>
 #include <unordered_map>
 
 namespace b200 {
@@ -66,12 +67,20 @@ cudaError_t DevBuf::reserve(size_t n) {
 // its source at every launch.
 namespace {
 thread_local std::vector<void*>* t_capture_pinned = nullptr;
+std::atomic<unsigned> g_graph_epoch{0};
 }
+
+std::vector<void*>*& capture_pinned() { return t_capture_pinned; }
+void note_graph_launch() { ++g_graph_epoch; }
 
 cudaError_t DevBuf::upload(const void* src, size_t n, cudaStream_t s) {
     cudaError_t e = reserve(n);
     if (e != cudaSuccess) return e;
-    if (last.size() == n && n > 0 && std::memcmp(last.data(), src, n) == 0) return cudaSuccess;
+    const unsigned ep = g_graph_epoch.load();
+    if (!t_capture_pinned && epoch == ep && last.size() == n && n > 0 &&
+        std::memcmp(last.data(), src, n) == 0)
+        return cudaSuccess;
+    epoch = ep;
     if (t_capture_pinned) {
         void* h = nullptr;
         e = cudaMallocHost(&h, n);
@@ -277,6 +286,7 @@ int Instance::endCapture(int* graph) {
 int Instance::launchGraph(int graph) {
     if (capturing_ || graph < 0 || graph >= (int)graphs_.size() || !graphs_[graph].exec)
         return kErrRange;
+    note_graph_launch();
     CK(cudaGraphLaunch(graphs_[graph].exec, stream_));
     for (const Pending& pd : graphs_[graph].deliveries) pending_.push_back(pd);
     return kSuccess;

@@ -16,10 +16,20 @@ struct DevBuf {
     void* ptr = nullptr;
     size_t bytes = 0;
     std::vector<uint8_t> last;     // last uploaded contents (upload is skipped if equal)
+    unsigned epoch = 0;            // graph-launch epoch of `last`
     cudaError_t reserve(size_t n);
     cudaError_t upload(const void* src, size_t n, cudaStream_t s);
     void release();
 };
+
+// Every CUDA-graph launch (of an instance or a batch) starts a new upload
+// epoch: a graph's copy nodes rewrite tables behind DevBuf::last, so an
+// upload skips only when nothing was launched since its previous copy.  While
+// a thread captures, every upload copies (through graph-owned pinned memory).
+void note_graph_launch();
+// Graph-owned pinned blocks of the capture this thread is recording (null
+// when not capturing).
+std::vector<void*>*& capture_pinned();
 
 class Instance {
 public:

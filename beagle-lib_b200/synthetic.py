@@ -519,9 +519,14 @@ def batch_evaluate(batch, problems, lengths=None):
             pre_idx=[nr + p.pre(0) for nr, p in zip(nonroot, problems)],
             dmat=[np.full(p.B, p.B, dtype=np.int32) for p in problems], zeros=[0] * n,
             none=[OP_NONE] * n)
-    n = plan["n"]
     ts = [p.lengths if lengths is None else lengths[i] for i, p in enumerate(problems)]
     batch.updateTransitionMatrices(plan["zeros"], plan["idx"], ts)
+    lnl, sums = _batch_after_matrices(batch, plan)
+    batch.wait()
+    return lnl, sums
+
+
+def _batch_after_matrices(batch, plan):
     batch.updatePartials(plan["post"], plan["none"])
     if plan["rescale"]:
         batch.accumulateScaleFactors(plan["scales"], plan["cums"], reset=True)
@@ -531,5 +536,30 @@ def batch_evaluate(batch, problems, lengths=None):
     batch.updatePrePartials(plan["pre"])
     sums, _ = batch.calculateEdgeDerivatives(plan["idx"], plan["pre_idx"], plan["dmat"],
                                              plan["zeros"])
-    batch.wait()
     return lnl, sums
+
+
+def batch_capture(batch, problems):
+    """Record one batched evaluation after the transition matrices as a CUDA
+    graph of the batch (every member ASYNCH); returns (graph, lnL array,
+    gradient arrays) that each launch fills at the next wait.  Runs the
+    sequence once first, as the capture requires."""
+    batch_evaluate(batch, problems)
+    plan = batch._plan
+    batch.beginCapture()
+    try:
+        lnl, sums = _batch_after_matrices(batch, plan)
+    finally:
+        graph = batch.endCapture()
+    return graph, lnl, sums
+
+
+def batch_evaluate_graph(batch, problems, graph, lengths=None):
+    """One batched evaluation through a captured graph: new transition
+    matrices (outside the graph), the graph, then the wait that delivers lnL
+    and the gradients into the captured arrays."""
+    plan = batch._plan
+    ts = [p.lengths if lengths is None else lengths[i] for i, p in enumerate(problems)]
+    batch.updateTransitionMatrices(plan["zeros"], plan["idx"], ts)
+    batch.launchGraph(graph)
+    batch.wait()

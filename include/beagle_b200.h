@@ -449,6 +449,16 @@ int beagleB200BatchCalculateEdgeDerivatives(int batch, const int* const* postBuf
                                             const int* counts,
                                             double* const* outSumDerivatives,
                                             double* const* outSumSquaredDerivatives);
+/* Batch CUDA graphs (every member ASYNCH): the batch calls between
+ * BeginCapture and EndCapture are recorded once as one graph of the batch's
+ * stream (batched kernels, members' own launches, table uploads and result
+ * copies); LaunchGraph replays it, and the captured calls' results reach the
+ * caller's arrays at the next beagleB200BatchWait.  Run the sequence once
+ * before capturing it.  Calls that wait for results are refused while
+ * capturing. */
+int beagleB200BatchBeginCapture(int batch);
+int beagleB200BatchEndCapture(int batch, int* outGraph);
+int beagleB200BatchLaunchGraph(int batch, int graph);
 /* Wait for everything queued on the batch's stream and write the deferred
  * results of ASYNCH members. */
 int beagleB200BatchWait(int batch);

@@ -71,3 +71,31 @@ def test_batch_rejects_bad_members(b200, pkg, syn):
     batch.finalize()
     a.finalize()
     b.finalize()
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_batch_graph_replay(b200, pkg, syn, precision):
+    """One batched evaluation captured as a CUDA graph of the batch (batched
+    kernels, the 3-category and 20-state members' own launches, uploads and
+    result copies), replayed with new branch lengths against plain batched
+    evaluations of a second batch."""
+    probs = _problems(syn)
+    plain = pkg.binding.Batch(b200, [_create(b200, pr, precision, True) for pr in probs])
+    graphed = pkg.binding.Batch(b200, [_create(b200, pr, precision, True) for pr in probs])
+    graph, lnl_g, sums_g = syn.batch_capture(graphed, probs)
+    rng = np.random.default_rng(5)
+    tol = TOL[precision]
+    for step in range(3):
+        ts = [p.lengths * (1 + 0.05 * rng.standard_normal(p.B)) for p in probs]
+        lnl0, sums0 = syn.batch_evaluate(plain, probs, lengths=ts)
+        syn.batch_evaluate_graph(graphed, probs, graph, lengths=ts)
+        for i in range(len(probs)):
+            assert rel(lnl_g[i], lnl0[i]) <= tol["lnl"], (step, i)
+            assert grad_err(sums_g[i], sums0[i]) <= tol["grad"], (step, i)
+    # a result call that would wait is refused while capturing
+    graphed.beginCapture()
+    with pytest.raises(Exception):
+        graphed.wait()
+    graphed.endCapture()
+    plain.finalize()
+    graphed.finalize()
