@@ -253,6 +253,8 @@ int Batch::updatePartials(const int* const* ops, const int* counts, const int* c
         int nops;
     };
     std::map<int, std::vector<Member>> groups;   // C -> batched 4-state members
+    // (S, Sg, C) -> FP32 members of the batched tensor-core walk
+    std::map<std::tuple<int, int, int>, std::vector<Member>> tcgroups;
     std::vector<unsigned char> table;
     std::vector<int> fallback;
     for (int i = 0; i < n; ++i) {
@@ -260,6 +262,17 @@ int Batch::updatePartials(const int* const* ops, const int* counts, const int* c
         const int cum = cumulative ? cumulative[i] : -1;
         if (cum != -1 && (cum < 0 || cum >= in->nscale_)) return kErrRange;
         if (!batched4(in, in->S_, in->C_)) {
+            if (!dbl_ && tc_supported(in->dims())) {
+                std::vector<OpDesc> tab;
+                std::vector<uint8_t> dep;
+                bool idem = true, has_cum = false;
+                const int rc = in->build_walk(ops[i], counts[i], 7, pre, tab, dep, idem, has_cum);
+                if (rc) return rc;
+                if (tab.empty()) continue;
+                tcgroups[std::make_tuple(in->S_, in->Sg_, in->C_)].push_back(
+                    Member{i, append(table, tab), (int)tab.size()});
+                continue;
+            }
             fallback.push_back(i);
             continue;
         }
@@ -277,7 +290,7 @@ int Batch::updatePartials(const int* const* ops, const int* counts, const int* c
                                           pre);
         if (rc) return rc;
     }
-    if (groups.empty()) return kSuccess;
+    if (groups.empty() && tcgroups.empty()) return kSuccess;
     CK(t_a_.upload(table.data(), table.size(), stream_));
     // Segment tables (device pointers into t_a_), one per category count.
     std::vector<unsigned char> segtab;
@@ -288,6 +301,36 @@ int Batch::updatePartials(const int* const* ops, const int* counts, const int* c
         int ncta;
     };
     std::vector<G> gl;
+    struct TG {
+        Dims d;
+        size_t off;
+        int nseg;
+        int ntiles;
+        std::vector<int> members;
+    };
+    std::vector<TG> tgl;
+    for (auto& kv : tcgroups) {
+        std::vector<WalkSeg> segs;
+        TG tg{};
+        tg.d = Dims{std::get<0>(kv.first), std::get<1>(kv.first), 0, 0, std::get<2>(kv.first)};
+        for (const Member& mb : kv.second) {
+            Instance* in = m_[mb.i];
+            const int cum = cumulative ? cumulative[mb.i] : -1;
+            WalkSeg sg{};
+            sg.ops = (const OpDesc*)((unsigned char*)t_a_.ptr + mb.ops_off);
+            sg.cum = (!pre && cum >= 0) ? in->scale(cum) : nullptr;
+            sg.nops = mb.nops;
+            sg.Pp = in->Pp_;
+            sg.log_scalers = (int)in->log_scalers_;
+            sg.first_cta = tg.ntiles;                  // counted in 128-pattern tiles
+            tg.ntiles += in->Pp_ / tc_tile_patterns();
+            segs.push_back(sg);
+            tg.members.push_back(mb.i);
+        }
+        tg.off = append(segtab, segs);
+        tg.nseg = (int)segs.size();
+        tgl.push_back(tg);
+    }
     for (auto& kv : groups) {
         const int C = kv.first;
         std::vector<WalkSeg> segs;
@@ -311,6 +354,22 @@ int Batch::updatePartials(const int* const* ops, const int* counts, const int* c
     for (const G& g : gl)
         CK(LAUNCH(launch_walk4_batch, (const WalkSeg*)((unsigned char*)t_b_.ptr + g.off), g.nseg,
                   g.ncta, g.C, pre, stream_));
+    for (const TG& g : tgl) {
+        cudaError_t e = launch_walk_tc_batch((const WalkSeg*)((unsigned char*)t_b_.ptr + g.off),
+                                             g.nseg, g.ntiles, pre, g.d, stream_);
+        if (e == cudaErrorInvalidConfiguration) {
+            // the tensor-core shape cannot launch here: the members' own walks
+            (void)cudaGetLastError();
+            for (int i : g.members) {
+                const int rc = m_[i]->post_or_pre(ops[i], counts[i], 7,
+                                                  cumulative ? cumulative[i] : -1, pre);
+                if (rc) return rc;
+            }
+            continue;
+        }
+        CK(e);
+        for (int i : g.members) m_[i]->tc_used_ = true;
+    }
     return kSuccess;
 }
 
@@ -451,30 +510,41 @@ int Batch::edgeDerivatives(const int* const* post, const int* const* pre,
         int nblk;
     };
     std::map<int, std::vector<Member>> groups;
+    std::map<std::tuple<int, int, int>, std::vector<Member>> tcgroups;   // (S, Sg, C), FP32
     std::vector<unsigned char> table;
     std::vector<int> fallback;
     for (int i = 0; i < n; ++i) {
         Instance* in = m_[i];
         if (counts[i] <= 0) continue;
-        if (!batched4(in, in->S_, in->C_)) {
+        const bool tc = !batched4(in, in->S_, in->C_) && !dbl_ && deriv_tc_launchable(in->dims());
+        if (!batched4(in, in->S_, in->C_) && !tc) {
             fallback.push_back(i);
             continue;
         }
         std::vector<DerivDesc> tab;
         const int rc = in->build_deriv(post[i], pre[i], dmat[i], &cw[i], counts[i], tab);
         if (rc) return rc;
-        groups[in->C_].push_back(
-            Member{i, append(table, tab), counts[i], ceil_div(in->P_, deriv4_batch_tile(in->C_))});
+        if (tc)
+            tcgroups[std::make_tuple(in->S_, in->Sg_, in->C_)].push_back(
+                Member{i, append(table, tab), counts[i], in->Pp_ / tc_tile_patterns()});
+        else
+            groups[in->C_].push_back(Member{i, append(table, tab), counts[i],
+                                            ceil_div(in->P_, deriv4_batch_tile(in->C_))});
     }
     for (int i : fallback) {
         const int rc = m_[i]->calculateEdgeDerivatives(post[i], pre[i], dmat[i], &cw[i],
                                                        counts[i], nullptr, sums[i], sumsq[i]);
         if (rc) return rc;
     }
-    if (groups.empty()) return kSuccess;
+    if (groups.empty() && tcgroups.empty()) return kSuccess;
     CK(t_a_.upload(table.data(), table.size(), stream_));
     size_t blocks = 0, outs = 0;
     for (auto& kv : groups)
+        for (const Member& mb : kv.second) {
+            blocks += (size_t)2 * mb.nb * mb.nblk;
+            outs += (size_t)2 * mb.nb;
+        }
+    for (auto& kv : tcgroups)
         for (const Member& mb : kv.second) {
             blocks += (size_t)2 * mb.nb * mb.nblk;
             outs += (size_t)2 * mb.nb;
@@ -521,11 +591,58 @@ int Batch::edgeDerivatives(const int* const* post, const int* const* pre,
         }
         gl.push_back(G{kv.first, append(segtab, segs), (int)segs.size(), cta});
     }
+    // tensor-core groups: segment first_cta counts (branch, tile) clusters
+    struct TG {
+        Dims d;
+        size_t off;
+        int nseg;
+        int nclusters;
+        std::vector<int> members;
+    };
+    std::vector<TG> tgl;
+    for (auto& kv : tcgroups) {
+        std::vector<DerivSeg> segs;
+        TG tg{};
+        tg.d = Dims{std::get<0>(kv.first), std::get<1>(kv.first), 0, 0, std::get<2>(kv.first)};
+        for (const Member& mb : kv.second) {
+            Instance* in = m_[mb.i];
+            DerivSeg sg{};
+            sg.desc = (const DerivDesc*)((unsigned char*)t_a_.ptr + mb.desc_off);
+            sg.catw = in->d_catw_ + (size_t)cw[mb.i] * in->C_;
+            sg.patw = in->d_patw_;
+            sg.block = (double*)t_block_.ptr + boff;
+            sg.nb = mb.nb;
+            sg.P = in->P_;
+            sg.nblk = mb.nblk;
+            sg.first_cta = tg.nclusters;
+            tg.nclusters += mb.nb * mb.nblk;
+            segs.push_back(sg);
+            tg.members.push_back(mb.i);
+            FinalSeg f{};
+            f.block = sg.block;
+            f.out = (double*)t_out2_.ptr + ooff;
+            f.nblk = mb.nblk;
+            f.nout = 2 * mb.nb;
+            f.first_out = (int)ooff;
+            fin.push_back(f);
+            out_of.emplace_back(mb.i, ooff);
+            boff += (size_t)2 * mb.nb * mb.nblk;
+            ooff += (size_t)2 * mb.nb;
+        }
+        tg.off = append(segtab, segs);
+        tg.nseg = (int)segs.size();
+        tgl.push_back(tg);
+    }
     const size_t foff = append(segtab, fin);
     CK(t_b_.upload(segtab.data(), segtab.size(), stream_));
     for (const G& g : gl)
         CK(LAUNCH(launch_deriv4_batch, (const DerivSeg*)((unsigned char*)t_b_.ptr + g.off),
                   g.nseg, g.ncta, g.C, stream_));
+    for (const TG& g : tgl) {
+        CK(launch_deriv_tc_batch((const DerivSeg*)((unsigned char*)t_b_.ptr + g.off), g.nseg,
+                                 g.nclusters, g.d, stream_));
+        for (int i : g.members) m_[i]->tc_used_ = true;
+    }
     CK(launch_final_batch((const FinalSeg*)((unsigned char*)t_b_.ptr + foff), (int)fin.size(),
                           (int)ooff, stream_));
     double* h = stage(ooff);

@@ -69,6 +69,15 @@ cudaError_t launch_opwalk_tc(const OpDesc* d_ops, int nops, bool pre, const Dims
 cudaError_t launch_deriv_tc(const DerivDesc* d_desc, int nb, const double* catw,
                             const double* patw, const Dims& d, double* d_site, double* d_block,
                             cudaStream_t s);
+// Batched tensor-core walks and derivatives over instances with one (S, C),
+// FP32 (d gives S, Sg and C; its pattern counts are unused).  Walk segments
+// count pattern tiles of 128 in first_cta; derivative segments count
+// (branch, tile) clusters, nblk = the instance's tiles.
+cudaError_t launch_walk_tc_batch(const WalkSeg* d_segs, int nseg, int ntiles, bool pre,
+                                 const Dims& d, cudaStream_t s);
+cudaError_t launch_deriv_tc_batch(const DerivSeg* d_segs, int nseg, int nclusters, const Dims& d,
+                                  cudaStream_t s);
+bool deriv_tc_launchable(const Dims& d);
 // The flag a tensor-core kernel sets when a bounded wait on its tensor-core
 // work timed out: queue its copy into pinned host memory on `s` (read it after
 // the stream completes), and clear it (synchronises `s`).

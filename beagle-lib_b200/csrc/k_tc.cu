@@ -453,16 +453,41 @@ __device__ __forceinline__ void finish_row(TcSmem& sm, const OpDesc& op, float o
 
 // At least 3 resident CTAs per SM (<= 170 registers a thread): with 316-CTA
 // grids of 10k-pattern, 4-category data that keeps a launch in one wave.
+// Segment of a batched launch holding pattern tile q (segs sorted by first_cta,
+// which counts tiles for the tensor-core kernels).
+template <typename Seg>
+__device__ __forceinline__ int tc_find_seg(const Seg* segs, int nseg, int q) {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (segs[mid].first_cta <= q) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// segs != null: a batched launch over several instances with the same S and
+// C; tile q of the grid belongs to the segment whose tiles hold it, and that
+// segment's op list, cumulative buffer and scaler kind replace the arguments.
 template <int NP, int KC, bool PRE>
 __global__ void __launch_bounds__(kTT, 3)
 k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double* cum,
-          int log_scalers) {
+          int log_scalers, const WalkSeg* __restrict__ segs, int nseg) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     TcSmem& sm = *reinterpret_cast<TcSmem*>(smem_raw);
     using G = TcGeo<NP>;
     const int t = threadIdx.x;
     const int c = blockIdx.x % C;
-    const int p0 = (blockIdx.x / C) * kTM;
+    int q = blockIdx.x / C;
+    if (segs) {
+        const WalkSeg& sg = segs[tc_find_seg(segs, nseg, q)];
+        ops = sg.ops;
+        nops = sg.nops;
+        cum = PRE ? nullptr : sg.cum;
+        log_scalers = sg.log_scalers;
+        q -= sg.first_cta;
+    }
+    const int p0 = q * kTM;
     const int p = p0 + t;
     constexpr int NKC = chunks_of<NP>();
     const size_t xs = (size_t)C * Sg;            // partials row stride (elements)
@@ -575,18 +600,35 @@ k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double
 // Edge derivatives: cluster = (pattern tile, branch), CTA = category (the
 // decomposition of k_deriv_x in k_generic.cu).  Y = post . D^T on the tensor
 // cores; num / den per category in FP32, combined over categories in FP64.
+// segs != null: a batched launch (same S and C); cluster q belongs to the
+// segment whose (branch, tile) clusters hold it, and that segment's branches,
+// weights, pattern count and block partials replace the arguments.
 template <int NP, int KC>
 __global__ void __launch_bounds__(kTT, 3)
 k_deriv_tc(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
            const double* __restrict__ patw, int S, int Sg, int C, int P, int ntiles,
-           double* site, double* block) {
+           double* site, double* block, const DerivSeg* __restrict__ segs, int nseg) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     TcSmem& sm = *reinterpret_cast<TcSmem*>(smem_raw);
     using G = TcGeo<NP>;
     const int t = threadIdx.x;
     const int c = blockIdx.x % C;
-    const int tile = (blockIdx.x / C) % ntiles;
-    const int b = blockIdx.x / (C * ntiles);
+    int q = blockIdx.x / C;
+    int nb_all = gridDim.x / (C * ntiles);
+    if (segs) {
+        const DerivSeg& sg = segs[tc_find_seg(segs, nseg, q)];
+        desc = sg.desc;
+        catw = sg.catw;
+        patw = sg.patw;
+        P = sg.P;
+        ntiles = sg.nblk;
+        block = sg.block;
+        site = nullptr;
+        nb_all = sg.nb;
+        q -= sg.first_cta;
+    }
+    const int tile = q % ntiles;
+    const int b = q / ntiles;
     const int p0 = tile * kTM;
     const int p = p0 + t;
     constexpr int NKC = chunks_of<NP>();
@@ -679,9 +721,8 @@ k_deriv_tc(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
                 t1 += sm.red[k * 2 + 0];
                 t2 += sm.red[k * 2 + 1];
             }
-            const int nb = gridDim.x / (C * ntiles);
             block[(size_t)b * ntiles + tile] = t1;
-            block[(size_t)(nb + b) * ntiles + tile] = t2;
+            block[(size_t)(nb_all + b) * ntiles + tile] = t2;
         }
     }
     cluster.sync();   // remote reads done before any CTA of the cluster exits
@@ -730,10 +771,22 @@ cudaError_t run_walk_tc(const OpDesc* ops, int nops, bool pre, const Dims& d, do
                         int ls, cudaStream_t s) {
     const int cols = TcGeo<NP>::TCOLS;
     const int grid = (d.Pp / kTM) * d.C;
+    const WalkSeg* none = nullptr;
     return pre ? launch_tc(k_walk_tc<NP, KC, true>, grid, tc_smem(cols), d.C, cols, s, ops, nops,
-                           d.S, d.Sg, d.C, (double*)nullptr, ls)
+                           d.S, d.Sg, d.C, (double*)nullptr, ls, none, 0)
                : launch_tc(k_walk_tc<NP, KC, false>, grid, tc_smem(cols), d.C, cols, s, ops,
-                           nops, d.S, d.Sg, d.C, cum, ls);
+                           nops, d.S, d.Sg, d.C, cum, ls, none, 0);
+}
+
+template <int NP, int KC>
+cudaError_t run_walk_tc_batch(const WalkSeg* segs, int nseg, int ntiles, bool pre,
+                              const Dims& d, cudaStream_t s) {
+    const int cols = TcGeo<NP>::TCOLS;
+    const OpDesc* no_ops = nullptr;
+    return pre ? launch_tc(k_walk_tc<NP, KC, true>, ntiles * d.C, tc_smem(cols), d.C, cols, s,
+                           no_ops, 0, d.S, d.Sg, d.C, (double*)nullptr, 0, segs, nseg)
+               : launch_tc(k_walk_tc<NP, KC, false>, ntiles * d.C, tc_smem(cols), d.C, cols, s,
+                           no_ops, 0, d.S, d.Sg, d.C, (double*)nullptr, 0, segs, nseg);
 }
 
 template <int NP, int KC>
@@ -741,8 +794,20 @@ cudaError_t run_deriv_tc(const DerivDesc* desc, int nb, const double* catw, cons
                          const Dims& d, double* site, double* block, cudaStream_t s) {
     const int cols = TcGeo<NP>::DCOLS;
     const int ntiles = d.Pp / kTM;
+    const DerivSeg* none = nullptr;
     return launch_tc(k_deriv_tc<NP, KC>, ntiles * d.C * nb, tc_smem(cols), d.C, cols, s, desc,
-                     catw, patw, d.S, d.Sg, d.C, d.P, ntiles, site, block);
+                     catw, patw, d.S, d.Sg, d.C, d.P, ntiles, site, block, none, 0);
+}
+
+template <int NP, int KC>
+cudaError_t run_deriv_tc_batch(const DerivSeg* segs, int nseg, int nclusters, const Dims& d,
+                               cudaStream_t s) {
+    const int cols = TcGeo<NP>::DCOLS;
+    const DerivDesc* no_desc = nullptr;
+    const double* no_w = nullptr;
+    return launch_tc(k_deriv_tc<NP, KC>, nclusters * d.C, tc_smem(cols), d.C, cols, s, no_desc,
+                     no_w, no_w, d.S, d.Sg, d.C, 0, 1, (double*)nullptr, (double*)nullptr, segs,
+                     nseg);
 }
 
 // (N, KC) of a padded state count: N = Sg rounded up to 16, KC as above.
@@ -779,6 +844,51 @@ cudaError_t launch_deriv_tc(const DerivDesc* desc, int nb, const double* catw,
 #define DER_(NP, KC) run_deriv_tc<NP, KC>(desc, nb, catw, patw, d, site, block, s)
     return B200_TC_DISPATCH(d.Sg, DER_);
 #undef DER_
+}
+
+// Whether the tensor-core derivative kernel of this shape can launch without
+// oversubscribing TMEM (the check launch_tc makes before launching).
+template <int NP, int KC>
+bool deriv_tc_fits() {
+    const int cols = TcGeo<NP>::DCOLS;
+    const size_t smem = tc_smem(cols);
+    if (cudaFuncSetAttribute(k_deriv_tc<NP, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_deriv_tc<NP, KC>, kTT, smem) !=
+        cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return per_sm * cols <= 512;
+}
+
+bool deriv_tc_launchable(const Dims& d) {
+    if (!tc_supported(d)) return false;
+#define FIT_(NP, KC) deriv_tc_fits<NP, KC>()
+    return B200_TC_DISPATCH(d.Sg, FIT_);
+#undef FIT_
+}
+
+cudaError_t launch_walk_tc_batch(const WalkSeg* d_segs, int nseg, int ntiles, bool pre,
+                                const Dims& d, cudaStream_t s) {
+    if (nseg == 0 || ntiles == 0) return cudaSuccess;
+    if (!tc_supported(d)) return cudaErrorInvalidValue;
+#define WALKB_(NP, KC) run_walk_tc_batch<NP, KC>(d_segs, nseg, ntiles, pre, d, s)
+    return B200_TC_DISPATCH(d.Sg, WALKB_);
+#undef WALKB_
+}
+
+cudaError_t launch_deriv_tc_batch(const DerivSeg* d_segs, int nseg, int nclusters, const Dims& d,
+                                  cudaStream_t s) {
+    if (nseg == 0 || nclusters == 0) return cudaSuccess;
+    if (!tc_supported(d)) return cudaErrorInvalidValue;
+#define DERB_(NP, KC) run_deriv_tc_batch<NP, KC>(d_segs, nseg, nclusters, d, s)
+    return B200_TC_DISPATCH(d.Sg, DERB_);
+#undef DERB_
 }
 
 cudaError_t tc_status_async(int* pinned_dst, cudaStream_t s) {
