@@ -466,10 +466,10 @@ __device__ __forceinline__ int tc_find_seg(const Seg* segs, int nseg, int q) {
     return lo;
 }
 
-// segs != null: a batched launch over several instances with the same S and
-// C; tile q of the grid belongs to the segment whose tiles hold it, and that
+// BATCH: a launch over several instances with the same S and C (segs); tile
+// q of the grid belongs to the segment whose tiles hold it, and that
 // segment's op list, cumulative buffer and scaler kind replace the arguments.
-template <int NP, int KC, bool PRE>
+template <int NP, int KC, bool PRE, bool BATCH>
 __global__ void __launch_bounds__(kTT, 3)
 k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double* cum,
           int log_scalers, const WalkSeg* __restrict__ segs, int nseg) {
@@ -479,7 +479,7 @@ k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double
     const int t = threadIdx.x;
     const int c = blockIdx.x % C;
     int q = blockIdx.x / C;
-    if (segs) {
+    if constexpr (BATCH) {
         const WalkSeg& sg = segs[tc_find_seg(segs, nseg, q)];
         ops = sg.ops;
         nops = sg.nops;
@@ -600,10 +600,10 @@ k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double
 // Edge derivatives: cluster = (pattern tile, branch), CTA = category (the
 // decomposition of k_deriv_x in k_generic.cu).  Y = post . D^T on the tensor
 // cores; num / den per category in FP32, combined over categories in FP64.
-// segs != null: a batched launch (same S and C); cluster q belongs to the
+// BATCH: a launch over several instances (same S and C); cluster q belongs to the
 // segment whose (branch, tile) clusters hold it, and that segment's branches,
 // weights, pattern count and block partials replace the arguments.
-template <int NP, int KC>
+template <int NP, int KC, bool BATCH>
 __global__ void __launch_bounds__(kTT, 3)
 k_deriv_tc(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
            const double* __restrict__ patw, int S, int Sg, int C, int P, int ntiles,
@@ -615,7 +615,7 @@ k_deriv_tc(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
     const int c = blockIdx.x % C;
     int q = blockIdx.x / C;
     int nb_all = gridDim.x / (C * ntiles);
-    if (segs) {
+    if constexpr (BATCH) {
         const DerivSeg& sg = segs[tc_find_seg(segs, nseg, q)];
         desc = sg.desc;
         catw = sg.catw;
@@ -772,9 +772,9 @@ cudaError_t run_walk_tc(const OpDesc* ops, int nops, bool pre, const Dims& d, do
     const int cols = TcGeo<NP>::TCOLS;
     const int grid = (d.Pp / kTM) * d.C;
     const WalkSeg* none = nullptr;
-    return pre ? launch_tc(k_walk_tc<NP, KC, true>, grid, tc_smem(cols), d.C, cols, s, ops, nops,
+    return pre ? launch_tc(k_walk_tc<NP, KC, true, false>, grid, tc_smem(cols), d.C, cols, s, ops, nops,
                            d.S, d.Sg, d.C, (double*)nullptr, ls, none, 0)
-               : launch_tc(k_walk_tc<NP, KC, false>, grid, tc_smem(cols), d.C, cols, s, ops,
+               : launch_tc(k_walk_tc<NP, KC, false, false>, grid, tc_smem(cols), d.C, cols, s, ops,
                            nops, d.S, d.Sg, d.C, cum, ls, none, 0);
 }
 
@@ -783,9 +783,9 @@ cudaError_t run_walk_tc_batch(const WalkSeg* segs, int nseg, int ntiles, bool pr
                               const Dims& d, cudaStream_t s) {
     const int cols = TcGeo<NP>::TCOLS;
     const OpDesc* no_ops = nullptr;
-    return pre ? launch_tc(k_walk_tc<NP, KC, true>, ntiles * d.C, tc_smem(cols), d.C, cols, s,
+    return pre ? launch_tc(k_walk_tc<NP, KC, true, true>, ntiles * d.C, tc_smem(cols), d.C, cols, s,
                            no_ops, 0, d.S, d.Sg, d.C, (double*)nullptr, 0, segs, nseg)
-               : launch_tc(k_walk_tc<NP, KC, false>, ntiles * d.C, tc_smem(cols), d.C, cols, s,
+               : launch_tc(k_walk_tc<NP, KC, false, true>, ntiles * d.C, tc_smem(cols), d.C, cols, s,
                            no_ops, 0, d.S, d.Sg, d.C, (double*)nullptr, 0, segs, nseg);
 }
 
@@ -795,7 +795,7 @@ cudaError_t run_deriv_tc(const DerivDesc* desc, int nb, const double* catw, cons
     const int cols = TcGeo<NP>::DCOLS;
     const int ntiles = d.Pp / kTM;
     const DerivSeg* none = nullptr;
-    return launch_tc(k_deriv_tc<NP, KC>, ntiles * d.C * nb, tc_smem(cols), d.C, cols, s, desc,
+    return launch_tc(k_deriv_tc<NP, KC, false>, ntiles * d.C * nb, tc_smem(cols), d.C, cols, s, desc,
                      catw, patw, d.S, d.Sg, d.C, d.P, ntiles, site, block, none, 0);
 }
 
@@ -805,7 +805,7 @@ cudaError_t run_deriv_tc_batch(const DerivSeg* segs, int nseg, int nclusters, co
     const int cols = TcGeo<NP>::DCOLS;
     const DerivDesc* no_desc = nullptr;
     const double* no_w = nullptr;
-    return launch_tc(k_deriv_tc<NP, KC>, nclusters * d.C, tc_smem(cols), d.C, cols, s, no_desc,
+    return launch_tc(k_deriv_tc<NP, KC, true>, nclusters * d.C, tc_smem(cols), d.C, cols, s, no_desc,
                      no_w, no_w, d.S, d.Sg, d.C, 0, 1, (double*)nullptr, (double*)nullptr, segs,
                      nseg);
 }
@@ -852,13 +852,13 @@ template <int NP, int KC>
 bool deriv_tc_fits() {
     const int cols = TcGeo<NP>::DCOLS;
     const size_t smem = tc_smem(cols);
-    if (cudaFuncSetAttribute(k_deriv_tc<NP, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(k_deriv_tc<NP, KC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem) != cudaSuccess) {
         (void)cudaGetLastError();
         return false;
     }
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_deriv_tc<NP, KC>, kTT, smem) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_deriv_tc<NP, KC, true>, kTT, smem) !=
         cudaSuccess) {
         (void)cudaGetLastError();
         return false;
