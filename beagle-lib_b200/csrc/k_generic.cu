@@ -43,7 +43,7 @@ struct GCfg {
     static constexpr int TILE = TP * XS;
     static constexpr int STAGE = 2 * MAT + 2 * TILE;
     static constexpr int CH = 16 / sizeof(Real);   // elements per 16-byte chunk
-    static size_t smem() { return sizeof(Real) * (2 * STAGE + TP * SG + TP); }
+    static size_t smem() { return sizeof(Real) * (2 * STAGE + TP * SG + 2 * TP); }
 };
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pred) {
@@ -139,6 +139,11 @@ __device__ __forceinline__ void tip4x4(const Real* A, const int s[4], int S, Rea
 
 // Per-pattern maximum over the cluster's categories of out[q][r] (states < S).
 // Threads of one pattern group reduce through `red`, CTAs through DSMEM.
+// `smax` alternates between two buffers (the caller passes rescaling k's
+// buffer k & 1), so one cluster barrier per rescaling suffices: a CTA writes
+// a buffer again only after the next rescaling's barrier, which every CTA of
+// the cluster reaches after its reads of that buffer.  The walk ends with a
+// cluster barrier, so no CTA exits while another reads its buffer.
 template <typename Real, int SPAD>
 __device__ __forceinline__ void cluster_max(const Real out[4][4], int S, int i0, int pg, int sg,
                                             Real* red, Real* smax, int C, Real m[4]) {
@@ -175,7 +180,6 @@ __device__ __forceinline__ void cluster_max(const Real out[4][4], int S, int i0,
         }
         m[q] = v;
     }
-    cluster.sync();
 }
 
 // Shared epilogue of post- and pre-order ops: optional rescale (cluster-wide
@@ -256,7 +260,7 @@ k_opwalk_x(const OpDesc* __restrict__ ops, const uint8_t* __restrict__ dep_prev,
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Real* stages = reinterpret_cast<Real*>(smem_raw);
     Real* s_red = stages + 2 * G::STAGE;     // [TP][SG]
-    Real* s_max = s_red + G::TP * G::SG;     // [TP]
+    Real* s_max = s_red + G::TP * G::SG;     // [2][TP], alternating per rescaling
     const int tid = threadIdx.x;
     const int sg = tid % G::SG, pg = tid / G::SG;
     const int i0 = sg * 4, pl = pg * 4;
@@ -265,6 +269,7 @@ k_opwalk_x(const OpDesc* __restrict__ ops, const uint8_t* __restrict__ dep_prev,
     if (nops == 0) return;
     issue_op<Real, SPAD, PRE>(ops[0], stages, p0, c, C, Sg, tid, G::NT);
     int cur = 0;
+    int nresc = 0;   // rescalings so far: rescaling k uses s_max buffer k & 1
     for (int o = 0; o < nops; ++o) {
         const OpDesc op = ops[o];
         const bool next = o + 1 < nops;
@@ -326,14 +331,17 @@ k_opwalk_x(const OpDesc* __restrict__ ops, const uint8_t* __restrict__ dep_prev,
             // dest[p][j] = sum_i z[p][i] P[i][j]
             mm4x4<Real, SPAD>(X2, A1, Sg, pl, i0, out);
         }
-        finish_tile<Real, SPAD>(op, out, p0, pl, i0, pg, sg, c, S, Sg, C, s_red, s_max,
-                                PRE ? nullptr : cum, log_scalers);
+        finish_tile<Real, SPAD>(op, out, p0, pl, i0, pg, sg, c, S, Sg, C, s_red,
+                                s_max + (nresc & 1) * G::TP, PRE ? nullptr : cum, log_scalers);
+        if (op.scale_write) ++nresc;
         __syncthreads();   // stage `cur` free, stores of this op visible to the CTA
         if (next && !early)
             issue_op<Real, SPAD, PRE>(ops[o + 1], stages + (cur ^ 1) * G::STAGE, p0, c, C, Sg, tid,
                                       G::NT);
         cur ^= 1;
     }
+    // no CTA leaves while another reads its s_max through DSMEM
+    cg::this_cluster().sync();
 }
 
 // Edge derivatives: cluster = (pattern tile, branch), CTA = category.

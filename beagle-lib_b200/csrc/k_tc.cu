@@ -195,14 +195,14 @@ template <int NP>
 __host__ __device__ constexpr int chunks_of() { return NP >= 48 ? 2 : 1; }
 
 // Shared memory of one CTA (floats unless noted):
-//   A_hi, A_lo [kTM * 32]   B_hi, B_lo [64 * 32]   smax [kTM]
+//   A_hi, A_lo [kTM * 32]   B_hi, B_lo [64 * 32]   smax [2][kTM]
 //   nd [kTM * 2] doubles, red [kTT * 2] doubles, mbarrier, TMEM address.
 struct TcSmem {
     float a_hi[kTM * 32];
     float a_lo[kTM * 32];
     float b_hi[64 * 32];
     float b_lo[64 * 32];
-    float smax[kTM];
+    float smax[2 * kTM];     // alternating per rescaling (see finish_row)
     double nd[kTM * 2];
     double red[kTT * 2];
     uint64_t bar;
@@ -410,10 +410,16 @@ __device__ __forceinline__ void mul_operand(float out[NP], bool states, uint32_t
 // Rescale (cluster-wide maximum over categories and states < S) or fixed
 // scaling, then store row t of the tile.  Same arithmetic as finish_tile in
 // k_generic.cu.
+//
+// The maximum is exchanged through sm.smax, whose two halves alternate per
+// rescaling (`nresc` counts them): a CTA writes a half again only after the
+// next rescaling's cluster barrier, which every CTA of the cluster reaches
+// after reading that half, so one barrier per rescaling suffices.  The walk
+// ends with a cluster barrier, so no CTA exits while another reads its smax.
 template <int NP>
 __device__ __forceinline__ void finish_row(TcSmem& sm, const OpDesc& op, float out[NP], int p,
                                            int c, int C, int S, int Sg, double* cum,
-                                           int log_scalers) {
+                                           int log_scalers, int& nresc) {
     const bool mine = p >= op.p_begin && p < op.p_end;   // the op's pattern range
     if (op.cum) cum = op.cum;
     if (op.scale_write) {
@@ -421,15 +427,16 @@ __device__ __forceinline__ void finish_row(TcSmem& sm, const OpDesc& op, float o
 #pragma unroll
         for (int i = 0; i < NP; ++i)
             if (i < S) m = out[i] > m ? out[i] : m;
-        sm.smax[threadIdx.x] = m;
+        float* sx = sm.smax + (nresc & 1) * kTM;
+        ++nresc;
+        sx[threadIdx.x] = m;
         cg::cluster_group cluster = cg::this_cluster();
         cluster.sync();
         m = 0.f;
         for (int r = 0; r < C; ++r) {
-            const float u = cluster.map_shared_rank(sm.smax, r)[threadIdx.x];
+            const float u = cluster.map_shared_rank(sx, r)[threadIdx.x];
             m = u > m ? u : m;
         }
-        cluster.sync();
         if (m == 0.f) m = 1.f;
         const float inv = 1.f / m;
 #pragma unroll
@@ -508,6 +515,7 @@ k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double
     Pipe pp;
 
     ChunkRegs cr;
+    int nresc = 0;
     for (int o = 0; o < nops; ++o) {
         const OpDesc& op = ops[o];
         const bool st1 = !PRE && (op.kind & kX1States), st2 = op.kind & kX2States;
@@ -585,7 +593,7 @@ k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double
 #pragma unroll
             for (int j = 0; j < NP / 16; ++j) tmem_chunk(tmem, NP, j, out + 16 * j);
         }
-        finish_row<NP>(sm, op, out, p, c, C, S, Sg, PRE ? nullptr : cum, log_scalers);
+        finish_row<NP>(sm, op, out, p, c, C, S, Sg, PRE ? nullptr : cum, log_scalers, nresc);
         // TMEM reads of this op done before the next op's MMAs overwrite them;
         // this op's stores visible to the CTA before the next op's loads.
         tc_fence_before();
@@ -593,7 +601,7 @@ k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double
     }
     pipe_drain(sm, pp);
     tc_fence_after();
-    __syncthreads();
+    cg::this_cluster().sync();   // every remote read of this CTA's smax is done
     if (t < 32) tmem_dealloc(tmem, G::TCOLS);
 }
 
