@@ -397,6 +397,18 @@ class Instance:
         (self._graph_keep if self._capturing else self._keep).append((o2, o3))
         return (None if o1 is None else o1.reshape(n, self.patternCount)), o2, o3
 
+    def calculateCrossProductDerivative(self, post, pre, crates, cw, lengths, out, check=True):
+        """beagleCalculateCrossProductDerivative: adds, over the listed
+        branches, the S x S cross-product sums into `out` (float64, S * S,
+        row-major; the caller clears it) and returns it."""
+        a, b = _i32(post), _i32(pre)
+        r, w = _i32(crates), _i32(cw)
+        t = _f64(lengths)
+        assert out.dtype == np.float64 and out.flags.c_contiguous
+        self._call("CalculateCrossProductDerivative", _ptr(a), _ptr(b), _ptr(r), _ptr(w), _ptr(t),
+                   len(a), _ptr(out), None, check=check)
+        return out
+
     def supports(self, name):
         """Whether the library exports <prefix><name>."""
         return name in self.blib.fn

@@ -368,9 +368,13 @@ int beagleB200GetTunedVariants(int h, int* out) {
         return BEAGLE_B200_SUCCESS;
     });
 }
-int beagleB200CalculateCrossProductDerivative(int h, const int*, const int*, const int*,
-                                              const int*, const double*, int, double*, double*) {
-    return call(h, [](b200::Instance*) { return BEAGLE_B200_ERROR_NO_IMPLEMENTATION; });
+int beagleB200CalculateCrossProductDerivative(int h, const int* post, const int* pre,
+                                              const int* rates, const int* w, const double* t,
+                                              int n, double* sum, double* sumsq) {
+    (void)sumsq;   // not written, as in the reference CPU implementation
+    return call(h, [&](b200::Instance* in) {
+        return in->calculateCrossProducts(post, pre, rates, w, t, n, sum);
+    });
 }
 int beagleB200CalculateEdgeLogLikelihoods(int h, const int* pa, const int* ch, const int* pm,
                                           const int* d1, const int* d2, const int* w,

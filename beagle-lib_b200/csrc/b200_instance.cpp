@@ -122,7 +122,7 @@ Instance::~Instance() {
     for (void* p : bufs)
         if (p) cudaFree(p);
     for (DevBuf* b : {&t_ops_post_, &t_ops_pre_, &t_jobs_, &t_deriv_, &t_idx_, &t_ptr_,
-                      &scratch_, &out_, &site_d_, &t_dep_post_, &t_dep_pre_})
+                      &scratch_, &out_, &site_d_, &t_dep_post_, &t_dep_pre_, &t_cross_})
         b->release();
     if (h_out_) cudaFreeHost(h_out_);
     if (h_tc_status_) cudaFreeHost(h_tc_status_);
@@ -1261,6 +1261,52 @@ int Instance::updatePrePartialsWithDerivatives(const int* ops, int count, const 
     picked_[kTuneFused] = v;
     CK(e);
     return deliver_sums(count, nullptr, outSum, outSumSq);
+}
+
+// beagleCalculateCrossProductDerivative (CPU/BeagleCPUImpl.hpp:1865-1937):
+// the S x S sums over the listed branches are added into the caller's array
+// (the reference adds, it does not clear); sums of squares are not written,
+// as in the reference.  Synchronous.
+int Instance::calculateCrossProducts(const int* post, const int* pre, const int* rates_idx,
+                                     const int* cw, const double* lengths, int count,
+                                     double* outSum) {
+    if (count < 0 || (count > 0 && (!post || !pre || !rates_idx || !cw || !lengths)))
+        return kErrRange;
+    if (count == 0) return kSuccess;
+    if (!outSum) return kErrRange;
+    if (S_ > 64) return kErrNoImpl;
+    const int ri = rates_idx[0], w = cw[0];
+    if (ri < 0 || ri >= neig_ || !rates_set_[ri] || w < 0 || w >= neig_ || !catw_set_[w])
+        return kErrRange;
+    std::vector<DerivDesc> tab(count);
+    std::vector<double> fac((size_t)count * C_);
+    for (int k = 0; k < count; ++k) {
+        if (!has_data(post[k]) || !buf_ok(pre[k]) || !partials_[pre[k]]) return kErrRange;
+        DerivDesc& d = tab[k];
+        d = DerivDesc{};
+        d.post = states_[post[k]] ? (const void*)states_[post[k]] : partials_[post[k]];
+        d.post_is_states = states_[post[k]] ? 1 : 0;
+        d.pre = partials_[pre[k]];
+        for (int c = 0; c < C_; ++c)
+            fac[(size_t)k * C_ + c] =
+                h_catw_[(size_t)w * C_ + c] * h_rates_[(size_t)ri * C_ + c] * lengths[k];
+    }
+    const Dims dm = dims();
+    const int ntiles = (P_ + cross_tile_patterns(dm, dbl_) - 1) / cross_tile_patterns(dm, dbl_);
+    const int SS = S_ * S_;
+    CK(t_deriv_.upload(tab.data(), sizeof(DerivDesc) * count, stream_));
+    CK(t_cross_.upload(fac.data(), sizeof(double) * fac.size(), stream_));
+    CK(scratch_.reserve(sizeof(double) * (size_t)SS * ntiles));
+    CK(out_.reserve(sizeof(double) * SS));
+    CK(LAUNCH(launch_cross_products, (const DerivDesc*)t_deriv_.ptr, count,
+              d_catw_ + (size_t)w * C_, (const double*)t_cross_.ptr, d_patw_, dm,
+              (double*)scratch_.ptr, (double*)out_.ptr, stream_));
+    std::vector<double> h(SS);
+    CK(cudaMemcpyAsync(h.data(), out_.ptr, sizeof(double) * SS, cudaMemcpyDeviceToHost, stream_));
+    const int rc = sync();
+    if (rc) return rc;
+    for (int q = 0; q < SS; ++q) outSum[q] += h[q];
+    return kSuccess;
 }
 
 int Instance::calculateEdgeLogLikelihoods(const int* parents, const int* children,

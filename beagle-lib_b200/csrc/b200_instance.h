@@ -100,6 +100,9 @@ public:
     // pre-order walk, 3 edge derivatives, 4 fused pre-order + derivatives;
     // -1 = default shape, -2 = not run yet).
     int picked(int kind) const { return kind >= 1 && kind <= 4 ? picked_[kind] : -2; }
+    int calculateCrossProducts(const int* post, const int* pre, const int* rates_idx,
+                               const int* cw, const double* lengths, int count,
+                               double* outSum);
     // updatePrePartials + calculateEdgeDerivatives (sums only) in one walk.
     int updatePrePartialsWithDerivatives(const int* ops, int count, const int* post,
                                          const int* dmat, const int* cw, double* outSum,
@@ -181,6 +184,7 @@ private:
     std::vector<int> partition_start_;     // pattern partitions (empty = one partition)
 
     DevBuf t_ops_post_, t_ops_pre_, t_jobs_, t_deriv_, t_idx_, t_ptr_, scratch_, out_, site_d_;
+    DevBuf t_cross_;                       // cross-product factors w_c r_c t_b
     DevBuf t_dep_post_, t_dep_pre_;        // per op: reads the previous op's output
     double* h_out_ = nullptr;              // pinned result staging (SYNCH calls)
     size_t h_out_n_ = 0;

@@ -142,6 +142,16 @@ cudaError_t launch_deriv_final(const double* d_block, int nblk, int nb, double* 
 // Fused pre-order partials + edge derivatives (k_fused.cu): S = 4, C in
 // {1, 2, 4, 8}, at most 256 ops.  d_block needs 2 * nops * fused_blocks(d)
 // doubles; d_sums receives the nops sums, then the nops sums of squares.
+// Cross-product derivative sums (k_reduce.cu), S <= 64: d_out receives the
+// S * S sums over the nb branches (desc: post, pre, post_is_states used; fac
+// [nb][C] = w_c r_c t_b); d_block needs S * S * ceil(P / cross_tile_patterns)
+// doubles.
+int cross_tile_patterns(const Dims& d, bool dbl);
+template <typename Real>
+cudaError_t launch_cross_products(const DerivDesc* d_desc, int nb, const double* catw,
+                                  const double* fac, const double* patw, const Dims& d,
+                                  double* d_block, double* d_out, cudaStream_t s);
+
 bool fused_supported(const Dims& d, int nops);
 int fused_blocks(const Dims& d);
 // variant 1: the walk of k_fused.cu; 2: pairs-only FP32 lists, 2 patterns a

@@ -830,6 +830,122 @@ cudaError_t launch_deriv_final(const double* d_block, int nblk, int nb, double* 
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------- cross products
+// beagleCalculateCrossProductDerivative (CPU/BeagleCPUImpl.hpp:1865-1937,
+// :2122-2237): for every listed branch b and pattern p,
+//   den = sum_c w_c sum_k pre[c,p,k] post[c,p,k]
+//   out[k][j] += W_p / den * sum_c fac[b][c] pre[c,p,k] post[c,p,j],
+// fac[b][c] = w_c r_c t_b, a tip's post row one-hot (all ones when missing).
+// CTA = a tile of TP patterns, looping over the branches: the tile's rows are
+// staged in shared memory, the pre rows scaled by W_p / den * fac, and each
+// thread keeps up to 16 of the S x S sums (S <= 64) in FP64, adding the
+// tile's TP * C terms in the partials' precision.  block[q][tile] holds the
+// tile sums; k_final_sum adds the tiles in a fixed order.
+constexpr int kCrossThreads = 256;
+
+template <typename Real>
+__global__ void __launch_bounds__(kCrossThreads)
+k_cross_products(const DerivDesc* __restrict__ desc, int nb, const double* __restrict__ catw,
+                 const double* __restrict__ fac, const double* __restrict__ patw, int S, int Sg,
+                 int C, int P, int TP, double* block) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* coef = reinterpret_cast<double*>(smem_raw);            // [TP]
+    Real* a = reinterpret_cast<Real*>(coef + TP);                  // [TP * C][Sg]
+    Real* x = a + (size_t)TP * C * Sg;                             // [TP * C][Sg]
+    const int tid = threadIdx.x;
+    const int tile = blockIdx.x, ntiles = gridDim.x;
+    const int p0 = tile * TP;
+    const int row = C * Sg, n = TP * row, SS = S * S;
+    double acc[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) acc[r] = 0.0;
+    for (int b = 0; b < nb; ++b) {
+        const DerivDesc d = desc[b];
+        __syncthreads();   // the previous branch's reads of a, x, coef are done
+        const Real* pre = static_cast<const Real*>(d.pre) + (size_t)p0 * row;
+        for (int e = tid; e < n; e += kCrossThreads) {
+            const int p = p0 + e / row;
+            const int i = e % Sg;
+            Real pv = 0, xv = 0;
+            if (p < P) {
+                pv = pre[e];
+                if (d.post_is_states) {
+                    const int st = static_cast<const int*>(d.post)[p];
+                    xv = (i < S && (st >= S || st == i)) ? Real(1) : Real(0);
+                } else {
+                    xv = static_cast<const Real*>(d.post)[(size_t)p0 * row + e];
+                }
+            }
+            a[e] = pv;
+            x[e] = xv;
+        }
+        __syncthreads();
+        for (int pl = tid; pl < TP; pl += kCrossThreads) {
+            const int p = p0 + pl;
+            double den = 0;
+            for (int c = 0; c < C; ++c) {
+                double dc = 0;
+                for (int k = 0; k < S; ++k)
+                    dc += (double)a[(pl * C + c) * Sg + k] * (double)x[(pl * C + c) * Sg + k];
+                den += catw[c] * dc;
+            }
+            coef[pl] = p < P ? patw[p] / den : 0.0;
+        }
+        __syncthreads();
+        for (int e = tid; e < n; e += kCrossThreads) {
+            const int pl = e / row, c = (e / Sg) % C;
+            a[e] = (Real)((double)a[e] * coef[pl] * fac[(size_t)b * C + c]);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+            const int q = tid + kCrossThreads * r;
+            if (q < SS) {
+                const int k = q / S, j = q - (q / S) * S;
+                Real sum = 0;
+                for (int pc = 0; pc < TP * C; ++pc) sum += a[pc * Sg + k] * x[pc * Sg + j];
+                acc[r] += (double)sum;
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+        const int q = tid + kCrossThreads * r;
+        if (q < SS) block[(size_t)q * ntiles + tile] = acc[r];
+    }
+}
+
+// Patterns per tile and tiles of a cross-product launch.
+int cross_tile_patterns(const Dims& d, bool dbl) {
+    const int elems = dbl ? 2048 : 4096;
+    int tp = elems / (d.C * d.Sg);
+    tp = tp < 1 ? 1 : tp > 128 ? 128 : tp;
+    return tp;
+}
+
+template <typename Real>
+cudaError_t launch_cross_products(const DerivDesc* d_desc, int nb, const double* catw,
+                                  const double* fac, const double* patw, const Dims& d,
+                                  double* d_block, double* d_out, cudaStream_t s) {
+    if (nb == 0) return cudaSuccess;
+    if (d.S > 64) return cudaErrorInvalidValue;
+    const int tp = cross_tile_patterns(d, sizeof(Real) == 8);
+    const int ntiles = (d.P + tp - 1) / tp;
+    const size_t smem = sizeof(double) * tp + 2 * sizeof(Real) * (size_t)tp * d.C * d.Sg;
+    k_cross_products<Real><<<ntiles, kCrossThreads, smem, s>>>(d_desc, nb, catw, fac, patw, d.S,
+                                                               d.Sg, d.C, d.P, tp, d_block);
+    const int SS = d.S * d.S;
+    k_final_sum<<<SS, kRB, 0, s>>>(d_block, ntiles, SS, d_out);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_cross_products<float>(const DerivDesc*, int, const double*,
+                                                  const double*, const double*, const Dims&,
+                                                  double*, double*, cudaStream_t);
+template cudaError_t launch_cross_products<double>(const DerivDesc*, int, const double*,
+                                                   const double*, const double*, const Dims&,
+                                                   double*, double*, cudaStream_t);
+
 // Per-block partial sums an edge-derivative launch needs (per branch, twice),
 // for the variant with the most blocks.
 int deriv_blocks(const Dims& d) {

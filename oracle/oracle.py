@@ -395,6 +395,40 @@ class OracleInstance:
         sumsq = (per_site * per_site) @ self.patw
         return per_site, sums, sumsq
 
+    def calculateCrossProductDerivative(self, post, pre, crates, cw, lengths, out):
+        """CPU/BeagleCPUImpl.hpp:1865-1937 (calcCrossProducts), :2122-2237
+        (calcCrossProductsStates / calcCrossProductsPartials); the 4-state
+        forms (CPU/BeagleCPU4StateImpl.hpp:1088-1251) compute the same sums.
+
+        For every listed branch b and pattern p, with w = category weights
+        [cw[0]], r = category rates [crates[0]] and t = lengths[b]:
+          den = sum_c w_c sum_k pre[c,p,k] post[c,p,k]
+          out[k][j] += W_p / den * sum_c w_c r_c t pre[c,p,k] post[c,p,j]
+        A compact (tip-state) post buffer is its one-hot row, all ones for the
+        missing state.  `out` (S x S, row-major, the caller's array) is added
+        to, not cleared, as in the reference; sums of squares are not
+        computed there either."""
+        w = self.catw[cw[0]]
+        r = self.rates[crates[0]]
+        S = self.S
+        acc = np.zeros((S, S))
+        for b in range(len(post)):
+            prb = self.partials[pre[b]]                         # [C][P][S]
+            if self.states[post[b]] is not None:
+                st = self.states[post[b]]
+                x = np.zeros_like(prb)
+                ok = st < S
+                x[:, np.where(ok)[0], st[ok]] = 1.0
+                x[:, ~ok, :] = 1.0
+            else:
+                x = self.partials[post[b]]
+            den = np.einsum('c,cpk,cpk->p', w, prb, x)
+            coef = self.patw / den
+            acc += np.einsum('c,p,cpk,cpj->kj', w * r * lengths[b], coef, prb, x)
+        out = np.asarray(out)
+        out += acc.reshape(out.shape)
+        return out
+
     def calculateEdgeLogLikelihoods(self, parent, child, prob, d1, d2, cw, sf, cum):
         """CPU/BeagleCPUImpl.hpp:3209-3322, 3753-3994: for one edge,
         L[c,p,i] = parent[c,p,i] * (P . child)[c,p,i];

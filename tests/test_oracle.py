@@ -124,3 +124,33 @@ def test_partitions_match_reference(reflib, syn, oracle, S, rescale):
         b = oi.getPartials(v).reshape(pr.C, pr.P, pr.S)[:, last]
         assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(b))
     ref.finalize()
+
+
+def _with_missing_tip_states(pr, tips=(0, 1), every=7):
+    """Some compact tip cells set to the missing state (S)."""
+    for t in tips:
+        if t not in pr.tip_partials:
+            pr.tip_states[t][::every] = pr.S
+    return pr
+
+
+@pytest.mark.parametrize("S,amb", [(4, 0.0), (4, 0.04), (5, 0.0), (20, 0.0)])
+def test_cross_products_match_reference(reflib, syn, oracle, S, amb):
+    """beagleCalculateCrossProductDerivative: the oracle's S x S sums against
+    the compiled reference after a full evaluation; compact tips with missing
+    states and ambiguous tips given as partials; the output is added to."""
+    pr = _with_missing_tip_states(syn.make_problem(S=S, N=9, P=60, C=3, seed=31 + S,
+                                                   rescale=True, ambiguous=amb))
+    nodes = np.arange(pr.B, dtype=np.int32)
+    outs = []
+    for make in (lambda: oracle.OracleInstance(*pr.create_args(), flags=SCALERS_LOG),
+                 lambda: reflib.create(*pr.create_args(),
+                                       preferenceFlags=DOUBLE | PROCESSOR_CPU | SCALERS_LOG,
+                                       requirementFlags=DOUBLE)):
+        inst = make()
+        pr.load(inst)
+        pr.evaluate(inst)
+        out = np.full(S * S, 0.5)
+        inst.calculateCrossProductDerivative(nodes, nodes + pr.pre(0), [0], [0], pr.lengths, out)
+        outs.append(out)
+    assert np.max(np.abs(outs[0] - outs[1])) <= 1e-12 * np.max(np.abs(outs[1]))
