@@ -9,7 +9,7 @@ fallback: without the built library, or without an sm_100 device,
 """
 import os
 
-from . import binding, checkpoint, synthetic  # noqa: F401
+from . import binding, checkpoint, shard, synthetic  # noqa: F401
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libbeagle_b200.so")
