@@ -136,6 +136,7 @@ class CheckpointPlan:
 
         stack = [pb.root]
         self.n_blocks = 0
+        self.blocks = []        # per block: (post ops, pre ops, deriv step)
         while stack:
             r = stack.pop()
             self.n_blocks += 1
@@ -158,8 +159,9 @@ class CheckpointPlan:
                     rec.append(post_op(v))
             # postorder() descends into checkpoints too; keep only this block's
             # nodes, which it emits children first.
+            block_post = np.array(rec, dtype=np.int32).reshape(-1, 7)
             if rec:
-                steps.append(("post", np.array(rec, dtype=np.int32)))
+                steps.append(("post", block_post))
             # 2. pre-order partials of every node below r in the block
             pre_ops, branches = [], []
             order = [r]
@@ -181,6 +183,7 @@ class CheckpointPlan:
             br = np.array(branches, dtype=np.int32)
             steps.append(("deriv", br, np.array([post[v] for v in branches], dtype=np.int32),
                           np.array([pre[v] for v in branches], dtype=np.int32)))
+            self.blocks.append((block_post, steps[-2][1], steps[-1]))
             # Free: r's pre-order partials, inner nodes' post and pre, tips' pre,
             # and the edge checkpoints' post (their branch is done).  The edge
             # checkpoints' pre-order partials root the blocks below.
@@ -291,6 +294,12 @@ class CheckpointPlan:
         return graph, gradient
 
 
+def quick_plan(problem, transposed_pre=False):
+    """One plan with blocks of about sqrt(N / 2) internal nodes: within a few
+    buffers of the smallest plan, built in one pass (for many trees)."""
+    return CheckpointPlan(problem, max(2, int(round((problem.N / 2) ** 0.5))), transposed_pre)
+
+
 def plan_for_budget(problem, max_buffers, transposed_pre=False):
     """The plan with the fewest calls whose tip + pool buffers fit in
     ``max_buffers``; raises ValueError when no block size fits."""
@@ -312,3 +321,48 @@ def smallest_plan(problem, transposed_pre=False):
         if best is None or (plan.n_buffers, plan.calls) < (best.n_buffers, best.calls):
             best = plan
     return best
+
+
+def batch_checkpointed_evaluate(batch, plans, lengths=None):
+    """One lnL + gradient evaluation of every member of a batch, each with its
+    own checkpoint plan (members in plan order; S > 4 members need
+    PREORDER_TRANSPOSE_AUTO).  The members' schedules run side by side: one
+    batched forward walk, scale accumulation and root lnL, then for block
+    i = 0, 1, ... one batched recomputation, pre-order walk and derivative call
+    over every member that has an i-th block (the others pass empty lists).
+    Returns (lnL[n], [gradient_m])."""
+    n = len(plans)
+    pbs = [pl.pb for pl in plans]
+    resc = [p.rescale for p in pbs]
+    if any(resc) and not all(resc):
+        raise ValueError("a batch rescales all members or none")
+    zeros, none = [0] * n, [OP_NONE] * n
+    idx = [np.arange(p.B, dtype=np.int32) for p in pbs]
+    ts = [p.lengths if lengths is None else lengths[i] for i, p in enumerate(pbs)]
+    batch.updateTransitionMatrices(zeros, idx, ts)
+    batch.updatePartials([pl.forward_ops for pl in plans], none)
+    cums = none
+    if all(resc):
+        cums = [p.cumulative for p in pbs]
+        batch.accumulateScaleFactors([np.arange(p.N - 1, dtype=np.int32) for p in pbs], cums,
+                                     reset=True)
+    lnl = batch.calculateRootLogLikelihoods([pl.root_buffer for pl in plans], zeros, zeros, cums)
+    batch.setRootPrePartials([pl.root_pre_buffer for pl in plans], zeros)
+    grads = [np.zeros(p.B) for p in pbs]
+    empty_ops = np.zeros((0, 7), dtype=np.int32)
+    empty_idx = np.zeros(0, dtype=np.int32)
+    parts = []
+    for i in range(max(len(pl.blocks) for pl in plans)):
+        blk = [pl.blocks[i] if i < len(pl.blocks) else None for pl in plans]
+        batch.updatePartials([b[0] if b else empty_ops for b in blk], none)
+        batch.updatePrePartials([b[1] if b else empty_ops for b in blk])
+        post = [b[2][2] if b else empty_idx for b in blk]
+        pre = [b[2][3] if b else empty_idx for b in blk]
+        dmat = [np.full(len(q), p.B, dtype=np.int32) for q, p in zip(post, pbs)]
+        sums, _ = batch.calculateEdgeDerivatives(post, pre, dmat, zeros)
+        parts.append([(b[2][1] if b else empty_idx, sm) for b, sm in zip(blk, sums)])
+    batch.wait()
+    for step in parts:
+        for m, (br, sm) in enumerate(step):
+            grads[m][br] = sm
+    return lnl, grads

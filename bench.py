@@ -615,6 +615,109 @@ def run_batch_arm(args):
     print(json.dumps(line))
 
 
+def run_batch_full_arm(args):
+    """--workload batch256_p50k: the batched multi-instance configuration at
+    its own pattern range (log-uniform 100-50,000; 178 GB of FP32 partials
+    with every buffer alive).  Every tree runs a subtree checkpoint plan
+    (checkpoint.quick_plan: pooled buffers, per-block recomputation); the
+    mixed path runs the 256 plans side by side through batched calls
+    (checkpoint.batch_checkpointed_evaluate); plain_fp64 runs the same plans
+    one instance at a time.  Device-timed with CUDA events on the shared
+    stream."""
+    import torch
+    pkg = importlib.import_module("beagle-lib_b200")
+    syn, ck = pkg.synthetic, pkg.checkpoint
+    lib = pkg.load()
+    probs = syn.batched_problems(count=256, seed=2000, max_patterns=50000)
+    plans = [ck.quick_plan(pr) for pr in probs]
+    n = len(probs)
+
+    def bytes_of(pr, bufs, w):
+        return bufs * pr.P * pr.C * pr.S * w
+
+    full_gb = sum(bytes_of(pr, pl.full_buffers() - pr.N, 4) for pr, pl in zip(probs, plans)) / 1e9
+    pool_gb = sum(bytes_of(pr, pl.pool, 4) for pr, pl in zip(probs, plans)) / 1e9
+
+    def instances(precision):
+        pref = (SINGLE if precision == "single" else DOUBLE) | SCALERS_LOG | PROC_GPU | ASYNCH
+        req = (SINGLE if precision == "single" else DOUBLE) | FW_CUDA
+        out = []
+        for pr, pl in zip(probs, plans):
+            inst = lib.create(*pl.create_args(), resources=[0],
+                              preferenceFlags=pref | (PRE_AUTO if pr.S > 4 else PRE_MANUAL),
+                              requirementFlags=req)
+            pr.load(inst)
+            out.append(inst)
+        return out
+
+    def timed(stream, body, steps, warmup):
+        for _ in range(warmup):
+            body()
+        torch.cuda.synchronize()
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(steps):
+            body()
+        end.record(stream)
+        end.synchronize()
+        return start.elapsed_time(end)
+
+    steps = max(2, min(args.steps, 5))
+    insts = instances("single")
+    batch = pkg.binding.Batch(lib, insts)
+    stream = torch.cuda.ExternalStream(insts[0].cudaStream())
+    state = {}
+
+    def batched():
+        state["lnl"], _ = ck.batch_checkpointed_evaluate(batch, plans)
+
+    ms_b = timed(stream, batched, steps, 2)
+    lnl32 = np.array(state["lnl"])
+    batch.finalize()
+    for x in insts:
+        x.finalize()
+    del insts, batch
+    insts = instances("double")
+    batch = pkg.binding.Batch(lib, insts)        # only to share one stream
+    stream = torch.cuda.ExternalStream(insts[0].cudaStream())
+    lnl64 = np.zeros(n)
+
+    def per_instance():
+        for pl, inst in zip(plans, insts):
+            pl.evaluate(inst)
+
+    ms_64 = timed(stream, per_instance, 1, 1)
+    for i, inst in enumerate(insts):
+        lnl64[i] = inst.getLogLikelihood()       # ASYNCH: the last evaluation's lnL
+    batch.finalize()
+    for x in insts:
+        x.finalize()
+    value = n * steps / (ms_b / 1000.0)
+    v_64 = n / (ms_64 / 1000.0)
+    line = {
+        "metric": "tree lnL+gradient evals/s, 256-tree batch at 100-50,000 patterns, "
+                  "checkpointed, mixed batched vs FP64 per-instance",
+        "value": value, "unit": "tree-evals/s", "n_gpus": 1, "steps": steps, "warmup": 2,
+        "ms_per_step": ms_b / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "trees": n,
+                   "patterns_total": int(sum(p.P for p in probs)),
+                   "states": {"4": sum(p.S == 4 for p in probs),
+                              "20": sum(p.S == 20 for p in probs)},
+                   "patterns": "log-uniform 100-50,000",
+                   "checkpointing": "quick_plan per tree (blocks of about sqrt(N/2) internal nodes)",
+                   "fp32_partials_gb_full": full_gb, "fp32_partials_gb_pooled": pool_gb},
+        "plain_fp64": {"value": v_64, "unit": "tree-evals/s",
+                       "how": "the same plans, one instance at a time, FP64",
+                       "batched_mixed_over_fp64": value / v_64,
+                       "mixed_vs_fp64_max_rel_lnl_err":
+                           float(np.max(np.abs(lnl32 - lnl64) / np.abs(lnl64)))},
+        "gpu_launches": None,
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -623,6 +726,8 @@ def main():
         run_profile_case(args)
     elif args.workload == BATCH_WORKLOAD:
         run_batch_arm(args)
+    elif args.workload == BATCH_WORKLOAD + "_p50k":
+        run_batch_full_arm(args)
     else:
         run_b200_arm(args)
 

@@ -99,3 +99,34 @@ def test_batch_graph_replay(b200, pkg, syn, precision):
     graphed.endCapture()
     plain.finalize()
     graphed.finalize()
+
+
+@pytest.mark.parametrize("asynch", [False, True], ids=["synch", "asynch"])
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_batch_checkpointed_matches_single_instances(b200, pkg, syn, precision, asynch):
+    """Every member with its own subtree checkpoint plan (pooled buffers,
+    per-block recomputation), the plans run side by side through batched
+    calls, against full evaluations one instance at a time."""
+    probs = _problems(syn)
+    singles = [_create(b200, pr, precision) for pr in probs]
+    ref = [pr.evaluate(inst, transposed_pre=False) for pr, inst in zip(probs, singles)]
+    plans = [pkg.checkpoint.smallest_plan(pr) for pr in probs]
+    pref, req = gpu_flags(precision, auto_transpose=True)
+    if asynch:
+        pref |= 1 << 3
+    members = []
+    for pr, pl in zip(probs, plans):
+        assert pl.n_buffers < pl.full_buffers()
+        inst = b200.create(*pl.create_args(), preferenceFlags=pref, requirementFlags=req)
+        pr.load(inst)
+        members.append(inst)
+    batch = pkg.binding.Batch(b200, members)
+    tol = TOL[precision]
+    for _ in range(2):
+        lnl, grads = pkg.checkpoint.batch_checkpointed_evaluate(batch, plans)
+        for i, (l0, g0) in enumerate(ref):
+            assert rel(lnl[i], l0) <= tol["lnl"], (i, lnl[i], l0)
+            assert grad_err(grads[i], g0) <= tol["grad"], i
+    batch.finalize()
+    for x in singles + members:
+        x.finalize()
