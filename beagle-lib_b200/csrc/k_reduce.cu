@@ -656,9 +656,12 @@ __global__ void k_accumulate_batch(const AccSeg* __restrict__ segs, int nseg) {
     const int p = (blockIdx.x - sg.first_cta) * blockDim.x + threadIdx.x;
     if (p >= sg.P) return;
     double acc = sg.reset ? 0.0 : sg.cum[p];
-    for (int i = 0; i < sg.n; ++i) {
-        const double v = sg.pool[(size_t)sg.idx[i] * sg.Pp + p];
-        acc += sg.log_scalers ? v : log(v);
+    if (sg.log_scalers) {
+#pragma unroll 8
+        for (int i = 0; i < sg.n; ++i) acc += sg.pool[(size_t)__ldg(sg.idx + i) * sg.Pp + p];
+    } else {
+#pragma unroll 8
+        for (int i = 0; i < sg.n; ++i) acc += log(sg.pool[(size_t)__ldg(sg.idx + i) * sg.Pp + p]);
     }
     sg.cum[p] = acc;
 }
@@ -690,10 +693,14 @@ __global__ void k_accumulate_scale(double* cum, const double* __restrict__ pool,
                                    int p_end, double sign, int log_scalers) {
     const int p = p_begin + blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= p_end) return;
+    // eight independent loads in flight per thread, added in buffer order
     double acc = 0;
-    for (int i = 0; i < n; ++i) {
-        const double v = pool[(size_t)idx[i] * Pp + p];
-        acc += log_scalers ? v : log(v);
+    if (log_scalers) {
+#pragma unroll 8
+        for (int i = 0; i < n; ++i) acc += pool[(size_t)__ldg(idx + i) * Pp + p];
+    } else {
+#pragma unroll 8
+        for (int i = 0; i < n; ++i) acc += log(pool[(size_t)__ldg(idx + i) * Pp + p]);
     }
     cum[p] += sign * acc;
 }
