@@ -122,7 +122,8 @@ Instance::~Instance() {
     for (void* p : bufs)
         if (p) cudaFree(p);
     for (DevBuf* b : {&t_ops_post_, &t_ops_pre_, &t_jobs_, &t_deriv_, &t_idx_, &t_ptr_,
-                      &scratch_, &out_, &site_d_, &t_dep_post_, &t_dep_pre_, &t_cross_})
+                      &scratch_, &out_, &site_d_, &t_dep_post_, &t_dep_pre_, &t_cross_,
+                      &d_maps_, &t_tc_maps_})
         b->release();
     if (h_out_) cudaFreeHost(h_out_);
     if (h_tc_status_) cudaFreeHost(h_tc_status_);
@@ -824,6 +825,69 @@ void assign_slots(const int* ops, int count, int stride, std::vector<OpDesc>& ta
     }
 }
 
+// TMA tensor map of partials buffer b (entry b) or of matrix m (entry nbuf + m)
+// in a device array created once; encoded and copied on first use.
+const TmaMap* Instance::tma_map(int entry, const void* base, bool matrix) {
+    const size_t n = (size_t)nbuf_ + 2 * (size_t)nmat_;
+    if (h_maps_.empty()) {
+        if (d_maps_.reserve(sizeof(TmaMap) * n) != cudaSuccess) return nullptr;
+        h_maps_.resize(n);
+        map_ok_.assign(n, 0);
+    }
+    TmaMap* dev = (TmaMap*)d_maps_.ptr + entry;
+    if (!map_ok_[entry]) {
+        if (tc_encode_map(&h_maps_[entry], base, matrix, dims()) != cudaSuccess) return nullptr;
+        const void* src = &h_maps_[entry];
+        if (capture_pinned()) {   // a captured copy reads its source at every launch
+            void* h = nullptr;
+            if (cudaMallocHost(&h, sizeof(TmaMap)) != cudaSuccess) return nullptr;
+            capture_pinned()->push_back(h);
+            std::memcpy(h, src, sizeof(TmaMap));
+            src = h;
+        }
+        if (cudaMemcpyAsync(dev, src, sizeof(TmaMap), cudaMemcpyHostToDevice, stream_) !=
+            cudaSuccess)
+            return nullptr;
+        map_ok_[entry] = 1;
+    }
+    return dev;
+}
+
+// Per-op tensor maps of a walk (TcOpMaps into t_tc_maps_): post-order, both
+// children and their matrices; pre-order, the sibling and its matrix (a2,
+// b2) and the image of the node's matrix that the second product reads as
+// rows of P_node^T (b1): the op's matrix itself when it is given transposed
+// (kM1Transposed), else its transposed image (entries nbuf + nmat + m).
+int Instance::tc_op_maps(const int* ops, int count, int stride, bool pre) {
+    std::vector<TcOpMaps> tab(count);
+    const bool given_transposed = S_ > 4 && !pre_auto_;
+    for (int k = 0; k < count; ++k) {
+        const int* op = ops + (size_t)k * stride;
+        TcOpMaps& m = tab[k];
+        m = TcOpMaps{nullptr, nullptr, nullptr, nullptr};
+        auto part = [&](int b) -> const TmaMap* {
+            return states_[b] ? nullptr : tma_map(b, partials_[b], false);
+        };
+        if (!pre && !states_[op[3]]) {
+            m.a1 = part(op[3]);
+            m.b1 = tma_map(nbuf_ + op[4], mat(op[4]), true);
+            if (!m.a1 || !m.b1) return kErrGeneral;
+        }
+        if (!states_[op[5]]) {
+            m.a2 = part(op[5]);
+            m.b2 = tma_map(nbuf_ + op[6], mat(op[6]), true);
+            if (!m.a2 || !m.b2) return kErrGeneral;
+        }
+        if (pre) {
+            m.b1 = given_transposed ? tma_map(nbuf_ + op[4], mat(op[4]), true)
+                                    : tma_map(nbuf_ + nmat_ + op[4], mat_t(op[4]), true);
+            if (!m.b1) return kErrGeneral;
+        }
+    }
+    CK(t_tc_maps_.upload(tab.data(), sizeof(TcOpMaps) * count, stream_));
+    return kSuccess;
+}
+
 int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative, bool pre) {
     if (cumulative != -1 && (cumulative < 0 || cumulative >= nscale_)) return kErrRange;
     std::vector<OpDesc> tab;
@@ -841,8 +905,15 @@ int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative,
         const OpDesc* d_ops = (const OpDesc*)t.ptr;
         const Dims dm = dims();
         const int ls = (int)log_scalers_;
-        // variant 0: CUDA-core cluster kernels; 1: tensor cores (FP32 only)
+        // variant 0: CUDA-core cluster kernels; 1: tensor cores (FP32 only);
+        // 2: tensor cores fed by TMA (FP32 only)
         auto run = [&](int v) -> cudaError_t {
+            if (v == 2) {
+                if (tc_op_maps(ops, count, stride, pre) != kSuccess) return cudaErrorInvalidValue;
+                tc_used_ = true;
+                return launch_opwalk_tc_tma(d_ops, (const TcOpMaps*)t_tc_maps_.ptr, count, pre,
+                                            dm, cum, ls, stream_);
+            }
             if (v == 1) {
                 tc_used_ = true;
                 return launch_opwalk_tc(d_ops, count, pre, dm, cum, ls, stream_);
@@ -853,14 +924,15 @@ int Instance::post_or_pre(const int* ops, int count, int stride, int cumulative,
         const bool tc = !dbl_ && tc_supported(dm);
         const TuneKey key{pre ? kTuneWalkPre : kTuneWalkPost, (int)dbl_, C_ * 100 + Sg_, Pp_,
                           tune_count_class(count), device_};
-        int v = tune_pick(key, tc ? 2 : 1, idempotent && !cum && !has_op_cum, stream_, run);
+        int v = tune_pick(key, tc ? 3 : 1, idempotent && !cum && !has_op_cum, stream_, run);
         if (v < 0) v = tc ? 1 : 0;
-        picked_[pre ? kTuneWalkPre : kTuneWalkPost] = v;
         cudaError_t e = run(v);
-        if (e == cudaErrorInvalidConfiguration && v == 1) {
+        if ((e == cudaErrorInvalidConfiguration || e == cudaErrorInvalidValue) && v >= 1) {
             (void)cudaGetLastError();
+            v = 0;
             e = run(0);
         }
+        picked_[pre ? kTuneWalkPre : kTuneWalkPost] = v;
         CK(e);
     } else {
         const OpDesc* d_ops = (const OpDesc*)t.ptr;

@@ -185,6 +185,11 @@ private:
 
     DevBuf t_ops_post_, t_ops_pre_, t_jobs_, t_deriv_, t_idx_, t_ptr_, scratch_, out_, site_d_;
     DevBuf t_cross_;                       // cross-product factors w_c r_c t_b
+    DevBuf d_maps_, t_tc_maps_;            // TMA tensor maps; per-op map table
+    std::vector<TmaMap> h_maps_;
+    std::vector<char> map_ok_;
+    const TmaMap* tma_map(int entry, const void* base, bool matrix);
+    int tc_op_maps(const int* ops, int count, int stride, bool pre);
     DevBuf t_dep_post_, t_dep_pre_;        // per op: reads the previous op's output
     double* h_out_ = nullptr;              // pinned result staging (SYNCH calls)
     size_t h_out_n_ = 0;

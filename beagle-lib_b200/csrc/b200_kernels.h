@@ -78,6 +78,11 @@ cudaError_t launch_walk_tc_batch(const WalkSeg* d_segs, int nseg, int ntiles, bo
 cudaError_t launch_deriv_tc_batch(const DerivSeg* d_segs, int nseg, int nclusters, const Dims& d,
                                   cudaStream_t s);
 bool deriv_tc_launchable(const Dims& d);
+// TMA-fed tensor-core walk (FP32, 4 < S <= 64): maps[k] gives op k's tensor
+// maps (tc_encode_map: a partials buffer, or a matrix buffer, of this shape).
+cudaError_t tc_encode_map(TmaMap* out, const void* base, bool matrix, const Dims& d);
+cudaError_t launch_opwalk_tc_tma(const OpDesc* d_ops, const TcOpMaps* d_maps, int nops, bool pre,
+                                 const Dims& d, double* cum, int ls, cudaStream_t s);
 // The flag a tensor-core kernel sets when a bounded wait on its tensor-core
 // work timed out: queue its copy into pinned host memory on `s` (read it after
 // the stream completes), and clear it (synchronises `s`).

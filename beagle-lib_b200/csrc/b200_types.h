@@ -78,6 +78,20 @@ struct PreDerivOp {
     int reserved;
 };
 
+// An opaque TMA tensor map (CUtensorMap: 128 bytes, 64-byte aligned) in
+// device memory, and the four maps one tensor-core op reads through: the
+// partials of its two operands and their matrices (null: not a partials
+// operand).
+struct alignas(64) TmaMap {
+    unsigned char bytes[128];
+};
+struct TcOpMaps {
+    const TmaMap* a1;
+    const TmaMap* a2;
+    const TmaMap* b1;
+    const TmaMap* b2;
+};
+
 // One branch of an edge-derivative launch.
 struct DerivDesc {
     const void* post;           // post-order partials (or tip states) below the branch

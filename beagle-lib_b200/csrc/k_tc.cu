@@ -43,6 +43,8 @@
 #include <cooperative_groups.h>
 
 #include "b200_kernels.h"
+#include <cuda.h>
+
 #include "b200_vec.cuh"
 
 namespace cg = cooperative_groups;
@@ -416,8 +418,8 @@ __device__ __forceinline__ void mul_operand(float out[NP], bool states, uint32_t
 // next rescaling's cluster barrier, which every CTA of the cluster reaches
 // after reading that half, so one barrier per rescaling suffices.  The walk
 // ends with a cluster barrier, so no CTA exits while another reads its smax.
-template <int NP>
-__device__ __forceinline__ void finish_row(TcSmem& sm, const OpDesc& op, float out[NP], int p,
+template <int NP, typename SM>
+__device__ __forceinline__ void finish_row(SM& sm, const OpDesc& op, float out[NP], int p,
                                            int c, int C, int S, int Sg, double* cum,
                                            int log_scalers, int& nresc) {
     const bool mine = p >= op.p_begin && p < op.p_end;   // the op's pattern range
@@ -600,6 +602,317 @@ k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double
         __syncthreads();
     }
     pipe_drain(sm, pp);
+    tc_fence_after();
+    cg::this_cluster().sync();   // every remote read of this CTA's smax is done
+    if (t < 32) tmem_dealloc(tmem, G::TCOLS);
+}
+
+// ------------------------------------------------ TMA-fed walk (variant 2)
+// The walk of k_walk_tc with every contraction chunk brought into shared
+// memory by TMA (cp.async.bulk.tensor) in the 128-byte swizzled K-major
+// layout that the MMA reads directly.
+//
+// K is cut into chunks of 32 states, one 128-byte row per pattern (A: box
+// {32, 1, 128} of the [Pp][C][Sg] partials) and per matrix row (B: box
+// {32, NP, 1} of [C][Sg][Sg]); states and rows past Sg are the tensor map's
+// zero fill.  The tensor core reads the top 19 bits of each 32-bit value for
+// kind::tf32, so the raw tile is the hi half of the 3 x tf32 split as it
+// stands.  Threads only write lo = x - hi (same swizzled positions, so the
+// pass is elementwise) for A and B.  Two stages: a chunk's loads fly while the
+// previous chunk is split and multiplied.  A stage, and its lo buffer, are
+// reused once the MMAs that read them have committed (their mbarrier).  The
+// pre-order's second product takes its A rows from registers (z), written
+// hi and lo at their swizzled positions.
+constexpr int kTK = 32;                          // K states per chunk (128-byte rows)
+struct TcTma {
+    float ahi[2][kTM * kTK];
+    float alo[2][kTM * kTK];
+    float bhi[2][64 * kTK];
+    float blo[2][64 * kTK];
+    float smax[2 * kTM];
+    double nd[kTM * 2];
+    uint64_t tma_bar[2];
+    uint64_t mma_bar[2];
+    uint32_t tmem;
+};
+
+__device__ __forceinline__ void tma_expect(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// Box at (x, y, z) of a 3-D tensor map into shared memory, completing on bar.
+__device__ __forceinline__ void tma_load3(void* dst, const TmaMap* map, int x, int y, int z,
+                                          uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Shared-memory descriptor of a K-major tile with 128-byte swizzle (sm100
+// layout type 2): rows of 128 bytes, 8-row groups 1024 bytes apart.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr) {
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;                       // leading byte offset (unused here)
+    d |= (uint64_t)((1024u >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
+    return d;
+}
+
+// lo = x - hi of n floats (multiple of 512) of a tile, elementwise.
+__device__ __forceinline__ void write_lo(float* lo, const float* hi, int n) {
+    for (int i = threadIdx.x * 4; i < n; i += kTT * 4) {
+        const float4 x = *reinterpret_cast<const float4*>(hi + i);
+        float4 l;
+        float h;
+        split_tf32(x.x, h, l.x);
+        split_tf32(x.y, h, l.y);
+        split_tf32(x.z, h, l.z);
+        split_tf32(x.w, h, l.w);
+        *reinterpret_cast<float4*>(lo + i) = l;
+    }
+}
+
+// Row t (this thread's) of an A tile from registers: z[Q kTK + k], hi and lo,
+// at the swizzled positions (16-byte piece kc of row t at kc ^ (t & 7)).
+template <int NP, int Q>
+__device__ __forceinline__ void store_row_sw(float* hi, float* lo, const float z[NP]) {
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int kc = 0; kc < kTK / 4; ++kc) {
+        float h4[4], l4[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int k = Q * kTK + kc * 4 + q;
+            split_tf32(k < NP ? z[k < NP ? k : 0] : 0.f, h4[q], l4[q]);
+        }
+        const int off = t * kTK + ((kc ^ (t & 7)) * 4);
+        st4(hi + off, h4);
+        st4(lo + off, l4);
+    }
+}
+
+// The MMAs of one chunk (thread 0): 4 K steps of 8, hi.hi + hi.lo + lo.hi,
+// committed to the stage's mbarrier.
+template <int NP>
+__device__ __forceinline__ void issue_chunk_sw(TcTma& sm, int s, uint32_t d_tmem, bool first) {
+    const uint32_t idesc = idesc_tf32(kTM, NP);
+    const uint32_t ah = smem_u32(sm.ahi[s]), al = smem_u32(sm.alo[s]);
+    const uint32_t bh = smem_u32(sm.bhi[s]), bl = smem_u32(sm.blo[s]);
+    tc_fence_after();
+#pragma unroll
+    for (int k = 0; k < kTK / 8; ++k) {
+        const uint32_t o = (uint32_t)k * 32u;
+        const uint64_t dah = smem_desc_sw128(ah + o), dal = smem_desc_sw128(al + o);
+        const uint64_t dbh = smem_desc_sw128(bh + o), dbl = smem_desc_sw128(bl + o);
+        mma_tf32(d_tmem, dah, dbh, idesc, (first && k == 0) ? 0u : 1u);
+        mma_tf32(d_tmem, dah, dbl, idesc, 1u);
+        mma_tf32(d_tmem, dal, dbh, idesc, 1u);
+    }
+    mma_commit(&sm.mma_bar[s]);
+}
+
+// Chunk pipeline state: chunks are numbered over the whole walk; chunk g uses
+// stage g & 1.  Phases of each stage's two barriers, and whether an MMA
+// commit on a stage is still unwaited.
+struct TmaPipe {
+    uint32_t tphase[2] = {0, 0};
+    uint32_t mphase[2] = {0, 0};
+    bool mpending[2] = {false, false};
+    bool failed = false;
+    int g = 0;
+};
+
+__device__ __forceinline__ void mma_wait_stage(TcTma& sm, TmaPipe& tp, int s) {
+    if (tp.mpending[s]) {
+        mbar_wait(&sm.mma_bar[s], tp.mphase[s], tp.failed);
+        tp.mphase[s] ^= 1u;
+        tp.mpending[s] = false;
+    }
+}
+
+// One chunk job: A from a tensor map (a != null) or from registers, B from a
+// tensor map.
+struct TmaJob {
+    const TmaMap* a;
+    const TmaMap* b;
+    uint32_t col;       // TMEM accumulator column
+    int q;              // K chunk
+};
+
+// Thread 0: load job j's tiles into stage s.  Every thread has waited, just
+// before, for the MMAs that last read the stage (mma_wait_stage), so that all
+// threads keep the same barrier phases.
+template <int NP>
+__device__ __forceinline__ void tma_issue(TcTma& sm, int s, const TmaJob& j, int c, int p0) {
+    if (!j.b) {
+        // no tensor map: report it, and complete the stage's phase without
+        // loading so that no wait runs out
+        atomicExch(&b200_tc_status, 1);
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&sm.tma_bar[s]))
+                     : "memory");
+        return;
+    }
+    const uint32_t bytes = (uint32_t)((j.a ? kTM : 0) + NP) * kTK * 4;
+    tma_expect(&sm.tma_bar[s], bytes);
+    if (j.a) tma_load3(sm.ahi[s], j.a, j.q * kTK, c, p0, &sm.tma_bar[s]);
+    tma_load3(sm.bhi[s], j.b, j.q * kTK, 0, c, &sm.tma_bar[s]);
+}
+
+// Run n chunk jobs (A from tensor maps); job i + 1's loads are issued before
+// job i is split and multiplied.
+template <int NP>
+__device__ __forceinline__ void run_jobs_sw(TcTma& sm, TmaPipe& tp, uint32_t tmem,
+                                            const TmaJob (&jobs)[4], int n, int c, int p0) {
+    if (n > 0) {
+        mma_wait_stage(sm, tp, tp.g & 1);
+        if (threadIdx.x == 0) tma_issue<NP>(sm, tp.g & 1, jobs[0], c, p0);
+    }
+    for (int i = 0; i < n; ++i) {
+        const int s = (tp.g + i) & 1;
+        if (i + 1 < n) {
+            mma_wait_stage(sm, tp, s ^ 1);
+            if (threadIdx.x == 0) tma_issue<NP>(sm, s ^ 1, jobs[i + 1], c, p0);
+        }
+        mbar_wait(&sm.tma_bar[s], tp.tphase[s], tp.failed);
+        tp.tphase[s] ^= 1u;
+        write_lo(sm.alo[s], sm.ahi[s], kTM * kTK);
+        write_lo(sm.blo[s], sm.bhi[s], NP * kTK);
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        if (threadIdx.x == 0) issue_chunk_sw<NP>(sm, s, tmem + jobs[i].col, jobs[i].q == 0);
+        tp.mpending[s] = true;
+    }
+    tp.g += n;
+}
+
+// Wait for every committed MMA (both stages).
+__device__ __forceinline__ void mma_drain(TcTma& sm, TmaPipe& tp) {
+    mma_wait_stage(sm, tp, 0);
+    mma_wait_stage(sm, tp, 1);
+}
+
+template <int NP, bool PRE>
+__global__ void __launch_bounds__(kTT, 2)
+k_walk_tc_tma(const OpDesc* __restrict__ ops, const TcOpMaps* __restrict__ maps, int nops,
+              int S, int Sg, int C, double* cum, int log_scalers) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // tiles at a 1024-byte aligned shared address (the swizzle's period; the
+    // launch adds 1 KB of slack)
+    unsigned char* base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    TcTma& sm = *reinterpret_cast<TcTma*>(base);
+    using G = TcGeo<NP>;
+    const int t = threadIdx.x;
+    const int c = blockIdx.x % C;
+    const int p0 = (blockIdx.x / C) * kTM;
+    const int p = p0 + t;
+    constexpr int NKC = NP > kTK ? 2 : 1;
+    const size_t mo = (size_t)c * Sg * Sg;
+
+    if (t == 0) {
+        for (int k = 0; k < 2; ++k) {
+            mbar_init(&sm.tma_bar[k], 1);
+            mbar_init(&sm.mma_bar[k], 1);
+        }
+        mbar_init_fence();
+    }
+    if (t < 32) {
+        tmem_alloc(&sm.tmem, G::TCOLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = sm.tmem;
+    TmaPipe tp;
+    int nresc = 0;
+    for (int o = 0; o < nops; ++o) {
+        const OpDesc& op = ops[o];
+        const TcOpMaps mp = maps[o];
+        const bool st1 = !PRE && (op.kind & kX1States), st2 = op.kind & kX2States;
+        TmaJob jobs[4];
+        int nj = 0;
+        float out[NP];
+        if (!PRE) {
+            // child 1 -> columns [0, NP), child 2 -> [NP, 2 NP)
+            for (int q = 0; q < NKC; ++q)
+                if (!st1) jobs[nj++] = TmaJob{mp.a1, mp.b1, 0u, q};
+            for (int q = 0; q < NKC; ++q)
+                if (!st2) jobs[nj++] = TmaJob{mp.a2, mp.b2, (uint32_t)NP, q};
+            run_jobs_sw<NP>(sm, tp, tmem, jobs, nj, c, p0);
+            int s1 = 0, s2 = 0;
+            if (st1) s1 = static_cast<const int*>(op.x1)[p];
+            if (st2) s2 = static_cast<const int*>(op.x2)[p];
+            mma_drain(sm, tp);
+            tc_fence_after();
+#pragma unroll
+            for (int i = 0; i < NP; ++i) out[i] = 1.f;
+            mul_operand<NP>(out, st1, tmem, 0, static_cast<const float*>(op.m1t) + mo, s1, S, Sg,
+                            (float)op.pad1);
+            mul_operand<NP>(out, st2, tmem, NP, static_cast<const float*>(op.m2t) + mo, s2, S, Sg,
+                            (float)op.pad2);
+        } else {
+            // GEMM 1: (P_sib . x_sib) -> columns [0, NP)
+            for (int q = 0; q < NKC; ++q)
+                if (!st2) jobs[nj++] = TmaJob{mp.a2, mp.b2, 0u, q};
+            run_jobs_sw<NP>(sm, tp, tmem, jobs, nj, c, p0);
+            float par[NP];
+            {
+                const float* pr = static_cast<const float*>(op.x1) + ((size_t)p * C + c) * Sg;
+#pragma unroll
+                for (int j = 0; j < NP / 4; ++j) {
+                    par[4 * j] = par[4 * j + 1] = par[4 * j + 2] = par[4 * j + 3] = 0.f;
+                    if (4 * j < Sg) ld4(pr + 4 * j, par + 4 * j);
+                }
+            }
+            int s2 = 0;
+            if (st2) s2 = static_cast<const int*>(op.x2)[p];
+            // GEMM 2's first B chunk (rows of P_node^T) while GEMM 1 runs
+            const TmaJob j0{nullptr, mp.b1, (uint32_t)NP, 0};
+            mma_wait_stage(sm, tp, tp.g & 1);
+            if (t == 0) tma_issue<NP>(sm, tp.g & 1, j0, c, p0);
+            mma_drain(sm, tp);
+            tc_fence_after();
+            float* z = par;
+            mul_operand<NP>(z, st2, tmem, 0, static_cast<const float*>(op.m2t) + mo, s2, S, Sg,
+                            (float)op.pad2);
+            // GEMM 2: dest = z . P_node -> columns [NP, 2 NP); A rows from z
+#pragma unroll
+            for (int q = 0; q < NKC; ++q) {
+                const int s = tp.g & 1;
+                if (q + 1 < NKC) {
+                    mma_wait_stage(sm, tp, s ^ 1);
+                    if (t == 0)
+                        tma_issue<NP>(sm, s ^ 1, TmaJob{nullptr, mp.b1, (uint32_t)NP, q + 1}, c,
+                                      p0);
+                }
+                if (q == 0) store_row_sw<NP, 0>(sm.ahi[s], sm.alo[s], z);
+                else store_row_sw<NP, 1>(sm.ahi[s], sm.alo[s], z);
+                mbar_wait(&sm.tma_bar[s], tp.tphase[s], tp.failed);
+                tp.tphase[s] ^= 1u;
+                write_lo(sm.blo[s], sm.bhi[s], NP * kTK);
+                fence_async_smem();
+                tc_fence_before();
+                __syncthreads();
+                if (t == 0) issue_chunk_sw<NP>(sm, s, tmem + NP, q == 0);
+                tp.mpending[s] = true;
+                ++tp.g;
+            }
+            mma_drain(sm, tp);
+            tc_fence_after();
+#pragma unroll
+            for (int j = 0; j < NP / 16; ++j) tmem_chunk(tmem, NP, j, out + 16 * j);
+        }
+        finish_row<NP>(sm, op, out, p, c, C, S, Sg, PRE ? nullptr : cum, log_scalers, nresc);
+        tc_fence_before();
+        __syncthreads();
+    }
+    mma_drain(sm, tp);
     tc_fence_after();
     cg::this_cluster().sync();   // every remote read of this CTA's smax is done
     if (t < 32) tmem_dealloc(tmem, G::TCOLS);
@@ -897,6 +1210,82 @@ cudaError_t launch_deriv_tc_batch(const DerivSeg* d_segs, int nseg, int ncluster
 #define DERB_(NP, KC) run_deriv_tc_batch<NP, KC>(d_segs, nseg, nclusters, d, s)
     return B200_TC_DISPATCH(d.Sg, DERB_);
 #undef DERB_
+}
+
+// ------------------------------------------------------- TMA tensor maps
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library).  Partials [Pp][C][Sg] (FP32): a 3-D map
+// {Sg, C, Pp} with box {KC, 1, 128}; matrices [C][Sg][Sg]: {Sg, Sg, C} with
+// box {KC, NP, 1}.  Elements past Sg are zero-filled; with KC = 32 (128-byte
+// rows) the 128-byte swizzle, otherwise none.
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        (void)cudaGetLastError();
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+static int tc_np(int Sg) { return Sg <= 16 ? 16 : Sg <= 32 ? 32 : Sg <= 48 ? 48 : 64; }
+
+cudaError_t tc_encode_map(TmaMap* out, const void* base, bool matrix, const Dims& d) {
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn || !tc_supported(d)) return cudaErrorNotSupported;
+    const int NP = tc_np(d.Sg), KC = kTK;
+    cuuint64_t dims[3], strides[2];
+    cuuint32_t box[3], es[3] = {1, 1, 1};
+    if (!matrix) {
+        dims[0] = (cuuint64_t)d.Sg; dims[1] = (cuuint64_t)d.C; dims[2] = (cuuint64_t)d.Pp;
+        strides[0] = (cuuint64_t)d.Sg * 4; strides[1] = (cuuint64_t)d.C * d.Sg * 4;
+        box[0] = (cuuint32_t)KC; box[1] = 1; box[2] = (cuuint32_t)kTM;
+    } else {
+        dims[0] = (cuuint64_t)d.Sg; dims[1] = (cuuint64_t)d.Sg; dims[2] = (cuuint64_t)d.C;
+        strides[0] = (cuuint64_t)d.Sg * 4; strides[1] = (cuuint64_t)d.Sg * d.Sg * 4;
+        box[0] = (cuuint32_t)KC; box[1] = (cuuint32_t)NP; box[2] = 1;
+    }
+    const CUresult r = fn(reinterpret_cast<CUtensorMap*>(out), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                          const_cast<void*>(base), dims, strides, box, es,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_128B,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+template <int NP>
+cudaError_t run_walk_tc_tma(const OpDesc* ops, const TcOpMaps* maps, int nops, bool pre,
+                            const Dims& d, double* cum, int ls, cudaStream_t s) {
+    const int cols = TcGeo<NP>::TCOLS;
+    const int grid = (d.Pp / kTM) * d.C;
+    const size_t need = sizeof(TcTma) + 1024;
+    const size_t floor_smem = tc_smem(cols);
+    const size_t smem = need > floor_smem ? need : floor_smem;
+    return pre ? launch_tc(k_walk_tc_tma<NP, true>, grid, smem, d.C, cols, s, ops, maps, nops,
+                           d.S, d.Sg, d.C, (double*)nullptr, ls)
+               : launch_tc(k_walk_tc_tma<NP, false>, grid, smem, d.C, cols, s, ops, maps, nops,
+                           d.S, d.Sg, d.C, cum, ls);
+}
+
+cudaError_t launch_opwalk_tc_tma(const OpDesc* ops, const TcOpMaps* maps, int nops, bool pre,
+                                 const Dims& d, double* cum, int ls, cudaStream_t s) {
+    if (nops == 0) return cudaSuccess;
+    if (!tc_supported(d) || !encode_tiled()) return cudaErrorInvalidValue;
+    switch (tc_np(d.Sg)) {
+        case 16: return run_walk_tc_tma<16>(ops, maps, nops, pre, d, cum, ls, s);
+        case 32: return run_walk_tc_tma<32>(ops, maps, nops, pre, d, cum, ls, s);
+        case 48: return run_walk_tc_tma<48>(ops, maps, nops, pre, d, cum, ls, s);
+        default: return run_walk_tc_tma<64>(ops, maps, nops, pre, d, cum, ls, s);
+    }
 }
 
 cudaError_t tc_status_async(int* pinned_dst, cudaStream_t s) {

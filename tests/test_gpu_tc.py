@@ -1,6 +1,8 @@
-"""The FP32 path for 4 < S <= 64 has two kernel families that compute the same
-results: CUDA-core cluster kernels (variant 0) and tensor-core tcgen05 kernels
-with 3 x tf32 split products (variant 1, k_tc.cu).  Each is forced in turn
+"""The FP32 path for 4 < S <= 64 has kernel families that compute the same
+results: CUDA-core cluster kernels (variant 0), tensor-core tcgen05 kernels
+with 3 x tf32 split products (variant 1, k_tc.cu), and for the walks the same
+tensor-core kernels fed by TMA (variant 2; the derivative runs variant 1 then).
+Each is forced in turn
 (BEAGLE_B200_FORCE_VARIANT) and checked against the oracle: lnL and gradient
 at the mixed-path tolerances, and the intermediate buffers (partials, scale
 factors, pre-order partials, per-site derivatives) at 2e-4 of the buffer
@@ -17,13 +19,16 @@ pytestmark = pytest.mark.gpu
 CASES = [(5, 3), (13, 2), (20, 4), (33, 2), (48, 8), (61, 4), (61, 1)]
 
 
-@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("variant", [0, 1, 2])
 @pytest.mark.parametrize("S,C", CASES, ids=[f"S{s}C{c}" for s, c in CASES])
 def test_fp32_generic_kernels(b200, syn, oracle, monkeypatch, variant, S, C):
     monkeypatch.setenv("BEAGLE_B200_FORCE_VARIANT", str(variant))
     pr = syn.make_problem(S=S, N=10, P=700, C=C, seed=500 + S + C, rescale=True,
                           ambiguous=0.01)
     inst, lnl, g = run_b200(b200, pr, "single")
+    if variant == 2:   # the TMA-fed walks ran (no fallback to the CUDA-core kernels)
+        tv = inst.tunedVariants()
+        assert tv["post"] == 2 and tv["pre"] == 2, tv
     oi, lo, go = run_oracle(oracle, pr)
     tol = TOL["single"]
     assert rel(lnl, lo) <= tol["lnl"], (lnl, lo)
@@ -44,7 +49,7 @@ def test_fp32_generic_kernels(b200, syn, oracle, monkeypatch, variant, S, C):
     inst.finalize()
 
 
-@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("variant", [0, 1, 2])
 def test_fp32_generic_auto_transpose_and_raw_scalers(b200, syn, oracle, monkeypatch, variant):
     monkeypatch.setenv("BEAGLE_B200_FORCE_VARIANT", str(variant))
     pr = syn.make_problem(S=61, N=8, P=300, C=2, seed=77, rescale=True)
