@@ -445,6 +445,26 @@ class Instance:
         return (code, float(o[0]), None if o1 is None else float(o1[0]),
                 None if o2 is None else float(o2[0]))
 
+    def calculateEdgeLogLikelihoodsByPartition(self, parents, children, probs, d1s, d2s, cw,
+                                               sf, cum, parts, check=True):
+        """Per partition i, the edge lnL of (parents[i], children[i], probs[i])
+        over partition parts[i]; d1s / d2s both None (lnL only) or both lists.
+        Returns (code, lnL by partition, lnL, d1 by partition or None, d1,
+        d2 by partition or None, d2)."""
+        p = _i32(parts)
+        n = len(p)
+        arr = [_i32(parents), _i32(children), _i32(probs),
+               None if d1s is None else _i32(d1s), None if d2s is None else _i32(d2s),
+               _i32(cw), _i32(sf), _i32(cum), p]
+        byp, tot = np.zeros(n), np.zeros(1)
+        d1p, d1t = (np.zeros(n), np.zeros(1)) if d1s is not None else (None, None)
+        d2p, d2t = (np.zeros(n), np.zeros(1)) if d2s is not None else (None, None)
+        code = self._call("CalculateEdgeLogLikelihoodsByPartition", *[_ptr(x) for x in arr], n,
+                          1, _ptr(byp), _ptr(tot), _ptr(d1p), _ptr(d1t), _ptr(d2p), _ptr(d2t),
+                          check=check)
+        return (code, byp, float(tot[0]), d1p, None if d1t is None else float(d1t[0]), d2p,
+                None if d2t is None else float(d2t[0]))
+
     def getLogLikelihood(self, check=True):
         o = np.zeros(1)
         code = self._call("GetLogLikelihood", _ptr(o), check=False)

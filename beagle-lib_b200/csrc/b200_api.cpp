@@ -384,6 +384,15 @@ int beagleB200CalculateEdgeLogLikelihoods(int h, const int* pa, const int* ch, c
         return in->calculateEdgeLogLikelihoods(pa, ch, pm, d1, d2, w, f, c, n, o, o1, o2);
     });
 }
+int beagleB200CalculateEdgeLogLikelihoodsByPartition(
+    int h, const int* pa, const int* ch, const int* pm, const int* d1, const int* d2,
+    const int* w, const int* f, const int* c, const int* parts, int np, int n, double* byp,
+    double* o, double* d1byp, double* o1, double* d2byp, double* o2) {
+    return call(h, [&](b200::Instance* in) {
+        return in->calculateEdgeLogLikelihoodsByPartition(pa, ch, pm, d1, d2, w, f, c, parts, np,
+                                                          n, byp, o, d1byp, o1, d2byp, o2);
+    });
+}
 int beagleB200GetLogLikelihood(int h, double* o) {
     return call(h, [&](b200::Instance* in) { return in->getLogLikelihood(o); });
 }

@@ -1419,6 +1419,89 @@ int Instance::calculateEdgeLogLikelihoods(const int* parents, const int* childre
     return std::isnan(*outLnL) ? kErrFP : kSuccess;
 }
 
+// CPU/BeagleCPUImpl.hpp:3008-3110 (count 1): per partition i the edge lnL of
+// (parents[i], children[i], prob[i]) over partition parts[i]'s patterns, and
+// their total; with both derivative matrices, the first and second derivative
+// sums as well (:3452-3587).  A first derivative without a second is
+// NO_IMPLEMENTATION there, and here.
+int Instance::calculateEdgeLogLikelihoodsByPartition(
+    const int* parents, const int* children, const int* prob, const int* d1, const int* d2,
+    const int* cw, const int* sf, const int* cum, const int* parts, int nparts, int count,
+    double* outByPart, double* out, double* outD1ByPart, double* outD1, double* outD2ByPart,
+    double* outD2) {
+    if (count != 1) return kErrNoImpl;
+    if ((d1 != nullptr) != (d2 != nullptr)) return kErrNoImpl;
+    const bool derivs = d1 != nullptr;
+    if (nparts < 1 || !parents || !children || !prob || !cw || !sf || !parts || !outByPart ||
+        !out)
+        return kErrRange;
+    if (derivs && (!outD1ByPart || !outD1 || !outD2ByPart || !outD2)) return kErrRange;
+    if (partition_start_.empty()) return kErrRange;
+    const int npart_defined = (int)partition_start_.size() - 1;
+    int total_blocks = 0;
+    for (int i = 0; i < nparts; ++i) {
+        const int pa = parents[i], ch = children[i], pm = prob[i], w = cw[i], f = sf[i];
+        const int c = cum ? cum[i] : -1, q = parts[i];
+        if (!buf_ok(pa) || !partials_[pa] || !has_data(ch)) return kErrRange;
+        if (pm < 0 || pm >= nmat_) return kErrRange;
+        if (derivs && (d1[i] < 0 || d1[i] >= nmat_ || d2[i] < 0 || d2[i] >= nmat_))
+            return kErrRange;
+        if (w < 0 || w >= neig_ || !catw_set_[w] || f < 0 || f >= neig_ || !freqs_set_[f])
+            return kErrRange;
+        if (c != -1 && (c < 0 || c >= nscale_)) return kErrRange;
+        if (q < 0 || q >= npart_defined) return kErrRange;
+        total_blocks += 3 * reduction_blocks(partition_start_[q + 1] - partition_start_[q]);
+    }
+    CK(scratch_.reserve(sizeof(double) * std::max(total_blocks, 1)));
+    CK(out_.reserve(sizeof(double) * 3 * nparts));
+    double* blocks = (double*)scratch_.ptr;
+    for (int i = 0; i < nparts; ++i) {
+        const int pa = parents[i], ch = children[i], pm = prob[i], w = cw[i], f = sf[i];
+        const int c = cum ? cum[i] : -1, q = parts[i];
+        const int p0 = partition_start_[q], p1 = partition_start_[q + 1];
+        const int m1 = derivs ? d1[i] : -1, m2 = derivs ? d2[i] : -1;
+        const bool st = states_[ch] != nullptr;
+        CK(LAUNCH(launch_edge_lnl_range, partials_[pa],
+                  st ? (const void*)states_[ch] : partials_[ch], (int)st, mat(pm), mat_pad_[pm],
+                  m1 >= 0 ? mat(m1) : nullptr, m1 >= 0 ? mat_pad_[m1] : 0.0,
+                  m2 >= 0 ? mat(m2) : nullptr, m2 >= 0 ? mat_pad_[m2] : 0.0,
+                  d_catw_ + (size_t)w * C_, d_freqs_ + (size_t)f * S_,
+                  c >= 0 ? scale(c) : nullptr, d_patw_, dims(), p0, p1, d_site_, d_site1_,
+                  d_site2_, blocks, (double*)out_.ptr + 3 * i, stream_));
+        blocks += 3 * reduction_blocks(p1 - p0);
+    }
+    if ((size_t)(3 * nparts) > h_out_n_) {
+        cudaFreeHost(h_out_);
+        h_out_ = nullptr;
+        h_out_n_ = 3 * nparts;
+        CK(cudaMallocHost(&h_out_, sizeof(double) * h_out_n_));
+    }
+    CK(cudaMemcpyAsync(h_out_, out_.ptr, sizeof(double) * 3 * nparts, cudaMemcpyDeviceToHost,
+                       stream_));
+    int rc = sync();
+    if (rc) return rc;
+    double tot = 0, tot1 = 0, tot2 = 0;
+    for (int i = 0; i < nparts; ++i) {
+        outByPart[i] = h_out_[3 * i];
+        tot += h_out_[3 * i];
+        if (derivs) {
+            outD1ByPart[i] = h_out_[3 * i + 1];
+            outD2ByPart[i] = h_out_[3 * i + 2];
+            tot1 += h_out_[3 * i + 1];
+            tot2 += h_out_[3 * i + 2];
+        }
+    }
+    *out = tot;
+    last_lnl_ = tot;
+    if (derivs) {
+        *outD1 = tot1;
+        *outD2 = tot2;
+        last_d1_ = tot1;
+        last_d2_ = tot2;
+    }
+    return (std::isnan(tot) || std::isnan(tot1) || std::isnan(tot2)) ? kErrFP : kSuccess;
+}
+
 int Instance::getLogLikelihood(double* out) {
     if (!out) return kErrRange;
     int rc = sync();

@@ -111,6 +111,13 @@ public:
                                     const int* d1, const int* d2, const int* cw, const int* sf,
                                     const int* cum, int count, double* outLnL, double* outD1,
                                     double* outD2);
+    int calculateEdgeLogLikelihoodsByPartition(const int* parents, const int* children,
+                                               const int* prob, const int* d1, const int* d2,
+                                               const int* cw, const int* sf, const int* cum,
+                                               const int* parts, int nparts, int count,
+                                               double* outByPart, double* out,
+                                               double* outD1ByPart, double* outD1,
+                                               double* outD2ByPart, double* outD2);
     int getLogLikelihood(double* out);
     int getDerivatives(double* d1, double* d2);
     int getSiteLogLikelihoods(double* out);

@@ -116,6 +116,17 @@ cudaError_t launch_edge_lnl(const void* parent, const void* child, int child_is_
                             double* d_site1, double* d_site2, double* d_block,
                             double* d_out, cudaStream_t s);
 
+// The same over patterns [p_begin, p_end) only: d_out gets that range's three
+// sums, d_site / d_site1 / d_site2 only its entries.
+template <typename Real>
+cudaError_t launch_edge_lnl_range(const void* parent, const void* child, int child_is_states,
+                                  const void* pmat, double ppad, const void* d1mat, double d1pad,
+                                  const void* d2mat, double d2pad, const double* catw,
+                                  const double* freqs, const double* cumulative,
+                                  const double* patw, const Dims& d, int p_begin, int p_end,
+                                  double* d_site, double* d_site1, double* d_site2,
+                                  double* d_block, double* d_out, cudaStream_t s);
+
 // Edge derivatives for `nb` branches; per-site values optional (d_site may be
 // null), sums and sums of squares into d_sums[2*nb].  d_block holds
 // 2 * nb * deriv_blocks(d) doubles of per-block partial sums.  `variant`

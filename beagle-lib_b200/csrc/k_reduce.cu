@@ -137,11 +137,12 @@ k_edge_lnl(const Real* __restrict__ par, const void* child, int states, const Re
            double ppad, const Real* d1m, double d1pad, const Real* d2m, double d2pad,
            const double* __restrict__ catw, const double* __restrict__ freqs,
            const double* __restrict__ cum, const double* __restrict__ patw, int S, int Sg,
-           int C, int P, double* site, double* site1, double* site2, double* block) {
+           int C, int p_begin, int p_end, double* site, double* site1, double* site2,
+           double* block) {
     __shared__ double sh[kRB / 32];
-    const int p = blockIdx.x * kRB + threadIdx.x;
+    const int p = p_begin + blockIdx.x * kRB + threadIdx.x;
     double v0 = 0, v1 = 0, v2 = 0;
-    if (p < P) {
+    if (p < p_end) {
         const double L = edge_integrate(par, child, states, pm, ppad, catw, freqs, S, Sg, C, p);
         double l = log(L);
         if (cum) l += cum[p];
@@ -737,11 +738,26 @@ cudaError_t launch_edge_lnl(const void* parent, const void* child, int child_is_
                             const double* freqs, const double* cum, const double* patw,
                             const Dims& d, double* d_site, double* d_site1, double* d_site2,
                             double* d_block, double* d_out, cudaStream_t s) {
-    const int nblk = reduction_blocks(d.P);
+    return launch_edge_lnl_range<Real>(parent, child, child_is_states, pmat, ppad, d1mat, d1pad,
+                                       d2mat, d2pad, catw, freqs, cum, patw, d, 0, d.P, d_site,
+                                       d_site1, d_site2, d_block, d_out, s);
+}
+
+template <typename Real>
+cudaError_t launch_edge_lnl_range(const void* parent, const void* child, int child_is_states,
+                                  const void* pmat, double ppad, const void* d1mat, double d1pad,
+                                  const void* d2mat, double d2pad, const double* catw,
+                                  const double* freqs, const double* cum, const double* patw,
+                                  const Dims& d, int p_begin, int p_end, double* d_site,
+                                  double* d_site1, double* d_site2, double* d_block,
+                                  double* d_out, cudaStream_t s) {
+    const int nblk = reduction_blocks(p_end - p_begin);
+    if (nblk == 0) return cudaMemsetAsync(d_out, 0, 3 * sizeof(double), s);
     k_edge_lnl<Real><<<nblk, kRB, 0, s>>>(
         static_cast<const Real*>(parent), child, child_is_states, static_cast<const Real*>(pmat),
         ppad, static_cast<const Real*>(d1mat), d1pad, static_cast<const Real*>(d2mat), d2pad,
-        catw, freqs, cum, patw, d.S, d.Sg, d.C, d.P, d_site, d_site1, d_site2, d_block);
+        catw, freqs, cum, patw, d.S, d.Sg, d.C, p_begin, p_end, d_site, d_site1, d_site2,
+        d_block);
     k_final_sum<<<3, kRB, 0, s>>>(d_block, nblk, 3, d_out);
     return cudaGetLastError();
 }
@@ -1026,6 +1042,10 @@ template cudaError_t launch_root_batch<double>(const RootSeg*, int, int, cudaStr
                                             const double*, const double*, const double*,         \
                                             const double*, const Dims&, double*, double*,        \
                                             double*, double*, double*, cudaStream_t);            \
+    template cudaError_t launch_edge_lnl_range<R>(                                               \
+        const void*, const void*, int, const void*, double, const void*, double, const void*,    \
+        double, const double*, const double*, const double*, const double*, const Dims&, int,    \
+        int, double*, double*, double*, double*, double*, cudaStream_t);                         \
     template cudaError_t launch_edge_derivatives<R>(const DerivDesc*, int, const double*,        \
                                                     const double*, const Dims&, double*,         \
                                                     double*, double*, cudaStream_t, int);

@@ -208,11 +208,15 @@ public:
         return beagleB200CalculateEdgeLogLikelihoods(h_, pa, ch, p, d1, d2, w, f, s, n, lnl, o1,
                                                      o2);
     }
-    int calculateEdgeLogLikelihoodsByPartition(const int*, const int*, const int*, const int*,
-                                               const int*, const int*, const int*, const int*,
-                                               const int*, int, int, double*, double*, double*,
-                                               double*, double*, double*) override {
-        return BEAGLE_ERROR_NO_IMPLEMENTATION;
+    int calculateEdgeLogLikelihoodsByPartition(const int* pa, const int* ch, const int* p,
+                                               const int* d1, const int* d2, const int* w,
+                                               const int* f, const int* s, const int* parts,
+                                               int np, int n, double* byp, double* lnl,
+                                               double* d1byp, double* o1, double* d2byp,
+                                               double* o2) override {
+        return beagleB200CalculateEdgeLogLikelihoodsByPartition(h_, pa, ch, p, d1, d2, w, f, s,
+                                                                parts, np, n, byp, lnl, d1byp,
+                                                                o1, d2byp, o2);
     }
     int getLogLikelihood(double* out) override { return beagleB200GetLogLikelihood(h_, out); }
     int getDerivatives(double* d1, double* d2) override {

@@ -316,6 +316,18 @@ int beagleB200CalculateEdgeLogLikelihoods(int instance, const int* parentBufferI
                                           double* outSumLogLikelihood,
                                           double* outSumFirstDerivative,
                                           double* outSumSecondDerivative);
+/* replaces beagleCalculateEdgeLogLikelihoodsByPartition (beagle.h:1314-1332): count 1;
+ * lnL alone, or with both derivative sums (a first derivative alone returns
+ * BEAGLE_B200_ERROR_NO_IMPLEMENTATION, as the reference CPU implementation does) */
+int beagleB200CalculateEdgeLogLikelihoodsByPartition(
+    int instance, const int* parentBufferIndices, const int* childBufferIndices,
+    const int* probabilityIndices, const int* firstDerivativeIndices,
+    const int* secondDerivativeIndices, const int* categoryWeightsIndices,
+    const int* stateFrequenciesIndices, const int* cumulativeScaleIndices,
+    const int* partitionIndices, int partitionCount, int count,
+    double* outSumLogLikelihoodByPartition, double* outSumLogLikelihood,
+    double* outSumFirstDerivativeByPartition, double* outSumFirstDerivative,
+    double* outSumSecondDerivativeByPartition, double* outSumSecondDerivative);
 /* replaces beagleGetLogLikelihood (beagle.h:1350-1351) */
 int beagleB200GetLogLikelihood(int instance, double* outSumLogLikelihood);
 /* replaces beagleGetDerivatives (beagle.h:1368-1370) */

@@ -24,6 +24,7 @@ import numpy as np
 SUCCESS = 0
 ERROR_GENERAL = -1
 ERROR_OUT_OF_RANGE = -5
+ERROR_NO_IMPLEMENTATION = -7
 ERROR_FLOATING_POINT = -8
 OP_NONE = -1
 FLAG_PRECISION_SINGLE = 1 << 0
@@ -460,3 +461,51 @@ class OracleInstance:
                 s2 = float(np.dot(g2, self.patw))
         code = ERROR_FLOATING_POINT if total != total else SUCCESS
         return code, total, s1, s2
+
+    def calculateEdgeLogLikelihoodsByPartition(self, parents, children, probs, d1s, d2s, cws,
+                                               sfs, cums, parts):
+        """CPU/BeagleCPUImpl.hpp:3008-3110 with :3325-3450 and :3452-3587
+        (count 1): for entry i, the edge lnL of (parents[i], children[i],
+        probs[i]) over partition parts[i]'s patterns, with the site values of
+        calculateEdgeLogLikelihoods written for those patterns; with both
+        derivative lists, also the d1 and d2 sums (d1 alone is
+        NO_IMPLEMENTATION there).  Returns (code, lnL by entry, lnL, d1 by
+        entry, d1, d2 by entry, d2)."""
+        if d1s is not None and d2s is None:
+            return ERROR_NO_IMPLEMENTATION, None, None, None, None, None, None
+        derivs = d1s is not None
+        for name in ('site_lnl', 'site_d1', 'site_d2'):
+            if getattr(self, name, None) is None:
+                setattr(self, name, np.zeros(self.P))
+        byp, d1p, d2p = [], [], []
+        for i, part in enumerate(parts):
+            rng = self._range(part)
+            par = self.partials[parents[i]][:, rng, :]
+            f = self.freqs[sfs[i]]
+            w = self.catw[cws[i]]
+
+            def integ(mat):
+                y = self._child(children[i], mat)[:, rng, :]
+                return np.einsum('c,cpi,i->p', w, par * y, f)
+
+            L = integ(probs[i])
+            site = np.log(L)
+            if cums[i] != OP_NONE:
+                site = site + self.scale[cums[i]][rng]
+            self.site_lnl[rng] = site
+            byp.append(float(np.dot(site, self.patw[rng])))
+            if derivs:
+                g1 = integ(d1s[i]) / L
+                g2 = integ(d2s[i]) / L - g1 * g1
+                self.site_d1[rng] = g1
+                self.site_d2[rng] = g2
+                d1p.append(float(np.dot(g1, self.patw[rng])))
+                d2p.append(float(np.dot(g2, self.patw[rng])))
+        total = float(sum(byp))
+        code = ERROR_FLOATING_POINT if total != total else SUCCESS
+        if not derivs:
+            return code, np.array(byp), total, None, None, None, None
+        t1, t2 = float(sum(d1p)), float(sum(d2p))
+        if t1 != t1 or t2 != t2:
+            code = ERROR_FLOATING_POINT
+        return code, np.array(byp), total, np.array(d1p), t1, np.array(d2p), t2

@@ -57,7 +57,7 @@ def partitioned_args(problem, nparts):
     """create_args with room for per-partition matrices, scale buffers and
     cumulative buffers."""
     args = list(problem.create_args())
-    args[6] = max(args[6], nparts * problem.B + 1)
+    args[6] = max(args[6], nparts * problem.B + 1 + 2 * nparts)
     args[8] = max(args[8], nparts * (problem.N - 1) + nparts)
     return args
 
@@ -102,3 +102,28 @@ def run_partitioned(inst, problem, nparts, rescale=True, pre=True):
                              q, -1])
         inst.updatePrePartialsByPartition(np.array(pops, dtype=np.int32))
     return np.asarray(byp), tot
+
+
+def edge_by_partition(inst, problem, nparts, v, derivs, parent=None):
+    """calculateEdgeLogLikelihoodsByPartition after run_partitioned: for each
+    partition q the edge between node v's parent's pre-order partials (or the
+    buffer `parent`) and v (post-order partials or a tip), with partition q's
+    matrix of branch v; with
+    `derivs`, its first and second derivative matrices are formed first in the
+    spare matrices nparts * B + 1 + (0 .. 2 nparts).  Returns the call's tuple
+    and the site log-likelihoods."""
+    pr = problem
+    d1 = d2 = None
+    if derivs:
+        base = nparts * pr.B + 1
+        d1 = [base + q for q in range(nparts)]
+        d2 = [base + nparts + q for q in range(nparts)]
+        for q in range(nparts):
+            inst.updateTransitionMatrices(0, [q * pr.B + v], [d1[q]], [d2[q]],
+                                          [pr.lengths[v] * (1 + 0.3 * q)])
+    par = pr.pre(int(pr.parent[v])) if parent is None else parent
+    cum0 = nparts * (pr.N - 1)
+    res = inst.calculateEdgeLogLikelihoodsByPartition(
+        [par] * nparts, [v] * nparts, [q * pr.B + v for q in range(nparts)], d1, d2,
+        [0] * nparts, [0] * nparts, [cum0 + q for q in range(nparts)], list(range(nparts)))
+    return res, inst.getSiteLogLikelihoods()

@@ -248,3 +248,39 @@ def test_partitions(b200, syn, oracle, monkeypatch, precision, S, C, variant):
         a, b = inst.getScaleFactors(s), oi.getScaleFactors(s)
         assert np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b))) <= big, s
     inst.finalize()
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+@pytest.mark.parametrize("S,derivs", [(4, False), (4, True), (20, True)])
+def test_edge_by_partition(b200, syn, oracle, precision, S, derivs):
+    """calculateEdgeLogLikelihoodsByPartition (per-partition launches over
+    pattern ranges) against the oracle: lnL and derivative sums per partition,
+    totals, site values; internal and tip children; d1 alone -> -7."""
+    from helpers import PRE_AUTO, SCALERS_LOG, edge_by_partition, partitioned_args, \
+        run_partitioned
+    pr = syn.make_problem(S=S, N=10, P=777, C=4, seed=110 + S, rescale=True)
+    args = partitioned_args(pr, 3)
+    pref, req = gpu_flags(precision, auto_transpose=True)
+    inst = b200.create(*args, preferenceFlags=pref, requirementFlags=req)
+    oi = oracle.OracleInstance(*args, flags=SCALERS_LOG)
+    got = []
+    for x in (inst, oi):
+        pr.load(x)
+        run_partitioned(x, pr, 3)
+        got.append([edge_by_partition(x, pr, 3, v, derivs) for v in (pr.N + 2, 1)])
+    tol = TOL[precision]
+    for (g, site_g), (o, site_o) in zip(*got):
+        assert g[0] == o[0] == 0
+        assert np.max(np.abs(g[1] - o[1]) / np.abs(o[1])) <= tol["lnl"]
+        assert rel(g[2], o[2]) <= tol["lnl"]
+        assert np.max(np.abs(site_g - site_o) / np.abs(site_o)) <= 100 * tol["lnl"]
+        if derivs:
+            for a, b in ((g[3], o[3]), (g[5], o[5])):
+                assert np.max(np.abs(a - b)) <= tol["grad"] * max(1.0, np.max(np.abs(b)))
+            assert abs(g[4] - o[4]) <= tol["grad"] * max(1.0, abs(o[4]))
+            assert abs(g[6] - o[6]) <= tol["grad"] * max(1.0, abs(o[6]))
+    code = inst.calculateEdgeLogLikelihoodsByPartition([pr.root], [1], [1], [3 * pr.B + 1],
+                                                       None, [0], [0], [-1], [0],
+                                                       check=False)[0]
+    assert code == -7
+    inst.finalize()

@@ -126,6 +126,45 @@ def test_partitions_match_reference(reflib, syn, oracle, S, rescale):
     ref.finalize()
 
 
+@pytest.mark.parametrize("S,derivs", [(4, False), (4, True), (20, False), (20, True)])
+def test_edge_by_partition_matches_reference(reflib, syn, oracle, S, derivs):
+    """calculateEdgeLogLikelihoodsByPartition (lnL, and with both derivative
+    matrices d1 and d2) per partition, for an internal and a tip child,
+    against the compiled reference; and a first derivative alone is
+    NO_IMPLEMENTATION in both."""
+    from helpers import edge_by_partition, partitioned_args, run_partitioned
+    pr = syn.make_problem(S=S, N=9, P=240, C=3, seed=70 + S, rescale=True)
+    args = partitioned_args(pr, 3)
+    ref = reflib.create(*args, preferenceFlags=(1 << 1) | (1 << 10) | (1 << 12),
+                        requirementFlags=(1 << 1) | (1 << 15))
+    oi = oracle.OracleInstance(*args, flags=1 << 10)
+    got = []
+    for x in (ref, oi):
+        pr.load(x)
+        run_partitioned(x, pr, 3)
+        # S != 4: the reference keeps only the last partition of pre-order
+        # buffers, so the parent side is the root's post-order partials there.
+        parent = None if S == 4 else pr.root
+        got.append([edge_by_partition(x, pr, 3, v, derivs, parent) for v in (pr.N + 2, 1)])
+    for (r, site_r), (o, site_o) in zip(*got):
+        assert r[0] == o[0] == 0
+        assert np.max(np.abs(r[1] - o[1]) / np.abs(o[1])) <= 1e-12
+        assert abs(r[2] - o[2]) <= 1e-12 * abs(o[2])
+        assert np.max(np.abs(site_r - site_o)) <= 1e-12 * np.max(np.abs(site_o))
+        if derivs:
+            for a, b in ((r[3], o[3]), (r[5], o[5])):
+                assert np.max(np.abs(a - b)) <= 1e-9 * max(1.0, np.max(np.abs(b)))
+            assert abs(r[4] - o[4]) <= 1e-9 * max(1.0, abs(o[4]))
+            assert abs(r[6] - o[6]) <= 1e-9 * max(1.0, abs(o[6]))
+    one = [3 * pr.B + 1]
+    r = ref.calculateEdgeLogLikelihoodsByPartition([pr.root], [1], [1], one, None, [0], [0],
+                                                   [-1], [0], check=False)
+    o = oi.calculateEdgeLogLikelihoodsByPartition([pr.root], [1], [1], one, None, [0], [0],
+                                                  [-1], [0])
+    assert r[0] == o[0] == -7
+    ref.finalize()
+
+
 def _with_missing_tip_states(pr, tips=(0, 1), every=7):
     """Some compact tip cells set to the missing state (S)."""
     for t in tips:
