@@ -154,10 +154,15 @@ int deriv_blocks(const Dims& d);
 // Final pass of an edge-derivative launch: sums[k] over nblk block partials.
 cudaError_t launch_deriv_final(const double* d_block, int nblk, int nb, double* d_sums,
                                cudaStream_t s);
+// The same with the sums to d_sums[0, nb) and the sums of squares to
+// d_sumsq[0, nb) (a slice of a longer list's output).
+cudaError_t launch_deriv_final_at(const double* d_block, int nblk, int nb, double* d_sums,
+                                  double* d_sumsq, cudaStream_t s);
 
 // Fused pre-order partials + edge derivatives (k_fused.cu): S = 4, C in
-// {1, 2, 4, 8}, at most 256 ops.  d_block needs 2 * nops * fused_blocks(d)
-// doubles; d_sums receives the nops sums, then the nops sums of squares.
+// {1, 2, 4, 8}, any list length (one launch per 256 ops).  d_block needs
+// 2 * nops * fused_blocks(d) doubles; d_sums receives the nops sums, then the
+// nops sums of squares.
 // Cross-product derivative sums (k_reduce.cu), S <= 64: d_out receives the
 // S * S sums over the nb branches (desc: post, pre, post_is_states used; fac
 // [nb][C] = w_c r_c t_b); d_block needs S * S * ceil(P / cross_tile_patterns)

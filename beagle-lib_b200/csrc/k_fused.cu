@@ -387,19 +387,24 @@ k_pre_deriv4_pairs(const __grid_constant__ FusedParams F, int nops, int P, int P
 
 int fused_blocks(const Dims& d) { return (d.Pp + kT4 / d.C - 1) / (kT4 / d.C) * (kT4 / 32); }
 
-bool fused_supported(const Dims& d, int nops) {
-    return d.S == 4 && d.Sg == 4 && (d.C == 1 || d.C == 2 || d.C == 4 || d.C == 8) &&
-           nops <= kFusedOps;
+bool fused_supported(const Dims& d, int /*nops*/) {
+    return d.S == 4 && d.Sg == 4 && (d.C == 1 || d.C == 2 || d.C == 4 || d.C == 8);
 }
 
+namespace {
+
+// One launch of the fused walk over at most kFusedOps ops; the sums of op k
+// go to d_sums[k] and d_sums[nsum + k] (nsum: the whole list's length).
 template <typename Real>
-cudaError_t launch_pre_deriv4(const PreDerivOp* h_ops, int nops, const Dims& d,
-                              const double* catw, const double* patw, int ls, double* d_block,
-                              double* d_sums, cudaStream_t s, int variant) {
-    if (nops == 0) return cudaSuccess;
-    if (!fused_supported(d, nops)) return cudaErrorInvalidValue;
-    static thread_local FusedParams prm;
+cudaError_t pre_deriv4_chunk(const PreDerivOp* h_ops, int nops, const Dims& d,
+                             const double* catw, const double* patw, int ls, double* d_block,
+                             double* d_sums, int nsum, cudaStream_t s, int variant) {
+    static thread_local FusedParams prm;   // copied into the launch
     std::memcpy(prm.op, h_ops, sizeof(PreDerivOp) * nops);
+    auto final_sums = [&](int nblk) {
+        if (nsum == nops) return launch_deriv_final(d_block, nblk, nops, d_sums, s);
+        return launch_deriv_final_at(d_block, nblk, nops, d_sums, d_sums + nsum, s);
+    };
     if (variant == 2) {
         // pairs-only lists, FP32, 2 patterns per thread
         constexpr int kAll = kPairFirst | kPairMats | kPairD;
@@ -415,7 +420,7 @@ cudaError_t launch_pre_deriv4(const PreDerivOp* h_ops, int nops, const Dims& d,
         }
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
-        return launch_deriv_final(d_block, grid2 * (kT4 / 32), nops, d_sums, s);
+        return final_sums(grid2 * (kT4 / 32));
     }
     const int grid = (d.Pp + kT4 / d.C - 1) / (kT4 / d.C);
     bool shared_d = true;             // one derivative matrix for every branch
@@ -443,7 +448,30 @@ cudaError_t launch_pre_deriv4(const PreDerivOp* h_ops, int nops, const Dims& d,
 #undef PD_
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    return launch_deriv_final(d_block, fused_blocks(d), nops, d_sums, s);
+    return final_sums(fused_blocks(d));
+}
+
+}  // namespace
+
+// Lists longer than kFusedOps run as consecutive launches, cut between
+// sibling pairs: a launch boundary orders every write of one launch before
+// every read of the next, so the cut changes only the launch count.  The
+// scratch d_block is reused by each launch in stream order.
+template <typename Real>
+cudaError_t launch_pre_deriv4(const PreDerivOp* h_ops, int nops, const Dims& d,
+                              const double* catw, const double* patw, int ls, double* d_block,
+                              double* d_sums, cudaStream_t s, int variant) {
+    if (nops == 0) return cudaSuccess;
+    if (!fused_supported(d, nops)) return cudaErrorInvalidValue;
+    for (int o0 = 0; o0 < nops;) {
+        int e = std::min(nops, o0 + kFusedOps);
+        if (e < nops && (h_ops[e - 1].kind & kPairFirst)) --e;   // keep the pair together
+        const cudaError_t r = pre_deriv4_chunk<Real>(h_ops + o0, e - o0, d, catw, patw, ls,
+                                                     d_block, d_sums + o0, nops, s, variant);
+        if (r != cudaSuccess) return r;
+        o0 = e;
+    }
+    return cudaSuccess;
 }
 
 template cudaError_t launch_pre_deriv4<float>(const PreDerivOp*, int, const Dims&, const double*,

@@ -616,8 +616,7 @@ k_walk4_batch(const WalkSeg* __restrict__ segs, int nseg) {
 template <typename Real>
 constexpr int kMinB6 = sizeof(Real) == 4 ? 6 : 1;
 //   7,8    1 or 2 patterns per thread with the op list passed by value as a
-//          kernel parameter (lists of up to kParamOps ops; otherwise the
-//          launch is refused and the tuner skips the variant).
+//          kernel parameter (one launch per kParamOps ops).
 //   9,10   7, 8 with results that later ops read kept in shared-memory slots;
 //   11-13  the list reordered by dependency level, groups of 2, 4 or 8
 //          independent ops loaded together (one pattern per thread).
@@ -669,22 +668,30 @@ cudaError_t run_pre4_ppt(const OpDesc* ops, int nops, const Dims& d, int ls, cud
     return cudaGetLastError();
 }
 
+// Lists longer than kParamOps run as consecutive launches of at most
+// kParamOps ops: a launch boundary orders every write of one launch before
+// every read of the next, so the cut changes only the launch count.
 template <typename Real, int C, int PPT>
 cudaError_t run_param4(const OpDesc* h_ops, int nops, const Dims& d, double* cum, int ls,
                        cudaStream_t s, bool ranged, bool pre) {
-    if (!h_ops || nops > kParamOps) return cudaErrorInvalidValue;
+    if (!h_ops) return cudaErrorInvalidValue;
     static thread_local OpParams prm;    // 28 KB: copied into the launch
-    std::memcpy(prm.op, h_ops, sizeof(OpDesc) * nops);
     const int ppb = kT4 / C * PPT;
     const int grid = (d.Pp + ppb - 1) / ppb;
-    if (pre) {
-        if (ranged) k_pre4c<Real, C, PPT, true><<<grid, kT4, 0, s>>>(prm, nops, d.Pp, ls);
-        else k_pre4c<Real, C, PPT, false><<<grid, kT4, 0, s>>>(prm, nops, d.Pp, ls);
-    } else {
-        if (ranged) k_post4c<Real, C, PPT, true><<<grid, kT4, 0, s>>>(prm, nops, d.Pp, cum, ls);
-        else k_post4c<Real, C, PPT, false><<<grid, kT4, 0, s>>>(prm, nops, d.Pp, cum, ls);
+    for (int o0 = 0; o0 < nops; o0 += kParamOps) {
+        const int n = std::min(kParamOps, nops - o0);
+        std::memcpy(prm.op, h_ops + o0, sizeof(OpDesc) * n);
+        if (pre) {
+            if (ranged) k_pre4c<Real, C, PPT, true><<<grid, kT4, 0, s>>>(prm, n, d.Pp, ls);
+            else k_pre4c<Real, C, PPT, false><<<grid, kT4, 0, s>>>(prm, n, d.Pp, ls);
+        } else {
+            if (ranged) k_post4c<Real, C, PPT, true><<<grid, kT4, 0, s>>>(prm, n, d.Pp, cum, ls);
+            else k_post4c<Real, C, PPT, false><<<grid, kT4, 0, s>>>(prm, n, d.Pp, cum, ls);
+        }
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
     }
-    return cudaGetLastError();
+    return cudaSuccess;
 }
 
 // Variants 9, 10: the slot walks.  Lists of partition ops carry no slots and

@@ -853,6 +853,13 @@ cudaError_t launch_deriv_final(const double* d_block, int nblk, int nb, double* 
     return cudaGetLastError();
 }
 
+cudaError_t launch_deriv_final_at(const double* d_block, int nblk, int nb, double* d_sums,
+                                  double* d_sumsq, cudaStream_t s) {
+    k_final_sum<<<nb, kRB, 0, s>>>(d_block, nblk, nb, d_sums);
+    k_final_sum<<<nb, kRB, 0, s>>>(d_block + (size_t)nb * nblk, nblk, nb, d_sumsq);
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------- cross products
 // beagleCalculateCrossProductDerivative (CPU/BeagleCPUImpl.hpp:1865-1937,
 // :2122-2237): for every listed branch b and pattern p,

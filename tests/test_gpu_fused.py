@@ -2,8 +2,8 @@
 derivatives of its branches in one kernel (4-state) against the two separate
 calls and the oracle, for every category count the fused walk takes, tips as
 states and as partials, with and without rescaling; lists without sibling
-pairs, lists too long for the fused walk, other state counts (both run as
-the separate calls), and a captured graph."""
+pairs, lists longer than one launch takes, other state counts (run as the
+separate calls), and a captured graph."""
 import numpy as np
 import pytest
 
@@ -76,17 +76,28 @@ def test_fused_without_sibling_pairs(b200, syn, precision):
     inst.finalize()
 
 
-@pytest.mark.parametrize("S,N", [(4, 150), (20, 12)])
-def test_fused_call_falls_back_to_separate_calls(b200, syn, oracle, S, N):
-    """More than 256 ops (N = 150: 298) or S != 4: the same call runs the two
-    separate calls, same results."""
-    pr = syn.make_problem(S=S, N=N, P=500, C=4, seed=7 + S, rescale=True)
-    inst = _pair(b200, pr, "double")
+@pytest.mark.parametrize("precision", ["double", "single"])
+@pytest.mark.parametrize("S,N", [(4, 150), (4, 300), (20, 12)])
+def test_fused_long_lists_and_other_state_counts(b200, syn, oracle, monkeypatch, precision, S,
+                                                 N):
+    """More than 256 ops (N = 150: 298; N = 300: 598): the fused walk (forced)
+    runs as consecutive launches cut between sibling pairs; S != 4 runs the
+    two separate calls.  Same results as the separate calls and the oracle."""
+    monkeypatch.setenv("BEAGLE_B200_FORCE_VARIANT", "-1,-1,-1,1")
+    pr = syn.make_problem(S=S, N=N, P=500, C=4, seed=7 + S + N, rescale=True)
+    inst = _pair(b200, pr, precision)
     tr = S > 4
     l0, g0 = pr.evaluate(inst, transposed_pre=tr)
     l1, sums = pr.evaluate(inst, transposed_pre=tr, fused=True)
+    g1 = pr.branch_gradient(sums)
+    tol = TOL[precision]
     assert rel(l1, l0) == 0.0
-    assert grad_err(pr.branch_gradient(sums), g0) <= 1e-12
+    assert grad_err(g1, g0) <= (1e-12 if precision == "double" else tol["grad"] * 1e-2)
+    if S == 4:
+        assert inst.tunedVariants()["fused"] == 1      # the fused walk ran
+    _, lo, go = run_oracle(oracle, pr)
+    assert rel(l1, lo) <= tol["lnl"]
+    assert grad_err(g1, go) <= tol["grad"]
     inst.finalize()
 
 

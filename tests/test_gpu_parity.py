@@ -192,6 +192,24 @@ def test_s4_kernel_variants(b200, syn, oracle, monkeypatch, precision, variant):
 
 
 @pytest.mark.parametrize("precision", ["double", "single"])
+@pytest.mark.parametrize("variant", [7, 8])
+def test_s4_parameter_walks_longer_than_one_launch(b200, syn, oracle, monkeypatch, precision,
+                                                   variant):
+    """The parameter-list walks take 256 ops a launch: a 300-taxon tree (299
+    post-order, 598 pre-order ops) runs as consecutive launches."""
+    monkeypatch.setenv("BEAGLE_B200_FORCE_VARIANT", str(variant))
+    pr = syn.make_problem(S=4, N=300, P=700, C=4, seed=77 + variant, rescale=True)
+    inst, lnl, g = run_b200(b200, pr, precision)
+    tv = inst.tunedVariants()
+    assert tv["post"] == variant and tv["pre"] == variant, tv
+    _, lo, go = run_oracle(oracle, pr)
+    tol = TOL[precision]
+    assert rel(lnl, lo) <= tol["lnl"], (lnl, lo)
+    assert grad_err(g, go) <= tol["grad"], grad_err(g, go)
+    inst.finalize()
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
 @pytest.mark.parametrize("variant", [9, 10, 12])
 def test_s4_slot_walks_more_live_values_than_slots(b200, syn, oracle, monkeypatch, precision,
                                                    variant):
