@@ -285,6 +285,15 @@ class Instance:
         return self._call("UpdateTransitionMatricesWithMultipleModels", _ptr(e), _ptr(r),
                           _ptr(p), _ptr(d1), _ptr(d2), _ptr(t), len(p))
 
+    def updateTransitionMatricesWithModelCategories(self, eig, probIdx, d1Idx, d2Idx,
+                                                    lengths):
+        e, p = _i32(eig), _i32(probIdx)
+        d1 = None if d1Idx is None else _i32(d1Idx)
+        d2 = None if d2Idx is None else _i32(d2Idx)
+        t = _f64(lengths)
+        return self._call("UpdateTransitionMatricesWithModelCategories", _ptr(e), _ptr(p),
+                          _ptr(d1), _ptr(d2), _ptr(t), len(p))
+
     def setTransitionMatrix(self, m, mat, padded=1.0):
         a = _f64(mat)
         return self._call("SetTransitionMatrix", m, _ptr(a), float(padded))

@@ -123,7 +123,7 @@ Instance::~Instance() {
         if (p) cudaFree(p);
     for (DevBuf* b : {&t_ops_post_, &t_ops_pre_, &t_jobs_, &t_deriv_, &t_idx_, &t_ptr_,
                       &scratch_, &out_, &site_d_, &t_dep_post_, &t_dep_pre_, &t_cross_,
-                      &d_maps_, &t_tc_maps_})
+                      &d_maps_, &t_tc_maps_, &t_cateig_})
         b->release();
     if (h_out_) cudaFreeHost(h_out_);
     if (h_tc_status_) cudaFreeHost(h_tc_status_);
@@ -703,9 +703,25 @@ int Instance::updateTransitionMatrices(int e, const int* prob, const int* d1, co
                                                       count);
 }
 
-int Instance::updateTransitionMatricesWithModelCategories(const int*, const int*, const int*,
-                                                          const int*, const double*, int) {
-    return kErrNoImpl;   // per-category eigen systems: not on this resource
+// CPU/EigenDecompositionCube.hpp:326-470: category c of every listed matrix
+// from eigen system eig[c], exp(lambda t) without a category rate.
+int Instance::updateTransitionMatricesWithModelCategories(const int* eig, const int* prob,
+                                                          const int* d1, const int* d2,
+                                                          const double* t, int count) {
+    if (count < 0 || (count > 0 && !eig)) return kErrRange;
+    if (count == 0) return kSuccess;
+    for (int c = 0; c < C_; ++c)
+        if (eig[c] < 0 || eig[c] >= neig_ || !eig_set_[eig[c]]) return kErrRange;
+    std::vector<MatJob> jobs;
+    const int rc = build_matrix_jobs(nullptr, nullptr, prob, d1, d2, t, count, jobs);
+    if (rc) return rc;
+    CK(t_cateig_.upload(eig, sizeof(int) * C_, stream_));
+    for (MatJob& j : jobs) {
+        j.cube = d_cube_;
+        j.evals = d_evals_;
+        j.cat_eig = (const int*)t_cateig_.ptr;
+    }
+    return run_matrix_jobs(jobs);
 }
 
 // ---------------------------------------------------------------- partials

@@ -192,6 +192,7 @@ private:
 
     DevBuf t_ops_post_, t_ops_pre_, t_jobs_, t_deriv_, t_idx_, t_ptr_, scratch_, out_, site_d_;
     DevBuf t_cross_;                       // cross-product factors w_c r_c t_b
+    DevBuf t_cateig_;                      // eigen system of each category (model categories)
     DevBuf d_maps_, t_tc_maps_;            // TMA tensor maps; per-op map table
     std::vector<TmaMap> h_maps_;
     std::vector<char> map_ok_;

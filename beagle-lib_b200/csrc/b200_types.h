@@ -116,6 +116,9 @@ struct MatJob {
     const double* evals;        // eigenvalues [S]
     const double* rates;        // category rates [C]
     double t;
+    // Model categories: category c uses eigen system cat_eig[c] (cube and
+    // evals are then the bases of all systems) with rate 1; null otherwise.
+    const int* cat_eig;
 };
 
 // ---- batched launches over several instances (b200_batch.cpp) ----------

@@ -3,7 +3,9 @@
 //
 // P[c][i][j] = max(0, sum_k cube[i][j][k] * exp(lambda_k * (t * r_c))),
 // dP = sum_k cube[i][j][k] * (lambda_k r_c) e^(..), d2P with (lambda_k r_c)^2,
-// following CPU/EigenDecompositionCube.hpp:105-322 (cube from :69-100).  The
+// following CPU/EigenDecompositionCube.hpp:105-322 (cube from :69-100); with
+// model categories, category c takes its own eigen system and r_c = 1
+// (:326-470).  The
 // missing-state column of the reference's padded layout is not stored here:
 // its value travels with each matrix (1 for P, 0 for derivatives).
 #include "b200_kernels.h"
@@ -25,9 +27,19 @@ k_update_matrices(const MatJob* __restrict__ jobs, int S, int Sg) {
     const MatJob jb = jobs[blockIdx.x];
     const int c = blockIdx.y;
     const int C = gridDim.y;
-    const double r = jb.rates[c];
+    const double* cube = jb.cube;
+    const double* evals = jb.evals;
+    double r;
+    if (jb.cat_eig) {           // CPU/EigenDecompositionCube.hpp:326-470: no category rate
+        const int e = jb.cat_eig[c];
+        cube += (size_t)e * S * S * S;
+        evals += (size_t)e * S;
+        r = 1.0;
+    } else {
+        r = jb.rates[c];
+    }
     for (int k = threadIdx.x; k < S; k += blockDim.x) {
-        const double lam = jb.evals[k];
+        const double lam = evals[k];
         const double v = exp(lam * (jb.t * r));
         const double sl = lam * r;
         ex[k] = v;
@@ -43,7 +55,7 @@ k_update_matrices(const MatJob* __restrict__ jobs, int S, int Sg) {
         const int i = idx / Sg, j = idx - (idx / Sg) * Sg;
         double s0 = 0.0, s1 = 0.0, s2 = 0.0;
         if (i < S && j < S) {
-            const double* cu = jb.cube + ((size_t)i * S + j) * S;
+            const double* cu = cube + ((size_t)i * S + j) * S;
             if (D1) {
                 for (int k = 0; k < S; ++k) {
                     const double cv = cu[k];

@@ -155,6 +155,33 @@ class OracleInstance:
                         self.matrices[d2Idx[u]][c, :, :self.S] = cube @ (sl * sl * ex)
                         self.matrices[d2Idx[u]][c, :, self.S] = 0.0
 
+    def updateTransitionMatricesWithMultipleModels(self, eig, rix, probIdx, d1Idx, d2Idx, t):
+        """CPU/BeagleCPUImpl.hpp:1256-1289: matrix u from eigen system eig[u]
+        and category rates rix[u] (updateTransitionMatrices one at a time)."""
+        for u in range(len(probIdx)):
+            self.updateTransitionMatrices(
+                eig[u], [probIdx[u]], None if d1Idx is None else [d1Idx[u]],
+                None if (d1Idx is None or d2Idx is None) else [d2Idx[u]], [t[u]],
+                rates=self.rates[rix[u]])
+
+    def updateTransitionMatricesWithModelCategories(self, eig, probIdx, d1Idx, d2Idx, t):
+        """CPU/EigenDecompositionCube.hpp:326-470: category c of every matrix
+        from eigen system eig[c], exp(lambda t) with no category rate; pad
+        column 1 for P, 0 for the derivatives."""
+        for u in range(len(probIdx)):
+            for c in range(self.C):
+                lam, cube = self.evals[eig[c]], self.cube[eig[c]]
+                ex = np.exp(lam * t[u])
+                P = cube @ ex
+                self.matrices[probIdx[u]][c, :, :self.S] = np.where(P > 0, P, 0.0)
+                self.matrices[probIdx[u]][c, :, self.S] = 1.0
+                if d1Idx is not None:
+                    self.matrices[d1Idx[u]][c, :, :self.S] = cube @ (lam * ex)
+                    self.matrices[d1Idx[u]][c, :, self.S] = 0.0
+                    if d2Idx is not None:
+                        self.matrices[d2Idx[u]][c, :, :self.S] = cube @ (lam * lam * ex)
+                        self.matrices[d2Idx[u]][c, :, self.S] = 0.0
+
     def setTransitionMatrix(self, m, mat, padded):
         """CPU/BeagleCPUImpl.hpp:1035-1054: [C][S][S] in, pad column = paddedValue."""
         self.matrices[m][:, :, :self.S] = np.asarray(mat, dtype=np.float64).reshape(

@@ -127,3 +127,49 @@ def edge_by_partition(inst, problem, nparts, v, derivs, parent=None):
         [par] * nparts, [v] * nparts, [q * pr.B + v for q in range(nparts)], d1, d2,
         [0] * nparts, [0] * nparts, [cum0 + q for q in range(nparts)], list(range(nparts)))
     return res, inst.getSiteLogLikelihoods()
+
+
+def model_variant_args(problem):
+    """create_args with 3 eigen systems (and rate sets) and 4 spare matrices
+    after the problem's own (derivatives of branches 0 and 1)."""
+    args = list(problem.create_args())
+    args[5] = 3
+    args[6] = max(args[6], problem.B + 5)
+    return args
+
+
+def run_model_variants(inst, problem, kind):
+    """The problem's tree (no rescaling) evaluated with matrices from
+    updateTransitionMatricesWithMultipleModels (kind "multiple": branch u from
+    eigen system u % 3 and rate set (u // 3) % 2) or
+    updateTransitionMatricesWithModelCategories ("categories": category c
+    from eigen system c % 3, no category rate), plus the first and second
+    derivative matrices of branches 0 and 1 (matrices B+1 .. B+4).  Eigen
+    systems 1, 2 and rate set 1 come from a fixed seed.  Returns (lnL, the
+    matrices 0, 1, 2, 3, B+1 .. B+4)."""
+    from importlib import import_module
+    syn = import_module("beagle-lib_b200").synthetic
+    pr = problem
+    rng = np.random.Generator(np.random.PCG64(4242))
+    for e in (1, 2):
+        Q, pi = syn.gtr_model(rng) if pr.S == 4 else syn.amino_model(rng, pr.S)
+        V, Vi, lam = syn.eigen_reversible(Q, pi)
+        inst.setEigenDecomposition(e, V.reshape(-1), Vi.reshape(-1), lam)
+    inst.setCategoryRatesWithIndex(1, np.linspace(0.3, 2.0, pr.C))
+    B = pr.B
+    probs = np.arange(B, dtype=np.int32)
+    d1, d2 = [B + 1, B + 2], [B + 3, B + 4]
+    if kind == "multiple":
+        eig = [u % 3 for u in range(B)]
+        rix = [(u // 3) % 2 for u in range(B)]
+        inst.updateTransitionMatricesWithMultipleModels(eig, rix, probs, None, None, pr.lengths)
+        inst.updateTransitionMatricesWithMultipleModels(eig[:2], rix[:2], [0, 1], d1, d2,
+                                                        pr.lengths[:2])
+    else:
+        eig = [c % 3 for c in range(pr.C)]
+        inst.updateTransitionMatricesWithModelCategories(eig, probs, None, None, pr.lengths)
+        inst.updateTransitionMatricesWithModelCategories(eig, [0, 1], d1, d2, pr.lengths[:2])
+    inst.updatePartials(pr.post_ops())
+    lnl = inst.calculateRootLogLikelihoods([pr.root], [0], [0], [-1])
+    mats = [inst.getTransitionMatrix(m) for m in (0, 1, 2, 3, B + 1, B + 2, B + 3, B + 4)]
+    return lnl, mats

@@ -302,3 +302,28 @@ def test_edge_by_partition(b200, syn, oracle, precision, S, derivs):
                                                        check=False)[0]
     assert code == -7
     inst.finalize()
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+@pytest.mark.parametrize("S,kind", [(4, "multiple"), (4, "categories"), (20, "multiple"),
+                                    (20, "categories"), (61, "categories")])
+def test_model_variant_matrices(b200, syn, oracle, precision, S, kind):
+    """updateTransitionMatricesWithMultipleModels / ...WithModelCategories on
+    the device (P, dP, d2P from the FP64 cubes of three eigen systems) and the
+    lnL of a tree built on them, against the oracle."""
+    from helpers import model_variant_args, run_model_variants
+    pr = syn.make_problem(S=S, N=8, P=300, C=4, seed=140 + S)
+    args = model_variant_args(pr)
+    pref, req = gpu_flags(precision)
+    inst = b200.create(*args, preferenceFlags=pref, requirementFlags=req)
+    oi = oracle.OracleInstance(*args, flags=SCALERS_LOG)
+    got = []
+    for x in (inst, oi):
+        pr.load(x)
+        got.append(run_model_variants(x, pr, kind))
+    (l1, m1), (l2, m2) = got
+    assert rel(l1, l2) <= TOL[precision]["lnl"]
+    mt = 1e-12 if precision == "double" else 1e-6
+    for a, b in zip(m1, m2):
+        assert np.max(np.abs(a - b)) <= mt * max(1.0, np.max(np.abs(b)))
+    inst.finalize()

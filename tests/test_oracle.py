@@ -165,6 +165,30 @@ def test_edge_by_partition_matches_reference(reflib, syn, oracle, S, derivs):
     ref.finalize()
 
 
+@pytest.mark.parametrize("S,kind", [(4, "multiple"), (4, "categories"), (20, "multiple"),
+                                    (20, "categories")])
+def test_model_variant_matrices_match_reference(reflib, syn, oracle, S, kind):
+    """updateTransitionMatricesWithMultipleModels (eigen system and rate set
+    per matrix) and updateTransitionMatricesWithModelCategories (eigen system
+    per category): P, dP, d2P and the tree's lnL against the compiled
+    reference."""
+    from helpers import model_variant_args, run_model_variants
+    pr = syn.make_problem(S=S, N=8, P=150, C=4, seed=130 + S)
+    args = model_variant_args(pr)
+    ref = reflib.create(*args, preferenceFlags=(1 << 1) | (1 << 10) | (1 << 12),
+                        requirementFlags=(1 << 1) | (1 << 15))
+    oi = oracle.OracleInstance(*args, flags=1 << 10)
+    got = []
+    for x in (ref, oi):
+        pr.load(x)
+        got.append(run_model_variants(x, pr, kind))
+    (l1, m1), (l2, m2) = got
+    assert abs(l1 - l2) <= 1e-12 * abs(l2)
+    for a, b in zip(m1, m2):
+        assert np.max(np.abs(a - b)) <= 1e-12 * max(1.0, np.max(np.abs(b)))
+    ref.finalize()
+
+
 def _with_missing_tip_states(pr, tips=(0, 1), every=7):
     """Some compact tip cells set to the missing state (S)."""
     for t in tips:
