@@ -9,7 +9,7 @@ relative lnL <= 1e-6 and gradient error <= 1e-4.
 import numpy as np
 import pytest
 
-from helpers import SCALERS_LOG, TOL, grad_err, rel, run_b200, run_oracle, gpu_flags
+from helpers import SCALERS_LOG, SCALERS_RAW, TOL, grad_err, rel, run_b200, run_oracle, gpu_flags
 
 pytestmark = pytest.mark.gpu
 
@@ -326,4 +326,47 @@ def test_model_variant_matrices(b200, syn, oracle, precision, S, kind):
     mt = 1e-12 if precision == "double" else 1e-6
     for a, b in zip(m1, m2):
         assert np.max(np.abs(a - b)) <= mt * max(1.0, np.max(np.abs(b)))
+    inst.finalize()
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+@pytest.mark.parametrize("S", [4, 20])
+def test_fixed_scaling_transpose_convolve_and_set_matrices(b200, syn, oracle, precision, S):
+    """Read-only (fixed) scale factors, matrix transposition and convolution,
+    matrices set by the caller (setTransitionMatrices, setDifferentialMatrix),
+    and a post-order op on a convolved matrix (an epoch boundary), against
+    the oracle."""
+    pr = syn.make_problem(S=S, N=10, P=190, C=2, seed=150 + S, rescale=True)
+    pref, req = gpu_flags(precision, log_scalers=False)
+    inst = b200.create(*pr.create_args(), preferenceFlags=pref, requirementFlags=req)
+    oi = oracle.OracleInstance(*pr.create_args(), flags=SCALERS_RAW)
+    rng = np.random.default_rng(S)
+    given = rng.random((2, pr.C * S * S))
+    res = []
+    for x in (inst, oi):
+        pr.load(x)
+        x.updateTransitionMatrices(0, np.arange(pr.B), None, None, pr.lengths)
+        x.updatePartials(pr.post_ops())
+        ops = pr.post_ops()
+        ops[:, 2] = ops[:, 1]      # read the factors just written ...
+        ops[:, 1] = -1             # ... without writing new ones
+        x.updatePartials(ops)
+        x.transposeTransitionMatrices([0, 1], [pr.B + 1, pr.B + 2])
+        x.convolveTransitionMatrices([0], [1], [pr.B + 3])
+        if x is inst:
+            x.setTransitionMatrices([pr.B + 4, pr.B + 5], given.reshape(-1), [1.0, 0.5])
+            x.setDifferentialMatrix(pr.B + 6, given[0])
+        else:
+            x.setTransitionMatrix(pr.B + 4, given[0], 1.0)
+            x.setTransitionMatrix(pr.B + 5, given[1], 0.5)
+            x.setTransitionMatrix(pr.B + 6, given[0], 0.0)
+        # one more op with a convolved matrix and a caller-set one
+        c1, c2 = (int(v) for v in pr.children[pr.root])
+        x.updatePartials(np.array([[pr.root, -1, -1, c1, pr.B + 3, c2, pr.B + 5]],
+                                  dtype=np.int32))
+        res.append([x.getPartials(pr.root)] +
+                   [x.getTransitionMatrix(m) for m in (pr.B + 1, pr.B + 3, pr.B + 5, pr.B + 6)])
+    tol = 1e-12 if precision == "double" else 2e-5
+    for a, b in zip(*res):
+        assert np.max(np.abs(a - b)) <= tol * max(1.0, np.max(np.abs(b)))
     inst.finalize()
