@@ -323,6 +323,13 @@ class OracleInstance:
             s = self.scale[i][rng]
             self.scale[cumulative][rng] += s if self.log_scalers else np.log(s)
 
+    def removeScaleFactorsByPartition(self, idxs, cumulative, part):
+        """CPU/BeagleCPUImpl.hpp:2850-2870."""
+        rng = self._range(part)
+        for i in idxs:
+            s = self.scale[i][rng]
+            self.scale[cumulative][rng] -= s if self.log_scalers else np.log(s)
+
     def calculateRootLogLikelihoodsByPartition(self, bufs, cws, sfs, cums, parts):
         """CPU/BeagleCPUImpl.hpp:2349-2388 (count 1): per partition i the lnL of
         root bufs[i] over partition parts[i]'s patterns; and their total."""

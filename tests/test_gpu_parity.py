@@ -370,3 +370,70 @@ def test_fixed_scaling_transpose_convolve_and_set_matrices(b200, syn, oracle, pr
     for a, b in zip(*res):
         assert np.max(np.abs(a - b)) <= tol * max(1.0, np.max(np.abs(b)))
     inst.finalize()
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+@pytest.mark.parametrize("log_scalers", [True, False])
+def test_scale_factor_calls_and_getters(b200, syn, oracle, precision, log_scalers):
+    """Accumulate / remove / copy / reset of scale factors, whole and by
+    partition, read back through root log-likelihoods and getScaleFactors;
+    setRootPrePartials; an edge lnL's getDerivatives and getSiteDerivatives;
+    waitForPartials -- against the oracle (RAW and LOG scalers)."""
+    pr = syn.make_problem(S=4, N=12, P=500, C=3, seed=170, rescale=True)
+    pref, req = gpu_flags(precision, log_scalers=log_scalers)
+    inst = b200.create(*pr.create_args(), preferenceFlags=pref, requirementFlags=req)
+    oi = oracle.OracleInstance(*pr.create_args(),
+                               flags=SCALERS_LOG if log_scalers else SCALERS_RAW)
+    nodes = list(range(pr.N - 1))
+    cum, cum2 = pr.cumulative, pr.N - 1          # N - 1: a free scale buffer here
+    parts = (np.arange(pr.P) >= 200).astype(np.int32)
+    res = []
+    for x in (inst, oi):
+        pr.load(x)
+        idx = np.arange(pr.B)
+        x.updateTransitionMatrices(0, idx, idx + pr.B + 1, None, pr.lengths)
+        x.updatePartials(pr.post_ops())
+        x.resetScaleFactors(cum)
+        x.accumulateScaleFactors(nodes, cum)
+        x.removeScaleFactors(nodes[:3], cum)
+        x.copyScaleFactors(cum2, cum)
+        x.accumulateScaleFactors(nodes[:3], cum)
+        out = [x.calculateRootLogLikelihoods([pr.root], [0], [0], [cum]),
+               x.calculateRootLogLikelihoods([pr.root], [0], [0], [cum2]),
+               x.getScaleFactors(cum2)]
+        x.setPatternPartitions(2, parts)
+        for q in (0, 1):
+            x.resetScaleFactorsByPartition(cum2, q)
+            x.accumulateScaleFactorsByPartition(nodes, cum2, q)
+        x.removeScaleFactorsByPartition(nodes[:4], cum2, 1)
+        byp, tot = x.calculateRootLogLikelihoodsByPartition([pr.root] * 2, [0, 0], [0, 0],
+                                                            [cum2, cum2], [0, 1])
+        out += [np.asarray(byp), tot, x.getScaleFactors(cum2)]
+        x.setRootPrePartials([pr.pre(pr.root)], [0])
+        out.append(x.getPartials(pr.pre(pr.root)))
+        v = pr.N + 1
+        x.updatePrePartials(pr.pre_ops())
+        code, lnl, d1, d2 = x.calculateEdgeLogLikelihoods(pr.pre(int(pr.parent[v])), v, v,
+                                                          v + pr.B + 1, None, 0, 0, -1)
+        out += [lnl, d1]
+        if x is inst:
+            assert x.waitForPartials([pr.root]) == 0
+            g1, _ = x.getDerivatives()
+            assert g1 == d1
+            site_d1, _ = x.getSiteDerivatives()
+        else:
+            site_d1 = x.site_d1
+        out.append(site_d1)
+        res.append(out)
+    tol = TOL[precision]
+    g, o = res
+    for k in (0, 1, 4, 7):
+        assert rel(g[k], o[k]) <= tol["lnl"], k
+    assert np.max(np.abs(g[3] - o[3]) / np.abs(o[3])) <= tol["lnl"]
+    for k in (2, 5):
+        assert np.max(np.abs(g[k] - o[k]) / np.maximum(1.0, np.abs(o[k]))) <= \
+            (1e-12 if precision == "double" else 1e-5), k
+    assert np.max(np.abs(g[6] - o[6])) <= 1e-15 * np.max(np.abs(o[6])) + 1e-7 * (precision != "double")
+    assert abs(g[8] - o[8]) <= tol["grad"] * max(1.0, abs(o[8]))
+    assert np.max(np.abs(g[9] - o[9])) <= tol["grad"] * max(1.0, np.max(np.abs(o[9])))
+    inst.finalize()
