@@ -33,9 +33,10 @@
 // MMAs (up to 4 CTAs per SM).
 //
 // TMEM: a CTA allocates 2 N (post / pre) or N (derivative) columns, rounded up
-// to a power of two.  The launch reserves enough shared memory per CTA that
-// the CTAs resident on one SM can never ask for more than the 512 columns an
-// SM has, so an allocation never waits on another cluster's CTA.
+// to a power of two.  Every launch reserves shared memory in proportion to
+// its columns (tc_smem), so the CTAs resident on one SM, from any mix of
+// these launches, can never ask for more than the 512 columns an SM has, and
+// an allocation never waits on another cluster's CTA.
 //
 // Every wait on an mbarrier is bounded (about a second); on time-out the
 // thread sets b200_tc_status, stops waiting for the rest of the launch, keeps
@@ -1053,12 +1054,16 @@ k_deriv_tc(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
     if (t < 32) tmem_dealloc(tmem, G::DCOLS);
 }
 
-// Dynamic shared memory of a launch: the struct, raised so that at most
-// 512 / cols CTAs fit on one SM (228 KB per SM, 1 KB reserved per CTA).
+// Dynamic shared memory of a launch: the struct, raised to the TMEM
+// columns' share of the SM's shared memory.  An SM has 228 KB (233,472 B)
+// and reserves 1 KB per CTA, so a CTA asking for `cols` of the 512 columns
+// takes at least 233,472 * cols / 512 = 456 * cols bytes in all.  Any set of
+// CTAs resident on one SM -- of one launch, or of several tensor-core
+// launches from different streams or instances -- then holds at most 512
+// columns, and a tcgen05.alloc never waits on a CTA that waits on it.
 size_t tc_smem(int cols) {
     const size_t need = sizeof(TcSmem) + 1024;   // + alignment slack
-    const int max_ctas = 512 / cols;
-    const size_t floor_bytes = 233472 / (max_ctas + 1) + 1;
+    const size_t floor_bytes = (size_t)456 * cols - 1024;
     return need > floor_bytes ? need : floor_bytes;
 }
 
