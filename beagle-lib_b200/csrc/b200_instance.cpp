@@ -476,14 +476,16 @@ int Instance::getPartials(int b, int scaleIndex, double* out) {
 int Instance::setEigenDecomposition(int e, const double* evec, const double* ivec,
                                     const double* evals) {
     if (e < 0 || e >= neig_ || !evec || !ivec || !evals) return kErrRange;
-    // Cube C[i][j][k] = V[i][k] * Vinv[k][j] (CPU/EigenDecompositionCube.hpp:69-100).
+    // Cube of the products V[i][k] * Vinv[k][j] (CPU/EigenDecompositionCube.hpp:69-100),
+    // stored [i][k][j] so that the threads forming consecutive entries (i, j)
+    // of a row read consecutive words for each k.
     const size_t S = S_;
     std::vector<double> cube(S * S * S);
     for (size_t i = 0; i < S; ++i)
-        for (size_t j = 0; j < S; ++j)
-            for (size_t k = 0; k < S; ++k) {
+        for (size_t k = 0; k < S; ++k)
+            for (size_t j = 0; j < S; ++j) {
                 const double vi = invevec_t_ ? ivec[k + j * S] : ivec[k * S + j];
-                cube[(i * S + j) * S + k] = evec[i * S + k] * vi;
+                cube[(i * S + k) * S + j] = evec[i * S + k] * vi;
             }
     CK(cudaMemcpyAsync(d_cube_ + (size_t)e * S * S * S, cube.data(), sizeof(double) * S * S * S,
                        cudaMemcpyHostToDevice, stream_));
@@ -1046,7 +1048,7 @@ int Instance::calculateRootLogLikelihoods(const int* bufs, const int* cw, const 
     if (w < 0 || w >= neig_ || !catw_set_[w] || f < 0 || f >= neig_ || !freqs_set_[f])
         return kErrRange;
     if (c != -1 && (c < 0 || c >= nscale_)) return kErrRange;
-    const int nblk = reduction_blocks(P_);
+    const int nblk = root_blocks(dims(), P_, true);
     CK(scratch_.reserve(sizeof(double) * nblk));
     CK(out_.reserve(sizeof(double) * 4));
     CK(LAUNCH(launch_root_lnl, partials_[b], d_catw_ + (size_t)w * C_, d_freqs_ + (size_t)f * S_,
@@ -1087,7 +1089,7 @@ int Instance::calculateRootLogLikelihoodsByPartition(const int* bufs, const int*
             return kErrRange;
         if (c != -1 && (c < 0 || c >= nscale_)) return kErrRange;
         if (q < 0 || q >= npart_defined) return kErrRange;
-        total_blocks += reduction_blocks(partition_start_[q + 1] - partition_start_[q]);
+        total_blocks += root_blocks(dims(), partition_start_[q + 1] - partition_start_[q], true);
     }
     CK(scratch_.reserve(sizeof(double) * std::max(total_blocks, 1)));
     CK(out_.reserve(sizeof(double) * std::max(nparts, 4)));
@@ -1098,7 +1100,7 @@ int Instance::calculateRootLogLikelihoodsByPartition(const int* bufs, const int*
         CK(LAUNCH(launch_root_lnl_range, partials_[b], d_catw_ + (size_t)w * C_,
                   d_freqs_ + (size_t)f * S_, c >= 0 ? scale(c) : nullptr, d_patw_, dims(), p0, p1,
                   d_site_, blocks, (double*)out_.ptr + i, stream_));
-        blocks += reduction_blocks(p1 - p0);
+        blocks += root_blocks(dims(), p1 - p0, true);
     }
     if ((size_t)nparts > h_out_n_) {
         cudaFreeHost(h_out_);

@@ -94,17 +94,23 @@ cudaError_t bulk_status_async(int* pinned_dst, cudaStream_t s);
 cudaError_t bulk_clear_status(cudaStream_t s);
 
 // Root log-likelihood: site lnL into d_site[P]; the weighted total into d_out[0].
+// d_block holds root_blocks(d, P, wide) doubles: `wide` spreads a pattern
+// over several lanes (root_lanes), otherwise one thread per pattern and
+// reduction_blocks(P) partial sums.
 template <typename Real>
 cudaError_t launch_root_lnl(const void* root, const double* catw, const double* freqs,
                             const double* cumulative, const double* patw, const Dims& d,
-                            double* d_site, double* d_block, double* d_out, cudaStream_t s);
+                            double* d_site, double* d_block, double* d_out, cudaStream_t s,
+                            bool wide = true);
 // The same over patterns [p_begin, p_end) (one partition); d_block holds
-// reduction_blocks(p_end - p_begin) doubles.
+// root_blocks(d, p_end - p_begin, wide) doubles.
 template <typename Real>
 cudaError_t launch_root_lnl_range(const void* root, const double* catw, const double* freqs,
                                   const double* cumulative, const double* patw, const Dims& d,
                                   int p_begin, int p_end, double* d_site, double* d_block,
-                                  double* d_out, cudaStream_t s);
+                                  double* d_out, cudaStream_t s, bool wide = true);
+int root_lanes(const Dims& d);
+int root_blocks(const Dims& d, int n, bool wide);
 
 // Edge log-likelihood (+ optional first / second derivative sums).
 template <typename Real>

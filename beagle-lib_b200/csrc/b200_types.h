@@ -112,7 +112,7 @@ struct MatJob {
     void* pt;                   // transposed images (written alongside)
     void* d1t;
     void* d2t;
-    const double* cube;         // eigen cube [S][S][S] (i, j, k)
+    const double* cube;         // eigen cube [S][S][S] (i, k, j)
     const double* evals;        // eigenvalues [S]
     const double* rates;        // category rates [C]
     double t;

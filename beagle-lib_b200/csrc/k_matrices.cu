@@ -14,9 +14,11 @@ namespace b200 {
 
 namespace {
 
-// One block per (job, category).  exp(.) is evaluated once per eigenvalue in
-// shared memory; each thread then forms entries (i, j) with a sequential FP64
-// sum over k (the reference's order), clamps P at 0 and rounds to Real.
+// One block per (job, category, slice of the entries).  exp(.) is evaluated
+// once per eigenvalue in shared memory; each thread then forms entries (i, j)
+// with a sequential FP64 sum over k (the reference's order), clamps P at 0
+// and rounds to Real.  The cube is stored [i][k][j], so for each k a warp's
+// consecutive entries of a row read consecutive words.
 template <typename Real>
 __global__ void __launch_bounds__(256)
 k_update_matrices(const MatJob* __restrict__ jobs, int S, int Sg) {
@@ -51,20 +53,21 @@ k_update_matrices(const MatJob* __restrict__ jobs, int S, int Sg) {
     Real* D1 = jb.d1 ? static_cast<Real*>(jb.d1) + (size_t)c * Sg * Sg : nullptr;
     Real* D2 = jb.d2 ? static_cast<Real*>(jb.d2) + (size_t)c * Sg * Sg : nullptr;
     (void)C;
-    for (int idx = threadIdx.x; idx < Sg * Sg; idx += blockDim.x) {
+    for (int idx = blockIdx.z * blockDim.x + threadIdx.x; idx < Sg * Sg;
+         idx += gridDim.z * blockDim.x) {
         const int i = idx / Sg, j = idx - (idx / Sg) * Sg;
         double s0 = 0.0, s1 = 0.0, s2 = 0.0;
         if (i < S && j < S) {
-            const double* cu = cube + ((size_t)i * S + j) * S;
+            const double* cu = cube + (size_t)i * S * S + j;
             if (D1) {
                 for (int k = 0; k < S; ++k) {
-                    const double cv = cu[k];
+                    const double cv = cu[(size_t)k * S];
                     s0 += cv * ex[k];
                     s1 += cv * e1[k];
                     s2 += cv * e2[k];
                 }
             } else {
-                for (int k = 0; k < S; ++k) s0 += cu[k] * ex[k];
+                for (int k = 0; k < S; ++k) s0 += cu[(size_t)k * S] * ex[k];
             }
             if (!(s0 > 0.0)) s0 = 0.0;
         }
@@ -113,7 +116,9 @@ template <typename Real>
 cudaError_t launch_update_matrices(const MatJob* d_jobs, int njobs, const Dims& d,
                                    cudaStream_t s) {
     if (njobs == 0) return cudaSuccess;
-    dim3 grid(njobs, d.C);
+    // Entries split over blocks in slices of 1024 (4 a thread): 4 slices for
+    // 61 states, one for 20 or fewer.
+    dim3 grid(njobs, d.C, (d.Sg * d.Sg + 1023) / 1024);
     k_update_matrices<Real><<<grid, 256, 3 * d.S * sizeof(double), s>>>(d_jobs, d.S, d.Sg);
     return cudaGetLastError();
 }

@@ -82,11 +82,11 @@ extern "C" int beagleB200RootLogLikelihoodsNoAlloc(
                 ? b200::launch_root_lnl<double>(rootPartials, categoryWeights, stateFrequencies,
                                                 cumulativeScaleFactors, patternWeights, d,
                                                 outSiteLogLikelihoods, scratch,
-                                                outSumLogLikelihood, s)
+                                                outSumLogLikelihood, s, false)
                 : b200::launch_root_lnl<float>(rootPartials, categoryWeights, stateFrequencies,
                                                cumulativeScaleFactors, patternWeights, d,
                                                outSiteLogLikelihoods, scratch,
-                                               outSumLogLikelihood, s);
+                                               outSumLogLikelihood, s, false);
     }
     cudaSetDevice(prev);
     if (e != cudaSuccess) {

@@ -75,17 +75,43 @@ __device__ __forceinline__ double integrate_site(const Real* x, const double* ca
     return sum;
 }
 
-template <typename Real>
+// Root log-likelihood of patterns [p_begin, p_end) with LP lanes per pattern
+// (a power of two <= 32).  A pattern's C x Sg values are C * Sg / 4
+// four-state groups, contiguous in the [pattern][category][state] layout;
+// lane l of the pattern's group adds freqs[i] * (w_c * x[c][i]) over groups
+// l, l + LP, ..., and a shuffle sum inside the lane group gives the site
+// value.  The reference sums over categories first
+// (CPU/BeagleCPUImpl.hpp:2646-2673); the terms are the same, added in
+// another order, so the site values agree to FP64 rounding.  Several lanes
+// per pattern keep a few thousand patterns of 61 states on every SM.
+template <typename Real, int LP>
 __global__ void __launch_bounds__(kRB)
 k_root_lnl(const Real* __restrict__ root, const double* __restrict__ catw,
            const double* __restrict__ freqs, const double* __restrict__ cum,
            const double* __restrict__ patw, int S, int Sg, int C, int p_begin, int p_end,
            double* site, double* block) {
     __shared__ double sh[kRB / 32];
-    const int p = p_begin + blockIdx.x * kRB + threadIdx.x;
-    double v = 0;
+    const int lane = threadIdx.x % LP;
+    const int p = p_begin + blockIdx.x * (kRB / LP) + threadIdx.x / LP;
+    const int G = Sg / 4;
+    double acc = 0;
     if (p < p_end) {
-        double l = log(integrate_site(root, catw, freqs, S, Sg, C, p));
+        const Real* xp = root + (size_t)p * C * Sg;
+        for (int t = lane; t < C * G; t += LP) {
+            const int c = t / G, i0 = 4 * (t - c * G);
+            Real x[4];
+            ld4(xp + 4 * (size_t)t, x);
+            const double w = catw[c];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (i0 + q < S) acc += freqs[i0 + q] * (w * (double)x[q]);
+        }
+    }
+#pragma unroll
+    for (int o = LP / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    double v = 0;
+    if (lane == 0 && p < p_end) {
+        double l = log(acc);
         if (cum) l += cum[p];
         site[p] = l;
         v = l * patw[p];
@@ -710,23 +736,50 @@ __global__ void k_accumulate_scale(double* cum, const double* __restrict__ pool,
 
 int reduction_blocks(int Pp) { return (Pp + kRB - 1) / kRB; }
 
+// Lanes per pattern of the root reduction: enough that a lane adds at most
+// 4 of a pattern's C * Sg / 4 four-state groups (1 for 4 states and up to 4
+// categories, 16 for 61 states and 4 categories), at most 32.
+int root_lanes(const Dims& d) {
+    const int items = d.C * (d.Sg / 4);
+    int lp = 1;
+    while (lp < 32 && lp * 4 < items) lp <<= 1;
+    return lp;
+}
+
+int root_blocks(const Dims& d, int n, bool wide) {
+    const int ppb = kRB / (wide ? root_lanes(d) : 1);
+    return (n + ppb - 1) / ppb;
+}
+
 template <typename Real>
 cudaError_t launch_root_lnl(const void* root, const double* catw, const double* freqs,
                             const double* cum, const double* patw, const Dims& d,
-                            double* d_site, double* d_block, double* d_out, cudaStream_t s) {
+                            double* d_site, double* d_block, double* d_out, cudaStream_t s,
+                            bool wide) {
     return launch_root_lnl_range<Real>(root, catw, freqs, cum, patw, d, 0, d.P, d_site, d_block,
-                                       d_out, s);
+                                       d_out, s, wide);
 }
 
 template <typename Real>
 cudaError_t launch_root_lnl_range(const void* root, const double* catw, const double* freqs,
                                   const double* cum, const double* patw, const Dims& d,
                                   int p_begin, int p_end, double* d_site, double* d_block,
-                                  double* d_out, cudaStream_t s) {
-    const int nblk = reduction_blocks(p_end - p_begin);
+                                  double* d_out, cudaStream_t s, bool wide) {
+    const int nblk = root_blocks(d, p_end - p_begin, wide);
     if (nblk == 0) return cudaMemsetAsync(d_out, 0, sizeof(double), s);
-    k_root_lnl<Real><<<nblk, kRB, 0, s>>>(static_cast<const Real*>(root), catw, freqs, cum, patw,
-                                          d.S, d.Sg, d.C, p_begin, p_end, d_site, d_block);
+    const Real* r = static_cast<const Real*>(root);
+#define RL_(LP)                                                                            \
+    k_root_lnl<Real, LP><<<nblk, kRB, 0, s>>>(r, catw, freqs, cum, patw, d.S, d.Sg, d.C,  \
+                                              p_begin, p_end, d_site, d_block)
+    switch (wide ? root_lanes(d) : 1) {
+        case 1: RL_(1); break;
+        case 2: RL_(2); break;
+        case 4: RL_(4); break;
+        case 8: RL_(8); break;
+        case 16: RL_(16); break;
+        default: RL_(32); break;
+    }
+#undef RL_
     k_final_sum<<<1, kRB, 0, s>>>(d_block, nblk, 1, d_out);
     return cudaGetLastError();
 }
@@ -1039,11 +1092,11 @@ template cudaError_t launch_root_batch<double>(const RootSeg*, int, int, cudaStr
 #define INST(R)                                                                                  \
     template cudaError_t launch_root_lnl<R>(const void*, const double*, const double*,           \
                                             const double*, const double*, const Dims&, double*,  \
-                                            double*, double*, cudaStream_t);                     \
+                                            double*, double*, cudaStream_t, bool);               \
     template cudaError_t launch_root_lnl_range<R>(const void*, const double*, const double*,     \
                                                   const double*, const double*, const Dims&,     \
                                                   int, int, double*, double*, double*,           \
-                                                  cudaStream_t);                                 \
+                                                  cudaStream_t, bool);                           \
     template cudaError_t launch_edge_lnl<R>(const void*, const void*, int, const void*, double,  \
                                             const void*, double, const void*, double,            \
                                             const double*, const double*, const double*,         \
