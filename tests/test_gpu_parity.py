@@ -437,3 +437,29 @@ def test_scale_factor_calls_and_getters(b200, syn, oracle, precision, log_scaler
     assert abs(g[8] - o[8]) <= tol["grad"] * max(1.0, abs(o[8]))
     assert np.max(np.abs(g[9] - o[9])) <= tol["grad"] * max(1.0, np.max(np.abs(o[9])))
     inst.finalize()
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+@pytest.mark.parametrize("S", [4, 20])
+def test_repeat_determinism_and_site_derivative_sums(b200, syn, precision, S):
+    """Repeated evaluations give the same lnL and gradient bits (fixed-order
+    reductions, the autotuner's pick cached after the first call), as the
+    reference's rep-to-rep check expects (synthetictest.cpp:2436-2447); and
+    the per-site derivatives, weighted and summed, give the reduced sums
+    (hmctest.cpp:716-722), as do the sums of squares."""
+    pr = syn.make_problem(S=S, N=18, P=1500, C=4, seed=180 + S, rescale=True)
+    inst, l0, g0 = run_b200(b200, pr, precision)
+    for _ in range(3):
+        l1, g1 = pr.evaluate(inst, transposed_pre=S > 4)
+        assert l1 == l0
+        assert np.array_equal(g1, g0)
+    nonroot = np.arange(pr.B, dtype=np.int32)
+    site, sums, sumsq = inst.calculateEdgeDerivatives(
+        nonroot, nonroot + pr.pre(0), np.full(pr.B, pr.B, dtype=np.int32), [0])
+    # the per-site output may come from another derivative kernel shape than
+    # the sums-only call: equal to FP64 reduction rounding
+    assert np.max(np.abs(sums - g0)) <= 1e-12 * np.max(np.abs(g0))
+    w = pr.patw
+    assert np.max(np.abs(site @ w - sums)) <= 1e-10 * np.max(np.abs(sums))
+    assert np.max(np.abs((site * site) @ w - sumsq)) <= 1e-9 * np.max(np.abs(sumsq))
+    inst.finalize()
