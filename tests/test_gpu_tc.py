@@ -58,3 +58,25 @@ def test_fp32_generic_auto_transpose_and_raw_scalers(b200, syn, oracle, monkeypa
     _, lo, go = run_oracle(oracle, pr)
     assert rel(l1, lo) <= 1e-6 and rel(l2, lo) <= 1e-6
     assert grad_err(g1, go) <= 1e-4 and grad_err(g2, go) <= 1e-4
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("S", [20, 61])
+def test_fp32_generic_missing_compact_states(b200, syn, oracle, monkeypatch, variant, S):
+    """Compact tips with missing states (state S, an all-ones partial): the
+    walks read the matrix's pad value for them (post-order child and
+    pre-order sibling), and the derivative an all-ones row; every kernel
+    family against the oracle, whose missing state is an all-ones partial
+    on every path."""
+    monkeypatch.setenv("BEAGLE_B200_FORCE_VARIANT", str(variant))
+    pr = syn.make_problem(S=S, N=12, P=650, C=4, seed=600 + S, rescale=True)
+    rng = np.random.default_rng(S)
+    pr.tip_states[rng.random(pr.tip_states.shape) < 0.08] = S
+    inst, lnl, g = run_b200(b200, pr, "single")
+    oi, lo, go = run_oracle(oracle, pr)
+    assert rel(lnl, lo) <= TOL["single"]["lnl"], (lnl, lo)
+    assert grad_err(g, go) <= TOL["single"]["grad"], grad_err(g, go)
+    for v in [pr.root, pr.pre(0), pr.pre(pr.N)]:
+        a, b = inst.getPartials(v), oi.getPartials(v)
+        assert np.max(np.abs(a - b)) <= 2e-4 * np.max(np.abs(b)), v
+    inst.finalize()
