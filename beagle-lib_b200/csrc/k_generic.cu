@@ -438,20 +438,29 @@ k_deriv_x(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
                 v2 += dv * dv * patw[p];
             }
         }
-        // block reduction (fixed order) of v1, v2 over the CTA's threads
+        // block reduction (fixed order) of v1, v2 over the CTA's threads: the
+        // 32 threads of warp 0 each add a strided subset, then a shuffle tree
+        // (NT need not be a multiple of 32)
         double* red = s_nd;   // reuse: [NT][2]
         red[tid * 2 + 0] = v1;
         red[tid * 2 + 1] = v2;
         __syncthreads();
-        if (tid == 0) {
+        if (tid < 32) {
             double t1 = 0, t2 = 0;
-            for (int k = 0; k < G::NT; ++k) {
+            for (int k = tid; k < G::NT; k += 32) {
                 t1 += red[k * 2 + 0];
                 t2 += red[k * 2 + 1];
             }
-            const int nb = gridDim.x / (C * ntiles);
-            block[(size_t)b * ntiles + tile] = t1;
-            block[(size_t)(nb + b) * ntiles + tile] = t2;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                t1 += __shfl_xor_sync(0xffffffffu, t1, o);
+                t2 += __shfl_xor_sync(0xffffffffu, t2, o);
+            }
+            if (tid == 0) {
+                const int nb = gridDim.x / (C * ntiles);
+                block[(size_t)b * ntiles + tile] = t1;
+                block[(size_t)(nb + b) * ntiles + tile] = t2;
+            }
         }
     }
     cluster.sync();   // remote reads done before any CTA of the cluster exits

@@ -1034,12 +1034,21 @@ k_deriv_tc(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
             v1 = dv * patw[p];
             v2 = dv * dv * patw[p];
         }
-        sm.red[t * 2 + 0] = v1;
-        sm.red[t * 2 + 1] = v2;
+        // The tile's sums: a shuffle tree inside each warp, then the warps in
+        // order (a fixed order, so the result is the same every run).
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+            v2 += __shfl_xor_sync(0xffffffffu, v2, o);
+        }
+        if ((t & 31) == 0) {
+            sm.red[(t >> 5) * 2 + 0] = v1;
+            sm.red[(t >> 5) * 2 + 1] = v2;
+        }
         __syncthreads();
         if (t == 0) {
             double t1 = 0, t2 = 0;
-            for (int k = 0; k < kTT; ++k) {
+            for (int k = 0; k < kTT / 32; ++k) {
                 t1 += sm.red[k * 2 + 0];
                 t2 += sm.red[k * 2 + 1];
             }
