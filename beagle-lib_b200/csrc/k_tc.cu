@@ -426,10 +426,19 @@ __device__ __forceinline__ void finish_row(SM& sm, const OpDesc& op, float out[N
     const bool mine = p >= op.p_begin && p < op.p_end;   // the op's pattern range
     if (op.cum) cum = op.cum;
     if (op.scale_write) {
-        float m = 0.f;
+        // maximum over states < S as a pairwise tree (6 dependent steps for
+        // 64 states instead of a 64-step chain); the same value.  Step h
+        // folds entry i + h into entry i for every i that is a multiple of
+        // 2h, which covers any NP (48 included), not only powers of two.
+        float mx[NP];
 #pragma unroll
-        for (int i = 0; i < NP; ++i)
-            if (i < S) m = out[i] > m ? out[i] : m;
+        for (int i = 0; i < NP; ++i) mx[i] = (i < S && out[i] > 0.f) ? out[i] : 0.f;
+#pragma unroll
+        for (int h = 1; h < NP; h <<= 1)
+#pragma unroll
+            for (int i = 0; i + h < NP; i += 2 * h)
+                mx[i] = mx[i + h] > mx[i] ? mx[i + h] : mx[i];
+        float m = mx[0];
         float* sx = sm.smax + (nresc & 1) * kTM;
         ++nresc;
         sx[threadIdx.x] = m;
@@ -1000,7 +1009,9 @@ k_deriv_tc(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
     }
     pipe_drain(sm, pp);
     tc_fence_after();
-    float n = 0.f, d = 0.f;
+    // four interleaved partial sums each for n and d (shorter dependent
+    // chains), added pairwise at the end
+    float nq[4] = {0.f, 0.f, 0.f, 0.f}, dq[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
     for (int j = 0; j < NP / 16; ++j) {
         float y[16];
@@ -1011,10 +1022,12 @@ k_deriv_tc(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
             const int i = 16 * j + q;
             if (i >= S) continue;
             const float x = states ? ((s < 0 || s >= S || s == i) ? 1.f : 0.f) : xv[i];
-            n += pv[i] * y[q];
-            d += pv[i] * x;
+            nq[q & 3] += pv[i] * y[q];
+            dq[q & 3] += pv[i] * x;
         }
     }
+    const float n = (nq[0] + nq[1]) + (nq[2] + nq[3]);
+    const float d = (dq[0] + dq[1]) + (dq[2] + dq[3]);
     const double w = catw[c];
     sm.nd[t * 2 + 0] = w * (double)n;
     sm.nd[t * 2 + 1] = w * (double)d;
