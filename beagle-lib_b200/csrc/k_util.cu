@@ -1,20 +1,25 @@
 // Small device utilities used by the host instance: filling pre-order root
 // partials with the state frequencies.
 #include "b200_kernels.h"
+#include "b200_vec.cuh"
 
 namespace b200 {
 
 namespace {
 
 // dest[p][c][i] = freqs[i] for i < S, 0 for the padded states
-// (CPU/BeagleCPUImpl.hpp:621-676, beagleSetRootPrePartials).
+// (CPU/BeagleCPUImpl.hpp:621-676, beagleSetRootPrePartials).  One thread per
+// four-state group (Sg is a multiple of 4): one vector store each.
 template <typename Real>
 __global__ void k_fill_root(Real* dest, const double* __restrict__ freqs, int S, int Sg,
-                            size_t n) {
-    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= n) return;
-    const int i = (int)(idx % Sg);
-    dest[idx] = (i < S) ? (Real)freqs[i] : Real(0);
+                            size_t ngroups) {
+    const size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ngroups) return;
+    const int i0 = 4 * (int)(g % (size_t)(Sg / 4));
+    Real v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] = (i0 + q < S) ? (Real)freqs[i0 + q] : Real(0);
+    st4(dest + 4 * g, v);
 }
 
 // The same for several instances (b200_batch.cpp): 256 values per CTA.
@@ -52,9 +57,9 @@ template cudaError_t launch_fill_batch<double>(const FillSeg*, int, int, cudaStr
 
 template <typename Real>
 cudaError_t launch_fill_root(void* dest, const double* freqs, const Dims& d, cudaStream_t s) {
-    const size_t n = (size_t)d.Pp * d.C * d.Sg;
-    k_fill_root<Real><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(static_cast<Real*>(dest), freqs,
-                                                                   d.S, d.Sg, n);
+    const size_t ng = (size_t)d.Pp * d.C * d.Sg / 4;
+    k_fill_root<Real><<<(unsigned)((ng + 255) / 256), 256, 0, s>>>(static_cast<Real*>(dest), freqs,
+                                                                    d.S, d.Sg, ng);
     return cudaGetLastError();
 }
 
