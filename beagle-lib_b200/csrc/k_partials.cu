@@ -72,9 +72,10 @@ k_pre4(const OpDesc* __restrict__ ops, int nops, int Pp, int log_scalers) {
 }
 
 // The same walks with the op list passed by value as a kernel parameter (at
-// most kParamOps ops, CUDA 12.1+ on sm_70+): descriptor fields are then
-// warp-uniform constant-bank reads instead of shared-memory loads, and no
-// staging or barriers are needed between ops.
+// most kParamOps ops a launch, CUDA 12.1+ on sm_70+; longer lists run as
+// consecutive launches, run_param4): descriptor fields are then warp-uniform
+// constant-bank reads instead of shared-memory loads, and no staging or
+// barriers are needed between ops.
 constexpr int kParamOps = 256;
 struct OpParams {
     OpDesc op[kParamOps];
