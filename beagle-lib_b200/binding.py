@@ -65,6 +65,7 @@ _SIGS = {
     "CalculateRootLogLikelihoodsByPartition": [_i, _p, _p, _p, _p, _p, _i, _i, _p, _p],
     "CalculateEdgeDerivatives": [_i, _p, _p, _p, _p, _i, _p, _p, _p],
     "UpdatePrePartialsWithDerivatives": [_i, _p, _i, _p, _p, _p, _p, _p],
+    "UpdatePartialsWithRootLogLikelihood": [_i, _p, _i, _i, _i, _i, _i, _p],
     "GetTunedVariants": [_i, _p],
     "CalculateCrossProductDerivative": [_i, _p, _p, _p, _p, _p, _i, _p, _p],
     "CalculateEdgeLogLikelihoods": [_i, _p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p, _p],
@@ -427,6 +428,17 @@ class Instance:
         o = np.zeros(4, dtype=np.int32)
         self._call("GetTunedVariants", _ptr(o))
         return dict(zip(("post", "pre", "deriv", "fused"), (int(x) for x in o)))
+
+    def updatePartialsWithRootLogLikelihood(self, ops, cumulative, root, cw, sf, check=True):
+        """beagleB200UpdatePartialsWithRootLogLikelihood: updatePartials, the
+        cumulative scale factors of the list (reset first; -1 for none) and the
+        root lnL in one call.  Returns lnL (ASYNCH instances: delivered by
+        getLogLikelihood, the return value is then not meaningful)."""
+        o = _i32(ops).reshape(-1)
+        out = np.zeros(1)
+        code = self._call("UpdatePartialsWithRootLogLikelihood", _ptr(o), o.size // 7,
+                          cumulative, root, cw, sf, _ptr(out), check=check)
+        return (code, float(out[0])) if not check else float(out[0])
 
     def updatePrePartialsWithDerivatives(self, ops, post, dmat, cw, check=True):
         """Pre-order ops, then the edge derivative of each op's node from

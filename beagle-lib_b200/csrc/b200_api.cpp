@@ -354,6 +354,13 @@ int beagleB200CalculateEdgeDerivatives(int h, const int* post, const int* pre, c
         return in->calculateEdgeDerivatives(post, pre, d, w, n, o, s, sq);
     });
 }
+int beagleB200UpdatePartialsWithRootLogLikelihood(int h, const int* ops, int count,
+                                                   int cumulative, int root, int cw, int sf,
+                                                   double* out) {
+    return call(h, [&](b200::Instance* in) {
+        return in->updatePartialsWithRootLogLikelihood(ops, count, cumulative, root, cw, sf, out);
+    });
+}
 int beagleB200UpdatePrePartialsWithDerivatives(int h, const int* ops, int count,
                                                const int* post, const int* dmat, const int* cw,
                                                double* s, double* sq) {

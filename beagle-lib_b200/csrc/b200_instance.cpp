@@ -1054,9 +1054,13 @@ int Instance::calculateRootLogLikelihoods(const int* bufs, const int* cw, const 
     CK(LAUNCH(launch_root_lnl, partials_[b], d_catw_ + (size_t)w * C_, d_freqs_ + (size_t)f * S_,
               c >= 0 ? scale(c) : nullptr, d_patw_, dims(), d_site_, (double*)scratch_.ptr,
               (double*)out_.ptr, stream_));
+    return deliver_lnl(out);
+}
+
+// The lnL in out_[0] to the caller: now, or (ASYNCH, GPU/BeagleGPUImpl.hpp:
+// 3398-3407) at beagleGetLogLikelihood, with nothing written to *out here.
+int Instance::deliver_lnl(double* out) {
     if (async_) {
-        // ASYNCH (GPU/BeagleGPUImpl.hpp:3398-3407): the value is delivered by
-        // beagleGetLogLikelihood; nothing is written to *out here.
         double* slot = stage(1);
         if (!slot) return kErrOOM;
         CK(cudaMemcpyAsync(slot, out_.ptr, sizeof(double), cudaMemcpyDeviceToHost, stream_));
@@ -1069,6 +1073,53 @@ int Instance::calculateRootLogLikelihoods(const int* bufs, const int* cw, const 
     *out = h_out_[0];
     last_lnl_ = *out;
     return std::isnan(*out) ? kErrFP : kSuccess;
+}
+
+// updatePartials(ops, count, NONE); with a cumulative buffer, resetScaleFactors
+// on it and accumulateScaleFactors of the list's scale buffers; then
+// calculateRootLogLikelihoods of `root` -- in one launch (k_post4root) when
+// the root is the last op's destination and the list is a plain S = 4 one
+// of at most 256 ops, otherwise as those calls.
+int Instance::updatePartialsWithRootLogLikelihood(const int* ops, int count, int cumulative,
+                                                  int root, int cw, int sf, double* out) {
+    if (!out) return kErrRange;
+    if (cumulative != -1 && (cumulative < 0 || cumulative >= nscale_)) return kErrRange;
+    std::vector<int> written;
+    for (int k = 0; ops && k < count; ++k)
+        if (ops[(size_t)k * 7 + 1] >= 0) written.push_back(ops[(size_t)k * 7 + 1]);
+    auto separate = [&]() -> int {
+        int rc = updatePartials(ops, count, -1);
+        if (rc) return rc;
+        if (cumulative >= 0) {
+            rc = resetScaleFactors(cumulative, -1);
+            if (rc) return rc;
+            rc = accumulateScaleFactors(written.data(), (int)written.size(), cumulative, 1.0, -1);
+            if (rc) return rc;
+        }
+        const int* cp = cumulative >= 0 ? &cumulative : nullptr;
+        return calculateRootLogLikelihoods(&root, &cw, &sf, cp, 1, out);
+    };
+    bool fused = S_ == 4 && (C_ == 1 || C_ == 2 || C_ == 4 || C_ == 8) && count >= 1 &&
+                 count <= 256 && ops && ops[(size_t)(count - 1) * 7] == root;
+    for (int k = 0; fused && k < (int)written.size(); ++k)
+        if (written[k] == cumulative) fused = false;   // the list rewrites the cumulative buffer
+    if (!fused) return separate();
+    if (!buf_ok(root) || cw < 0 || cw >= neig_ || !catw_set_[cw] || sf < 0 || sf >= neig_ ||
+        !freqs_set_[sf])
+        return kErrRange;
+    std::vector<OpDesc> tab;
+    std::vector<uint8_t> dep;
+    bool idempotent = true, has_op_cum = false;
+    int rc = build_walk(ops, count, 7, false, tab, dep, idempotent, has_op_cum);
+    if (rc) return rc;
+    const Dims dm = dims();
+    CK(scratch_.reserve(sizeof(double) * post_root_blocks(dm)));
+    CK(out_.reserve(sizeof(double) * 4));
+    CK(LAUNCH(launch_post4_root, tab.data(), count, dm, cumulative >= 0 ? scale(cumulative) : nullptr,
+              (int)log_scalers_, d_catw_ + (size_t)cw * C_, d_freqs_ + (size_t)sf * S_, d_patw_,
+              d_site_, (double*)scratch_.ptr, (double*)out_.ptr, stream_));
+    picked_[kTuneWalkPost] = 7;
+    return deliver_lnl(out);
 }
 
 // CPU/BeagleCPUImpl.hpp:2349-2388: one root per partition (count == 1), the

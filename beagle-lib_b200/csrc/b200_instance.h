@@ -103,6 +103,10 @@ public:
     int calculateCrossProducts(const int* post, const int* pre, const int* rates_idx,
                                const int* cw, const double* lengths, int count,
                                double* outSum);
+    // updatePartials + (reset and accumulate of the list's scale factors) +
+    // calculateRootLogLikelihoods in one walk (S = 4) or as those calls.
+    int updatePartialsWithRootLogLikelihood(const int* ops, int count, int cumulative, int root,
+                                            int cw, int sf, double* out);
     // updatePrePartials + calculateEdgeDerivatives (sums only) in one walk.
     int updatePrePartialsWithDerivatives(const int* ops, int count, const int* post,
                                          const int* dmat, const int* cw, double* outSum,
@@ -190,6 +194,7 @@ private:
     std::vector<double> h_patw_;
     std::vector<int> partition_start_;     // pattern partitions (empty = one partition)
 
+    int deliver_lnl(double* out);
     DevBuf t_ops_post_, t_ops_pre_, t_jobs_, t_deriv_, t_idx_, t_ptr_, scratch_, out_, site_d_;
     DevBuf t_cross_;                       // cross-product factors w_c r_c t_b
     DevBuf t_cateig_;                      // eigen system of each category (model categories)

@@ -160,6 +160,20 @@ int deriv_blocks(const Dims& d);
 // Final pass of an edge-derivative launch: sums[k] over nblk block partials.
 cudaError_t launch_deriv_final(const double* d_block, int nblk, int nb, double* d_sums,
                                cudaStream_t s);
+// out[k] = the fixed-order sum of block[k * nblk .. k * nblk + nblk), k < nout.
+cudaError_t launch_final_sum(const double* d_block, int nblk, int nout, double* d_out,
+                             cudaStream_t s);
+// Post-order walk + scale accumulation + root lnL in one launch (S = 4, C in
+// {1, 2, 4, 8}, at most 256 ops, the root the last op's destination; k_partials.cu):
+// the list's scale buffers as updatePartials writes them; with `cum`, its
+// patterns' sums of log scale factors (reset, then accumulated); site lnL into
+// `site`, the weighted total into out[0].  `block` holds post_root_blocks(d)
+// doubles.
+int post_root_blocks(const Dims& d);
+template <typename Real>
+cudaError_t launch_post4_root(const OpDesc* h_ops, int nops, const Dims& d, double* cum, int ls,
+                              const double* catw, const double* freqs, const double* patw,
+                              double* site, double* block, double* out, cudaStream_t s);
 // The same with the sums to d_sums[0, nb) and the sums of squares to
 // d_sumsq[0, nb) (a slice of a longer list's output).
 cudaError_t launch_deriv_final_at(const double* d_block, int nblk, int nb, double* d_sums,

@@ -10,13 +10,15 @@ namespace b200 {
 namespace {
 
 // Store the scale factor of one pattern (see the file comment): its log
-// (scale_log) stored and accumulated in FP64.
+// (scale_log) stored and accumulated in FP64, into the cumulative buffer
+// `cum` and/or the caller's register `acc` when given.
 template <typename Real>
 __device__ __forceinline__ void store_scale(Real m, double* scale_write, double* cum, int p,
-                                            int log_scalers) {
+                                            int log_scalers, double* acc = nullptr) {
     const double lm = scale_log(m);
     scale_write[p] = log_scalers ? lm : (double)m;
     if (cum) cum[p] += lm;
+    if (acc) *acc += lm;
 }
 
 // ------------------------------------------------------------ S = 4 kernels
@@ -71,7 +73,7 @@ __device__ __forceinline__ Real group_max(Real v) {
 // buffer); whole-instance lists skip those checks.
 template <typename Real, int C, bool RANGED = true>
 __device__ __forceinline__ void finish4c(const OpDesc& op, Real out[4], int p, bool valid, int c,
-                                         double* cum, int log_scalers) {
+                                         double* cum, int log_scalers, double* acc = nullptr) {
     if (RANGED) {
         valid = valid && p >= op.p_begin && p < op.p_end;
         if (op.cum) cum = op.cum;
@@ -85,7 +87,7 @@ __device__ __forceinline__ void finish4c(const OpDesc& op, Real out[4], int p, b
         const Real inv = Real(1) / m;
 #pragma unroll
         for (int i = 0; i < 4; ++i) out[i] *= inv;
-        if (valid && c == 0) store_scale(m, op.scale_write, cum, p, log_scalers);
+        if (valid && c == 0) store_scale(m, op.scale_write, cum, p, log_scalers, acc);
     } else if (op.scale_read) {
         const Real inv = Real(1) / (Real)op.scale_read[p];
 #pragma unroll
@@ -95,9 +97,11 @@ __device__ __forceinline__ void finish4c(const OpDesc& op, Real out[4], int p, b
 }
 
 // One post-order op for this thread's PPT patterns (p0 + k pstride).
+// acc (PPT = 1): a register that also receives this pattern's log scale
+// factor (lane c == 0).
 template <typename Real, int C, int PPT, bool RANGED>
 __device__ __forceinline__ void post4_op(const OpDesc& op, int c, int p0, int pstride, int Pp,
-                                         double* cum, int log_scalers) {
+                                         double* cum, int log_scalers, double* acc = nullptr) {
     const bool st1 = op.kind & kX1States, st2 = op.kind & kX2States;
     const Real* M1 = static_cast<const Real*>(op.m1) + c * 16;
     const Real* M2 = static_cast<const Real*>(op.m2) + c * 16;
@@ -119,7 +123,7 @@ __device__ __forceinline__ void post4_op(const OpDesc& op, int c, int p0, int ps
         operand4c(M2, st2, s2[k], x2[k], (Real)op.pad2, y2);
 #pragma unroll
         for (int i = 0; i < 4; ++i) y1[i] *= y2[i];
-        finish4c<Real, C, RANGED>(op, y1, min(p, Pp - 1), p < Pp, c, cum, log_scalers);
+        finish4c<Real, C, RANGED>(op, y1, min(p, Pp - 1), p < Pp, c, cum, log_scalers, acc);
     }
 }
 

@@ -103,6 +103,48 @@ k_pre4c(const __grid_constant__ OpParams P, int nops, int Pp, int log_scalers) {
         pre4_op<Real, C, PPT, RANGED>(P.op[o], c, p0, pstride, Pp, log_scalers);
 }
 
+// The parameter-list post-order walk with the scale accumulation and the
+// root log-likelihood fused (beagleB200UpdatePartialsWithRootLogLikelihood):
+// each thread keeps its pattern's sum of log scale factors in a register
+// (CPU/BeagleCPUImpl.hpp:2763-2801, as resetScaleFactors + accumulateScale-
+// Factors over the list's scale buffers), re-reads the root row it wrote in
+// the last op, and forms the site lnL of CPU/BeagleCPUImpl.hpp:2630-2691:
+// log sum_c w_c sum_i pi_i root[c][i] + cumulative, the category sum by
+// shuffles inside the pattern's lane group.  Per-warp weighted sums go to
+// `block` for the final fixed-order sum.
+template <typename Real, int C>
+__global__ void __launch_bounds__(kT4)
+k_post4root(const __grid_constant__ OpParams P, int nops, int Pp, int Pn, double* cum,
+            int log_scalers, const double* __restrict__ catw, const double* __restrict__ freqs,
+            const double* __restrict__ patw, double* site, double* block) {
+    const int c = threadIdx.x % C;
+    const int p0 = blockIdx.x * (kT4 / C) + threadIdx.x / C;
+    double acc = 0;
+    for (int o = 0; o < nops; ++o)
+        post4_op<Real, C, 1, false>(P.op[o], c, p0, 0, Pp, nullptr, log_scalers, &acc);
+    Real x[4];
+    ld4(static_cast<const Real*>(P.op[nops - 1].dest) + ((size_t)min(p0, Pp - 1) * C + c) * 4, x);
+    const double w = catw[c];
+    double l = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) l += freqs[i] * (w * (double)x[i]);
+#pragma unroll
+    for (int o = 1; o < C; o <<= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+    double v = 0;
+    if (c == 0 && p0 < Pn) {
+        double sl = log(l);
+        if (cum) {
+            sl += acc;
+            cum[p0] = acc;
+        }
+        site[p0] = sl;
+        v = sl * patw[p0];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) block[(size_t)blockIdx.x * (kT4 / 32) + threadIdx.x / 32] = v;
+}
+
 // -------------------------------------------------- S = 4, slot walks
 // The parameter-list walks with a per-thread cache in shared memory: an op
 // whose result a later op of the list reads also writes it to a slot, and the
@@ -857,6 +899,40 @@ cudaError_t run_pre4(const OpDesc* ops, const OpDesc* h_ops, int nops, const Dim
 }
 
 }  // namespace
+
+int post_root_blocks(const Dims& d) { return (d.Pp + kT4 / d.C - 1) / (kT4 / d.C) * (kT4 / 32); }
+
+template <typename Real>
+cudaError_t launch_post4_root(const OpDesc* h_ops, int nops, const Dims& d, double* cum, int ls,
+                              const double* catw, const double* freqs, const double* patw,
+                              double* site, double* block, double* out, cudaStream_t s) {
+    if (d.S != 4 || (d.C != 1 && d.C != 2 && d.C != 4 && d.C != 8) || nops < 1 ||
+        nops > kParamOps || !h_ops)
+        return cudaErrorInvalidValue;
+    static thread_local OpParams prm;
+    std::memcpy(prm.op, h_ops, sizeof(OpDesc) * nops);
+    const int grid = (d.Pp + kT4 / d.C - 1) / (kT4 / d.C);
+#define PR_(CC)                                                                            \
+    k_post4root<Real, CC><<<grid, kT4, 0, s>>>(prm, nops, d.Pp, d.P, cum, ls, catw, freqs,  \
+                                               patw, site, block)
+    switch (d.C) {
+        case 1: PR_(1); break;
+        case 2: PR_(2); break;
+        case 4: PR_(4); break;
+        default: PR_(8); break;
+    }
+#undef PR_
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_final_sum(block, post_root_blocks(d), 1, out, s);
+}
+
+template cudaError_t launch_post4_root<float>(const OpDesc*, int, const Dims&, double*, int,
+                                              const double*, const double*, const double*,
+                                              double*, double*, double*, cudaStream_t);
+template cudaError_t launch_post4_root<double>(const OpDesc*, int, const Dims&, double*, int,
+                                               const double*, const double*, const double*,
+                                               double*, double*, double*, cudaStream_t);
 
 int s4_walk_variants(int C) { return (32 % C == 0) ? 14 : 1; }
 

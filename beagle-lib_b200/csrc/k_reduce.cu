@@ -906,6 +906,12 @@ cudaError_t launch_deriv_final(const double* d_block, int nblk, int nb, double* 
     return cudaGetLastError();
 }
 
+cudaError_t launch_final_sum(const double* d_block, int nblk, int nout, double* d_out,
+                             cudaStream_t s) {
+    k_final_sum<<<nout, kRB, 0, s>>>(d_block, nblk, nout, d_out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_deriv_final_at(const double* d_block, int nblk, int nb, double* d_sums,
                                   double* d_sumsq, cudaStream_t s) {
     k_final_sum<<<nb, kRB, 0, s>>>(d_block, nblk, nb, d_sums);

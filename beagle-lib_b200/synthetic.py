@@ -316,9 +316,11 @@ class Problem:
         updateTransitionMatrices (all B branches) -> updatePartials (N-1 ops) ->
         scale accumulation -> root lnL -> root pre-partials -> updatePrePartials
         (B ops) -> calculateEdgeDerivatives (all B branches, sums only).
-        With ``fused`` the last two are one beagleB200UpdatePrePartialsWithDerivatives
-        call, whose sums come in pre-order op order (``fused_branches()``
-        names the branch of each; ``branch_gradient`` reorders them).
+        With ``fused`` the post-order walk, scale accumulation and root lnL are
+        one beagleB200UpdatePartialsWithRootLogLikelihood call, and the last
+        two are one beagleB200UpdatePrePartialsWithDerivatives call, whose
+        sums come in pre-order op order (``fused_branches()`` names the branch
+        of each; ``branch_gradient`` reorders them).
         Returns (lnL, gradient[B] or None)."""
         mark = mark or (lambda name: None)
         t = self.lengths if lengths is None else lengths
@@ -340,16 +342,22 @@ class Problem:
 
     def _after_matrices(self, inst, gradient, transposed_pre, mark, fused=False):
         idx = np.arange(self.B, dtype=np.int32)
-        inst.updatePartials(self.post_ops(), OP_NONE)
-        mark("post")
-        cum = OP_NONE
-        if self.rescale:
-            cum = self.cumulative
-            inst.resetScaleFactors(cum)
-            inst.accumulateScaleFactors(np.arange(self.N - 1, dtype=np.int32), cum)
-        mark("scale")
-        lnl = inst.calculateRootLogLikelihoods([self.root], [0], [0], [cum])
-        mark("root")
+        cum = self.cumulative if self.rescale else OP_NONE
+        if fused:
+            # post-order walk, cumulative scale factors and root lnL in one call
+            lnl = inst.updatePartialsWithRootLogLikelihood(self.post_ops(), cum, self.root, 0, 0)
+            mark("post")
+            mark("scale")
+            mark("root")
+        else:
+            inst.updatePartials(self.post_ops(), OP_NONE)
+            mark("post")
+            if self.rescale:
+                inst.resetScaleFactors(cum)
+                inst.accumulateScaleFactors(np.arange(self.N - 1, dtype=np.int32), cum)
+            mark("scale")
+            lnl = inst.calculateRootLogLikelihoods([self.root], [0], [0], [cum])
+            mark("root")
         if not gradient:
             return lnl, None
         if transposed_pre:
@@ -426,7 +434,13 @@ class Problem:
             else:
                 fused += L + rd(a[5]) + rd(a[0] - self.pre(0)) + L + sc
                 k += 1
-        return dict(matrices=mats, post=post, pre=pre, deriv=deriv, fused=fused)
+        # scale accumulation: reset (write), N - 1 buffers and the cumulative
+        # buffer read, the cumulative buffer written; root lnL: the root row,
+        # cumulative and pattern weights read, site values written
+        scale = (self.N + 2) * 8 * self.P if self.rescale else 0
+        root = L + (8 * self.P if self.rescale else 0) + 16 * self.P
+        return dict(matrices=mats, post=post, pre=pre, deriv=deriv, fused=fused, scale=scale,
+                    root=root)
 
 
 def make_problem(S, N, P, C, seed, mean_length=0.1, ambiguous=0.0, rescale=False,

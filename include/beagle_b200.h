@@ -277,12 +277,30 @@ int beagleB200CalculateEdgeDerivatives(int instance, const int* postBufferIndice
                                        const int* categoryWeightsIndices, int count,
                                        double* outDerivatives, double* outSumDerivatives,
                                        double* outSumSquaredDerivatives);
+/* Extension, no beagle.h counterpart: beagleUpdatePartials(operations, count,
+ * BEAGLE_OP_NONE); then, when cumulativeScaleIndex is not BEAGLE_OP_NONE,
+ * beagleResetScaleFactors(cumulativeScaleIndex) and
+ * beagleAccumulateScaleFactors of every scale buffer the operations write;
+ * then beagleCalculateRootLogLikelihoods(rootBufferIndex,
+ * categoryWeightsIndex, stateFrequenciesIndex, cumulativeScaleIndex).  Same
+ * results (to FP64 rounding of the sums) and error codes as those calls, and
+ * the same ASYNCH delivery as beagleCalculateRootLogLikelihoods.  For 4-state
+ * instances with 1, 2, 4 or 8 categories, at most 256 operations and the
+ * root the last operation's destination, one kernel walks the list, keeps
+ * each pattern's log scale factors in a register and forms the site
+ * log-likelihood from the root row it has just written; other lists run as
+ * the separate calls. */
+int beagleB200UpdatePartialsWithRootLogLikelihood(int instance, const int* operations, int count,
+                                                  int cumulativeScaleIndex, int rootBufferIndex,
+                                                  int categoryWeightsIndex,
+                                                  int stateFrequenciesIndex,
+                                                  double* outSumLogLikelihood);
 /* Extension, no beagle.h counterpart: beagleUpdatePrePartials(operations,
  * count, BEAGLE_OP_NONE) followed by beagleCalculateEdgeDerivatives over
  * (postBufferIndices[k], destination of operation k, derivativeMatrixIndices[k])
  * for k < count, sums only.  Same results and error codes as those two calls.
- * For 4-state instances with 1, 2, 4 or 8 categories and at most 256
- * operations, one kernel walks the list and forms each branch's derivative
+ * For 4-state instances with 1, 2, 4 or 8 categories, one kernel walks the
+ * list (one launch per 256 operations) and forms each branch's derivative
  * from the pre-order row it has just computed (sibling pairs share their
  * loads); other shapes run the two calls. */
 int beagleB200UpdatePrePartialsWithDerivatives(int instance, const int* operations, int count,

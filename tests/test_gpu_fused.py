@@ -38,7 +38,9 @@ def test_fused_matches_separate_calls_and_oracle(b200, syn, oracle, monkeypatch,
     g1 = pr.branch_gradient(sums)
     _, lo, go = run_oracle(oracle, pr)
     tol = TOL[precision]
-    assert rel(l1, l0) == 0.0
+    # the fused post-order call: its FP64 sums run in another order, and the
+    # separate call's autotuner may have picked another post-order kernel shape
+    assert rel(l1, l0) <= (1e-13 if precision == "double" else 1e-6)
     assert grad_err(g1, g0) <= tol["grad"] * 1e-2, grad_err(g1, g0)
     assert grad_err(g1, go) <= tol["grad"], grad_err(g1, go)
     # the pre-order buffers the fused walk wrote are the separate walk's, up to
@@ -91,7 +93,9 @@ def test_fused_long_lists_and_other_state_counts(b200, syn, oracle, monkeypatch,
     l1, sums = pr.evaluate(inst, transposed_pre=tr, fused=True)
     g1 = pr.branch_gradient(sums)
     tol = TOL[precision]
-    assert rel(l1, l0) == 0.0
+    # the fused post-order call: its FP64 sums run in another order, and the
+    # separate call's autotuner may have picked another post-order kernel shape
+    assert rel(l1, l0) <= (1e-13 if precision == "double" else 1e-6)
     assert grad_err(g1, g0) <= (1e-12 if precision == "double" else tol["grad"] * 1e-2)
     if S == 4:
         assert inst.tunedVariants()["fused"] == 1      # the fused walk ran
