@@ -23,6 +23,7 @@ _p = ctypes.c_void_p
 # name -> argtypes (all return int unless listed in _RESTYPES)
 _SIGS = {
     "BeginCapture": [_i], "EndCapture": [_i, _p], "LaunchGraph": [_i, _i],
+    "LaunchGraphWithLengths": [_i, _i, _p, _i],
     "FinalizeInstance": [_i],
     "Finalize": [],
     "SetCPUThreadCount": [_i, _i],
@@ -208,6 +209,12 @@ class Instance:
 
     def launchGraph(self, graph):
         return self._call("LaunchGraph", graph)
+
+    def launchGraphWithLengths(self, graph, lengths):
+        """Launch a graph whose captured matrix updates read new branch
+        lengths (all of them, in capture order)."""
+        t = _f64(lengths)
+        return self._call("LaunchGraphWithLengths", graph, _ptr(t), t.size)
 
     def finalize(self):
         if self.h is not None and self.h >= 0:

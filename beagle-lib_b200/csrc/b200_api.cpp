@@ -567,4 +567,10 @@ int beagleB200LaunchGraph(int instance, int graph) {
     return call(instance, [&](b200::Instance* in) { return in->launchGraph(graph); });
 }
 
+int beagleB200LaunchGraphWithLengths(int instance, int graph, const double* lengths, int count) {
+    return call(instance, [&](b200::Instance* in) {
+        return in->launchGraphWithLengths(graph, lengths, count);
+    });
+}
+
 }  // extern "C"

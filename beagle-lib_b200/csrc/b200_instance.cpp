@@ -257,6 +257,10 @@ int Instance::beginCapture() {
     int rc = sync();
     if (rc) return rc;
     cap_ = GraphRec{};
+    // room for the branch lengths of the captured matrix updates (allocated
+    // before the capture starts: the graph keeps the address)
+    cap_.len_cap = 4 * nmat_;
+    CK(cudaMalloc(&cap_.d_len, sizeof(double) * cap_.len_cap));
     CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed));
     capturing_ = true;
     t_capture_pinned = &cap_.pinned;
@@ -276,10 +280,30 @@ int Instance::endCapture(int* graph) {
         free_graph(cap_);
         return kErrGeneral;
     }
+    // the capture-time lengths, which launchGraph replays until
+    // launchGraphWithLengths replaces them
+    if (!cap_.len.empty())
+        CK(cudaMemcpy(cap_.d_len, cap_.len.data(), sizeof(double) * cap_.len.size(),
+                      cudaMemcpyHostToDevice));
     graphs_.push_back(cap_);
     cap_ = GraphRec{};
     *graph = (int)graphs_.size() - 1;
     return kSuccess;
+}
+
+// Replace the branch lengths of the graph's captured transition-matrix
+// updates (count = all of them, in capture order), then launch it.  The copy
+// is stream-ordered before the launch, and a pageable source is read before
+// this call returns.
+int Instance::launchGraphWithLengths(int graph, const double* lengths, int count) {
+    if (capturing_ || graph < 0 || graph >= (int)graphs_.size() || !graphs_[graph].exec)
+        return kErrRange;
+    const GraphRec& g = graphs_[graph];
+    if (!g.len_all || count != (int)g.len.size() || (count > 0 && !lengths)) return kErrRange;
+    if (count > 0)
+        CK(cudaMemcpyAsync(g.d_len, lengths, sizeof(double) * count, cudaMemcpyHostToDevice,
+                           stream_));
+    return launchGraph(graph);
 }
 
 // Launch a captured graph on the instance's stream; its deferred results
@@ -297,6 +321,7 @@ void Instance::free_graph(GraphRec& g) {
     if (g.exec) cudaGraphExecDestroy(g.exec);
     if (g.graph) cudaGraphDestroy(g.graph);
     for (void* p : g.pinned) cudaFreeHost(p);
+    if (g.d_len) cudaFree(g.d_len);
     g = GraphRec{};
 }
 
@@ -664,7 +689,23 @@ int Instance::updateTransitionMatricesWithMultipleModels(const int* eig, const i
     std::vector<MatJob> jobs;
     const int rc = build_matrix_jobs(eig, rix, prob, d1, d2, t, count, jobs);
     if (rc) return rc;
+    capture_lengths(jobs);
     return run_matrix_jobs(jobs);
+}
+
+// While capturing, the jobs read their branch lengths from the graph's
+// lengths buffer (capture order), so that launchGraphWithLengths can replace
+// them; past the buffer's room they keep the captured values.
+void Instance::capture_lengths(std::vector<MatJob>& jobs) {
+    if (!capturing_ || !cap_.d_len) return;
+    if ((int)(cap_.len.size() + jobs.size()) > cap_.len_cap) {
+        cap_.len_all = false;
+        return;
+    }
+    for (MatJob& j : jobs) {
+        j.tlen = cap_.d_len + cap_.len.size();
+        cap_.len.push_back(j.t);
+    }
 }
 
 // Validate and resolve transition-matrix requests into device jobs.
@@ -691,6 +732,7 @@ int Instance::build_matrix_jobs(const int* eig, const int* rix, const int* prob,
         j.evals = d_evals_ + (size_t)e * S_;
         j.rates = d_rates_ + (size_t)r * C_;
         j.t = t[u];
+        j.tlen = nullptr;
         mat_pad_[prob[u]] = 1.0;
         if (j.d1) mat_pad_[d1[u]] = 0.0;
         if (j.d2) mat_pad_[d2[u]] = 0.0;
@@ -723,6 +765,7 @@ int Instance::updateTransitionMatricesWithModelCategories(const int* eig, const 
         j.evals = d_evals_;
         j.cat_eig = (const int*)t_cateig_.ptr;
     }
+    capture_lengths(jobs);
     return run_matrix_jobs(jobs);
 }
 

@@ -131,6 +131,7 @@ public:
     int beginCapture();
     int endCapture(int* graph);
     int launchGraph(int graph);
+    int launchGraphWithLengths(int graph, const double* lengths, int count);
 
     // For batched calls (b200_batch.cpp).
     int use_stream(cudaStream_t s);
@@ -194,6 +195,7 @@ private:
     std::vector<double> h_patw_;
     std::vector<int> partition_start_;     // pattern partitions (empty = one partition)
 
+    void capture_lengths(std::vector<MatJob>& jobs);
     int deliver_lnl(double* out);
     DevBuf t_ops_post_, t_ops_pre_, t_jobs_, t_deriv_, t_idx_, t_ptr_, scratch_, out_, site_d_;
     DevBuf t_cross_;                       // cross-product factors w_c r_c t_b
@@ -224,6 +226,13 @@ private:
         cudaGraphExec_t exec = nullptr;
         std::vector<Pending> deliveries;
         std::vector<void*> pinned;
+        // branch lengths of the captured transition-matrix updates, read by
+        // the graph from d_len (capture order); replaced by
+        // launchGraphWithLengths
+        double* d_len = nullptr;
+        int len_cap = 0;
+        std::vector<double> len;
+        bool len_all = true;      // every captured update reads d_len
     };
     std::vector<GraphRec> graphs_;
     GraphRec cap_;

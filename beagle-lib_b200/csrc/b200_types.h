@@ -119,6 +119,9 @@ struct MatJob {
     // Model categories: category c uses eigen system cat_eig[c] (cube and
     // evals are then the bases of all systems) with rate 1; null otherwise.
     const int* cat_eig;
+    // Branch length read on the device at run time instead of `t` (a CUDA
+    // graph's lengths buffer); null otherwise.
+    const double* tlen;
 };
 
 // ---- batched launches over several instances (b200_batch.cpp) ----------

@@ -40,9 +40,10 @@ k_update_matrices(const MatJob* __restrict__ jobs, int S, int Sg) {
     } else {
         r = jb.rates[c];
     }
+    const double t = jb.tlen ? *jb.tlen : jb.t;
     for (int k = threadIdx.x; k < S; k += blockDim.x) {
         const double lam = evals[k];
-        const double v = exp(lam * (jb.t * r));
+        const double v = exp(lam * (t * r));
         const double sl = lam * r;
         ex[k] = v;
         e1[k] = sl * v;

@@ -394,6 +394,28 @@ class Problem:
             graph = inst.endCapture()
         return graph, grad
 
+    def capture_step(self, inst, transposed_pre=False, fused=False):
+        """Record one whole evaluation, the transition matrices included, as a
+        CUDA graph of an ASYNCH instance; the graph reads the branch lengths
+        on the device, and ``evaluate_graph_step`` replaces them per launch.
+        Returns (graph, gradient array the graph fills)."""
+        self.evaluate(inst, transposed_pre=transposed_pre, fused=fused)
+        inst.getLogLikelihood()
+        inst.beginCapture()
+        try:
+            _, grad = self.evaluate(inst, transposed_pre=transposed_pre, fused=fused)
+        finally:
+            graph = inst.endCapture()
+        return graph, grad
+
+    def evaluate_graph_step(self, inst, graph, grad, lengths=None):
+        """One evaluation through a graph from ``capture_step``: the new branch
+        lengths and the graph in one call, then lnL and the gradient."""
+        t = self.lengths if lengths is None else lengths
+        inst.launchGraphWithLengths(graph, t)
+        lnl = inst.getLogLikelihood()            # waits; delivers the gradient too
+        return lnl, grad
+
     def evaluate_graph(self, inst, graph, grad, lengths=None):
         """One evaluation through a captured graph: new transition matrices
         (outside the graph), the graph, then lnL and the gradient."""

@@ -9,8 +9,10 @@ rescaling, FP64 P(t) and reductions):
     -> scale accumulation -> root lnL -> root pre-partials
     -> updatePrePartials (254 ops) -> calculateEdgeDerivatives (254 branches)
 
-through libbeagle_b200.so's C ABI, the last two as one
-beagleB200UpdatePrePartialsWithDerivatives call.  ``value`` queues K evaluations on the
+through libbeagle_b200.so's C ABI: the post-order walk, scale accumulation and
+root lnL as one beagleB200UpdatePartialsWithRootLogLikelihood call, and the
+last two as one beagleB200UpdatePrePartialsWithDerivatives call.  ``value``
+queues K evaluations on the
 instance's stream (ASYNCH instance, inputs resident) and times them with CUDA
 events on that stream; ``e2e`` runs K evaluations that each copy new branch
 lengths in and read lnL and the gradient back (host round trip per step).
@@ -318,22 +320,24 @@ def timed_e2e(torch, inst, pr, steps):
 
 
 def timed_e2e_graph(torch, inst, pr, steps):
-    """As timed_e2e, with everything after the transition matrices replayed
-    from a CUDA graph captured once (beagleB200BeginCapture / LaunchGraph)."""
+    """As timed_e2e, with the whole step -- transition matrices included --
+    replayed from a CUDA graph captured once: per step the new branch lengths
+    and the graph go in one beagleB200LaunchGraphWithLengths call, then one
+    wait for lnL and the gradient."""
     stream = torch.cuda.ExternalStream(inst.cudaStream())
-    graph, grad = pr.capture(inst, transposed_pre=pr.S > 4, fused=True)
+    graph, grad = pr.capture_step(inst, transposed_pre=pr.S > 4, fused=True)
     rng = np.random.default_rng(7)
     lengths = torch.empty(pr.B, dtype=torch.float64).pin_memory()
     host = lengths.numpy()
     for _ in range(2):
-        pr.evaluate_graph(inst, graph, grad)
+        pr.evaluate_graph_step(inst, graph, grad)
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
     inst.waitForPartials([])
     start.record(stream)
     for _ in range(steps):
         host[:] = pr.lengths * (1.0 + 1e-3 * rng.standard_normal(pr.B))
-        pr.evaluate_graph(inst, graph, grad, lengths=host)
+        pr.evaluate_graph_step(inst, graph, grad, lengths=host)
         pr.branch_gradient(grad)
     end.record(stream)
     end.synchronize()
@@ -510,7 +514,8 @@ def run_b200_arm(args):
             "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "e2e_graph": {"value": e2e_graph_value, "unit": "evals/s",
-                          "how": "same steps, post-matrix work replayed from a CUDA graph"},
+                          "how": "same steps, each one graph launch with the new branch "
+                                 "lengths (P(t) included) and one wait"},
             "checkpointed": ckpt,
             "plain_fp64": {"value": value64, "unit": "evals/s", "ms_per_step": ms64 / k64,
                            "mixed_over_fp64": value / value64,

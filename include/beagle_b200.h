@@ -409,12 +409,22 @@ int beagleB200RootLogLikelihoodsNoAlloc(int device, void* stream, const void* ro
  * argument tables that differ are copied through pinned memory the graph
  * keeps.  Typical use: capture partials, scaling, root lnL, pre-order partials
  * and edge derivatives once, then per step update the transition matrices
- * (outside the graph) and launch the graph.  Graphs live until the instance
- * is finalized. */
+ * (outside the graph) and launch the graph; or capture the matrix update too
+ * and launch with beagleB200LaunchGraphWithLengths.  Graphs live until the
+ * instance is finalized. */
 int beagleB200BeginCapture(int instance);
 /* Returns the graph index in *graph. */
 int beagleB200EndCapture(int instance, int* graph);
 int beagleB200LaunchGraph(int instance, int graph);
+/* The branch lengths of the transition-matrix updates captured in the graph
+ * are read on the device when it runs.  This call replaces them (count = all
+ * the captured updates' lengths, in capture order), then launches the graph,
+ * so that a whole step -- P(t), partials, scaling, root lnL, pre-order
+ * partials, derivatives -- is one call and one wait.  The lengths are copied
+ * before the call returns, and stay: beagleB200LaunchGraph replays the lengths
+ * last given (the capture's until this call replaces them).
+ * BEAGLE_B200_ERROR_OUT_OF_RANGE when count does not match the capture. */
+int beagleB200LaunchGraphWithLengths(int instance, int graph, const double* lengths, int count);
 
 /* ---- batches of instances (no beagle.h counterpart) ------------------
  * Many independent trees or partitions of uneven pattern and state counts,
