@@ -76,6 +76,7 @@ _SIGS = {
     "GetSiteLogLikelihoods": [_i, _p],
     "GetSiteDerivatives": [_i, _p, _p],
     "GetCudaStream": [_i, _p],
+    "InjectKernelTimeout": [_i, _i],
 }
 
 ERRORS = {
@@ -429,6 +430,11 @@ class Instance:
     def supports(self, name):
         """Whether the library exports <prefix><name>."""
         return name in self.blib.fn
+
+    def injectKernelTimeout(self, which):
+        """Raise the device flag of a timed-out kernel wait (0: tensor-core
+        kernels, 1: bulk-copy derivative); the next result call reports it."""
+        self._call("InjectKernelTimeout", which)
 
     def tunedVariants(self):
         """{kind: variant} the autotuner last ran (beagleB200GetTunedVariants)."""

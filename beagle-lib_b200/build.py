@@ -6,8 +6,8 @@ g++ for the host instance and the C ABI, linked in-tree into ``lib/``.
 
 Object files go to ``_build/`` at the repository root (git-ignored).
 
-When the BEAGLE sources are at hand (``BEAGLE_REF`` or the default path
-below), it also builds ``lib/libhmsbeagle-cuda.so.40.0.0``: the plugin that
+When the BEAGLE sources are at hand (their folder in ``BEAGLE_REF``; no
+default), it also builds ``lib/libhmsbeagle-cuda.so.40.0.0``: the plugin that
 lets the stock libhmsbeagle.so dispatcher run on this library
 (``plugin/b200_plugin.cpp``, compiled against the dispatcher's public headers
 BeagleImpl.h / Plugin.h / beagle.h).  Without them the plugin is not rebuilt.
@@ -28,7 +28,7 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 LIBNAME = "libbeagle_b200.so"
 PLUGIN = "libhmsbeagle-cuda.so.40.0.0"     # name the dispatcher dlopens (PLUGIN_VERSION 40)
 PLUGIN_SRC = os.path.join(HERE, "plugin", "b200_plugin.cpp")
-BEAGLE_REF = os.environ.get("BEAGLE_REF", "/root/reference")
+BEAGLE_REF = os.environ.get("BEAGLE_REF", "")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 INC = ["-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
@@ -101,15 +101,16 @@ def build(verbose=False):
 def build_plugin(lib, verbose=False):
     """libhmsbeagle-cuda.so.40.0.0 beside libbeagle_b200.so (run path
     $ORIGIN).  Returns its path, or None when the BEAGLE headers are absent."""
-    hdr = os.path.join(BEAGLE_REF, "libhmsbeagle", "BeagleImpl.h")
+    ref = os.environ.get("BEAGLE_REF", BEAGLE_REF)
+    hdr = os.path.join(ref, "libhmsbeagle", "BeagleImpl.h")
     out = os.path.join(LIBDIR, PLUGIN)
-    if not os.path.exists(hdr):
+    if not ref or not os.path.exists(hdr):
         return out if os.path.exists(out) else None
     deps = [PLUGIN_SRC, lib, os.path.join(ROOT, "include", "beagle_b200.h")]
     if os.path.exists(out) and all(os.path.getmtime(d) <= os.path.getmtime(out) for d in deps):
         return out
     cmd = ["g++", "-std=c++11", "-O2", "-fPIC", "-shared", "-Wall", "-Wno-unused-function",
-           "-Wno-delete-non-virtual-dtor", "-I" + BEAGLE_REF, "-I" + os.path.join(ROOT, "include"), PLUGIN_SRC, "-o", out,
+           "-Wno-delete-non-virtual-dtor", "-I" + ref, "-I" + os.path.join(ROOT, "include"), PLUGIN_SRC, "-o", out,
            "-L" + LIBDIR, "-l:" + LIBNAME, "-Wl,-soname," + PLUGIN, "-Wl,-rpath,$ORIGIN"]
     cmd, rc, outp = _compile(cmd)
     if verbose or rc:

@@ -422,6 +422,10 @@ int beagleB200GetCudaStream(int h, void** out) {
 }
 
 
+int beagleB200InjectKernelTimeout(int h, int which) {
+    return call(h, [&](b200::Instance* in) { return in->injectKernelTimeout(which); });
+}
+
 int beagleB200CreateBatch(const int* instances, int count) {
     if (!instances || count <= 0) return BEAGLE_B200_ERROR_OUT_OF_RANGE;
     std::vector<b200::Instance*> members;

@@ -261,7 +261,12 @@ int Instance::beginCapture() {
     // before the capture starts: the graph keeps the address)
     cap_.len_cap = 4 * nmat_;
     CK(cudaMalloc(&cap_.d_len, sizeof(double) * cap_.len_cap));
-    CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed));
+    const cudaError_t e = cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        free_graph(cap_);
+        return kErrGeneral;
+    }
     capturing_ = true;
     t_capture_pinned = &cap_.pinned;
     return kSuccess;
@@ -282,9 +287,20 @@ int Instance::endCapture(int* graph) {
     }
     // the capture-time lengths, which launchGraph replays until
     // launchGraphWithLengths replaces them
-    if (!cap_.len.empty())
-        CK(cudaMemcpy(cap_.d_len, cap_.len.data(), sizeof(double) * cap_.len.size(),
-                      cudaMemcpyHostToDevice));
+    if (!cap_.len.empty()) {
+        e = cudaMemcpy(cap_.d_len, cap_.len.data(), sizeof(double) * cap_.len.size(),
+                       cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMallocHost(&cap_.h_len_ring,
+                               sizeof(double) * cap_.len.size() * GraphRec::kLenRing);
+        for (int k = 0; k < GraphRec::kLenRing && e == cudaSuccess; ++k)
+            e = cudaEventCreateWithFlags(&cap_.len_ev[k], cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            (void)cudaGetLastError();
+            free_graph(cap_);
+            return kErrGeneral;
+        }
+    }
     graphs_.push_back(cap_);
     cap_ = GraphRec{};
     *graph = (int)graphs_.size() - 1;
@@ -292,17 +308,27 @@ int Instance::endCapture(int* graph) {
 }
 
 // Replace the branch lengths of the graph's captured transition-matrix
-// updates (count = all of them, in capture order), then launch it.  The copy
-// is stream-ordered before the launch, and a pageable source is read before
-// this call returns.
+// updates (count = all of them, in capture order), then launch it.  The
+// lengths are copied on the host into one of the graph's pinned staging slots
+// before this call returns, whatever kind of memory the caller's array is;
+// the slot's copy to the device is stream-ordered before the launch.  A slot
+// is reused once the copy last queued from it has run (an event wait that
+// only blocks when more than kLenRing launches are still queued ahead of it).
 int Instance::launchGraphWithLengths(int graph, const double* lengths, int count) {
     if (capturing_ || graph < 0 || graph >= (int)graphs_.size() || !graphs_[graph].exec)
         return kErrRange;
-    const GraphRec& g = graphs_[graph];
+    GraphRec& g = graphs_[graph];
     if (!g.len_all || count != (int)g.len.size() || (count > 0 && !lengths)) return kErrRange;
-    if (count > 0)
-        CK(cudaMemcpyAsync(g.d_len, lengths, sizeof(double) * count, cudaMemcpyHostToDevice,
+    if (count > 0) {
+        const int k = g.ring_i;
+        g.ring_i = (k + 1) % GraphRec::kLenRing;
+        CK(cudaEventSynchronize(g.len_ev[k]));
+        double* slot = g.h_len_ring + (size_t)k * count;
+        std::copy(lengths, lengths + count, slot);
+        CK(cudaMemcpyAsync(g.d_len, slot, sizeof(double) * count, cudaMemcpyHostToDevice,
                            stream_));
+        CK(cudaEventRecord(g.len_ev[k], stream_));
+    }
     return launchGraph(graph);
 }
 
@@ -317,11 +343,26 @@ int Instance::launchGraph(int graph) {
     return kSuccess;
 }
 
+int Instance::injectKernelTimeout(int which) {
+    if (capturing_ || (which != 0 && which != 1)) return kErrRange;
+    if (which == 0) {
+        CK(tc_raise_status(stream_));
+        tc_used_ = true;
+    } else {
+        CK(bulk_raise_status(stream_));
+        bulk_used_ = true;
+    }
+    return kSuccess;
+}
+
 void Instance::free_graph(GraphRec& g) {
     if (g.exec) cudaGraphExecDestroy(g.exec);
     if (g.graph) cudaGraphDestroy(g.graph);
     for (void* p : g.pinned) cudaFreeHost(p);
     if (g.d_len) cudaFree(g.d_len);
+    for (cudaEvent_t ev : g.len_ev)
+        if (ev) cudaEventDestroy(ev);
+    if (g.h_len_ring) cudaFreeHost(g.h_len_ring);
     g = GraphRec{};
 }
 
@@ -1242,6 +1283,15 @@ int Instance::build_deriv(const int* post, const int* pre, const int* dmat, cons
 int Instance::calculateEdgeDerivatives(const int* post, const int* pre, const int* dmat,
                                        const int* cw, int count, double* outDerivs,
                                        double* outSum, double* outSumSq) {
+    const int rc = queue_edge_derivatives(post, pre, dmat, cw, count, outDerivs != nullptr);
+    if (rc || count == 0) return rc;
+    return deliver_sums(count, outDerivs, outSum, outSumSq);
+}
+
+// The launches of calculateEdgeDerivatives: the 2 * count sums into out_ and,
+// with `site`, the per-site values into site_d_; nothing is delivered.
+int Instance::queue_edge_derivatives(const int* post, const int* pre, const int* dmat,
+                                     const int* cw, int count, bool site_values) {
     std::vector<DerivDesc> tab;
     const int rc0 = build_deriv(post, pre, dmat, cw, count, tab);
     if (rc0) return rc0;
@@ -1253,11 +1303,11 @@ int Instance::calculateEdgeDerivatives(const int* post, const int* pre, const in
     CK(t_deriv_.upload(tab.data(), sizeof(DerivDesc) * count, stream_));
     CK(scratch_.reserve(sizeof(double) * 2 * (size_t)count * nblk));
     CK(out_.reserve(sizeof(double) * 2 * count));
-    if (outDerivs) CK(site_d_.reserve(sizeof(double) * (size_t)count * P_));
+    if (site_values) CK(site_d_.reserve(sizeof(double) * (size_t)count * P_));
     if (S_ == 4) {
         const DerivDesc* d_desc = (const DerivDesc*)t_deriv_.ptr;
         const double* catw = d_catw_ + (size_t)w * C_;
-        double* site = outDerivs ? (double*)site_d_.ptr : nullptr;
+        double* site = site_values ? (double*)site_d_.ptr : nullptr;
         const Dims dm = dims();
         auto run = [&](int v) -> cudaError_t {
             return LAUNCH(launch_edge_derivatives, d_desc, count, catw, d_patw_, dm, site,
@@ -1271,7 +1321,7 @@ int Instance::calculateEdgeDerivatives(const int* post, const int* pre, const in
     } else {
         const DerivDesc* d_desc = (const DerivDesc*)t_deriv_.ptr;
         const double* catw = d_catw_ + (size_t)w * C_;
-        double* site = outDerivs ? (double*)site_d_.ptr : nullptr;
+        double* site = site_values ? (double*)site_d_.ptr : nullptr;
         const Dims dm = dims();
         // variant 0: CUDA-core cluster kernel; 1: tensor cores (FP32 only)
         auto run = [&](int v) -> cudaError_t {
@@ -1301,7 +1351,7 @@ int Instance::calculateEdgeDerivatives(const int* post, const int* pre, const in
         }
         CK(e);
     }
-    return deliver_sums(count, outDerivs, outSum, outSumSq);
+    return kSuccess;
 }
 
 // The 2 * count sums of an edge-derivative launch (out_), and the per-site
@@ -1354,7 +1404,8 @@ int Instance::updatePrePartialsWithDerivatives(const int* ops, int count, const 
                                         outSumSq);
     };
     const Dims dm = dims();
-    if (count == 0 || !fused_supported(dm, count)) return separate();
+    const bool tc_fused = !dbl_ && tc_supported(dm);
+    if (count == 0 || !(fused_supported(dm, count) || tc_fused)) return separate();
     std::vector<OpDesc> tab;
     std::vector<uint8_t> dep;
     bool idempotent = false, has_op_cum = false;
@@ -1367,6 +1418,8 @@ int Instance::updatePrePartialsWithDerivatives(const int* ops, int count, const 
     for (int k = 0; k < count; ++k) ++writes[pre[k]];
     for (int k = 0; k < count; ++k)
         if (writes[pre[k]] != 1 || writes.count(post[k])) return separate();
+    if (S_ != 4) return prederiv_tc(ops, count, post, pre.data(), dmat, cw, tab, dtab,
+                                    idempotent, outSum, outSumSq);
     std::vector<PreDerivOp> fops(count);
     for (int k = 0; k < count; ++k) {
         const OpDesc& t = tab[k];
@@ -1441,6 +1494,53 @@ int Instance::updatePrePartialsWithDerivatives(const int* ops, int count, const 
         (void)cudaGetLastError();
         v = 1;
         e = run(v);
+    }
+    picked_[kTuneFused] = v;
+    CK(e);
+    return deliver_sums(count, nullptr, outSum, outSumSq);
+}
+
+// updatePrePartialsWithDerivatives for 4 < S <= 64 on the FP32 path.
+// Variant 0: the two calls' kernels (each tuned as its own call); 1: the
+// tensor-core fused walk (k_tc.cu k_prederiv_tc).  The autotuner times them
+// when the list may run repeatedly.
+int Instance::prederiv_tc(const int* ops, int count, const int* post, const int* pre,
+                          const int* dmat, const int* cw, const std::vector<OpDesc>& tab,
+                          const std::vector<DerivDesc>& dtab, bool idempotent, double* outSum,
+                          double* outSumSq) {
+    const Dims dm = dims();
+    const int nblk = prederiv_tc_blocks(dm);
+    CK(scratch_.reserve(sizeof(double) * 2 * (size_t)count * nblk));
+    CK(out_.reserve(sizeof(double) * 2 * count));
+    const double* catw = d_catw_ + (size_t)cw[0] * C_;
+    const int ls = (int)log_scalers_;
+    auto run = [&](int v) -> cudaError_t {
+        if (v == 0) {
+            if (post_or_pre(ops, count, 7, -1, true) != kSuccess) return cudaErrorUnknown;
+            if (queue_edge_derivatives(post, pre, dmat, cw, count, false) != kSuccess)
+                return cudaErrorUnknown;
+            return cudaSuccess;
+        }
+        cudaError_t e = t_ops_pre_.upload(tab.data(), sizeof(OpDesc) * count, stream_);
+        if (e == cudaSuccess) e = t_deriv_.upload(dtab.data(), sizeof(DerivDesc) * count, stream_);
+        if (e != cudaSuccess) return e;
+        tc_used_ = true;
+        e = launch_prederiv_tc((const OpDesc*)t_ops_pre_.ptr, (const DerivDesc*)t_deriv_.ptr,
+                               count, count, catw, d_patw_, dm, ls, (double*)scratch_.ptr,
+                               stream_);
+        if (e != cudaSuccess) return e;
+        return launch_final_sum((double*)scratch_.ptr, nblk, 2 * count, (double*)out_.ptr,
+                                stream_);
+    };
+    const TuneKey key{kTuneFused, (int)dbl_, C_ * 100 + Sg_, Pp_, tune_count_class(count),
+                      device_};
+    int v = tune_pick(key, 2, idempotent, stream_, run);
+    if (v < 0) v = 1;
+    cudaError_t e = run(v);
+    if (e == cudaErrorInvalidConfiguration && v == 1) {   // TMEM could be oversubscribed
+        (void)cudaGetLastError();
+        v = 0;
+        e = run(0);
     }
     picked_[kTuneFused] = v;
     CK(e);

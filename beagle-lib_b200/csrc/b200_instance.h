@@ -131,6 +131,10 @@ public:
     int beginCapture();
     int endCapture(int* graph);
     int launchGraph(int graph);
+    // Raise, on this instance's stream, the device flag a kernel sets when a
+    // bounded wait runs out (which 0: tensor-core kernels, 1: bulk-copy
+    // derivative), as if one had; the next result call reports it.
+    int injectKernelTimeout(int which);
     int launchGraphWithLengths(int graph, const double* lengths, int count);
 
     // For batched calls (b200_batch.cpp).
@@ -156,6 +160,12 @@ private:
     int run_matrix_jobs(const std::vector<MatJob>& jobs);
     int post_or_pre(const int* ops, int count, int stride, int cumulative, bool pre);
     int deliver_sums(int count, double* outDerivs, double* outSum, double* outSumSq);
+    int queue_edge_derivatives(const int* post, const int* pre, const int* dmat, const int* cw,
+                               int count, bool site_values);
+    int prederiv_tc(const int* ops, int count, const int* post, const int* pre, const int* dmat,
+                    const int* cw, const std::vector<OpDesc>& tab,
+                    const std::vector<DerivDesc>& dtab, bool idempotent, double* outSum,
+                    double* outSumSq);
     int sync();
     double* stage(size_t n);     // pinned result staging (ASYNCH results)
     Dims dims() const { return Dims{S_, Sg_, P_, Pp_, C_}; }
@@ -233,6 +243,14 @@ private:
         int len_cap = 0;
         std::vector<double> len;
         bool len_all = true;      // every captured update reads d_len
+        // launchGraphWithLengths stages the caller's lengths in a ring of
+        // pinned slots (allocated at EndCapture), so the caller's buffer is
+        // free again when the call returns; slot k is rewritten only after
+        // the copy recorded by len_ev[k] has run
+        static constexpr int kLenRing = 4;
+        double* h_len_ring = nullptr;
+        cudaEvent_t len_ev[kLenRing] = {};
+        int ring_i = 0;
     };
     std::vector<GraphRec> graphs_;
     GraphRec cap_;

@@ -78,6 +78,15 @@ cudaError_t launch_walk_tc_batch(const WalkSeg* d_segs, int nseg, int ntiles, bo
 cudaError_t launch_deriv_tc_batch(const DerivSeg* d_segs, int nseg, int nclusters, const Dims& d,
                                   cudaStream_t s);
 bool deriv_tc_launchable(const Dims& d);
+// Fused pre-order walk + edge derivatives on the tensor cores (FP32, S > 4):
+// ops as launch_opwalk_tc's pre-order list, d_desc[k] the derivative of op k's
+// branch (post = the node's post-order operand, pre = op k's destination);
+// the sums of op k into d_block rows k and nsum + k, prederiv_tc_blocks(d)
+// partials each (add them with launch_final_sum).
+int prederiv_tc_blocks(const Dims& d);
+cudaError_t launch_prederiv_tc(const OpDesc* d_ops, const DerivDesc* d_desc, int nops, int nsum,
+                               const double* catw, const double* patw, const Dims& d, int ls,
+                               double* d_block, cudaStream_t s);
 // TMA-fed tensor-core walk (FP32, 4 < S <= 64): maps[k] gives op k's tensor
 // maps (tc_encode_map: a partials buffer, or a matrix buffer, of this shape).
 cudaError_t tc_encode_map(TmaMap* out, const void* base, bool matrix, const Dims& d);
@@ -88,10 +97,12 @@ cudaError_t launch_opwalk_tc_tma(const OpDesc* d_ops, const TcOpMaps* d_maps, in
 // the stream completes), and clear it (synchronises `s`).
 cudaError_t tc_status_async(int* pinned_dst, cudaStream_t s);
 cudaError_t tc_clear_status(cudaStream_t s);
+cudaError_t tc_raise_status(cudaStream_t s);      // as a timed-out wait would
 // The same for the bulk-copy derivative stream (k_reduce.cu); clearing does
 // not synchronise.
 cudaError_t bulk_status_async(int* pinned_dst, cudaStream_t s);
 cudaError_t bulk_clear_status(cudaStream_t s);
+cudaError_t bulk_raise_status(cudaStream_t s);    // as a timed-out wait would
 
 // Root log-likelihood: site lnL into d_site[P]; the weighted total into d_out[0].
 // d_block holds root_blocks(d, P, wide) doubles: `wide` spreads a pattern

@@ -16,7 +16,7 @@
 // reads (one partial per pattern block) before reading it.  Two calls that
 // overlap on the GPU (different streams, or different host threads on the
 // same device) race on the array; callers must order them.
-#include <mutex>
+#include <cstdint>
 
 #include "b200_kernels.h"
 #include "beagle_b200.h"
@@ -27,24 +27,22 @@ namespace {
 constexpr int kScratchDoubles = 8192;   // 64 KiB: one double per 128-pattern block
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mu;
-double* g_scratch_ptr[kMaxDevices] = {};
+// The array's device address on the current device.  In host code the symbol
+// g_noalloc_scratch is a host-side stand-in, not a device address.  The
+// address is looked up on every call rather than cached, so that it is the
+// current context's even after a cudaDeviceReset or under another primary
+// context.  The lookup is cheap once the module is loaded; the first call on
+// a device may load it, which is why that call must come before any stream
+// capture.
+cudaError_t scratch_address(double** out) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    *out = static_cast<double*>(p);
+    return e;
+}
 
-// The array's device address on `device`.  In host code the symbol
-// g_noalloc_scratch is a host-side stand-in, not a device address, so it is
-// looked up once per device, with that device current, and cached.
-cudaError_t scratch_on(int device, double** out) {
-    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lk(g_scratch_mu);
-    if (!g_scratch_ptr[device]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return e;
-        g_scratch_ptr[device] = static_cast<double*>(p);
-    }
-    *out = g_scratch_ptr[device];
-    return cudaSuccess;
+bool aligned(const void* p, std::uintptr_t a) {
+    return (reinterpret_cast<std::uintptr_t>(p) % a) == 0;
 }
 
 }  // namespace
@@ -60,6 +58,14 @@ extern "C" int beagleB200RootLogLikelihoodsNoAlloc(
         return BEAGLE_B200_ERROR_OUT_OF_RANGE;
     if (stateCount < 2 || stateCount > 64 || categoryCount < 1 || patternCount < 1)
         return BEAGLE_B200_ERROR_OUT_OF_RANGE;
+    // Partials rows are read as 16-byte vectors; the FP64 arrays as doubles.
+    // A misaligned pointer (an offset view into a larger allocation) is
+    // refused here, before anything is queued.
+    if (!b200::aligned(rootPartials, 16) || !b200::aligned(categoryWeights, 8) ||
+        !b200::aligned(stateFrequencies, 8) || !b200::aligned(patternWeights, 8) ||
+        !b200::aligned(cumulativeScaleFactors, 8) || !b200::aligned(outSiteLogLikelihoods, 8) ||
+        !b200::aligned(outSumLogLikelihood, 8))
+        return BEAGLE_B200_ERROR_OUT_OF_RANGE;
     // One scratch double per 128-pattern block: at most 8192 * 128 patterns.
     if (b200::reduction_blocks(patternCount) > b200::kScratchDoubles)
         return BEAGLE_B200_ERROR_OUT_OF_RANGE;
@@ -69,7 +75,7 @@ extern "C" int beagleB200RootLogLikelihoodsNoAlloc(
         return BEAGLE_B200_ERROR_NO_RESOURCE;
     }
     double* scratch = nullptr;
-    cudaError_t e = b200::scratch_on(device, &scratch);
+    cudaError_t e = b200::scratch_address(&scratch);
     if (e == cudaSuccess) {
         b200::Dims d;
         d.S = stateCount;

@@ -3,6 +3,7 @@
 // deterministic: fixed 128-thread blocks reduce by warp shuffles and shared
 // memory into per-block partial sums, and a second pass (one CTA per output)
 // adds the partials in a fixed order.
+#include <cstdlib>
 #include "b200_kernels.h"
 #include "b200_vec.cuh"
 
@@ -423,20 +424,34 @@ __device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t b
         : "memory");
 }
 
-__device__ __forceinline__ void bulk_wait(uint64_t* bar, uint32_t parity, bool& failed) {
+// A wait bounded below the default polls with the non-blocking test_wait:
+// try_wait may suspend the thread until the phase completes, which would
+// outlast a short bound.
+__device__ __forceinline__ void bulk_wait(uint64_t* bar, uint32_t parity, bool& failed,
+                                          long long limit = kBulkWaitCycles) {
     if (failed) return;
+    const bool poll = limit < kBulkWaitCycles;
     const long long t0 = clock64();
     for (;;) {
         uint32_t ok;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(ok)
-            : "r"(smem_addr(bar)), "r"(parity)
-            : "memory");
+        if (poll)
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                "selp.u32 %0, 1, 0, p;\n\t}"
+                : "=r"(ok)
+                : "r"(smem_addr(bar)), "r"(parity)
+                : "memory");
+        else
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                "selp.u32 %0, 1, 0, p;\n\t}"
+                : "=r"(ok)
+                : "r"(smem_addr(bar)), "r"(parity)
+                : "memory");
         if (ok) return;
-        if (clock64() - t0 > kBulkWaitCycles) {
+        if (clock64() - t0 > limit) {
             failed = true;
             atomicExch(&b200_bulk_status, 1);
             return;
@@ -474,7 +489,7 @@ template <typename Real, int C>
 __global__ void __launch_bounds__(kBulkThreads)
 k_edge_deriv4_bulk(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
                    const double* __restrict__ patw, int P, int Pp, int nb, double* site,
-                   double* block) {
+                   double* block, long long wait_cycles) {
     constexpr int kTile = bulk_tile<Real, C>();
     constexpr size_t kStageBytes = kBulkStageBytes;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -492,13 +507,18 @@ k_edge_deriv4_bulk(const DerivDesc* __restrict__ desc, const double* __restrict_
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    // Copies issued into each stage (thread 0's count; stage s's k-th copy
+    // completes the barrier's phase k, of parity k & 1).
+    int issued[kBulkStages] = {};
     // Prologue: the first kBulkStages items of this CTA.
     if (threadIdx.x == 0) {
         for (int s = 0; s < kBulkStages; ++s) {
             const int item = blockIdx.x + s * gridDim.x;
-            if (item < nitems)
+            if (item < nitems) {
                 bulk_issue<Real, C>(desc, item, nchunks, Pp, st_pre + s * kStageBytes,
                                     st_post + s * kStageBytes, &bars[s]);
+                ++issued[s];
+            }
         }
     }
     bool failed = false;
@@ -507,7 +527,7 @@ k_edge_deriv4_bulk(const DerivDesc* __restrict__ desc, const double* __restrict_
     for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
         const int b = item / nchunks, q = item - b * nchunks;
         const DerivDesc& dd = desc[b];
-        bulk_wait(&bars[s], phase[s], failed);
+        bulk_wait(&bars[s], phase[s], failed, wait_cycles);
         phase[s] ^= 1u;
         const Real* pre = reinterpret_cast<const Real*>(st_pre + s * kStageBytes);
         const Real* post = reinterpret_cast<const Real*>(st_post + s * kStageBytes);
@@ -568,16 +588,34 @@ k_edge_deriv4_bulk(const DerivDesc* __restrict__ desc, const double* __restrict_
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 bulk_issue<Real, C>(desc, next, nchunks, Pp, st_pre + s * kStageBytes,
                                     st_post + s * kStageBytes, &bars[s]);
+                ++issued[s];
             }
         }
         s = (s + 1) % kBulkStages;
     }
     // After a time-out, copies may still be in flight into this CTA's shared
-    // memory: wait for them (bounded again) before the CTA exits.
+    // memory: wait (with the full bound, whatever wait_cycles was) until the
+    // phase of the last copy issued into each stage has completed, before the
+    // CTA exits.  A completed phase returns at once.
     if (failed && threadIdx.x == 0) {
-        bool again = false;
-        for (int k = 0; k < kBulkStages; ++k) bulk_wait(&bars[k], phase[k], again);
+        for (int k = 0; k < kBulkStages; ++k) {
+            if (issued[k] == 0) continue;
+            bool again = false;
+            bulk_wait(&bars[k], (uint32_t)((issued[k] - 1) & 1), again);
+        }
     }
+}
+
+// BEAGLE_B200_WAIT_CYCLES: the bound, in clock cycles, of the bulk-copy
+// derivative's waits on its stages (default 2e9, about one second).  Lower
+// values exist so that tests can make a wait run out on purpose and check
+// that the time-out is reported; the wait for copies still in flight before
+// a CTA exits always keeps the full bound.
+long long bulk_wait_cycles() {
+    const char* v = std::getenv("BEAGLE_B200_WAIT_CYCLES");
+    if (!v || !*v) return kBulkWaitCycles;
+    const long long x = std::atoll(v);
+    return x > 0 ? x : kBulkWaitCycles;
 }
 
 template <typename Real, int C>
@@ -598,7 +636,8 @@ cudaError_t run_deriv4_bulk(const DerivDesc* desc, int nb, const double* catw,
     const int nitems = nb * ((d.Pp + kTile - 1) / kTile);
     const int slots = sms * (per_sm > 0 ? per_sm : 1);
     const int grid = nitems < slots ? nitems : slots;
-    kern<<<grid, kBulkThreads, smem, s>>>(desc, catw, patw, d.P, d.Pp, nb, site, block);
+    kern<<<grid, kBulkThreads, smem, s>>>(desc, catw, patw, d.P, d.Pp, nb, site, block,
+                                          bulk_wait_cycles());
     return cudaGetLastError();
 }
 
@@ -892,6 +931,12 @@ cudaError_t launch_edge_derivatives(const DerivDesc* desc, int nb, const double*
 cudaError_t bulk_status_async(int* pinned_dst, cudaStream_t s) {
     return cudaMemcpyFromSymbolAsync(pinned_dst, b200_bulk_status, sizeof(int), 0,
                                      cudaMemcpyDeviceToHost, s);
+}
+
+cudaError_t bulk_raise_status(cudaStream_t s) {
+    static const int one = 1;
+    return cudaMemcpyToSymbolAsync(b200_bulk_status, &one, sizeof(int), 0,
+                                   cudaMemcpyHostToDevice, s);
 }
 
 cudaError_t bulk_clear_status(cudaStream_t s) {

@@ -316,8 +316,8 @@ __device__ __forceinline__ void store_row(float* hi, float* lo, const float z[NP
 
 // Issue the 3 x KC / 8 MMAs of one chunk (thread 0 only); `first` clears the
 // accumulator with the first MMA.  Completion arrives on sm.bar.
-template <int KC>
-__device__ __forceinline__ void issue_chunk(TcSmem& sm, uint32_t d_tmem, int N, bool first) {
+template <int KC, typename SM>
+__device__ __forceinline__ void issue_chunk(SM& sm, uint32_t d_tmem, int N, bool first) {
     const uint32_t idesc = idesc_tf32(kTM, N);
     const uint32_t ah = smem_u32(sm.a_hi), al = smem_u32(sm.a_lo);
     const uint32_t bh = smem_u32(sm.b_hi), bl = smem_u32(sm.b_lo);
@@ -343,7 +343,8 @@ struct Pipe {
     bool failed = false;
 };
 
-__device__ __forceinline__ void pipe_drain(TcSmem& sm, Pipe& pp) {
+template <typename SM>
+__device__ __forceinline__ void pipe_drain(SM& sm, Pipe& pp) {
     if (pp.pending) {
         mbar_wait(&sm.bar, pp.phase, pp.failed);
         pp.phase ^= 1u;
@@ -353,8 +354,8 @@ __device__ __forceinline__ void pipe_drain(TcSmem& sm, Pipe& pp) {
 
 // Run up to 4 chunk jobs through the single chunk buffer: the registers of
 // job i + 1 are gathered while the MMAs of job i run.
-template <int NP, int KC>
-__device__ __forceinline__ void run_jobs(TcSmem& sm, Pipe& pp, uint32_t tmem, const Job (&jobs)[4],
+template <int NP, int KC, typename SM>
+__device__ __forceinline__ void run_jobs(SM& sm, Pipe& pp, uint32_t tmem, const Job (&jobs)[4],
                                          int n, size_t xs, int Sg, ChunkRegs& cr) {
     if (n > 0) gather_job<NP, KC>(cr, jobs[0], xs, Sg);
 #pragma unroll
@@ -1076,6 +1077,243 @@ k_deriv_tc(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
     if (t < 32) tmem_dealloc(tmem, G::DCOLS);
 }
 
+// ------------------------------------ fused pre-order walk + derivatives
+// The pre-order walk of k_walk_tc with each branch's edge derivative taken
+// from the registers of its new row (the S > 4 counterpart of the S = 4
+// fused walk in k_fused.cu): per op, three contractions on the tensor cores,
+//   GEMM 1: Y1 = sib . P_sib^T                  (TMEM columns [0, NP))
+//   GEMM 3: Y3 = post_b . D_b^T                 (columns [NP, 2 NP))
+//   GEMM 2: pre_b = (pre_parent o Y1) . P_b     (columns [0, NP) again, once
+//                                                Y1 has been read)
+// GEMM 3 needs nothing the walk computes, so it is issued with GEMM 1 and its
+// loads overlap GEMM 1's; the CTA holds 2 NP columns, as the walk does.  From
+// pre_b before rescaling, per category c,
+//   n_c = sum_i pre_b[i] Y3[i],   q_c = sum_i pre_b[i] post_b[i],
+// are exchanged over the cluster with the rescaling maximum (one cluster
+// barrier per op, the exchange buffers alternating by op parity), and
+// category 0's CTA forms d_p = sum_c w_c n_c / sum_c w_c q_c, the quantity of
+// k_deriv_tc (CPU/BeagleCPUImpl.hpp:1940-2083).  The tile's w_p d_p and
+// w_p d_p^2 go to block[op][tile] and block[nsum + op][tile]; launch_final_sum
+// adds the tiles in a fixed order.  A separate derivative pass would read
+// every pre_b back from memory; here it never leaves the registers.
+struct TcFusedSmem {
+    float a_hi[kTM * 32];
+    float a_lo[kTM * 32];
+    float b_hi[64 * 32];
+    float b_lo[64 * 32];
+    float smax[2][kTM];          // alternating by op parity
+    double nd[2][kTM * 2];       // w_c n_c, w_c q_c per row, alternating by op parity
+    double red[kTT / 32 * 2];
+    uint64_t bar;
+    uint32_t tmem;
+};
+
+template <int NP>
+struct TcFusedGeo {
+    static constexpr int COLS = TcGeo<NP>::TCOLS;
+};
+
+template <int NP, int KC>
+__global__ void __launch_bounds__(kTT, 3)
+k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds, int nops,
+              int nsum, int S, int Sg, int C, int P, const double* __restrict__ catw,
+              const double* __restrict__ patw, int log_scalers, double* block) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    TcFusedSmem& sm = *reinterpret_cast<TcFusedSmem*>(smem_raw);
+    constexpr int COLS = TcFusedGeo<NP>::COLS;
+    const int t = threadIdx.x;
+    const int c = blockIdx.x % C;
+    const int tile = blockIdx.x / C;
+    const int ntiles = gridDim.x / C;
+    const int p0 = tile * kTM;
+    const int p = p0 + t;
+    constexpr int NKC = chunks_of<NP>();
+    const size_t xs = (size_t)C * Sg;
+    const size_t mo = (size_t)c * Sg * Sg;
+    const double wc = catw[c];
+
+    if (t == 0) {
+        mbar_init(&sm.bar, 1);
+        mbar_init_fence();
+    }
+    if (t < 32) {
+        tmem_alloc(&sm.tmem, COLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = sm.tmem;
+    Pipe pp;
+    ChunkRegs cr;
+    cg::cluster_group cluster = cg::this_cluster();
+    for (int o = 0; o < nops; ++o) {
+        const OpDesc& op = ops[o];
+        const DerivDesc& dd = dds[o];
+        const bool st2 = op.kind & kX2States;
+        const bool pst = dd.post_is_states;
+        const float* x2 = static_cast<const float*>(op.x2);
+        const float* post = static_cast<const float*>(dd.post);
+        // GEMM 1, then GEMM 3 (two calls of at most NKC jobs each: the
+        // first gather of GEMM 3 still overlaps GEMM 1's last MMAs, and the
+        // shorter job lists keep the walk within its register budget)
+        {
+            Job jobs[4];
+            int nj = 0;
+            for (int q = 0; q < NKC; ++q)
+                if (!st2) jobs[nj++] = Job{x2 + (size_t)p0 * xs + (size_t)c * Sg,
+                                           static_cast<const float*>(op.m2) + mo, 0u, q};
+            run_jobs<NP, KC>(sm, pp, tmem, jobs, nj, xs, Sg, cr);
+        }
+        {
+            Job jobs[4];
+            int nj = 0;
+            for (int q = 0; q < NKC; ++q)
+                if (!pst) jobs[nj++] = Job{post + (size_t)p0 * xs + (size_t)c * Sg,
+                                           static_cast<const float*>(dd.dmat) + mo,
+                                           (uint32_t)NP, q};
+            run_jobs<NP, KC>(sm, pp, tmem, jobs, nj, xs, Sg, cr);
+        }
+        // While they run: the parent row, the tip states and GEMM 2's first
+        // B chunk (rows of P_node^T).
+        const float* mt =
+            static_cast<const float*>((op.kind & kM1Transposed) ? op.m1 : op.m1t) + mo;
+        float z[NP];
+        {
+            const float* pr = static_cast<const float*>(op.x1) + ((size_t)p * C + c) * Sg;
+#pragma unroll
+            for (int j = 0; j < NP / 4; ++j) {
+                z[4 * j] = z[4 * j + 1] = z[4 * j + 2] = z[4 * j + 3] = 0.f;
+                if (4 * j < Sg) ld4(pr + 4 * j, z + 4 * j);
+            }
+        }
+        const int s2 = st2 ? static_cast<const int*>(op.x2)[p] : 0;
+        const int sp = pst ? static_cast<const int*>(dd.post)[p] : 0;
+        gather<NP, KC, true>(cr.b, mt, Sg, Sg, 0, Sg);
+        pipe_drain(sm, pp);
+        tc_fence_after();
+        mul_operand<NP>(z, st2, tmem, 0, static_cast<const float*>(op.m2t) + mo, s2, S, Sg,
+                        (float)op.pad2);
+        for (int q = 0; q < NKC; ++q) {
+            pipe_drain(sm, pp);
+            if (q == 0) store_row<NP, KC, 0>(sm.a_hi, sm.a_lo, z);
+            else store_row<NP, KC, 1>(sm.a_hi, sm.a_lo, z);
+            scatter<NP, KC>(cr.b, sm.b_hi, sm.b_lo);
+            fence_async_smem();
+            tc_fence_before();
+            __syncthreads();
+            if (t == 0) issue_chunk<KC>(sm, tmem, NP, q == 0);   // over Y1, now read
+            pp.pending = true;
+            if (q + 1 < NKC) gather<NP, KC, true>(cr.b, mt, Sg, Sg, (q + 1) * KC, Sg);
+        }
+        pipe_drain(sm, pp);
+        tc_fence_after();
+        float out[NP];
+#pragma unroll
+        for (int j = 0; j < NP / 16; ++j) tmem_chunk(tmem, 0, j, out + 16 * j);
+        // derivative terms of this row and category, from pre_b as computed
+        float nq[4] = {0.f, 0.f, 0.f, 0.f}, dq[4] = {0.f, 0.f, 0.f, 0.f};
+        float mq[4] = {0.f, 0.f, 0.f, 0.f};       // rescaling maximum, four chains
+        const float* xr = post + ((size_t)p * C + c) * Sg;
+#pragma unroll
+        for (int j = 0; j < NP / 16; ++j) {
+            float y[16], x[16];
+            if (pst) tip_chunk(static_cast<const float*>(dd.dmatt) + mo, sp, S, Sg,
+                               (float)dd.dpad, j, y);
+            else tmem_chunk(tmem, NP, j, y);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                x[4 * k] = x[4 * k + 1] = x[4 * k + 2] = x[4 * k + 3] = 0.f;
+                if (!pst && 16 * j + 4 * k < Sg) ld4(xr + 16 * j + 4 * k, x + 4 * k);
+            }
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                const int i = 16 * j + q;
+                if (i >= S) continue;
+                const float xv = pst ? ((sp < 0 || sp >= S || sp == i) ? 1.f : 0.f) : x[q];
+                nq[q & 3] += out[i] * y[q];
+                dq[q & 3] += out[i] * xv;
+                mq[q & 3] = out[i] > mq[q & 3] ? out[i] : mq[q & 3];
+            }
+        }
+        const int par = o & 1;
+        sm.nd[par][t * 2 + 0] = wc * (double)((nq[0] + nq[1]) + (nq[2] + nq[3]));
+        sm.nd[par][t * 2 + 1] = wc * (double)((dq[0] + dq[1]) + (dq[2] + dq[3]));
+        if (op.scale_write) {
+            const float m01 = mq[1] > mq[0] ? mq[1] : mq[0];
+            const float m23 = mq[3] > mq[2] ? mq[3] : mq[2];
+            sm.smax[par][t] = m23 > m01 ? m23 : m01;
+        }
+        // One barrier per op: every CTA's maximum and derivative terms are
+        // written; the halves of parity `par` are rewritten at op o + 2, after
+        // the next op's barrier, which every CTA reaches after reading them.
+        cluster.sync();
+        const bool mine = p >= op.p_begin && p < op.p_end;
+        if (op.scale_write) {
+            float m = 0.f;
+            for (int r = 0; r < C; ++r) {
+                const float u = cluster.map_shared_rank(sm.smax[par], r)[t];
+                m = u > m ? u : m;
+            }
+            if (m == 0.f) m = 1.f;
+            const float inv = 1.f / m;
+#pragma unroll
+            for (int i = 0; i < NP; ++i) out[i] *= inv;
+            if (c == 0 && mine) {
+                const double lm = scale_log(m);
+                op.scale_write[p] = log_scalers ? lm : (double)m;
+            }
+        }
+        if (mine) {
+            float* dst = static_cast<float*>(op.dest) + ((size_t)p * C + c) * Sg;
+#pragma unroll
+            for (int j = 0; j < NP / 4; ++j)
+                if (4 * j < Sg) st4(dst + 4 * j, out + 4 * j);
+        }
+        if (c == 0) {
+            double nn = 0, dn = 0;
+            for (int r = 0; r < C; ++r) {
+                const double* rem = cluster.map_shared_rank(sm.nd[par], r);
+                nn += rem[t * 2 + 0];
+                dn += rem[t * 2 + 1];
+            }
+            double v1 = 0, v2 = 0;
+            if (p < P) {
+                const double dv = nn / dn;
+                v1 = dv * patw[p];
+                v2 = dv * dv * patw[p];
+            }
+#pragma unroll
+            for (int sh = 16; sh > 0; sh >>= 1) {
+                v1 += __shfl_xor_sync(0xffffffffu, v1, sh);
+                v2 += __shfl_xor_sync(0xffffffffu, v2, sh);
+            }
+            if ((t & 31) == 0) {
+                sm.red[(t >> 5) * 2 + 0] = v1;
+                sm.red[(t >> 5) * 2 + 1] = v2;
+            }
+            __syncthreads();
+            if (t == 0) {
+                double t1 = 0, t2 = 0;
+                for (int k = 0; k < kTT / 32; ++k) {
+                    t1 += sm.red[k * 2 + 0];
+                    t2 += sm.red[k * 2 + 1];
+                }
+                block[(size_t)o * ntiles + tile] = t1;
+                block[(size_t)(nsum + o) * ntiles + tile] = t2;
+            }
+        }
+        // TMEM reads of this op done before the next op's MMAs overwrite
+        // them; this op's stores visible to the CTA before later loads.
+        tc_fence_before();
+        __syncthreads();
+    }
+    pipe_drain(sm, pp);
+    tc_fence_after();
+    cluster.sync();   // every remote read of this CTA's exchange buffers is done
+    if (t < 32) tmem_dealloc(tmem, COLS);
+}
+
 // Dynamic shared memory of a launch: the struct, raised to the TMEM
 // columns' share of the SM's shared memory.  An SM has 228 KB (233,472 B)
 // and reserves 1 KB per CTA, so a CTA asking for `cols` of the 512 columns
@@ -1158,6 +1396,19 @@ cudaError_t run_deriv_tc_batch(const DerivSeg* segs, int nseg, int nclusters, co
                      nseg);
 }
 
+template <int NP, int KC>
+cudaError_t run_prederiv_tc(const OpDesc* ops, const DerivDesc* dds, int nops, int nsum,
+                            const double* catw, const double* patw, const Dims& d, int ls,
+                            double* block, cudaStream_t s) {
+    const int cols = TcFusedGeo<NP>::COLS;
+    const size_t need = sizeof(TcFusedSmem) + 1024;
+    const size_t floor_smem = tc_smem(cols);
+    const size_t smem = need > floor_smem ? need : floor_smem;
+    const int grid = (d.Pp / kTM) * d.C;
+    return launch_tc(k_prederiv_tc<NP, KC>, grid, smem, d.C, cols, s, ops, dds, nops, nsum, d.S,
+                     d.Sg, d.C, d.P, catw, patw, ls, block);
+}
+
 // (N, KC) of a padded state count: N = Sg rounded up to 16, KC as above.
 #define B200_TC_DISPATCH(Sg, CALL)                                         \
     ((Sg) <= 8    ? CALL(16, 8)                                            \
@@ -1192,6 +1443,18 @@ cudaError_t launch_deriv_tc(const DerivDesc* desc, int nb, const double* catw,
 #define DER_(NP, KC) run_deriv_tc<NP, KC>(desc, nb, catw, patw, d, site, block, s)
     return B200_TC_DISPATCH(d.Sg, DER_);
 #undef DER_
+}
+
+int prederiv_tc_blocks(const Dims& d) { return d.Pp / kTM; }
+
+cudaError_t launch_prederiv_tc(const OpDesc* d_ops, const DerivDesc* d_desc, int nops, int nsum,
+                               const double* catw, const double* patw, const Dims& d, int ls,
+                               double* d_block, cudaStream_t s) {
+    if (nops == 0) return cudaSuccess;
+    if (!tc_supported(d)) return cudaErrorInvalidValue;
+#define PD_(NP, KC) run_prederiv_tc<NP, KC>(d_ops, d_desc, nops, nsum, catw, patw, d, ls, d_block, s)
+    return B200_TC_DISPATCH(d.Sg, PD_);
+#undef PD_
 }
 
 // Whether the tensor-core derivative kernel of this shape can launch without
@@ -1318,6 +1581,12 @@ cudaError_t launch_opwalk_tc_tma(const OpDesc* ops, const TcOpMaps* maps, int no
 cudaError_t tc_status_async(int* pinned_dst, cudaStream_t s) {
     return cudaMemcpyFromSymbolAsync(pinned_dst, b200_tc_status, sizeof(int), 0,
                                      cudaMemcpyDeviceToHost, s);
+}
+
+cudaError_t tc_raise_status(cudaStream_t s) {
+    static const int one = 1;
+    return cudaMemcpyToSymbolAsync(b200_tc_status, &one, sizeof(int), 0,
+                                   cudaMemcpyHostToDevice, s);
 }
 
 cudaError_t tc_clear_status(cudaStream_t s) {

@@ -465,6 +465,31 @@ class Problem:
                     root=root)
 
 
+GRAD_FLOOR = 0.1     # absolute floor of the per-branch error, in units of rms(gradient)
+
+
+def gradient_errors(g, gref):
+    """Errors of a branch gradient against a reference gradient.
+
+    ``branch``: the worst per-branch relative error,
+    max_b |g_b - gref_b| / (|gref_b| + 0.1 rms(gref)).  Branch b's own
+    magnitude sets its bar; the floor of a tenth of the gradient's rms only
+    keeps a branch whose reference derivative sits near zero (a sum over
+    patterns that cancels) from dividing by nothing.
+    ``branch_unfloored``: max_b |g_b - gref_b| / |gref_b| over branches with
+    gref_b != 0.  ``max_norm``: max_b |g_b - gref_b| / max_b |gref_b|."""
+    g = np.asarray(g, dtype=np.float64)
+    r = np.asarray(gref, dtype=np.float64)
+    d = np.abs(g - r)
+    rms = float(np.sqrt(np.mean(r * r))) if r.size else 0.0
+    floor = max(GRAD_FLOOR * rms, 1e-300)
+    nz = r != 0
+    return {"branch": float(np.max(d / (np.abs(r) + floor))) if r.size else 0.0,
+            "branch_unfloored": float(np.max(d[nz] / np.abs(r[nz]))) if nz.any() else 0.0,
+            "max_norm": float(np.max(d) / max(float(np.max(np.abs(r))), 1e-300))
+            if r.size else 0.0}
+
+
 def make_problem(S, N, P, C, seed, mean_length=0.1, ambiguous=0.0, rescale=False,
                  alpha=0.5, weights=(1, 5), name=""):
     """Build a Problem: random-join tree, Exp(mean_length) branch lengths, a

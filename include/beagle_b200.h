@@ -363,6 +363,19 @@ int beagleB200GetSiteDerivatives(int instance, double* outFirstDerivatives,
  * The stream belongs to the instance and lives until it is finalised. */
 int beagleB200GetCudaStream(int instance, void** outStream);
 
+/* No counterpart in the reference (whose CUDA error path exits the process,
+ * GPU/GPUInterfaceCUDA.cpp:98-104).  Every wait in this library's kernels (on
+ * tensor-core completion or on bulk copies) is bounded; a wait that runs out
+ * sets a device flag, the kernel finishes without its result, and the next
+ * result call (getters, waitForPartials, synchronous calls) returns
+ * BEAGLE_B200_ERROR_GENERAL, clears the flag and drops that evaluation's
+ * pending results; the instance stays usable.  This call raises that flag on
+ * the instance's stream as if a wait had run out (which = 0: tensor-core
+ * kernels, 1: the bulk-copy derivative), so that a caller can exercise its
+ * error path without a real time-out.  BEAGLE_B200_ERROR_OUT_OF_RANGE for
+ * another `which` or while capturing. */
+int beagleB200InjectKernelTimeout(int instance, int which);
+
 /* No counterpart in the reference.  The pattern-weighted root log-likelihood
  * of caller-owned device buffers, for callers that cannot let a library call
  * cudaMalloc: frameworks that own all device memory through their own
@@ -377,15 +390,19 @@ int beagleB200GetCudaStream(int instance, void** outStream);
  *   rootPartials            [patternCount][categoryCount][Sg], Sg = stateCount
  *                           rounded up to a multiple of 4 (this library's
  *                           partials layout); float if doublePrecision == 0,
- *                           else double
+ *                           else double; 16-byte aligned (rows are read as
+ *                           16-byte vectors)
  *   categoryWeights         [categoryCount]     stateFrequencies  [stateCount]
  *   cumulativeScaleFactors  [patternCount] log scale factors, or NULL
  *   patternWeights          [patternCount]
  *   outSiteLogLikelihoods   [patternCount]      outSumLogLikelihood  [1]
+ * The FP64 arrays must be 8-byte aligned.  A misaligned pointer returns
+ * BEAGLE_B200_ERROR_OUT_OF_RANGE before anything is queued.
  * The work is queued on `stream` (a cudaStream_t; NULL = the default stream)
- * and the call returns without waiting.  The first call on a device looks up
- * the scratch array's device address; make that first call before any stream
- * capture.  Every call shares the array, so calls that overlap on the GPU race:
+ * and the call returns without waiting.  Every call looks up the scratch
+ * array's device address in the current context; the first call on a device
+ * may load the library's device code to do so, so make that first call before
+ * any stream capture.  Every call shares the array, so calls that overlap on the GPU race:
  * order them on one stream.  Calls from different host threads that target the
  * same device must not overlap either. */
 int beagleB200RootLogLikelihoodsNoAlloc(int device, void* stream, const void* rootPartials,
@@ -421,8 +438,12 @@ int beagleB200LaunchGraph(int instance, int graph);
  * the captured updates' lengths, in capture order), then launches the graph,
  * so that a whole step -- P(t), partials, scaling, root lnL, pre-order
  * partials, derivatives -- is one call and one wait.  The lengths are copied
- * before the call returns, and stay: beagleB200LaunchGraph replays the lengths
- * last given (the capture's until this call replaces them).
+ * on the host (into pinned staging memory the graph owns) before the call
+ * returns, so the caller may overwrite its array at once, pinned or not; they
+ * stay: beagleB200LaunchGraph replays the lengths last given (the capture's
+ * until this call replaces them).  Only the transition-matrix updates read
+ * their lengths on the device: a captured beagleB200CalculateCrossProductDerivative
+ * keeps the branch lengths it was captured with.
  * BEAGLE_B200_ERROR_OUT_OF_RANGE when count does not match the capture. */
 int beagleB200LaunchGraphWithLengths(int instance, int graph, const double* lengths, int count);
 

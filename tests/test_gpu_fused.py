@@ -83,8 +83,11 @@ def test_fused_without_sibling_pairs(b200, syn, precision):
 def test_fused_long_lists_and_other_state_counts(b200, syn, oracle, monkeypatch, precision, S,
                                                  N):
     """More than 256 ops (N = 150: 298; N = 300: 598): the fused walk (forced)
-    runs as consecutive launches cut between sibling pairs; S != 4 runs the
-    two separate calls.  Same results as the separate calls and the oracle."""
+    runs as consecutive launches cut between sibling pairs.  S = 20 runs the
+    tensor-core fused walk in FP32 (its derivative from the unscaled row and
+    split products, so it agrees with the separate calls to the mixed path's
+    tolerance) and the two separate calls in FP64.  Same results as the
+    separate calls and the oracle."""
     monkeypatch.setenv("BEAGLE_B200_FORCE_VARIANT", "-1,-1,-1,1")
     pr = syn.make_problem(S=S, N=N, P=500, C=4, seed=7 + S + N, rescale=True)
     inst = _pair(b200, pr, precision)
@@ -96,7 +99,8 @@ def test_fused_long_lists_and_other_state_counts(b200, syn, oracle, monkeypatch,
     # the fused post-order call: its FP64 sums run in another order, and the
     # separate call's autotuner may have picked another post-order kernel shape
     assert rel(l1, l0) <= (1e-13 if precision == "double" else 1e-6)
-    assert grad_err(g1, g0) <= (1e-12 if precision == "double" else tol["grad"] * 1e-2)
+    assert grad_err(g1, g0) <= (1e-12 if precision == "double" else
+                                tol["grad"] * (1e-2 if S == 4 else 1.0))
     if S == 4:
         assert inst.tunedVariants()["fused"] == 1      # the fused walk ran
     _, lo, go = run_oracle(oracle, pr)

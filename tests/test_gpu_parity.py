@@ -113,21 +113,28 @@ def test_edge_loglikelihood_and_derivatives(b200, syn, oracle, precision):
     res = []
     # edge between node v's pre-order partials and its post-order partials
     v = pr.N + 1
+    w = pr.B + 1 + (v + 1) % pr.B          # a spare matrix for d2P/dt2 of branch v
     for x in (inst, oi):
         pr.load(x)
         idx = np.arange(pr.B)
         x.updateTransitionMatrices(0, idx, idx + pr.B + 1, None, pr.lengths)
-        # matrix indices B+1.. hold dP/dt here
+        # matrix indices B+1.. hold dP/dt here; branch v's d2P/dt2 goes to w
+        x.updateTransitionMatrices(0, [v], [v + pr.B + 1], [w], [pr.lengths[v]])
         x.updatePartials(pr.post_ops())
         x.calculateRootLogLikelihoods([pr.root], [0], [0], [-1])
         pr.set_root_pre(x)
         x.updatePrePartials(pr.pre_ops(False))
         res.append(x.calculateEdgeLogLikelihoods(pr.pre(int(pr.parent[v])), v, v,
                                                  v + pr.B + 1, None, 0, 0, -1))
-    (c0, l0, d0, _), (c1, l1, d1, _) = res
+        res.append(x.calculateEdgeLogLikelihoods(pr.pre(int(pr.parent[v])), v, v,
+                                                 v + pr.B + 1, w, 0, 0, -1))
+    (_, l0, d0, _), (_, l0b, d0b, e0), (_, l1, d1, _), (_, l1b, d1b, e1) = res
     tol = TOL[precision]
-    assert rel(l0, l1) <= tol["lnl"]
+    assert rel(l0, l1) <= tol["lnl"] and rel(l0b, l1b) <= tol["lnl"]
     assert abs(d0 - d1) <= tol["grad"] * max(1.0, abs(d1))
+    assert abs(d0b - d1b) <= tol["grad"] * max(1.0, abs(d1b))
+    # the second derivative (edge lnL with d1 and d2 in one call)
+    assert abs(e0 - e1) <= tol["grad"] * max(1.0, abs(e1)), (e0, e1)
 
 
 def test_missing_states_and_ragged_patterns(b200, syn, oracle):

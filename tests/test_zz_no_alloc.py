@@ -71,6 +71,27 @@ def test_no_alloc_matches_instance_path(b200, syn, precision, S):
         assert np.max(np.abs(s - site) / np.abs(site)) <= 100 * TOL[precision]["lnl"]
 
 
+def test_no_alloc_rejects_misaligned_partials(b200):
+    """An offset view of the root partials (8 bytes into an allocation) is
+    refused before any launch: the rows are read as 16-byte vectors."""
+    import torch
+    dev = torch.device("cuda:0")
+    P, C, S = 256, 2, 4
+    rootd = torch.ones(P * C * S + 2, dtype=torch.float64, device=dev)
+    w = torch.full((max(P, S, C),), 0.25, dtype=torch.float64, device=dev)
+    out = torch.zeros(P + 1, dtype=torch.float64, device=dev)
+    fn = b200.lib.beagleB200RootLogLikelihoodsNoAlloc
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                   ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 6
+    p = ctypes.c_void_p
+    code = fn(0, None, p(rootd.data_ptr() + 8), 1, S, P, C, p(w.data_ptr()), p(w.data_ptr()),
+              None, p(w.data_ptr()), p(out.data_ptr()), p(out.data_ptr() + 8 * P))
+    assert code == -5
+    torch.cuda.synchronize(dev)
+    assert float(out.abs().sum().item()) == 0.0      # nothing was written
+
+
 def test_no_alloc_rejects_too_many_patterns(b200):
     fn = b200.lib.beagleB200RootLogLikelihoodsNoAlloc
     fn.restype = ctypes.c_int
