@@ -543,6 +543,8 @@ _BATCH_SIGS = {
     "BatchCalculateRootLogLikelihoods": [_i, _p, _p, _p, _p, _p],
     "BatchCalculateEdgeDerivatives": [_i, _p, _p, _p, _p, _p, _p, _p],
     "BatchWait": [_i],
+    "BatchUpdatePrePartialsWithDerivatives": [_i, _p, _p, _p, _p, _p, _p, _p],
+    "BatchLaunchGraphWithLengths": [_i, _i, _p, _i],
 }
 
 
@@ -637,6 +639,28 @@ class Batch:
 
     def launchGraph(self, graph):
         return self._call("BatchLaunchGraph", graph)
+
+    def launchGraphWithLengths(self, graph, lengths):
+        """New branch lengths for the graph's captured matrix updates (all of
+        them, members in batch order), then the graph."""
+        t = _f64(lengths)
+        return self._call("BatchLaunchGraphWithLengths", graph, _ptr(t), len(t))
+
+    def updatePrePartialsWithDerivatives(self, ops, post, dmat, cw):
+        """Per member: the pre-order ops with each op's branch derivative
+        (post-order operand post[i][k], derivative matrix dmat[i][k]); returns
+        (sums, sums of squares) per member, in op order, filled at wait() for
+        ASYNCH members."""
+        ot, k1 = self._ptrs([np.asarray(o).reshape(-1) for o in ops], np.int32)
+        cnt = _i32([np.asarray(o).size // 7 for o in ops])
+        pt, k2 = self._ptrs(post, np.int32)
+        dt, k3 = self._ptrs(dmat, np.int32)
+        st, k4 = self._ptrs([np.zeros(int(c)) for c in cnt], np.float64)
+        qt, k5 = self._ptrs([np.zeros(int(c)) for c in cnt], np.float64)
+        self._call("BatchUpdatePrePartialsWithDerivatives", ot, _ptr(cnt), pt, dt, _ptr(_i32(cw)),
+                   st, qt)
+        self._keep_result(k4, k5)
+        return k4, k5
 
     def _keep_result(self, *arrays):
         """Result arrays stay alive until the wait() that fills them (ASYNCH

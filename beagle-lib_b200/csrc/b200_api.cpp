@@ -542,6 +542,30 @@ int beagleB200BatchCalculateEdgeDerivatives(int batch, const int* const* post,
     });
 }
 
+int beagleB200BatchUpdatePrePartialsWithDerivatives(int batch, const int* const* operations,
+                                                    const int* counts,
+                                                    const int* const* postBufferIndices,
+                                                    const int* const* derivativeMatrixIndices,
+                                                    const int* categoryWeightsIndices,
+                                                    double* const* outSumDerivatives,
+                                                    double* const* outSumSquaredDerivatives) {
+    if (!operations || !counts || !postBufferIndices || !derivativeMatrixIndices ||
+        !categoryWeightsIndices || !outSumDerivatives || !outSumSquaredDerivatives)
+        return BEAGLE_B200_ERROR_OUT_OF_RANGE;
+    return call_batch(batch, [&](b200::Batch* b) {
+        return b->preDerivatives(operations, counts, postBufferIndices, derivativeMatrixIndices,
+                                 categoryWeightsIndices, outSumDerivatives,
+                                 outSumSquaredDerivatives);
+    });
+}
+
+int beagleB200BatchLaunchGraphWithLengths(int batch, int graph, const double* lengths,
+                                          int count) {
+    return call_batch(batch, [&](b200::Batch* b) {
+        return b->launchGraphWithLengths(graph, lengths, count);
+    });
+}
+
 int beagleB200BatchBeginCapture(int batch) {
     return call_batch(batch, [&](b200::Batch* b) { return b->beginCapture(); });
 }

@@ -157,7 +157,16 @@ int Batch::beginCapture() {
     int rc = sync();
     if (rc) return rc;
     cap_ = GraphRec{};
-    CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed));
+    // room for the captured matrix updates' branch lengths (allocated before
+    // the capture starts: the graph keeps the address)
+    for (Instance* in : m_) cap_.len_cap += 4 * in->nmat_;
+    CK(cudaMalloc(&cap_.d_len, sizeof(double) * std::max(cap_.len_cap, 1)));
+    const cudaError_t e = cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        free_graph(cap_);
+        return kErrGeneral;
+    }
     capturing_ = true;
     capture_pinned() = &cap_.pinned;
     for (Instance* in : m_) {
@@ -188,10 +197,45 @@ int Batch::endCapture(int* graph) {
         free_graph(cap_);
         return kErrGeneral;
     }
+    if (!cap_.len.empty()) {
+        e = cudaMemcpy(cap_.d_len, cap_.len.data(), sizeof(double) * cap_.len.size(),
+                       cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMallocHost(&cap_.h_len_ring,
+                               sizeof(double) * cap_.len.size() * GraphRec::kLenRing);
+        for (int k = 0; k < GraphRec::kLenRing && e == cudaSuccess; ++k)
+            e = cudaEventCreateWithFlags(&cap_.len_ev[k], cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            (void)cudaGetLastError();
+            free_graph(cap_);
+            return kErrGeneral;
+        }
+    }
     graphs_.push_back(std::move(cap_));
     cap_ = GraphRec{};
     *graph = (int)graphs_.size() - 1;
     return kSuccess;
+}
+
+// The lengths are copied on the host into one of the graph's pinned slots
+// before this call returns; the slot's copy to the device is stream-ordered
+// before the launch, and a slot is rewritten only after its last copy ran.
+int Batch::launchGraphWithLengths(int graph, const double* lengths, int count) {
+    if (capturing_ || graph < 0 || graph >= (int)graphs_.size() || !graphs_[graph].exec)
+        return kErrRange;
+    GraphRec& g = graphs_[graph];
+    if (!g.len_all || count != (int)g.len.size() || (count > 0 && !lengths)) return kErrRange;
+    if (count > 0) {
+        const int k = g.ring_i;
+        g.ring_i = (k + 1) % GraphRec::kLenRing;
+        CK(cudaEventSynchronize(g.len_ev[k]));
+        double* slot = g.h_len_ring + (size_t)k * count;
+        std::copy(lengths, lengths + count, slot);
+        CK(cudaMemcpyAsync(g.d_len, slot, sizeof(double) * count, cudaMemcpyHostToDevice,
+                           stream_));
+        CK(cudaEventRecord(g.len_ev[k], stream_));
+    }
+    return launchGraph(graph);
 }
 
 int Batch::launchGraph(int graph) {
@@ -210,6 +254,10 @@ void Batch::free_graph(GraphRec& g) {
     if (g.exec) cudaGraphExecDestroy(g.exec);
     if (g.graph) cudaGraphDestroy(g.graph);
     for (void* p : g.pinned) cudaFreeHost(p);
+    if (g.d_len) cudaFree(g.d_len);
+    for (cudaEvent_t ev : g.len_ev)
+        if (ev) cudaEventDestroy(ev);
+    if (g.h_len_ring) cudaFreeHost(g.h_len_ring);
     g = GraphRec{};
 }
 
@@ -225,6 +273,17 @@ int Batch::updateTransitionMatrices(const int* eig, const int* const* prob,
         const int rc = in->build_matrix_jobs(e.data(), r.data(), prob[i], nullptr, nullptr, t[i],
                                              counts[i], jobs);
         if (rc) return rc;
+        if (capturing_ && cap_.d_len) {
+            // the graph reads these lengths from d_len (launchGraphWithLengths)
+            if ((int)(cap_.len.size() + jobs.size()) > cap_.len_cap) {
+                cap_.len_all = false;
+            } else {
+                for (MatJob& j : jobs) {
+                    j.tlen = cap_.d_len + cap_.len.size();
+                    cap_.len.push_back(j.t);
+                }
+            }
+        }
         auto& g = groups[std::make_tuple(in->S_, in->Sg_, in->C_)];
         g.insert(g.end(), jobs.begin(), jobs.end());
     }
@@ -652,6 +711,192 @@ int Batch::edgeDerivatives(const int* const* post, const int* const* pre,
         const int i = mo.first, nb = counts[i];
         if (sums[i]) push_pending(Pending{h + mo.second, sums[i], (size_t)nb, -1});
         if (sumsq[i]) push_pending(Pending{h + mo.second + nb, sumsq[i], (size_t)nb, -1});
+    }
+    if (deferred()) return kSuccess;   // delivered by wait()
+    return sync();
+}
+
+// ------------------------------------- fused pre-order walk + derivatives
+// Per member, updatePrePartialsWithDerivatives(ops, post, dmat, cw): the
+// pre-order walk and the edge derivatives of its branches, sums in op order.
+// 4-state members with 1, 2, 4 or 8 categories run the batched fused walk
+// (one launch per category count); FP32 members with 4 < S <= 64 run the
+// batched tensor-core fused walk (one launch per (S, C) group); any other
+// member, or a list the fused walks cannot take, runs its own call on the
+// shared stream.
+int Batch::preDerivatives(const int* const* ops, const int* counts, const int* const* post,
+                          const int* const* dmat, const int* cw, double* const* sums,
+                          double* const* sumsq) {
+    const int n = size();
+    struct Member {
+        int i;
+        size_t a_off;     // fused op list (S = 4) or walk table (tensor cores)
+        size_t d_off;     // derivative table (tensor cores)
+        int nops;
+    };
+    std::map<int, std::vector<Member>> groups;                           // C -> 4-state
+    std::map<std::tuple<int, int, int>, std::vector<Member>> tcgroups;   // (S, Sg, C)
+    std::vector<unsigned char> table;
+    std::vector<int> fallback;
+    for (int i = 0; i < n; ++i) {
+        Instance* in = m_[i];
+        if (counts[i] < 0) return kErrRange;
+        if (counts[i] == 0) continue;
+        std::vector<OpDesc> tab;
+        std::vector<DerivDesc> dtab;
+        std::vector<PreDerivOp> fops;
+        bool idem = false;
+        const int rc = in->build_prederiv(ops[i], counts[i], post[i], dmat[i], &cw[i], tab, dtab,
+                                          fops, idem);
+        if (rc == Instance::kNotFused) {
+            fallback.push_back(i);
+            continue;
+        }
+        if (rc) return rc;
+        if (in->S_ == 4) {
+            if (!batched4(in, in->S_, in->C_)) {
+                fallback.push_back(i);
+                continue;
+            }
+            groups[in->C_].push_back(Member{i, append(table, fops), 0, counts[i]});
+        } else {
+            const size_t a = append(table, tab);
+            tcgroups[std::make_tuple(in->S_, in->Sg_, in->C_)].push_back(
+                Member{i, a, append(table, dtab), counts[i]});
+        }
+    }
+    auto own_call = [&](int i) {
+        return m_[i]->updatePrePartialsWithDerivatives(ops[i], counts[i], post[i], dmat[i], &cw[i],
+                                                       sums[i], sumsq[i]);
+    };
+    for (int i : fallback) {
+        const int rc = own_call(i);
+        if (rc) return rc;
+    }
+    if (groups.empty() && tcgroups.empty()) return kSuccess;
+    CK(t_a_.upload(table.data(), table.size(), stream_));
+    auto nblk_of = [&](const Instance* in) {
+        return in->S_ == 4 ? ceil_div(in->Pp_, pre_deriv4_batch_patterns(in->C_)) * 8
+                           : in->Pp_ / tc_tile_patterns();
+    };
+    size_t blocks = 0, outs = 0;
+    for (auto* grp : {&groups})
+        for (auto& kv : *grp)
+            for (const Member& mb : kv.second) {
+                blocks += (size_t)2 * mb.nops * nblk_of(m_[mb.i]);
+                outs += (size_t)2 * mb.nops;
+            }
+    for (auto& kv : tcgroups)
+        for (const Member& mb : kv.second) {
+            blocks += (size_t)2 * mb.nops * nblk_of(m_[mb.i]);
+            outs += (size_t)2 * mb.nops;
+        }
+    CK(t_block_.reserve(sizeof(double) * blocks));
+    CK(t_out2_.reserve(sizeof(double) * outs));
+    std::vector<unsigned char> segtab;
+    std::vector<FinalSeg> fin;
+    std::vector<std::pair<int, size_t>> out_of;   // (member, first output) in t_out2_
+    size_t boff = 0, ooff = 0;
+    auto seg_of = [&](const Member& mb, int first) {
+        Instance* in = m_[mb.i];
+        PreDerivSeg sg{};
+        const unsigned char* base = (const unsigned char*)t_a_.ptr;
+        if (in->S_ == 4) {
+            sg.fops = (const PreDerivOp*)(base + mb.a_off);
+        } else {
+            sg.ops = (const OpDesc*)(base + mb.a_off);
+            sg.dds = (const DerivDesc*)(base + mb.d_off);
+        }
+        sg.catw = in->d_catw_ + (size_t)cw[mb.i] * in->C_;
+        sg.patw = in->d_patw_;
+        sg.block = (double*)t_block_.ptr + boff;
+        sg.nops = mb.nops;
+        sg.P = in->P_;
+        sg.Pp = in->Pp_;
+        sg.nblk = nblk_of(in);
+        sg.log_scalers = (int)in->log_scalers_;
+        sg.first_cta = first;
+        FinalSeg f{};
+        f.block = sg.block;
+        f.out = (double*)t_out2_.ptr + ooff;
+        f.nblk = sg.nblk;
+        f.nout = 2 * mb.nops;
+        f.first_out = (int)ooff;
+        fin.push_back(f);
+        out_of.emplace_back(mb.i, ooff);
+        boff += (size_t)2 * mb.nops * sg.nblk;
+        ooff += (size_t)2 * mb.nops;
+        return sg;
+    };
+    struct G {
+        int C;
+        size_t off;
+        int nseg;
+        int ncta;
+    };
+    std::vector<G> gl;
+    for (auto& kv : groups) {
+        std::vector<PreDerivSeg> segs;
+        int cta = 0;
+        for (const Member& mb : kv.second) {
+            segs.push_back(seg_of(mb, cta));
+            cta += ceil_div(m_[mb.i]->Pp_, pre_deriv4_batch_patterns(kv.first));
+        }
+        gl.push_back(G{kv.first, append(segtab, segs), (int)segs.size(), cta});
+    }
+    struct TG {
+        Dims d;
+        size_t off;
+        int nseg;
+        int ntiles;
+        std::vector<int> members;
+    };
+    std::vector<TG> tgl;
+    for (auto& kv : tcgroups) {
+        std::vector<PreDerivSeg> segs;
+        TG tg{};
+        tg.d = Dims{std::get<0>(kv.first), std::get<1>(kv.first), 0, 0, std::get<2>(kv.first)};
+        for (const Member& mb : kv.second) {
+            segs.push_back(seg_of(mb, tg.ntiles));
+            tg.ntiles += m_[mb.i]->Pp_ / tc_tile_patterns();
+            tg.members.push_back(mb.i);
+        }
+        tg.off = append(segtab, segs);
+        tg.nseg = (int)segs.size();
+        tgl.push_back(tg);
+    }
+    const size_t foff = append(segtab, fin);
+    CK(t_b_.upload(segtab.data(), segtab.size(), stream_));
+    for (const G& g : gl)
+        CK(LAUNCH(launch_pre_deriv4_batch, (const PreDerivSeg*)((unsigned char*)t_b_.ptr + g.off),
+                  g.nseg, g.ncta, g.C, stream_));
+    std::vector<int> late;   // tensor-core groups that cannot launch here: own calls
+    for (const TG& g : tgl) {
+        const cudaError_t e = launch_prederiv_tc_batch(
+            (const PreDerivSeg*)((unsigned char*)t_b_.ptr + g.off), g.nseg, g.ntiles, g.d,
+            stream_);
+        if (e == cudaErrorInvalidConfiguration) {
+            (void)cudaGetLastError();
+            late.insert(late.end(), g.members.begin(), g.members.end());
+            continue;
+        }
+        CK(e);
+        for (int i : g.members) m_[i]->tc_used_ = true;
+    }
+    CK(launch_final_batch((const FinalSeg*)((unsigned char*)t_b_.ptr + foff), (int)fin.size(),
+                          (int)ooff, stream_));
+    double* h = stage(ooff);
+    if (!h) return kErrOOM;
+    CK(cudaMemcpyAsync(h, t_out2_.ptr, sizeof(double) * ooff, cudaMemcpyDeviceToHost, stream_));
+    for (const auto& mo : out_of) {
+        const int i = mo.first, nb = counts[i];
+        if (std::find(late.begin(), late.end(), i) != late.end()) continue;
+        if (sums[i]) push_pending(Pending{h + mo.second, sums[i], (size_t)nb, -1});
+        if (sumsq[i]) push_pending(Pending{h + mo.second + nb, sumsq[i], (size_t)nb, -1});
+    }
+    for (int i : late) {
+        const int rc = own_call(i);
+        if (rc) return rc;
     }
     if (deferred()) return kSuccess;   // delivered by wait()
     return sync();

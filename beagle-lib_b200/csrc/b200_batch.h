@@ -39,6 +39,9 @@ public:
     int edgeDerivatives(const int* const* post, const int* const* pre,
                         const int* const* dmat, const int* cw, const int* counts,
                         double* const* sums, double* const* sumsq);
+    int preDerivatives(const int* const* ops, const int* counts, const int* const* post,
+                       const int* const* dmat, const int* cw, double* const* sums,
+                       double* const* sumsq);
     // Wait for the batch's queued work and deliver deferred results.
     int wait();
     // CUDA graph of the calls between beginCapture and endCapture (every
@@ -46,6 +49,9 @@ public:
     int beginCapture();
     int endCapture(int* graph);
     int launchGraph(int graph);
+    // New branch lengths for the graph's captured matrix updates (count = all
+    // of them, in capture order), then launchGraph.
+    int launchGraphWithLengths(int graph, const double* lengths, int count);
     // Members back on their own streams.
     void release();
 
@@ -70,6 +76,18 @@ private:
         std::vector<Pending> deliveries;
         std::vector<std::pair<int, std::vector<Instance::Pending>>> member_deliveries;
         std::vector<void*> pinned;
+        // branch lengths of the captured transition-matrix updates, read by
+        // the graph from d_len (capture order: members in batch order, each
+        // member's lengths in its call order); replaced per launch by
+        // launchGraphWithLengths through a ring of pinned staging slots
+        double* d_len = nullptr;
+        int len_cap = 0;
+        std::vector<double> len;
+        bool len_all = true;
+        static constexpr int kLenRing = 4;
+        double* h_len_ring = nullptr;
+        cudaEvent_t len_ev[kLenRing] = {};
+        int ring_i = 0;
     };
     std::vector<GraphRec> graphs_;
     GraphRec cap_;

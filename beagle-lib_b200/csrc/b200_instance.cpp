@@ -1391,36 +1391,37 @@ int Instance::deliver_sums(int count, double* outDerivs, double* outSum, double*
 // destination written twice, or a post-order operand that is also a
 // destination).  Otherwise the two calls run as they are; where the fused
 // walk can run, the autotuner picks it or the two calls' kernels by time.
-int Instance::updatePrePartialsWithDerivatives(const int* ops, int count, const int* post,
-                                               const int* dmat, const int* cw, double* outSum,
-                                               double* outSumSq) {
+// Resolve the fused call's list: the pre-order walk table `tab`, the
+// derivative table `dtab` and, for S = 4, the fused op list `fops` with its
+// sibling-pair marks.  Returns kSuccess, kNotFused when only the two
+// separate calls can run the list (no fused kernel for this shape, an op
+// rewriting a buffer that an earlier op's derivative reads: a destination
+// written twice, or a post-order operand that is also a destination), or an
+// error code.
+int Instance::build_prederiv(const int* ops, int count, const int* post, const int* dmat,
+                             const int* cw, std::vector<OpDesc>& tab,
+                             std::vector<DerivDesc>& dtab, std::vector<PreDerivOp>& fops,
+                             bool& idempotent) {
     if (count < 0 || (count > 0 && (!ops || !post || !dmat || !cw))) return kErrRange;
-    std::vector<int> pre(count);
-    for (int k = 0; k < count; ++k) pre[k] = ops[(size_t)k * 7];
-    auto separate = [&]() -> int {
-        int rc = updatePrePartials(ops, count, -1);
-        if (rc) return rc;
-        return calculateEdgeDerivatives(post, pre.data(), dmat, cw, count, nullptr, outSum,
-                                        outSumSq);
-    };
     const Dims dm = dims();
     const bool tc_fused = !dbl_ && tc_supported(dm);
-    if (count == 0 || !(fused_supported(dm, count) || tc_fused)) return separate();
-    std::vector<OpDesc> tab;
+    if (count == 0 || !(fused_supported(dm, count) || tc_fused)) return kNotFused;
+    std::vector<int> pre(count);
+    for (int k = 0; k < count; ++k) pre[k] = ops[(size_t)k * 7];
     std::vector<uint8_t> dep;
-    bool idempotent = false, has_op_cum = false;
+    bool has_op_cum = false;
+    idempotent = false;
     int rc = build_walk(ops, count, 7, true, tab, dep, idempotent, has_op_cum);
     if (rc) return rc;
-    std::vector<DerivDesc> dtab;
     rc = build_deriv(post, pre.data(), dmat, cw, count, dtab);
     if (rc) return rc;
     std::unordered_map<int, int> writes;
     for (int k = 0; k < count; ++k) ++writes[pre[k]];
     for (int k = 0; k < count; ++k)
-        if (writes[pre[k]] != 1 || writes.count(post[k])) return separate();
-    if (S_ != 4) return prederiv_tc(ops, count, post, pre.data(), dmat, cw, tab, dtab,
-                                    idempotent, outSum, outSumSq);
-    std::vector<PreDerivOp> fops(count);
+        if (writes[pre[k]] != 1 || writes.count(post[k])) return kNotFused;
+    fops.clear();
+    if (S_ != 4) return kSuccess;
+    fops.resize(count);
     for (int k = 0; k < count; ++k) {
         const OpDesc& t = tab[k];
         const DerivDesc& d = dtab[k];
@@ -1456,6 +1457,31 @@ int Instance::updatePrePartialsWithDerivatives(const int* ops, int count, const 
             ++k;
         }
     }
+    return kSuccess;
+}
+
+int Instance::updatePrePartialsWithDerivatives(const int* ops, int count, const int* post,
+                                               const int* dmat, const int* cw, double* outSum,
+                                               double* outSumSq) {
+    if (count < 0 || (count > 0 && (!ops || !post || !dmat || !cw))) return kErrRange;
+    std::vector<int> pre(count);
+    for (int k = 0; k < count; ++k) pre[k] = ops[(size_t)k * 7];
+    auto separate = [&]() -> int {
+        int rc = updatePrePartials(ops, count, -1);
+        if (rc) return rc;
+        return calculateEdgeDerivatives(post, pre.data(), dmat, cw, count, nullptr, outSum,
+                                        outSumSq);
+    };
+    std::vector<OpDesc> tab;
+    std::vector<DerivDesc> dtab;
+    std::vector<PreDerivOp> fops;
+    bool idempotent = false;
+    const int rc = build_prederiv(ops, count, post, dmat, cw, tab, dtab, fops, idempotent);
+    if (rc == kNotFused) return separate();
+    if (rc) return rc;
+    const Dims dm = dims();
+    if (S_ != 4) return prederiv_tc(ops, count, post, pre.data(), dmat, cw, tab, dtab,
+                                    idempotent, outSum, outSumSq);
     const int w = cw[0];
     const int nblk = std::max(fused_blocks(dm), deriv_blocks(dm));
     CK(scratch_.reserve(sizeof(double) * 2 * (size_t)count * nblk));

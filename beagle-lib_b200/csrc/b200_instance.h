@@ -160,6 +160,10 @@ private:
     int run_matrix_jobs(const std::vector<MatJob>& jobs);
     int post_or_pre(const int* ops, int count, int stride, int cumulative, bool pre);
     int deliver_sums(int count, double* outDerivs, double* outSum, double* outSumSq);
+    static constexpr int kNotFused = 1;   // build_prederiv: the list needs the separate calls
+    int build_prederiv(const int* ops, int count, const int* post, const int* dmat,
+                       const int* cw, std::vector<OpDesc>& tab, std::vector<DerivDesc>& dtab,
+                       std::vector<PreDerivOp>& fops, bool& idempotent);
     int queue_edge_derivatives(const int* post, const int* pre, const int* dmat, const int* cw,
                                int count, bool site_values);
     int prederiv_tc(const int* ops, int count, const int* post, const int* pre, const int* dmat,

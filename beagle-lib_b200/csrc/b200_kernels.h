@@ -84,6 +84,10 @@ bool deriv_tc_launchable(const Dims& d);
 // the sums of op k into d_block rows k and nsum + k, prederiv_tc_blocks(d)
 // partials each (add them with launch_final_sum).
 int prederiv_tc_blocks(const Dims& d);
+// ... over several instances with one (S, C): segment first_cta counts
+// 128-pattern tiles, ntiles their total; each segment's sums into its block.
+cudaError_t launch_prederiv_tc_batch(const PreDerivSeg* d_segs, int nseg, int ntiles,
+                                     const Dims& d, cudaStream_t s);
 cudaError_t launch_prederiv_tc(const OpDesc* d_ops, const DerivDesc* d_desc, int nops, int nsum,
                                const double* catw, const double* patw, const Dims& d, int ls,
                                double* d_block, cudaStream_t s);
@@ -212,6 +216,15 @@ template <typename Real>
 cudaError_t launch_pre_deriv4(const PreDerivOp* h_ops, int nops, const Dims& d,
                               const double* catw, const double* patw, int ls, double* d_block,
                               double* d_sums, cudaStream_t s, int variant);
+
+// Batched fused pre-order walk + edge derivatives (S = 4, C in {1, 2, 4, 8};
+// k_fused.cu): one CTA per pre_deriv4_batch_patterns(C) patterns of a member;
+// a member's sums of op k into its block rows k and nops + k, nblk = its CTAs
+// x 8 warp partials each.
+int pre_deriv4_batch_patterns(int C);
+template <typename Real>
+cudaError_t launch_pre_deriv4_batch(const PreDerivSeg* d_segs, int nseg, int ncta, int C,
+                                    cudaStream_t s);
 
 // ---- batched launches over several instances (segment tables on the device;
 // ncta = the segments' total CTAs; see b200_types.h) ------------------------

@@ -150,6 +150,22 @@ struct DerivSeg {
     int first_cta;
 };
 
+// One instance's list in a batched fused pre-order + edge-derivative launch.
+struct PreDerivSeg {
+    const PreDerivOp* fops;     // S = 4: the fused op list
+    const OpDesc* ops;          // S > 4 (tensor cores): the pre-order walk table
+    const DerivDesc* dds;       //   ... and the derivative of each op's branch
+    const double* catw;
+    const double* patw;
+    double* block;              // this instance's 2 * nops * nblk block partial sums
+    int nops;
+    int P;
+    int Pp;
+    int nblk;                   // block partials per output
+    int log_scalers;
+    int first_cta;              // S = 4: CTAs; tensor cores: 128-pattern tiles
+};
+
 // One instance's root log-likelihood in a batched launch (any state count).
 struct RootSeg {
     const void* root;

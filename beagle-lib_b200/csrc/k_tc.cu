@@ -1113,18 +1113,37 @@ struct TcFusedGeo {
     static constexpr int COLS = TcGeo<NP>::TCOLS;
 };
 
-template <int NP, int KC>
+// BATCH: a launch over several instances with the same S and C (segs): tile
+// q of the grid belongs to the segment whose tiles hold it, and that
+// segment's lists, weights, pattern count and block partials replace the
+// arguments.
+template <int NP, int KC, bool BATCH>
 __global__ void __launch_bounds__(kTT, 3)
 k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds, int nops,
               int nsum, int S, int Sg, int C, int P, const double* __restrict__ catw,
-              const double* __restrict__ patw, int log_scalers, double* block) {
+              const double* __restrict__ patw, int log_scalers, double* block,
+              const PreDerivSeg* __restrict__ segs, int nseg) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     TcFusedSmem& sm = *reinterpret_cast<TcFusedSmem*>(smem_raw);
     constexpr int COLS = TcFusedGeo<NP>::COLS;
     const int t = threadIdx.x;
     const int c = blockIdx.x % C;
-    const int tile = blockIdx.x / C;
-    const int ntiles = gridDim.x / C;
+    int tile = blockIdx.x / C;
+    int ntiles = gridDim.x / C;
+    if constexpr (BATCH) {
+        const PreDerivSeg& sg = segs[tc_find_seg(segs, nseg, tile)];
+        ops = sg.ops;
+        dds = sg.dds;
+        nops = sg.nops;
+        nsum = sg.nops;
+        P = sg.P;
+        catw = sg.catw;
+        patw = sg.patw;
+        log_scalers = sg.log_scalers;
+        block = sg.block;
+        ntiles = sg.nblk;
+        tile -= sg.first_cta;
+    }
     const int p0 = tile * kTM;
     const int p = p0 + t;
     constexpr int NKC = chunks_of<NP>();
@@ -1405,8 +1424,23 @@ cudaError_t run_prederiv_tc(const OpDesc* ops, const DerivDesc* dds, int nops, i
     const size_t floor_smem = tc_smem(cols);
     const size_t smem = need > floor_smem ? need : floor_smem;
     const int grid = (d.Pp / kTM) * d.C;
-    return launch_tc(k_prederiv_tc<NP, KC>, grid, smem, d.C, cols, s, ops, dds, nops, nsum, d.S,
-                     d.Sg, d.C, d.P, catw, patw, ls, block);
+    const PreDerivSeg* none = nullptr;
+    return launch_tc(k_prederiv_tc<NP, KC, false>, grid, smem, d.C, cols, s, ops, dds, nops, nsum,
+                     d.S, d.Sg, d.C, d.P, catw, patw, ls, block, none, 0);
+}
+
+template <int NP, int KC>
+cudaError_t run_prederiv_tc_batch(const PreDerivSeg* segs, int nseg, int ntiles, const Dims& d,
+                                  cudaStream_t s) {
+    const int cols = TcFusedGeo<NP>::COLS;
+    const size_t need = sizeof(TcFusedSmem) + 1024;
+    const size_t floor_smem = tc_smem(cols);
+    const size_t smem = need > floor_smem ? need : floor_smem;
+    const OpDesc* no_ops = nullptr;
+    const DerivDesc* no_dds = nullptr;
+    const double* no_w = nullptr;
+    return launch_tc(k_prederiv_tc<NP, KC, true>, ntiles * d.C, smem, d.C, cols, s, no_ops, no_dds,
+                     0, 0, d.S, d.Sg, d.C, 0, no_w, no_w, 0, (double*)nullptr, segs, nseg);
 }
 
 // (N, KC) of a padded state count: N = Sg rounded up to 16, KC as above.
@@ -1455,6 +1489,15 @@ cudaError_t launch_prederiv_tc(const OpDesc* d_ops, const DerivDesc* d_desc, int
 #define PD_(NP, KC) run_prederiv_tc<NP, KC>(d_ops, d_desc, nops, nsum, catw, patw, d, ls, d_block, s)
     return B200_TC_DISPATCH(d.Sg, PD_);
 #undef PD_
+}
+
+cudaError_t launch_prederiv_tc_batch(const PreDerivSeg* d_segs, int nseg, int ntiles,
+                                     const Dims& d, cudaStream_t s) {
+    if (nseg == 0 || ntiles == 0) return cudaSuccess;
+    if (!tc_supported(d)) return cudaErrorInvalidValue;
+#define PDB_(NP, KC) run_prederiv_tc_batch<NP, KC>(d_segs, nseg, ntiles, d, s)
+    return B200_TC_DISPATCH(d.Sg, PDB_);
+#undef PDB_
 }
 
 // Whether the tensor-core derivative kernel of this shape can launch without

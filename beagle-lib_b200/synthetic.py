@@ -558,11 +558,7 @@ def batched_problems(count=256, seed=2000, max_patterns=50000):
     return out
 
 
-def batch_evaluate(batch, problems, lengths=None):
-    """One lnL + gradient evaluation of every problem of a batch (members in
-    the same order), the call sequence of Problem.evaluate with one batched
-    call per step.  S > 4 members need PREORDER_TRANSPOSE_AUTO (their pre-order
-    ops carry untransposed matrices).  Returns (lnL[n], [gradient_m])."""
+def _batch_plan(batch, problems):
     plan = getattr(batch, "_plan", None)
     if plan is None or plan["problems"] is not problems:
         n = len(problems)
@@ -578,41 +574,93 @@ def batch_evaluate(batch, problems, lengths=None):
             scales=[np.arange(p.N - 1, dtype=np.int32) for p in problems],
             roots=[p.root for p in problems], roots_pre=[p.pre(p.root) for p in problems],
             pre_idx=[nr + p.pre(0) for nr, p in zip(nonroot, problems)],
+            fnodes=[p.fused_branches().astype(np.int32) for p in problems],
             dmat=[np.full(p.B, p.B, dtype=np.int32) for p in problems], zeros=[0] * n,
             none=[OP_NONE] * n)
+    return plan
+
+
+def batch_gradients(problems, sums, fused):
+    """Per-member gradients in branch order from a batched evaluation's sums
+    (op order with ``fused``)."""
+    if not fused:
+        return [np.asarray(g) for g in sums]
+    return [p.branch_gradient(g) for p, g in zip(problems, sums)]
+
+
+def batch_evaluate(batch, problems, lengths=None, fused=False):
+    """One lnL + gradient evaluation of every problem of a batch (members in
+    the same order), the call sequence of Problem.evaluate with one batched
+    call per step; with ``fused`` the pre-order walk and the derivatives are
+    one beagleB200BatchUpdatePrePartialsWithDerivatives call.  S > 4 members
+    need PREORDER_TRANSPOSE_AUTO (their pre-order ops carry untransposed
+    matrices).  Returns (lnL[n], [gradient_m] in branch order)."""
+    plan = _batch_plan(batch, problems)
     ts = [p.lengths if lengths is None else lengths[i] for i, p in enumerate(problems)]
     batch.updateTransitionMatrices(plan["zeros"], plan["idx"], ts)
-    lnl, sums = _batch_after_matrices(batch, plan)
+    lnl, sums = _batch_after_matrices(batch, plan, fused)
     batch.wait()
-    return lnl, sums
+    return lnl, batch_gradients(problems, sums, fused)
 
 
-def _batch_after_matrices(batch, plan):
+def _batch_after_matrices(batch, plan, fused=False):
     batch.updatePartials(plan["post"], plan["none"])
     if plan["rescale"]:
         batch.accumulateScaleFactors(plan["scales"], plan["cums"], reset=True)
     lnl = batch.calculateRootLogLikelihoods(plan["roots"], plan["zeros"], plan["zeros"],
                                             plan["cums"])
     batch.setRootPrePartials(plan["roots_pre"], plan["zeros"])
+    if fused:
+        sums, _ = batch.updatePrePartialsWithDerivatives(plan["pre"], plan["fnodes"],
+                                                         plan["dmat"], plan["zeros"])
+        return lnl, sums
     batch.updatePrePartials(plan["pre"])
     sums, _ = batch.calculateEdgeDerivatives(plan["idx"], plan["pre_idx"], plan["dmat"],
                                              plan["zeros"])
     return lnl, sums
 
 
-def batch_capture(batch, problems):
+def batch_capture(batch, problems, fused=False):
     """Record one batched evaluation after the transition matrices as a CUDA
     graph of the batch (every member ASYNCH); returns (graph, lnL array,
-    gradient arrays) that each launch fills at the next wait.  Runs the
-    sequence once first, as the capture requires."""
-    batch_evaluate(batch, problems)
+    gradient arrays: branch order, or op order with ``fused``) that each
+    launch fills at the next wait.  Runs the sequence once first, as the
+    capture requires."""
+    batch_evaluate(batch, problems, fused=fused)
     plan = batch._plan
     batch.beginCapture()
     try:
-        lnl, sums = _batch_after_matrices(batch, plan)
+        lnl, sums = _batch_after_matrices(batch, plan, fused)
     finally:
         graph = batch.endCapture()
     return graph, lnl, sums
+
+
+def batch_capture_step(batch, problems, fused=False):
+    """Record one whole batched evaluation, the transition matrices
+    included, as a CUDA graph of the batch; the graph reads the branch
+    lengths on the device and ``batch_evaluate_graph_step`` replaces them per
+    launch.  Returns (graph, lnL array, gradient arrays) as batch_capture."""
+    batch_evaluate(batch, problems, fused=fused)
+    plan = batch._plan
+    batch.beginCapture()
+    try:
+        batch.updateTransitionMatrices(plan["zeros"], plan["idx"],
+                                       [p.lengths for p in problems])
+        lnl, sums = _batch_after_matrices(batch, plan, fused)
+    finally:
+        graph = batch.endCapture()
+    return graph, lnl, sums
+
+
+def batch_evaluate_graph_step(batch, problems, graph, lengths=None):
+    """One batched evaluation through a graph from ``batch_capture_step``: all
+    members' new branch lengths (concatenated in member order) and the graph
+    in one call, then the wait that delivers lnL and the gradients into the
+    captured arrays."""
+    ts = [p.lengths if lengths is None else lengths[i] for i, p in enumerate(problems)]
+    batch.launchGraphWithLengths(graph, np.concatenate(ts))
+    batch.wait()
 
 
 def batch_evaluate_graph(batch, problems, graph, lengths=None):

@@ -538,15 +538,28 @@ def batched_trees(torch, lib, probs, steps, warmup, device=0, reference_members=
     stream = torch.cuda.ExternalStream(insts[0].cudaStream())
     state = {}
 
-    def batched():
-        state["lnl"], state["grad"] = syn.batch_evaluate(batch, probs)
+    def batched(fused):
+        state["lnl"], state["grad"] = syn.batch_evaluate(batch, probs, fused=fused)
 
-    ms_b = timed_batch(torch, stream, batched, steps, warmup)
-    graph, lnl_g, grad_g = syn.batch_capture(batch, probs)
-    ms_g = timed_batch(torch, stream, lambda: syn.batch_evaluate_graph(batch, probs, graph),
-                       steps, warmup)
+    ms_u = timed_batch(torch, stream, lambda: batched(False), steps, warmup)
+    ms_b = timed_batch(torch, stream, lambda: batched(True), steps, warmup)
+    # the whole step (matrices included) as one graph of the batch, launched
+    # with each step's new branch lengths
+    graph, lnl_g, grad_g = syn.batch_capture_step(batch, probs, fused=True)
+    rng = np.random.default_rng(11)
+    steps_t = [[p.lengths * (1.0 + 1e-3 * rng.standard_normal(p.B)) for p in probs]
+               for _ in range(2)]
+    cnt = {"k": 0}
+
+    def graph_step():
+        cnt["k"] += 1
+        syn.batch_evaluate_graph_step(batch, probs, graph, steps_t[cnt["k"] % 2])
+
+    ms_g = timed_batch(torch, stream, graph_step, steps, warmup)
+    syn.batch_evaluate_graph_step(batch, probs, graph)            # the problems' own lengths
     lnl32 = np.array(lnl_g, dtype=np.float64)
-    grad32 = [np.array(g, dtype=np.float64) for g in grad_g]
+    grad32 = [np.array(g, dtype=np.float64)
+              for g in syn.batch_gradients(probs, grad_g, fused=True)]
     graph_err = float(np.max(np.abs(lnl32 - np.asarray(state["lnl"])) / np.abs(lnl32)))
     k_i = max(2, steps // 2)
     ms_i = timed_batch(torch, stream, lambda: per_instance(insts), k_i, 1)
@@ -569,10 +582,17 @@ def batched_trees(torch, lib, probs, steps, warmup, device=0, reference_members=
     e32 = [errors_vs(lnl32[i], grad32[i], lnl64[i], grad64[i]) for i in range(n)]
     rec = {"value": value, "unit": "tree-evals/s", "trees": n, "steps": steps,
            "ms_per_step": ms_g / steps,
-           "how": "batched calls captured once as a CUDA graph of the batch; per step new "
-                  "transition matrices (one batched call), one graph launch, one wait",
+           "how": "the whole batched step (matrices, post-order walks, scaling, root lnL, "
+                  "fused pre-order walks with derivatives) captured once as a CUDA graph of "
+                  "the batch; per step one launch with every tree's new branch lengths, one "
+                  "wait",
            "batched_calls": {"value": n * steps / (ms_b / 1000.0), "unit": "tree-evals/s",
+                             "how": "the same batched calls issued every step",
                              "graph_vs_calls_max_rel_lnl_diff": graph_err},
+           "batched_calls_unfused": {"value": n * steps / (ms_u / 1000.0),
+                                     "unit": "tree-evals/s",
+                                     "how": "pre-order walk and derivatives as two batched "
+                                            "calls"},
            "per_instance_mixed": {"value": n * k_i / (ms_i / 1000.0), "unit": "tree-evals/s"},
            "plain_fp64": {"value": v_64, "unit": "tree-evals/s",
                           "how": "one instance per tree, each its own launches, one stream"},

@@ -510,6 +510,21 @@ int beagleB200BatchCalculateEdgeDerivatives(int batch, const int* const* postBuf
                                             const int* counts,
                                             double* const* outSumDerivatives,
                                             double* const* outSumSquaredDerivatives);
+/* No beagle.h counterpart: beagleB200UpdatePrePartialsWithDerivatives for
+ * every member (operations[i]: counts[i] pre-order ops, postBufferIndices[i]
+ * and derivativeMatrixIndices[i]: the node's post-order operand and
+ * derivative matrix of each op's branch), sums in op order.  4-state members
+ * with 1, 2, 4 or 8 categories run one batched fused walk per category
+ * count; FP32 members with 4 < S <= 64 one batched tensor-core fused walk per
+ * (S, C); other members their own call on the batch's stream.  Results as
+ * beagleB200BatchCalculateEdgeDerivatives delivers them. */
+int beagleB200BatchUpdatePrePartialsWithDerivatives(int batch, const int* const* operations,
+                                                    const int* counts,
+                                                    const int* const* postBufferIndices,
+                                                    const int* const* derivativeMatrixIndices,
+                                                    const int* categoryWeightsIndices,
+                                                    double* const* outSumDerivatives,
+                                                    double* const* outSumSquaredDerivatives);
 /* Batch CUDA graphs (every member ASYNCH): the batch calls between
  * BeginCapture and EndCapture are recorded once as one graph of the batch's
  * stream (batched kernels, members' own launches, table uploads and result
@@ -520,6 +535,17 @@ int beagleB200BatchCalculateEdgeDerivatives(int batch, const int* const* postBuf
 int beagleB200BatchBeginCapture(int batch);
 int beagleB200BatchEndCapture(int batch, int* outGraph);
 int beagleB200BatchLaunchGraph(int batch, int graph);
+/* The branch lengths of the batch's transition-matrix updates captured in the
+ * graph are read on the device when it runs.  This call replaces them, then
+ * launches the graph, so that a whole batched step (matrices included) is
+ * one call and one wait.  `lengths` holds all of them in capture order:
+ * member by member in batch order, each member's lengths in the order its
+ * captured calls listed them; count must match the capture
+ * (BEAGLE_B200_ERROR_OUT_OF_RANGE otherwise).  They are copied on the host
+ * before the call returns; beagleB200BatchLaunchGraph replays the lengths
+ * last given. */
+int beagleB200BatchLaunchGraphWithLengths(int batch, int graph, const double* lengths,
+                                          int count);
 /* Wait for everything queued on the batch's stream and write the deferred
  * results of ASYNCH members. */
 int beagleB200BatchWait(int batch);

@@ -130,3 +130,108 @@ def test_batch_checkpointed_matches_single_instances(b200, pkg, syn, precision, 
     batch.finalize()
     for x in singles + members:
         x.finalize()
+
+
+@pytest.mark.parametrize("asynch", [False, True], ids=["synch", "asynch"])
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_batch_fused_matches_single_instances_and_oracle(b200, pkg, syn, oracle, precision,
+                                                         asynch):
+    """beagleB200BatchUpdatePrePartialsWithDerivatives: the batched fused walks
+    (4-state members with 1/4/8 categories; FP32 20-state members on the
+    tensor cores) and the members' own calls (3 categories; FP64 20 states)
+    against separate single-instance calls and the oracle."""
+    probs = _problems(syn)
+    singles = [_create(b200, pr, precision) for pr in probs]
+    ref = [pr.evaluate(inst, transposed_pre=False) for pr, inst in zip(probs, singles)]
+    members = [_create(b200, pr, precision, asynch) for pr in probs]
+    batch = pkg.binding.Batch(b200, members)
+    tol = TOL[precision]
+    for rep in range(2):
+        lnl, grads = syn.batch_evaluate(batch, probs, fused=True)
+        for k, (l1, g1) in enumerate(ref):
+            assert rel(lnl[k], l1) <= (1e-12 if precision == "double" else tol["lnl"]), k
+            assert grad_err(grads[k], g1) <= (1e-10 if precision == "double" else tol["grad"]), \
+                (k, grad_err(grads[k], g1))
+    for k in (0, 3, len(probs) - 1):
+        _, lo, go = run_oracle(oracle, probs[k])
+        assert rel(lnl[k], lo) <= tol["lnl"]
+        assert grad_err(grads[k], go) <= tol["grad"]
+    batch.finalize()
+    for x in singles + members:
+        x.finalize()
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_batch_whole_step_graph(b200, pkg, syn, precision):
+    """The whole batched step -- transition matrices, post-order walks,
+    scaling, root lnL, the fused pre-order walks with derivatives -- captured
+    once; each launch takes every member's new branch lengths
+    (beagleB200BatchLaunchGraphWithLengths).  Against plain batched
+    evaluations with the same lengths; the caller's length arrays are
+    overwritten right after each launch call (they are copied on the host)."""
+    probs = _problems(syn)
+    plain = pkg.binding.Batch(b200, [_create(b200, pr, precision, True) for pr in probs])
+    graphed = pkg.binding.Batch(b200, [_create(b200, pr, precision, True) for pr in probs])
+    graph, lnl_g, sums_g = syn.batch_capture_step(graphed, probs, fused=True)
+    rng = np.random.default_rng(9)
+    tol = TOL[precision]
+    for step in range(3):
+        ts = [p.lengths * (1 + 0.05 * rng.standard_normal(p.B)) for p in probs]
+        lnl0, g0 = syn.batch_evaluate(plain, probs, lengths=ts, fused=True)
+        flat = np.concatenate(ts)
+        graphed.launchGraphWithLengths(graph, flat)
+        flat[:] = 1e9                         # the call has its own copy
+        graphed.wait()
+        g1 = syn.batch_gradients(probs, sums_g, fused=True)
+        for i in range(len(probs)):
+            assert rel(lnl_g[i], lnl0[i]) <= (1e-12 if precision == "double" else tol["lnl"]), \
+                (step, i)
+            assert grad_err(g1[i], g0[i]) <= (1e-10 if precision == "double" else tol["grad"]), \
+                (step, i)
+    with pytest.raises(pkg.binding.BeagleError):
+        graphed.launchGraphWithLengths(graph, np.ones(3))     # count must match the capture
+    plain.finalize()
+    graphed.finalize()
+
+
+@pytest.mark.slow
+def test_batch_configuration_shapes_checkpointed(b200, pkg, syn, oracle):
+    """Trees drawn as the batched configuration draws them, at its own
+    pattern range (log-uniform 100-50,000): every member with a subtree
+    checkpoint plan, the plans side by side through batched calls on the
+    mixed path, against the same plans one instance at a time on the FP64
+    path, and two members against the oracle."""
+    probs = syn.batched_problems(count=16, seed=2100, max_patterns=50000)
+    plans = [pkg.checkpoint.quick_plan(pr) for pr in probs]
+    assert max(p.P for p in probs) > 20000
+
+    def members(precision, asynch):
+        pref, req = gpu_flags(precision, auto_transpose=True)
+        out = []
+        for pr, pl in zip(probs, plans):
+            inst = b200.create(*pl.create_args(), preferenceFlags=pref | (asynch << 3),
+                               requirementFlags=req)
+            pr.load(inst)
+            out.append(inst)
+        return out
+
+    m32 = members("single", 1)
+    batch = pkg.binding.Batch(b200, m32)
+    lnl32, g32 = pkg.checkpoint.batch_checkpointed_evaluate(batch, plans)
+    lnl32 = np.array(lnl32)
+    g32 = [np.array(g) for g in g32]
+    batch.finalize()
+    for x in m32:
+        x.finalize()
+    m64 = members("double", 0)
+    tol = TOL["single"]
+    for i, (pl, inst) in enumerate(zip(plans, m64)):
+        l64, g64 = pl.evaluate(inst)
+        assert rel(lnl32[i], l64) <= tol["lnl"], (i, lnl32[i], l64)
+        assert grad_err(g32[i], g64) <= tol["grad"], (i, grad_err(g32[i], g64))
+        inst.finalize()
+    small = sorted(range(len(probs)), key=lambda i: probs[i].P * probs[i].N)[:2]
+    for i in small:
+        _, lo, go = run_oracle(oracle, probs[i])
+        assert rel(lnl32[i], lo) <= tol["lnl"]
+        assert grad_err(g32[i], go) <= tol["grad"]
