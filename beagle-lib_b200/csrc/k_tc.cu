@@ -272,6 +272,90 @@ __device__ __forceinline__ void scatter(const float v[][4], float* hi, float* lo
         }
 }
 
+// The 128-byte swizzled K-major layout (what TMA's SWIZZLE_128B writes and
+// smem_desc_sw128 describes), used for chunks of 32 states: row r of a tile
+// is the 128-byte line at r * 128 bytes, and its 16-byte piece kc sits at
+// piece kc ^ (r & 7) of that line; tiles start on 1024-byte boundaries.  Lane
+// l of warp w handles rows 4 w + (l >> 3) + 16 i and piece l & 7, so one
+// warp load covers 4 whole rows (4 x 128 contiguous bytes) and one warp store
+// writes each of those rows' 8 pieces to 8 distinct bank groups of its line.
+template <int NROWS, bool RO>
+__device__ __forceinline__ void gather_sw(float v[][4], const float* src, size_t rstride,
+                                          int nvalid, int k0, int Sg) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r0 = warp * 4 + (lane >> 3), k = k0 + 4 * (lane & 7);
+    const float* base = src + (size_t)r0 * rstride + k;
+#pragma unroll
+    for (int i = 0; i < NROWS / 16; ++i) {
+        float* d = v[i];
+        d[0] = d[1] = d[2] = d[3] = 0.f;
+        if (r0 + 16 * i < nvalid && k < Sg) {
+            const float* g = base + (size_t)(16 * i) * rstride;
+            if (RO) ldg4(g, d);
+            else ld4(g, d);
+        }
+    }
+}
+
+template <int NROWS>
+__device__ __forceinline__ void scatter_sw(const float v[][4], float* hi, float* lo) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r0 = warp * 4 + (lane >> 3), kc = lane & 7;
+    // rows r0 + 16 i share r0 & 7, so every piece lands at the same swizzled column
+    const int off0 = r0 * 32 + ((kc ^ (r0 & 7)) * 4);
+#pragma unroll
+    for (int i = 0; i < NROWS / 16; ++i) {
+        float h4[4], l4[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) split_tf32(v[i][q], h4[q], l4[q]);
+        st4(hi + off0 + i * 16 * 32, h4);
+        st4(lo + off0 + i * 16 * 32, l4);
+    }
+}
+
+// Row t of an A tile (swizzled layout) from registers: z[Q 32 .. Q 32 + 32).
+template <int NP, int Q>
+__device__ __forceinline__ void store_row_sw128(float* hi, float* lo, const float z[NP]) {
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int kc = 0; kc < 8; ++kc) {
+        float h4[4], l4[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int k = Q * 32 + kc * 4 + q;
+            split_tf32(k < NP ? z[k < NP ? k : 0] : 0.f, h4[q], l4[q]);
+        }
+        const int off = t * 32 + ((kc ^ (t & 7)) * 4);
+        st4(hi + off, h4);
+        st4(lo + off, l4);
+    }
+}
+
+// Shared-memory descriptor of a K-major tile with 128-byte swizzle (sm100
+// layout type 2): rows of 128 bytes, 8-row groups 1024 bytes apart.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr) {
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;                       // leading byte offset (unused here)
+    d |= (uint64_t)((1024u >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
+    return d;
+}
+
+// Chunk helpers for either layout: KC == 32 uses the swizzled layout.
+template <int NROWS, int KC, bool RO>
+__device__ __forceinline__ void gather_any(float v[][4], const float* src, size_t rstride,
+                                           int nvalid, int k0, int Sg) {
+    if constexpr (KC == 32) gather_sw<NROWS, RO>(v, src, rstride, nvalid, k0, Sg);
+    else gather<NROWS, KC, RO>(v, src, rstride, nvalid, k0, Sg);
+}
+
+template <int NROWS, int KC>
+__device__ __forceinline__ void scatter_any(const float v[][4], float* hi, float* lo) {
+    if constexpr (KC == 32) scatter_sw<NROWS>(v, hi, lo);
+    else scatter<NROWS, KC>(v, hi, lo);
+}
+
 // One K chunk in flight: this lane's pieces of A and of B.
 struct ChunkRegs {
     float a[8][4];
@@ -290,8 +374,8 @@ struct Job {
 
 template <int NP, int KC>
 __device__ __forceinline__ void gather_job(ChunkRegs& cr, const Job& jb, size_t xs, int Sg) {
-    gather<kTM, KC, false>(cr.a, jb.x, xs, kTM, jb.q * KC, Sg);
-    gather<NP, KC, true>(cr.b, jb.m, Sg, Sg, jb.q * KC, Sg);
+    gather_any<kTM, KC, false>(cr.a, jb.x, xs, kTM, jb.q * KC, Sg);
+    gather_any<NP, KC, true>(cr.b, jb.m, Sg, Sg, jb.q * KC, Sg);
 }
 
 // Row t of A chunk Q from registers: z[Q KC .. Q KC + KC).  Compile-time
@@ -319,6 +403,23 @@ __device__ __forceinline__ void store_row(float* hi, float* lo, const float z[NP
 template <int KC, typename SM>
 __device__ __forceinline__ void issue_chunk(SM& sm, uint32_t d_tmem, int N, bool first) {
     const uint32_t idesc = idesc_tf32(kTM, N);
+    if constexpr (KC == 32) {
+        // swizzled tiles: 4 K steps of 8 tf32 (32 bytes) along each 128-byte row
+        const uint32_t ah = smem_u32(sm.a_hi), al = smem_u32(sm.a_lo);
+        const uint32_t bh = smem_u32(sm.b_hi), bl = smem_u32(sm.b_lo);
+        tc_fence_after();
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t o = (uint32_t)k * 32u;
+            const uint64_t dah = smem_desc_sw128(ah + o), dal = smem_desc_sw128(al + o);
+            const uint64_t dbh = smem_desc_sw128(bh + o), dbl = smem_desc_sw128(bl + o);
+            mma_tf32(d_tmem, dah, dbh, idesc, (first && k == 0) ? 0u : 1u);
+            mma_tf32(d_tmem, dah, dbl, idesc, 1u);
+            mma_tf32(d_tmem, dal, dbh, idesc, 1u);
+        }
+        mma_commit(&sm.bar);
+        return;
+    }
     const uint32_t ah = smem_u32(sm.a_hi), al = smem_u32(sm.a_lo);
     const uint32_t bh = smem_u32(sm.b_hi), bl = smem_u32(sm.b_lo);
     constexpr uint32_t sbo = (uint32_t)KC * 32u;   // bytes between 8-row groups
@@ -362,8 +463,8 @@ __device__ __forceinline__ void run_jobs(SM& sm, Pipe& pp, uint32_t tmem, const 
     for (int i = 0; i < 4; ++i) {
         if (i >= n) break;
         pipe_drain(sm, pp);   // chunk buffer free
-        scatter<kTM, KC>(cr.a, sm.a_hi, sm.a_lo);
-        scatter<NP, KC>(cr.b, sm.b_hi, sm.b_lo);
+        scatter_any<kTM, KC>(cr.a, sm.a_hi, sm.a_lo);
+        scatter_any<NP, KC>(cr.b, sm.b_hi, sm.b_lo);
         fence_async_smem();
         __syncthreads();
         if (threadIdx.x == 0) issue_chunk<KC>(sm, tmem + jobs[i].col, NP, jobs[i].q == 0);
@@ -420,7 +521,91 @@ __device__ __forceinline__ void mul_operand(float out[NP], bool states, uint32_t
 // next rescaling's cluster barrier, which every CTA of the cluster reaches
 // after reading that half, so one barrier per rescaling suffices.  The walk
 // ends with a cluster barrier, so no CTA exits while another reads its smax.
+// Rows read through the same staging tiles: load_tile_sw issues the
+// coalesced loads of rows p0 .. p0 + 127 of category c into registers (lane
+// mapping of gather_sw, 4 whole rows per warp instruction; states >= Sg are
+// zero), stage_tile_sw writes them to the staging tiles once those are free,
+// and after a barrier row_from_stage gives each thread its own row.
+template <int NP>
+__device__ __forceinline__ void load_tile_sw(float v[][4], const float* src, int p0, int c,
+                                             int C, int Sg) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r0 = warp * 4 + (lane >> 3), k8 = lane & 7;
+#pragma unroll
+    for (int h = 0; h < (NP + 31) / 32; ++h) {
+        const int col = 32 * h + 4 * k8;
+#pragma unroll
+        for (int i = 0; i < kTM / 16; ++i) {
+            float* d = v[h * (kTM / 16) + i];
+            d[0] = d[1] = d[2] = d[3] = 0.f;
+            if (col < Sg) ld4(src + ((size_t)(p0 + r0 + 16 * i) * C + c) * Sg + col, d);
+        }
+    }
+}
+
 template <int NP, typename SM>
+__device__ __forceinline__ void stage_tile_sw(SM& sm, const float v[][4]) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r0 = warp * 4 + (lane >> 3), k8 = lane & 7;
+#pragma unroll
+    for (int h = 0; h < (NP + 31) / 32; ++h) {
+        float* half = h == 0 ? sm.a_hi : sm.a_lo;
+#pragma unroll
+        for (int i = 0; i < kTM / 16; ++i) {
+            const int r = r0 + 16 * i;
+            st4(half + r * 32 + ((k8 ^ (r & 7)) * 4), v[h * (kTM / 16) + i]);
+        }
+    }
+}
+
+template <int NP, typename SM>
+__device__ __forceinline__ void row_from_stage(SM& sm, float z[NP]) {
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int kc = 0; kc < NP / 4; ++kc) {
+        const float* half = kc < 8 ? sm.a_hi : sm.a_lo;
+        ld4(half + t * 32 + (((kc & 7) ^ (t & 7)) * 4), z + 4 * kc);
+    }
+}
+
+// A tile of rows stored through the swizzled staging tiles (sm.a_hi: states
+// 0-31, sm.a_lo: 32-63; free once the op's MMAs have completed): each thread
+// writes its row, then every warp stores 4 whole rows (128 contiguous bytes
+// each) per instruction, instead of 32 rows 16 bytes apiece.  Rows outside the
+// op's pattern range are not stored.  Ends with the staging tiles still in
+// use by the stores' reads: the caller's barrier before the next op's chunk
+// writes covers them.
+template <int NP, typename SM>
+__device__ __forceinline__ void store_tile_sw(SM& sm, const OpDesc& op, const float out[NP],
+                                              int p0, int c, int C, int Sg) {
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int kc = 0; kc < NP / 4; ++kc) {
+        float* half = kc < 8 ? sm.a_hi : sm.a_lo;
+        st4(half + t * 32 + (((kc & 7) ^ (t & 7)) * 4), out + 4 * kc);
+    }
+    __syncthreads();
+    const int warp = t >> 5, lane = t & 31;
+    const int r0 = warp * 4 + (lane >> 3), k8 = lane & 7;
+    float* dest = static_cast<float*>(op.dest);
+#pragma unroll
+    for (int h = 0; h < (NP + 31) / 32; ++h) {
+        const float* half = h == 0 ? sm.a_hi : sm.a_lo;
+        const int col = 32 * h + 4 * k8;
+        if (col >= Sg) continue;
+#pragma unroll
+        for (int i = 0; i < kTM / 16; ++i) {
+            const int r = r0 + 16 * i;
+            const int p = p0 + r;
+            if (p < op.p_begin || p >= op.p_end) continue;
+            float v[4];
+            ld4(half + r * 32 + ((k8 ^ (r & 7)) * 4), v);
+            st4(dest + ((size_t)p * C + c) * Sg + col, v);
+        }
+    }
+}
+
+template <int NP, typename SM, bool STORE = true>
 __device__ __forceinline__ void finish_row(SM& sm, const OpDesc& op, float out[NP], int p,
                                            int c, int C, int S, int Sg, double* cum,
                                            int log_scalers, int& nresc) {
@@ -464,7 +649,7 @@ __device__ __forceinline__ void finish_row(SM& sm, const OpDesc& op, float out[N
 #pragma unroll
         for (int i = 0; i < NP; ++i) out[i] *= inv;
     }
-    if (!mine) return;
+    if (!STORE || !mine) return;
     float* d = static_cast<float*>(op.dest) + ((size_t)p * C + c) * Sg;
 #pragma unroll
     for (int j = 0; j < NP / 4; ++j)
@@ -494,7 +679,9 @@ __global__ void __launch_bounds__(kTT, 3)
 k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double* cum,
           int log_scalers, const WalkSeg* __restrict__ segs, int nseg) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    TcSmem& sm = *reinterpret_cast<TcSmem*>(smem_raw);
+    // tiles on 1024-byte boundaries (the swizzle's period; launches add 1 KB)
+    TcSmem& sm = *reinterpret_cast<TcSmem*>(
+        smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u));
     using G = TcGeo<NP>;
     const int t = threadIdx.x;
     const int c = blockIdx.x % C;
@@ -571,18 +758,28 @@ k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double
             const float* mt =
                 static_cast<const float*>((op.kind & kM1Transposed) ? op.m1 : op.m1t) + mo;
             float par[NP];
-            {
+            if constexpr (KC == 32) {
+                // the parent tile by coalesced loads, through the staging
+                // tiles once GEMM 1 has read them
+                float v[2 * kTM / 16][4];
+                load_tile_sw<NP>(v, x1, p0, c, C, Sg);
+                gather_any<NP, KC, true>(cr.b, mt, Sg, Sg, 0, Sg);
+                pipe_drain(sm, pp);
+                stage_tile_sw<NP>(sm, v);
+                __syncthreads();
+                row_from_stage<NP>(sm, par);
+            } else {
                 const float* pr = x1 + ((size_t)p * C + c) * Sg;
 #pragma unroll
                 for (int j = 0; j < NP / 4; ++j) {
                     par[4 * j] = par[4 * j + 1] = par[4 * j + 2] = par[4 * j + 3] = 0.f;
                     if (4 * j < Sg) ld4(pr + 4 * j, par + 4 * j);
                 }
+                gather_any<NP, KC, true>(cr.b, mt, Sg, Sg, 0, Sg);
+                pipe_drain(sm, pp);
             }
             int s2 = 0;
             if (st2) s2 = static_cast<const int*>(op.x2)[p];
-            gather<NP, KC, true>(cr.b, mt, Sg, Sg, 0, Sg);
-            pipe_drain(sm, pp);
             tc_fence_after();
             // z = pre_parent (.) y, in place; states >= Sg stay zero (K padding)
             float* z = par;
@@ -591,22 +788,34 @@ k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double
             // GEMM 2: dest = z . P_node -> columns [NP, 2 NP)
             for (int q = 0; q < NKC; ++q) {
                 pipe_drain(sm, pp);
-                if (q == 0) store_row<NP, KC, 0>(sm.a_hi, sm.a_lo, z);
-                else store_row<NP, KC, 1>(sm.a_hi, sm.a_lo, z);
-                scatter<NP, KC>(cr.b, sm.b_hi, sm.b_lo);
+                if constexpr (KC == 32) {
+                    if (q == 0) store_row_sw128<NP, 0>(sm.a_hi, sm.a_lo, z);
+                    else store_row_sw128<NP, 1>(sm.a_hi, sm.a_lo, z);
+                } else {
+                    if (q == 0) store_row<NP, KC, 0>(sm.a_hi, sm.a_lo, z);
+                    else store_row<NP, KC, 1>(sm.a_hi, sm.a_lo, z);
+                }
+                scatter_any<NP, KC>(cr.b, sm.b_hi, sm.b_lo);
                 fence_async_smem();
                 tc_fence_before();
                 __syncthreads();
                 if (t == 0) issue_chunk<KC>(sm, tmem + NP, NP, q == 0);
                 pp.pending = true;
-                if (q + 1 < NKC) gather<NP, KC, true>(cr.b, mt, Sg, Sg, (q + 1) * KC, Sg);
+                if (q + 1 < NKC) gather_any<NP, KC, true>(cr.b, mt, Sg, Sg, (q + 1) * KC, Sg);
             }
             pipe_drain(sm, pp);
             tc_fence_after();
 #pragma unroll
             for (int j = 0; j < NP / 16; ++j) tmem_chunk(tmem, NP, j, out + 16 * j);
         }
-        finish_row<NP>(sm, op, out, p, c, C, S, Sg, PRE ? nullptr : cum, log_scalers, nresc);
+        if constexpr (KC == 32) {
+            finish_row<NP, TcSmem, false>(sm, op, out, p, c, C, S, Sg, PRE ? nullptr : cum,
+                                          log_scalers, nresc);
+            store_tile_sw<NP>(sm, op, out, p0, c, C, Sg);
+        } else {
+            finish_row<NP>(sm, op, out, p, c, C, S, Sg, PRE ? nullptr : cum, log_scalers,
+                           nresc);
+        }
         // TMEM reads of this op done before the next op's MMAs overwrite them;
         // this op's stores visible to the CTA before the next op's loads.
         tc_fence_before();
@@ -663,16 +872,6 @@ __device__ __forceinline__ void tma_load3(void* dst, const TmaMap* map, int x, i
         : "memory");
 }
 
-// Shared-memory descriptor of a K-major tile with 128-byte swizzle (sm100
-// layout type 2): rows of 128 bytes, 8-row groups 1024 bytes apart.
-__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr) {
-    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
-    d |= (uint64_t)1 << 16;                       // leading byte offset (unused here)
-    d |= (uint64_t)((1024u >> 4) & 0x3FFFu) << 32;
-    d |= (uint64_t)1 << 46;
-    d |= (uint64_t)2 << 61;
-    return d;
-}
 
 // lo = x - hi of n floats (multiple of 512) of a tile, elementwise.
 __device__ __forceinline__ void write_lo(float* lo, const float* hi, int n) {
@@ -941,7 +1140,9 @@ k_deriv_tc(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
            const double* __restrict__ patw, int S, int Sg, int C, int P, int ntiles,
            double* site, double* block, const DerivSeg* __restrict__ segs, int nseg) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    TcSmem& sm = *reinterpret_cast<TcSmem*>(smem_raw);
+    // tiles on 1024-byte boundaries (the swizzle's period; launches add 1 KB)
+    TcSmem& sm = *reinterpret_cast<TcSmem*>(
+        smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u));
     using G = TcGeo<NP>;
     const int t = threadIdx.x;
     const int c = blockIdx.x % C;
@@ -1124,7 +1325,8 @@ k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds,
               const double* __restrict__ patw, int log_scalers, double* block,
               const PreDerivSeg* __restrict__ segs, int nseg) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    TcFusedSmem& sm = *reinterpret_cast<TcFusedSmem*>(smem_raw);
+    TcFusedSmem& sm = *reinterpret_cast<TcFusedSmem*>(
+        smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u));
     constexpr int COLS = TcFusedGeo<NP>::COLS;
     const int t = threadIdx.x;
     const int c = blockIdx.x % C;
@@ -1198,34 +1400,59 @@ k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds,
         const float* mt =
             static_cast<const float*>((op.kind & kM1Transposed) ? op.m1 : op.m1t) + mo;
         float z[NP];
-        {
+        if constexpr (KC == 32) {
+            float v[2 * kTM / 16][4];
+            load_tile_sw<NP>(v, static_cast<const float*>(op.x1), p0, c, C, Sg);
+            gather_any<NP, KC, true>(cr.b, mt, Sg, Sg, 0, Sg);
+            pipe_drain(sm, pp);
+            stage_tile_sw<NP>(sm, v);
+            __syncthreads();
+            row_from_stage<NP>(sm, z);
+        } else {
             const float* pr = static_cast<const float*>(op.x1) + ((size_t)p * C + c) * Sg;
 #pragma unroll
             for (int j = 0; j < NP / 4; ++j) {
                 z[4 * j] = z[4 * j + 1] = z[4 * j + 2] = z[4 * j + 3] = 0.f;
                 if (4 * j < Sg) ld4(pr + 4 * j, z + 4 * j);
             }
+            gather_any<NP, KC, true>(cr.b, mt, Sg, Sg, 0, Sg);
+            pipe_drain(sm, pp);
         }
         const int s2 = st2 ? static_cast<const int*>(op.x2)[p] : 0;
         const int sp = pst ? static_cast<const int*>(dd.post)[p] : 0;
-        gather<NP, KC, true>(cr.b, mt, Sg, Sg, 0, Sg);
-        pipe_drain(sm, pp);
         tc_fence_after();
         mul_operand<NP>(z, st2, tmem, 0, static_cast<const float*>(op.m2t) + mo, s2, S, Sg,
                         (float)op.pad2);
         for (int q = 0; q < NKC; ++q) {
             pipe_drain(sm, pp);
-            if (q == 0) store_row<NP, KC, 0>(sm.a_hi, sm.a_lo, z);
-            else store_row<NP, KC, 1>(sm.a_hi, sm.a_lo, z);
-            scatter<NP, KC>(cr.b, sm.b_hi, sm.b_lo);
+            if constexpr (KC == 32) {
+                if (q == 0) store_row_sw128<NP, 0>(sm.a_hi, sm.a_lo, z);
+                else store_row_sw128<NP, 1>(sm.a_hi, sm.a_lo, z);
+            } else {
+                if (q == 0) store_row<NP, KC, 0>(sm.a_hi, sm.a_lo, z);
+                else store_row<NP, KC, 1>(sm.a_hi, sm.a_lo, z);
+            }
+            scatter_any<NP, KC>(cr.b, sm.b_hi, sm.b_lo);
             fence_async_smem();
             tc_fence_before();
             __syncthreads();
             if (t == 0) issue_chunk<KC>(sm, tmem, NP, q == 0);   // over Y1, now read
             pp.pending = true;
-            if (q + 1 < NKC) gather<NP, KC, true>(cr.b, mt, Sg, Sg, (q + 1) * KC, Sg);
+            if (q + 1 < NKC) gather_any<NP, KC, true>(cr.b, mt, Sg, Sg, (q + 1) * KC, Sg);
         }
-        pipe_drain(sm, pp);
+        if constexpr (KC == 32) {
+            // this node's post-order tile by coalesced loads through the
+            // staging tiles, free once GEMM 2 has completed (issued before
+            // the drain, the loads would need registers the walk does not
+            // have)
+            float v[2 * kTM / 16][4];
+            pipe_drain(sm, pp);
+            if (!pst) load_tile_sw<NP>(v, post, p0, c, C, Sg);
+            if (!pst) stage_tile_sw<NP>(sm, v);
+            __syncthreads();
+        } else {
+            pipe_drain(sm, pp);
+        }
         tc_fence_after();
         float out[NP];
 #pragma unroll
@@ -1243,7 +1470,14 @@ k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds,
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 x[4 * k] = x[4 * k + 1] = x[4 * k + 2] = x[4 * k + 3] = 0.f;
-                if (!pst && 16 * j + 4 * k < Sg) ld4(xr + 16 * j + 4 * k, x + 4 * k);
+                if constexpr (KC == 32) {
+                    const int kc = 4 * j + k;    // this row's piece, from the staging tiles
+                    const float* half = kc < 8 ? sm.a_hi : sm.a_lo;
+                    if (!pst && kc < NP / 4)
+                        ld4(half + t * 32 + (((kc & 7) ^ (t & 7)) * 4), x + 4 * k);
+                } else {
+                    if (!pst && 16 * j + 4 * k < Sg) ld4(xr + 16 * j + 4 * k, x + 4 * k);
+                }
             }
 #pragma unroll
             for (int q = 0; q < 16; ++q) {
@@ -1283,7 +1517,9 @@ k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds,
                 op.scale_write[p] = log_scalers ? lm : (double)m;
             }
         }
-        if (mine) {
+        if constexpr (KC == 32) {
+            store_tile_sw<NP>(sm, op, out, p0, c, C, Sg);
+        } else if (mine) {
             float* dst = static_cast<float*>(op.dest) + ((size_t)p * C + c) * Sg;
 #pragma unroll
             for (int j = 0; j < NP / 4; ++j)
@@ -1447,9 +1683,8 @@ cudaError_t run_prederiv_tc_batch(const PreDerivSeg* segs, int nseg, int ntiles,
 #define B200_TC_DISPATCH(Sg, CALL)                                         \
     ((Sg) <= 8    ? CALL(16, 8)                                            \
      : (Sg) <= 16 ? CALL(16, 16)                                           \
-     : (Sg) <= 24 ? CALL(32, 24)                                           \
      : (Sg) <= 32 ? CALL(32, 32)                                           \
-     : (Sg) <= 48 ? CALL(48, 24)                                           \
+     : (Sg) <= 48 ? CALL(48, 32)                                           \
                   : CALL(64, 32))
 
 }  // namespace
