@@ -360,22 +360,43 @@ __device__ __forceinline__ void scatter_any(const float v[][4], float* hi, float
 struct ChunkRegs {
     float a[8][4];
     float b[4][4];
+    int s;              // this thread's tip state (one-hot A rows)
 };
 
 // One K chunk of a contraction Y[p][i] = sum_k X[p][k] M[i][k]: A rows from
-// partials `x`, B rows from matrix `m` (row stride Sg), the accumulator at
-// TMEM column `col`, chunk index `q`.
+// partials `x`, or (st, 32-state chunks) one-hot rows of the tile's compact
+// tip states, so that Y[p][i] = M[i][state p] comes out of the same MMAs; B
+// rows from matrix `m` (row stride Sg), the accumulator at TMEM column `col`,
+// chunk index `q`.
 struct Job {
     const float* x;
     const float* m;
+    const int* st;
     uint32_t col;
     int q;
 };
 
-template <int NP, int KC>
+template <int NP, int KC, bool ONEHOT>
 __device__ __forceinline__ void gather_job(ChunkRegs& cr, const Job& jb, size_t xs, int Sg) {
-    gather_any<kTM, KC, false>(cr.a, jb.x, xs, kTM, jb.q * KC, Sg);
+    if (ONEHOT && jb.st) cr.s = jb.st[threadIdx.x];
+    else gather_any<kTM, KC, false>(cr.a, jb.x, xs, kTM, jb.q * KC, Sg);
     gather_any<NP, KC, true>(cr.b, jb.m, Sg, Sg, jb.q * KC, Sg);
+}
+
+// Row t of a one-hot A chunk (swizzled layout, hi half only: the lo half of
+// 0 and 1 is 0): 1 at state s when s falls in chunk q, zeros elsewhere; a
+// missing state (outside [0, S)) is a zero row, and the epilogue puts the
+// matrix's pad value in its place.
+__device__ __forceinline__ void onehot_row_sw(float* hi, int s, int q, int S) {
+    const int t = threadIdx.x;
+    const int k = (s >= 0 && s < S) ? s - 32 * q : -1;
+#pragma unroll
+    for (int kc = 0; kc < 8; ++kc) {
+        float v[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) v[e] = (k == 4 * kc + e) ? 1.f : 0.f;
+        st4(hi + t * 32 + ((kc ^ (t & 7)) * 4), v);
+    }
 }
 
 // Row t of A chunk Q from registers: z[Q KC .. Q KC + KC).  Compile-time
@@ -401,7 +422,8 @@ __device__ __forceinline__ void store_row(float* hi, float* lo, const float z[NP
 // Issue the 3 x KC / 8 MMAs of one chunk (thread 0 only); `first` clears the
 // accumulator with the first MMA.  Completion arrives on sm.bar.
 template <int KC, typename SM>
-__device__ __forceinline__ void issue_chunk(SM& sm, uint32_t d_tmem, int N, bool first) {
+__device__ __forceinline__ void issue_chunk(SM& sm, uint32_t d_tmem, int N, bool first,
+                                            bool onehot = false) {
     const uint32_t idesc = idesc_tf32(kTM, N);
     if constexpr (KC == 32) {
         // swizzled tiles: 4 K steps of 8 tf32 (32 bytes) along each 128-byte row
@@ -415,7 +437,7 @@ __device__ __forceinline__ void issue_chunk(SM& sm, uint32_t d_tmem, int N, bool
             const uint64_t dbh = smem_desc_sw128(bh + o), dbl = smem_desc_sw128(bl + o);
             mma_tf32(d_tmem, dah, dbh, idesc, (first && k == 0) ? 0u : 1u);
             mma_tf32(d_tmem, dah, dbl, idesc, 1u);
-            mma_tf32(d_tmem, dal, dbh, idesc, 1u);
+            if (!onehot) mma_tf32(d_tmem, dal, dbh, idesc, 1u);   // one-hot rows: lo = 0
         }
         mma_commit(&sm.bar);
         return;
@@ -455,21 +477,26 @@ __device__ __forceinline__ void pipe_drain(SM& sm, Pipe& pp) {
 
 // Run up to 4 chunk jobs through the single chunk buffer: the registers of
 // job i + 1 are gathered while the MMAs of job i run.
-template <int NP, int KC, typename SM>
+// ONEHOT: jobs may be one-hot tip jobs (32-state chunks only).
+template <int NP, int KC, bool ONEHOT = false, typename SM>
 __device__ __forceinline__ void run_jobs(SM& sm, Pipe& pp, uint32_t tmem, const Job (&jobs)[4],
-                                         int n, size_t xs, int Sg, ChunkRegs& cr) {
-    if (n > 0) gather_job<NP, KC>(cr, jobs[0], xs, Sg);
+                                         int n, size_t xs, int Sg, int S, ChunkRegs& cr) {
+    static_assert(!ONEHOT || KC == 32, "one-hot jobs use the swizzled 32-state chunks");
+    if (n > 0) gather_job<NP, KC, ONEHOT>(cr, jobs[0], xs, Sg);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         if (i >= n) break;
         pipe_drain(sm, pp);   // chunk buffer free
-        scatter_any<kTM, KC>(cr.a, sm.a_hi, sm.a_lo);
+        if (ONEHOT && jobs[i].st) onehot_row_sw(sm.a_hi, cr.s, jobs[i].q, S);
+        else scatter_any<kTM, KC>(cr.a, sm.a_hi, sm.a_lo);
         scatter_any<NP, KC>(cr.b, sm.b_hi, sm.b_lo);
         fence_async_smem();
         __syncthreads();
-        if (threadIdx.x == 0) issue_chunk<KC>(sm, tmem + jobs[i].col, NP, jobs[i].q == 0);
+        if (threadIdx.x == 0)
+            issue_chunk<KC>(sm, tmem + jobs[i].col, NP, jobs[i].q == 0,
+                            ONEHOT && jobs[i].st != nullptr);
         pp.pending = true;
-        if (i + 1 < n) gather_job<NP, KC>(cr, jobs[i + 1], xs, Sg);
+        if (i + 1 < n) gather_job<NP, KC, ONEHOT>(cr, jobs[i + 1], xs, Sg);
     }
 }
 
@@ -493,6 +520,25 @@ __device__ __forceinline__ void tip_chunk(const float* mt, int s, int S, int Sg,
         for (int q = 0; q < 4; ++q) {
             const int i = 16 * j + 4 * k + q;
             y[4 * k + q] = i < S ? (ok ? v[q] : pad) : 0.f;
+        }
+    }
+}
+
+// out[16 j + q] *= operand chunk j, for all chunks, from TMEM columns
+// [col, col + NP) for partials and for one-hot tip rows alike; a missing tip
+// state takes the matrix's pad value (zero for states >= S).
+template <int NP>
+__device__ __forceinline__ void mul_operand_oh(float out[NP], bool states, uint32_t tmem, int col,
+                                               int s, int S, float pad) {
+    const bool miss = states && (s < 0 || s >= S);
+#pragma unroll
+    for (int j = 0; j < NP / 16; ++j) {
+        float y[16];
+        tmem_chunk(tmem, col, j, y);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int i = 16 * j + q;
+            out[i] *= miss ? (i < S ? pad : 0.f) : y[q];
         }
     }
 }
@@ -686,13 +732,15 @@ k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double
     const int t = threadIdx.x;
     const int c = blockIdx.x % C;
     int q = blockIdx.x / C;
+    // BATCH: the CTA's segment lives in shared memory and its op list,
+    // cumulative buffer and scaler kind are read where they are used, instead
+    // of occupying registers for the whole walk
+    __shared__ WalkSeg s_sg;
     if constexpr (BATCH) {
-        const WalkSeg& sg = segs[tc_find_seg(segs, nseg, q)];
-        ops = sg.ops;
-        nops = sg.nops;
-        cum = PRE ? nullptr : sg.cum;
-        log_scalers = sg.log_scalers;
-        q -= sg.first_cta;
+        if (t == 0) s_sg = segs[tc_find_seg(segs, nseg, q)];
+        __syncthreads();
+        nops = s_sg.nops;
+        q -= s_sg.first_cta;
     }
     const int p0 = q * kTM;
     const int p = p0 + t;
@@ -717,7 +765,7 @@ k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double
     ChunkRegs cr;
     int nresc = 0;
     for (int o = 0; o < nops; ++o) {
-        const OpDesc& op = ops[o];
+        const OpDesc& op = (BATCH ? s_sg.ops : ops)[o];
         const bool st1 = !PRE && (op.kind & kX1States), st2 = op.kind & kX2States;
         const float* x1 = static_cast<const float*>(op.x1);
         const float* x2 = static_cast<const float*>(op.x2);
@@ -726,15 +774,21 @@ k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double
         float out[NP];
         if (!PRE) {
             // child 1 -> columns [0, NP), child 2 -> [NP, 2 NP)
+            // (32-state chunks: a tip child is a one-hot job too)
             for (int q = 0; q < NKC; ++q) {
-                if (!st1) jobs[nj++] = Job{x1 + (size_t)p0 * xs + (size_t)c * Sg,
-                                           static_cast<const float*>(op.m1) + mo, 0u, q};
+                if (!st1 || KC == 32)
+                    jobs[nj++] = Job{st1 ? nullptr : x1 + (size_t)p0 * xs + (size_t)c * Sg,
+                                     static_cast<const float*>(op.m1) + mo,
+                                     st1 ? static_cast<const int*>(op.x1) + p0 : nullptr, 0u, q};
             }
             for (int q = 0; q < NKC; ++q) {
-                if (!st2) jobs[nj++] = Job{x2 + (size_t)p0 * xs + (size_t)c * Sg,
-                                           static_cast<const float*>(op.m2) + mo, (uint32_t)NP, q};
+                if (!st2 || KC == 32)
+                    jobs[nj++] = Job{st2 ? nullptr : x2 + (size_t)p0 * xs + (size_t)c * Sg,
+                                     static_cast<const float*>(op.m2) + mo,
+                                     st2 ? static_cast<const int*>(op.x2) + p0 : nullptr,
+                                     (uint32_t)NP, q};
             }
-            run_jobs<NP, KC>(sm, pp, tmem, jobs, nj, xs, Sg, cr);
+            run_jobs<NP, KC, KC == 32>(sm, pp, tmem, jobs, nj, xs, Sg, S, cr);
             int s1 = 0, s2 = 0;
             if (st1) s1 = static_cast<const int*>(op.x1)[p];
             if (st2) s2 = static_cast<const int*>(op.x2)[p];
@@ -742,17 +796,24 @@ k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double
             tc_fence_after();
 #pragma unroll
             for (int i = 0; i < NP; ++i) out[i] = 1.f;
-            mul_operand<NP>(out, st1, tmem, 0, static_cast<const float*>(op.m1t) + mo, s1, S, Sg,
-                            (float)op.pad1);
-            mul_operand<NP>(out, st2, tmem, NP, static_cast<const float*>(op.m2t) + mo, s2, S, Sg,
-                            (float)op.pad2);
+            if constexpr (KC == 32) {
+                mul_operand_oh<NP>(out, st1, tmem, 0, s1, S, (float)op.pad1);
+                mul_operand_oh<NP>(out, st2, tmem, NP, s2, S, (float)op.pad2);
+            } else {
+                mul_operand<NP>(out, st1, tmem, 0, static_cast<const float*>(op.m1t) + mo, s1, S,
+                                Sg, (float)op.pad1);
+                mul_operand<NP>(out, st2, tmem, NP, static_cast<const float*>(op.m2t) + mo, s2, S,
+                                Sg, (float)op.pad2);
+            }
         } else {
-            // GEMM 1: (P_sib . x_sib) -> columns [0, NP)
+            // GEMM 1: (P_sib . x_sib) -> columns [0, NP); a tip sibling's
+            // operand is read from the matrix image in the epilogue (one-hot
+            // jobs here would cost the walk registers it does not have)
             for (int q = 0; q < NKC; ++q) {
                 if (!st2) jobs[nj++] = Job{x2 + (size_t)p0 * xs + (size_t)c * Sg,
-                                           static_cast<const float*>(op.m2) + mo, 0u, q};
+                                           static_cast<const float*>(op.m2) + mo, nullptr, 0u, q};
             }
-            run_jobs<NP, KC>(sm, pp, tmem, jobs, nj, xs, Sg, cr);
+            run_jobs<NP, KC>(sm, pp, tmem, jobs, nj, xs, Sg, S, cr);
             // While GEMM 1 runs: the parent row, the sibling's tip state and the
             // first B chunk of GEMM 2 (rows of P_node^T).
             const float* mt =
@@ -808,13 +869,13 @@ k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double
 #pragma unroll
             for (int j = 0; j < NP / 16; ++j) tmem_chunk(tmem, NP, j, out + 16 * j);
         }
+        double* const cum_o = PRE ? nullptr : (BATCH ? s_sg.cum : cum);
+        const int ls_o = BATCH ? s_sg.log_scalers : log_scalers;
         if constexpr (KC == 32) {
-            finish_row<NP, TcSmem, false>(sm, op, out, p, c, C, S, Sg, PRE ? nullptr : cum,
-                                          log_scalers, nresc);
+            finish_row<NP, TcSmem, false>(sm, op, out, p, c, C, S, Sg, cum_o, ls_o, nresc);
             store_tile_sw<NP>(sm, op, out, p0, c, C, Sg);
         } else {
-            finish_row<NP>(sm, op, out, p, c, C, S, Sg, PRE ? nullptr : cum, log_scalers,
-                           nresc);
+            finish_row<NP>(sm, op, out, p, c, C, S, Sg, cum_o, ls_o, nresc);
         }
         // TMEM reads of this op done before the next op's MMAs overwrite them;
         // this op's stores visible to the CTA before the next op's loads.
@@ -1189,10 +1250,12 @@ k_deriv_tc(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
     Job jobs[4];
     int nj = 0;
     for (int q = 0; q < NKC; ++q) {
-        if (!states) jobs[nj++] = Job{post + (size_t)p0 * xs + (size_t)c * Sg,
-                                      static_cast<const float*>(dd.dmat) + mo, 0u, q};
+        if (!states || KC == 32)
+            jobs[nj++] = Job{states ? nullptr : post + (size_t)p0 * xs + (size_t)c * Sg,
+                             static_cast<const float*>(dd.dmat) + mo,
+                             states ? static_cast<const int*>(dd.post) + p0 : nullptr, 0u, q};
     }
-    run_jobs<NP, KC>(sm, pp, tmem, jobs, nj, xs, Sg, cr);
+    run_jobs<NP, KC, KC == 32>(sm, pp, tmem, jobs, nj, xs, Sg, S, cr);
     // While the MMAs run: this row of the pre-order partials and of the
     // post-order partials (or the tip state).
     const float* pre = static_cast<const float*>(dd.pre) + ((size_t)p * C + c) * Sg;
@@ -1217,8 +1280,16 @@ k_deriv_tc(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
 #pragma unroll
     for (int j = 0; j < NP / 16; ++j) {
         float y[16];
-        if (states) tip_chunk(static_cast<const float*>(dd.dmatt) + mo, s, S, Sg, (float)dd.dpad, j, y);
-        else tmem_chunk(tmem, 0, j, y);
+        if constexpr (KC == 32) {
+            tmem_chunk(tmem, 0, j, y);     // one-hot rows for a tip
+            if (states && (s < 0 || s >= S))
+#pragma unroll
+                for (int q = 0; q < 16; ++q) y[q] = (float)dd.dpad;
+        } else if (states) {
+            tip_chunk(static_cast<const float*>(dd.dmatt) + mo, s, S, Sg, (float)dd.dpad, j, y);
+        } else {
+            tmem_chunk(tmem, 0, j, y);
+        }
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
             const int i = 16 * j + q;
@@ -1332,26 +1403,24 @@ k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds,
     const int c = blockIdx.x % C;
     int tile = blockIdx.x / C;
     int ntiles = gridDim.x / C;
+    // BATCH: the CTA's segment lives in shared memory and its fields are read
+    // where they are used (as the other form reads its kernel parameters),
+    // instead of occupying registers for the whole walk
+    __shared__ PreDerivSeg s_sg;
     if constexpr (BATCH) {
-        const PreDerivSeg& sg = segs[tc_find_seg(segs, nseg, tile)];
-        ops = sg.ops;
-        dds = sg.dds;
-        nops = sg.nops;
-        nsum = sg.nops;
-        P = sg.P;
-        catw = sg.catw;
-        patw = sg.patw;
-        log_scalers = sg.log_scalers;
-        block = sg.block;
-        ntiles = sg.nblk;
-        tile -= sg.first_cta;
+        if (t == 0) s_sg = segs[tc_find_seg(segs, nseg, tile)];
+        __syncthreads();
+        ntiles = s_sg.nblk;
+        tile -= s_sg.first_cta;
+        nops = s_sg.nops;
     }
+#define SEG_(field, arg) (BATCH ? s_sg.field : (arg))
     const int p0 = tile * kTM;
     const int p = p0 + t;
     constexpr int NKC = chunks_of<NP>();
     const size_t xs = (size_t)C * Sg;
     const size_t mo = (size_t)c * Sg * Sg;
-    const double wc = catw[c];
+    const double wc = SEG_(catw, catw)[c];
 
     if (t == 0) {
         mbar_init(&sm.bar, 1);
@@ -1369,8 +1438,8 @@ k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds,
     ChunkRegs cr;
     cg::cluster_group cluster = cg::this_cluster();
     for (int o = 0; o < nops; ++o) {
-        const OpDesc& op = ops[o];
-        const DerivDesc& dd = dds[o];
+        const OpDesc& op = SEG_(ops, ops)[o];
+        const DerivDesc& dd = SEG_(dds, dds)[o];
         const bool st2 = op.kind & kX2States;
         const bool pst = dd.post_is_states;
         const float* x2 = static_cast<const float*>(op.x2);
@@ -1383,17 +1452,17 @@ k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds,
             int nj = 0;
             for (int q = 0; q < NKC; ++q)
                 if (!st2) jobs[nj++] = Job{x2 + (size_t)p0 * xs + (size_t)c * Sg,
-                                           static_cast<const float*>(op.m2) + mo, 0u, q};
-            run_jobs<NP, KC>(sm, pp, tmem, jobs, nj, xs, Sg, cr);
+                                           static_cast<const float*>(op.m2) + mo, nullptr, 0u, q};
+            run_jobs<NP, KC>(sm, pp, tmem, jobs, nj, xs, Sg, S, cr);
         }
         {
             Job jobs[4];
             int nj = 0;
             for (int q = 0; q < NKC; ++q)
                 if (!pst) jobs[nj++] = Job{post + (size_t)p0 * xs + (size_t)c * Sg,
-                                           static_cast<const float*>(dd.dmat) + mo,
+                                           static_cast<const float*>(dd.dmat) + mo, nullptr,
                                            (uint32_t)NP, q};
-            run_jobs<NP, KC>(sm, pp, tmem, jobs, nj, xs, Sg, cr);
+            run_jobs<NP, KC>(sm, pp, tmem, jobs, nj, xs, Sg, S, cr);
         }
         // While they run: the parent row, the tip states and GEMM 2's first
         // B chunk (rows of P_node^T).
@@ -1514,7 +1583,7 @@ k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds,
             for (int i = 0; i < NP; ++i) out[i] *= inv;
             if (c == 0 && mine) {
                 const double lm = scale_log(m);
-                op.scale_write[p] = log_scalers ? lm : (double)m;
+                op.scale_write[p] = SEG_(log_scalers, log_scalers) ? lm : (double)m;
             }
         }
         if constexpr (KC == 32) {
@@ -1533,10 +1602,11 @@ k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds,
                 dn += rem[t * 2 + 1];
             }
             double v1 = 0, v2 = 0;
-            if (p < P) {
+            if (p < SEG_(P, P)) {
                 const double dv = nn / dn;
-                v1 = dv * patw[p];
-                v2 = dv * dv * patw[p];
+                const double wp = SEG_(patw, patw)[p];
+                v1 = dv * wp;
+                v2 = dv * dv * wp;
             }
 #pragma unroll
             for (int sh = 16; sh > 0; sh >>= 1) {
@@ -1554,8 +1624,9 @@ k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds,
                     t1 += sm.red[k * 2 + 0];
                     t2 += sm.red[k * 2 + 1];
                 }
-                block[(size_t)o * ntiles + tile] = t1;
-                block[(size_t)(nsum + o) * ntiles + tile] = t2;
+                double* blk = SEG_(block, block);
+                blk[(size_t)o * ntiles + tile] = t1;
+                blk[(size_t)(SEG_(nops, nsum) + o) * ntiles + tile] = t2;
             }
         }
         // TMEM reads of this op done before the next op's MMAs overwrite
@@ -1563,6 +1634,7 @@ k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds,
         tc_fence_before();
         __syncthreads();
     }
+#undef SEG_
     pipe_drain(sm, pp);
     tc_fence_after();
     cluster.sync();   // every remote read of this CTA's exchange buffers is done

@@ -628,7 +628,9 @@ def workload_record(torch, lib, name, args, device):
     ms, _, _ = timed_value(torch, inst, pr, steps, warm)
     mixed = steps / (ms / 1000.0)
     tuned = inst.tunedVariants()
-    fused_walk = pr.S == 4 and tuned.get("fused") == 1
+    # the fused pre-order + derivative walk (S = 4 kernel, or the tensor-core
+    # one for S > 4) when the autotuner picked it
+    fused_walk = tuned.get("fused") == 1
     ph_ms = phase_times(torch, inst, pr, 5, fused_walk)
     peak, peak_kind = peaks()
     roof = roofline_of(pr, ph_ms, fused_walk, peak, peak_kind, traffic_table())
