@@ -33,6 +33,11 @@ __device__ __forceinline__ void st4(double* p, const double v[4]) {
     reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
 }
 
+// 1 / x correctly rounded (the IEEE quotient of 1 by x, the value `1 / x`
+// gives), through the reciprocal intrinsics instead of a division.
+__device__ __forceinline__ float recip(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double recip(double x) { return __drcp_rn(x); }
+
 // Natural log of a positive rescaling factor, in FP64.  FP64 partials: log.
 // FP32 partials: m = 2^e f with f in [1, 2), log m = (e + log2 f) ln 2 with the
 // integer part exact and log2 f from the hardware base-2 logarithm (__log2f,

@@ -84,12 +84,12 @@ __device__ __forceinline__ void finish4c(const OpDesc& op, Real out[4], int p, b
         for (int i = 1; i < 4; ++i) m = out[i] > m ? out[i] : m;
         m = group_max<C>(m);
         if (m == Real(0)) m = Real(1);
-        const Real inv = Real(1) / m;
+        const Real inv = recip(m);
 #pragma unroll
         for (int i = 0; i < 4; ++i) out[i] *= inv;
         if (valid && c == 0) store_scale(m, op.scale_write, cum, p, log_scalers, acc);
     } else if (op.scale_read) {
-        const Real inv = Real(1) / (Real)op.scale_read[p];
+        const Real inv = recip((Real)op.scale_read[p]);
 #pragma unroll
         for (int i = 0; i < 4; ++i) out[i] *= inv;
     }

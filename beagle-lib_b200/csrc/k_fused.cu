@@ -49,7 +49,7 @@ __device__ __forceinline__ void rescale_store4(const PreDerivOp& op, Real out[4]
         for (int i = 1; i < 4; ++i) m = out[i] > m ? out[i] : m;
         m = group_max<C>(m);
         if (m == Real(0)) m = Real(1);
-        const Real inv = Real(1) / m;
+        const Real inv = recip(m);
 #pragma unroll
         for (int i = 0; i < 4; ++i) out[i] *= inv;
         if (valid && c == 0) store_scale(m, op.scale_write, nullptr, p, log_scalers);

@@ -196,7 +196,7 @@ __device__ __forceinline__ void finish_tile(const OpDesc& op, Real out[4][4], in
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             Real mq = m[q] == Real(0) ? Real(1) : m[q];
-            const Real inv = Real(1) / mq;
+            const Real inv = recip(mq);
 #pragma unroll
             for (int r = 0; r < 4; ++r) out[q][r] *= inv;
             const int p = p0 + pl + q;
@@ -209,7 +209,7 @@ __device__ __forceinline__ void finish_tile(const OpDesc& op, Real out[4][4], in
     } else if (op.scale_read) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const Real inv = Real(1) / (Real)op.scale_read[p0 + pl + q];
+            const Real inv = recip((Real)op.scale_read[p0 + pl + q]);
 #pragma unroll
             for (int r = 0; r < 4; ++r) out[q][r] *= inv;
         }

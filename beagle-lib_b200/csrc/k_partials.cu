@@ -531,14 +531,14 @@ __device__ __forceinline__ void finish4(const OpDesc& op, Real out[C][4], int p,
 #pragma unroll
             for (int i = 0; i < 4; ++i) m = out[c][i] > m ? out[c][i] : m;
         if (m == Real(0)) m = Real(1);
-        const Real inv = Real(1) / m;
+        const Real inv = recip(m);
 #pragma unroll
         for (int c = 0; c < C; ++c)
 #pragma unroll
             for (int i = 0; i < 4; ++i) out[c][i] *= inv;
         store_scale(m, op.scale_write, cum, p, log_scalers);
     } else if (op.scale_read) {
-        const Real inv = Real(1) / (Real)op.scale_read[p];
+        const Real inv = recip((Real)op.scale_read[p]);
 #pragma unroll
         for (int c = 0; c < C; ++c)
 #pragma unroll

@@ -682,7 +682,7 @@ __device__ __forceinline__ void finish_row(SM& sm, const OpDesc& op, float out[N
             m = u > m ? u : m;
         }
         if (m == 0.f) m = 1.f;
-        const float inv = 1.f / m;
+        const float inv = recip(m);
 #pragma unroll
         for (int i = 0; i < NP; ++i) out[i] *= inv;
         if (c == 0 && mine) {
@@ -691,7 +691,7 @@ __device__ __forceinline__ void finish_row(SM& sm, const OpDesc& op, float out[N
             if (cum) cum[p] += lm;
         }
     } else if (op.scale_read) {
-        const float inv = 1.f / (float)op.scale_read[p];
+        const float inv = recip((float)op.scale_read[p]);
 #pragma unroll
         for (int i = 0; i < NP; ++i) out[i] *= inv;
     }
@@ -1578,7 +1578,7 @@ k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds,
                 m = u > m ? u : m;
             }
             if (m == 0.f) m = 1.f;
-            const float inv = 1.f / m;
+            const float inv = recip(m);
 #pragma unroll
             for (int i = 0; i < NP; ++i) out[i] *= inv;
             if (c == 0 && mine) {
