@@ -279,17 +279,32 @@ __device__ __forceinline__ void scatter(const float v[][4], float* hi, float* lo
 // l of warp w handles rows 4 w + (l >> 3) + 16 i and piece l & 7, so one
 // warp load covers 4 whole rows (4 x 128 contiguous bytes) and one warp store
 // writes each of those rows' 8 pieces to 8 distinct bank groups of its line.
+// 16-byte pieces of chunk q that its MMAs read: whole 8-state K steps up to
+// Sg (the rest of the 32-state row is never read, so it is neither loaded
+// nor stored).
+// NP = 64 (49 to 64 states) keeps whole chunks: trimming its second chunk
+// would save little and the run-time counts cost the widest walks registers
+// they do not have.
+template <int NP>
+__device__ __forceinline__ int chunk_pieces(int Sg, int q) {
+    if constexpr (NP == 64) return 8;
+    int k = Sg - 32 * q;
+    k = k < 32 ? k : 32;
+    return (k + 7) / 8 * 2;
+}
+
 template <int NROWS, bool RO>
 __device__ __forceinline__ void gather_sw(float v[][4], const float* src, size_t rstride,
-                                          int nvalid, int k0, int Sg) {
+                                          int nvalid, int k0, int Sg, int npieces) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int r0 = warp * 4 + (lane >> 3), k = k0 + 4 * (lane & 7);
+    const bool piece = (lane & 7) < npieces;
     const float* base = src + (size_t)r0 * rstride + k;
 #pragma unroll
     for (int i = 0; i < NROWS / 16; ++i) {
         float* d = v[i];
         d[0] = d[1] = d[2] = d[3] = 0.f;
-        if (r0 + 16 * i < nvalid && k < Sg) {
+        if (piece && r0 + 16 * i < nvalid && k < Sg) {
             const float* g = base + (size_t)(16 * i) * rstride;
             if (RO) ldg4(g, d);
             else ld4(g, d);
@@ -298,9 +313,11 @@ __device__ __forceinline__ void gather_sw(float v[][4], const float* src, size_t
 }
 
 template <int NROWS>
-__device__ __forceinline__ void scatter_sw(const float v[][4], float* hi, float* lo) {
+__device__ __forceinline__ void scatter_sw(const float v[][4], float* hi, float* lo,
+                                           int npieces) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int r0 = warp * 4 + (lane >> 3), kc = lane & 7;
+    if (kc >= npieces) return;
     // rows r0 + 16 i share r0 & 7, so every piece lands at the same swizzled column
     const int off0 = r0 * 32 + ((kc ^ (r0 & 7)) * 4);
 #pragma unroll
@@ -343,16 +360,18 @@ __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr) {
 }
 
 // Chunk helpers for either layout: KC == 32 uses the swizzled layout.
-template <int NROWS, int KC, bool RO>
+template <int NROWS, int KC, bool RO, int NP>
 __device__ __forceinline__ void gather_any(float v[][4], const float* src, size_t rstride,
                                            int nvalid, int k0, int Sg) {
-    if constexpr (KC == 32) gather_sw<NROWS, RO>(v, src, rstride, nvalid, k0, Sg);
+    if constexpr (KC == 32)
+        gather_sw<NROWS, RO>(v, src, rstride, nvalid, k0, Sg, chunk_pieces<NP>(Sg, k0 / 32));
     else gather<NROWS, KC, RO>(v, src, rstride, nvalid, k0, Sg);
 }
 
-template <int NROWS, int KC>
-__device__ __forceinline__ void scatter_any(const float v[][4], float* hi, float* lo) {
-    if constexpr (KC == 32) scatter_sw<NROWS>(v, hi, lo);
+template <int NROWS, int KC, int NP>
+__device__ __forceinline__ void scatter_any(const float v[][4], float* hi, float* lo, int Sg,
+                                            int q) {
+    if constexpr (KC == 32) scatter_sw<NROWS>(v, hi, lo, chunk_pieces<NP>(Sg, q));
     else scatter<NROWS, KC>(v, hi, lo);
 }
 
@@ -379,8 +398,8 @@ struct Job {
 template <int NP, int KC, bool ONEHOT>
 __device__ __forceinline__ void gather_job(ChunkRegs& cr, const Job& jb, size_t xs, int Sg) {
     if (ONEHOT && jb.st) cr.s = jb.st[threadIdx.x];
-    else gather_any<kTM, KC, false>(cr.a, jb.x, xs, kTM, jb.q * KC, Sg);
-    gather_any<NP, KC, true>(cr.b, jb.m, Sg, Sg, jb.q * KC, Sg);
+    else gather_any<kTM, KC, false, NP>(cr.a, jb.x, xs, kTM, jb.q * KC, Sg);
+    gather_any<NP, KC, true, NP>(cr.b, jb.m, Sg, Sg, jb.q * KC, Sg);
 }
 
 // Row t of a one-hot A chunk (swizzled layout, hi half only: the lo half of
@@ -423,15 +442,17 @@ __device__ __forceinline__ void store_row(float* hi, float* lo, const float z[NP
 // accumulator with the first MMA.  Completion arrives on sm.bar.
 template <int KC, typename SM>
 __device__ __forceinline__ void issue_chunk(SM& sm, uint32_t d_tmem, int N, bool first,
-                                            bool onehot = false) {
+                                            bool onehot = false, int ksteps = 4) {
     const uint32_t idesc = idesc_tf32(kTM, N);
     if constexpr (KC == 32) {
-        // swizzled tiles: 4 K steps of 8 tf32 (32 bytes) along each 128-byte row
+        // swizzled tiles: up to 4 K steps of 8 tf32 (32 bytes) along each
+        // 128-byte row (only those that hold states < Sg)
         const uint32_t ah = smem_u32(sm.a_hi), al = smem_u32(sm.a_lo);
         const uint32_t bh = smem_u32(sm.b_hi), bl = smem_u32(sm.b_lo);
         tc_fence_after();
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
+            if (k >= ksteps) break;
             const uint32_t o = (uint32_t)k * 32u;
             const uint64_t dah = smem_desc_sw128(ah + o), dal = smem_desc_sw128(al + o);
             const uint64_t dbh = smem_desc_sw128(bh + o), dbl = smem_desc_sw128(bl + o);
@@ -488,13 +509,13 @@ __device__ __forceinline__ void run_jobs(SM& sm, Pipe& pp, uint32_t tmem, const 
         if (i >= n) break;
         pipe_drain(sm, pp);   // chunk buffer free
         if (ONEHOT && jobs[i].st) onehot_row_sw(sm.a_hi, cr.s, jobs[i].q, S);
-        else scatter_any<kTM, KC>(cr.a, sm.a_hi, sm.a_lo);
-        scatter_any<NP, KC>(cr.b, sm.b_hi, sm.b_lo);
+        else scatter_any<kTM, KC, NP>(cr.a, sm.a_hi, sm.a_lo, Sg, jobs[i].q);
+        scatter_any<NP, KC, NP>(cr.b, sm.b_hi, sm.b_lo, Sg, jobs[i].q);
         fence_async_smem();
         __syncthreads();
         if (threadIdx.x == 0)
             issue_chunk<KC>(sm, tmem + jobs[i].col, NP, jobs[i].q == 0,
-                            ONEHOT && jobs[i].st != nullptr);
+                            ONEHOT && jobs[i].st != nullptr, chunk_pieces<NP>(Sg, jobs[i].q) / 2);
         pp.pending = true;
         if (i + 1 < n) gather_job<NP, KC, ONEHOT>(cr, jobs[i + 1], xs, Sg);
     }
@@ -824,7 +845,7 @@ k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double
                 // tiles once GEMM 1 has read them
                 float v[2 * kTM / 16][4];
                 load_tile_sw<NP>(v, x1, p0, c, C, Sg);
-                gather_any<NP, KC, true>(cr.b, mt, Sg, Sg, 0, Sg);
+                gather_any<NP, KC, true, NP>(cr.b, mt, Sg, Sg, 0, Sg);
                 pipe_drain(sm, pp);
                 stage_tile_sw<NP>(sm, v);
                 __syncthreads();
@@ -836,7 +857,7 @@ k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double
                     par[4 * j] = par[4 * j + 1] = par[4 * j + 2] = par[4 * j + 3] = 0.f;
                     if (4 * j < Sg) ld4(pr + 4 * j, par + 4 * j);
                 }
-                gather_any<NP, KC, true>(cr.b, mt, Sg, Sg, 0, Sg);
+                gather_any<NP, KC, true, NP>(cr.b, mt, Sg, Sg, 0, Sg);
                 pipe_drain(sm, pp);
             }
             int s2 = 0;
@@ -856,13 +877,14 @@ k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double
                     if (q == 0) store_row<NP, KC, 0>(sm.a_hi, sm.a_lo, z);
                     else store_row<NP, KC, 1>(sm.a_hi, sm.a_lo, z);
                 }
-                scatter_any<NP, KC>(cr.b, sm.b_hi, sm.b_lo);
+                scatter_any<NP, KC, NP>(cr.b, sm.b_hi, sm.b_lo, Sg, q);
                 fence_async_smem();
                 tc_fence_before();
                 __syncthreads();
-                if (t == 0) issue_chunk<KC>(sm, tmem + NP, NP, q == 0);
+                if (t == 0)
+                    issue_chunk<KC>(sm, tmem + NP, NP, q == 0, false, chunk_pieces<NP>(Sg, q) / 2);
                 pp.pending = true;
-                if (q + 1 < NKC) gather_any<NP, KC, true>(cr.b, mt, Sg, Sg, (q + 1) * KC, Sg);
+                if (q + 1 < NKC) gather_any<NP, KC, true, NP>(cr.b, mt, Sg, Sg, (q + 1) * KC, Sg);
             }
             pipe_drain(sm, pp);
             tc_fence_after();
@@ -1472,7 +1494,7 @@ k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds,
         if constexpr (KC == 32) {
             float v[2 * kTM / 16][4];
             load_tile_sw<NP>(v, static_cast<const float*>(op.x1), p0, c, C, Sg);
-            gather_any<NP, KC, true>(cr.b, mt, Sg, Sg, 0, Sg);
+            gather_any<NP, KC, true, NP>(cr.b, mt, Sg, Sg, 0, Sg);
             pipe_drain(sm, pp);
             stage_tile_sw<NP>(sm, v);
             __syncthreads();
@@ -1484,7 +1506,7 @@ k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds,
                 z[4 * j] = z[4 * j + 1] = z[4 * j + 2] = z[4 * j + 3] = 0.f;
                 if (4 * j < Sg) ld4(pr + 4 * j, z + 4 * j);
             }
-            gather_any<NP, KC, true>(cr.b, mt, Sg, Sg, 0, Sg);
+            gather_any<NP, KC, true, NP>(cr.b, mt, Sg, Sg, 0, Sg);
             pipe_drain(sm, pp);
         }
         const int s2 = st2 ? static_cast<const int*>(op.x2)[p] : 0;
@@ -1501,13 +1523,14 @@ k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds,
                 if (q == 0) store_row<NP, KC, 0>(sm.a_hi, sm.a_lo, z);
                 else store_row<NP, KC, 1>(sm.a_hi, sm.a_lo, z);
             }
-            scatter_any<NP, KC>(cr.b, sm.b_hi, sm.b_lo);
+            scatter_any<NP, KC, NP>(cr.b, sm.b_hi, sm.b_lo, Sg, q);
             fence_async_smem();
             tc_fence_before();
             __syncthreads();
-            if (t == 0) issue_chunk<KC>(sm, tmem, NP, q == 0);   // over Y1, now read
+            if (t == 0)   // over Y1, now read
+                issue_chunk<KC>(sm, tmem, NP, q == 0, false, chunk_pieces<NP>(Sg, q) / 2);
             pp.pending = true;
-            if (q + 1 < NKC) gather_any<NP, KC, true>(cr.b, mt, Sg, Sg, (q + 1) * KC, Sg);
+            if (q + 1 < NKC) gather_any<NP, KC, true, NP>(cr.b, mt, Sg, Sg, (q + 1) * KC, Sg);
         }
         if constexpr (KC == 32) {
             // this node's post-order tile by coalesced loads through the
