@@ -221,15 +221,18 @@ class CheckpointPlan:
 
     # ------------------------------------------------------------- evaluation
 
-    def evaluate(self, inst, lengths=None):
+    def evaluate(self, inst, lengths=None, fused=False):
         """One lnL + gradient evaluation; returns (lnL, gradient[B]).  The
-        instance holds the problem's data (``Problem.load``)."""
+        instance holds the problem's data (``Problem.load``).  With ``fused``
+        each block's pre-order walk and derivatives are one
+        beagleB200UpdatePrePartialsWithDerivatives call (its sums come in
+        the block's branch order, the pre-order ops' order)."""
         pb = self.pb
         t = pb.lengths if lengths is None else lengths
         inst.updateTransitionMatrices(0, np.arange(pb.B, dtype=np.int32), None, None, t)
-        return self._after_matrices(inst)
+        return self._after_matrices(inst, fused)
 
-    def _after_matrices(self, inst):
+    def _after_matrices(self, inst, fused=False):
         pb = self.pb
         if self.transposed_pre:
             idx = np.arange(pb.B, dtype=np.int32)
@@ -244,12 +247,19 @@ class CheckpointPlan:
         self._set_root_pre(inst)
         grad = np.zeros(pb.B)
         parts = []
-        for s in self.steps:
+        steps = self.steps
+        for i, s in enumerate(steps):
             if s[0] == "post":
                 inst.updatePartials(s[1], OP_NONE)
             elif s[0] == "pre":
-                inst.updatePrePartials(s[1], OP_NONE)
-            else:
+                if fused:                  # with the "deriv" step that follows it
+                    _, br, pst, _ = steps[i + 1]
+                    sums, _ = inst.updatePrePartialsWithDerivatives(
+                        s[1], pst, np.full(len(br), pb.B, dtype=np.int32), [0])
+                    parts.append((br, sums))
+                else:
+                    inst.updatePrePartials(s[1], OP_NONE)
+            elif not fused:
                 _, br, pst, prb = s
                 _, sums, _ = inst.calculateEdgeDerivatives(
                     pst, prb, np.full(len(br), pb.B, dtype=np.int32), [0], per_site=False,
@@ -271,16 +281,16 @@ class CheckpointPlan:
         elif code < 0:
             raise RuntimeError(f"setRootPrePartials returned {code}")
 
-    def capture(self, inst):
+    def capture(self, inst, fused=False):
         """Record the evaluation after the transition matrices as a CUDA graph
         of an ASYNCH instance; returns (graph, gradient getter).  The getter,
         called after ``getLogLikelihood`` following a launch, assembles the
         gradient from the per-block sums the graph delivers."""
-        self.evaluate(inst)
+        self.evaluate(inst, fused=fused)
         inst.getLogLikelihood()
         inst.beginCapture()
         try:
-            self._after_matrices(inst)
+            self._after_matrices(inst, fused)
         finally:
             graph = inst.endCapture()
         parts = self._parts
@@ -323,13 +333,15 @@ def smallest_plan(problem, transposed_pre=False):
     return best
 
 
-def batch_checkpointed_evaluate(batch, plans, lengths=None):
+def batch_checkpointed_evaluate(batch, plans, lengths=None, fused=False):
     """One lnL + gradient evaluation of every member of a batch, each with its
     own checkpoint plan (members in plan order; S > 4 members need
     PREORDER_TRANSPOSE_AUTO).  The members' schedules run side by side: one
     batched forward walk, scale accumulation and root lnL, then for block
     i = 0, 1, ... one batched recomputation, pre-order walk and derivative call
-    over every member that has an i-th block (the others pass empty lists).
+    over every member that has an i-th block (the others pass empty lists);
+    with ``fused`` the pre-order walk and the derivatives of each block index
+    are one beagleB200BatchUpdatePrePartialsWithDerivatives call.
     Returns (lnL[n], [gradient_m])."""
     n = len(plans)
     pbs = [pl.pb for pl in plans]
@@ -355,11 +367,15 @@ def batch_checkpointed_evaluate(batch, plans, lengths=None):
     for i in range(max(len(pl.blocks) for pl in plans)):
         blk = [pl.blocks[i] if i < len(pl.blocks) else None for pl in plans]
         batch.updatePartials([b[0] if b else empty_ops for b in blk], none)
-        batch.updatePrePartials([b[1] if b else empty_ops for b in blk])
         post = [b[2][2] if b else empty_idx for b in blk]
         pre = [b[2][3] if b else empty_idx for b in blk]
         dmat = [np.full(len(q), p.B, dtype=np.int32) for q, p in zip(post, pbs)]
-        sums, _ = batch.calculateEdgeDerivatives(post, pre, dmat, zeros)
+        if fused:
+            sums, _ = batch.updatePrePartialsWithDerivatives(
+                [b[1] if b else empty_ops for b in blk], post, dmat, zeros)
+        else:
+            batch.updatePrePartials([b[1] if b else empty_ops for b in blk])
+            sums, _ = batch.calculateEdgeDerivatives(post, pre, dmat, zeros)
         parts.append([(b[2][1] if b else empty_idx, sm) for b, sm in zip(blk, sums)])
     batch.wait()
     for step in parts:

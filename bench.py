@@ -400,7 +400,7 @@ def timed_checkpointed(torch, lib, pr, device, steps, ref_lnl, ref_grad):
                       requirementFlags=SINGLE | FW_CUDA)
     pr.load(inst)
     stream = torch.cuda.ExternalStream(inst.cudaStream())
-    graph, gradient = plan.capture(inst)
+    graph, gradient = plan.capture(inst, fused=True)
     idx = np.arange(pr.B, dtype=np.int32)
 
     def step(t):
@@ -943,7 +943,7 @@ def run_batch_full_arm(args):
     state = {}
 
     def batched():
-        state["lnl"], _ = ck.batch_checkpointed_evaluate(batch, plans)
+        state["lnl"], _ = ck.batch_checkpointed_evaluate(batch, plans, fused=True)
 
     ms_b = timed(stream, batched, steps, 2)
     lnl32 = np.array(state["lnl"])
@@ -958,7 +958,7 @@ def run_batch_full_arm(args):
 
     def per_instance():
         for pl, inst in zip(plans, insts):
-            pl.evaluate(inst)
+            pl.evaluate(inst, fused=True)
 
     ms_64 = timed(stream, per_instance, 1, 1)
     for i, inst in enumerate(insts):

@@ -59,9 +59,12 @@ def test_plan_structure(pkg, syn):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("fused", [False, True], ids=["calls", "fused"])
 @pytest.mark.parametrize("precision", ["double", "single"])
 @pytest.mark.parametrize("S,N,C", [(4, 40, 4), (20, 20, 2), (61, 12, 4)])
-def test_checkpointed_gpu_matches_full(b200, pkg, syn, precision, S, N, C):
+def test_checkpointed_gpu_matches_full(b200, pkg, syn, precision, S, N, C, fused):
+    """fused: each block's pre-order walk and derivatives as one
+    beagleB200UpdatePrePartialsWithDerivatives call."""
     ck = pkg.checkpoint
     pr = syn.make_problem(S=S, N=N, P=1500, C=C, seed=950 + S, rescale=True)
     pref, req = gpu_flags(precision)
@@ -73,14 +76,14 @@ def test_checkpointed_gpu_matches_full(b200, pkg, syn, precision, S, N, C):
     assert plan.n_buffers < plan.full_buffers()
     inst = b200.create(*plan.create_args(), preferenceFlags=pref, requirementFlags=req)
     pr.load(inst)
-    l1, g1 = plan.evaluate(inst)
+    l1, g1 = plan.evaluate(inst, fused=fused)
     tol = TOL[precision]
     assert rel(l1, l0) <= tol["lnl"], (l1, l0)
     assert grad_err(g1, g0) <= tol["grad"]
     # captured as one graph on an ASYNCH instance, replayed with new lengths
     gi = b200.create(*plan.create_args(), preferenceFlags=pref | ASYNCH, requirementFlags=req)
     pr.load(gi)
-    graph, gradient = plan.capture(gi)
+    graph, gradient = plan.capture(gi, fused=fused)
     rng = np.random.default_rng(3)
     for step in range(2):
         t = pr.lengths * (1 + 0.05 * rng.standard_normal(pr.B))

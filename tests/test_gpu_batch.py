@@ -101,9 +101,10 @@ def test_batch_graph_replay(b200, pkg, syn, precision):
     graphed.finalize()
 
 
+@pytest.mark.parametrize("fused", [False, True], ids=["calls", "fused"])
 @pytest.mark.parametrize("asynch", [False, True], ids=["synch", "asynch"])
 @pytest.mark.parametrize("precision", ["double", "single"])
-def test_batch_checkpointed_matches_single_instances(b200, pkg, syn, precision, asynch):
+def test_batch_checkpointed_matches_single_instances(b200, pkg, syn, precision, asynch, fused):
     """Every member with its own subtree checkpoint plan (pooled buffers,
     per-block recomputation), the plans run side by side through batched
     calls, against full evaluations one instance at a time."""
@@ -123,7 +124,7 @@ def test_batch_checkpointed_matches_single_instances(b200, pkg, syn, precision, 
     batch = pkg.binding.Batch(b200, members)
     tol = TOL[precision]
     for _ in range(2):
-        lnl, grads = pkg.checkpoint.batch_checkpointed_evaluate(batch, plans)
+        lnl, grads = pkg.checkpoint.batch_checkpointed_evaluate(batch, plans, fused=fused)
         for i, (l0, g0) in enumerate(ref):
             assert rel(lnl[i], l0) <= tol["lnl"], (i, lnl[i], l0)
             assert grad_err(grads[i], g0) <= tol["grad"], i
@@ -200,7 +201,8 @@ def test_batch_configuration_shapes_checkpointed(b200, pkg, syn, oracle):
     pattern range (log-uniform 100-50,000): every member with a subtree
     checkpoint plan, the plans side by side through batched calls on the
     mixed path, against the same plans one instance at a time on the FP64
-    path, and two members against the oracle."""
+    path, and two members against the oracle.  The mixed path runs each
+    block's pre-order walk and derivatives as one batched fused call."""
     probs = syn.batched_problems(count=16, seed=2100, max_patterns=50000)
     plans = [pkg.checkpoint.quick_plan(pr) for pr in probs]
     assert max(p.P for p in probs) > 20000
@@ -217,7 +219,7 @@ def test_batch_configuration_shapes_checkpointed(b200, pkg, syn, oracle):
 
     m32 = members("single", 1)
     batch = pkg.binding.Batch(b200, m32)
-    lnl32, g32 = pkg.checkpoint.batch_checkpointed_evaluate(batch, plans)
+    lnl32, g32 = pkg.checkpoint.batch_checkpointed_evaluate(batch, plans, fused=True)
     lnl32 = np.array(lnl32)
     g32 = [np.array(g) for g in g32]
     batch.finalize()
