@@ -82,6 +82,71 @@ k_update_matrices(const MatJob* __restrict__ jobs, int S, int Sg) {
     }
 }
 
+// The same for small state counts (Sg <= 8, at most 64 entries a matrix):
+// a 256-thread block takes 256 / Sg^2 (job, category) items, one group of
+// Sg^2 threads each, instead of one item with most threads idle.  Each
+// group's exponentials go to its own slice of shared memory.
+template <typename Real, int SG>
+__global__ void __launch_bounds__(256)
+k_update_matrices_small(const MatJob* __restrict__ jobs, int nitems, int C, int S) {
+    constexpr int E = SG * SG, G = 256 / E;
+    __shared__ double ex[G][SG], e1[G][SG], e2[G][SG];
+    const int g = threadIdx.x / E, e = threadIdx.x - (threadIdx.x / E) * E;
+    const int item = blockIdx.x * G + g;
+    const bool active = g < G && item < nitems;
+    const int c = active ? item % C : 0;
+    const MatJob& jb = jobs[active ? item / C : 0];
+    const double* cube = jb.cube;
+    const double* evals = jb.evals;
+    double r;
+    if (jb.cat_eig) {           // CPU/EigenDecompositionCube.hpp:326-470: no category rate
+        const int ce = jb.cat_eig[c];
+        cube += (size_t)ce * S * S * S;
+        evals += (size_t)ce * S;
+        r = 1.0;
+    } else {
+        r = jb.rates[c];
+    }
+    if (active && e < S) {
+        const double t = jb.tlen ? *jb.tlen : jb.t;
+        const double lam = evals[e];
+        const double v = exp(lam * (t * r));
+        const double sl = lam * r;
+        ex[g][e] = v;
+        e1[g][e] = sl * v;
+        e2[g][e] = sl * sl * v;
+    }
+    __syncthreads();
+    if (!active) return;
+    const size_t off = (size_t)c * SG * SG;
+    Real* P = static_cast<Real*>(jb.p) + off;
+    Real* D1 = jb.d1 ? static_cast<Real*>(jb.d1) + off : nullptr;
+    Real* D2 = jb.d2 ? static_cast<Real*>(jb.d2) + off : nullptr;
+    const int i = e / SG, j = e - (e / SG) * SG;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    if (i < S && j < S) {
+        const double* cu = cube + (size_t)i * S * S + j;
+        if (D1) {
+            for (int k = 0; k < S; ++k) {
+                const double cv = cu[(size_t)k * S];
+                s0 += cv * ex[g][k];
+                s1 += cv * e1[g][k];
+                s2 += cv * e2[g][k];
+            }
+        } else {
+            for (int k = 0; k < S; ++k) s0 += cu[(size_t)k * S] * ex[g][k];
+        }
+        if (!(s0 > 0.0)) s0 = 0.0;
+    }
+    P[e] = (Real)s0;
+    if (D1) D1[e] = (Real)s1;
+    if (D2) D2[e] = (Real)s2;
+    const size_t tix = off + j * SG + i;   // transposed image
+    static_cast<Real*>(jb.pt)[tix] = (Real)s0;
+    if (D1) static_cast<Real*>(jb.d1t)[tix] = (Real)s1;
+    if (D2) static_cast<Real*>(jb.d2t)[tix] = (Real)s2;
+}
+
 // op 0: out = a . b (convolution, CPU/BeagleCPUImpl.hpp:1096-1160);
 // op 1: out = transpose(a) (CPU/BeagleCPUImpl.hpp:1175-1222).
 // `out` holds 2n pointers: the n results, then their transposed images.
@@ -117,6 +182,17 @@ template <typename Real>
 cudaError_t launch_update_matrices(const MatJob* d_jobs, int njobs, const Dims& d,
                                    cudaStream_t s) {
     if (njobs == 0) return cudaSuccess;
+    const int nitems = njobs * d.C;
+    if (d.Sg == 4) {
+        k_update_matrices_small<Real, 4><<<(nitems + 15) / 16, 256, 0, s>>>(d_jobs, nitems, d.C,
+                                                                            d.S);
+        return cudaGetLastError();
+    }
+    if (d.Sg == 8) {
+        k_update_matrices_small<Real, 8><<<(nitems + 3) / 4, 256, 0, s>>>(d_jobs, nitems, d.C,
+                                                                          d.S);
+        return cudaGetLastError();
+    }
     // Entries split over blocks in slices of 1024 (4 a thread): 4 slices for
     // 61 states, one for 20 or fewer.
     dim3 grid(njobs, d.C, (d.Sg * d.Sg + 1023) / 1024);

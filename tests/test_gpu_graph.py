@@ -77,3 +77,33 @@ def test_whole_step_graph_with_new_lengths(b200, syn, precision, S, C, fused):
     assert rel(graphed.getLogLikelihood(), l2) <= (1e-13 if precision == "double" else tol["lnl"])
     plain.finalize()
     graphed.finalize()
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_graph_lengths_buffer_reusable_at_once(b200, syn, precision):
+    """beagleB200LaunchGraphWithLengths copies the lengths on the host before
+    it returns, pinned memory included: a caller that writes the next step's
+    lengths into the same pinned buffer right after the call (before any
+    wait), several launches deep, still gets each launch's own lengths."""
+    import torch
+    pr = syn.make_problem(S=4, N=12, P=700, C=4, seed=97, rescale=True)
+    pref, req = gpu_flags(precision)
+    plain = b200.create(*pr.create_args(), preferenceFlags=pref, requirementFlags=req)
+    graphed = b200.create(*pr.create_args(), preferenceFlags=pref | ASYNCH,
+                          requirementFlags=req)
+    for x in (plain, graphed):
+        pr.load(x)
+    graph, grad = pr.capture_step(graphed, fused=True)
+    buf = torch.empty(pr.B, dtype=torch.float64).pin_memory().numpy()
+    rng = np.random.default_rng(4)
+    steps = [pr.lengths * (1 + 0.05 * rng.standard_normal(pr.B)) for _ in range(6)]
+    for t in steps:                       # six launches queued, the buffer reused each time
+        buf[:] = t
+        graphed.launchGraphWithLengths(graph, buf)
+        buf[:] = 123.0                    # overwritten before the launch could have run
+    lnl_last = graphed.getLogLikelihood()  # the last launch's result
+    l0, _ = pr.evaluate(plain, lengths=steps[-1], fused=True)
+    tol = 1e-13 if precision == "double" else TOL[precision]["lnl"]
+    assert rel(lnl_last, l0) <= tol, (lnl_last, l0)
+    plain.finalize()
+    graphed.finalize()
