@@ -1491,7 +1491,8 @@ int Instance::updatePrePartialsWithDerivatives(const int* ops, int count, const 
     const int ls = (int)log_scalers_;
     // Every variant leaves the sums in out_.  0: the pre-order walk and the
     // derivative kernels of the two calls; 1: the fused walk; 2: its
-    // pairs-only form with 2 patterns a thread (FP32 lists of sibling pairs).  The autotuner
+    // pairs-only form with 2 patterns a thread (FP32 lists of sibling pairs);
+    // 3: the fused walk with its matrices staged in shared memory.  The autotuner
     // times them when the list may run repeatedly (no op reads what a later
     // op writes); the first, untimed run also settles the two calls' own
     // autotuner choices.
@@ -1513,7 +1514,7 @@ int Instance::updatePrePartialsWithDerivatives(const int* ops, int count, const 
                       (double*)scratch_.ptr, (double*)out_.ptr, stream_, v);
     };
     const TuneKey key{kTuneFused, (int)dbl_, C_, Pp_, tune_count_class(count), device_};
-    int v = tune_pick(key, 3, idempotent, stream_, run);
+    int v = tune_pick(key, 4, idempotent, stream_, run);
     if (v < 0) v = 1;
     cudaError_t e = run(v);
     if (e == cudaErrorInvalidValue && v == 2) {   // a forced pairs-only form the list refuses

@@ -383,6 +383,204 @@ k_pre_deriv4_pairs(const __grid_constant__ FusedParams F, int nops, int P, int P
     }
 }
 
+// ------------------------------------------------- staged-matrix fused walk
+// The fused walk with each op's three matrices in shared memory instead of
+// registers or per-lane global loads.  A chunk of ops' matrices is copied
+// into shared memory by the whole CTA, each in the orientation its op reads
+// it, as rows of 4 values:
+//   node   rows of P (the op's matrix given transposed is turned back), for
+//          out_j = sum_i P[i][j] z_i;
+//   sib    rows of P_sib for a partials sibling (y = P_sib x), its
+//          transpose for a tip sibling (column s = one row);
+//   deriv  rows of D for a partials post-order row, its transpose for a tip.
+// Within a category's 4 rows the order is rotated by c / 2, so the lanes of
+// one pattern group (one category each) reading the same row index hit
+// distinct banks.  Chunks never split a sibling pair.
+template <typename Real, int C>
+constexpr int fused_chunk() {
+    return 12288 / (3 * C * 16 * (int)sizeof(Real)) < 32 ? 12288 / (3 * C * 16 * (int)sizeof(Real))
+                                                         : 32;
+}
+
+template <int C>
+__device__ __forceinline__ int mat3_row(int k, int w, int c, int i) {
+    return (((k * 3 + w) * C + c) * 4 + ((i + (c >> 1)) & 3)) * 4;
+}
+
+template <typename Real>
+__device__ __forceinline__ void lds4(const Real* r, Real m[4]) {
+    if constexpr (sizeof(Real) == 4) {
+        const float4 q = *reinterpret_cast<const float4*>(r);
+        m[0] = q.x; m[1] = q.y; m[2] = q.z; m[3] = q.w;
+    } else {
+        const double2 a = reinterpret_cast<const double2*>(r)[0];
+        const double2 b = reinterpret_cast<const double2*>(r)[1];
+        m[0] = a.x; m[1] = a.y; m[2] = b.x; m[3] = b.y;
+    }
+}
+
+template <typename Real, int C>
+__device__ __forceinline__ void stage_mats3(Real* sm, const PreDerivOp* ops, int n) {
+    for (int u = threadIdx.x; u < n * 3 * C * 4; u += kT4) {
+        const int i = u & 3, c = (u >> 2) % C, w = (u / (4 * C)) % 3, k = u / (12 * C);
+        const PreDerivOp& op = ops[k];
+        const void* src = w == 0 ? op.mnode : w == 1 ? op.msib : op.dmat;
+        const bool tr = w == 0 ? (op.kind & kM1Transposed) != 0
+                      : w == 1 ? (op.kind & kX2States) != 0
+                               : (op.kind & kPostStates) != 0;
+        const Real* M = static_cast<const Real*>(src) + c * 16;
+        Real v[4];
+        if (tr) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[j] = __ldg(M + j * 4 + i);
+        } else {
+            ldg4(M + i * 4, v);
+        }
+        Real* d = sm + mat3_row<C>(k, w, c, i);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) d[j] = v[j];
+    }
+}
+
+// y = P_sib x, or column s of P_sib for a tip (pad for the missing state).
+template <typename Real, int C>
+__device__ __forceinline__ void sib_operand(const Real* sm, int k, int c, bool states, int s,
+                                            const Real x[4], Real pad, Real y[4]) {
+    if (states) {
+        lds4(sm + mat3_row<C>(k, 1, c, s & 3), y);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) y[i] = s < 4 ? y[i] : pad;
+    } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            Real m[4];
+            lds4(sm + mat3_row<C>(k, 1, c, i), m);
+            y[i] = m[0] * x[0] + m[1] * x[1] + m[2] * x[2] + m[3] * x[3];
+        }
+    }
+}
+
+// out_j = sum_i P[i][j] z_i.
+template <typename Real, int C>
+__device__ __forceinline__ void node_apply(const Real* sm, int k, int c, const Real z[4],
+                                           Real out[4]) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) out[j] = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        Real m[4];
+        lds4(sm + mat3_row<C>(k, 0, c, i), m);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) out[j] += m[j] * z[i];
+    }
+}
+
+// deriv_value with D's rows (or its transpose's, for a tip) from the chunk.
+template <typename Real, int C>
+__device__ __forceinline__ Real deriv_staged(const Real* sm, int k, Real dpad, const Real pre[4],
+                                             const Real x[4], int s, bool states, int c, Real w) {
+    Real n = 0, q = 0;
+    if (states) {
+        Real d[4];
+        lds4(sm + mat3_row<C>(k, 2, c, s & 3), d);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            n += pre[j] * (s < 4 ? d[j] : dpad);
+            q += (s >= 4 || j == s) ? pre[j] : Real(0);
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            Real m[4];
+            lds4(sm + mat3_row<C>(k, 2, c, j), m);
+            const Real y = m[0] * x[0] + m[1] * x[1] + m[2] * x[2] + m[3] * x[3];
+            n += pre[j] * y;
+            q += pre[j] * x[j];
+        }
+    }
+    Real num = w * n, den = w * q;
+#pragma unroll
+    for (int o = 1; o < C; o <<= 1) {
+        num += __shfl_xor_sync(0xffffffffu, num, o);
+        den += __shfl_xor_sync(0xffffffffu, den, o);
+    }
+    return quotient(num, den);
+}
+
+template <typename Real, int C>
+__global__ void __launch_bounds__(kT4, sizeof(Real) == 4 ? 4 : 2)
+k_pre_deriv4s(const __grid_constant__ FusedParams F, int nops, int P, int Pp,
+              const double* __restrict__ catw, const double* __restrict__ patw, int log_scalers,
+              double* block) {
+    constexpr int K = fused_chunk<Real, C>();
+    __shared__ __align__(16) Real s_m[K * 3 * C * 16];
+    const int c = threadIdx.x % C;
+    const int p = blockIdx.x * (kT4 / C) + threadIdx.x / C;
+    const bool valid = p < Pp;
+    const int pc = valid ? p : Pp - 1;
+    const Real w = (Real)catw[c];
+    const bool counted = c == 0 && p < P;
+    const Real wp = counted ? (Real)patw[p] : Real(0);
+    const int nblk = gridDim.x * (kT4 / 32);
+    const int wid = blockIdx.x * (kT4 / 32) + threadIdx.x / 32;
+    for (int o0 = 0; o0 < nops;) {
+        int n = min(K, nops - o0);
+        if (o0 + n < nops && (F.op[o0 + n - 1].kind & kPairFirst)) --n;
+        __syncthreads();
+        stage_mats3<Real, C>(s_m, F.op + o0, n);
+        __syncthreads();
+        for (int k = 0; k < n;) {
+            const PreDerivOp& A = F.op[o0 + k];
+            Real pv[4];
+            ld4(static_cast<const Real*>(A.parent) + ((size_t)pc * C + c) * 4, pv);
+            if (A.kind & kPairFirst) {
+                const PreDerivOp& B = F.op[o0 + k + 1];
+                const bool sta = A.kind & kPostStates, stb = A.kind & kX2States;
+                Real xa[4], xb[4];
+                int sa = 0, sb = 0;
+                load_row(A.post, sta, pc, C, c, xa, sa);     // post[a] (= B's sibling)
+                load_row(A.sib, stb, pc, C, c, xb, sb);      // post[b] (= A's sibling)
+                Real y[4], z[4], pa[4], pb[4];
+                sib_operand<Real, C>(s_m, k, c, stb, sb, xb, (Real)A.pad_sib, y);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) z[i] = pv[i] * y[i];
+                node_apply<Real, C>(s_m, k, c, z, pa);
+                sib_operand<Real, C>(s_m, k + 1, c, sta, sa, xa, (Real)B.pad_sib, y);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) z[i] = pv[i] * y[i];
+                node_apply<Real, C>(s_m, k + 1, c, z, pb);
+                rescale_store4<Real, C>(A, pa, pc, valid, c, log_scalers);
+                rescale_store4<Real, C>(B, pb, pc, valid, c, log_scalers);
+                const Real da =
+                    deriv_staged<Real, C>(s_m, k, (Real)A.dpad, pa, xa, sa, sta, c, w);
+                const Real db =
+                    deriv_staged<Real, C>(s_m, k + 1, (Real)B.dpad, pb, xb, sb, stb, c, w);
+                warp_emit<Real, C>(counted ? da : Real(0), wp, o0 + k, nops, nblk, wid, block);
+                warp_emit<Real, C>(counted ? db : Real(0), wp, o0 + k + 1, nops, nblk, wid,
+                                   block);
+                k += 2;
+            } else {
+                const bool sts = A.kind & kX2States, stp = A.kind & kPostStates;
+                Real xs[4], xp[4];
+                int ss = 0, sp = 0;
+                load_row(A.sib, sts, pc, C, c, xs, ss);
+                load_row(A.post, stp, pc, C, c, xp, sp);
+                Real y[4], z[4], pa[4];
+                sib_operand<Real, C>(s_m, k, c, sts, ss, xs, (Real)A.pad_sib, y);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) z[i] = pv[i] * y[i];
+                node_apply<Real, C>(s_m, k, c, z, pa);
+                rescale_store4<Real, C>(A, pa, pc, valid, c, log_scalers);
+                const Real da =
+                    deriv_staged<Real, C>(s_m, k, (Real)A.dpad, pa, xp, sp, stp, c, w);
+                warp_emit<Real, C>(counted ? da : Real(0), wp, o0 + k, nops, nblk, wid, block);
+                k += 1;
+            }
+        }
+        o0 += n;
+    }
+}
+
 // ------------------------------------------------------ batched fused walk
 // The fused walk over several instances with one category count: CTA x
 // belongs to the segment whose first_cta is the largest one <= x, and walks
@@ -579,6 +777,18 @@ cudaError_t pre_deriv4_chunk(const PreDerivOp* h_ops, int nops, const Dims& d,
         return final_sums(grid2 * (kT4 / 32));
     }
     const int grid = (d.Pp + kT4 / d.C - 1) / (kT4 / d.C);
+    if (variant == 3) {
+        // the staged-matrix walk
+        switch (d.C) {
+            case 1: k_pre_deriv4s<Real, 1><<<grid, kT4, 0, s>>>(prm, nops, d.P, d.Pp, catw, patw, ls, d_block); break;
+            case 2: k_pre_deriv4s<Real, 2><<<grid, kT4, 0, s>>>(prm, nops, d.P, d.Pp, catw, patw, ls, d_block); break;
+            case 4: k_pre_deriv4s<Real, 4><<<grid, kT4, 0, s>>>(prm, nops, d.P, d.Pp, catw, patw, ls, d_block); break;
+            default: k_pre_deriv4s<Real, 8><<<grid, kT4, 0, s>>>(prm, nops, d.P, d.Pp, catw, patw, ls, d_block); break;
+        }
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        return final_sums(fused_blocks(d));
+    }
     bool shared_d = true;             // one derivative matrix for every branch
     for (int k = 1; k < nops; ++k)
         shared_d = shared_d && h_ops[k].dmat == h_ops[0].dmat && h_ops[k].dpad == h_ops[0].dpad;

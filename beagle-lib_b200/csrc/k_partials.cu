@@ -112,18 +112,108 @@ k_pre4c(const __grid_constant__ OpParams P, int nops, int Pp, int log_scalers) {
 // log sum_c w_c sum_i pi_i root[c][i] + cumulative, the category sum by
 // shuffles inside the pattern's lane group.  Per-warp weighted sums go to
 // `block` for the final fixed-order sum.
+// Matrices of a chunk of root_chunk ops (16 KB) in shared memory,
+// [op][M1, M2][c][row] rows of 4 values.  The row order inside a category's block is rotated by
+// c / 2 so the C lane-group members reading row i of their own category hit
+// distinct banks (FP32: C 16-byte pieces in one wavefront).
 template <typename Real, int C>
-__global__ void __launch_bounds__(kT4)
+constexpr int root_chunk() {
+    return 16384 / (2 * C * 16 * (int)sizeof(Real)) < 64 ? 16384 / (2 * C * 16 * (int)sizeof(Real))
+                                                         : 64;
+}
+
+template <typename Real, int C>
+__device__ __forceinline__ int mat_row(int k, int w, int c, int i) {
+    return (((k * 2 + w) * C + c) * 4 + ((i + (c >> 1)) & 3)) * 4;
+}
+
+// An operand given as tip states reads one column of M_c, so its matrix is
+// staged transposed: that column is then one row of 4 values.
+template <typename Real, int C>
+__device__ __forceinline__ void stage_mats(Real* sm, const OpParams& P, int o0, int n) {
+    for (int u = threadIdx.x; u < n * 2 * C * 4; u += kT4) {
+        const int i = u & 3, c = (u >> 2) % C, w = (u / (4 * C)) & 1, k = u / (8 * C);
+        const OpDesc& op = P.op[o0 + k];
+        const Real* M = static_cast<const Real*>(w ? op.m2 : op.m1) + c * 16;
+        Real v[4];
+        if (op.kind & (w ? kX2States : kX1States)) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[j] = __ldg(M + j * 4 + i);
+        } else {
+            ldg4(M + i * 4, v);
+        }
+        Real* d = sm + mat_row<Real, C>(k, w, c, i);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) d[j] = v[j];
+    }
+}
+
+template <typename Real>
+__device__ __forceinline__ void lds4(const Real* r, Real m[4]) {
+    if constexpr (sizeof(Real) == 4) {
+        const float4 q = *reinterpret_cast<const float4*>(r);
+        m[0] = q.x; m[1] = q.y; m[2] = q.z; m[3] = q.w;
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) m[j] = r[j];
+    }
+}
+
+// y = M_c . x (or column s of M_c, a row of the transposed image) with the
+// rows from the staged chunk.
+template <typename Real, int C>
+__device__ __forceinline__ void operand4s(const Real* sm, int k, int w, int c, bool states, int s,
+                                          const Real x[4], Real pad, Real y[4]) {
+    if (states) {
+        lds4(sm + mat_row<Real, C>(k, w, c, s & 3), y);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) y[i] = s < 4 ? y[i] : pad;
+    } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            Real m[4];
+            lds4(sm + mat_row<Real, C>(k, w, c, i), m);
+            y[i] = m[0] * x[0] + m[1] * x[1] + m[2] * x[2] + m[3] * x[3];
+        }
+    }
+}
+
+template <typename Real, int C>
+__global__ void __launch_bounds__(kT4, sizeof(Real) == 4 ? 6 : 1)
 k_post4root(const __grid_constant__ OpParams P, int nops, int Pp, int Pn, double* cum,
             int log_scalers, const double* __restrict__ catw, const double* __restrict__ freqs,
             const double* __restrict__ patw, double* site, double* block) {
+    constexpr int K = root_chunk<Real, C>();
+    __shared__ __align__(16) Real s_m[K * 2 * C * 16];
     const int c = threadIdx.x % C;
     const int p0 = blockIdx.x * (kT4 / C) + threadIdx.x / C;
+    const int p = min(p0, Pp - 1);
+    const bool valid = p0 < Pp;
     double acc = 0;
-    for (int o = 0; o < nops; ++o)
-        post4_op<Real, C, 1, false>(P.op[o], c, p0, 0, Pp, nullptr, log_scalers, &acc);
+    for (int o0 = 0; o0 < nops; o0 += K) {
+        const int n = min(K, nops - o0);
+        __syncthreads();
+        stage_mats<Real, C>(s_m, P, o0, n);
+        __syncthreads();
+        for (int k = 0; k < n; ++k) {
+            const OpDesc& op = P.op[o0 + k];
+            const bool st1 = op.kind & kX1States, st2 = op.kind & kX2States;
+            Real x1[4], x2[4];
+            int s1 = 0, s2 = 0;
+            if (st1) s1 = static_cast<const int*>(op.x1)[p];
+            else ld4(static_cast<const Real*>(op.x1) + ((size_t)p * C + c) * 4, x1);
+            if (st2) s2 = static_cast<const int*>(op.x2)[p];
+            else ld4(static_cast<const Real*>(op.x2) + ((size_t)p * C + c) * 4, x2);
+            Real y1[4], y2[4];
+            operand4s<Real, C>(s_m, k, 0, c, st1, s1, x1, (Real)op.pad1, y1);
+            operand4s<Real, C>(s_m, k, 1, c, st2, s2, x2, (Real)op.pad2, y2);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) y1[i] *= y2[i];
+            finish4c<Real, C, false>(op, y1, p, valid, c, nullptr, log_scalers, &acc);
+        }
+    }
     Real x[4];
-    ld4(static_cast<const Real*>(P.op[nops - 1].dest) + ((size_t)min(p0, Pp - 1) * C + c) * 4, x);
+    ld4(static_cast<const Real*>(P.op[nops - 1].dest) + ((size_t)p * C + c) * 4, x);
     const double w = catw[c];
     double l = 0;
 #pragma unroll

@@ -719,7 +719,7 @@ def run_b200_arm(args):
     # With the fused walk picked, the "deriv" phase is that one kernel (plus
     # its final sum); otherwise the phases of the two calls are timed apart.
     tuned = inst.tunedVariants()
-    fused_walk = tuned["fused"] == 1
+    fused_walk = tuned["fused"] > 0          # any fused-walk variant (1-3)
     nph = max(5, min(50, args.steps // 4))
     ph_ms = phase_times(torch, inst, pr, nph, fused_walk)
     peak, peak_kind = peaks()

@@ -25,11 +25,12 @@ def _pair(b200, pr, precision, **kw):
 @pytest.mark.parametrize("precision", ["double", "single"])
 @pytest.mark.parametrize("C,rescale,amb", [(1, True, 0.0), (2, False, 0.03), (4, True, 0.03),
                                            (8, True, 0.0)])
-@pytest.mark.parametrize("form", [1, 2])
+@pytest.mark.parametrize("form", [1, 2, 3])
 def test_fused_matches_separate_calls_and_oracle(b200, syn, oracle, monkeypatch, precision, C,
                                                  rescale, amb, form):
     """form 1: the fused walk; 2: its pairs-only, 2-patterns-a-thread form
-    (FP32 only: an FP64 instance forced to it runs form 1)."""
+    (FP32 only: an FP64 instance forced to it runs form 1); 3: the fused walk
+    with its matrices staged in shared memory."""
     monkeypatch.setenv("BEAGLE_B200_FORCE_VARIANT", f"-1,-1,-1,{form}")
     pr = syn.make_problem(S=4, N=33, P=1300, C=C, seed=500 + C, rescale=rescale, ambiguous=amb)
     inst = _pair(b200, pr, precision)
@@ -57,9 +58,11 @@ def test_fused_matches_separate_calls_and_oracle(b200, syn, oracle, monkeypatch,
 
 
 @pytest.mark.parametrize("precision", ["double", "single"])
-def test_fused_without_sibling_pairs(b200, syn, precision):
+@pytest.mark.parametrize("form", [1, 3])
+def test_fused_without_sibling_pairs(b200, syn, monkeypatch, precision, form):
     """Pre-order ops sorted by depth, then by node: siblings are not adjacent,
     so every op runs on its own (three loads, one store)."""
+    monkeypatch.setenv("BEAGLE_B200_FORCE_VARIANT", f"-1,-1,-1,{form}")
     pr = syn.make_problem(S=4, N=40, P=900, C=4, seed=61, rescale=True)
     inst = _pair(b200, pr, precision)
     l0, g0 = pr.evaluate(inst)
@@ -72,6 +75,7 @@ def test_fused_without_sibling_pairs(b200, syn, precision):
     assert adjacent < len(ops) // 4
     nodes = ops[:, 0] - pr.pre(0)
     sums, _ = inst.updatePrePartialsWithDerivatives(ops, nodes, np.full(pr.B, pr.B), [0])
+    assert inst.tunedVariants()["fused"] == form
     g1 = np.empty(pr.B)
     g1[nodes] = sums
     assert grad_err(g1, g0) <= TOL[precision]["grad"] * 1e-2
@@ -79,16 +83,19 @@ def test_fused_without_sibling_pairs(b200, syn, precision):
 
 
 @pytest.mark.parametrize("precision", ["double", "single"])
-@pytest.mark.parametrize("S,N", [(4, 150), (4, 300), (20, 12)])
+@pytest.mark.parametrize("S,N,form", [(4, 150, 1), (4, 300, 1), (4, 150, 3), (4, 300, 3),
+                                      (20, 12, 1)])
 def test_fused_long_lists_and_other_state_counts(b200, syn, oracle, monkeypatch, precision, S,
-                                                 N):
-    """More than 256 ops (N = 150: 298; N = 300: 598): the fused walk (forced)
-    runs as consecutive launches cut between sibling pairs.  S = 20 runs the
+                                                 N, form):
+    """More than 256 ops (N = 150: 298; N = 300: 598): the fused walk (forced,
+    form 1 or the staged form 3, whose shared-memory chunks are also cut
+    between sibling pairs) runs as consecutive launches cut between sibling
+    pairs.  S = 20 runs the
     tensor-core fused walk in FP32 (its derivative from the unscaled row and
     split products, so it agrees with the separate calls to the mixed path's
     tolerance) and the two separate calls in FP64.  Same results as the
     separate calls and the oracle."""
-    monkeypatch.setenv("BEAGLE_B200_FORCE_VARIANT", "-1,-1,-1,1")
+    monkeypatch.setenv("BEAGLE_B200_FORCE_VARIANT", f"-1,-1,-1,{form}")
     pr = syn.make_problem(S=S, N=N, P=500, C=4, seed=7 + S + N, rescale=True)
     inst = _pair(b200, pr, precision)
     tr = S > 4
@@ -102,7 +109,7 @@ def test_fused_long_lists_and_other_state_counts(b200, syn, oracle, monkeypatch,
     assert grad_err(g1, g0) <= (1e-12 if precision == "double" else
                                 tol["grad"] * (1e-2 if S == 4 else 1.0))
     if S == 4:
-        assert inst.tunedVariants()["fused"] == 1      # the fused walk ran
+        assert inst.tunedVariants()["fused"] == form   # the fused walk ran
     _, lo, go = run_oracle(oracle, pr)
     assert rel(l1, lo) <= tol["lnl"]
     assert grad_err(g1, go) <= tol["grad"]
