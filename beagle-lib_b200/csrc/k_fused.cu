@@ -507,6 +507,30 @@ __device__ __forceinline__ Real deriv_staged(const Real* sm, int k, Real dpad, c
     return quotient(num, den);
 }
 
+// warp_emit for the two branches of a sibling pair at once: the four sums
+// (w d and w d^2 of branches k and k + 1) are reduced over the warp's
+// patterns by recursive halving -- at the first two levels each lane passes
+// on half of what it holds -- so 3 + log2(32 / C) - 2 shuffles replace
+// 4 log2(32 / C); lanes 0, C, 2C, 3C then hold one sum each and store it.
+template <typename Real, int C>
+__device__ __forceinline__ void warp_emit_pair(Real va, Real vb, Real wp, int k, int nops,
+                                               int nblk, int wid, double* block) {
+    const int lane = threadIdx.x & 31;
+    const bool h1 = lane & C, h2 = lane & (2 * C);
+    const Real a1 = va * wp, a2 = va * va * wp, b1 = vb * wp, b2 = vb * vb * wp;
+    // level 1: lanes with h1 keep branch k + 1's sums, the others branch k's
+    Real u0 = h1 ? b1 : a1, u1 = h1 ? b2 : a2;
+    u0 += __shfl_xor_sync(0xffffffffu, h1 ? a1 : b1, C);
+    u1 += __shfl_xor_sync(0xffffffffu, h1 ? a2 : b2, C);
+    // level 2: lanes with h2 keep the square sum, the others the plain sum
+    Real v = h2 ? u1 : u0;
+    v += __shfl_xor_sync(0xffffffffu, h2 ? u0 : u1, 2 * C);
+#pragma unroll
+    for (int o = 4 * C; o < 32; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane < 4 * C && lane % C == 0)
+        block[(size_t)((h2 ? nops : 0) + k + (h1 ? 1 : 0)) * nblk + wid] = (double)v;
+}
+
 template <typename Real, int C>
 __global__ void __launch_bounds__(kT4, sizeof(Real) == 4 ? 4 : 2)
 k_pre_deriv4s(const __grid_constant__ FusedParams F, int nops, int P, int Pp,
@@ -555,9 +579,8 @@ k_pre_deriv4s(const __grid_constant__ FusedParams F, int nops, int P, int Pp,
                     deriv_staged<Real, C>(s_m, k, (Real)A.dpad, pa, xa, sa, sta, c, w);
                 const Real db =
                     deriv_staged<Real, C>(s_m, k + 1, (Real)B.dpad, pb, xb, sb, stb, c, w);
-                warp_emit<Real, C>(counted ? da : Real(0), wp, o0 + k, nops, nblk, wid, block);
-                warp_emit<Real, C>(counted ? db : Real(0), wp, o0 + k + 1, nops, nblk, wid,
-                                   block);
+                warp_emit_pair<Real, C>(counted ? da : Real(0), counted ? db : Real(0), wp,
+                                        o0 + k, nops, nblk, wid, block);
                 k += 2;
             } else {
                 const bool sts = A.kind & kX2States, stp = A.kind & kPostStates;
