@@ -605,102 +605,19 @@ k_pre_deriv4s(const __grid_constant__ FusedParams F, int nops, int P, int Pp,
 }
 
 // ------------------------------------------------------ batched fused walk
-// The fused walk over several instances with one category count: CTA x
-// belongs to the segment whose first_cta is the largest one <= x, and walks
-// that instance's op list (device memory, staged in shared memory in chunks
-// that never split a sibling pair).  Per op the same arithmetic as
-// k_pre_deriv4; whether a pair's matrices (kPairMats) and derivative matrix
-// (kPairD) are shared is read per op.
-constexpr int kBatchOps = 64;
-
+// The staged fused walk over several instances with one category count: CTA
+// x belongs to the segment whose first_cta is the largest one <= x, and walks
+// that instance's op list (device memory): each chunk's descriptors and
+// matrices are staged in shared memory together, chunks never splitting a
+// sibling pair.  Per op the arithmetic of k_pre_deriv4s.  The segment itself
+// stays in shared memory; its fields are read where they are used.
 template <typename Real, int C>
-__device__ __forceinline__ int pre_deriv4_step(const PreDerivOp* ops, int oi, int k, int nops,
-                                               int nblk, int wid, int pc, bool valid, int c,
-                                               Real w, bool counted, Real wp, int log_scalers,
-                                               double* block) {
-    const PreDerivOp& A = ops[oi];
-    const bool tra = A.kind & kM1Transposed;
-    Real pv[4];
-    ld4(static_cast<const Real*>(A.parent) + ((size_t)pc * C + c) * 4, pv);
-    if (A.kind & kPairFirst) {
-        const PreDerivOp& B = ops[oi + 1];
-        const bool sta = A.kind & kPostStates, stb = A.kind & kX2States;
-        Real xa[4], xb[4];
-        int sa = 0, sb = 0;
-        load_row(A.post, sta, pc, C, c, xa, sa);
-        load_row(A.sib, stb, pc, C, c, xb, sb);
-        Real ya[4], yb[4], za[4], zb[4], pa[4], pb[4];
-        if (A.kind & kPairMats) {
-            Real ma[16], mb[16];
-            const Real* Ma = static_cast<const Real*>(A.mnode) + c * 16;
-            const Real* Mb = static_cast<const Real*>(A.msib) + c * 16;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                ldg4(Ma + 4 * q, ma + 4 * q);
-                ldg4(Mb + 4 * q, mb + 4 * q);
-            }
-            operand4r(mb, stb, sb, xb, (Real)A.pad_sib, yb);
-            operand4r(ma, sta, sa, xa, (Real)B.pad_sib, ya);
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                za[i] = pv[i] * yb[i];
-                zb[i] = pv[i] * ya[i];
-            }
-            apply_reg(ma, za, pa);
-            apply_reg(mb, zb, pb);
-        } else {
-            operand4c(static_cast<const Real*>(A.msib) + c * 16, stb, sb, xb, (Real)A.pad_sib,
-                      yb);
-            operand4c(static_cast<const Real*>(B.msib) + c * 16, sta, sa, xa, (Real)B.pad_sib,
-                      ya);
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                za[i] = pv[i] * yb[i];
-                zb[i] = pv[i] * ya[i];
-            }
-            apply_node(static_cast<const Real*>(A.mnode) + c * 16, tra, za, pa);
-            apply_node(static_cast<const Real*>(B.mnode) + c * 16,
-                       (B.kind & kM1Transposed) != 0, zb, pb);
-        }
-        rescale_store4<Real, C>(A, pa, pc, valid, c, log_scalers);
-        rescale_store4<Real, C>(B, pb, pc, valid, c, log_scalers);
-        Real da, db;
-        if (A.kind & kPairD) {
-            Real dp[16];
-            const Real* D = static_cast<const Real*>(A.dmat) + c * 16;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) ldg4(D + 4 * q, dp + 4 * q);
-            da = deriv_value<Real, C, true>(A, dp, pa, xa, sa, sta, c, w);
-            db = deriv_value<Real, C, true>(B, dp, pb, xb, sb, stb, c, w);
-        } else {
-            da = deriv_value<Real, C, false>(A, nullptr, pa, xa, sa, sta, c, w);
-            db = deriv_value<Real, C, false>(B, nullptr, pb, xb, sb, stb, c, w);
-        }
-        warp_emit<Real, C>(counted ? da : Real(0), wp, k, nops, nblk, wid, block);
-        warp_emit<Real, C>(counted ? db : Real(0), wp, k + 1, nops, nblk, wid, block);
-        return 2;
-    }
-    const bool sts = A.kind & kX2States, stp = A.kind & kPostStates;
-    Real xs[4], xp[4];
-    int ss = 0, sp = 0;
-    load_row(A.sib, sts, pc, C, c, xs, ss);
-    load_row(A.post, stp, pc, C, c, xp, sp);
-    Real y[4], z[4], pa[4];
-    operand4c(static_cast<const Real*>(A.msib) + c * 16, sts, ss, xs, (Real)A.pad_sib, y);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) z[i] = pv[i] * y[i];
-    apply_node(static_cast<const Real*>(A.mnode) + c * 16, tra, z, pa);
-    rescale_store4<Real, C>(A, pa, pc, valid, c, log_scalers);
-    const Real da = deriv_value<Real, C, false>(A, nullptr, pa, xp, sp, stp, c, w);
-    warp_emit<Real, C>(counted ? da : Real(0), wp, k, nops, nblk, wid, block);
-    return 1;
-}
-
-template <typename Real, int C>
-__global__ void __launch_bounds__(kT4, sizeof(Real) == 4 ? 3 : 2)
+__global__ void __launch_bounds__(kT4, sizeof(Real) == 4 ? 4 : 2)
 k_pre_deriv4_batch(const PreDerivSeg* __restrict__ segs, int nseg) {
-    __shared__ PreDerivOp s_ops[kBatchOps];
-    __shared__ int s_seg;
+    constexpr int K = fused_chunk<Real, C>();
+    __shared__ PreDerivOp s_ops[K];
+    __shared__ __align__(16) Real s_m[K * 3 * C * 16];
+    __shared__ PreDerivSeg sg;
     if (threadIdx.x == 0) {
         int lo = 0, hi = nseg - 1;
         while (lo < hi) {
@@ -708,33 +625,81 @@ k_pre_deriv4_batch(const PreDerivSeg* __restrict__ segs, int nseg) {
             if (segs[mid].first_cta <= (int)blockIdx.x) lo = mid;
             else hi = mid - 1;
         }
-        s_seg = lo;
+        sg = segs[lo];
     }
     __syncthreads();
-    const PreDerivSeg sg = segs[s_seg];
     const int c = threadIdx.x % C;
     const int local = blockIdx.x - sg.first_cta;
     const int p = local * (kT4 / C) + threadIdx.x / C;
-    const bool valid = p < sg.Pp;
-    const int pc = valid ? p : sg.Pp - 1;
+    const int Pp = sg.Pp;
+    const bool valid = p < Pp;
+    const int pc = valid ? p : Pp - 1;
     const Real w = (Real)sg.catw[c];
     const bool counted = c == 0 && p < sg.P;
     const Real wp = counted ? (Real)sg.patw[p] : Real(0);
     const int wid = local * (kT4 / 32) + threadIdx.x / 32;
-    for (int o0 = 0; o0 < sg.nops;) {
-        int n = min(kBatchOps, sg.nops - o0);
-        if (o0 + n < sg.nops && (sg.fops[o0 + n - 1].kind & kPairFirst)) --n;
+    const int nops = sg.nops;
+    for (int o0 = 0; o0 < nops;) {
+        const PreDerivOp* fops = sg.fops + o0;
+        int n = min(K, nops - o0);
+        if (o0 + n < nops && (fops[n - 1].kind & kPairFirst)) --n;
         __syncthreads();
         {
-            const int* src = reinterpret_cast<const int*>(sg.fops + o0);
+            const int* src = reinterpret_cast<const int*>(fops);
             int* dst = reinterpret_cast<int*>(s_ops);
             const int words = n * (int)(sizeof(PreDerivOp) / sizeof(int));
             for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
         }
+        stage_mats3<Real, C>(s_m, fops, n);
         __syncthreads();
-        for (int oi = 0; oi < n;)
-            oi += pre_deriv4_step<Real, C>(s_ops, oi, o0 + oi, sg.nops, sg.nblk, wid, pc, valid, c,
-                                           w, counted, wp, sg.log_scalers, sg.block);
+        for (int k = 0; k < n;) {
+            const PreDerivOp& A = s_ops[k];
+            Real pv[4];
+            ld4(static_cast<const Real*>(A.parent) + ((size_t)pc * C + c) * 4, pv);
+            if (A.kind & kPairFirst) {
+                const PreDerivOp& B = s_ops[k + 1];
+                const bool sta = A.kind & kPostStates, stb = A.kind & kX2States;
+                Real xa[4], xb[4];
+                int sa = 0, sb = 0;
+                load_row(A.post, sta, pc, C, c, xa, sa);
+                load_row(A.sib, stb, pc, C, c, xb, sb);
+                Real y[4], z[4], pa[4], pb[4];
+                sib_operand<Real, C>(s_m, k, c, stb, sb, xb, (Real)A.pad_sib, y);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) z[i] = pv[i] * y[i];
+                node_apply<Real, C>(s_m, k, c, z, pa);
+                sib_operand<Real, C>(s_m, k + 1, c, sta, sa, xa, (Real)B.pad_sib, y);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) z[i] = pv[i] * y[i];
+                node_apply<Real, C>(s_m, k + 1, c, z, pb);
+                rescale_store4<Real, C>(A, pa, pc, valid, c, sg.log_scalers);
+                rescale_store4<Real, C>(B, pb, pc, valid, c, sg.log_scalers);
+                const Real da =
+                    deriv_staged<Real, C>(s_m, k, (Real)A.dpad, pa, xa, sa, sta, c, w);
+                const Real db =
+                    deriv_staged<Real, C>(s_m, k + 1, (Real)B.dpad, pb, xb, sb, stb, c, w);
+                warp_emit_pair<Real, C>(counted ? da : Real(0), counted ? db : Real(0), wp,
+                                        o0 + k, nops, sg.nblk, wid, sg.block);
+                k += 2;
+            } else {
+                const bool sts = A.kind & kX2States, stp = A.kind & kPostStates;
+                Real xs[4], xp[4];
+                int ss = 0, sp = 0;
+                load_row(A.sib, sts, pc, C, c, xs, ss);
+                load_row(A.post, stp, pc, C, c, xp, sp);
+                Real y[4], z[4], pa[4];
+                sib_operand<Real, C>(s_m, k, c, sts, ss, xs, (Real)A.pad_sib, y);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) z[i] = pv[i] * y[i];
+                node_apply<Real, C>(s_m, k, c, z, pa);
+                rescale_store4<Real, C>(A, pa, pc, valid, c, sg.log_scalers);
+                const Real da =
+                    deriv_staged<Real, C>(s_m, k, (Real)A.dpad, pa, xp, sp, stp, c, w);
+                warp_emit<Real, C>(counted ? da : Real(0), wp, o0 + k, nops, sg.nblk, wid,
+                                   sg.block);
+                k += 1;
+            }
+        }
         o0 += n;
     }
 }
