@@ -129,14 +129,20 @@ __device__ __forceinline__ int mat_row(int k, int w, int c, int i) {
 
 // An operand given as tip states reads one column of M_c, so its matrix is
 // staged transposed: that column is then one row of 4 values.
-template <typename Real, int C>
+// PRE (pre-order ops): the first matrix is P of the op's branch, applied as
+// out_j = sum_i P[i][j] z_i, so it is staged as rows of P (given transposed,
+// kM1Transposed, it is turned back); the second is the sibling's, as for a
+// post-order child.
+template <typename Real, int C, bool PRE = false>
 __device__ __forceinline__ void stage_mats(Real* sm, const OpParams& P, int o0, int n) {
     for (int u = threadIdx.x; u < n * 2 * C * 4; u += kT4) {
         const int i = u & 3, c = (u >> 2) % C, w = (u / (4 * C)) & 1, k = u / (8 * C);
         const OpDesc& op = P.op[o0 + k];
         const Real* M = static_cast<const Real*>(w ? op.m2 : op.m1) + c * 16;
+        const bool tr = w ? (op.kind & kX2States) != 0
+                          : (op.kind & (PRE ? kM1Transposed : kX1States)) != 0;
         Real v[4];
-        if (op.kind & (w ? kX2States : kX1States)) {
+        if (tr) {
 #pragma unroll
             for (int j = 0; j < 4; ++j) v[j] = __ldg(M + j * 4 + i);
         } else {
@@ -233,6 +239,64 @@ k_post4root(const __grid_constant__ OpParams P, int nops, int Pp, int Pn, double
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if ((threadIdx.x & 31) == 0) block[(size_t)blockIdx.x * (kT4 / 32) + threadIdx.x / 32] = v;
+}
+
+// The parameter-list walks (variant 7) with each chunk of ops' matrices
+// staged in shared memory as k_post4root stages them (variant 14): the
+// per-op matrix reads are one-wavefront shared-memory rows instead of
+// per-lane global loads of the lane's category.
+template <typename Real, int C, bool PRE, bool RANGED>
+__global__ void __launch_bounds__(kT4, sizeof(Real) == 4 ? 6 : 1)
+k_walk4st(const __grid_constant__ OpParams P, int nops, int Pp, double* cum, int log_scalers) {
+    constexpr int K = root_chunk<Real, C>();
+    __shared__ __align__(16) Real s_m[K * 2 * C * 16];
+    const int c = threadIdx.x % C;
+    const int p0 = blockIdx.x * (kT4 / C) + threadIdx.x / C;
+    const int p = min(p0, Pp - 1);
+    const bool valid = p0 < Pp;
+    for (int o0 = 0; o0 < nops; o0 += K) {
+        const int n = min(K, nops - o0);
+        __syncthreads();
+        stage_mats<Real, C, PRE>(s_m, P, o0, n);
+        __syncthreads();
+        for (int k = 0; k < n; ++k) {
+            const OpDesc& op = P.op[o0 + k];
+            const bool st2 = op.kind & kX2States;
+            Real x2[4];
+            int s2 = 0;
+            if (st2) s2 = static_cast<const int*>(op.x2)[p];
+            else ld4(static_cast<const Real*>(op.x2) + ((size_t)p * C + c) * 4, x2);
+            Real y[4], out[4];
+            if constexpr (PRE) {
+                Real pv[4];
+                ld4(static_cast<const Real*>(op.x1) + ((size_t)p * C + c) * 4, pv);
+                operand4s<Real, C>(s_m, k, 1, c, st2, s2, x2, (Real)op.pad2, y);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) y[i] *= pv[i];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) out[j] = 0;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    Real m[4];
+                    lds4(s_m + mat_row<Real, C>(k, 0, c, i), m);
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) out[j] += m[j] * y[i];
+                }
+                finish4c<Real, C, RANGED>(op, out, p, valid, c, nullptr, log_scalers);
+            } else {
+                const bool st1 = op.kind & kX1States;
+                Real x1[4];
+                int s1 = 0;
+                if (st1) s1 = static_cast<const int*>(op.x1)[p];
+                else ld4(static_cast<const Real*>(op.x1) + ((size_t)p * C + c) * 4, x1);
+                operand4s<Real, C>(s_m, k, 0, c, st1, s1, x1, (Real)op.pad1, out);
+                operand4s<Real, C>(s_m, k, 1, c, st2, s2, x2, (Real)op.pad2, y);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) out[i] *= y[i];
+                finish4c<Real, C, RANGED>(op, out, p, valid, c, cum, log_scalers);
+            }
+        }
+    }
 }
 
 // -------------------------------------------------- S = 4, slot walks
@@ -752,7 +816,9 @@ constexpr int kMinB6 = sizeof(Real) == 4 ? 6 : 1;
 //          kernel parameter (one launch per kParamOps ops).
 //   9,10   7, 8 with results that later ops read kept in shared-memory slots;
 //   11-13  the list reordered by dependency level, groups of 2, 4 or 8
-//          independent ops loaded together (one pattern per thread).
+//          independent ops loaded together (one pattern per thread);
+//   14     7 with each chunk of ops' matrices staged in shared memory
+//          (k_walk4st).
 // variant < 0 picks the default: the smallest patterns-per-thread whose grid
 // fits in one resident wave, thread per pattern when C does not divide 32.
 template <typename K>
@@ -820,6 +886,29 @@ cudaError_t run_param4(const OpDesc* h_ops, int nops, const Dims& d, double* cum
         } else {
             if (ranged) k_post4c<Real, C, PPT, true><<<grid, kT4, 0, s>>>(prm, n, d.Pp, cum, ls);
             else k_post4c<Real, C, PPT, false><<<grid, kT4, 0, s>>>(prm, n, d.Pp, cum, ls);
+        }
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// Variant 14: the staged walks, one launch per kParamOps ops.
+template <typename Real, int C>
+cudaError_t run_stage4(const OpDesc* h_ops, int nops, const Dims& d, double* cum, int ls,
+                       cudaStream_t s, bool ranged, bool pre) {
+    if (!h_ops) return cudaErrorInvalidValue;
+    static thread_local OpParams prm;
+    const int grid = (d.Pp + kT4 / C - 1) / (kT4 / C);
+    for (int o0 = 0; o0 < nops; o0 += kParamOps) {
+        const int n = std::min(kParamOps, nops - o0);
+        std::memcpy(prm.op, h_ops + o0, sizeof(OpDesc) * n);
+        if (pre) {
+            if (ranged) k_walk4st<Real, C, true, true><<<grid, kT4, 0, s>>>(prm, n, d.Pp, nullptr, ls);
+            else k_walk4st<Real, C, true, false><<<grid, kT4, 0, s>>>(prm, n, d.Pp, nullptr, ls);
+        } else {
+            if (ranged) k_walk4st<Real, C, false, true><<<grid, kT4, 0, s>>>(prm, n, d.Pp, cum, ls);
+            else k_walk4st<Real, C, false, false><<<grid, kT4, 0, s>>>(prm, n, d.Pp, cum, ls);
         }
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
@@ -953,6 +1042,7 @@ cudaError_t run_post4(const OpDesc* ops, const OpDesc* h_ops, int nops, const Di
             case 11: return run_group4<Real, CC, 2>(h_ops, nops, d, cum, ls, s, ranged, false);
             case 12: return run_group4<Real, CC, 4>(h_ops, nops, d, cum, ls, s, ranged, false);
             case 13: return run_group4<Real, CC, 8>(h_ops, nops, d, cum, ls, s, ranged, false);
+            case 14: return run_stage4<Real, CC>(h_ops, nops, d, cum, ls, s, ranged, false);
             case 1: return run_post4_ppt<Real, CC, 1>(ops, nops, d, cum, ls, s, ranged);
             case 2: return run_post4_ppt<Real, CC, 2>(ops, nops, d, cum, ls, s, ranged);
             default: return run_post4_ppt<Real, CC, 4>(ops, nops, d, cum, ls, s, ranged);
@@ -979,6 +1069,7 @@ cudaError_t run_pre4(const OpDesc* ops, const OpDesc* h_ops, int nops, const Dim
             case 11: return run_group4<Real, CC, 2>(h_ops, nops, d, nullptr, ls, s, ranged, true);
             case 12: return run_group4<Real, CC, 4>(h_ops, nops, d, nullptr, ls, s, ranged, true);
             case 13: return run_group4<Real, CC, 8>(h_ops, nops, d, nullptr, ls, s, ranged, true);
+            case 14: return run_stage4<Real, CC>(h_ops, nops, d, nullptr, ls, s, ranged, true);
             case 1: return run_pre4_ppt<Real, CC, 1>(ops, nops, d, ls, s, ranged);
             case 2: return run_pre4_ppt<Real, CC, 2>(ops, nops, d, ls, s, ranged);
             default: return run_pre4_ppt<Real, CC, 4>(ops, nops, d, ls, s, ranged);
@@ -1024,7 +1115,7 @@ template cudaError_t launch_post4_root<double>(const OpDesc*, int, const Dims&, 
                                                const double*, const double*, const double*,
                                                double*, double*, double*, cudaStream_t);
 
-int s4_walk_variants(int C) { return (32 % C == 0) ? 14 : 1; }
+int s4_walk_variants(int C) { return (32 % C == 0) ? 15 : 1; }
 
 template <typename Real>
 cudaError_t launch_update_partials(const OpDesc* ops, int nops, const Dims& d, double* cum,

@@ -181,7 +181,7 @@ def test_full_size_configs(b200, syn, oracle, name, precision):
 
 
 @pytest.mark.parametrize("precision", ["double", "single"])
-@pytest.mark.parametrize("variant", list(range(14)))
+@pytest.mark.parametrize("variant", list(range(15)))
 def test_s4_kernel_variants(b200, syn, oracle, monkeypatch, precision, variant):
     """Every S = 4 op-walk and derivative kernel shape the autotuner can pick
     (forced through BEAGLE_B200_FORCE_VARIANT) against the oracle, with C = 4
@@ -199,11 +199,12 @@ def test_s4_kernel_variants(b200, syn, oracle, monkeypatch, precision, variant):
 
 
 @pytest.mark.parametrize("precision", ["double", "single"])
-@pytest.mark.parametrize("variant", [7, 8])
+@pytest.mark.parametrize("variant", [7, 8, 14])
 def test_s4_parameter_walks_longer_than_one_launch(b200, syn, oracle, monkeypatch, precision,
                                                    variant):
-    """The parameter-list walks take 256 ops a launch: a 300-taxon tree (299
-    post-order, 598 pre-order ops) runs as consecutive launches."""
+    """The parameter-list walks (7, 8, and 14 with staged matrices) take 256
+    ops a launch: a 300-taxon tree (299 post-order, 598 pre-order ops) runs
+    as consecutive launches."""
     monkeypatch.setenv("BEAGLE_B200_FORCE_VARIANT", str(variant))
     pr = syn.make_problem(S=4, N=300, P=700, C=4, seed=77 + variant, rescale=True)
     inst, lnl, g = run_b200(b200, pr, precision)
@@ -245,7 +246,8 @@ def test_s4_slot_walks_more_live_values_than_slots(b200, syn, oracle, monkeypatc
 
 
 @pytest.mark.parametrize("precision", ["double", "single"])
-@pytest.mark.parametrize("S,C,variant", [(4, 4, 1), (4, 4, 4), (4, 3, 0), (20, 4, 0), (20, 4, 1)])
+@pytest.mark.parametrize("S,C,variant", [(4, 4, 1), (4, 4, 4), (4, 4, 14), (4, 3, 0), (20, 4, 0),
+                                         (20, 4, 1)])
 def test_partitions(b200, syn, oracle, monkeypatch, precision, S, C, variant):
     """updatePartialsByPartition / updatePrePartialsByPartition (one launch
     each over every partition's ops) and calculateRootLogLikelihoodsByPartition
