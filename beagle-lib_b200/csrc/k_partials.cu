@@ -134,10 +134,10 @@ __device__ __forceinline__ int mat_row(int k, int w, int c, int i) {
 // kM1Transposed, it is turned back); the second is the sibling's, as for a
 // post-order child.
 template <typename Real, int C, bool PRE = false>
-__device__ __forceinline__ void stage_mats(Real* sm, const OpParams& P, int o0, int n) {
+__device__ __forceinline__ void stage_mats(Real* sm, const OpDesc* ops, int n) {
     for (int u = threadIdx.x; u < n * 2 * C * 4; u += kT4) {
         const int i = u & 3, c = (u >> 2) % C, w = (u / (4 * C)) & 1, k = u / (8 * C);
-        const OpDesc& op = P.op[o0 + k];
+        const OpDesc& op = ops[k];
         const Real* M = static_cast<const Real*>(w ? op.m2 : op.m1) + c * 16;
         const bool tr = w ? (op.kind & kX2States) != 0
                           : (op.kind & (PRE ? kM1Transposed : kX1States)) != 0;
@@ -199,7 +199,7 @@ k_post4root(const __grid_constant__ OpParams P, int nops, int Pp, int Pn, double
     for (int o0 = 0; o0 < nops; o0 += K) {
         const int n = min(K, nops - o0);
         __syncthreads();
-        stage_mats<Real, C>(s_m, P, o0, n);
+        stage_mats<Real, C>(s_m, P.op + o0, n);
         __syncthreads();
         for (int k = 0; k < n; ++k) {
             const OpDesc& op = P.op[o0 + k];
@@ -245,6 +245,47 @@ k_post4root(const __grid_constant__ OpParams P, int nops, int Pp, int Pn, double
 // staged in shared memory as k_post4root stages them (variant 14): the
 // per-op matrix reads are one-wavefront shared-memory rows instead of
 // per-lane global loads of the lane's category.
+// One op of the staged walks: op k of the staged chunk, this thread's
+// pattern p (stores only when valid).
+template <typename Real, int C, bool PRE, bool RANGED>
+__device__ __forceinline__ void walk4st_op(const OpDesc& op, const Real* s_m, int k, int c, int p,
+                                           bool valid, double* cum, int log_scalers) {
+    const bool st2 = op.kind & kX2States;
+    Real x2[4];
+    int s2 = 0;
+    if (st2) s2 = static_cast<const int*>(op.x2)[p];
+    else ld4(static_cast<const Real*>(op.x2) + ((size_t)p * C + c) * 4, x2);
+    Real y[4], out[4];
+    if constexpr (PRE) {
+        Real pv[4];
+        ld4(static_cast<const Real*>(op.x1) + ((size_t)p * C + c) * 4, pv);
+        operand4s<Real, C>(s_m, k, 1, c, st2, s2, x2, (Real)op.pad2, y);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) y[i] *= pv[i];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) out[j] = 0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            Real m[4];
+            lds4(s_m + mat_row<Real, C>(k, 0, c, i), m);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) out[j] += m[j] * y[i];
+        }
+        finish4c<Real, C, RANGED>(op, out, p, valid, c, nullptr, log_scalers);
+    } else {
+        const bool st1 = op.kind & kX1States;
+        Real x1[4];
+        int s1 = 0;
+        if (st1) s1 = static_cast<const int*>(op.x1)[p];
+        else ld4(static_cast<const Real*>(op.x1) + ((size_t)p * C + c) * 4, x1);
+        operand4s<Real, C>(s_m, k, 0, c, st1, s1, x1, (Real)op.pad1, out);
+        operand4s<Real, C>(s_m, k, 1, c, st2, s2, x2, (Real)op.pad2, y);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) out[i] *= y[i];
+        finish4c<Real, C, RANGED>(op, out, p, valid, c, cum, log_scalers);
+    }
+}
+
 template <typename Real, int C, bool PRE, bool RANGED>
 __global__ void __launch_bounds__(kT4, sizeof(Real) == 4 ? 6 : 1)
 k_walk4st(const __grid_constant__ OpParams P, int nops, int Pp, double* cum, int log_scalers) {
@@ -257,45 +298,10 @@ k_walk4st(const __grid_constant__ OpParams P, int nops, int Pp, double* cum, int
     for (int o0 = 0; o0 < nops; o0 += K) {
         const int n = min(K, nops - o0);
         __syncthreads();
-        stage_mats<Real, C, PRE>(s_m, P, o0, n);
+        stage_mats<Real, C, PRE>(s_m, P.op + o0, n);
         __syncthreads();
-        for (int k = 0; k < n; ++k) {
-            const OpDesc& op = P.op[o0 + k];
-            const bool st2 = op.kind & kX2States;
-            Real x2[4];
-            int s2 = 0;
-            if (st2) s2 = static_cast<const int*>(op.x2)[p];
-            else ld4(static_cast<const Real*>(op.x2) + ((size_t)p * C + c) * 4, x2);
-            Real y[4], out[4];
-            if constexpr (PRE) {
-                Real pv[4];
-                ld4(static_cast<const Real*>(op.x1) + ((size_t)p * C + c) * 4, pv);
-                operand4s<Real, C>(s_m, k, 1, c, st2, s2, x2, (Real)op.pad2, y);
-#pragma unroll
-                for (int i = 0; i < 4; ++i) y[i] *= pv[i];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) out[j] = 0;
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    Real m[4];
-                    lds4(s_m + mat_row<Real, C>(k, 0, c, i), m);
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) out[j] += m[j] * y[i];
-                }
-                finish4c<Real, C, RANGED>(op, out, p, valid, c, nullptr, log_scalers);
-            } else {
-                const bool st1 = op.kind & kX1States;
-                Real x1[4];
-                int s1 = 0;
-                if (st1) s1 = static_cast<const int*>(op.x1)[p];
-                else ld4(static_cast<const Real*>(op.x1) + ((size_t)p * C + c) * 4, x1);
-                operand4s<Real, C>(s_m, k, 0, c, st1, s1, x1, (Real)op.pad1, out);
-                operand4s<Real, C>(s_m, k, 1, c, st2, s2, x2, (Real)op.pad2, y);
-#pragma unroll
-                for (int i = 0; i < 4; ++i) out[i] *= y[i];
-                finish4c<Real, C, RANGED>(op, out, p, valid, c, cum, log_scalers);
-            }
-        }
+        for (int k = 0; k < n; ++k)
+            walk4st_op<Real, C, PRE, RANGED>(P.op[o0 + k], s_m, k, c, p, valid, cum, log_scalers);
     }
 }
 
@@ -777,26 +783,34 @@ __device__ __forceinline__ int find_walk_seg(const WalkSeg* segs, int nseg, int 
     return lo;
 }
 
+// The batched walk: CTA x walks the op list (device memory) of the segment
+// whose first_cta is the largest one <= x, each chunk's descriptors and
+// matrices staged in shared memory together (as k_walk4st).  The segment
+// itself stays in shared memory.
 template <typename Real, int C, bool PRE>
-__global__ void __launch_bounds__(kT4)
+__global__ void __launch_bounds__(kT4, sizeof(Real) == 4 ? 5 : 1)
 k_walk4_batch(const WalkSeg* __restrict__ segs, int nseg) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    OpDesc* s_ops = reinterpret_cast<OpDesc*>(smem_raw);
-    __shared__ int s_seg;
-    if (threadIdx.x == 0) s_seg = find_walk_seg(segs, nseg, blockIdx.x);
+    constexpr int K = root_chunk<Real, C>();
+    __shared__ OpDesc s_ops[K];
+    __shared__ __align__(16) Real s_m[K * 2 * C * 16];
+    __shared__ WalkSeg sg;
+    if (threadIdx.x == 0) sg = segs[find_walk_seg(segs, nseg, blockIdx.x)];
     __syncthreads();
-    const WalkSeg sg = segs[s_seg];
     const int c = threadIdx.x % C;
     const int p0 = (blockIdx.x - sg.first_cta) * (kT4 / C) + threadIdx.x / C;
-    for (int o0 = 0; o0 < sg.nops; o0 += kOpChunk) {
-        const int n = min(kOpChunk, sg.nops - o0);
+    const int Pp = sg.Pp;
+    const int p = min(p0, Pp - 1);
+    const bool valid = p0 < Pp;
+    const int nops = sg.nops;
+    for (int o0 = 0; o0 < nops; o0 += K) {
+        const int n = min(K, nops - o0);
         __syncthreads();
         stage_ops(s_ops, sg.ops + o0, n);
+        stage_mats<Real, C, PRE>(s_m, sg.ops + o0, n);
         __syncthreads();
-        for (int oi = 0; oi < n; ++oi) {
-            if (PRE) pre4_op<Real, C, 1, false>(s_ops[oi], c, p0, 0, sg.Pp, sg.log_scalers);
-            else post4_op<Real, C, 1, false>(s_ops[oi], c, p0, 0, sg.Pp, sg.cum, sg.log_scalers);
-        }
+        for (int k = 0; k < n; ++k)
+            walk4st_op<Real, C, PRE, false>(s_ops[k], s_m, k, c, p, valid, PRE ? nullptr : sg.cum,
+                                            sg.log_scalers);
     }
 }
 
@@ -1162,10 +1176,9 @@ template <typename Real>
 cudaError_t launch_walk4_batch(const WalkSeg* d_segs, int nseg, int ncta, int C, bool pre,
                                cudaStream_t s) {
     if (nseg == 0 || ncta == 0) return cudaSuccess;
-    const size_t sm = kOpChunk * sizeof(OpDesc);
 #define WB_(CC)                                                                         \
-    (pre ? (k_walk4_batch<Real, CC, true><<<ncta, kT4, sm, s>>>(d_segs, nseg), 0)        \
-         : (k_walk4_batch<Real, CC, false><<<ncta, kT4, sm, s>>>(d_segs, nseg), 0))
+    (pre ? (k_walk4_batch<Real, CC, true><<<ncta, kT4, 0, s>>>(d_segs, nseg), 0)         \
+         : (k_walk4_batch<Real, CC, false><<<ncta, kT4, 0, s>>>(d_segs, nseg), 0))
     switch (C) {
         case 1: WB_(1); break;
         case 2: WB_(2); break;
