@@ -579,6 +579,40 @@ __device__ __forceinline__ void mul_operand(float out[NP], bool states, uint32_t
     }
 }
 
+// Cluster exchanges: entry i of every CTA's shared array, the C <= 8 remote
+// loads issued together (a loop bounded by the run-time C would wait for each
+// load before the next), then combined in rank order.
+__device__ __forceinline__ float cluster_max(cg::cluster_group& cl, float* a, int i, int C) {
+    float u[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) u[r] = r < C ? cl.map_shared_rank(a, r < C ? r : 0)[i] : 0.f;
+    float m = 0.f;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) m = u[r] > m ? u[r] : m;
+    return m;
+}
+
+// Sums over the cluster's CTAs of entries 2 i and 2 i + 1, in rank order.
+__device__ __forceinline__ void cluster_sum2(cg::cluster_group& cl, double* a, int i, int C,
+                                             double& s0, double& s1) {
+    double u[8], v[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const double* rem = cl.map_shared_rank(a, r < C ? r : 0);
+        u[r] = r < C ? rem[2 * i] : 0.0;
+        v[r] = r < C ? rem[2 * i + 1] : 0.0;
+    }
+    s0 = 0;
+    s1 = 0;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        if (r < C) {
+            s0 += u[r];
+            s1 += v[r];
+        }
+    }
+}
+
 // Rescale (cluster-wide maximum over categories and states < S) or fixed
 // scaling, then store row t of the tile.  Same arithmetic as finish_tile in
 // k_generic.cu.
@@ -697,11 +731,7 @@ __device__ __forceinline__ void finish_row(SM& sm, const OpDesc& op, float out[N
         sx[threadIdx.x] = m;
         cg::cluster_group cluster = cg::this_cluster();
         cluster.sync();
-        m = 0.f;
-        for (int r = 0; r < C; ++r) {
-            const float u = cluster.map_shared_rank(sx, r)[threadIdx.x];
-            m = u > m ? u : m;
-        }
+        m = cluster_max(cluster, sx, threadIdx.x, C);
         if (m == 0.f) m = 1.f;
         const float inv = recip(m);
 #pragma unroll
@@ -1329,12 +1359,8 @@ k_deriv_tc(const DerivDesc* __restrict__ desc, const double* __restrict__ catw,
     cg::cluster_group cluster = cg::this_cluster();
     cluster.sync();
     if (c == 0) {
-        double nn = 0, dn = 0;
-        for (int r = 0; r < C; ++r) {
-            const double* rem = cluster.map_shared_rank(sm.nd, r);
-            nn += rem[t * 2 + 0];
-            dn += rem[t * 2 + 1];
-        }
+        double nn, dn;
+        cluster_sum2(cluster, sm.nd, t, C, nn, dn);
         double v1 = 0, v2 = 0;
         if (p < P) {
             const double dv = nn / dn;
@@ -1595,11 +1621,7 @@ k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds,
         cluster.sync();
         const bool mine = p >= op.p_begin && p < op.p_end;
         if (op.scale_write) {
-            float m = 0.f;
-            for (int r = 0; r < C; ++r) {
-                const float u = cluster.map_shared_rank(sm.smax[par], r)[t];
-                m = u > m ? u : m;
-            }
+            float m = cluster_max(cluster, sm.smax[par], t, C);
             if (m == 0.f) m = 1.f;
             const float inv = recip(m);
 #pragma unroll
@@ -1618,12 +1640,8 @@ k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds,
                 if (4 * j < Sg) st4(dst + 4 * j, out + 4 * j);
         }
         if (c == 0) {
-            double nn = 0, dn = 0;
-            for (int r = 0; r < C; ++r) {
-                const double* rem = cluster.map_shared_rank(sm.nd[par], r);
-                nn += rem[t * 2 + 0];
-                dn += rem[t * 2 + 1];
-            }
+            double nn, dn;
+            cluster_sum2(cluster, sm.nd[par], t, C, nn, dn);
             double v1 = 0, v2 = 0;
             if (p < SEG_(P, P)) {
                 const double dv = nn / dn;
