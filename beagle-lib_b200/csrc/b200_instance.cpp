@@ -1420,7 +1420,23 @@ int Instance::build_prederiv(const int* ops, int count, const int* post, const i
     for (int k = 0; k < count; ++k)
         if (writes[pre[k]] != 1 || writes.count(post[k])) return kNotFused;
     fops.clear();
-    if (S_ != 4) return kSuccess;
+    // Sibling pairs: same parent, each op's sibling the other's node, and
+    // neither op's destination read by the other.
+    std::vector<uint8_t> first(count, 0);
+    for (int k = 0; k + 1 < count; ++k) {
+        const int* a = ops + (size_t)k * 7;
+        const int* b = a + 7;
+        const bool pair = a[3] == b[3] && a[5] == post[k + 1] && b[5] == post[k] &&
+                          a[0] != b[0] && a[0] != b[3] && a[0] != b[5] && a[0] != post[k + 1] &&
+                          b[0] != a[5] && b[0] != post[k];
+        if (pair) first[k++] = 1;
+    }
+    if (S_ != 4) {
+        // the tensor-core pair walk reads the marks from the op list
+        for (int k = 0; k < count; ++k)
+            if (first[k]) tab[k].kind |= kPairFirst;
+        return kSuccess;
+    }
     fops.resize(count);
     for (int k = 0; k < count; ++k) {
         const OpDesc& t = tab[k];
@@ -1439,15 +1455,8 @@ int Instance::build_prederiv(const int* ops, int count, const int* post, const i
         f.kind = (t.kind & (kX2States | kM1Transposed)) | (d.post_is_states ? kPostStates : 0);
         f.reserved = 0;
     }
-    // Sibling pairs: same parent, each op's sibling the other's node, and
-    // neither op's destination read by the other.
     for (int k = 0; k + 1 < count; ++k) {
-        const int* a = ops + (size_t)k * 7;
-        const int* b = a + 7;
-        const bool pair = a[3] == b[3] && a[5] == post[k + 1] && b[5] == post[k] &&
-                          a[0] != b[0] && a[0] != b[3] && a[0] != b[5] && a[0] != post[k + 1] &&
-                          b[0] != a[5] && b[0] != post[k];
-        if (pair) {
+        if (first[k]) {
             fops[k].kind |= kPairFirst;
             const PreDerivOp &fa = fops[k], &fb = fops[k + 1];
             if (fa.mnode == fb.msib && fa.msib == fb.mnode &&
@@ -1529,8 +1538,10 @@ int Instance::updatePrePartialsWithDerivatives(const int* ops, int count, const 
 
 // updatePrePartialsWithDerivatives for 4 < S <= 64 on the FP32 path.
 // Variant 0: the two calls' kernels (each tuned as its own call); 1: the
-// tensor-core fused walk (k_tc.cu k_prederiv_tc).  The autotuner times them
-// when the list may run repeatedly.
+// tensor-core fused walk (k_tc.cu k_prederiv_tc); 2: its sibling-pair form
+// (k_prederiv_tc_pairs: 17 to 32 padded states, lists made only of sibling
+// pairs; other lists run variant 1).  The autotuner times them when the list
+// may run repeatedly.
 int Instance::prederiv_tc(const int* ops, int count, const int* post, const int* pre,
                           const int* dmat, const int* cw, const std::vector<OpDesc>& tab,
                           const std::vector<DerivDesc>& dtab, bool idempotent, double* outSum,
@@ -1541,6 +1552,9 @@ int Instance::prederiv_tc(const int* ops, int count, const int* post, const int*
     CK(out_.reserve(sizeof(double) * 2 * count));
     const double* catw = d_catw_ + (size_t)cw[0] * C_;
     const int ls = (int)log_scalers_;
+    bool pairs_only = count % 2 == 0;          // every even op starts a sibling pair
+    for (int k = 0; pairs_only && k < count; k += 2)
+        pairs_only = (tab[k].kind & kPairFirst) != 0;
     auto run = [&](int v) -> cudaError_t {
         if (v == 0) {
             if (post_or_pre(ops, count, 7, -1, true) != kSuccess) return cudaErrorUnknown;
@@ -1548,23 +1562,32 @@ int Instance::prederiv_tc(const int* ops, int count, const int* post, const int*
                 return cudaErrorUnknown;
             return cudaSuccess;
         }
+        if (v == 2 && !pairs_only) return cudaErrorInvalidValue;
         cudaError_t e = t_ops_pre_.upload(tab.data(), sizeof(OpDesc) * count, stream_);
         if (e == cudaSuccess) e = t_deriv_.upload(dtab.data(), sizeof(DerivDesc) * count, stream_);
         if (e != cudaSuccess) return e;
         tc_used_ = true;
-        e = launch_prederiv_tc((const OpDesc*)t_ops_pre_.ptr, (const DerivDesc*)t_deriv_.ptr,
-                               count, count, catw, d_patw_, dm, ls, (double*)scratch_.ptr,
-                               stream_);
+        e = v == 2 ? launch_prederiv_tc_pairs((const OpDesc*)t_ops_pre_.ptr,
+                                              (const DerivDesc*)t_deriv_.ptr, count, count, catw,
+                                              d_patw_, dm, ls, (double*)scratch_.ptr, stream_)
+                   : launch_prederiv_tc((const OpDesc*)t_ops_pre_.ptr,
+                                        (const DerivDesc*)t_deriv_.ptr, count, count, catw,
+                                        d_patw_, dm, ls, (double*)scratch_.ptr, stream_);
         if (e != cudaSuccess) return e;
         return launch_final_sum((double*)scratch_.ptr, nblk, 2 * count, (double*)out_.ptr,
                                 stream_);
     };
     const TuneKey key{kTuneFused, (int)dbl_, C_ * 100 + Sg_, Pp_, tune_count_class(count),
                       device_};
-    int v = tune_pick(key, 2, idempotent, stream_, run);
+    int v = tune_pick(key, 3, idempotent, stream_, run);
     if (v < 0) v = 1;
     cudaError_t e = run(v);
-    if (e == cudaErrorInvalidConfiguration && v == 1) {   // TMEM could be oversubscribed
+    if (e == cudaErrorInvalidValue && v == 2) {   // not a pairs-only list, or another width
+        (void)cudaGetLastError();
+        v = 1;
+        e = run(v);
+    }
+    if (e == cudaErrorInvalidConfiguration && v >= 1) {   // TMEM could be oversubscribed
         (void)cudaGetLastError();
         v = 0;
         e = run(0);

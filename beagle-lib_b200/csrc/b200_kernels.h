@@ -91,6 +91,13 @@ cudaError_t launch_prederiv_tc_batch(const PreDerivSeg* d_segs, int nseg, int nt
 cudaError_t launch_prederiv_tc(const OpDesc* d_ops, const DerivDesc* d_desc, int nops, int nsum,
                                const double* catw, const double* patw, const Dims& d, int ls,
                                double* d_block, cudaStream_t s);
+// The same for 17 to 32 padded states on lists made only of sibling pairs
+// (OpDesc::kind kPairFirst on every even op; the caller checks): a pair a
+// step, each post-order tile feeding two products (k_prederiv_tc_pairs).
+// cudaErrorInvalidValue for other shapes.
+cudaError_t launch_prederiv_tc_pairs(const OpDesc* d_ops, const DerivDesc* d_desc, int nops,
+                                     int nsum, const double* catw, const double* patw,
+                                     const Dims& d, int ls, double* d_block, cudaStream_t s);
 // TMA-fed tensor-core walk (FP32, 4 < S <= 64): maps[k] gives op k's tensor
 // maps (tc_encode_map: a partials buffer, or a matrix buffer, of this shape).
 cudaError_t tc_encode_map(TmaMap* out, const void* base, bool matrix, const Dims& d);

@@ -1639,7 +1639,9 @@ k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds,
             for (int j = 0; j < NP / 4; ++j)
                 if (4 * j < Sg) st4(dst + 4 * j, out + 4 * j);
         }
-        if (c == 0) {
+        // op o's derivative sums on the cluster's CTA o mod C (spread over
+        // the cluster: the others wait for it at the next barrier)
+        if (c == o % C) {
             double nn, dn;
             cluster_sum2(cluster, sm.nd[par], t, C, nn, dn);
             double v1 = 0, v2 = 0;
@@ -1680,6 +1682,387 @@ k_prederiv_tc(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds,
     tc_fence_after();
     cluster.sync();   // every remote read of this CTA's exchange buffers is done
     if (t < 32) tmem_dealloc(tmem, COLS);
+}
+
+// ------------------------------------------ tensor-core fused walk, pairs
+// k_prederiv_tc for 17 to 32 states (N = K = 32) on lists made only of
+// sibling pairs (kPairFirst on every even op; the launcher refuses other
+// lists), one pair a step.  Ops a and b share their parent and each is the
+// other's sibling, so the four products their GEMM 1 and GEMM 3 make,
+//   Y1_a = post_b . P_b^T    Y3_b = post_b . D_b^T    (A tile post_b)
+//   Y1_b = post_a . P_a^T    Y3_a = post_a . D_a^T    (A tile post_a),
+// come two from each A tile: the tile is gathered and split once and
+// multiplied by two matrices staged side by side (B rows 0-31 and 32-63).
+// The parent tile is loaded once for both GEMM 2s, both epilogues' post-order
+// rows are staged together, and one cluster barrier exchanges both rescaling
+// maxima and both ops' derivative terms.  TMEM: four 32-column accumulators
+// (Y1_a, Y3_b, Y1_b, Y3_a); GEMM 2 of each op overwrites its Y1.
+struct TcPairSmem {
+    float a_hi[kTM * 32];
+    float a_lo[kTM * 32];
+    float b_hi[64 * 32];
+    float b_lo[64 * 32];
+    float smax[2][2][kTM];        // [step parity][op of the pair]
+    double nd[2][2][kTM * 2];     // [step parity][op of the pair]: w_c n_c, w_c q_c per row
+    float inv[2][kTM];            // each row's rescaling factor 1 / m, per op of the pair
+    double red[kTT / 32 * 2];
+    uint64_t bar;
+    uint32_t tmem;
+};
+constexpr int kPairCols = 128;
+
+// Both products of the A tile in shared memory: 3 x tf32 split MMAs into d1
+// (B rows 0-31) and d2 (B rows 32-63), N = 32, ksteps K steps, one commit.
+__device__ __forceinline__ void issue_dual(TcPairSmem& sm, uint32_t d1, uint32_t d2, int ksteps) {
+    const uint32_t idesc = idesc_tf32(kTM, 32);
+    const uint32_t ah = smem_u32(sm.a_hi), al = smem_u32(sm.a_lo);
+    const uint32_t bh = smem_u32(sm.b_hi), bl = smem_u32(sm.b_lo);
+    constexpr uint32_t kB2 = 32u * 128u;     // B rows 32-63: 4 KB in, 1024-byte aligned
+    tc_fence_after();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (k >= ksteps) break;
+        const uint32_t o = (uint32_t)k * 32u;
+        const uint64_t dah = smem_desc_sw128(ah + o), dal = smem_desc_sw128(al + o);
+        const uint64_t b1h = smem_desc_sw128(bh + o), b1l = smem_desc_sw128(bl + o);
+        const uint64_t b2h = smem_desc_sw128(bh + kB2 + o), b2l = smem_desc_sw128(bl + kB2 + o);
+        const uint32_t acc = k == 0 ? 0u : 1u;
+        mma_tf32(d1, dah, b1h, idesc, acc);
+        mma_tf32(d1, dah, b1l, idesc, 1u);
+        mma_tf32(d1, dal, b1h, idesc, 1u);
+        mma_tf32(d2, dah, b2h, idesc, acc);
+        mma_tf32(d2, dah, b2l, idesc, 1u);
+        mma_tf32(d2, dal, b2h, idesc, 1u);
+    }
+    mma_commit(&sm.bar);
+}
+
+// Rows p0 .. p0 + 127 of one 32-column half (registers from load_tile_sw)
+// into a staging tile, and this thread's row back out of one.
+__device__ __forceinline__ void stage_half_sw(float* half, const float v[][4]) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r0 = warp * 4 + (lane >> 3), k8 = lane & 7;
+#pragma unroll
+    for (int i = 0; i < kTM / 16; ++i) {
+        const int r = r0 + 16 * i;
+        st4(half + r * 32 + ((k8 ^ (r & 7)) * 4), v[i]);
+    }
+}
+
+// Derivative terms (n, q) and the rescaling maximum of one op's new row
+// `out` (32 states): D . post from TMEM column `col` (a tip's column of D
+// from the transposed image), the post-order row from the staging tile.
+__device__ __forceinline__ void pair_terms(const float out[32], bool pst, int sp,
+                                           const DerivDesc& dd, size_t mo, uint32_t tmem,
+                                           uint32_t col, const float* stage, int S, int Sg,
+                                           float& n, float& q, float& mx) {
+    const int t = threadIdx.x;
+    float nq[4] = {0.f, 0.f, 0.f, 0.f}, dq[4] = {0.f, 0.f, 0.f, 0.f}, mq[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        float y[16], x[16];
+        if (pst) tip_chunk(static_cast<const float*>(dd.dmatt) + mo, sp, S, Sg, (float)dd.dpad, j,
+                           y);
+        else tmem_chunk(tmem, (int)col, j, y);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            x[4 * k] = x[4 * k + 1] = x[4 * k + 2] = x[4 * k + 3] = 0.f;
+            const int kc = 4 * j + k;
+            if (!pst) ld4(stage + t * 32 + ((kc ^ (t & 7)) * 4), x + 4 * k);
+        }
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+            const int i = 16 * j + e;
+            if (i >= S) continue;
+            const float xv = pst ? ((sp < 0 || sp >= S || sp == i) ? 1.f : 0.f) : x[e];
+            nq[e & 3] += out[i] * y[e];
+            dq[e & 3] += out[i] * xv;
+            mq[e & 3] = out[i] > mq[e & 3] ? out[i] : mq[e & 3];
+        }
+    }
+    n = (nq[0] + nq[1]) + (nq[2] + nq[3]);
+    q = (dq[0] + dq[1]) + (dq[2] + dq[3]);
+    const float m01 = mq[1] > mq[0] ? mq[1] : mq[0];
+    const float m23 = mq[3] > mq[2] ? mq[3] : mq[2];
+    mx = m23 > m01 ? m23 : m01;
+}
+
+template <bool BATCH>
+__global__ void __launch_bounds__(kTT, 3)
+k_prederiv_tc_pairs(const OpDesc* __restrict__ ops, const DerivDesc* __restrict__ dds, int nops,
+                    int nsum, int S, int Sg, int C, int P, const double* __restrict__ catw,
+                    const double* __restrict__ patw, int log_scalers, double* block,
+                    const PreDerivSeg* __restrict__ segs, int nseg) {
+    constexpr int NP = 32;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    TcPairSmem& sm = *reinterpret_cast<TcPairSmem*>(
+        smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u));
+    const int t = threadIdx.x;
+    const int c = blockIdx.x % C;
+    int tile = blockIdx.x / C;
+    int ntiles = gridDim.x / C;
+    __shared__ PreDerivSeg s_sg;
+    if constexpr (BATCH) {
+        if (t == 0) s_sg = segs[tc_find_seg(segs, nseg, tile)];
+        __syncthreads();
+        ntiles = s_sg.nblk;
+        tile -= s_sg.first_cta;
+        nops = s_sg.nops;
+    }
+#define SEG_(field, arg) (BATCH ? s_sg.field : (arg))
+    const int p0 = tile * kTM;
+    const int p = p0 + t;
+    const size_t xs = (size_t)C * Sg;
+    const size_t mo = (size_t)c * Sg * Sg;
+    const double wc = SEG_(catw, catw)[c];
+    const int np = chunk_pieces<NP>(Sg, 0);        // 16-byte pieces of a row the MMAs read
+    const int ks = np / 2;
+    constexpr uint32_t cY1a = 0, cY3b = 32, cY1b = 64, cY3a = 96;
+
+    if (t == 0) {
+        mbar_init(&sm.bar, 1);
+        mbar_init_fence();
+    }
+    if (t < 32) {
+        tmem_alloc(&sm.tmem, kPairCols);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = sm.tmem;
+    Pipe pp;
+    ChunkRegs cr;
+    cg::cluster_group cluster = cg::this_cluster();
+    // The weighted derivative of op oo for each of this tile's rows from
+    // every category's terms (nd), then the tile's block sums.
+    auto emit_sums = [&](int oo, double* nd) {
+        double nn, dn;
+        cluster_sum2(cluster, nd, t, C, nn, dn);
+        double v1 = 0, v2 = 0;
+        if (p < SEG_(P, P)) {
+            const double dv = nn / dn;
+            const double wp = SEG_(patw, patw)[p];
+            v1 = dv * wp;
+            v2 = dv * dv * wp;
+        }
+#pragma unroll
+        for (int sh = 16; sh > 0; sh >>= 1) {
+            v1 += __shfl_xor_sync(0xffffffffu, v1, sh);
+            v2 += __shfl_xor_sync(0xffffffffu, v2, sh);
+        }
+        if ((t & 31) == 0) {
+            sm.red[(t >> 5) * 2 + 0] = v1;
+            sm.red[(t >> 5) * 2 + 1] = v2;
+        }
+        __syncthreads();
+        if (t == 0) {
+            double t1 = 0, t2 = 0;
+            for (int k = 0; k < kTT / 32; ++k) {
+                t1 += sm.red[k * 2 + 0];
+                t2 += sm.red[k * 2 + 1];
+            }
+            double* blk = SEG_(block, block);
+            blk[(size_t)oo * ntiles + tile] = t1;
+            blk[(size_t)(SEG_(nops, nsum) + oo) * ntiles + tile] = t2;
+        }
+        __syncthreads();   // sm.red free for the next use
+    };
+    for (int o = 0; o + 1 < nops; o += 2) {
+        const OpDesc& A = SEG_(ops, ops)[o];
+        const OpDesc& B = SEG_(ops, ops)[o + 1];
+        const DerivDesc& Ad = SEG_(dds, dds)[o];
+        const DerivDesc& Bd = SEG_(dds, dds)[o + 1];
+        const bool tb = A.kind & kX2States;       // post_b is tip states (a's sibling)
+        const bool ta = B.kind & kX2States;       // post_a is tip states (b's sibling)
+        const float* post_b = static_cast<const float*>(A.x2);
+        const float* post_a = static_cast<const float*>(B.x2);
+        // 1. Y1_a, Y3_b from the A tile post_b; Y1_b, Y3_a from post_a (a tip
+        // tile is none: its products are matrix columns, read in place)
+        if (!tb) {
+            gather_sw<kTM, false>(cr.a, post_b + (size_t)p0 * xs + (size_t)c * Sg, xs, kTM, 0, Sg,
+                                  np);
+            gather_sw<32, true>(cr.b, static_cast<const float*>(A.m2) + mo, Sg, Sg, 0, Sg, np);
+            gather_sw<32, true>(cr.b + 2, static_cast<const float*>(Bd.dmat) + mo, Sg, Sg, 0, Sg,
+                                np);
+            pipe_drain(sm, pp);
+            scatter_sw<kTM>(cr.a, sm.a_hi, sm.a_lo, np);
+            scatter_sw<32>(cr.b, sm.b_hi, sm.b_lo, np);
+            scatter_sw<32>(cr.b + 2, sm.b_hi + 32 * 32, sm.b_lo + 32 * 32, np);
+            fence_async_smem();
+            tc_fence_before();
+            __syncthreads();
+            if (t == 0) issue_dual(sm, tmem + cY1a, tmem + cY3b, ks);
+            pp.pending = true;
+        }
+        if (!ta) {
+            gather_sw<kTM, false>(cr.a, post_a + (size_t)p0 * xs + (size_t)c * Sg, xs, kTM, 0, Sg,
+                                  np);
+            gather_sw<32, true>(cr.b, static_cast<const float*>(B.m2) + mo, Sg, Sg, 0, Sg, np);
+            gather_sw<32, true>(cr.b + 2, static_cast<const float*>(Ad.dmat) + mo, Sg, Sg, 0, Sg,
+                                np);
+            pipe_drain(sm, pp);
+            scatter_sw<kTM>(cr.a, sm.a_hi, sm.a_lo, np);
+            scatter_sw<32>(cr.b, sm.b_hi, sm.b_lo, np);
+            scatter_sw<32>(cr.b + 2, sm.b_hi + 32 * 32, sm.b_lo + 32 * 32, np);
+            fence_async_smem();
+            tc_fence_before();
+            __syncthreads();
+            if (t == 0) issue_dual(sm, tmem + cY1b, tmem + cY3a, ks);
+            pp.pending = true;
+        }
+        // 2. the parent tile through the staging tile once the products have
+        // read the A tiles, and GEMM 2a's B rows (P_a^T)
+        const float* mta =
+            static_cast<const float*>((A.kind & kM1Transposed) ? A.m1 : A.m1t) + mo;
+        const float* mtb =
+            static_cast<const float*>((B.kind & kM1Transposed) ? B.m1 : B.m1t) + mo;
+        float par[NP];
+        {
+            float v[kTM / 16][4];
+            load_tile_sw<NP>(v, static_cast<const float*>(A.x1), p0, c, C, Sg);
+            gather_sw<32, true>(cr.b, mta, Sg, Sg, 0, Sg, np);
+            pipe_drain(sm, pp);
+            stage_half_sw(sm.a_hi, v);
+            __syncthreads();
+            row_from_stage<NP>(sm, par);
+        }
+        tc_fence_after();
+        const int sb = tb ? static_cast<const int*>(A.x2)[p] : 0;
+        const int sa = ta ? static_cast<const int*>(B.x2)[p] : 0;
+        // 3. GEMM 2a: out_a = (parent (.) Y1_a) . P_a into Y1_a's columns,
+        // then GEMM 2b the same way (its operand formed while 2a runs)
+        float z[NP];
+#pragma unroll
+        for (int i = 0; i < NP; ++i) z[i] = par[i];
+        mul_operand<NP>(z, tb, tmem, (int)cY1a, static_cast<const float*>(A.m2t) + mo, sb, S, Sg,
+                        (float)A.pad2);
+        store_row_sw128<NP, 0>(sm.a_hi, sm.a_lo, z);
+        scatter_sw<32>(cr.b, sm.b_hi, sm.b_lo, np);
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        if (t == 0) issue_chunk<32>(sm, tmem + cY1a, NP, true, false, ks);
+        pp.pending = true;
+#pragma unroll
+        for (int i = 0; i < NP; ++i) z[i] = par[i];
+        mul_operand<NP>(z, ta, tmem, (int)cY1b, static_cast<const float*>(B.m2t) + mo, sa, S, Sg,
+                        (float)B.pad2);
+        gather_sw<32, true>(cr.b, mtb, Sg, Sg, 0, Sg, np);
+        pipe_drain(sm, pp);
+        store_row_sw128<NP, 0>(sm.a_hi, sm.a_lo, z);
+        scatter_sw<32>(cr.b, sm.b_hi, sm.b_lo, np);
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        if (t == 0) issue_chunk<32>(sm, tmem + cY1b, NP, true, false, ks);
+        pp.pending = true;
+        // 4. both post-order tiles (coalesced), post_a while GEMM 2b runs,
+        // staged once it has read the A tile: post_a in a_hi, post_b in a_lo
+        {
+            float v[kTM / 16][4];
+            if (!ta) load_tile_sw<NP>(v, post_a, p0, c, C, Sg);
+            pipe_drain(sm, pp);
+            if (!ta) stage_half_sw(sm.a_hi, v);
+            if (!tb) load_tile_sw<NP>(v, post_b, p0, c, C, Sg);
+            if (!tb) stage_half_sw(sm.a_lo, v);
+        }
+        __syncthreads();
+        tc_fence_after();
+        // 5. each op's new row: derivative terms and rescaling maximum, then
+        // the row itself (unscaled) over this thread's post-order row in the
+        // staging tile, which only this thread reads; one exchange for both
+        const int par_ = (o >> 1) & 1;
+        {
+            float out[NP], n, q, mx;
+#pragma unroll
+            for (int j = 0; j < NP / 16; ++j) tmem_chunk(tmem, (int)cY1a, j, out + 16 * j);
+            pair_terms(out, ta, sa, Ad, mo, tmem, cY3a, sm.a_hi, S, Sg, n, q, mx);
+            sm.nd[par_][0][t * 2 + 0] = wc * (double)n;
+            sm.nd[par_][0][t * 2 + 1] = wc * (double)q;
+            sm.smax[par_][0][t] = mx;
+#pragma unroll
+            for (int kc = 0; kc < 8; ++kc) st4(sm.a_hi + t * 32 + ((kc ^ (t & 7)) * 4), out + 4 * kc);
+#pragma unroll
+            for (int j = 0; j < NP / 16; ++j) tmem_chunk(tmem, (int)cY1b, j, out + 16 * j);
+            pair_terms(out, tb, sb, Bd, mo, tmem, cY3b, sm.a_lo, S, Sg, n, q, mx);
+            sm.nd[par_][1][t * 2 + 0] = wc * (double)n;
+            sm.nd[par_][1][t * 2 + 1] = wc * (double)q;
+            sm.smax[par_][1][t] = mx;
+#pragma unroll
+            for (int kc = 0; kc < 8; ++kc) st4(sm.a_lo + t * 32 + ((kc ^ (t & 7)) * 4), out + 4 * kc);
+        }
+        // Exchange halves of parity par_ are rewritten two steps later, after
+        // the next step's barrier, which every CTA reaches after reading them.
+        cluster.sync();
+        const int ls = SEG_(log_scalers, log_scalers);
+        {
+            float ia = 1.f, ib = 1.f;
+            if (A.scale_write) {
+                float m = cluster_max(cluster, sm.smax[par_][0], t, C);
+                if (m == 0.f) m = 1.f;
+                ia = recip(m);
+                if (c == 0 && p >= A.p_begin && p < A.p_end) {
+                    const double lm = scale_log(m);
+                    A.scale_write[p] = ls ? lm : (double)m;
+                }
+            }
+            if (B.scale_write) {
+                float m = cluster_max(cluster, sm.smax[par_][1], t, C);
+                if (m == 0.f) m = 1.f;
+                ib = recip(m);
+                if (c == 0 && p >= B.p_begin && p < B.p_end) {
+                    const double lm = scale_log(m);
+                    B.scale_write[p] = ls ? lm : (double)m;
+                }
+            }
+            sm.inv[0][t] = ia;
+            sm.inv[1][t] = ib;
+        }
+        __syncthreads();
+        // 6. both new tiles out in whole-row stores, each row scaled by its
+        // factor on the way
+        {
+            const int warp = t >> 5, lane = t & 31;
+            const int r0 = warp * 4 + (lane >> 3), k8 = lane & 7;
+            const int col = 4 * k8;
+            if (col < Sg) {
+#pragma unroll
+                for (int i = 0; i < kTM / 16; ++i) {
+                    const int r = r0 + 16 * i;
+                    const int pr = p0 + r;
+                    float v[4];
+                    if (pr >= A.p_begin && pr < A.p_end) {
+                        ld4(sm.a_hi + r * 32 + ((k8 ^ (r & 7)) * 4), v);
+                        const float f = sm.inv[0][r];
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) v[e] *= f;
+                        st4(static_cast<float*>(A.dest) + ((size_t)pr * C + c) * Sg + col, v);
+                    }
+                    if (pr >= B.p_begin && pr < B.p_end) {
+                        ld4(sm.a_lo + r * 32 + ((k8 ^ (r & 7)) * 4), v);
+                        const float f = sm.inv[1][r];
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) v[e] *= f;
+                        st4(static_cast<float*>(B.dest) + ((size_t)pr * C + c) * Sg + col, v);
+                    }
+                }
+            }
+        }
+        // 7. both ops' derivative sums, op k's on the cluster's CTA k mod C
+        // (spread over the cluster: the others wait for it at the next barrier)
+        if (c == o % C) emit_sums(o, sm.nd[par_][0]);
+        if (c == (o + 1) % C) emit_sums(o + 1, sm.nd[par_][1]);
+        // TMEM reads of this step done before the next step's MMAs overwrite
+        // them; this step's stores visible to the CTA before later loads.
+        tc_fence_before();
+        __syncthreads();
+    }
+#undef SEG_
+    pipe_drain(sm, pp);
+    tc_fence_after();
+    cluster.sync();   // every remote read of this CTA's exchange buffers is done
+    if (t < 32) tmem_dealloc(tmem, kPairCols);
 }
 
 // Dynamic shared memory of a launch: the struct, raised to the TMEM
@@ -1837,6 +2220,20 @@ cudaError_t launch_prederiv_tc(const OpDesc* d_ops, const DerivDesc* d_desc, int
 #define PD_(NP, KC) run_prederiv_tc<NP, KC>(d_ops, d_desc, nops, nsum, catw, patw, d, ls, d_block, s)
     return B200_TC_DISPATCH(d.Sg, PD_);
 #undef PD_
+}
+
+cudaError_t launch_prederiv_tc_pairs(const OpDesc* d_ops, const DerivDesc* d_desc, int nops,
+                                     int nsum, const double* catw, const double* patw,
+                                     const Dims& d, int ls, double* d_block, cudaStream_t s) {
+    if (nops == 0) return cudaSuccess;
+    if (!tc_supported(d) || d.Sg <= 16 || d.Sg > 32 || nops % 2) return cudaErrorInvalidValue;
+    const size_t need = sizeof(TcPairSmem) + 1024;
+    const size_t floor_smem = tc_smem(kPairCols);
+    const size_t smem = need > floor_smem ? need : floor_smem;
+    const int grid = (d.Pp / kTM) * d.C;
+    const PreDerivSeg* none = nullptr;
+    return launch_tc(k_prederiv_tc_pairs<false>, grid, smem, d.C, kPairCols, s, d_ops, d_desc,
+                     nops, nsum, d.S, d.Sg, d.C, d.P, catw, patw, ls, d_block, none, 0);
 }
 
 cudaError_t launch_prederiv_tc_batch(const PreDerivSeg* d_segs, int nseg, int ntiles,
