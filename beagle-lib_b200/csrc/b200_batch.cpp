@@ -736,6 +736,7 @@ int Batch::preDerivatives(const int* const* ops, const int* counts, const int* c
     };
     std::map<int, std::vector<Member>> groups;                           // C -> 4-state
     std::map<std::tuple<int, int, int>, std::vector<Member>> tcgroups;   // (S, Sg, C)
+    std::map<std::tuple<int, int, int>, bool> tcpairs;   // every member's list all sibling pairs
     std::vector<unsigned char> table;
     std::vector<int> fallback;
     for (int i = 0; i < n; ++i) {
@@ -761,8 +762,12 @@ int Batch::preDerivatives(const int* const* ops, const int* counts, const int* c
             groups[in->C_].push_back(Member{i, append(table, fops), 0, counts[i]});
         } else {
             const size_t a = append(table, tab);
-            tcgroups[std::make_tuple(in->S_, in->Sg_, in->C_)].push_back(
-                Member{i, a, append(table, dtab), counts[i]});
+            const auto key = std::make_tuple(in->S_, in->Sg_, in->C_);
+            tcgroups[key].push_back(Member{i, a, append(table, dtab), counts[i]});
+            bool pairs = counts[i] % 2 == 0;
+            for (int k = 0; pairs && k < counts[i]; k += 2) pairs = (tab[k].kind & kPairFirst) != 0;
+            auto it = tcpairs.find(key);
+            tcpairs[key] = (it == tcpairs.end() ? true : it->second) && pairs;
         }
     }
     auto own_call = [&](int i) {
@@ -849,6 +854,7 @@ int Batch::preDerivatives(const int* const* ops, const int* counts, const int* c
         size_t off;
         int nseg;
         int ntiles;
+        bool pairs;
         std::vector<int> members;
     };
     std::vector<TG> tgl;
@@ -856,6 +862,7 @@ int Batch::preDerivatives(const int* const* ops, const int* counts, const int* c
         std::vector<PreDerivSeg> segs;
         TG tg{};
         tg.d = Dims{std::get<0>(kv.first), std::get<1>(kv.first), 0, 0, std::get<2>(kv.first)};
+        tg.pairs = tcpairs[kv.first];
         for (const Member& mb : kv.second) {
             segs.push_back(seg_of(mb, tg.ntiles));
             tg.ntiles += m_[mb.i]->Pp_ / tc_tile_patterns();
@@ -872,9 +879,15 @@ int Batch::preDerivatives(const int* const* ops, const int* counts, const int* c
                   g.nseg, g.ncta, g.C, stream_));
     std::vector<int> late;   // tensor-core groups that cannot launch here: own calls
     for (const TG& g : tgl) {
-        const cudaError_t e = launch_prederiv_tc_batch(
-            (const PreDerivSeg*)((unsigned char*)t_b_.ptr + g.off), g.nseg, g.ntiles, g.d,
-            stream_);
+        // the sibling-pair form where every member's list is made of pairs
+        // and the width has it (17 to 32 padded states), else the op walk
+        const PreDerivSeg* segs = (const PreDerivSeg*)((unsigned char*)t_b_.ptr + g.off);
+        cudaError_t e = cudaErrorInvalidValue;
+        if (g.pairs) e = launch_prederiv_tc_pairs_batch(segs, g.nseg, g.ntiles, g.d, stream_);
+        if (e == cudaErrorInvalidValue) {
+            (void)cudaGetLastError();
+            e = launch_prederiv_tc_batch(segs, g.nseg, g.ntiles, g.d, stream_);
+        }
         if (e == cudaErrorInvalidConfiguration) {
             (void)cudaGetLastError();
             late.insert(late.end(), g.members.begin(), g.members.end());

@@ -98,6 +98,10 @@ cudaError_t launch_prederiv_tc(const OpDesc* d_ops, const DerivDesc* d_desc, int
 cudaError_t launch_prederiv_tc_pairs(const OpDesc* d_ops, const DerivDesc* d_desc, int nops,
                                      int nsum, const double* catw, const double* patw,
                                      const Dims& d, int ls, double* d_block, cudaStream_t s);
+// Its batched form over segments as launch_prederiv_tc_batch (every
+// segment's list made of sibling pairs; the caller checks).
+cudaError_t launch_prederiv_tc_pairs_batch(const PreDerivSeg* d_segs, int nseg, int ntiles,
+                                           const Dims& d, cudaStream_t s);
 // TMA-fed tensor-core walk (FP32, 4 < S <= 64): maps[k] gives op k's tensor
 // maps (tc_encode_map: a partials buffer, or a matrix buffer, of this shape).
 cudaError_t tc_encode_map(TmaMap* out, const void* base, bool matrix, const Dims& d);

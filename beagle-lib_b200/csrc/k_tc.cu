@@ -2236,6 +2236,21 @@ cudaError_t launch_prederiv_tc_pairs(const OpDesc* d_ops, const DerivDesc* d_des
                      nops, nsum, d.S, d.Sg, d.C, d.P, catw, patw, ls, d_block, none, 0);
 }
 
+cudaError_t launch_prederiv_tc_pairs_batch(const PreDerivSeg* d_segs, int nseg, int ntiles,
+                                           const Dims& d, cudaStream_t s) {
+    if (nseg == 0 || ntiles == 0) return cudaSuccess;
+    if (!tc_supported(d) || d.Sg <= 16 || d.Sg > 32) return cudaErrorInvalidValue;
+    const size_t need = sizeof(TcPairSmem) + 1024;
+    const size_t floor_smem = tc_smem(kPairCols);
+    const size_t smem = need > floor_smem ? need : floor_smem;
+    const OpDesc* no_ops = nullptr;
+    const DerivDesc* no_dds = nullptr;
+    const double* no_w = nullptr;
+    return launch_tc(k_prederiv_tc_pairs<true>, ntiles * d.C, smem, d.C, kPairCols, s, no_ops,
+                     no_dds, 0, 0, d.S, d.Sg, d.C, 0, no_w, no_w, 0, (double*)nullptr, d_segs,
+                     nseg);
+}
+
 cudaError_t launch_prederiv_tc_batch(const PreDerivSeg* d_segs, int nseg, int ntiles,
                                      const Dims& d, cudaStream_t s) {
     if (nseg == 0 || ntiles == 0) return cudaSuccess;

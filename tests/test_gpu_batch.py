@@ -237,3 +237,39 @@ def test_batch_configuration_shapes_checkpointed(b200, pkg, syn, oracle):
         _, lo, go = run_oracle(oracle, probs[i])
         assert rel(lnl32[i], lo) <= tol["lnl"]
         assert grad_err(g32[i], go) <= tol["grad"]
+
+
+@pytest.mark.parametrize("unpaired", [False, True], ids=["pairs", "one_member_unpaired"])
+def test_batch_tc_fused_pair_walk_and_unpaired_lists(b200, pkg, syn, unpaired):
+    """FP32 20-state members in one (S, C) group: the batched sibling-pair
+    tensor-core walk when every member's list is made of sibling pairs, the
+    batched single-op walk for the whole group when one member's list is
+    sorted by depth (siblings not adjacent).  Gradients against separate
+    single-instance calls."""
+    probs = [syn.make_problem(S=20, N=12 + 3 * k, P=400 + 150 * k, C=4, seed=960 + k,
+                              rescale=True) for k in range(3)]
+    singles = [_create(b200, pr, "single") for pr in probs]
+    ref = [pr.evaluate(inst) for pr, inst in zip(probs, singles)]
+    members = [_create(b200, pr, "single") for pr in probs]
+    batch = pkg.binding.Batch(b200, members)
+    syn.batch_evaluate(batch, probs, fused=True)   # leaves every member's post-order side in place
+    plan = batch._plan
+    pre, nodes = list(plan["pre"]), list(plan["fnodes"])
+    if unpaired:
+        pr = probs[1]
+        ops = pre[1]
+        depth = {pr.pre(pr.root): 0}
+        for op in ops:
+            depth[op[0]] = depth[op[3]] + 1
+        ops = ops[np.lexsort((ops[:, 0] % 7, [depth[o[0]] for o in ops]))]
+        pre[1] = ops
+        nodes[1] = (ops[:, 0] - pr.pre(0)).astype(np.int32)
+    sums, _ = batch.updatePrePartialsWithDerivatives(pre, nodes, plan["dmat"], plan["zeros"])
+    batch.wait()
+    for k, pr in enumerate(probs):
+        g = np.empty(pr.B)
+        g[nodes[k]] = sums[k]
+        assert grad_err(g, ref[k][1]) <= TOL["single"]["grad"], (k, grad_err(g, ref[k][1]))
+    batch.finalize()
+    for x in singles + members:
+        x.finalize()
