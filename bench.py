@@ -628,9 +628,9 @@ def workload_record(torch, lib, name, args, device):
     ms, _, _ = timed_value(torch, inst, pr, steps, warm)
     mixed = steps / (ms / 1000.0)
     tuned = inst.tunedVariants()
-    # the fused pre-order + derivative walk (S = 4 kernel, or the tensor-core
-    # one for S > 4) when the autotuner picked it
-    fused_walk = tuned.get("fused") == 1
+    # the fused pre-order + derivative walk (S = 4 kernels, or the tensor-core
+    # ones for S > 4) when the autotuner picked any of its forms
+    fused_walk = tuned.get("fused", 0) > 0
     ph_ms = phase_times(torch, inst, pr, 5, fused_walk)
     peak, peak_kind = peaks()
     roof = roofline_of(pr, ph_ms, fused_walk, peak, peak_kind, traffic_table())
@@ -719,7 +719,7 @@ def run_b200_arm(args):
     # With the fused walk picked, the "deriv" phase is that one kernel (plus
     # its final sum); otherwise the phases of the two calls are timed apart.
     tuned = inst.tunedVariants()
-    fused_walk = tuned["fused"] > 0          # any fused-walk variant (1-3)
+    fused_walk = tuned["fused"] > 0          # any fused-walk form (variants 1-3)
     nph = max(5, min(50, args.steps // 4))
     ph_ms = phase_times(torch, inst, pr, nph, fused_walk)
     peak, peak_kind = peaks()
