@@ -545,6 +545,7 @@ _BATCH_SIGS = {
     "BatchWait": [_i],
     "BatchUpdatePrePartialsWithDerivatives": [_i, _p, _p, _p, _p, _p, _p, _p],
     "BatchLaunchGraphWithLengths": [_i, _i, _p, _i],
+    "BatchUpdatePartialsWithRootLogLikelihood": [_i, _p, _p, _p, _p, _p, _p, _p],
 }
 
 
@@ -675,6 +676,20 @@ class Batch:
         out = np.zeros(len(self.members))
         self._call("BatchCalculateRootLogLikelihoods", _ptr(_i32(bufs)), _ptr(_i32(cw)),
                    _ptr(_i32(sf)), _ptr(_i32(cum)), _ptr(out))
+        self._keep_result(out)
+        return out
+
+    def updatePartialsWithRootLogLikelihood(self, ops, cumulative, roots, cw, sf):
+        """beagleB200BatchUpdatePartialsWithRootLogLikelihood: per member the
+        post-order ops, the cumulative scale buffer (reset, then the list's
+        scale buffers added; -1 for none) and the root lnL; returns the lnL
+        array (filled at wait() for ASYNCH members)."""
+        ot, k1 = self._ptrs([np.asarray(o).reshape(-1) for o in ops], np.int32)
+        cnt = _i32([np.asarray(o).size // 7 for o in ops])
+        out = np.zeros(len(self.members))
+        self._call("BatchUpdatePartialsWithRootLogLikelihood", ot, _ptr(cnt),
+                   _ptr(_i32(cumulative)), _ptr(_i32(roots)), _ptr(_i32(cw)), _ptr(_i32(sf)),
+                   _ptr(out))
         self._keep_result(out)
         return out
 

@@ -531,6 +531,17 @@ int beagleB200BatchCalculateRootLogLikelihoods(int batch, const int* bufs, const
     });
 }
 
+int beagleB200BatchUpdatePartialsWithRootLogLikelihood(int batch, const int* const* ops,
+                                                        const int* counts, const int* cumulative,
+                                                        const int* roots, const int* cw,
+                                                        const int* sf, double* out) {
+    if (!ops || !counts || !cumulative || !roots || !cw || !sf || !out)
+        return BEAGLE_B200_ERROR_OUT_OF_RANGE;
+    return call_batch(batch, [&](b200::Batch* b) {
+        return b->postRoot(ops, counts, cumulative, roots, cw, sf, out);
+    });
+}
+
 int beagleB200BatchCalculateEdgeDerivatives(int batch, const int* const* post,
                                             const int* const* pre, const int* const* dmat,
                                             const int* cw, const int* counts,

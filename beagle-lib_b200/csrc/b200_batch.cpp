@@ -557,6 +557,145 @@ int Batch::rootLogLikelihoods(const int* bufs, const int* cw, const int* sf, con
     return nan ? kErrFP : kSuccess;
 }
 
+// ---------------------------------- post-order walk + scaling + root lnL
+// Per member, updatePartialsWithRootLogLikelihood (Instance:: semantics):
+// updatePartials(ops, NONE); with a cumulative buffer, resetScaleFactors on
+// it and accumulateScaleFactors of the list's scale buffers; then the root
+// lnL.  When every member is a 4-state one with 1, 2, 4 or 8 categories, a
+// list of at least one op ending at its root and not rewriting its
+// cumulative buffer: one k_post4root_batch launch per category count, one
+// final sum for all.  Otherwise the batched calls of the three steps.
+int Batch::postRoot(const int* const* ops, const int* counts, const int* cumulative,
+                    const int* roots, const int* cw, const int* sf, double* out) {
+    const int n = size();
+    bool fused = true;
+    for (int i = 0; i < n; ++i) {
+        Instance* in = m_[i];
+        const int cum = cumulative[i];
+        if (counts[i] < 0 || (counts[i] > 0 && !ops[i])) return kErrRange;
+        if (cum != -1 && (cum < 0 || cum >= in->nscale_)) return kErrRange;
+        bool ok = batched4(in, in->S_, in->C_) && in->Sg_ == 4 && counts[i] >= 1 &&
+                  ops[i][(size_t)(counts[i] - 1) * 7] == roots[i];
+        for (int k = 0; ok && cum >= 0 && k < counts[i]; ++k)
+            if (ops[i][(size_t)k * 7 + 1] == cum) ok = false;   // rewrites the cumulative buffer
+        fused = fused && ok;
+    }
+    if (!fused) {
+        std::vector<int> none(n, -1);
+        int rc = updatePartials(ops, counts, none.data(), false);
+        if (rc) return rc;
+        std::vector<std::vector<int>> written(n);
+        bool any = false, all = true;
+        for (int i = 0; i < n; ++i) {
+            any = any || cumulative[i] >= 0;
+            all = all && cumulative[i] >= 0;
+            for (int k = 0; k < counts[i]; ++k)
+                if (ops[i][(size_t)k * 7 + 1] >= 0) written[i].push_back(ops[i][(size_t)k * 7 + 1]);
+        }
+        if (any && all) {
+            std::vector<const int*> ip(n);
+            std::vector<int> cnt(n);
+            for (int i = 0; i < n; ++i) {
+                ip[i] = written[i].data();
+                cnt[i] = (int)written[i].size();
+            }
+            rc = accumulateScaleFactors(ip.data(), cnt.data(), cumulative, 1);
+            if (rc) return rc;
+        } else if (any) {
+            for (int i = 0; i < n; ++i) {
+                if (cumulative[i] < 0) continue;
+                rc = m_[i]->resetScaleFactors(cumulative[i], -1);
+                if (!rc)
+                    rc = m_[i]->accumulateScaleFactors(written[i].data(), (int)written[i].size(),
+                                                       cumulative[i], 1.0, -1);
+                if (rc) return rc;
+            }
+        }
+        return rootLogLikelihoods(roots, cw, sf, cumulative, out);
+    }
+    struct Member {
+        int i;
+        size_t off;
+    };
+    std::map<int, std::vector<Member>> groups;   // C -> members
+    std::vector<unsigned char> table;
+    for (int i = 0; i < n; ++i) {
+        Instance* in = m_[i];
+        const int w = cw[i], f = sf[i];
+        if (!in->buf_ok(roots[i]) || w < 0 || w >= in->neig_ || !in->catw_set_[w] || f < 0 ||
+            f >= in->neig_ || !in->freqs_set_[f])
+            return kErrRange;
+        std::vector<OpDesc> tab;
+        std::vector<uint8_t> dep;
+        bool idem = true, has_cum = false;
+        const int rc = in->build_walk(ops[i], counts[i], 7, false, tab, dep, idem, has_cum);
+        if (rc) return rc;
+        groups[in->C_].push_back(Member{i, append(table, tab)});
+    }
+    CK(t_a_.upload(table.data(), table.size(), stream_));
+    size_t blocks = 0;
+    for (int i = 0; i < n; ++i) blocks += (size_t)post_root_blocks(m_[i]->dims());
+    CK(t_block_.reserve(sizeof(double) * std::max<size_t>(blocks, 1)));
+    CK(t_out_.reserve(sizeof(double) * n));
+    struct G {
+        int C;
+        size_t off;
+        int nseg;
+        int ncta;
+    };
+    std::vector<G> gl;
+    std::vector<unsigned char> segtab;
+    std::vector<FinalSeg> fin(n);
+    size_t boff = 0;
+    for (auto& kv : groups) {
+        const int C = kv.first;
+        std::vector<PostRootSeg> segs;
+        int cta = 0;
+        for (const Member& mb : kv.second) {
+            Instance* in = m_[mb.i];
+            PostRootSeg sg{};
+            sg.ops = (const OpDesc*)((unsigned char*)t_a_.ptr + mb.off);
+            sg.cum = cumulative[mb.i] >= 0 ? in->scale(cumulative[mb.i]) : nullptr;
+            sg.catw = in->d_catw_ + (size_t)cw[mb.i] * in->C_;
+            sg.freqs = in->d_freqs_ + (size_t)sf[mb.i] * in->S_;
+            sg.patw = in->d_patw_;
+            sg.site = in->d_site_;
+            sg.block = (double*)t_block_.ptr + boff;
+            sg.nops = counts[mb.i];
+            sg.Pp = in->Pp_;
+            sg.P = in->P_;
+            sg.log_scalers = (int)in->log_scalers_;
+            sg.first_cta = cta;
+            cta += ceil_div(in->Pp_, post_root_batch_patterns(C));
+            segs.push_back(sg);
+            FinalSeg& f = fin[mb.i];
+            f.block = sg.block;
+            f.out = (double*)t_out_.ptr + mb.i;
+            f.nblk = post_root_blocks(in->dims());
+            f.nout = 1;
+            f.first_out = mb.i;
+            boff += (size_t)f.nblk;
+        }
+        gl.push_back(G{C, append(segtab, segs), (int)segs.size(), cta});
+    }
+    const size_t foff = append(segtab, fin);
+    CK(t_b_.upload(segtab.data(), segtab.size(), stream_));
+    for (const G& g : gl)
+        CK(LAUNCH(launch_post4_root_batch, (const PostRootSeg*)((unsigned char*)t_b_.ptr + g.off),
+                  g.nseg, g.ncta, g.C, stream_));
+    CK(launch_final_batch((const FinalSeg*)((unsigned char*)t_b_.ptr + foff), n, n, stream_));
+    double* h = stage(n);
+    if (!h) return kErrOOM;
+    CK(cudaMemcpyAsync(h, t_out_.ptr, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_));
+    for (int i = 0; i < n; ++i) push_pending(Pending{h + i, out + i, 1, i});
+    if (deferred()) return kSuccess;   // delivered by wait()
+    int rc = sync();
+    if (rc) return rc;
+    bool nan = false;
+    for (int i = 0; i < n; ++i) nan = nan || std::isnan(out[i]);
+    return nan ? kErrFP : kSuccess;
+}
+
 // ------------------------------------------------------- edge derivatives
 int Batch::edgeDerivatives(const int* const* post, const int* const* pre,
                            const int* const* dmat, const int* cw, const int* counts,

@@ -11,7 +11,9 @@
 //     count for the 4-state members (k_walk4_batch, k_deriv4_batch); other
 //     members run their own single-instance launch on the shared stream;
 //   * scale accumulation, root pre-partials, root log-likelihoods and the
-//     final derivative sums: one launch for all members.
+//     final derivative sums: one launch for all members;
+//   * the fused post-order walk with scaling and root lnL: one launch per
+//     category count when every member is a 4-state one (k_post4root_batch).
 #pragma once
 #include <cuda_runtime.h>
 #include <vector>
@@ -36,6 +38,8 @@ public:
     int setRootPrePartials(const int* bufs, const int* freqs);
     int rootLogLikelihoods(const int* bufs, const int* cw, const int* sf, const int* cum,
                            double* out);
+    int postRoot(const int* const* ops, const int* counts, const int* cumulative,
+                 const int* roots, const int* cw, const int* sf, double* out);
     int edgeDerivatives(const int* const* post, const int* const* pre,
                         const int* const* dmat, const int* cw, const int* counts,
                         double* const* sums, double* const* sumsq);

@@ -195,6 +195,14 @@ cudaError_t launch_final_sum(const double* d_block, int nblk, int nout, double* 
 // patterns' sums of log scale factors (reset, then accumulated); site lnL into
 // `site`, the weighted total into out[0].  `block` holds post_root_blocks(d)
 // doubles.
+// The same over many 4-state instances (segments as k_walk4_batch; one
+// launch per category count, ncta = the segments' total CTAs, each CTA
+// post_root_batch_patterns(C) patterns; every member's block partials are
+// post_root_blocks of its shape).
+int post_root_batch_patterns(int C);
+template <typename Real>
+cudaError_t launch_post4_root_batch(const PostRootSeg* d_segs, int nseg, int ncta, int C,
+                                    cudaStream_t s);
 int post_root_blocks(const Dims& d);
 template <typename Real>
 cudaError_t launch_post4_root(const OpDesc* h_ops, int nops, const Dims& d, double* cum, int ls,

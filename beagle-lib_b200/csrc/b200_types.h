@@ -180,6 +180,24 @@ struct RootSeg {
     int reserved;
 };
 
+// One instance's fused post-order walk with scale accumulation and root lnL
+// in a batched launch (k_post4root_batch).
+struct PostRootSeg {
+    const OpDesc* ops;
+    double* cum;                // cumulative scale buffer (written once), or null
+    const double* catw;
+    const double* freqs;
+    const double* patw;
+    double* site;               // site log-likelihoods [P]
+    double* block;              // one partial sum per warp
+    int nops;
+    int Pp;
+    int P;
+    int log_scalers;
+    int first_cta;
+    int reserved;
+};
+
 // One instance's scale-factor accumulation (optionally after resetting the
 // cumulative buffer) in a batched launch.
 struct AccSeg {

@@ -773,7 +773,8 @@ k_pre4p(const OpDesc* __restrict__ ops, int nops, int Pp, int log_scalers) {
 // count (one pattern per thread, the shape of variant 1).  CTA x belongs to the
 // instance whose segment holds x; it walks that instance's list for its own
 // patterns, exactly as the single-instance kernel does.
-__device__ __forceinline__ int find_walk_seg(const WalkSeg* segs, int nseg, int x) {
+template <typename Seg>
+__device__ __forceinline__ int find_walk_seg(const Seg* segs, int nseg, int x) {
     int lo = 0, hi = nseg - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
@@ -812,6 +813,74 @@ k_walk4_batch(const WalkSeg* __restrict__ segs, int nseg) {
             walk4st_op<Real, C, PRE, false>(s_ops[k], s_m, k, c, p, valid, PRE ? nullptr : sg.cum,
                                             sg.log_scalers);
     }
+}
+
+// k_post4root over many instances: CTA x walks the op list (device memory)
+// of the segment whose first_cta is the largest one <= x, each chunk's
+// descriptors and matrices staged together as in k_walk4_batch, keeps its
+// patterns' log scale factors in registers and forms their site lnL from the
+// root row; the member's block partials get one sum per warp.
+template <typename Real, int C>
+__global__ void __launch_bounds__(kT4, sizeof(Real) == 4 ? 5 : 1)
+k_post4root_batch(const PostRootSeg* __restrict__ segs, int nseg) {
+    constexpr int K = root_chunk<Real, C>();
+    __shared__ OpDesc s_ops[K];
+    __shared__ __align__(16) Real s_m[K * 2 * C * 16];
+    __shared__ PostRootSeg sg;
+    if (threadIdx.x == 0) sg = segs[find_walk_seg(segs, nseg, blockIdx.x)];
+    __syncthreads();
+    const int c = threadIdx.x % C;
+    const int local = blockIdx.x - sg.first_cta;
+    const int p0 = local * (kT4 / C) + threadIdx.x / C;
+    const int Pp = sg.Pp;
+    const int p = min(p0, Pp - 1);
+    const bool valid = p0 < Pp;
+    const int nops = sg.nops;
+    double acc = 0;
+    for (int o0 = 0; o0 < nops; o0 += K) {
+        const int n = min(K, nops - o0);
+        __syncthreads();
+        stage_ops(s_ops, sg.ops + o0, n);
+        stage_mats<Real, C>(s_m, sg.ops + o0, n);
+        __syncthreads();
+        for (int k = 0; k < n; ++k) {
+            const OpDesc& op = s_ops[k];
+            const bool st1 = op.kind & kX1States, st2 = op.kind & kX2States;
+            Real x1[4], x2[4];
+            int s1 = 0, s2 = 0;
+            if (st1) s1 = static_cast<const int*>(op.x1)[p];
+            else ld4(static_cast<const Real*>(op.x1) + ((size_t)p * C + c) * 4, x1);
+            if (st2) s2 = static_cast<const int*>(op.x2)[p];
+            else ld4(static_cast<const Real*>(op.x2) + ((size_t)p * C + c) * 4, x2);
+            Real y1[4], y2[4];
+            operand4s<Real, C>(s_m, k, 0, c, st1, s1, x1, (Real)op.pad1, y1);
+            operand4s<Real, C>(s_m, k, 1, c, st2, s2, x2, (Real)op.pad2, y2);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) y1[i] *= y2[i];
+            finish4c<Real, C, false>(op, y1, p, valid, c, nullptr, sg.log_scalers, &acc);
+        }
+    }
+    Real x[4];
+    ld4(static_cast<const Real*>(sg.ops[nops - 1].dest) + ((size_t)p * C + c) * 4, x);
+    const double w = sg.catw[c];
+    double l = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) l += sg.freqs[i] * (w * (double)x[i]);
+#pragma unroll
+    for (int o = 1; o < C; o <<= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+    double v = 0;
+    if (c == 0 && p0 < sg.P) {
+        double sl = log(l);
+        if (sg.cum) {
+            sl += acc;
+            sg.cum[p0] = acc;
+        }
+        sg.site[p0] = sl;
+        v = sl * sg.patw[p0];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) sg.block[(size_t)local * (kT4 / 32) + threadIdx.x / 32] = v;
 }
 
 // Variants of the S = 4 op walks (chosen per shape by the instance's
@@ -1170,6 +1239,27 @@ cudaError_t launch_update_pre_partials(const OpDesc* ops, int nops, const Dims& 
     }
     return cudaErrorInvalidValue;   // other state counts: k_generic.cu
 }
+
+int post_root_batch_patterns(int C) { return kT4 / C; }
+
+template <typename Real>
+cudaError_t launch_post4_root_batch(const PostRootSeg* d_segs, int nseg, int ncta, int C,
+                                    cudaStream_t s) {
+    if (nseg == 0 || ncta == 0) return cudaSuccess;
+    switch (C) {
+        case 1: k_post4root_batch<Real, 1><<<ncta, kT4, 0, s>>>(d_segs, nseg); break;
+        case 2: k_post4root_batch<Real, 2><<<ncta, kT4, 0, s>>>(d_segs, nseg); break;
+        case 4: k_post4root_batch<Real, 4><<<ncta, kT4, 0, s>>>(d_segs, nseg); break;
+        case 8: k_post4root_batch<Real, 8><<<ncta, kT4, 0, s>>>(d_segs, nseg); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_post4_root_batch<float>(const PostRootSeg*, int, int, int,
+                                                    cudaStream_t);
+template cudaError_t launch_post4_root_batch<double>(const PostRootSeg*, int, int, int,
+                                                     cudaStream_t);
 
 // Batched walk: ncta = segs' total CTAs; C in {1, 2, 4, 8}.
 template <typename Real>

@@ -591,8 +591,10 @@ def batch_gradients(problems, sums, fused):
 def batch_evaluate(batch, problems, lengths=None, fused=False):
     """One lnL + gradient evaluation of every problem of a batch (members in
     the same order), the call sequence of Problem.evaluate with one batched
-    call per step; with ``fused`` the pre-order walk and the derivatives are
-    one beagleB200BatchUpdatePrePartialsWithDerivatives call.  S > 4 members
+    call per step; with ``fused`` the post-order walk, scaling and root lnL
+    are one beagleB200BatchUpdatePartialsWithRootLogLikelihood call and the
+    pre-order walk and the derivatives one
+    beagleB200BatchUpdatePrePartialsWithDerivatives call.  S > 4 members
     need PREORDER_TRANSPOSE_AUTO (their pre-order ops carry untransposed
     matrices).  Returns (lnL[n], [gradient_m] in branch order)."""
     plan = _batch_plan(batch, problems)
@@ -604,11 +606,17 @@ def batch_evaluate(batch, problems, lengths=None, fused=False):
 
 
 def _batch_after_matrices(batch, plan, fused=False):
-    batch.updatePartials(plan["post"], plan["none"])
-    if plan["rescale"]:
-        batch.accumulateScaleFactors(plan["scales"], plan["cums"], reset=True)
-    lnl = batch.calculateRootLogLikelihoods(plan["roots"], plan["zeros"], plan["zeros"],
-                                            plan["cums"])
+    if fused:
+        # the post-order walk, scaling and root lnL as one batched call
+        lnl = batch.updatePartialsWithRootLogLikelihood(plan["post"], plan["cums"],
+                                                        plan["roots"], plan["zeros"],
+                                                        plan["zeros"])
+    else:
+        batch.updatePartials(plan["post"], plan["none"])
+        if plan["rescale"]:
+            batch.accumulateScaleFactors(plan["scales"], plan["cums"], reset=True)
+        lnl = batch.calculateRootLogLikelihoods(plan["roots"], plan["zeros"], plan["zeros"],
+                                                plan["cums"])
     batch.setRootPrePartials(plan["roots_pre"], plan["zeros"])
     if fused:
         sums, _ = batch.updatePrePartialsWithDerivatives(plan["pre"], plan["fnodes"],

@@ -499,6 +499,23 @@ int beagleB200BatchCalculateRootLogLikelihoods(int batch, const int* bufferIndic
                                                const int* stateFrequenciesIndices,
                                                const int* cumulativeScaleIndices,
                                                double* outSumLogLikelihoods);
+/* No beagle.h counterpart: beagleB200UpdatePartialsWithRootLogLikelihood for
+ * every member (operations[i]: counts[i] 7-int post-order operations,
+ * cumulativeScaleIndices[i] or BEAGLE_OP_NONE, rootBufferIndices[i],
+ * categoryWeightsIndices[i], stateFrequenciesIndices[i]); lnL of member i in
+ * outSumLogLikelihoods[i].  When every member is a 4-state instance with 1,
+ * 2, 4 or 8 categories whose list ends at its root: one fused walk per
+ * category count (each pattern's log scale factors summed in a register,
+ * the site lnL formed from the root row); otherwise the batched calls of the
+ * three steps.  Results delivered as beagleB200BatchCalculateRootLogLikelihoods
+ * delivers them. */
+int beagleB200BatchUpdatePartialsWithRootLogLikelihood(int batch, const int* const* operations,
+                                                        const int* counts,
+                                                        const int* cumulativeScaleIndices,
+                                                        const int* rootBufferIndices,
+                                                        const int* categoryWeightsIndices,
+                                                        const int* stateFrequenciesIndices,
+                                                        double* outSumLogLikelihoods);
 /* beagleCalculateEdgeDerivatives for every member (sums only):
  * outSumDerivatives[m][counts[m]], outSumSquaredDerivatives[m][counts[m]]
  * (either may be NULL per member).  Waits for the results, or defers them to

@@ -273,3 +273,50 @@ def test_batch_tc_fused_pair_walk_and_unpaired_lists(b200, pkg, syn, unpaired):
     batch.finalize()
     for x in singles + members:
         x.finalize()
+
+
+@pytest.mark.parametrize("kind", ["all_4state", "mixed"])
+@pytest.mark.parametrize("asynch", [False, True], ids=["synch", "asynch"])
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_batch_post_root_matches_single_instances(b200, pkg, syn, oracle, precision, asynch,
+                                                  kind):
+    """beagleB200BatchUpdatePartialsWithRootLogLikelihood: 4-state members with
+    1, 2, 4 and 8 categories run the batched fused walk (k_post4root_batch);
+    with a 20-state member (or 3 categories) the batch runs the batched calls
+    of the three steps.  lnL and every member's cumulative scale buffer
+    against separate single-instance calls; two members against the oracle."""
+    probs = [syn.make_problem(S=4, N=8 + 9 * k, P=300 + 700 * k, C=(1, 2, 4, 8)[k % 4],
+                              seed=980 + k, rescale=True) for k in range(5)]
+    if kind == "mixed":
+        probs.append(syn.make_problem(S=20, N=9, P=300, C=4, seed=990, rescale=True))
+        probs.append(syn.make_problem(S=4, N=11, P=500, C=3, seed=991, rescale=True))
+    singles = [_create(b200, pr, precision) for pr in probs]
+    ref = []
+    for pr, inst in zip(probs, singles):
+        inst.updateTransitionMatrices(0, np.arange(pr.B, dtype=np.int32), None, None, pr.lengths)
+        inst.updatePartials(pr.post_ops(), -1)
+        inst.resetScaleFactors(pr.cumulative)
+        inst.accumulateScaleFactors(np.arange(pr.N - 1, dtype=np.int32), pr.cumulative)
+        ref.append(inst.calculateRootLogLikelihoods([pr.root], [0], [0], [pr.cumulative]))
+    members = [_create(b200, pr, precision, asynch) for pr in probs]
+    batch = pkg.binding.Batch(b200, members)
+    n = len(probs)
+    batch.updateTransitionMatrices([0] * n, [np.arange(p.B, dtype=np.int32) for p in probs],
+                                   [p.lengths for p in probs])
+    tol = 1e-12 if precision == "double" else TOL[precision]["lnl"]
+    for rep in range(2):
+        lnl = batch.updatePartialsWithRootLogLikelihood(
+            [p.post_ops() for p in probs], [p.cumulative for p in probs],
+            [p.root for p in probs], [0] * n, [0] * n)
+        batch.wait()
+        for k in range(n):
+            assert rel(lnl[k], ref[k]) <= tol, (rep, k, lnl[k], ref[k])
+    for k, (pr, inst, m) in enumerate(zip(probs, singles, members)):
+        a, b = m.getScaleFactors(pr.cumulative), inst.getScaleFactors(pr.cumulative)
+        assert np.max(np.abs(a - b)) <= 1e-12 * max(1.0, np.max(np.abs(b))), k
+    for k in (0, 3):
+        _, lo, _ = run_oracle(oracle, probs[k])
+        assert rel(lnl[k], lo) <= TOL[precision]["lnl"], k
+    batch.finalize()
+    for x in singles + members:
+        x.finalize()
