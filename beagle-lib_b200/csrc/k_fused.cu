@@ -531,6 +531,16 @@ __device__ __forceinline__ void warp_emit_pair(Real va, Real vb, Real wp, int k,
         block[(size_t)((h2 ? nops : 0) + k + (h1 ? 1 : 0)) * nblk + wid] = (double)v;
 }
 
+// L2 prefetch (a hint) of this thread's row of a partials operand, or of its
+// pattern's entry of a tip-state array.
+template <typename Real, int C>
+__device__ __forceinline__ void prefetch_row(const void* x, bool states, int pc, int c) {
+    const void* a = states ? static_cast<const void*>(static_cast<const int*>(x) + pc)
+                           : static_cast<const void*>(static_cast<const Real*>(x) +
+                                                      ((size_t)pc * C + c) * 4);
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+}
+
 template <typename Real, int C>
 __global__ void __launch_bounds__(kT4, sizeof(Real) == 4 ? 4 : 2)
 k_pre_deriv4s(const __grid_constant__ FusedParams F, int nops, int P, int Pp,
@@ -557,6 +567,16 @@ k_pre_deriv4s(const __grid_constant__ FusedParams F, int nops, int P, int Pp,
             const PreDerivOp& A = F.op[o0 + k];
             Real pv[4];
             ld4(static_cast<const Real*>(A.parent) + ((size_t)pc * C + c) * 4, pv);
+            {
+                // the next step's post-order operands (written by the post-order
+                // walk long before, so read from DRAM) into L2 a step ahead
+                const int kn = o0 + k + ((A.kind & kPairFirst) ? 2 : 1);
+                if (kn < nops) {
+                    const PreDerivOp& An = F.op[kn];
+                    prefetch_row<Real, C>(An.post, (An.kind & kPostStates) != 0, pc, c);
+                    prefetch_row<Real, C>(An.sib, (An.kind & kX2States) != 0, pc, c);
+                }
+            }
             if (A.kind & kPairFirst) {
                 const PreDerivOp& B = F.op[o0 + k + 1];
                 const bool sta = A.kind & kPostStates, stb = A.kind & kX2States;
