@@ -771,8 +771,13 @@ __device__ __forceinline__ int tc_find_seg(const Seg* segs, int nseg, int q) {
 // BATCH: a launch over several instances with the same S and C (segs); tile
 // q of the grid belongs to the segment whose tiles hold it, and that
 // segment's op list, cumulative buffer and scaler kind replace the arguments.
+// A batched launch of 32 or fewer states runs many waves of CTAs, so it takes
+// 4 CTAs per SM (128 registers): each chain runs a little slower, the SM
+// holds a third more of them (batch256: +2.5 %).  One instance's launch
+// keeps 3, which fit its grid in fewer waves (amino acid, 20k patterns:
+// 4 per SM was slower).
 template <int NP, int KC, bool PRE, bool BATCH>
-__global__ void __launch_bounds__(kTT, 3)
+__global__ void __launch_bounds__(kTT, (BATCH && NP <= 32) ? 4 : 3)
 k_walk_tc(const OpDesc* __restrict__ ops, int nops, int S, int Sg, int C, double* cum,
           int log_scalers, const WalkSeg* __restrict__ segs, int nseg) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
