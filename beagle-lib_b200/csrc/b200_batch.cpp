@@ -48,7 +48,22 @@ Batch::~Batch() {
     for (GraphRec& g : graphs_) free_graph(g);
     for (DevBuf* b : {&t_a_, &t_b_, &t_c_, &t_block_, &t_out_, &t_out2_}) b->release();
     for (auto& c : chunks_) cudaFreeHost(c.first);
+    if (fork_ev_) cudaEventDestroy(fork_ev_);
+    if (join_ev_) cudaEventDestroy(join_ev_);
+    if (side_) cudaStreamDestroy(side_);
     if (stream_) cudaStreamDestroy(stream_);
+}
+
+cudaError_t Batch::fork() {
+    cudaError_t e = cudaEventRecord(fork_ev_, stream_);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(side_, fork_ev_, 0);
+    return e;
+}
+
+cudaError_t Batch::join() {
+    cudaError_t e = cudaEventRecord(join_ev_, side_);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(stream_, join_ev_, 0);
+    return e;
 }
 
 int Batch::create(const std::vector<Instance*>& members) {
@@ -61,6 +76,9 @@ int Batch::create(const std::vector<Instance*>& members) {
         for (size_t j = i + 1; j < members.size(); ++j)
             if (members[i] == members[j]) return kErrRange;
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&join_ev_, cudaEventDisableTiming));
     for (Instance* in : members) {
         const int rc = in->use_stream(stream_);
         if (rc) return rc;
@@ -410,25 +428,39 @@ int Batch::updatePartials(const int* const* ops, const int* counts, const int* c
         gl.push_back(G{C, append(segtab, segs), (int)segs.size(), cta});
     }
     CK(t_b_.upload(segtab.data(), segtab.size(), stream_));
-    for (const G& g : gl)
-        CK(LAUNCH(launch_walk4_batch, (const WalkSeg*)((unsigned char*)t_b_.ptr + g.off), g.nseg,
-                  g.ncta, g.C, pre, stream_));
+    // the tensor-core groups on the second stream, beside the 4-state ones
+    const bool split = !gl.empty() && !tgl.empty();
+    if (split) CK(fork());
+    cudaError_t err = cudaSuccess;
+    std::vector<const TG*> late;   // tensor-core shapes that cannot launch here
     for (const TG& g : tgl) {
-        cudaError_t e = launch_walk_tc_batch((const WalkSeg*)((unsigned char*)t_b_.ptr + g.off),
-                                             g.nseg, g.ntiles, pre, g.d, stream_);
+        const cudaError_t e = launch_walk_tc_batch(
+            (const WalkSeg*)((unsigned char*)t_b_.ptr + g.off), g.nseg, g.ntiles, pre, g.d,
+            split ? side_ : stream_);
         if (e == cudaErrorInvalidConfiguration) {
-            // the tensor-core shape cannot launch here: the members' own walks
             (void)cudaGetLastError();
-            for (int i : g.members) {
-                const int rc = m_[i]->post_or_pre(ops[i], counts[i], 7,
-                                                  cumulative ? cumulative[i] : -1, pre);
-                if (rc) return rc;
-            }
+            late.push_back(&g);
             continue;
         }
-        CK(e);
+        if (e != cudaSuccess) err = e;
         for (int i : g.members) m_[i]->tc_used_ = true;
     }
+    for (const G& g : gl) {
+        if (err != cudaSuccess) break;
+        err = LAUNCH(launch_walk4_batch, (const WalkSeg*)((unsigned char*)t_b_.ptr + g.off),
+                     g.nseg, g.ncta, g.C, pre, stream_);
+    }
+    if (split) {
+        const cudaError_t e = join();
+        if (err == cudaSuccess) err = e;
+    }
+    CK(err);
+    for (const TG* g : late)   // the members' own walks
+        for (int i : g->members) {
+            const int rc = m_[i]->post_or_pre(ops[i], counts[i], 7,
+                                              cumulative ? cumulative[i] : -1, pre);
+            if (rc) return rc;
+        }
     return kSuccess;
 }
 
@@ -1013,28 +1045,41 @@ int Batch::preDerivatives(const int* const* ops, const int* counts, const int* c
     }
     const size_t foff = append(segtab, fin);
     CK(t_b_.upload(segtab.data(), segtab.size(), stream_));
-    for (const G& g : gl)
-        CK(LAUNCH(launch_pre_deriv4_batch, (const PreDerivSeg*)((unsigned char*)t_b_.ptr + g.off),
-                  g.nseg, g.ncta, g.C, stream_));
+    // the tensor-core groups on the second stream, beside the 4-state ones
+    const bool split = !gl.empty() && !tgl.empty();
+    if (split) CK(fork());
+    cudaStream_t ts = split ? side_ : stream_;
+    cudaError_t err = cudaSuccess;
     std::vector<int> late;   // tensor-core groups that cannot launch here: own calls
     for (const TG& g : tgl) {
         // the sibling-pair form where every member's list is made of pairs
         // and the width has it (17 to 32 padded states), else the op walk
         const PreDerivSeg* segs = (const PreDerivSeg*)((unsigned char*)t_b_.ptr + g.off);
         cudaError_t e = cudaErrorInvalidValue;
-        if (g.pairs) e = launch_prederiv_tc_pairs_batch(segs, g.nseg, g.ntiles, g.d, stream_);
+        if (g.pairs) e = launch_prederiv_tc_pairs_batch(segs, g.nseg, g.ntiles, g.d, ts);
         if (e == cudaErrorInvalidValue) {
             (void)cudaGetLastError();
-            e = launch_prederiv_tc_batch(segs, g.nseg, g.ntiles, g.d, stream_);
+            e = launch_prederiv_tc_batch(segs, g.nseg, g.ntiles, g.d, ts);
         }
         if (e == cudaErrorInvalidConfiguration) {
             (void)cudaGetLastError();
             late.insert(late.end(), g.members.begin(), g.members.end());
             continue;
         }
-        CK(e);
+        if (e != cudaSuccess) err = e;
         for (int i : g.members) m_[i]->tc_used_ = true;
     }
+    for (const G& g : gl) {
+        if (err != cudaSuccess) break;
+        err = LAUNCH(launch_pre_deriv4_batch,
+                     (const PreDerivSeg*)((unsigned char*)t_b_.ptr + g.off), g.nseg, g.ncta, g.C,
+                     stream_);
+    }
+    if (split) {
+        const cudaError_t e = join();
+        if (err == cudaSuccess) err = e;
+    }
+    CK(err);
     CK(launch_final_batch((const FinalSeg*)((unsigned char*)t_b_.ptr + foff), (int)fin.size(),
                           (int)ooff, stream_));
     double* h = stage(ooff);

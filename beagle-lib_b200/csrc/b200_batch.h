@@ -14,6 +14,8 @@
 //     final derivative sums: one launch for all members;
 //   * the fused post-order walk with scaling and root lnL: one launch per
 //     category count when every member is a 4-state one (k_post4root_batch).
+// Within the walk calls the tensor-core groups' launches run on a second
+// stream beside the 4-state groups' (fork / join around them).
 #pragma once
 #include <cuda_runtime.h>
 #include <vector>
@@ -102,6 +104,14 @@ private:
 
     std::vector<Instance*> m_;
     cudaStream_t stream_ = nullptr;
+    // A second stream for the tensor-core groups' launches of a call, so that
+    // they run beside the 4-state groups' (fork: it waits for everything the
+    // batch's stream has queued; join: the batch's stream waits for it).
+    // Under capture the two become parallel branches of the graph.
+    cudaStream_t side_ = nullptr;
+    cudaEvent_t fork_ev_ = nullptr, join_ev_ = nullptr;
+    cudaError_t fork();
+    cudaError_t join();
     int device_ = 0;
     bool dbl_ = false;
     DevBuf t_a_, t_b_, t_c_, t_block_, t_out_;   // per-call tables and scratch
